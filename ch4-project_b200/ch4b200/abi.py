@@ -1,0 +1,110 @@
+"""ctypes mirror of the C ABI declared in include/ch4.h (types and flag bits only).
+
+The reference solver is configured by compile-time flags (src/define.h) and the
+`prop` record filled from param.in (src/typedef.h:75-224, src/parameters.c:41-811);
+`Config` is that record for the implemented hot path.
+"""
+import ctypes as C
+
+NPOP = 19
+NK = 6
+
+OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_PARAM, ERR_UNSUPPORTED, ERR_NUMERIC, ERR_TIMEOUT, ERR_STATE = range(9)
+STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_PARAM",
+                5: "ERR_UNSUPPORTED", 6: "ERR_NUMERIC", 7: "ERR_TIMEOUT", 8: "ERR_STATE"}
+
+STORE_F64, STORE_F32, STORE_F16 = 0, 1, 2
+T0_MEAN, T0_REF, T0_TOP, T0_BOT = 0, 1, 2, 3
+
+# flag bits, same values as include/ch4.h (names are the define.h flags)
+FLAGS = {
+    "LB_FLUID": 1 << 0,
+    "LB_FLUID_FORCING": 1 << 1,
+    "LB_FLUID_FORCING_KOLMOGOROV": 1 << 2,
+    "LB_FLUID_FORCING_POISEUILLE": 1 << 3,
+    "LB_FLUID_FORCING_HIT": 1 << 4,
+    "LB_FLUID_FORCING_NOZEROMODE": 1 << 5,
+    "LB_TEMPERATURE": 1 << 6,
+    "LB_TEMPERATURE_BUOYANCY": 1 << 7,
+    "LB_SCALAR": 1 << 8,
+    "LB_SCALAR_BUOYANCY": 1 << 9,
+    "LB_FLUID_BC_Y": 1 << 10,
+    "LB_FLUID_BC_Y_P_SLIP": 1 << 11,
+    "LB_FLUID_BC_Y_M_SLIP": 1 << 12,
+    "LB_TEMPERATURE_BC_Y": 1 << 13,
+    "LB_TEMPERATURE_BC_Y_P_FLUX": 1 << 14,
+    "LB_TEMPERATURE_BC_Y_M_FLUX": 1 << 15,
+    "LB_TEMPERATURE_BC_Y_P_NOFLUX": 1 << 16,
+    "LB_TEMPERATURE_BC_Y_M_NOFLUX": 1 << 17,
+    "LB_SCALAR_BC_Y": 1 << 18,
+    "LB_FLUID_LES": 1 << 19,
+    "LAGRANGE": 1 << 20,
+    "LAGRANGE_GRADIENT": 1 << 21,
+    "LAGRANGE_ADDEDMASS": 1 << 22,
+    "LAGRANGE_TWOWAY": 1 << 23,
+    "LAGRANGE_TWOWAY_MOMENTUM": 1 << 24,
+    "LB_TEMPERATURE_FORCING": 1 << 25,
+    "LAGRANGE_WRAP": 1 << 26,
+    "LAGRANGE_GRADIENT_BRD2": 1 << 27,
+}
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("NX", C.c_int), ("NY", C.c_int), ("NZ", C.c_int),
+        ("flags", C.c_uint64),
+        ("t0_kind", C.c_int),
+        ("storage", C.c_int),
+        ("SX", C.c_double), ("SY", C.c_double), ("SZ", C.c_double),
+        ("time_dt", C.c_double),
+        ("tau_u", C.c_double), ("nu", C.c_double),
+        ("Amp_x", C.c_double), ("Amp_y", C.c_double), ("Amp_z", C.c_double),
+        ("gravity_x", C.c_double), ("gravity_y", C.c_double), ("gravity_z", C.c_double),
+        ("tau_t", C.c_double), ("kappa", C.c_double),
+        ("T_bot", C.c_double), ("T_top", C.c_double), ("T_ref", C.c_double), ("deltaT", C.c_double),
+        ("grad_T_bot", C.c_double), ("grad_T_top", C.c_double),
+        ("beta_t", C.c_double), ("beta2_t", C.c_double),
+        ("tau_s", C.c_double), ("chi", C.c_double),
+        ("S_bot", C.c_double), ("S_top", C.c_double), ("S_ref", C.c_double), ("deltaS", C.c_double),
+        ("beta_s", C.c_double),
+        ("C_smag", C.c_double),
+        ("time_dt_lagr_factor", C.c_double),
+        ("particle_number", C.c_int),
+        ("seed", C.c_uint64),
+    ]
+
+
+PARTICLE_FIELDS = [
+    "name", "tau_drag", "beta_coeff",
+    "x", "y", "z", "vx", "vy", "vz", "vx_old", "vy_old", "vz_old",
+    "ax", "ay", "az", "ax_old", "ay_old", "az_old",
+    "ux", "uy", "uz", "ux_old", "uy_old", "uz_old",
+    "dx_ux", "dy_ux", "dz_ux", "dx_uy", "dy_uy", "dz_uy", "dx_uz", "dy_uz", "dz_uz",
+    "Dt_ux", "Dt_uy", "Dt_uz",
+    "t", "t_old", "dt_t", "Dt_t",
+    "dx_t", "dy_t", "dz_t",
+]
+
+
+class Particle(C.Structure):
+    _fields_ = [(n, C.c_double) for n in PARTICLE_FIELDS]
+
+
+AVERAGE_FIELDS = ["rho", "ux", "uy", "uz", "ux2", "uy2", "uz2", "ene", "eps",
+                  "t", "t2", "epst", "dxt", "dyt", "dzt", "uxt", "uyt", "uzt", "nux", "nuy", "nuz",
+                  "s", "s2"]
+
+
+class Averages(C.Structure):
+    _fields_ = [(n, C.c_double) for n in AVERAGE_FIELDS]
+
+
+def flags_of(names):
+    v = 0
+    for n in names:
+        v |= FLAGS[n]
+    return v
+
+
+def set_flag_names(flags):
+    return [n for n, b in FLAGS.items() if flags & b]

@@ -1,0 +1,217 @@
+/*
+ * ch4.h -- C ABI of the B200 lattice-Boltzmann + Lagrangian-particle time step.
+ *
+ * The reference solver has no plugin/FFI layer: its "API" is the driver call
+ * sequence of src/main.c:3-196 on global arrays, configured by the compile-time
+ * flags of src/define.h and the runtime keys of param.in.  Each entry point
+ * below replaces one piece of that sequence (cited per function) and keeps the
+ * reference's data layout at the boundary: populations are exchanged as the
+ * reference's AoS `pop` records (src/typedef.h:66-68, NPOP=19 doubles per cell)
+ * in its halo-padded index order IDX(i,j,k) = (k*(LNY+2BRD)+j)*(LNX+2BRD)+i
+ * (src/typedef.h:342) with a caller-chosen halo width `brd` (0 = interior only).
+ *
+ * Conventions: every function returns a ch4_status (0 = success); nothing
+ * calls exit().  A handle is not thread-safe; each handle owns one CUDA stream
+ * and its device buffers; the caller owns all host buffers.
+ */
+#ifndef CH4_B200_H
+#define CH4_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CH4_OK = 0,
+  CH4_ERR_ARG = 1,         /* bad argument (NULL, size, unknown name) */
+  CH4_ERR_CUDA = 2,        /* CUDA runtime error (message in ch4_last_error) */
+  CH4_ERR_NOMEM = 3,       /* device or host allocation failed / admission refused */
+  CH4_ERR_PARAM = 4,       /* param.in key missing or file unreadable (src/parameters.c:15-35) */
+  CH4_ERR_UNSUPPORTED = 5, /* define.h flag outside the implemented hot path */
+  CH4_ERR_NUMERIC = 6,     /* non-finite value detected by the watchdog */
+  CH4_ERR_TIMEOUT = 7,     /* a bounded device-side wait gave up */
+  CH4_ERR_STATE = 8        /* call out of order (e.g. step before initialize) */
+} ch4_status;
+
+/* storage of the populations on the device; arithmetic is FP64 for CH4_STORE_F64
+ * and FP32 otherwise.  F16 stores the deviation f_i - w_i*rho0 as IEEE half. */
+typedef enum { CH4_STORE_F64 = 0, CH4_STORE_F32 = 1, CH4_STORE_F16 = 2 } ch4_storage;
+
+/* Compile-time flags of src/define.h that the hot path implements (bit set). */
+enum {
+  CH4_F_LB_FLUID = 1ull << 0,
+  CH4_F_LB_FLUID_FORCING = 1ull << 1,
+  CH4_F_FORCING_KOLMOGOROV = 1ull << 2,    /* src/forcing.c:390-400 */
+  CH4_F_FORCING_POISEUILLE = 1ull << 3,    /* src/forcing.c:365-370 */
+  CH4_F_FORCING_HIT = 1ull << 4,           /* src/forcing.c:576-588, phases 36-79 */
+  CH4_F_FORCING_NOZEROMODE = 1ull << 5,    /* src/forcing.c:1123-1152 */
+  CH4_F_LB_TEMPERATURE = 1ull << 6,
+  CH4_F_TEMPERATURE_BUOYANCY = 1ull << 7,  /* src/forcing.c:620-667 */
+  CH4_F_LB_SCALAR = 1ull << 8,
+  CH4_F_SCALAR_BUOYANCY = 1ull << 9,       /* src/forcing.c:696-707 */
+  CH4_F_FLUID_BC_Y = 1ull << 10,           /* no-slip bounce-back, src/boundary_conditions.c:775,798 */
+  CH4_F_FLUID_BC_Y_P_SLIP = 1ull << 11,    /* src/boundary_conditions.c:751-753 */
+  CH4_F_FLUID_BC_Y_M_SLIP = 1ull << 12,    /* src/boundary_conditions.c:784-786 */
+  CH4_F_TEMPERATURE_BC_Y = 1ull << 13,     /* fixed T walls, src/boundary_conditions.c:966-1081 */
+  CH4_F_TEMPERATURE_BC_Y_P_FLUX = 1ull << 14,
+  CH4_F_TEMPERATURE_BC_Y_M_FLUX = 1ull << 15,
+  CH4_F_TEMPERATURE_BC_Y_P_NOFLUX = 1ull << 16,
+  CH4_F_TEMPERATURE_BC_Y_M_NOFLUX = 1ull << 17,
+  CH4_F_SCALAR_BC_Y = 1ull << 18,          /* fixed S walls, src/boundary_conditions.c:1249-1380 */
+  CH4_F_FLUID_LES = 1ull << 19,            /* Smagorinsky, src/les.c:5-269 */
+  CH4_F_LAGRANGE = 1ull << 20,             /* src/lagrange.c */
+  CH4_F_LAGRANGE_GRADIENT = 1ull << 21,
+  CH4_F_LAGRANGE_ADDEDMASS = 1ull << 22,
+  CH4_F_LAGRANGE_TWOWAY = 1ull << 23,      /* src/lagrange_feedback.c:11-256 */
+  CH4_F_LAGRANGE_TWOWAY_MOMENTUM = 1ull << 24,
+  CH4_F_TEMPERATURE_FORCING = 1ull << 25,  /* t_source (plain source term), src/forcing.c:769,1475 */
+  CH4_F_LAGRANGE_WRAP = 1ull << 26,
+  CH4_F_LAGRANGE_GRADIENT_BRD2 = 1ull << 27
+};
+
+/* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
+typedef enum {
+  CH4_T0_MEAN = 0, /* default: 0.5*(T_bot+T_top) */
+  CH4_T0_REF = 1,  /* LB_TEMPERATURE_BUOYANCY_T0_REF */
+  CH4_T0_TOP = 2,  /* LB_TEMPERATURE_BUOYANCY_T0_TOP */
+  CH4_T0_BOT = 3   /* LB_TEMPERATURE_BUOYANCY_T0_BOT */
+} ch4_t0_kind;
+
+/* Compile-time flags + the `prop` record of src/typedef.h:75-224 that the hot
+ * path reads (names follow the param.in keys). */
+typedef struct {
+  int NX, NY, NZ;
+  uint64_t flags;   /* CH4_F_* bits */
+  int t0_kind;      /* ch4_t0_kind */
+  int storage;      /* ch4_storage */
+  double SX, SY, SZ;
+  double time_dt;
+  /* fluid */
+  double tau_u, nu;
+  double Amp_x, Amp_y, Amp_z;
+  double gravity_x, gravity_y, gravity_z;
+  /* temperature */
+  double tau_t, kappa;
+  double T_bot, T_top, T_ref, deltaT;
+  double grad_T_bot, grad_T_top;
+  double beta_t, beta2_t;
+  /* scalar */
+  double tau_s, chi;
+  double S_bot, S_top, S_ref, deltaS;
+  double beta_s;
+  /* LES: Smagorinsky constant (the reference hard-codes 0.18, src/les.c:10) */
+  double C_smag;
+  /* Lagrangian */
+  double time_dt_lagr_factor;
+  int particle_number;
+  /* drand48 seed of the host RNG (HIT phases), src/parallel.c:237-240 */
+  uint64_t seed;
+} ch4_config;
+
+/* One Lagrangian particle (the fields of point_particle, src/typedef.h:391-481,
+ * that the hot path reads or writes). */
+typedef struct {
+  double name, tau_drag, beta_coeff;
+  double x, y, z;
+  double vx, vy, vz;
+  double vx_old, vy_old, vz_old;
+  double ax, ay, az;
+  double ax_old, ay_old, az_old;
+  double ux, uy, uz;
+  double ux_old, uy_old, uz_old;
+  double dx_ux, dy_ux, dz_ux, dx_uy, dy_uy, dz_uy, dx_uz, dy_uz, dz_uz;
+  double Dt_ux, Dt_uy, Dt_uz;
+  double t, t_old, dt_t, Dt_t;
+  double dx_t, dy_t, dz_t;
+} ch4_particle;
+
+/* Global averages of dump_averages (src/output.c:63-~760), FP64 sums over the
+ * lattice normalised by SX*SY*SZ. */
+typedef struct {
+  double rho, ux, uy, uz, ux2, uy2, uz2, ene, eps;
+  double t, t2, epst, dxt, dyt, dzt, uxt, uyt, uzt, nux, nuy, nuz;
+  double s, s2;
+} ch4_averages;
+
+typedef struct ch4_handle ch4_handle;
+
+/* --- configuration (host only, no GPU needed) --------------------------- */
+
+/* Fill defaults (D3Q19 fluid, FP64 storage, C_smag 0.18, seed 1). */
+ch4_status ch4_config_default(ch4_config *cfg);
+
+/* Read the active `#define` lines of a define.h file into cfg->flags (replaces
+ * the compile-time configuration of src/define.h).  Flags outside the hot path
+ * give CH4_ERR_UNSUPPORTED with the flag's name in *bad (may be NULL). */
+ch4_status ch4_config_read_define(ch4_config *cfg, const char *define_h_path, char *bad, size_t bad_len);
+
+/* Read param.in with the reference's semantics (src/parameters.c:3-39: a
+ * whole-file rescan per key that takes the first number after the key) and
+ * derive nu, kappa, chi, deltaT as assign_parameters does
+ * (src/parameters.c:41-811).  A missing key gives CH4_ERR_PARAM and its name in *bad. */
+ch4_status ch4_config_read_param(ch4_config *cfg, const char *param_in_path, char *bad, size_t bad_len);
+
+/* Single key lookup with the read_parameter scan (src/parameters.c:3-39). */
+ch4_status ch4_read_parameter(const char *param_in_path, const char *key, double *value);
+
+/* --- lifetime -------------------------------------------------------------- */
+
+/* Allocate the device state (replaces allocate_fields, src/parameters.c:917,
+ * and allocate_particles, src/lagrange.c:6).  Populations start at the
+ * rest equilibrium p_i = w_i (src/initial_conditions.c:45), g = h = 0. */
+ch4_status ch4_create(const ch4_config *cfg, ch4_handle **out);
+ch4_status ch4_destroy(ch4_handle *h);
+const char *ch4_last_error(const ch4_handle *h);
+
+/* Bytes of device memory ch4_create would allocate for cfg (admission control). */
+ch4_status ch4_device_bytes(const ch4_config *cfg, size_t *bytes);
+
+/* --- state exchange (drop-in for the pop arrays and the restart path,
+ *     src/output_h5.c:347-728 write/read_pop_h5) ---------------------------- */
+
+/* which = 'p' (fluid), 'g' (temperature), 'h' (scalar). */
+ch4_status ch4_set_pop(ch4_handle *h, char which, const double *aos, int brd);
+ch4_status ch4_get_pop(ch4_handle *h, char which, double *aos, int brd);
+
+/* HIT forcing phases phi_u[nk] (nk = 6 vectors, src/initial_conditions.c:834-870). */
+ch4_status ch4_set_hit_phases(ch4_handle *h, const double *phi);
+ch4_status ch4_get_hit_phases(ch4_handle *h, double *phi);
+
+/* Particles (src/lagrange.c:72 initial_conditions_particles / part.h5). */
+ch4_status ch4_set_particles(ch4_handle *h, const ch4_particle *parts, int n);
+ch4_status ch4_get_particles(ch4_handle *h, ch4_particle *parts, int n);
+
+/* --- the time step ---------------------------------------------------------- */
+
+/* First reconstruction of the hydrodynamic fields and forcing, src/main.c:24-48:
+ * hydro_fields, build_forcing, hydro_fields. */
+ch4_status ch4_initialize(ch4_handle *h);
+
+/* nsteps iterations of the src/main.c:67-196 loop body: collision, forcing,
+ * boundary conditions, streaming, hydro fields and (with CH4_F_LAGRANGE) the
+ * particle sub-steps.  Asynchronous with respect to the host. */
+ch4_status ch4_step(ch4_handle *h, int nsteps);
+
+/* Wait for the handle's stream. */
+ch4_status ch4_synchronize(ch4_handle *h);
+
+/* Hydrodynamic fields as after hydro_fields (src/lb.c:420-539): dens, u (3 per
+ * cell), t, s.  Any pointer may be NULL. */
+ch4_status ch4_get_fields(ch4_handle *h, double *dens, double *u, double *t, double *s, int brd);
+
+/* Force field of the last build_forcing (src/forcing.c:5-1246), 3 per cell. */
+ch4_status ch4_get_force(ch4_handle *h, double *force, int brd);
+
+/* Global averages (src/output.c:63-~760) in FP64 from a deterministic device reduction. */
+ch4_status ch4_averages_get(ch4_handle *h, ch4_averages *out);
+
+/* Steps done so far (the reference's itime). */
+ch4_status ch4_get_itime(const ch4_handle *h, int *itime);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,662 @@
+/*
+ * CPU restatement of the reference lattice-Boltzmann time step (ORACLE; test
+ * infrastructure only -- see ch4_oracle.h).
+ *
+ * Formulation.  The reference (src/main.c:67-161, METHOD_STREAMING) runs one
+ * step as: copy rhs=f (src/fluid.c:267-284), BGK collision with the
+ * equilibrium of src/lb.c:382-415, build_forcing (src/forcing.c:5-1246), Guo
+ * forcing (src/forcing.c:1423-1435), halo + wall boundary conditions
+ * (src/boundary_conditions.c:419-1524), pull streaming (src/lb.c:544-584) and
+ * hydro_fields (src/lb.c:420-539).  Here the same arithmetic is written in push
+ * form on halo-free SoA arrays f[q][z][y][x]: each cell collides and sends its
+ * post-collision value rhs_q(x) to x+c_q; a value that would cross a wall is
+ * turned into the value the reference's wall loop writes into the halo slot
+ * the receiving cell pulls from.  Every floating-point expression keeps the
+ * reference's operand order so the result is bit-identical (FP contraction off).
+ *
+ * Force lag (src/main.c:120-160 with src/lb.c:464-466): the velocity of the
+ * equilibrium is u^n = mv(f^n)/rho + dt/2 F^{n-1}, while Guo uses F^n.  F^{n-1}
+ * is rebuilt from the previous temperature t^{n-1} (kept per cell) and the
+ * previous HIT phases.
+ */
+#include "ch4_oracle.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NPOP 19
+#define NK 6
+
+/* D3Q19 tables, src/lb.c:139-230 */
+static const int CX[NPOP] = {0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+static const int CY[NPOP] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
+static const int CZ[NPOP] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, -1, 1, -1};
+static const int INV[NPOP] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
+static const int INV_Y[NPOP] = {0, 1, 2, 4, 3, 5, 6, 8, 7, 10, 9, 11, 12, 13, 14, 17, 18, 15, 16};
+
+struct ch4o_state {
+  ch4_config cfg;
+  int NX, NY, NZ;
+  size_t N;
+  double w[NPOP];
+  double invcs2, invcs4, invtwocs2, invtwocs4;
+  double *f[3], *fn[3]; /* 0: p, 1: g, 2: h */
+  int nsets_on[3];
+  double *tprev, *sprev; /* t^{n-1}, s^{n-1} */
+  double *force;         /* F of the last build_forcing, 3 per cell */
+  double phi_prev[NK][3], phi_cur[NK][3];
+  double hit_fac[NK];
+  unsigned short rng[3];
+  int itime, initialized;
+  /* constant force tables */
+  double *kol_x, *kol_y, *kol_z; /* Kolmogorov: F.x(y), F.y(x), F.z(y) */
+  double pois[3];
+  /* per-step HIT sin tables for the previous and current phases */
+  double *hit_prev, *hit_cur; /* [NK][NX+NY+NZ] */
+  /* LES relaxation time field (src/les.c:266 tau_u_les_total) */
+  double *tau_les;
+  /* particles */
+  int npart;
+  ch4_particle *part;
+};
+
+/* ---- host RNG: drand48 stream (src/random.c:4-16 with SYSTEM_RANDOM48) ---- */
+static void rng_seed(ch4o_state *s, uint64_t seed) {
+  /* srand48(seed): X = seed<<16 | 0x330E */
+  s->rng[0] = 0x330E;
+  s->rng[1] = (unsigned short)(seed & 0xFFFF);
+  s->rng[2] = (unsigned short)((seed >> 16) & 0xFFFF);
+}
+static double myrand(ch4o_state *s) { return erand48(s->rng); }
+
+/* polar Box-Muller, src/random.c:82-100 */
+static double random_gauss(ch4o_state *s, double mu, double sigma) {
+  double U1, U2, W, mult, X1;
+  do {
+    U1 = -1 + ((double)myrand(s)) * 2;
+    U2 = -1 + ((double)myrand(s)) * 2;
+    W = pow(U1, 2) + pow(U2, 2);
+  } while (W >= 1 || W == 0);
+  mult = sqrt((-2 * log(W)) / W);
+  X1 = U1 * mult;
+  return (mu + sigma * (double)X1);
+}
+
+/* HIT phase random walk, src/forcing.c:43-69 */
+static void hit_phase_walk(ch4o_state *s) {
+  double t_turnover = (s->cfg.SX / 0.1);
+  double phi_diffusivity = 0.01 / t_turnover;
+  double fac1 = s->cfg.time_dt / t_turnover;
+  double fac2 = sqrt(2.0 * s->cfg.time_dt * phi_diffusivity);
+  for (int ii = 0; ii < NK; ii++)
+    for (int a = 0; a < 3; a++) {
+      double val = random_gauss(s, 0.0, 1.0);
+      s->phi_cur[ii][a] += -s->phi_cur[ii][a] * fac1 + val * fac2;
+    }
+}
+
+/* HIT modes, src/initial_conditions.c:841-849 */
+static const double VK[NK][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}};
+
+/* sin tables of src/forcing.c:582-584 for one phase set */
+static void hit_tables(ch4o_state *s, double phi[NK][3], double *tab) {
+  const double LX = s->cfg.SX, LY = s->cfg.SY, LZ = s->cfg.SZ;
+  const int L = s->NX + s->NY + s->NZ;
+  for (int ii = 0; ii < NK; ii++) {
+    double *ax = tab + ii * L, *ay = ax + s->NX, *az = ay + s->NY;
+    for (int i = 0; i < s->NX; i++) {
+      double x = (double)i + 0.5;
+      ax[i] = sin(2 * 3.14159265359 * (VK[ii][0] * x / LX + phi[ii][0]));
+    }
+    for (int j = 0; j < s->NY; j++) {
+      double y = (double)j + 0.5;
+      ay[j] = sin(2 * 3.14159265359 * (VK[ii][1] * y / LY + phi[ii][1]));
+    }
+    for (int k = 0; k < s->NZ; k++) {
+      double z = (double)k + 0.5;
+      az[k] = sin(2 * 3.14159265359 * (VK[ii][2] * z / LZ + phi[ii][2]));
+    }
+  }
+}
+
+/* per-cell force of build_forcing's grid loop, src/forcing.c:360-707 */
+static void cell_force(const ch4o_state *s, int i, int j, int k, double t, double sc, const double *hit, double F[3]) {
+  const ch4_config *c = &s->cfg;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  if (c->flags & CH4_F_FORCING_POISEUILLE) { /* src/forcing.c:365-370 */
+    fx += s->pois[0];
+    fy += s->pois[1];
+    fz += s->pois[2];
+  }
+  if (c->flags & CH4_F_FORCING_KOLMOGOROV) { /* src/forcing.c:390-400 */
+    fx += s->kol_x[j];
+    fy += s->kol_y[i];
+    fz += s->kol_z[j];
+  }
+  if (c->flags & CH4_F_FORCING_HIT) { /* src/forcing.c:576-588 */
+    const int L = s->NX + s->NY + s->NZ;
+    for (int ii = 0; ii < NK; ii++) {
+      const double *ax = hit + ii * L, *ay = ax + s->NX, *az = ay + s->NY;
+      double fac = s->hit_fac[ii];
+      fx += fac * c->Amp_x * (ay[j] + az[k]);
+      fy += fac * c->Amp_y * (ax[i] + az[k]);
+      fz += fac * c->Amp_z * (ay[j] + ax[i]);
+    }
+  }
+  if (c->flags & CH4_F_TEMPERATURE_BUOYANCY) { /* src/forcing.c:620-667 */
+    double temp;
+    switch (c->t0_kind) {
+      case CH4_T0_REF: temp = (t - c->T_ref); break;
+      case CH4_T0_TOP: temp = (t - c->T_top); break;
+      case CH4_T0_BOT: temp = (t - c->T_bot); break;
+      default: temp = t - 0.5 * (c->T_bot + c->T_top); break;
+    }
+    double fac = c->beta_t * temp;
+    if (c->beta2_t != 0.0) fac += c->beta2_t * temp * temp;
+    fx += fac * c->gravity_x;
+    fy += fac * c->gravity_y;
+    fz += fac * c->gravity_z;
+  }
+  if (c->flags & CH4_F_SCALAR_BUOYANCY) { /* src/forcing.c:696-707 */
+    double temp = sc - 0.5 * (c->S_bot + c->S_top);
+    double fac = c->beta_s * temp;
+    fx += fac * c->gravity_x;
+    fy += fac * c->gravity_y;
+    fz += fac * c->gravity_z;
+  }
+  F[0] = fx;
+  F[1] = fy;
+  F[2] = fz;
+}
+
+static inline size_t cidx(const ch4o_state *s, int i, int j, int k) {
+  return ((size_t)k * (size_t)s->NY + (size_t)j) * (size_t)s->NX + (size_t)i;
+}
+
+/* m(), mvx(), mvy(), mvz() macros, src/typedef.h:286-291 (fixed summation order) */
+static inline double mom0(const double *a) {
+  return (a[0] + a[1] + a[2] + a[3] + a[4] + a[5] + a[6] + a[7] + a[8] + a[9] + a[10] + a[11] + a[12] + a[13] + a[14] +
+          a[15] + a[16] + a[17] + a[18]);
+}
+static inline double momx(const double *a) {
+  return (a[1] - a[2] + a[7] + a[8] - a[9] - a[10] + a[11] - a[12] + a[13] - a[14]);
+}
+static inline double momy(const double *a) {
+  return (a[3] - a[4] + a[7] - a[8] + a[9] - a[10] + a[15] + a[16] - a[17] - a[18]);
+}
+static inline double momz(const double *a) {
+  return (a[5] - a[6] + a[11] + a[12] - a[13] - a[14] + a[15] - a[16] + a[17] - a[18]);
+}
+
+static void load_cell(const double *f, size_t N, size_t idx, double *a) {
+  for (int q = 0; q < NPOP; q++) a[q] = f[(size_t)q * N + idx];
+}
+
+/* |S| Smagorinsky relaxation time, src/les.c:5-269 with centred differences
+ * of src/gradients.c:78-~240 (one-sided 2nd order at walls) */
+static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k) {
+  const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+  const int walls = (s->cfg.flags & CH4_F_FLUID_BC_Y) != 0;
+  double g[3][3]; /* g[a][b] = d u_a / d x_b  (tens.ab with a=component) */
+  int ip = (i + 1) % NX, im = (i + NX - 1) % NX;
+  int kp = (k + 1) % NZ, km = (k + NZ - 1) % NZ;
+  for (int a = 0; a < 3; a++) {
+    g[a][0] = (u[3 * cidx(s, ip, j, k) + a] - u[3 * cidx(s, im, j, k) + a]) / 2.0;
+    g[a][2] = (u[3 * cidx(s, i, j, kp) + a] - u[3 * cidx(s, i, j, km) + a]) / 2.0;
+  }
+  if (walls && j == 0) {
+    /* h1 = h2 = 1: a0 = -(2+1)/(1*2), a1 = 2/1, a2 = -1/(1*2) */
+    double h1 = 1.0, h2 = 1.0;
+    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
+    for (int a = 0; a < 3; a++)
+      g[a][1] = a0 * u[3 * cidx(s, i, j, k) + a] + a1 * u[3 * cidx(s, i, j + 1, k) + a] +
+                a2 * u[3 * cidx(s, i, j + 2, k) + a];
+  } else if (walls && j == NY - 1) {
+    double h1 = 1.0, h2 = 1.0;
+    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
+    for (int a = 0; a < 3; a++)
+      g[a][1] = a0 * u[3 * cidx(s, i, j, k) + a] + a1 * u[3 * cidx(s, i, j - 1, k) + a] +
+                a2 * u[3 * cidx(s, i, j - 2, k) + a];
+  } else {
+    int jp = (j + 1) % NY, jm = (j + NY - 1) % NY;
+    for (int a = 0; a < 3; a++) g[a][1] = (u[3 * cidx(s, i, jp, k) + a] - u[3 * cidx(s, i, jm, k) + a]) / 2.0;
+  }
+  /* tens.xx = g[0][0], tens.xy = g[0][1] (d ux/dy), tens.yx = g[1][0] ... */
+  double xx = g[0][0], xy = g[0][1], xz = g[0][2];
+  double yx = g[1][0], yy = g[1][1], yz = g[1][2];
+  double zx = g[2][0], zy = g[2][1], zz = g[2][2];
+  double s_norm = sqrt(0.5 * ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) +
+                              (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
+                              (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
+  double vol = 1.0; /* (dx*dy*dz)^(1/3) on the unit lattice */
+  double nu_les = s_norm * pow(s->cfg.C_smag * vol, 2.0);
+  return 3.0 * (nu_les + s->cfg.nu) + 0.5;
+}
+
+/* hydro fields of src/lb.c:420-539 from the current populations and F^{n-1} */
+static void hydro(const ch4o_state *s, const double *hit, double *dens, double *u, double *t, double *sc) {
+  const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+  const size_t N = s->N;
+  const double hdt = 0.5 * s->cfg.time_dt;
+  for (int k = 0; k < NZ; k++)
+    for (int j = 0; j < NY; j++)
+      for (int i = 0; i < NX; i++) {
+        size_t idx = cidx(s, i, j, k);
+        double a[NPOP], F[3];
+        double tprev = s->tprev ? s->tprev[idx] : 0.0, sprev = s->sprev ? s->sprev[idx] : 0.0;
+        cell_force(s, i, j, k, tprev, sprev, hit, F);
+        if (!(s->cfg.flags & CH4_F_LB_FLUID_FORCING)) F[0] = F[1] = F[2] = 0.0;
+        load_cell(s->f[0], N, idx, a);
+        double rho = mom0(a);
+        if (dens) dens[idx] = rho;
+        if (u) {
+          u[3 * idx + 0] = momx(a) / rho + hdt * F[0];
+          u[3 * idx + 1] = momy(a) / rho + hdt * F[1];
+          u[3 * idx + 2] = momz(a) / rho + hdt * F[2];
+        }
+        if (t && s->nsets_on[1]) {
+          load_cell(s->f[1], N, idx, a);
+          t[idx] = mom0(a);
+        }
+        if (sc && s->nsets_on[2]) {
+          load_cell(s->f[2], N, idx, a);
+          sc[idx] = mom0(a);
+        }
+      }
+}
+
+/* one step of src/main.c:67-161 */
+static void one_step(ch4o_state *s) {
+  const ch4_config *c = &s->cfg;
+  const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+  const size_t N = s->N;
+  const int forcing = (c->flags & CH4_F_LB_FLUID_FORCING) != 0;
+  const double hdt = 0.5 * c->time_dt;
+  s->itime++;
+
+  /* build_forcing phase update (src/forcing.c:36-79) */
+  if (c->flags & CH4_F_FORCING_HIT) {
+    memcpy(s->phi_prev, s->phi_cur, sizeof(s->phi_cur));
+    double *tmp = s->hit_prev;
+    s->hit_prev = s->hit_cur;
+    s->hit_cur = tmp;
+    hit_phase_walk(s);
+    hit_tables(s, s->phi_cur, s->hit_cur);
+  }
+
+  /* u^n field (needed by LES gradients, src/fluid.c:1056-1075) */
+  double *uarr = NULL;
+  if (c->flags & CH4_F_FLUID_LES) {
+    uarr = (double *)malloc(sizeof(double) * 3 * N);
+    hydro(s, s->hit_prev, NULL, uarr, NULL, NULL);
+  }
+
+  const double invtau_u = 1.0 / c->tau_u;
+  const double fac_guo = (1.0 - 0.5 * c->time_dt * invtau_u); /* src/forcing.c:1289 */
+  const double invtau_set[3] = {invtau_u, s->nsets_on[1] ? 1.0 / c->tau_t : 0.0, s->nsets_on[2] ? 1.0 / c->tau_s : 0.0};
+
+  for (int k = 0; k < NZ; k++)
+    for (int j = 0; j < NY; j++)
+      for (int i = 0; i < NX; i++) {
+        size_t idx = cidx(s, i, j, k);
+        double a[NPOP], ga[NPOP], ha[NPOP];
+        load_cell(s->f[0], N, idx, a);
+        double rho = mom0(a);
+        double mx = momx(a), my = momy(a), mz = momz(a);
+        double tt = 0.0, ss = 0.0;
+        if (s->nsets_on[1]) {
+          load_cell(s->f[1], N, idx, ga);
+          tt = mom0(ga);
+        }
+        if (s->nsets_on[2]) {
+          load_cell(s->f[2], N, idx, ha);
+          ss = mom0(ha);
+        }
+        double Fp[3] = {0, 0, 0}, Fc[3] = {0, 0, 0};
+        if (forcing) {
+          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_prev, Fp);
+          cell_force(s, i, j, k, tt, ss, s->hit_cur, Fc);
+        }
+        double ux = mx / rho + hdt * Fp[0];
+        double uy = my / rho + hdt * Fp[1];
+        double uz = mz / rho + hdt * Fp[2];
+        s->force[3 * idx + 0] = Fc[0];
+        s->force[3 * idx + 1] = Fc[1];
+        s->force[3 * idx + 2] = Fc[2];
+        double u2 = (ux * ux + uy * uy + uz * uz);
+
+        double invtau = invtau_u;
+        if (c->flags & CH4_F_FLUID_LES) {
+          double tl = les_tau(s, uarr, i, j, k);
+          s->tau_les[idx] = tl;
+          invtau = 1.0 / tl;
+        }
+        double post[3][NPOP];
+        /* fluid: BGK (src/fluid.c:1163,1218) + Guo (src/forcing.c:1423-1435) */
+        for (int q = 0; q < NPOP; q++) {
+          double cu = (CX[q] * ux + CY[q] * uy + CZ[q] * uz);
+          double feq = rho * s->w[q] * (1.0 + s->invcs2 * cu + s->invtwocs4 * cu * cu - s->invtwocs2 * u2);
+          double r = a[q];
+          r += -invtau * (a[q] - feq);
+          if (forcing) {
+            double dx = (CX[q] - ux) * s->invcs2 + CX[q] * cu * s->invcs4;
+            double dy = (CY[q] - uy) * s->invcs2 + CY[q] * cu * s->invcs4;
+            double dz = (CZ[q] - uz) * s->invcs2 + CZ[q] * cu * s->invcs4;
+            r += fac_guo * s->w[q] * rho * Fc[0] * dx;
+            r += fac_guo * s->w[q] * rho * Fc[1] * dy;
+            r += fac_guo * s->w[q] * rho * Fc[2] * dz;
+          }
+          post[0][q] = r;
+        }
+        /* temperature and scalar: BGK with the fluid velocity */
+        for (int set = 1; set < 3; set++) {
+          if (!s->nsets_on[set]) continue;
+          const double *b = set == 1 ? ga : ha;
+          double m0 = set == 1 ? tt : ss;
+          for (int q = 0; q < NPOP; q++) {
+            double cu = (CX[q] * ux + CY[q] * uy + CZ[q] * uz);
+            double feq = m0 * s->w[q] * (1.0 + s->invcs2 * cu + s->invtwocs4 * cu * cu - s->invtwocs2 * u2);
+            double r = b[q];
+            r += -invtau_set[set] * (b[q] - feq);
+            post[set][q] = r;
+          }
+        }
+        /* streaming (push form of src/lb.c:557-572) with the wall rules */
+        for (int set = 0; set < 3; set++) {
+          if (!s->nsets_on[set]) continue;
+          double *out = s->fn[set];
+          int wall = 0, slip_p = 0, slip_m = 0;
+          double fac_top = 0.0, fac_bot = 0.0;
+          if (set == 0) {
+            wall = (c->flags & CH4_F_FLUID_BC_Y) != 0;
+            slip_p = (c->flags & CH4_F_FLUID_BC_Y_P_SLIP) != 0;
+            slip_m = (c->flags & CH4_F_FLUID_BC_Y_M_SLIP) != 0;
+          } else if (set == 1) {
+            wall = (c->flags & CH4_F_TEMPERATURE_BC_Y) != 0;
+            if (wall) { /* src/boundary_conditions.c:966-1081 */
+              double T_wall = c->T_top;
+              if (c->flags & CH4_F_TEMPERATURE_BC_Y_P_FLUX) T_wall = 0.5 * c->grad_T_top + tt + c->T_ref;
+              fac_top = 2.0 * ((T_wall - c->T_ref) - tt);
+              if (c->flags & CH4_F_TEMPERATURE_BC_Y_P_NOFLUX) fac_top = 0.0;
+              T_wall = c->T_bot;
+              if (c->flags & CH4_F_TEMPERATURE_BC_Y_M_FLUX) T_wall = -0.5 * c->grad_T_bot + tt + c->T_ref;
+              fac_bot = 2.0 * ((T_wall - c->T_ref) - tt);
+              if (c->flags & CH4_F_TEMPERATURE_BC_Y_M_NOFLUX) fac_bot = 0.0;
+            }
+          } else {
+            wall = (c->flags & CH4_F_SCALAR_BC_Y) != 0;
+            if (wall) { /* src/boundary_conditions.c:1249-1380 */
+              fac_top = 2.0 * ((c->S_top - c->S_ref) - ss);
+              fac_bot = 2.0 * ((c->S_bot - c->S_ref) - ss);
+            }
+          }
+          for (int q = 0; q < NPOP; q++) {
+            int ty = j + CY[q];
+            int tx = (i + CX[q] + NX) % NX, tz = (k + CZ[q] + NZ) % NZ;
+            if (wall && (ty < 0 || ty >= NY)) {
+              if (set == 0) {
+                int slip = ty >= NY ? slip_p : slip_m;
+                if (slip) /* specular: src/boundary_conditions.c:753,786 */
+                  out[(size_t)INV_Y[q] * N + cidx(s, tx, j, tz)] = post[0][q];
+                else /* no-slip bounce-back: src/boundary_conditions.c:775,798 */
+                  out[(size_t)INV[q] * N + idx] = post[0][q];
+              } else {
+                /* fixed-value walls: the slot pulled as inv[q] holds
+                 * rhs(x).p[inv q] + w[inv q]*fac (src/boundary_conditions.c:1019-1027,1065-1073) */
+                int r = INV[q];
+                double fac = ty >= NY ? fac_top : fac_bot;
+                out[(size_t)r * N + idx] = post[set][r] + s->w[r] * fac;
+              }
+            } else {
+              ty = (ty + NY) % NY;
+              out[(size_t)q * N + cidx(s, tx, ty, tz)] = post[set][q];
+            }
+          }
+        }
+        if (s->tprev) s->tprev[idx] = tt;
+        if (s->sprev) s->sprev[idx] = ss;
+      }
+  for (int set = 0; set < 3; set++) {
+    if (!s->nsets_on[set]) continue;
+    double *tmp = s->f[set];
+    s->f[set] = s->fn[set];
+    s->fn[set] = tmp;
+  }
+  free(uarr);
+}
+
+int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
+  if (!cfg || !out || cfg->NX <= 0 || cfg->NY <= 0 || cfg->NZ <= 0) return CH4_ERR_ARG;
+  ch4o_state *s = (ch4o_state *)calloc(1, sizeof(ch4o_state));
+  s->cfg = *cfg;
+  s->NX = cfg->NX;
+  s->NY = cfg->NY;
+  s->NZ = cfg->NZ;
+  s->N = (size_t)cfg->NX * cfg->NY * cfg->NZ;
+  /* weights and lattice constants, src/lb.c:139-160,368-377 */
+  s->w[0] = 1. / 3.;
+  for (int q = 1; q <= 6; q++) s->w[q] = 1. / 18.;
+  for (int q = 7; q < NPOP; q++) s->w[q] = 1. / 36.;
+  double cs = 1.0 / sqrt(3.0);
+  double cs2 = pow(cs, 2.0), cs4 = pow(cs, 4.0);
+  s->invcs2 = 1.0 / cs2;
+  s->invcs4 = 1.0 / cs4;
+  s->invtwocs2 = 1.0 / (2.0 * cs2);
+  s->invtwocs4 = 1.0 / (2.0 * cs4);
+  s->nsets_on[0] = 1;
+  s->nsets_on[1] = (cfg->flags & CH4_F_LB_TEMPERATURE) != 0;
+  s->nsets_on[2] = (cfg->flags & CH4_F_LB_SCALAR) != 0;
+  for (int set = 0; set < 3; set++) {
+    if (!s->nsets_on[set]) continue;
+    s->f[set] = (double *)calloc((size_t)NPOP * s->N, sizeof(double));
+    s->fn[set] = (double *)calloc((size_t)NPOP * s->N, sizeof(double));
+  }
+  for (size_t idx = 0; idx < s->N; idx++)
+    for (int q = 0; q < NPOP; q++) s->f[0][(size_t)q * s->N + idx] = s->w[q];
+  if (s->nsets_on[1]) s->tprev = (double *)calloc(s->N, sizeof(double));
+  if (s->nsets_on[2]) s->sprev = (double *)calloc(s->N, sizeof(double));
+  s->force = (double *)calloc(3 * s->N, sizeof(double));
+  s->tau_les = (double *)calloc(s->N, sizeof(double));
+  /* constant force tables */
+  const double LX = cfg->SX, LY = cfg->SY, nu = cfg->nu;
+  s->kol_x = (double *)calloc((size_t)s->NY, sizeof(double));
+  s->kol_y = (double *)calloc((size_t)s->NX, sizeof(double));
+  s->kol_z = (double *)calloc((size_t)s->NY, sizeof(double));
+  {
+    double kn = 1.0;
+    double fnx = nu * pow(2 * 3.14159265359 / LX, 2.0);
+    double fny = nu * pow(2 * 3.14159265359 / LY, 2.0);
+    for (int j = 0; j < s->NY; j++) {
+      double y = (double)j + 0.5;
+      s->kol_x[j] = cfg->Amp_x * fny * sin(kn * 2 * 3.14159265359 * y / LY);
+      s->kol_z[j] = cfg->Amp_z * fny * sin(kn * 2 * 3.14159265359 * y / LY);
+    }
+    for (int i = 0; i < s->NX; i++) {
+      double x = (double)i + 0.5;
+      s->kol_y[i] = cfg->Amp_y * fnx * sin(kn * 2 * 3.14159265359 * x / LX);
+    }
+  }
+  s->pois[0] = 2.0 * cfg->Amp_x * ((4. * nu) * pow(LY, -2.0));
+  s->pois[1] = 2.0 * cfg->Amp_y * ((4. * nu) * pow(LX, -2.0));
+  s->pois[2] = 2.0 * cfg->Amp_z * ((4. * nu) * pow(LY, -2.0));
+  /* HIT: modes and initial phases, src/initial_conditions.c:834-870 */
+  const int L = s->NX + s->NY + s->NZ;
+  s->hit_prev = (double *)calloc((size_t)NK * L, sizeof(double));
+  s->hit_cur = (double *)calloc((size_t)NK * L, sizeof(double));
+  rng_seed(s, cfg->seed);
+  if (cfg->flags & CH4_F_FORCING_HIT) {
+    for (int ii = 0; ii < NK; ii++) {
+      double vk2 = VK[ii][0] * VK[ii][0] + VK[ii][1] * VK[ii][1] + VK[ii][2] * VK[ii][2];
+      s->hit_fac[ii] = pow(vk2, -2. / 6.);
+      s->phi_cur[ii][0] = myrand(s);
+      s->phi_cur[ii][1] = myrand(s);
+      s->phi_cur[ii][2] = myrand(s);
+    }
+  }
+  *out = s;
+  return CH4_OK;
+}
+
+int ch4o_destroy(ch4o_state *s) {
+  if (!s) return CH4_OK;
+  for (int set = 0; set < 3; set++) {
+    free(s->f[set]);
+    free(s->fn[set]);
+  }
+  free(s->tprev);
+  free(s->sprev);
+  free(s->force);
+  free(s->tau_les);
+  free(s->kol_x);
+  free(s->kol_y);
+  free(s->kol_z);
+  free(s->hit_prev);
+  free(s->hit_cur);
+  free(s->part);
+  free(s);
+  return CH4_OK;
+}
+
+static int set_index(const ch4o_state *s, char which) {
+  int set = which == 'p' ? 0 : which == 'g' ? 1 : which == 'h' ? 2 : -1;
+  if (set < 0 || !s->nsets_on[set]) return -1;
+  return set;
+}
+
+int ch4o_set_pop(ch4o_state *s, char which, const double *aos, int brd) {
+  int set = set_index(s, which);
+  if (set < 0 || !aos || brd < 0) return CH4_ERR_ARG;
+  const int PX = s->NX + 2 * brd, PY = s->NY + 2 * brd;
+  for (int k = 0; k < s->NZ; k++)
+    for (int j = 0; j < s->NY; j++)
+      for (int i = 0; i < s->NX; i++) {
+        size_t src = (((size_t)(k + brd) * PY + (j + brd)) * PX + (i + brd)) * NPOP;
+        for (int q = 0; q < NPOP; q++) s->f[set][(size_t)q * s->N + cidx(s, i, j, k)] = aos[src + q];
+      }
+  return CH4_OK;
+}
+
+int ch4o_get_pop(ch4o_state *s, char which, double *aos, int brd) {
+  int set = set_index(s, which);
+  if (set < 0 || !aos || brd < 0) return CH4_ERR_ARG;
+  const int PX = s->NX + 2 * brd, PY = s->NY + 2 * brd;
+  for (int k = 0; k < s->NZ; k++)
+    for (int j = 0; j < s->NY; j++)
+      for (int i = 0; i < s->NX; i++) {
+        size_t dst = (((size_t)(k + brd) * PY + (j + brd)) * PX + (i + brd)) * NPOP;
+        for (int q = 0; q < NPOP; q++) aos[dst + q] = s->f[set][(size_t)q * s->N + cidx(s, i, j, k)];
+      }
+  return CH4_OK;
+}
+
+int ch4o_set_hit_phases(ch4o_state *s, const double *phi) {
+  if (!phi) return CH4_ERR_ARG;
+  for (int ii = 0; ii < NK; ii++)
+    for (int a = 0; a < 3; a++) s->phi_cur[ii][a] = phi[3 * ii + a];
+  return CH4_OK;
+}
+
+int ch4o_get_hit_phases(ch4o_state *s, double *phi) {
+  if (!phi) return CH4_ERR_ARG;
+  for (int ii = 0; ii < NK; ii++)
+    for (int a = 0; a < 3; a++) phi[3 * ii + a] = s->phi_cur[ii][a];
+  return CH4_OK;
+}
+
+int ch4o_initialize(ch4o_state *s) {
+  /* src/main.c:24-48: hydro_fields (force = 0), build_forcing (one phase
+   * update), hydro_fields again.  The per-cell t^0 becomes the "previous"
+   * temperature of step 1 and the updated phases its previous phases. */
+  const size_t N = s->N;
+  for (size_t idx = 0; idx < N; idx++) {
+    double a[NPOP];
+    if (s->nsets_on[1]) {
+      load_cell(s->f[1], N, idx, a);
+      s->tprev[idx] = mom0(a);
+    }
+    if (s->nsets_on[2]) {
+      load_cell(s->f[2], N, idx, a);
+      s->sprev[idx] = mom0(a);
+    }
+  }
+  if (s->cfg.flags & CH4_F_FORCING_HIT) {
+    hit_phase_walk(s);
+    hit_tables(s, s->phi_cur, s->hit_cur);
+    memcpy(s->hit_prev, s->hit_cur, sizeof(double) * NK * (s->NX + s->NY + s->NZ));
+    memcpy(s->phi_prev, s->phi_cur, sizeof(s->phi_cur));
+  }
+  /* force field of the initial build_forcing */
+  for (int k = 0; k < s->NZ; k++)
+    for (int j = 0; j < s->NY; j++)
+      for (int i = 0; i < s->NX; i++) {
+        size_t idx = cidx(s, i, j, k);
+        double F[3] = {0, 0, 0};
+        if (s->cfg.flags & CH4_F_LB_FLUID_FORCING)
+          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_cur, F);
+        s->force[3 * idx] = F[0];
+        s->force[3 * idx + 1] = F[1];
+        s->force[3 * idx + 2] = F[2];
+      }
+  s->initialized = 1;
+  return CH4_OK;
+}
+
+int ch4o_step(ch4o_state *s, int nsteps) {
+  if (!s->initialized) return CH4_ERR_STATE;
+  for (int n = 0; n < nsteps; n++) one_step(s);
+  return CH4_OK;
+}
+
+static void scatter_field(const ch4o_state *s, const double *src, int ncomp, double *dst, int brd) {
+  const int PX = s->NX + 2 * brd, PY = s->NY + 2 * brd;
+  for (int k = 0; k < s->NZ; k++)
+    for (int j = 0; j < s->NY; j++)
+      for (int i = 0; i < s->NX; i++) {
+        size_t d = ((size_t)(k + brd) * PY + (j + brd)) * PX + (i + brd);
+        for (int a = 0; a < ncomp; a++) dst[d * ncomp + a] = src[cidx(s, i, j, k) * ncomp + a];
+      }
+}
+
+int ch4o_get_fields(ch4o_state *s, double *dens, double *u, double *t, double *sc, int brd) {
+  const size_t N = s->N;
+  double *d0 = (double *)malloc(sizeof(double) * N), *u0 = (double *)malloc(sizeof(double) * 3 * N);
+  double *t0 = (double *)calloc(N, sizeof(double)), *s0 = (double *)calloc(N, sizeof(double));
+  /* between steps the kept temperature is t^n and the latest phases those of F^n */
+  hydro(s, s->hit_cur, d0, u0, t0, s0);
+  if (dens) scatter_field(s, d0, 1, dens, brd);
+  if (u) scatter_field(s, u0, 3, u, brd);
+  if (t) scatter_field(s, t0, 1, t, brd);
+  if (sc) scatter_field(s, s0, 1, sc, brd);
+  free(d0);
+  free(u0);
+  free(t0);
+  free(s0);
+  return CH4_OK;
+}
+
+int ch4o_get_force(ch4o_state *s, double *force, int brd) {
+  scatter_field(s, s->force, 3, force, brd);
+  return CH4_OK;
+}
+
+int ch4o_set_particles(ch4o_state *s, const ch4_particle *parts, int n) {
+  free(s->part);
+  s->part = (ch4_particle *)malloc(sizeof(ch4_particle) * (size_t)(n > 0 ? n : 1));
+  memcpy(s->part, parts, sizeof(ch4_particle) * (size_t)n);
+  s->npart = n;
+  return CH4_OK;
+}
+
+int ch4o_get_particles(ch4o_state *s, ch4_particle *parts, int n) {
+  if (n > s->npart) return CH4_ERR_ARG;
+  memcpy(parts, s->part, sizeof(ch4_particle) * (size_t)n);
+  return CH4_OK;
+}
+
+int ch4o_averages_get(ch4o_state *s, ch4_averages *out) {
+  memset(out, 0, sizeof(*out));
+  (void)s;
+  return CH4_ERR_UNSUPPORTED;
+}

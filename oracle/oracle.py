@@ -1,0 +1,230 @@
+"""Python side of the CPU oracle (test infrastructure only).
+
+Two checkers live here:
+
+* `Restatement` -- ctypes binding of oracle/libch4oracle.so, the project's own C
+  restatement of the reference time step (oracle/ch4_oracle.c), with the same
+  entry points as the product's C ABI (include/ch4.h).
+* `run_reference` -- runs the reference solver itself, compiled from its own
+  sources by oracle/Makefile into oracle/_ref/<flagset>/ch4ref, on injected
+  initial state (oracle/harness/ref_harness.c) and reads back its fields.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker / the timed CPU reference.
+"""
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+sys.path.insert(0, os.path.join(REPO, "ch4-project_b200"))
+from ch4b200 import abi  # noqa: E402  (interface types only)
+
+NPOP = abi.NPOP
+
+# flag sets of the compiled reference binaries (must match oracle/configs/<name>.h)
+FLAGSETS = {
+    "kolmogorov": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV"],
+    "rb": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
+           "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y"],
+}
+
+
+def ref_binary(flagset):
+    return os.path.join(HERE, "_ref", flagset, "ch4ref")
+
+
+def ref_available(flagset):
+    return os.path.exists(ref_binary(flagset))
+
+
+def make_config(NX, NY, NZ, flags, storage=abi.STORE_F64, **kw):
+    """Fill an abi.Config the way assign_parameters does (src/parameters.c:41-811)."""
+    c = abi.Config()
+    c.NX, c.NY, c.NZ = NX, NY, NZ
+    c.flags = abi.flags_of(flags) if isinstance(flags, (list, tuple)) else int(flags)
+    c.storage = storage
+    c.SX, c.SY, c.SZ = float(NX), float(NY), float(NZ)
+    c.time_dt = 1.0
+    c.tau_u = 1.0
+    c.tau_t = 1.0
+    c.tau_s = 1.0
+    c.C_smag = 0.18
+    c.time_dt_lagr_factor = 1.0
+    c.seed = 1
+    for k, v in kw.items():
+        setattr(c, k, v)
+    # derived quantities, src/parameters.c:156-160,233-240
+    c.nu = (c.tau_u - 0.5 * c.time_dt) / 3.0
+    c.kappa = (c.tau_t - 0.5 * c.time_dt) / 3.0
+    c.chi = (c.tau_s - 0.5 * c.time_dt) / 3.0
+    c.deltaT = c.T_bot - c.T_top
+    c.deltaS = c.S_bot - c.S_top
+    return c
+
+
+PARAM_KEYS = ["resume", "resume_u", "resume_t", "resume_s", "NX", "NY", "NZ", "SX", "SY", "SZ",
+              "time_dt", "time_start", "time_end", "time_dump_field", "time_dump_diagn",
+              "tau_u", "Amp_x", "Amp_y", "Amp_z", "gravity_x", "gravity_y", "gravity_z",
+              "tau_t", "T_bot", "T_top", "T_ref", "grad_T_bot", "grad_T_top", "beta_t", "beta2_t",
+              "tau_s", "S_bot", "S_top", "S_ref", "beta_s",
+              "time_dt_lagr_factor", "time_dump_lagr", "particle_number"]
+
+
+def write_param_in(path, cfg, nsteps=1):
+    vals = {"resume": 0, "resume_u": 0, "resume_t": 0, "resume_s": 0,
+            "time_start": 0.0, "time_end": float(nsteps), "time_dump_field": 1e12,
+            "time_dump_diagn": 1e12, "time_dump_lagr": 1e12}
+    with open(path, "w") as f:
+        for k in PARAM_KEYS:
+            v = vals[k] if k in vals else getattr(cfg, k)
+            f.write("%s %r\n" % (k, float(v) if not isinstance(v, int) else v))
+
+
+def aos_from_soa(f_soa, NX, NY, NZ):
+    """SoA [q][z][y][x] -> reference AoS interior order [z][y][x][q]."""
+    return np.ascontiguousarray(f_soa.reshape(NPOP, NZ, NY, NX).transpose(1, 2, 3, 0))
+
+
+def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=1, workdir=None):
+    """Run the compiled reference on injected populations.
+
+    pops: dict which -> AoS array [NZ][NY][NX][NPOP] (interior cells).
+    Returns dict of output arrays (AoS / per-cell) and the timing record.
+    """
+    exe = ref_binary(flagset)
+    if not os.path.exists(exe):
+        raise FileNotFoundError(exe)
+    tmp = workdir or tempfile.mkdtemp(prefix="ch4ref_")
+    write_param_in(os.path.join(tmp, "param.in"), cfg, nsteps)
+    for which, arr in pops.items():
+        np.ascontiguousarray(arr, dtype=np.float64).tofile(os.path.join(tmp, "in_%s.bin" % which))
+    if phi is not None:
+        np.ascontiguousarray(phi, dtype=np.float64).tofile(os.path.join(tmp, "in_phi.bin"))
+    r = subprocess.run([exe, str(nsteps), str(seed)], cwd=tmp, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference run failed: %s" % r.stderr[-2000:])
+    NX, NY, NZ = cfg.NX, cfg.NY, cfg.NZ
+    out = {}
+    shapes = {"p": (NZ, NY, NX, NPOP), "g": (NZ, NY, NX, NPOP), "h": (NZ, NY, NX, NPOP),
+              "u": (NZ, NY, NX, 3), "force": (NZ, NY, NX, 3), "dens": (NZ, NY, NX),
+              "t": (NZ, NY, NX), "s": (NZ, NY, NX), "phi": (abi.NK, 3)}
+    for name, shape in shapes.items():
+        fn = os.path.join(tmp, "out_%s.bin" % name)
+        if os.path.exists(fn):
+            out[name] = np.fromfile(fn, dtype=np.float64).reshape(shape)
+    with open(os.path.join(tmp, "timing.json")) as f:
+        out["timing"] = json.load(f)
+    return out
+
+
+class Restatement:
+    """ctypes binding of oracle/libch4oracle.so (entry points of oracle/ch4_oracle.h)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            path = os.path.join(HERE, "libch4oracle.so")
+            if not os.path.exists(path):
+                subprocess.run(["make", "-s", "-C", HERE, "restatement"], check=True)
+            lib = C.CDLL(path)
+            P = C.c_void_p
+            D = C.POINTER(C.c_double)
+            lib.ch4o_create.argtypes = [C.POINTER(abi.Config), C.POINTER(P)]
+            lib.ch4o_destroy.argtypes = [P]
+            lib.ch4o_set_pop.argtypes = [P, C.c_char, D, C.c_int]
+            lib.ch4o_get_pop.argtypes = [P, C.c_char, D, C.c_int]
+            lib.ch4o_set_hit_phases.argtypes = [P, D]
+            lib.ch4o_get_hit_phases.argtypes = [P, D]
+            lib.ch4o_initialize.argtypes = [P]
+            lib.ch4o_step.argtypes = [P, C.c_int]
+            lib.ch4o_get_fields.argtypes = [P, D, D, D, D, C.c_int]
+            lib.ch4o_get_force.argtypes = [P, D, C.c_int]
+            lib.ch4o_set_particles.argtypes = [P, C.POINTER(abi.Particle), C.c_int]
+            lib.ch4o_get_particles.argtypes = [P, C.POINTER(abi.Particle), C.c_int]
+            lib.ch4o_averages_get.argtypes = [P, C.POINTER(abi.Averages)]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.h = C.c_void_p()
+        rc = self.lib().ch4o_create(C.byref(cfg), C.byref(self.h))
+        if rc != 0:
+            raise RuntimeError("ch4o_create: %d" % rc)
+
+    def close(self):
+        if self.h:
+            self.lib().ch4o_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _ptr(a):
+        return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError("%s failed: %s" % (what, abi.STATUS_NAMES.get(rc, rc)))
+
+    def set_pop(self, which, aos, brd=0):
+        a = np.ascontiguousarray(aos, dtype=np.float64)
+        self._check(self.lib().ch4o_set_pop(self.h, which.encode(), self._ptr(a), brd), "set_pop")
+
+    def get_pop(self, which, brd=0):
+        c = self.cfg
+        a = np.empty((c.NZ + 2 * brd, c.NY + 2 * brd, c.NX + 2 * brd, NPOP))
+        self._check(self.lib().ch4o_get_pop(self.h, which.encode(), self._ptr(a), brd), "get_pop")
+        return a
+
+    def set_hit_phases(self, phi):
+        a = np.ascontiguousarray(phi, dtype=np.float64)
+        self._check(self.lib().ch4o_set_hit_phases(self.h, self._ptr(a)), "set_hit_phases")
+
+    def get_hit_phases(self):
+        a = np.empty((abi.NK, 3))
+        self._check(self.lib().ch4o_get_hit_phases(self.h, self._ptr(a)), "get_hit_phases")
+        return a
+
+    def initialize(self):
+        self._check(self.lib().ch4o_initialize(self.h), "initialize")
+
+    def step(self, n):
+        self._check(self.lib().ch4o_step(self.h, n), "step")
+
+    def fields(self):
+        c = self.cfg
+        dens = np.empty((c.NZ, c.NY, c.NX))
+        u = np.empty((c.NZ, c.NY, c.NX, 3))
+        t = np.empty((c.NZ, c.NY, c.NX))
+        s = np.empty((c.NZ, c.NY, c.NX))
+        self._check(self.lib().ch4o_get_fields(self.h, self._ptr(dens), self._ptr(u), self._ptr(t), self._ptr(s), 0),
+                    "get_fields")
+        return {"dens": dens, "u": u, "t": t, "s": s}
+
+    def force(self):
+        c = self.cfg
+        f = np.empty((c.NZ, c.NY, c.NX, 3))
+        self._check(self.lib().ch4o_get_force(self.h, self._ptr(f), 0), "get_force")
+        return f
+
+    def set_particles(self, parts):
+        self._check(self.lib().ch4o_set_particles(self.h, parts, len(parts)), "set_particles")
+
+    def get_particles(self, n):
+        arr = (abi.Particle * n)()
+        self._check(self.lib().ch4o_get_particles(self.h, arr, n), "get_particles")
+        return arr
