@@ -1,0 +1,320 @@
+"""Benchmark: lattice updates per second of the fused D3Q19 fluid+thermal step.
+
+Workload (one "step" = one iteration of the reference driver loop, src/main.c:67-161):
+3-D Rayleigh-Benard convection, 256x256x128 lattice (y vertical, no-slip bounce-back
+and fixed-temperature walls at y=0 and y=256, periodic in x and z), D3Q19 fluid +
+D3Q19 temperature populations, Boussinesq buoyancy, Ra = 1e8, Pr = 1, initial linear
+T profile + seeded uniform +-1e-3 noise.  Synthetic data (the reference ships no
+dataset); FP32 arithmetic with FP32 population storage by default.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|f64]
+  python bench.py --impl reference ...   (the reference solver's own CPU build)
+
+With N > 1 (torchrun, one process per GPU) every rank advances its own lattice
+(independent replicas: the single-lattice path has no exchange step here), timed as the
+max over ranks.  Prints ONE JSON line on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "ch4-project_b200"))
+
+NX, NY, NZ = 256, 256, 128
+RA, PR = 1e8, 1.0
+BYTES_PER_CELL = {  # algorithmic bytes per cell update: read+write of 2 x 19 populations + T_prev r/w
+    "f64": 2 * 2 * 19 * 8 + 2 * 8,
+    "f32": 2 * 2 * 19 * 4 + 2 * 4,
+    "f16": 2 * 2 * 19 * 2 + 2 * 4,
+}
+WORKLOAD = "rayleigh_benard_256x256x128_d3q19_fluid+thermal"
+
+
+def rb_params():
+    """tau, beta*g from Ra, Pr with a free-fall velocity of 0.05 lattice units."""
+    H = float(NY)
+    dT = 1.0
+    bg = (0.05 ** 2) / (H * dT)            # beta_t * g_y
+    nu = (bg * dT * H ** 3 * PR / RA) ** 0.5
+    kappa = nu / PR
+    return dict(tau_u=0.5 + 3 * nu, tau_t=0.5 + 3 * kappa, beta_t=1.0, gravity_y=bg,
+                T_bot=1.0, T_top=0.0, T_ref=0.5)
+
+
+def make_cfg(storage):
+    import ch4b200
+    from ch4b200 import abi
+    c = ch4b200.default_config()
+    c.NX, c.NY, c.NZ = NX, NY, NZ
+    c.SX, c.SY, c.SZ = float(NX), float(NY), float(NZ)
+    c.flags = abi.flags_of(["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
+                            "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y"])
+    c.storage = {"f64": abi.STORE_F64, "f32": abi.STORE_F32, "f16": abi.STORE_F16}[storage]
+    for k, v in rb_params().items():
+        setattr(c, k, v)
+    c.nu = (c.tau_u - 0.5 * c.time_dt) / 3.0
+    c.kappa = (c.tau_t - 0.5 * c.time_dt) / 3.0
+    c.deltaT = c.T_bot - c.T_top
+    return c
+
+
+def initial_state(seed=1234):
+    """rho=1, u=0 (p = w) and linear T with uniform +-1e-3 noise (g = w*T), AoS FP64."""
+    w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+    rng = np.random.default_rng(seed)
+    y = (np.arange(NY) + 0.5) / NY
+    T = (1.0 - y)[None, :, None] + 1e-3 * (2 * rng.random((NZ, NY, NX)) - 1)
+    p = np.broadcast_to(w, (NZ, NY, NX, 19))
+    g = T[..., None] * w
+    return np.ascontiguousarray(p), np.ascontiguousarray(g)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def measured_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(storage):
+    """dram bytes per launch of the step kernel from the committed ncu summary (or None)."""
+    path = os.path.join(REPO, "profiles", "lb_step_rb256_%s.json" % storage)
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch_full_lattice")
+    except Exception:
+        return None
+
+
+def cpu_reference_run(steps, workdir=None):
+    """Time the reference solver's own CPU build (oracle/_ref/rb, single rank) on the
+    full lattice from its rest state; returns MLUPS and the sample description."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    exe = O.ref_binary("rb")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/rb/ch4ref not built"
+    cfg = O.make_config(NX, NY, NZ, O.FLAGSETS["rb"], **rb_params())
+    tmp = workdir or tempfile.mkdtemp(prefix="ch4cpu_")
+    O.write_param_in(os.path.join(tmp, "param.in"), cfg, steps)
+    r = subprocess.run([exe, str(steps), "1"], cwd=tmp, capture_output=True, text=True)
+    if r.returncode != 0:
+        return None, "reference run failed: " + r.stderr[-300:]
+    with open(os.path.join(tmp, "timing.json")) as f:
+        t = json.load(f)
+    return t["mlups"], "%d step(s) of the full 256x256x128 lattice from the rest state, 1 MPI rank" % steps
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference_arm(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    k = max(1, min(args.steps, 6))
+    if args.warmup > 0:
+        cpu_reference_run(1)
+    mlups, sample = cpu_reference_run(k)
+    if mlups is None:
+        print(json.dumps({"impl": "reference", "unavailable": sample}))
+        return 0
+    line = {
+        "impl": "reference", "metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": NX * NY * NZ / mlups / 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "lattice": [NX, NY, NZ], "Ra": RA, "Pr": PR},
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "f64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--lattice", default=None, help="NX,NY,NZ override (profiling runs on a smaller case)")
+    args = ap.parse_args()
+    if args.lattice:
+        global NX, NY, NZ
+        NX, NY, NZ = (int(v) for v in args.lattice.split(","))
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import ch4b200
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    W = max(3, args.warmup)
+    K = args.steps
+    cfg = make_cfg(args.storage)
+    p0, g0 = initial_state(1234 + rank)
+    cells = NX * NY * NZ
+
+    # ---- device-resident timing --------------------------------------------
+    sim = ch4b200.Simulation(cfg)
+    sim.set_pop("p", p0)
+    sim.set_pop("g", g0)
+    sim.initialize()
+    stream = torch.cuda.ExternalStream(sim.stream_handle)
+    sim.step(W)
+    sim.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        sim.step(K)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    ms_step = ms / K
+    value = world * cells * K / (ms * 1e-3) / 1e6
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_CELL[args.storage] * cells / (ms_step * 1e-3) / 1e9
+    fields = sim.fields()
+    finite = bool(np.isfinite(fields["u"]).all() and np.isfinite(fields["t"]).all())
+    sim.close()
+
+    # ---- end to end through the C ABI with host buffers ---------------------
+    e2e = None
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with ch4b200.Simulation(cfg) as s2:
+            s2.set_pop("p", p0)
+            s2.set_pop("g", g0)
+            s2.initialize()
+            s2.step(K)
+            f2 = s2.fields()
+        t1 = time.perf_counter()
+        sec = t1 - t0
+        if world > 1:
+            t = torch.tensor([sec], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            sec = float(t.item())
+        h2d = 2 * p0.nbytes
+        d2h = 9 * cells * 8  # dens, u(3), t, s, force(3) planes of ch4_get_fields
+        e2e = {"value": world * cells * K / sec / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+               "includes": "create + AoS FP64 upload of p,g + initialize + K steps + hydro-field download"}
+        del f2
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        mlups, sample = cpu_reference_run(2)
+        if mlups is not None:
+            cpu = {"value": mlups, "unit": "MLUPS", "cores": 1, "kind": "reference", "sample": sample}
+        else:
+            cpu = {"value": None, "unit": "MLUPS", "cores": 1, "kind": "reference", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f32": "f32", "f16": "f32 (f16 storage)", "f64": "f64"}[args.storage], "data": "synthetic",
+            "config": {"workload": WORKLOAD, "lattice": [NX, NY, NZ], "Ra": RA, "Pr": PR,
+                       "storage": args.storage, "l2": "inputs larger than L2 (%.2f GB of populations)" %
+                       (2 * 19 * cells * {"f64": 8, "f32": 4, "f16": 2}[args.storage] / 1e9),
+                       "parallelism": "replicas%d" % world},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": ncu_traffic(args.storage),
+                         "bytes_per_cell": BYTES_PER_CELL[args.storage], "kernel": "lb_step_kernel"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": K,
+            "clocks": clk.summary(),
+            "finite": finite,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

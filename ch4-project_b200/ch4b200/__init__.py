@@ -1,0 +1,207 @@
+"""Python mirror of the B200 lattice-Boltzmann C ABI (include/ch4.h).
+
+`Simulation` follows the reference driver (src/main.c): configure (define.h flags +
+param.in keys), set the initial populations, `initialize()` (src/main.c:24-48),
+`step(n)` (src/main.c:67-196), read back populations / hydro fields.  Every call goes
+through libch4b200.so; there is no CPU fallback -- if the library or a GPU is
+missing, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import NPOP, Config, Particle, Averages, FLAGS, flags_of  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libch4b200.so")
+
+_lib = None
+
+
+class CH4Error(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (abi.STATUS_NAMES.get(status, status), msg))
+        self.status = status
+
+
+def lib():
+    """Load libch4b200.so (built in-tree by ch4-project_b200/build.py)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libch4b200.so is not built (run ch4-project_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        D = C.POINTER(C.c_double)
+        L.ch4_config_default.argtypes = [C.POINTER(Config)]
+        L.ch4_config_read_define.argtypes = [C.POINTER(Config), C.c_char_p, C.c_char_p, C.c_size_t]
+        L.ch4_config_read_param.argtypes = [C.POINTER(Config), C.c_char_p, C.c_char_p, C.c_size_t]
+        L.ch4_read_parameter.argtypes = [C.c_char_p, C.c_char_p, D]
+        L.ch4_create.argtypes = [C.POINTER(Config), C.POINTER(P)]
+        L.ch4_destroy.argtypes = [P]
+        L.ch4_last_error.argtypes = [P]
+        L.ch4_last_error.restype = C.c_char_p
+        L.ch4_device_bytes.argtypes = [C.POINTER(Config), C.POINTER(C.c_size_t)]
+        L.ch4_set_pop.argtypes = [P, C.c_char, D, C.c_int]
+        L.ch4_get_pop.argtypes = [P, C.c_char, D, C.c_int]
+        L.ch4_set_hit_phases.argtypes = [P, D]
+        L.ch4_get_hit_phases.argtypes = [P, D]
+        L.ch4_set_particles.argtypes = [P, C.POINTER(Particle), C.c_int]
+        L.ch4_get_particles.argtypes = [P, C.POINTER(Particle), C.c_int]
+        L.ch4_initialize.argtypes = [P]
+        L.ch4_step.argtypes = [P, C.c_int]
+        L.ch4_synchronize.argtypes = [P]
+        L.ch4_get_fields.argtypes = [P, D, D, D, D, C.c_int]
+        L.ch4_get_force.argtypes = [P, D, C.c_int]
+        L.ch4_averages_get.argtypes = [P, C.POINTER(Averages)]
+        L.ch4_get_itime.argtypes = [P, C.POINTER(C.c_int)]
+        L.ch4_get_stream.argtypes = [P, C.POINTER(C.c_void_p)]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def default_config():
+    c = Config()
+    lib().ch4_config_default(C.byref(c))
+    return c
+
+
+def read_define(cfg, path):
+    """Set cfg.flags from a reference define.h (CH4Error on a flag outside the hot path)."""
+    bad = C.create_string_buffer(256)
+    rc = lib().ch4_config_read_define(C.byref(cfg), path.encode(), bad, 256)
+    if rc:
+        raise CH4Error(rc, "define.h flag %s" % bad.value.decode())
+    return cfg
+
+
+def read_param(cfg, path):
+    """Fill cfg from param.in with the reference's read_parameter semantics."""
+    bad = C.create_string_buffer(256)
+    rc = lib().ch4_config_read_param(C.byref(cfg), path.encode(), bad, 256)
+    if rc:
+        raise CH4Error(rc, "param.in key %s" % bad.value.decode())
+    return cfg
+
+
+def read_parameter(path, key):
+    v = C.c_double()
+    rc = lib().ch4_read_parameter(path.encode(), key.encode(), C.byref(v))
+    if rc:
+        raise CH4Error(rc, "%s not found in %s" % (key, path))
+    return v.value
+
+
+def device_bytes(cfg):
+    n = C.c_size_t()
+    rc = lib().ch4_device_bytes(C.byref(cfg), C.byref(n))
+    if rc:
+        raise CH4Error(rc, "device_bytes")
+    return n.value
+
+
+class Simulation:
+    """One lattice on the current CUDA device (handle of include/ch4.h)."""
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.h = C.c_void_p()
+        rc = lib().ch4_create(C.byref(cfg), C.byref(self.h))
+        if rc:
+            raise CH4Error(rc, "ch4_create")
+
+    def close(self):
+        if self.h:
+            lib().ch4_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc:
+            raise CH4Error(rc, "%s: %s" % (what, lib().ch4_last_error(self.h).decode()))
+
+    def set_pop(self, which, aos, brd=0):
+        a = np.ascontiguousarray(aos, dtype=np.float64)
+        self._check(lib().ch4_set_pop(self.h, which.encode(), _dp(a), brd), "set_pop")
+
+    def get_pop(self, which, brd=0, out=None):
+        c = self.cfg
+        a = out if out is not None else np.empty((c.NZ + 2 * brd, c.NY + 2 * brd, c.NX + 2 * brd, NPOP))
+        self._check(lib().ch4_get_pop(self.h, which.encode(), _dp(a), brd), "get_pop")
+        return a
+
+    def set_hit_phases(self, phi):
+        a = np.ascontiguousarray(phi, dtype=np.float64)
+        self._check(lib().ch4_set_hit_phases(self.h, _dp(a)), "set_hit_phases")
+
+    def get_hit_phases(self):
+        a = np.empty((abi.NK, 3))
+        self._check(lib().ch4_get_hit_phases(self.h, _dp(a)), "get_hit_phases")
+        return a
+
+    def set_particles(self, parts):
+        self._check(lib().ch4_set_particles(self.h, parts, len(parts)), "set_particles")
+
+    def get_particles(self, n):
+        arr = (Particle * n)()
+        self._check(lib().ch4_get_particles(self.h, arr, n), "get_particles")
+        return arr
+
+    def initialize(self):
+        self._check(lib().ch4_initialize(self.h), "initialize")
+
+    def step(self, n=1):
+        self._check(lib().ch4_step(self.h, n), "step")
+
+    def synchronize(self):
+        self._check(lib().ch4_synchronize(self.h), "synchronize")
+
+    def fields(self):
+        c = self.cfg
+        dens = np.empty((c.NZ, c.NY, c.NX))
+        u = np.empty((c.NZ, c.NY, c.NX, 3))
+        t = np.empty((c.NZ, c.NY, c.NX))
+        s = np.empty((c.NZ, c.NY, c.NX))
+        self._check(lib().ch4_get_fields(self.h, _dp(dens), _dp(u), _dp(t), _dp(s), 0), "get_fields")
+        return {"dens": dens, "u": u, "t": t, "s": s}
+
+    def force(self):
+        c = self.cfg
+        f = np.empty((c.NZ, c.NY, c.NX, 3))
+        self._check(lib().ch4_get_force(self.h, _dp(f), 0), "get_force")
+        return f
+
+    def averages(self):
+        a = Averages()
+        self._check(lib().ch4_averages_get(self.h, C.byref(a)), "averages")
+        return {n: getattr(a, n) for n in abi.AVERAGE_FIELDS}
+
+    @property
+    def stream_handle(self):
+        """cudaStream_t of this handle as an integer (for torch.cuda.ExternalStream)."""
+        v = C.c_void_p()
+        self._check(lib().ch4_get_stream(self.h, C.byref(v)), "get_stream")
+        return v.value or 0
+
+    @property
+    def itime(self):
+        v = C.c_int()
+        self._check(lib().ch4_get_itime(self.h, C.byref(v)), "get_itime")
+        return v.value

@@ -1,0 +1,906 @@
+// Host implementation of the C ABI in include/ch4.h.
+//
+// Replaces the reference driver's configuration (src/define.h flags,
+// src/parameters.c param.in reading), allocation (src/parameters.c:917) and the
+// time loop of src/main.c:67-196 by one handle that owns the device state and
+// a CUDA stream.  Host work per step is limited to the HIT phase random walk
+// (src/forcing.c:36-79, 18 Gaussians from the drand48 stream) and its sin
+// tables, computed with the host libm exactly as the reference does.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ch4.h"
+#include "launch.h"
+
+using namespace ch4;
+
+namespace {
+
+constexpr int NPOP = Q;
+const double VK[NK][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}};
+
+// lattice constants of design_lb (src/lb.c:139-160, 368-377), host FP64
+struct Lattice {
+  double w[NPOP];
+  double invcs2, invcs4, invtwocs2, invtwocs4;
+  Lattice() {
+    w[0] = 1. / 3.;
+    for (int q = 1; q <= 6; q++) w[q] = 1. / 18.;
+    for (int q = 7; q < NPOP; q++) w[q] = 1. / 36.;
+    double cs = 1.0 / std::sqrt(3.0);
+    double cs2 = std::pow(cs, 2.0), cs4 = std::pow(cs, 4.0);
+    invcs2 = 1.0 / cs2;
+    invcs4 = 1.0 / cs4;
+    invtwocs2 = 1.0 / (2.0 * cs2);
+    invtwocs4 = 1.0 / (2.0 * cs4);
+  }
+};
+
+const uint64_t SUPPORTED =
+    CH4_F_LB_FLUID | CH4_F_LB_FLUID_FORCING | CH4_F_FORCING_KOLMOGOROV | CH4_F_FORCING_POISEUILLE | CH4_F_FORCING_HIT |
+    CH4_F_LB_TEMPERATURE | CH4_F_TEMPERATURE_BUOYANCY | CH4_F_LB_SCALAR | CH4_F_SCALAR_BUOYANCY | CH4_F_FLUID_BC_Y |
+    CH4_F_FLUID_BC_Y_P_SLIP | CH4_F_FLUID_BC_Y_M_SLIP | CH4_F_TEMPERATURE_BC_Y | CH4_F_TEMPERATURE_BC_Y_P_FLUX |
+    CH4_F_TEMPERATURE_BC_Y_M_FLUX | CH4_F_TEMPERATURE_BC_Y_P_NOFLUX | CH4_F_TEMPERATURE_BC_Y_M_NOFLUX |
+    CH4_F_SCALAR_BC_Y | CH4_F_FLUID_LES | CH4_F_TEMPERATURE_FORCING;
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// engine (one per precision)
+
+struct EngineBase {
+  virtual ~EngineBase() = default;
+  virtual ch4_status alloc() = 0;
+  virtual ch4_status set_pop(int set, const double* aos, int brd) = 0;
+  virtual ch4_status get_pop(int set, double* aos, int brd) = 0;
+  virtual ch4_status initialize() = 0;
+  virtual ch4_status step(int n) = 0;
+  virtual ch4_status fields(double* dens, double* u, double* t, double* s, double* force, int brd) = 0;
+  virtual size_t device_bytes() const = 0;
+};
+
+struct ch4_handle {
+  ch4_config cfg;
+  std::string err;
+  std::unique_ptr<EngineBase> eng;
+  cudaStream_t stream = nullptr;
+  // host RNG (drand48 stream, src/random.c:4-16) and HIT phases
+  unsigned short rng[3];
+  double phi[NK][3];
+  double hit_fac[NK];
+  int itime = 0;
+  bool initialized = false;
+  Lattice lat;
+
+  ch4_status fail(ch4_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return s;
+  }
+  ch4_status cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CH4_OK;
+    return fail(CH4_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+  double myrand() { return erand48(rng); }
+  // polar Box-Muller of src/random.c:82-100
+  double random_gauss(double mu, double sigma) {
+    double U1, U2, W, mult, X1;
+    do {
+      U1 = -1 + ((double)myrand()) * 2;
+      U2 = -1 + ((double)myrand()) * 2;
+      W = std::pow(U1, 2) + std::pow(U2, 2);
+    } while (W >= 1 || W == 0);
+    mult = std::sqrt((-2 * std::log(W)) / W);
+    X1 = U1 * mult;
+    return (mu + sigma * (double)X1);
+  }
+  // src/forcing.c:43-69
+  void phase_walk() {
+    double t_turnover = (cfg.SX / 0.1);
+    double phi_diffusivity = 0.01 / t_turnover;
+    double fac1 = cfg.time_dt / t_turnover;
+    double fac2 = std::sqrt(2.0 * cfg.time_dt * phi_diffusivity);
+    for (int ii = 0; ii < NK; ii++)
+      for (int a = 0; a < 3; a++) {
+        double val = random_gauss(0.0, 1.0);
+        phi[ii][a] += -phi[ii][a] * fac1 + val * fac2;
+      }
+  }
+  // sin tables of src/forcing.c:582-584 for the current phases
+  void hit_tables(double* tab) const {
+    const double LX = cfg.SX, LY = cfg.SY, LZ = cfg.SZ;
+    const int L = cfg.NX + cfg.NY + cfg.NZ;
+    for (int ii = 0; ii < NK; ii++) {
+      double *ax = tab + ii * L, *ay = ax + cfg.NX, *az = ay + cfg.NY;
+      for (int i = 0; i < cfg.NX; i++) ax[i] = std::sin(2 * 3.14159265359 * (VK[ii][0] * ((double)i + 0.5) / LX + phi[ii][0]));
+      for (int j = 0; j < cfg.NY; j++) ay[j] = std::sin(2 * 3.14159265359 * (VK[ii][1] * ((double)j + 0.5) / LY + phi[ii][1]));
+      for (int k = 0; k < cfg.NZ; k++) az[k] = std::sin(2 * 3.14159265359 * (VK[ii][2] * ((double)k + 0.5) / LZ + phi[ii][2]));
+    }
+  }
+};
+
+namespace {
+
+template <typename A>
+struct StorageOf;
+template <>
+struct StorageOf<double> {
+  static size_t bytes(int) { return 8; }
+};
+template <>
+struct StorageOf<float> {
+  static size_t bytes(int storage) { return storage == CH4_STORE_F16 ? 2 : 4; }
+};
+
+template <typename A>
+struct Engine : EngineBase {
+  ch4_handle* H;
+  const ch4_config& c;
+  long long N;
+  int nsets_on[3];
+  size_t sbytes;
+  void* f[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  int cur = 0;  // which of the two buffers holds f^n
+  A *tprev = nullptr, *sprev = nullptr;
+  A *kol = nullptr;
+  A *ules = nullptr, *tau_les = nullptr;
+  A *hit_ring = nullptr;  // (CHUNK+1) phase-table slots
+  A *hit_last = nullptr;  // tables of the latest phases (those of F^n)
+  double* staging_d = nullptr;  // device AoS chunk
+  double* staging_h = nullptr;  // pinned host chunk
+  A* hit_h = nullptr;           // pinned host phase tables
+  cudaEvent_t hit_ev = nullptr;
+  size_t chunk_planes = 0;
+  static constexpr int CHUNK = 256;
+  StepParams<A> P{};
+  LaunchShape shape{};
+
+  Engine(ch4_handle* h) : H(h), c(h->cfg) {
+    N = (long long)c.NX * c.NY * c.NZ;
+    nsets_on[0] = 1;
+    nsets_on[1] = (c.flags & CH4_F_LB_TEMPERATURE) != 0;
+    nsets_on[2] = (c.flags & CH4_F_LB_SCALAR) != 0;
+    sbytes = StorageOf<A>::bytes(c.storage);
+    shape.therm = nsets_on[1];
+    shape.scal = nsets_on[2];
+    shape.storage = c.storage;
+  }
+  ~Engine() override {
+    for (auto& s : f)
+      for (auto& b : s)
+        if (b) cudaFree(b);
+    cudaFree(tprev);
+    cudaFree(sprev);
+    cudaFree(kol);
+    cudaFree(ules);
+    cudaFree(tau_les);
+    cudaFree(hit_ring);
+    cudaFree(hit_last);
+    cudaFree(staging_d);
+    if (staging_h) cudaFreeHost(staging_h);
+    if (hit_h) cudaFreeHost(hit_h);
+    if (hit_ev) cudaEventDestroy(hit_ev);
+  }
+
+  int L() const { return c.NX + c.NY + c.NZ; }
+
+  size_t device_bytes() const override {
+    size_t b = 0;
+    for (int s = 0; s < 3; s++)
+      if (nsets_on[s]) b += 2 * (size_t)NPOP * N * sbytes;
+    if (nsets_on[1]) b += N * sizeof(A);
+    if (nsets_on[2]) b += N * sizeof(A);
+    if (c.flags & CH4_F_FLUID_LES) b += 4 * N * sizeof(A);
+    b += (size_t)(CHUNK + 2) * NK * L() * sizeof(A);
+    b += (size_t)c.NX * c.NY * NPOP * 8 * 4;  // staging
+    return b;
+  }
+
+  ch4_status alloc() override {
+    cudaError_t e;
+    for (int s = 0; s < 3; s++) {
+      if (!nsets_on[s]) continue;
+      for (int b = 0; b < 2; b++) {
+        e = cudaMalloc(&f[s][b], (size_t)NPOP * N * sbytes);
+        if (e != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "population buffer: %s", cudaGetErrorString(e));
+      }
+    }
+    if (nsets_on[1] && cudaMalloc(&tprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tprev");
+    if (nsets_on[2] && cudaMalloc(&sprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "sprev");
+    if (c.flags & CH4_F_FLUID_LES) {
+      if (cudaMalloc(&ules, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
+      if (cudaMalloc(&tau_les, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tau_les");
+    }
+    const int nk = 2 * c.NY + c.NX;
+    if (cudaMalloc(&kol, nk * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "kol");
+    if (cudaMalloc(&hit_ring, (size_t)(CHUNK + 1) * NK * L() * sizeof(A)) != cudaSuccess)
+      return H->fail(CH4_ERR_NOMEM, "hit ring");
+    if (cudaMalloc(&hit_last, (size_t)NK * L() * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "hit last");
+    if (cudaMallocHost(&hit_h, (size_t)(CHUNK + 1) * NK * L() * sizeof(A)) != cudaSuccess)
+      return H->fail(CH4_ERR_NOMEM, "pinned hit tables");
+    if (cudaEventCreateWithFlags(&hit_ev, cudaEventDisableTiming) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "event");
+    // staging for AoS exchange: a few z-planes at a time (<= 64 MiB)
+    const size_t plane = (size_t)c.NX * c.NY * NPOP * sizeof(double);
+    chunk_planes = std::max<size_t>(1, std::min<size_t>((size_t)c.NZ, (64u << 20) / plane));
+    if (cudaMalloc(&staging_d, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "staging");
+    if (cudaMallocHost(&staging_h, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "pinned staging");
+    fill_params();
+    // rest state p = w (src/initial_conditions.c:45), g = h = 0
+    std::vector<double> rest((size_t)c.NX * c.NY * NPOP * chunk_planes);
+    for (size_t i = 0; i < rest.size(); i++) rest[i] = H->lat.w[i % NPOP];
+    ch4_status st = upload_chunks(0, rest.data(), 0, true);
+    if (st) return st;
+    if (nsets_on[1]) {
+      std::fill(rest.begin(), rest.end(), 0.0);
+      if ((st = upload_chunks(1, rest.data(), 0, true))) return st;
+    }
+    if (nsets_on[2]) {
+      std::fill(rest.begin(), rest.end(), 0.0);
+      if ((st = upload_chunks(2, rest.data(), 0, true))) return st;
+    }
+    // Kolmogorov tables (src/forcing.c:390-400), host libm
+    {
+      std::vector<A> t(nk);
+      const double LX = c.SX, LY = c.SY, nu = c.nu, kn = 1.0;
+      double fnx = nu * std::pow(2 * 3.14159265359 / LX, 2.0);
+      double fny = nu * std::pow(2 * 3.14159265359 / LY, 2.0);
+      for (int j = 0; j < c.NY; j++) {
+        double y = (double)j + 0.5;
+        t[j] = (A)(c.Amp_x * fny * std::sin(kn * 2 * 3.14159265359 * y / LY));
+        t[c.NY + c.NX + j] = (A)(c.Amp_z * fny * std::sin(kn * 2 * 3.14159265359 * y / LY));
+      }
+      for (int i = 0; i < c.NX; i++) {
+        double x = (double)i + 0.5;
+        t[c.NY + i] = (A)(c.Amp_y * fnx * std::sin(kn * 2 * 3.14159265359 * x / LX));
+      }
+      if ((st = H->cuda(cudaMemcpy(kol, t.data(), nk * sizeof(A), cudaMemcpyHostToDevice), "kol upload"))) return st;
+    }
+    return CH4_OK;
+  }
+
+  void fill_params() {
+    const Lattice& lat = H->lat;
+    P.NX = c.NX;
+    P.NY = c.NY;
+    P.NZ = c.NZ;
+    P.N = N;
+    uint32_t F = 0;
+    const uint64_t fl = c.flags;
+    if (fl & CH4_F_LB_FLUID_FORCING) {
+      F |= K_FORCING;
+      if (fl & CH4_F_FORCING_KOLMOGOROV) F |= K_KOLMO;
+      if (fl & CH4_F_FORCING_POISEUILLE) F |= K_POIS;
+      if (fl & CH4_F_FORCING_HIT) F |= K_HIT;
+      if (fl & CH4_F_TEMPERATURE_BUOYANCY) F |= K_BUOY;
+      if (fl & CH4_F_SCALAR_BUOYANCY) F |= K_SBUOY;
+      if (c.beta2_t != 0.0) F |= K_BETA2;
+    }
+    if (fl & CH4_F_FLUID_BC_Y) F |= K_FWALL;
+    if (fl & CH4_F_FLUID_BC_Y_P_SLIP) F |= K_FSLIP_P;
+    if (fl & CH4_F_FLUID_BC_Y_M_SLIP) F |= K_FSLIP_M;
+    if (fl & CH4_F_TEMPERATURE_BC_Y) F |= K_TWALL;
+    if (fl & CH4_F_TEMPERATURE_BC_Y_P_FLUX) F |= K_TFLUX_P;
+    if (fl & CH4_F_TEMPERATURE_BC_Y_M_FLUX) F |= K_TFLUX_M;
+    if (fl & CH4_F_TEMPERATURE_BC_Y_P_NOFLUX) F |= K_TNOFLUX_P;
+    if (fl & CH4_F_TEMPERATURE_BC_Y_M_NOFLUX) F |= K_TNOFLUX_M;
+    if (fl & CH4_F_SCALAR_BC_Y) F |= K_SWALL;
+    if (fl & CH4_F_FLUID_LES) F |= K_LES;
+    P.feat = F;
+    for (int q = 0; q < NPOP; q++) P.w[q] = (A)lat.w[q];
+    const double invtau = 1.0 / c.tau_u;
+    const double fac = (1.0 - 0.5 * c.time_dt * invtau);  // src/forcing.c:1289
+    for (int q = 0; q < NPOP; q++) P.facw[q] = (A)(fac * lat.w[q]);
+    P.invcs2 = (A)lat.invcs2;
+    P.invcs4 = (A)lat.invcs4;
+    P.invtwocs2 = (A)lat.invtwocs2;
+    P.invtwocs4 = (A)lat.invtwocs4;
+    P.invtau[0] = (A)invtau;
+    P.invtau[1] = (A)(nsets_on[1] ? 1.0 / c.tau_t : 0.0);
+    P.invtau[2] = (A)(nsets_on[2] ? 1.0 / c.tau_s : 0.0);
+    P.hdt = (A)(0.5 * c.time_dt);
+    P.nu = (A)c.nu;
+    P.csmag2 = (A)std::pow(c.C_smag * 1.0, 2.0);
+    const double LX = c.SX, LY = c.SY, nu = c.nu;
+    P.pois[0] = (A)(2.0 * c.Amp_x * ((4. * nu) * std::pow(LY, -2.0)));
+    P.pois[1] = (A)(2.0 * c.Amp_y * ((4. * nu) * std::pow(LX, -2.0)));
+    P.pois[2] = (A)(2.0 * c.Amp_z * ((4. * nu) * std::pow(LY, -2.0)));
+    for (int ii = 0; ii < NK; ii++) {
+      P.hitamp[ii][0] = (A)(H->hit_fac[ii] * c.Amp_x);
+      P.hitamp[ii][1] = (A)(H->hit_fac[ii] * c.Amp_y);
+      P.hitamp[ii][2] = (A)(H->hit_fac[ii] * c.Amp_z);
+    }
+    double T0;
+    switch (c.t0_kind) {
+      case CH4_T0_REF: T0 = c.T_ref; break;
+      case CH4_T0_TOP: T0 = c.T_top; break;
+      case CH4_T0_BOT: T0 = c.T_bot; break;
+      default: T0 = 0.5 * (c.T_bot + c.T_top);
+    }
+    P.T0 = (A)T0;
+    P.beta_t = (A)c.beta_t;
+    P.beta2_t = (A)c.beta2_t;
+    P.S0 = (A)(0.5 * (c.S_bot + c.S_top));
+    P.beta_s = (A)c.beta_s;
+    P.grav[0] = (A)c.gravity_x;
+    P.grav[1] = (A)c.gravity_y;
+    P.grav[2] = (A)c.gravity_z;
+    P.T_top = (A)c.T_top;
+    P.T_bot = (A)c.T_bot;
+    P.T_ref = (A)c.T_ref;
+    P.grad_T_top = (A)c.grad_T_top;
+    P.grad_T_bot = (A)c.grad_T_bot;
+    P.S_top = (A)c.S_top;
+    P.S_bot = (A)c.S_bot;
+    P.S_ref = (A)c.S_ref;
+    // F16 storage shifts: rho0 = 1 for p, the buoyancy reference for g, S0 for h
+    P.shift[0] = 1.0f;
+    P.shift[1] = (float)T0;
+    P.shift[2] = (float)(0.5 * (c.S_bot + c.S_top));
+    P.tprev = tprev;
+    P.sprev = sprev;
+    P.ules = ules;
+    P.tau_les = tau_les;
+    P.kol = kol;
+    P.dcur = P.dprev = nullptr;
+  }
+
+  void bind_pops(int in) {
+    for (int s = 0; s < 3; s++) {
+      P.fin[s] = f[s][in];
+      P.fout[s] = f[s][in ^ 1];
+    }
+  }
+
+  // AoS (halo-padded by brd) -> device SoA; `repeat` uploads the same chunk to every slab
+  ch4_status upload_chunks(int set, const double* aos, int brd, bool repeat) {
+    const size_t row = (size_t)c.NX * NPOP;
+    const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
+    bind_pops(cur);
+    for (int z0 = 0; z0 < c.NZ; z0 += (int)chunk_planes) {
+      int nz = std::min<int>((int)chunk_planes, c.NZ - z0);
+      const double* src;
+      if (repeat) {
+        src = aos;
+      } else {
+        for (int zl = 0; zl < nz; zl++)
+          for (int y = 0; y < c.NY; y++)
+            std::memcpy(staging_h + ((size_t)zl * c.NY + y) * row,
+                        aos + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, row * sizeof(double));
+        src = staging_h;
+      }
+      ch4_status st = H->cuda(cudaMemcpyAsync(staging_d, src, (size_t)nz * c.NY * row * sizeof(double),
+                                              cudaMemcpyHostToDevice, H->stream),
+                              "upload");
+      if (st) return st;
+      if ((st = H->cuda(launch_aos_to_soa(P, shape, set, staging_d, f[set][cur], z0, nz, H->stream), "aos_to_soa")))
+        return st;
+      if ((st = H->cuda(cudaStreamSynchronize(H->stream), "upload sync"))) return st;
+    }
+    return CH4_OK;
+  }
+
+  ch4_status set_pop(int set, const double* aos, int brd) override {
+    if (!nsets_on[set]) return H->fail(CH4_ERR_ARG, "population set %d is not enabled", set);
+    H->initialized = false;
+    return upload_chunks(set, aos, brd, false);
+  }
+
+  ch4_status get_pop(int set, double* aos, int brd) override {
+    if (!nsets_on[set]) return H->fail(CH4_ERR_ARG, "population set %d is not enabled", set);
+    const size_t row = (size_t)c.NX * NPOP;
+    const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
+    bind_pops(cur);
+    for (int z0 = 0; z0 < c.NZ; z0 += (int)chunk_planes) {
+      int nz = std::min<int>((int)chunk_planes, c.NZ - z0);
+      ch4_status st;
+      if ((st = H->cuda(launch_soa_to_aos(P, shape, set, f[set][cur], staging_d, z0, nz, H->stream), "soa_to_aos")))
+        return st;
+      if ((st = H->cuda(cudaMemcpyAsync(staging_h, staging_d, (size_t)nz * c.NY * row * sizeof(double),
+                                        cudaMemcpyDeviceToHost, H->stream),
+                        "download")))
+        return st;
+      if ((st = H->cuda(cudaStreamSynchronize(H->stream), "download sync"))) return st;
+      for (int zl = 0; zl < nz; zl++)
+        for (int y = 0; y < c.NY; y++)
+          std::memcpy(aos + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
+                      staging_h + ((size_t)zl * c.NY + y) * row, row * sizeof(double));
+    }
+    return CH4_OK;
+  }
+
+  // host phase tables -> device slot
+  void tables_to(A* dst_h) {
+    std::vector<double> t((size_t)NK * L());
+    H->hit_tables(t.data());
+    for (size_t i = 0; i < t.size(); i++) dst_h[i] = (A)t[i];
+  }
+
+  ch4_status initialize() override {
+    bind_pops(cur);
+    ch4_status st;
+    if (nsets_on[1] || nsets_on[2])
+      if ((st = H->cuda(launch_init_prev(P, shape, H->stream), "init_prev"))) return st;
+    if (c.flags & CH4_F_FORCING_HIT) {
+      // build_forcing of src/main.c:38 advances the phases once
+      if ((st = H->cuda(cudaEventSynchronize(hit_ev), "hit event"))) return st;
+      H->phase_walk();
+      tables_to(hit_h);
+      if ((st = H->cuda(cudaMemcpyAsync(hit_last, hit_h, (size_t)NK * L() * sizeof(A), cudaMemcpyHostToDevice,
+                                        H->stream),
+                        "hit upload")))
+        return st;
+      if ((st = H->cuda(cudaEventRecord(hit_ev, H->stream), "hit event"))) return st;
+    }
+    return H->cuda(cudaStreamSynchronize(H->stream), "initialize");
+  }
+
+  ch4_status les_u() {
+    // u^n with dt/2 F^{n-1}: prev tables are P.hit_prev
+    return H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, nullptr, nullptr, nullptr, nullptr, nullptr, ules,
+                                H->stream),
+                   "les u");
+  }
+
+  ch4_status step(int n) override {
+    ch4_status st;
+    const bool hit = (c.flags & CH4_F_FORCING_HIT) != 0;
+    const size_t slot = (size_t)NK * L();
+    int done = 0;
+    while (done < n) {
+      const int m = std::min(CHUNK, n - done);
+      if (hit) {
+        // tables for phi_n (slot 0 = latest) and the m next phase sets
+        if ((st = H->cuda(cudaEventSynchronize(hit_ev), "hit event"))) return st;
+        for (int k = 1; k <= m; k++) {
+          H->phase_walk();
+          tables_to(hit_h + (size_t)k * slot);
+        }
+        if ((st = H->cuda(cudaMemcpyAsync(hit_ring, hit_last, slot * sizeof(A), cudaMemcpyDeviceToDevice, H->stream),
+                          "hit slot 0")))
+          return st;
+        if ((st = H->cuda(cudaMemcpyAsync(hit_ring + slot, hit_h + slot, (size_t)m * slot * sizeof(A),
+                                          cudaMemcpyHostToDevice, H->stream),
+                          "hit upload")))
+          return st;
+        if ((st = H->cuda(cudaEventRecord(hit_ev, H->stream), "hit event"))) return st;
+      }
+      for (int k = 0; k < m; k++) {
+        bind_pops(cur);
+        P.hit_prev = hit ? hit_ring + (size_t)k * slot : nullptr;
+        P.hit_cur = hit ? hit_ring + (size_t)(k + 1) * slot : nullptr;
+        if (c.flags & CH4_F_FLUID_LES)
+          if ((st = les_u())) return st;
+        if ((st = H->cuda(launch_step(P, shape, H->stream), "lb_step"))) return st;
+        cur ^= 1;
+        H->itime++;
+      }
+      if (hit && (st = H->cuda(cudaMemcpyAsync(hit_last, hit_ring + (size_t)m * slot, slot * sizeof(A),
+                                               cudaMemcpyDeviceToDevice, H->stream),
+                               "hit last")))
+        return st;
+      done += m;
+    }
+    return CH4_OK;
+  }
+
+  ch4_status fields(double* dens, double* u, double* t, double* s, double* force, int brd) override {
+    bind_pops(cur);
+    ch4_status st;
+    double* d = nullptr;
+    const size_t n1 = (size_t)N;
+    // scratch planes: dens | u (3) | t | s | force (3)
+    if ((st = H->cuda(cudaMalloc(&d, 9 * n1 * sizeof(double)), "fields scratch"))) return st;
+    double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *dfo = d + 6 * n1;
+    const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
+    st = H->cuda(launch_hydro(P, shape, hit, nullptr, dd, du, nsets_on[1] ? dt : nullptr, nsets_on[2] ? ds : nullptr,
+                              dfo, nullptr, H->stream),
+                 "hydro");
+    std::vector<double> hbuf(9 * n1);
+    if (!st) st = H->cuda(cudaMemcpyAsync(hbuf.data(), d, 9 * n1 * sizeof(double), cudaMemcpyDeviceToHost, H->stream),
+                          "fields download");
+    if (!st) st = H->cuda(cudaStreamSynchronize(H->stream), "fields sync");
+    cudaFree(d);
+    if (st) return st;
+    const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
+    for (int z = 0; z < c.NZ; z++)
+      for (int y = 0; y < c.NY; y++)
+        for (int x = 0; x < c.NX; x++) {
+          size_t i = ((size_t)z * c.NY + y) * c.NX + x;
+          size_t o = ((size_t)(z + brd) * PY + (y + brd)) * PX + (x + brd);
+          if (dens) dens[o] = hbuf[i];
+          if (u)
+            for (int a = 0; a < 3; a++) u[3 * o + a] = hbuf[(1 + a) * n1 + i];
+          if (t) t[o] = nsets_on[1] ? hbuf[4 * n1 + i] : 0.0;
+          if (s) s[o] = nsets_on[2] ? hbuf[5 * n1 + i] : 0.0;
+          if (force)
+            for (int a = 0; a < 3; a++) force[3 * o + a] = hbuf[(6 + a) * n1 + i];
+        }
+    return CH4_OK;
+  }
+};
+
+int set_of(char which) { return which == 'p' ? 0 : which == 'g' ? 1 : which == 'h' ? 2 : -1; }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+
+extern "C" {
+
+ch4_status ch4_config_default(ch4_config* cfg) {
+  if (!cfg) return CH4_ERR_ARG;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->NX = cfg->NY = cfg->NZ = 1;
+  cfg->flags = CH4_F_LB_FLUID;
+  cfg->storage = CH4_STORE_F64;
+  cfg->SX = cfg->SY = cfg->SZ = 1.0;
+  cfg->time_dt = 1.0;
+  cfg->tau_u = cfg->tau_t = cfg->tau_s = 1.0;
+  cfg->C_smag = 0.18;  // src/les.c:10
+  cfg->time_dt_lagr_factor = 1.0;
+  cfg->seed = 1;
+  return CH4_OK;
+}
+
+// read_parameter of src/parameters.c:3-39: scan "%s %lf" pairs from the start
+// of the file until the name matches; the first number after the key wins.
+ch4_status ch4_read_parameter(const char* path, const char* key, double* value) {
+  if (!path || !key || !value) return CH4_ERR_ARG;
+  FILE* fin = std::fopen(path, "r");
+  if (!fin) return CH4_ERR_PARAM;
+  char name[256] = "NULL";
+  double val;
+  for (;;) {
+    val = 0.0;
+    if (std::fscanf(fin, "%255s %lf", name, &val) < 0 && !std::feof(fin)) break;
+    if (std::strcmp(name, key) == 0) {
+      std::fclose(fin);
+      *value = val;
+      return CH4_OK;
+    }
+    if (std::feof(fin)) break;
+  }
+  std::fclose(fin);
+  return CH4_ERR_PARAM;
+}
+
+static void put_bad(char* bad, size_t n, const std::string& s) {
+  if (bad && n) {
+    std::strncpy(bad, s.c_str(), n - 1);
+    bad[n - 1] = 0;
+  }
+}
+
+ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, size_t bad_len) {
+  if (!cfg || !path) return CH4_ERR_ARG;
+  struct K {
+    const char* name;
+    double* dst;
+    bool needed;
+  };
+  double NX, NY, NZ, particle_number = 0;
+  const uint64_t fl = cfg->flags;
+  const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
+  const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
+  const bool grav = forcing && (fl & (CH4_F_TEMPERATURE_BUOYANCY | CH4_F_SCALAR_BUOYANCY));
+  std::vector<K> keys = {
+      {"NX", &NX, true}, {"NY", &NY, true}, {"NZ", &NZ, true}, {"SX", &cfg->SX, true}, {"SY", &cfg->SY, true},
+      {"SZ", &cfg->SZ, true}, {"time_dt", &cfg->time_dt, true}, {"tau_u", &cfg->tau_u, true},
+      {"Amp_x", &cfg->Amp_x, forcing}, {"Amp_y", &cfg->Amp_y, forcing}, {"Amp_z", &cfg->Amp_z, forcing},
+      {"gravity_x", &cfg->gravity_x, grav}, {"gravity_y", &cfg->gravity_y, grav}, {"gravity_z", &cfg->gravity_z, grav},
+      {"tau_t", &cfg->tau_t, T}, {"T_bot", &cfg->T_bot, T}, {"T_top", &cfg->T_top, T}, {"T_ref", &cfg->T_ref, T},
+      {"grad_T_bot", &cfg->grad_T_bot, T}, {"grad_T_top", &cfg->grad_T_top, T},
+      {"beta_t", &cfg->beta_t, T && (fl & CH4_F_TEMPERATURE_BUOYANCY)},
+      {"beta2_t", &cfg->beta2_t, T && (fl & CH4_F_TEMPERATURE_BUOYANCY)}, {"tau_s", &cfg->tau_s, S},
+      {"S_bot", &cfg->S_bot, S}, {"S_top", &cfg->S_top, S}, {"S_ref", &cfg->S_ref, S},
+      {"beta_s", &cfg->beta_s, S && (fl & CH4_F_SCALAR_BUOYANCY)},
+      {"time_dt_lagr_factor", &cfg->time_dt_lagr_factor, (fl & CH4_F_LAGRANGE) != 0},
+      {"particle_number", &particle_number, (fl & CH4_F_LAGRANGE) != 0},
+  };
+  for (auto& k : keys) {
+    if (!k.needed) continue;
+    double v;
+    ch4_status st = ch4_read_parameter(path, k.name, &v);
+    if (st != CH4_OK) {
+      put_bad(bad, bad_len, k.name);
+      return CH4_ERR_PARAM;
+    }
+    *k.dst = v;
+  }
+  cfg->NX = (int)NX;
+  cfg->NY = (int)NY;
+  cfg->NZ = (int)NZ;
+  cfg->particle_number = (int)particle_number;
+  // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
+  cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
+  cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;
+  cfg->chi = (cfg->tau_s - 0.5 * cfg->time_dt) / 3.0;
+  cfg->deltaT = cfg->T_bot - cfg->T_top;
+  cfg->deltaS = cfg->S_bot - cfg->S_top;
+  return CH4_OK;
+}
+
+ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, size_t bad_len) {
+  if (!cfg || !path) return CH4_ERR_ARG;
+  FILE* fp = std::fopen(path, "r");
+  if (!fp) return CH4_ERR_ARG;
+  std::string txt;
+  char buf[4096];
+  size_t n;
+  while ((n = std::fread(buf, 1, sizeof buf, fp)) > 0) txt.append(buf, n);
+  std::fclose(fp);
+  // strip comments
+  std::string clean;
+  for (size_t i = 0; i < txt.size();) {
+    if (txt.compare(i, 2, "//") == 0) {
+      while (i < txt.size() && txt[i] != '\n') i++;
+    } else if (txt.compare(i, 2, "/*") == 0) {
+      size_t e = txt.find("*/", i + 2);
+      i = e == std::string::npos ? txt.size() : e + 2;
+      clean += ' ';
+    } else {
+      clean += txt[i++];
+    }
+  }
+  struct M {
+    const char* name;
+    uint64_t bit;
+  };
+  static const M map[] = {
+      {"LB_FLUID", CH4_F_LB_FLUID},
+      {"LB_FLUID_FORCING", CH4_F_LB_FLUID_FORCING},
+      {"LB_FLUID_FORCING_KOLMOGOROV", CH4_F_FORCING_KOLMOGOROV},
+      {"LB_FLUID_FORCING_POISEUILLE", CH4_F_FORCING_POISEUILLE},
+      {"LB_FLUID_FORCING_HIT", CH4_F_FORCING_HIT},
+      {"LB_FLUID_FORCING_NOZEROMODE", CH4_F_FORCING_NOZEROMODE},
+      {"LB_TEMPERATURE", CH4_F_LB_TEMPERATURE},
+      {"LB_TEMPERATURE_BUOYANCY", CH4_F_TEMPERATURE_BUOYANCY},
+      {"LB_SCALAR", CH4_F_LB_SCALAR},
+      {"LB_SCALAR_BUOYANCY", CH4_F_SCALAR_BUOYANCY},
+      {"LB_FLUID_BC_Y", CH4_F_FLUID_BC_Y},
+      {"LB_FLUID_BC_Y_P_SLIP", CH4_F_FLUID_BC_Y_P_SLIP},
+      {"LB_FLUID_BC_Y_M_SLIP", CH4_F_FLUID_BC_Y_M_SLIP},
+      {"LB_TEMPERATURE_BC_Y", CH4_F_TEMPERATURE_BC_Y},
+      {"LB_TEMPERATURE_BC_Y_P_FLUX", CH4_F_TEMPERATURE_BC_Y_P_FLUX},
+      {"LB_TEMPERATURE_BC_Y_M_FLUX", CH4_F_TEMPERATURE_BC_Y_M_FLUX},
+      {"LB_TEMPERATURE_BC_Y_P_NOFLUX", CH4_F_TEMPERATURE_BC_Y_P_NOFLUX},
+      {"LB_TEMPERATURE_BC_Y_M_NOFLUX", CH4_F_TEMPERATURE_BC_Y_M_NOFLUX},
+      {"LB_SCALAR_BC_Y", CH4_F_SCALAR_BC_Y},
+      {"LB_FLUID_LES", CH4_F_FLUID_LES},
+      {"LAGRANGE", CH4_F_LAGRANGE},
+      {"LAGRANGE_GRADIENT", CH4_F_LAGRANGE_GRADIENT},
+      {"LAGRANGE_ADDEDMASS", CH4_F_LAGRANGE_ADDEDMASS},
+      {"LAGRANGE_TWOWAY", CH4_F_LAGRANGE_TWOWAY},
+      {"LAGRANGE_TWOWAY_MOMENTUM", CH4_F_LAGRANGE_TWOWAY_MOMENTUM},
+      {"LB_TEMPERATURE_FORCING", CH4_F_TEMPERATURE_FORCING},
+      {"LAGRANGE_WRAP", CH4_F_LAGRANGE_WRAP},
+      {"LAGRANGE_GRADIENT_BRD2", CH4_F_LAGRANGE_GRADIENT_BRD2},
+  };
+  // flags that select the configuration the hot path already is, or that only
+  // concern I/O, timing, debugging or initial-state generation
+  static const char* neutral[] = {"LB", "GRID_REGULAR", "GRID_POP_D3Q19", "METHOD_STREAMING", "METHOD_EDGES_AND_CORNERS",
+                                  "METHOD_FORCING_GUO", "LB_FLUID_FORCING_GRAVITY", "LB_FLUID_BC", "LB_TEMPERATURE_BC",
+                                  "LB_SCALAR_BC", "SYSTEM_RANDOM48", "SYSTEM_TIMING", "TIMING", "NEW_SENDRECV",
+                                  "OUTPUT_H5", "OUTPUT_H5_GRID", "OUTPUT_H5_TIMESTAMP_REAL", "OUTPUT_AT_START",
+                                  "OUTPUT_ASCII", "OUTPUT_DIAGN_APPEND", "VERBOSE", "LB_TEMPERATURE_BUOYANCY_T0_REF",
+                                  "LB_TEMPERATURE_BUOYANCY_T0_TOP", "LB_TEMPERATURE_BUOYANCY_T0_BOT", "LB_FLUID_LES_OUTPUT"};
+  uint64_t flags = 0;
+  int t0 = CH4_T0_MEAN;
+  bool d3q19 = false, streaming = false;
+  size_t pos = 0;
+  while ((pos = clean.find("#define", pos)) != std::string::npos) {
+    pos += 7;
+    while (pos < clean.size() && (clean[pos] == ' ' || clean[pos] == '\t')) pos++;
+    size_t e = pos;
+    while (e < clean.size() && (std::isalnum((unsigned char)clean[e]) || clean[e] == '_')) e++;
+    std::string name = clean.substr(pos, e - pos);
+    pos = e;
+    if (name.empty()) continue;
+    if (name == "GRID_POP_D3Q19") d3q19 = true;
+    if (name == "METHOD_STREAMING") streaming = true;
+    if (name == "LB_TEMPERATURE_BUOYANCY_T0_REF") t0 = CH4_T0_REF;
+    if (name == "LB_TEMPERATURE_BUOYANCY_T0_TOP") t0 = CH4_T0_TOP;
+    if (name == "LB_TEMPERATURE_BUOYANCY_T0_BOT") t0 = CH4_T0_BOT;
+    bool known = false;
+    for (const M& m : map)
+      if (name == m.name) {
+        flags |= m.bit;
+        known = true;
+      }
+    for (const char* nn : neutral)
+      if (name == nn) known = true;
+    if (!known && (name.rfind("DEBUG", 0) == 0 || name.find("_INITIAL_") != std::string::npos)) known = true;
+    if (!known) {
+      put_bad(bad, bad_len, name);
+      return CH4_ERR_UNSUPPORTED;
+    }
+  }
+  if (!d3q19) {
+    put_bad(bad, bad_len, "GRID_POP_D3Q19 (required)");
+    return CH4_ERR_UNSUPPORTED;
+  }
+  if (!streaming) {
+    put_bad(bad, bad_len, "METHOD_STREAMING (required)");
+    return CH4_ERR_UNSUPPORTED;
+  }
+  cfg->flags = flags | CH4_F_LB_FLUID;
+  cfg->t0_kind = t0;
+  return CH4_OK;
+}
+
+static ch4_status validate(const ch4_config* c, std::string& why) {
+  if (c->NX < 1 || c->NY < 1 || c->NZ < 1) return why = "lattice size must be positive", CH4_ERR_ARG;
+  if ((long long)c->NX * c->NY * c->NZ > (1ll << 34)) return why = "lattice too large", CH4_ERR_ARG;
+  if (c->flags & ~SUPPORTED) return why = "flag outside the implemented hot path", CH4_ERR_UNSUPPORTED;
+  if (c->storage < 0 || c->storage > 2) return why = "unknown storage", CH4_ERR_ARG;
+  if (c->time_dt != 1.0 || c->SX != c->NX || c->SY != c->NY || c->SZ != c->NZ)
+    return why = "streaming requires time_dt = 1 and S = N (src/parameters.c:135)", CH4_ERR_UNSUPPORTED;
+  if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
+    return why = "walls need NY >= 3", CH4_ERR_ARG;
+  if (!(c->tau_u > 0.5)) return why = "tau_u must exceed 0.5", CH4_ERR_ARG;
+  return CH4_OK;
+}
+
+ch4_status ch4_device_bytes(const ch4_config* cfg, size_t* bytes) {
+  if (!cfg || !bytes) return CH4_ERR_ARG;
+  std::string why;
+  ch4_status st = validate(cfg, why);
+  if (st) return st;
+  ch4_handle tmp;
+  tmp.cfg = *cfg;
+  if (cfg->storage == CH4_STORE_F64) *bytes = Engine<double>(&tmp).device_bytes();
+  else *bytes = Engine<float>(&tmp).device_bytes();
+  return CH4_OK;
+}
+
+ch4_status ch4_create(const ch4_config* cfg, ch4_handle** out) {
+  if (!cfg || !out) return CH4_ERR_ARG;
+  *out = nullptr;
+  std::string why;
+  ch4_status st = validate(cfg, why);
+  if (st) {
+    std::fprintf(stderr, "ch4_create: %s\n", why.c_str());
+    return st;
+  }
+  auto* h = new ch4_handle();
+  h->cfg = *cfg;
+  // srand48(seed) state (src/parallel.c:238-240 with a fixed seed)
+  h->rng[0] = 0x330E;
+  h->rng[1] = (unsigned short)(cfg->seed & 0xFFFF);
+  h->rng[2] = (unsigned short)((cfg->seed >> 16) & 0xFFFF);
+  std::memset(h->phi, 0, sizeof h->phi);
+  for (int ii = 0; ii < NK; ii++) {
+    double vk2 = VK[ii][0] * VK[ii][0] + VK[ii][1] * VK[ii][1] + VK[ii][2] * VK[ii][2];
+    h->hit_fac[ii] = std::pow(vk2, -2. / 6.);
+  }
+  if (cfg->flags & CH4_F_FORCING_HIT)  // initial phases, src/initial_conditions.c:863-869
+    for (int ii = 0; ii < NK; ii++)
+      for (int a = 0; a < 3; a++) h->phi[ii][a] = h->myrand();
+  if ((st = h->cuda(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream"))) {
+    delete h;
+    return st;
+  }
+  if (cfg->storage == CH4_STORE_F64) h->eng.reset(new Engine<double>(h));
+  else h->eng.reset(new Engine<float>(h));
+  if ((st = h->eng->alloc())) {
+    std::fprintf(stderr, "ch4_create: %s\n", h->err.c_str());
+    h->eng.reset();
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return st;
+  }
+  *out = h;
+  return CH4_OK;
+}
+
+ch4_status ch4_destroy(ch4_handle* h) {
+  if (!h) return CH4_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  h->eng.reset();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return CH4_OK;
+}
+
+const char* ch4_last_error(const ch4_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+ch4_status ch4_set_pop(ch4_handle* h, char which, const double* aos, int brd) {
+  if (!h || !aos || brd < 0) return CH4_ERR_ARG;
+  int s = set_of(which);
+  if (s < 0) return h->fail(CH4_ERR_ARG, "unknown population '%c'", which);
+  return h->eng->set_pop(s, aos, brd);
+}
+
+ch4_status ch4_get_pop(ch4_handle* h, char which, double* aos, int brd) {
+  if (!h || !aos || brd < 0) return CH4_ERR_ARG;
+  int s = set_of(which);
+  if (s < 0) return h->fail(CH4_ERR_ARG, "unknown population '%c'", which);
+  return h->eng->get_pop(s, aos, brd);
+}
+
+ch4_status ch4_set_hit_phases(ch4_handle* h, const double* phi) {
+  if (!h || !phi) return CH4_ERR_ARG;
+  for (int ii = 0; ii < NK; ii++)
+    for (int a = 0; a < 3; a++) h->phi[ii][a] = phi[3 * ii + a];
+  h->initialized = false;
+  return CH4_OK;
+}
+
+ch4_status ch4_get_hit_phases(ch4_handle* h, double* phi) {
+  if (!h || !phi) return CH4_ERR_ARG;
+  for (int ii = 0; ii < NK; ii++)
+    for (int a = 0; a < 3; a++) phi[3 * ii + a] = h->phi[ii][a];
+  return CH4_OK;
+}
+
+ch4_status ch4_set_particles(ch4_handle* h, const ch4_particle*, int) {
+  if (!h) return CH4_ERR_ARG;
+  return h->fail(CH4_ERR_UNSUPPORTED, "particles are not enabled in this build");
+}
+
+ch4_status ch4_get_particles(ch4_handle* h, ch4_particle*, int) {
+  if (!h) return CH4_ERR_ARG;
+  return h->fail(CH4_ERR_UNSUPPORTED, "particles are not enabled in this build");
+}
+
+ch4_status ch4_initialize(ch4_handle* h) {
+  if (!h) return CH4_ERR_ARG;
+  ch4_status st = h->eng->initialize();
+  if (!st) h->initialized = true;
+  return st;
+}
+
+ch4_status ch4_step(ch4_handle* h, int nsteps) {
+  if (!h || nsteps < 0) return CH4_ERR_ARG;
+  if (!h->initialized) return h->fail(CH4_ERR_STATE, "ch4_step before ch4_initialize");
+  return h->eng->step(nsteps);
+}
+
+ch4_status ch4_synchronize(ch4_handle* h) {
+  if (!h) return CH4_ERR_ARG;
+  return h->cuda(cudaStreamSynchronize(h->stream), "synchronize");
+}
+
+ch4_status ch4_get_stream(ch4_handle* h, void** stream) {
+  if (!h || !stream) return CH4_ERR_ARG;
+  *stream = (void*)h->stream;
+  return CH4_OK;
+}
+
+ch4_status ch4_get_fields(ch4_handle* h, double* dens, double* u, double* t, double* s, int brd) {
+  if (!h || brd < 0) return CH4_ERR_ARG;
+  return h->eng->fields(dens, u, t, s, nullptr, brd);
+}
+
+ch4_status ch4_get_force(ch4_handle* h, double* force, int brd) {
+  if (!h || !force || brd < 0) return CH4_ERR_ARG;
+  return h->eng->fields(nullptr, nullptr, nullptr, nullptr, force, brd);
+}
+
+ch4_status ch4_averages_get(ch4_handle* h, ch4_averages* out) {
+  if (!h || !out) return CH4_ERR_ARG;
+  return h->fail(CH4_ERR_UNSUPPORTED, "averages not built yet");
+}
+
+ch4_status ch4_get_itime(const ch4_handle* h, int* itime) {
+  if (!h || !itime) return CH4_ERR_ARG;
+  *itime = h->itime;
+  return CH4_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// D3Q19 lattice, per-launch parameter block and population storage codecs for
+// the B200 lattice-Boltzmann step.
+//
+// Lattice tables: src/lb.c:139-230 (weights, velocities, opposite directions).
+// Populations live on the device as SoA planes f[q][z][y][x] (x fastest), one
+// plane per direction q, so every warp access is a contiguous row segment.
+#pragma once
+#include <cuda_fp16.h>
+#include <cstdint>
+
+namespace ch4 {
+
+constexpr int Q = 19;
+constexpr int NK = 6;  // HIT forcing modes, src/initial_conditions.c:841-849
+
+__host__ __device__ constexpr int cx(int q) {
+  return q == 1 || q == 7 || q == 8 || q == 11 || q == 13 ? 1 : (q == 2 || q == 9 || q == 10 || q == 12 || q == 14 ? -1 : 0);
+}
+__host__ __device__ constexpr int cy(int q) {
+  return q == 3 || q == 7 || q == 9 || q == 15 || q == 16 ? 1 : (q == 4 || q == 8 || q == 10 || q == 17 || q == 18 ? -1 : 0);
+}
+__host__ __device__ constexpr int cz(int q) {
+  return q == 5 || q == 11 || q == 12 || q == 15 || q == 17 ? 1 : (q == 6 || q == 13 || q == 14 || q == 16 || q == 18 ? -1 : 0);
+}
+// opposite direction inv[q] and the y-mirror inv_y[q]
+__host__ __device__ constexpr int qinv(int q) {
+  return q == 0 ? 0 : (q <= 6 ? (q % 2 ? q + 1 : q - 1) : (q <= 10 ? 17 - q : (q <= 14 ? 25 - q : 33 - q)));
+}
+__host__ __device__ constexpr int qinv_y(int q) {
+  return q == 3 ? 4 : q == 4 ? 3 : q == 7 ? 8 : q == 8 ? 7 : q == 9 ? 10 : q == 10 ? 9 :
+         q == 15 ? 17 : q == 17 ? 15 : q == 16 ? 18 : q == 18 ? 16 : q;
+}
+
+// runtime feature bits (uniform over the grid)
+enum : uint32_t {
+  K_FORCING = 1u << 0,
+  K_KOLMO = 1u << 1,
+  K_POIS = 1u << 2,
+  K_HIT = 1u << 3,
+  K_BUOY = 1u << 4,
+  K_SBUOY = 1u << 5,
+  K_FWALL = 1u << 6,    // fluid walls at y = 0 and y = NY-1
+  K_FSLIP_P = 1u << 7,  // top wall specular
+  K_FSLIP_M = 1u << 8,  // bottom wall specular
+  K_TWALL = 1u << 9,
+  K_TFLUX_P = 1u << 10,
+  K_TFLUX_M = 1u << 11,
+  K_TNOFLUX_P = 1u << 12,
+  K_TNOFLUX_M = 1u << 13,
+  K_SWALL = 1u << 14,
+  K_LES = 1u << 15,
+  K_TWOWAY = 1u << 16,
+  K_BETA2 = 1u << 17,
+  K_TSRC = 1u << 18
+};
+
+template <typename A>
+struct StepParams {
+  int NX, NY, NZ;
+  long long N;  // cells
+  uint32_t feat;
+  // populations (storage type erased; cast in the kernel)
+  const void* fin[3];
+  void* fout[3];
+  // previous-step temperature / scalar (t^{n-1}), read and overwritten in place
+  A* tprev;
+  A* sprev;
+  // LES: u^n (3 SoA planes) and per-cell relaxation time output
+  const A* ules;
+  A* tau_les;
+  // two-way coupling deposit of this and the previous step (3 SoA planes each)
+  const A* dcur;
+  const A* dprev;
+  // constants (host-computed in FP64, then cast)
+  A w[Q];
+  A facw[Q];  // (1 - dt/(2 tau_u)) * w_q, the Guo prefactor of src/forcing.c:1289,1432
+  A invcs2, invcs4, invtwocs2, invtwocs4;
+  A invtau[3];
+  A hdt;  // 0.5*time_dt
+  A nu, csmag2;  // LES: nu and pow(C_smag*1, 2)
+  // storage shift (rho0 for p, T0 for g, S0 for h) used by the F16 codec
+  float shift[3];
+  // forcing
+  A pois[3];
+  const A* kol;  // [NY] F.x(y), [NX] F.y(x), [NY] F.z(y)
+  const A* hit_prev;  // [NK][NX+NY+NZ]: ax | ay | az sin tables
+  const A* hit_cur;
+  A hitamp[NK][3];  // pow(k^2,-1/3)*Amp_{x,y,z}
+  A T0, beta_t, beta2_t, S0, beta_s;
+  A grav[3];
+  // thermal / scalar walls
+  A T_top, T_bot, T_ref, grad_T_top, grad_T_bot;
+  A S_top, S_bot, S_ref;
+};
+
+#ifdef __CUDACC__
+// ---- storage codecs ------------------------------------------------------
+template <typename S, typename A>
+struct Codec;
+
+template <>
+struct Codec<double, double> {
+  __device__ __forceinline__ static double load(const double* p, long long i, double, double) { return __ldg(p + i); }
+  __device__ __forceinline__ static void store(double* p, long long i, double v, double, double) { p[i] = v; }
+};
+template <>
+struct Codec<float, float> {
+  __device__ __forceinline__ static float load(const float* p, long long i, float, float) { return __ldg(p + i); }
+  __device__ __forceinline__ static void store(float* p, long long i, float v, float, float) { p[i] = v; }
+};
+// IEEE half holding the deviation f_q - w_q * shift
+template <>
+struct Codec<__half, float> {
+  __device__ __forceinline__ static float load(const __half* p, long long i, float w, float shift) {
+    return __half2float(__ldg(p + i)) + w * shift;
+  }
+  __device__ __forceinline__ static void store(__half* p, long long i, float v, float w, float shift) {
+    p[i] = __float2half_rn(v - w * shift);
+  }
+};
+
+#endif  // __CUDACC__
+
+}  // namespace ch4

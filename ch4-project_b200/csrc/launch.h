@@ -1,0 +1,38 @@
+// Host-side launchers of the lattice-Boltzmann kernels (one set per arithmetic
+// precision; the FP64 set lives in lb_f64.cu, built without FMA contraction).
+#pragma once
+#include <cuda_runtime.h>
+#include "lattice.cuh"
+
+namespace ch4 {
+
+struct LaunchShape {
+  bool therm, scal;
+  int storage;  // 0 f64, 1 f32, 2 f16
+};
+
+// fused collide-force-stream step
+cudaError_t launch_step(const StepParams<double>& P, LaunchShape s, cudaStream_t st);
+cudaError_t launch_step(const StepParams<float>& P, LaunchShape s, cudaStream_t st);
+// t^{n-1} := m(g), s^{n-1} := m(h)
+cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStream_t st);
+cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStream_t st);
+// hydro fields / force (FP64 outputs), optional arithmetic-precision u planes
+cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep, double* dens,
+                         double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st);
+cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep, double* dens,
+                         double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st);
+// compact AoS chunk <-> SoA storage for one population set
+cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
+                              int nz, cudaStream_t st);
+cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
+                              int nz, cudaStream_t st);
+cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
+                              int nz, cudaStream_t st);
+cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
+                              int nz, cudaStream_t st);
+
+// block shape of the fused step kernel
+constexpr int STEP_BLOCK_X = 128;
+
+}  // namespace ch4

@@ -1,0 +1,453 @@
+// Fused lattice-Boltzmann step kernels (templated on storage S and arithmetic A).
+//
+// One launch = one iteration of the reference driver loop for the populations
+// (src/main.c:67-161 with METHOD_STREAMING): BGK collision (src/fluid.c:1033-1226)
+// with the equilibrium of src/lb.c:382-415, the build_forcing terms
+// (src/forcing.c:360-707), Guo forcing (src/forcing.c:1423-1435), the wall rules of
+// boundary_and_pbc_conditions_for_streaming (src/boundary_conditions.c:419-1524)
+// and streaming (src/lb.c:544-584), for the fluid p, temperature g and scalar h
+// sets.  Each population is read once and written once.
+//
+// Push form: the state between launches is the post-streaming f^n (exactly the
+// reference's p/g/h arrays).  A thread owns one cell, collides it, and writes
+// each post-collision value to the neighbour x + c_q; a value that would cross a
+// wall is written where the reference's wall loop puts it (the slot the
+// neighbour would pull from the halo), so the periodic and wall halos of the
+// reference never exist in memory.
+//
+// Arithmetic keeps the reference's operand order.  The FP64 instantiation is
+// compiled with FMA contraction off, which makes it bit-identical to the
+// reference CPU build.
+#pragma once
+#include "lattice.cuh"
+
+namespace ch4 {
+
+// c_q . u in the reference's order ((cx*ux + cy*uy) + cz*uz) with the zero
+// terms dropped (value-identical: the dropped terms are +-0).
+template <int q, typename A>
+__device__ __forceinline__ A cdot(A ux, A uy, A uz) {
+  constexpr int a = cx(q), b = cy(q), c = cz(q);
+  A r = A(0);
+  bool have = false;
+  if constexpr (a != 0) {
+    r = a > 0 ? ux : -ux;
+    have = true;
+  }
+  if constexpr (b != 0) {
+    A t = b > 0 ? uy : -uy;
+    r = have ? r + t : t;
+    have = true;
+  }
+  if constexpr (c != 0) {
+    A t = c > 0 ? uz : -uz;
+    r = have ? r + t : t;
+  }
+  (void)have;
+  return r;
+}
+
+// (c - u) * invcs2 + c * cu * invcs4 for one component (src/forcing.c:1427-1429)
+template <int cc, typename A>
+__device__ __forceinline__ A guo_d(A u, A cu, A invcs2, A invcs4) {
+  if constexpr (cc == 0) return (-u) * invcs2;
+  else if constexpr (cc > 0) return (A(1) - u) * invcs2 + cu * invcs4;
+  else return (A(-1) - u) * invcs2 + (-cu) * invcs4;
+}
+
+// m(), mvx(), mvy(), mvz() of src/typedef.h:286-291, fixed left-to-right order
+template <typename A>
+__device__ __forceinline__ A mom0(const A* a) {
+  return a[0] + a[1] + a[2] + a[3] + a[4] + a[5] + a[6] + a[7] + a[8] + a[9] + a[10] + a[11] + a[12] + a[13] + a[14] +
+         a[15] + a[16] + a[17] + a[18];
+}
+template <typename A>
+__device__ __forceinline__ A momx(const A* a) {
+  return a[1] - a[2] + a[7] + a[8] - a[9] - a[10] + a[11] - a[12] + a[13] - a[14];
+}
+template <typename A>
+__device__ __forceinline__ A momy(const A* a) {
+  return a[3] - a[4] + a[7] - a[8] + a[9] - a[10] + a[15] + a[16] - a[17] - a[18];
+}
+template <typename A>
+__device__ __forceinline__ A momz(const A* a) {
+  return a[5] - a[6] + a[11] + a[12] - a[13] - a[14] + a[15] - a[16] + a[17] - a[18];
+}
+
+// Per-cell force of build_forcing's grid loop (src/forcing.c:360-707) plus the
+// two-way deposit (src/lagrange_feedback.c:245-254), in the reference's order.
+template <typename A>
+__device__ __forceinline__ void cell_force(const StepParams<A>& P, int x, int y, int z, long long idx, A t, A s,
+                                           const A* hit, const A* dep, A& fx, A& fy, A& fz) {
+  fx = A(0);
+  fy = A(0);
+  fz = A(0);
+  const uint32_t F = P.feat;
+  if (F & K_POIS) {
+    fx += P.pois[0];
+    fy += P.pois[1];
+    fz += P.pois[2];
+  }
+  if (F & K_KOLMO) {
+    fx += P.kol[y];
+    fy += P.kol[P.NY + x];
+    fz += P.kol[P.NY + P.NX + y];
+  }
+  if (F & K_HIT) {
+    const int L = P.NX + P.NY + P.NZ;
+#pragma unroll
+    for (int ii = 0; ii < NK; ii++) {
+      const A ax = hit[ii * L + x], ay = hit[ii * L + P.NX + y], az = hit[ii * L + P.NX + P.NY + z];
+      fx += P.hitamp[ii][0] * (ay + az);
+      fy += P.hitamp[ii][1] * (ax + az);
+      fz += P.hitamp[ii][2] * (ay + ax);
+    }
+  }
+  if (F & K_BUOY) {
+    A temp = t - P.T0;
+    A fac = P.beta_t * temp;
+    if (F & K_BETA2) fac += P.beta2_t * temp * temp;
+    fx += fac * P.grav[0];
+    fy += fac * P.grav[1];
+    fz += fac * P.grav[2];
+  }
+  if (F & K_SBUOY) {
+    A temp = s - P.S0;
+    A fac = P.beta_s * temp;
+    fx += fac * P.grav[0];
+    fy += fac * P.grav[1];
+    fz += fac * P.grav[2];
+  }
+  if (dep) {
+    fx += dep[idx];
+    fy += dep[P.N + idx];
+    fz += dep[2 * P.N + idx];
+  }
+}
+
+__device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// Smagorinsky relaxation time of src/les.c:5-269 (centred differences of
+// src/gradients.c:78-~240, one-sided 2nd order at the y walls)
+template <typename A>
+__device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z) {
+  const int NX = P.NX, NY = P.NY, NZ = P.NZ;
+  const long long N = P.N;
+  const A* u = P.ules;
+  auto at = [&](int a, int i, int j, int k) { return u[a * N + ((long long)k * NY + j) * NX + i]; };
+  A g[3][3];
+  const int xp = wrap(x + 1, NX), xm = wrap(x - 1, NX), zp = wrap(z + 1, NZ), zm = wrap(z - 1, NZ);
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    g[a][0] = (at(a, xp, y, z) - at(a, xm, y, z)) / A(2);
+    g[a][2] = (at(a, x, y, zp) - at(a, x, y, zm)) / A(2);
+  }
+  const bool walls = (P.feat & K_FWALL) != 0;
+  if (walls && y == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) g[a][1] = A(-1.5) * at(a, x, 0, z) + A(2) * at(a, x, 1, z) + A(-0.5) * at(a, x, 2, z);
+  } else if (walls && y == NY - 1) {
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+      g[a][1] = A(1.5) * at(a, x, NY - 1, z) + A(-2) * at(a, x, NY - 2, z) + A(0.5) * at(a, x, NY - 3, z);
+  } else {
+    const int yp = wrap(y + 1, NY), ym = wrap(y - 1, NY);
+#pragma unroll
+    for (int a = 0; a < 3; a++) g[a][1] = (at(a, x, yp, z) - at(a, x, ym, z)) / A(2);
+  }
+  const A xx = g[0][0], xy = g[0][1], xz = g[0][2];
+  const A yx = g[1][0], yy = g[1][1], yz = g[1][2];
+  const A zx = g[2][0], zy = g[2][1], zz = g[2][2];
+  const A s_norm = sqrt(A(0.5) * ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) +
+                                  (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
+                                  (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
+  const A nu_les = s_norm * P.csmag2;
+  return A(3) * (nu_les + P.nu) + A(0.5);
+}
+
+// ---- the fused step -------------------------------------------------------
+
+template <typename S, typename A, int set>
+__device__ __forceinline__ void load_set(const StepParams<A>& P, long long idx, A* f) {
+  const S* in = static_cast<const S*>(P.fin[set]);
+#pragma unroll
+  for (int q = 0; q < Q; q++) f[q] = Codec<S, A>::load(in, (long long)q * P.N + idx, P.w[q], P.shift[set]);
+}
+
+// push one set; `wallmode`: 0 periodic in y, 1 fluid walls, 2 value walls (T or S)
+template <typename S, typename A, int set>
+__device__ __forceinline__ void push_set(const StepParams<A>& P, int x, int y, int z, long long idx, const A* post,
+                                         int wallmode, bool slip_top, bool slip_bot, A fac_top, A fac_bot) {
+  S* out = static_cast<S*>(P.fout[set]);
+  const int NX = P.NX, NY = P.NY, NZ = P.NZ;
+  const long long N = P.N;
+  const float sh = P.shift[set];
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const int ty = y + cy(q);
+    const int tx = wrap(x + cx(q), NX);
+    const int tz = wrap(z + cz(q), NZ);
+    if (cy(q) != 0 && wallmode != 0 && (ty < 0 || ty >= NY)) {
+      if (wallmode == 1) {
+        const bool slip = ty >= NY ? slip_top : slip_bot;
+        if (slip) {  // specular reflection, src/boundary_conditions.c:753,786
+          const long long d = ((long long)tz * NY + y) * NX + tx;
+          Codec<S, A>::store(out, (long long)qinv_y(q) * N + d, post[q], P.w[qinv_y(q)], sh);
+        } else {  // halfway bounce-back, src/boundary_conditions.c:775,798
+          Codec<S, A>::store(out, (long long)qinv(q) * N + idx, post[q], P.w[qinv(q)], sh);
+        }
+      } else {  // fixed value / flux wall: rhs(x).p[inv q] + w[inv q]*fac (src/boundary_conditions.c:1019-1027)
+        const int r = qinv(q);
+        const A fac = ty >= NY ? fac_top : fac_bot;
+        Codec<S, A>::store(out, (long long)r * N + idx, post[r] + P.w[r] * fac, P.w[r], sh);
+      }
+    } else {
+      const long long d = ((long long)tz * NY + wrap(ty, NY)) * NX + tx;
+      Codec<S, A>::store(out, (long long)q * N + d, post[q], P.w[q], sh);
+    }
+  }
+}
+
+template <typename S, typename A, bool THERM, bool SCAL>
+__global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int z = blockIdx.z;
+  if (x >= P.NX) return;
+  const long long idx = ((long long)z * P.NY + y) * P.NX + x;
+  const uint32_t F = P.feat;
+
+  A f[Q];
+  load_set<S, A, 0>(P, idx, f);
+  const A rho = mom0(f);
+  const A mx = momx(f), my = momy(f), mz = momz(f);
+
+  A g[Q], h[Q];
+  A tt = A(0), ss = A(0);
+  if constexpr (THERM) {
+    load_set<S, A, 1>(P, idx, g);
+    tt = mom0(g);
+  }
+  if constexpr (SCAL) {
+    load_set<S, A, 2>(P, idx, h);
+    ss = mom0(h);
+  }
+
+  // u^n = mv/rho + dt/2 F^{n-1} (src/lb.c:464-466); F^n for Guo (src/forcing.c:1423-1435)
+  A ux, uy, uz, Fx = A(0), Fy = A(0), Fz = A(0);
+  if (F & K_FORCING) {
+    A px, py, pz;
+    const A tp = THERM ? P.tprev[idx] : A(0);
+    const A sp = SCAL ? P.sprev[idx] : A(0);
+    cell_force(P, x, y, z, idx, tp, sp, P.hit_prev, (F & K_TWOWAY) ? P.dprev : nullptr, px, py, pz);
+    ux = mx / rho + P.hdt * px;
+    uy = my / rho + P.hdt * py;
+    uz = mz / rho + P.hdt * pz;
+    cell_force(P, x, y, z, idx, tt, ss, P.hit_cur, (F & K_TWOWAY) ? P.dcur : nullptr, Fx, Fy, Fz);
+  } else {
+    ux = mx / rho;
+    uy = my / rho;
+    uz = mz / rho;
+  }
+  if constexpr (THERM) P.tprev[idx] = tt;
+  if constexpr (SCAL) P.sprev[idx] = ss;
+
+  const A u2 = ux * ux + uy * uy + uz * uz;
+  A invtau = P.invtau[0];
+  if (F & K_LES) {
+    const A tl = les_tau(P, x, y, z);
+    P.tau_les[idx] = tl;
+    invtau = A(1) / tl;
+  }
+
+  // fluid: BGK + Guo, in place
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    A cu;
+    switch (q) {  // resolved at compile time after unrolling
+#define CH4_CU(Q_) \
+  case Q_: cu = cdot<Q_>(ux, uy, uz); break;
+      CH4_CU(0) CH4_CU(1) CH4_CU(2) CH4_CU(3) CH4_CU(4) CH4_CU(5) CH4_CU(6) CH4_CU(7) CH4_CU(8) CH4_CU(9)
+      CH4_CU(10) CH4_CU(11) CH4_CU(12) CH4_CU(13) CH4_CU(14) CH4_CU(15) CH4_CU(16) CH4_CU(17) CH4_CU(18)
+#undef CH4_CU
+      default: cu = A(0);
+    }
+    const A feq = rho * P.w[q] * (A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * u2);
+    A r = f[q];
+    r += -invtau * (f[q] - feq);
+    if (F & K_FORCING) {
+      A dx, dy, dz;
+      switch (q) {
+#define CH4_D(Q_)                                               \
+  case Q_:                                                      \
+    dx = guo_d<cx(Q_)>(ux, cu, P.invcs2, P.invcs4);             \
+    dy = guo_d<cy(Q_)>(uy, cu, P.invcs2, P.invcs4);             \
+    dz = guo_d<cz(Q_)>(uz, cu, P.invcs2, P.invcs4);             \
+    break;
+        CH4_D(0) CH4_D(1) CH4_D(2) CH4_D(3) CH4_D(4) CH4_D(5) CH4_D(6) CH4_D(7) CH4_D(8) CH4_D(9)
+        CH4_D(10) CH4_D(11) CH4_D(12) CH4_D(13) CH4_D(14) CH4_D(15) CH4_D(16) CH4_D(17) CH4_D(18)
+#undef CH4_D
+        default: dx = dy = dz = A(0);
+      }
+      r += P.facw[q] * rho * Fx * dx;
+      r += P.facw[q] * rho * Fy * dy;
+      r += P.facw[q] * rho * Fz * dz;
+    }
+    f[q] = r;
+  }
+  push_set<S, A, 0>(P, x, y, z, idx, f, (F & K_FWALL) ? 1 : 0, (F & K_FSLIP_P) != 0, (F & K_FSLIP_M) != 0, A(0), A(0));
+
+  // temperature / scalar: BGK with the fluid velocity (+ plain source), value walls
+  if constexpr (THERM) {
+    const A it = P.invtau[1];
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      A cu;
+      switch (q) {
+#define CH4_CU(Q_) \
+  case Q_: cu = cdot<Q_>(ux, uy, uz); break;
+        CH4_CU(0) CH4_CU(1) CH4_CU(2) CH4_CU(3) CH4_CU(4) CH4_CU(5) CH4_CU(6) CH4_CU(7) CH4_CU(8) CH4_CU(9)
+        CH4_CU(10) CH4_CU(11) CH4_CU(12) CH4_CU(13) CH4_CU(14) CH4_CU(15) CH4_CU(16) CH4_CU(17) CH4_CU(18)
+#undef CH4_CU
+        default: cu = A(0);
+      }
+      const A geq = tt * P.w[q] * (A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * u2);
+      A r = g[q];
+      r += -it * (g[q] - geq);
+      g[q] = r;
+    }
+    A fac_top = A(0), fac_bot = A(0);
+    if (F & K_TWALL) {  // src/boundary_conditions.c:966-1081
+      A T_wall = P.T_top;
+      if (F & K_TFLUX_P) T_wall = A(0.5) * P.grad_T_top + tt + P.T_ref;
+      fac_top = (F & K_TNOFLUX_P) ? A(0) : A(2) * ((T_wall - P.T_ref) - tt);
+      T_wall = P.T_bot;
+      if (F & K_TFLUX_M) T_wall = A(-0.5) * P.grad_T_bot + tt + P.T_ref;
+      fac_bot = (F & K_TNOFLUX_M) ? A(0) : A(2) * ((T_wall - P.T_ref) - tt);
+    }
+    push_set<S, A, 1>(P, x, y, z, idx, g, (F & K_TWALL) ? 2 : 0, false, false, fac_top, fac_bot);
+  }
+  if constexpr (SCAL) {
+    const A is = P.invtau[2];
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      A cu;
+      switch (q) {
+#define CH4_CU(Q_) \
+  case Q_: cu = cdot<Q_>(ux, uy, uz); break;
+        CH4_CU(0) CH4_CU(1) CH4_CU(2) CH4_CU(3) CH4_CU(4) CH4_CU(5) CH4_CU(6) CH4_CU(7) CH4_CU(8) CH4_CU(9)
+        CH4_CU(10) CH4_CU(11) CH4_CU(12) CH4_CU(13) CH4_CU(14) CH4_CU(15) CH4_CU(16) CH4_CU(17) CH4_CU(18)
+#undef CH4_CU
+        default: cu = A(0);
+      }
+      const A heq = ss * P.w[q] * (A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * u2);
+      A r = h[q];
+      r += -is * (h[q] - heq);
+      h[q] = r;
+    }
+    A fac_top = A(0), fac_bot = A(0);
+    if (F & K_SWALL) {  // src/boundary_conditions.c:1249-1380
+      fac_top = A(2) * ((P.S_top - P.S_ref) - ss);
+      fac_bot = A(2) * ((P.S_bot - P.S_ref) - ss);
+    }
+    push_set<S, A, 2>(P, x, y, z, idx, h, (F & K_SWALL) ? 2 : 0, false, false, fac_top, fac_bot);
+  }
+}
+
+// t^{n-1} := m(g^0), s^{n-1} := m(h^0) at initialisation (src/main.c:24-48)
+template <typename S, typename A, bool THERM, bool SCAL>
+__global__ void init_prev_kernel(const StepParams<A> P) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= P.N) return;
+  if constexpr (THERM) {
+    A g[Q];
+    load_set<S, A, 1>(P, idx, g);
+    P.tprev[idx] = mom0(g);
+  }
+  if constexpr (SCAL) {
+    A h[Q];
+    load_set<S, A, 2>(P, idx, h);
+    P.sprev[idx] = mom0(h);
+  }
+}
+
+// hydro_fields (src/lb.c:420-539): dens, u (with dt/2 of the force built from the
+// kept temperature and the given phase table), t, s -- all as FP64 SoA planes.
+// Also the force field itself when `force` is non-null.
+template <typename S, typename A, bool THERM, bool SCAL>
+__global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, double* dens, double* u, double* t,
+                             double* s, double* force, A* u_arith) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= P.N) return;
+  const int x = (int)(idx % P.NX);
+  const int y = (int)((idx / P.NX) % P.NY);
+  const int z = (int)(idx / ((long long)P.NX * P.NY));
+  A f[Q];
+  load_set<S, A, 0>(P, idx, f);
+  const A rho = mom0(f);
+  A Fx = A(0), Fy = A(0), Fz = A(0);
+  if (P.feat & K_FORCING) {
+    const A tp = THERM ? P.tprev[idx] : A(0);
+    const A sp = SCAL ? P.sprev[idx] : A(0);
+    cell_force(P, x, y, z, idx, tp, sp, hit, dep, Fx, Fy, Fz);
+  }
+  const A ux = momx(f) / rho + P.hdt * Fx;
+  const A uy = momy(f) / rho + P.hdt * Fy;
+  const A uz = momz(f) / rho + P.hdt * Fz;
+  if (dens) dens[idx] = (double)rho;
+  if (u) {
+    u[idx] = (double)ux;
+    u[P.N + idx] = (double)uy;
+    u[2 * P.N + idx] = (double)uz;
+  }
+  if (u_arith) {
+    u_arith[idx] = ux;
+    u_arith[P.N + idx] = uy;
+    u_arith[2 * P.N + idx] = uz;
+  }
+  if (force) {
+    force[idx] = (double)Fx;
+    force[P.N + idx] = (double)Fy;
+    force[2 * P.N + idx] = (double)Fz;
+  }
+  if constexpr (THERM) {
+    if (t) {
+      A g[Q];
+      load_set<S, A, 1>(P, idx, g);
+      t[idx] = (double)mom0(g);
+    }
+  }
+  if constexpr (SCAL) {
+    if (s) {
+      A h[Q];
+      load_set<S, A, 2>(P, idx, h);
+      s[idx] = (double)mom0(h);
+    }
+  }
+}
+
+// Compact AoS FP64 chunk (reference `pop` records of z-planes [z0, z0+nz), no
+// halo) <-> SoA storage.  The host moves the halo-padded caller arrays row by row.
+template <typename S, typename A>
+__global__ void aos_to_soa_kernel(const double* aos, S* soa, int NX, int NY, int z0, int nz, long long N, StepParams<A> P,
+                                  int set) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long cells = (long long)NX * NY * nz;
+  if (t >= cells * Q) return;
+  const int q = (int)(t % Q);
+  const long long c = t / Q;
+  Codec<S, A>::store(soa, (long long)q * N + (long long)z0 * NX * NY + c, (A)aos[t], P.w[q], P.shift[set]);
+}
+
+template <typename S, typename A>
+__global__ void soa_to_aos_kernel(const S* soa, double* aos, int NX, int NY, int z0, int nz, long long N,
+                                  StepParams<A> P, int set) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long cells = (long long)NX * NY * nz;
+  if (t >= cells * Q) return;
+  const int q = (int)(t % Q);
+  const long long c = t / Q;
+  aos[t] = (double)Codec<S, A>::load(soa, (long long)q * N + (long long)z0 * NX * NY + c, P.w[q], P.shift[set]);
+}
+
+}  // namespace ch4

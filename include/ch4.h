@@ -198,6 +198,11 @@ ch4_status ch4_step(ch4_handle *h, int nsteps);
 /* Wait for the handle's stream. */
 ch4_status ch4_synchronize(ch4_handle *h);
 
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or timing events after the step kernels.  No reference counterpart: the
+ * reference has no device and no asynchrony. */
+ch4_status ch4_get_stream(ch4_handle *h, void **stream);
+
 /* Hydrodynamic fields as after hydro_fields (src/lb.c:420-539): dens, u (3 per
  * cell), t, s.  Any pointer may be NULL. */
 ch4_status ch4_get_fields(ch4_handle *h, double *dens, double *u, double *t, double *s, int brd);

@@ -33,7 +33,18 @@ FLAGSETS = {
     "kolmogorov": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV"],
     "rb": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
            "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y"],
+    "hit": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT"],
+    "walls2": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_BC_Y",
+               "LB_FLUID_BC_Y_P_SLIP", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y",
+               "LB_TEMPERATURE_BC_Y_P_FLUX"],
+    "scalar": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_FLUID_BC_Y_M_SLIP", "LB_TEMPERATURE",
+               "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LB_SCALAR", "LB_SCALAR_BUOYANCY",
+               "LB_SCALAR_BC_Y"],
+    "les": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
+            "LB_FLUID_BC_Y", "LB_FLUID_LES"],
 }
+# non-flag configuration implied by a flag set (define.h variants of one setting)
+FLAGSET_EXTRA = {"walls2": {"t0_kind": abi.T0_REF}}
 
 
 def ref_binary(flagset):
@@ -92,7 +103,7 @@ def aos_from_soa(f_soa, NX, NY, NZ):
     return np.ascontiguousarray(f_soa.reshape(NPOP, NZ, NY, NX).transpose(1, 2, 3, 0))
 
 
-def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=1, workdir=None):
+def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None):
     """Run the compiled reference on injected populations.
 
     pops: dict which -> AoS array [NZ][NY][NX][NPOP] (interior cells).
@@ -107,6 +118,7 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=1, workdir=None):
         np.ascontiguousarray(arr, dtype=np.float64).tofile(os.path.join(tmp, "in_%s.bin" % which))
     if phi is not None:
         np.ascontiguousarray(phi, dtype=np.float64).tofile(os.path.join(tmp, "in_phi.bin"))
+    seed = int(cfg.seed) if seed is None else seed
     r = subprocess.run([exe, str(nsteps), str(seed)], cwd=tmp, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("reference run failed: %s" % r.stderr[-2000:])

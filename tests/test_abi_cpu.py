@@ -1,0 +1,93 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports every
+symbol include/ch4.h declares; the define.h / param.in readers follow the
+reference's semantics (src/parameters.c:3-39)."""
+import os
+import re
+
+import pytest
+
+import ch4b200
+from ch4b200 import abi
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    txt = open(os.path.join(REPO, "include", "ch4.h")).read()
+    return sorted(set(re.findall(r"^(?:ch4_status|const char \*)\s*(ch4_\w+)\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = ch4b200.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def test_config_default():
+    c = ch4b200.default_config()
+    assert c.C_smag == 0.18 and c.time_dt == 1.0 and c.flags == abi.FLAGS["LB_FLUID"]
+
+
+def test_read_param_semantics(tmp_path):
+    p = tmp_path / "param.in"
+    # first number after a key wins; extra numbers are consumed as junk pairs
+    p.write_text("NX 16\nNY 8\nNZ 4\nSX 16\nSY 8\nSZ 4\ntime_dt 1.0\n"
+                 "tau_u 0.6 0.51 0.52 0.53 0.54\nAmp_x 1.e-2\nAmp_y 0\nAmp_z 0\n")
+    c = ch4b200.default_config()
+    c.flags = abi.flags_of(["LB_FLUID", "LB_FLUID_FORCING"])
+    ch4b200.read_param(c, str(p))
+    assert (c.NX, c.NY, c.NZ) == (16, 8, 4)
+    assert c.tau_u == 0.6 and c.Amp_x == 1e-2
+    assert c.nu == (0.6 - 0.5 * 1.0) / 3.0
+    assert ch4b200.read_parameter(str(p), "tau_u") == 0.6
+
+
+def test_read_param_missing_key(tmp_path):
+    p = tmp_path / "param.in"
+    p.write_text("NX 16\nNY 8\n")
+    c = ch4b200.default_config()
+    with pytest.raises(ch4b200.CH4Error) as e:
+        ch4b200.read_param(c, str(p))
+    assert e.value.status == abi.ERR_PARAM and "NZ" in str(e.value)
+
+
+def test_read_define(tmp_path):
+    d = tmp_path / "define.h"
+    d.write_text("#define SYSTEM_RANDOM48\n//#define LB_SCALAR\n#define GRID_POP_D3Q19\n#define LB\n#define LB_FLUID\n"
+                 "#define LB_FLUID_FORCING /* force */\n#define LB_FLUID_FORCING_KOLMOGOROV\n#define METHOD_STREAMING\n"
+                 "/* #define LB_TEMPERATURE */\n#define LB_TEMPERATURE_BUOYANCY_T0_REF\n")
+    c = ch4b200.default_config()
+    ch4b200.read_define(c, str(d))
+    assert abi.set_flag_names(c.flags) == ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV"]
+    assert c.t0_kind == abi.T0_REF
+
+
+def test_read_define_rejects_out_of_scope_flag(tmp_path):
+    d = tmp_path / "define.h"
+    d.write_text("#define GRID_POP_D3Q19\n#define METHOD_STREAMING\n#define LB_TEMPERATURE_MELTING\n")
+    c = ch4b200.default_config()
+    with pytest.raises(ch4b200.CH4Error) as e:
+        ch4b200.read_define(c, str(d))
+    assert e.value.status == abi.ERR_UNSUPPORTED and "LB_TEMPERATURE_MELTING" in str(e.value)
+
+
+def test_read_define_requires_d3q19_streaming(tmp_path):
+    d = tmp_path / "define.h"
+    d.write_text("#define GRID_POP_D2Q9\n#define METHOD_STREAMING\n")
+    with pytest.raises(ch4b200.CH4Error):
+        ch4b200.read_define(ch4b200.default_config(), str(d))
+
+
+def test_device_bytes_admission():
+    c = ch4b200.default_config()
+    c.NX, c.NY, c.NZ = 256, 256, 128
+    c.SX, c.SY, c.SZ = 256.0, 256.0, 128.0
+    c.flags = abi.flags_of(["LB_FLUID", "LB_TEMPERATURE"])
+    c.storage = abi.STORE_F32
+    n = ch4b200.device_bytes(c)
+    cells = 256 * 256 * 128
+    assert n >= 2 * 2 * 19 * cells * 4
+    c.storage = abi.STORE_F16
+    assert ch4b200.device_bytes(c) < n

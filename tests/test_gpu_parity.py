@@ -1,0 +1,103 @@
+"""GPU parity: the CUDA step (through the C ABI, libch4b200.so) against the oracle.
+
+FP64 storage/arithmetic must be bit-identical to the oracle restatement and to the
+compiled reference (both FP64, contraction off).  The FP32 and FP16-deviation forms
+are checked against the FP64 oracle with the tolerances written below.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from lbcases import make_case, run_restatement
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import ch4b200  # noqa: E402
+
+
+def run_gpu(cfg, state, nsteps, phi=None):
+    with ch4b200.Simulation(cfg) as sim:
+        for k, v in state.items():
+            sim.set_pop(k, v)
+        if phi is not None:
+            sim.set_hit_phases(phi)
+        sim.initialize()
+        sim.step(nsteps)
+        out = {k: sim.get_pop(k) for k in state}
+        out.update(sim.fields())
+        out["force"] = sim.force()
+        out["itime"] = sim.itime
+        out["phi"] = sim.get_hit_phases()
+    return out
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+@pytest.mark.parametrize("name,nsteps", [("kolmogorov", 25), ("rb", 25), ("hit", 20), ("walls2", 25),
+                                          ("scalar", 25), ("les", 25)])
+def test_fp64_bit_identical_to_oracle(name, nsteps):
+    _, cfg, state = make_case(name, seed=11)
+    ref = run_restatement(cfg, state, nsteps)
+    gpu = run_gpu(cfg, state, nsteps)
+    assert gpu["itime"] == nsteps
+    for k in state:
+        assert np.array_equal(gpu[k], ref[k]), "%s: max |d| %g" % (k, np.abs(gpu[k] - ref[k]).max())
+    for k in ("u", "dens", "force"):
+        assert np.array_equal(gpu[k], ref[k]), k
+    if "g" in state:
+        assert np.array_equal(gpu["t"], ref["t"])
+    if "h" in state:
+        assert np.array_equal(gpu["s"], ref["s"])
+    if "phi" in ref:
+        assert np.array_equal(gpu["phi"], ref["phi"])
+
+
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "hit", "walls2", "scalar", "les"])
+def test_fp64_matches_compiled_reference(name):
+    flagset, cfg, state = make_case(name, seed=5)
+    if not O.ref_available(flagset):
+        pytest.skip("reference build missing")
+    ref = O.run_reference(flagset, cfg, 30, state)
+    gpu = run_gpu(cfg, state, 30)
+    for k in state:
+        assert np.array_equal(gpu[k], ref[k]), k
+    assert np.array_equal(gpu["u"], ref["u"])
+
+
+# reduced precision: FP32 arithmetic with FP32 / FP16-deviation storage
+# FP32: relative L2 of u within 1e-4, of T within 1e-6 (40 steps, u ~ 1e-3).
+# FP16 deviations (11-bit mantissa): u within 0.2, T within 2e-2.
+@pytest.mark.parametrize("storage,tol_u,tol_t", [(1, 1e-4, 1e-6), (2, 0.2, 2e-2)])
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "scalar"])
+def test_reduced_precision_error_bounds(name, storage, tol_u, tol_t):
+    _, cfg64, state = make_case(name, seed=2)
+    _, cfg, _ = make_case(name, seed=2, storage=storage)
+    ref = run_restatement(cfg64, state, 40)
+    gpu = run_gpu(cfg, state, 40)
+    eu = rel_l2(gpu["u"], ref["u"])
+    assert eu < tol_u, "u rel L2 %g" % eu
+    assert rel_l2(gpu["dens"], ref["dens"]) < 1e-5
+    if "g" in state:
+        et = rel_l2(gpu["t"], ref["t"])
+        assert et < tol_t, "t rel L2 %g" % et
+
+
+def test_larger_lattice_bit_identical():
+    # 32x24x16 thermal convection, 120 steps: FP64 GPU == oracle
+    _, cfg, state = make_case("rb", seed=9)
+    import lbcases
+    rng = np.random.default_rng(9)
+    cfg.NX, cfg.NY, cfg.NZ = 32, 24, 16
+    cfg.SX, cfg.SY, cfg.SZ = 32.0, 24.0, 16.0
+    state = {"p": lbcases.pops(rng, 32, 24, 16, 1.0, 1e-2),
+             "g": lbcases.rb_temperature_pops(rng, 32, 24, 16, 1.0, 0.0, 1e-2)}
+    ref = run_restatement(cfg, state, 120)
+    gpu = run_gpu(cfg, state, 120)
+    assert np.array_equal(gpu["p"], ref["p"])
+    assert np.array_equal(gpu["g"], ref["g"])

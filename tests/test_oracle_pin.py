@@ -1,0 +1,73 @@
+"""Pin the oracle: the C restatement (oracle/ch4_oracle.c) against the reference
+solver itself, compiled from its own sources (oracle/Makefile -> oracle/_ref), on
+the same seeded inputs.  The reference has no golden vectors of its own (its src/tests
+directory is empty), so the compiled reference is the pin; the committed fixtures in
+tests/golden/ (made by tests/golden/make_golden.py from the same binaries) keep the pin
+available where the reference build is absent."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from lbcases import CASES, make_case, run_restatement
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _assert_same(a, b, what):
+    assert a.shape == b.shape, what
+    # bit-identical (IEEE equality; +0 and -0 compare equal)
+    assert np.array_equal(a, b), "%s differs: max |d| = %g" % (what, np.abs(a - b).max())
+
+
+@pytest.mark.parametrize("name,nsteps", [("kolmogorov", 20), ("rb", 20), ("hit", 15), ("walls2", 20),
+                                          ("scalar", 20), ("les", 20)])
+def test_restatement_matches_compiled_reference(name, nsteps):
+    flagset, cfg, state = make_case(name, seed=3)
+    if not O.ref_available(flagset):
+        pytest.skip("reference build oracle/_ref/%s missing" % flagset)
+    ref = O.run_reference(flagset, cfg, nsteps, state)
+    mine = run_restatement(cfg, state, nsteps)
+    if "phi" in ref:
+        _assert_same(mine["phi"], ref["phi"], "HIT phases")
+    for k in state:
+        _assert_same(mine[k], ref[k], "%s populations" % k)
+    _assert_same(mine["u"], ref["u"], "u")
+    _assert_same(mine["dens"], ref["dens"], "dens")
+    if "t" in ref:
+        _assert_same(mine["t"], ref["t"], "t")
+    if "s" in ref:
+        _assert_same(mine["s"], ref["s"], "s")
+    _assert_same(mine["force"], ref["force"], "force")
+
+
+@pytest.mark.parametrize("flagset", sorted(O.FLAGSETS))
+def test_flagset_headers_match_product_flags(flagset):
+    """oracle/configs/<flagset>.h, read by the product's define.h reader, gives the
+    flag bits the tests use for that flag set."""
+    import ch4b200
+    from ch4b200 import abi
+    cfg = ch4b200.default_config()
+    ch4b200.read_define(cfg, os.path.join(os.path.dirname(O.__file__), "configs", flagset + ".h"))
+    assert cfg.flags == abi.flags_of(O.FLAGSETS[flagset])
+    assert cfg.t0_kind == O.FLAGSET_EXTRA.get(flagset, {}).get("t0_kind", abi.T0_MEAN)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_restatement_matches_golden_fixture(name):
+    path = os.path.join(GOLDEN, "%s.npz" % name)
+    if not os.path.exists(path):
+        pytest.skip("fixture %s not generated" % path)
+    g = np.load(path)
+    flagset, cfg, state = make_case(name, seed=int(g["seed"]))
+    import hashlib
+    for k in state:
+        h = hashlib.sha256(np.ascontiguousarray(state[k]).tobytes()).hexdigest()
+        assert h == str(g["in_sha256_" + k]), "case generator changed for %s" % k
+    mine = run_restatement(cfg, state, int(g["nsteps"]))
+    for k in state:
+        _assert_same(mine[k], g["out_" + k], k)
+    for k in ("u", "t", "s", "phi"):
+        if "out_" + k in g.files:
+            _assert_same(mine[k], g["out_" + k], k)
