@@ -745,7 +745,8 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
 
 static ch4_status validate(const ch4_config* c, std::string& why) {
   if (c->NX < 1 || c->NY < 1 || c->NZ < 1) return why = "lattice size must be positive", CH4_ERR_ARG;
-  if ((long long)c->NX * c->NY * c->NZ > (1ll << 34)) return why = "lattice too large", CH4_ERR_ARG;
+  if ((long long)c->NX * c->NY * c->NZ >= (1ll << 31)) return why = "lattice too large (cells >= 2^31)", CH4_ERR_ARG;
+  if (c->NY > 65535 || c->NZ > 65535) return why = "NY and NZ must be <= 65535 (launch grid)", CH4_ERR_ARG;
   if (c->flags & ~SUPPORTED) return why = "flag outside the implemented hot path", CH4_ERR_UNSUPPORTED;
   if (c->storage < 0 || c->storage > 2) return why = "unknown storage", CH4_ERR_ARG;
   if (c->time_dt != 1.0 || c->SX != c->NX || c->SY != c->NY || c->SZ != c->NZ)

@@ -165,194 +165,7 @@ __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z
   return A(3) * (nu_les + P.nu) + A(0.5);
 }
 
-// ---- the fused step -------------------------------------------------------
-
-template <typename S, typename A, int set>
-__device__ __forceinline__ void load_set(const StepParams<A>& P, long long idx, A* f) {
-  const S* in = static_cast<const S*>(P.fin[set]);
-#pragma unroll
-  for (int q = 0; q < Q; q++) f[q] = Codec<S, A>::load(in, (long long)q * P.N + idx, P.w[q], P.shift[set]);
-}
-
-// push one set; `wallmode`: 0 periodic in y, 1 fluid walls, 2 value walls (T or S)
-template <typename S, typename A, int set>
-__device__ __forceinline__ void push_set(const StepParams<A>& P, int x, int y, int z, long long idx, const A* post,
-                                         int wallmode, bool slip_top, bool slip_bot, A fac_top, A fac_bot) {
-  S* out = static_cast<S*>(P.fout[set]);
-  const int NX = P.NX, NY = P.NY, NZ = P.NZ;
-  const long long N = P.N;
-  const float sh = P.shift[set];
-#pragma unroll
-  for (int q = 0; q < Q; q++) {
-    const int ty = y + cy(q);
-    const int tx = wrap(x + cx(q), NX);
-    const int tz = wrap(z + cz(q), NZ);
-    if (cy(q) != 0 && wallmode != 0 && (ty < 0 || ty >= NY)) {
-      if (wallmode == 1) {
-        const bool slip = ty >= NY ? slip_top : slip_bot;
-        if (slip) {  // specular reflection, src/boundary_conditions.c:753,786
-          const long long d = ((long long)tz * NY + y) * NX + tx;
-          Codec<S, A>::store(out, (long long)qinv_y(q) * N + d, post[q], P.w[qinv_y(q)], sh);
-        } else {  // halfway bounce-back, src/boundary_conditions.c:775,798
-          Codec<S, A>::store(out, (long long)qinv(q) * N + idx, post[q], P.w[qinv(q)], sh);
-        }
-      } else {  // fixed value / flux wall: rhs(x).p[inv q] + w[inv q]*fac (src/boundary_conditions.c:1019-1027)
-        const int r = qinv(q);
-        const A fac = ty >= NY ? fac_top : fac_bot;
-        Codec<S, A>::store(out, (long long)r * N + idx, post[r] + P.w[r] * fac, P.w[r], sh);
-      }
-    } else {
-      const long long d = ((long long)tz * NY + wrap(ty, NY)) * NX + tx;
-      Codec<S, A>::store(out, (long long)q * N + d, post[q], P.w[q], sh);
-    }
-  }
-}
-
-template <typename S, typename A, bool THERM, bool SCAL>
-__global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  const int z = blockIdx.z;
-  if (x >= P.NX) return;
-  const long long idx = ((long long)z * P.NY + y) * P.NX + x;
-  const uint32_t F = P.feat;
-
-  A f[Q];
-  load_set<S, A, 0>(P, idx, f);
-  const A rho = mom0(f);
-  const A mx = momx(f), my = momy(f), mz = momz(f);
-
-  A g[Q], h[Q];
-  A tt = A(0), ss = A(0);
-  if constexpr (THERM) {
-    load_set<S, A, 1>(P, idx, g);
-    tt = mom0(g);
-  }
-  if constexpr (SCAL) {
-    load_set<S, A, 2>(P, idx, h);
-    ss = mom0(h);
-  }
-
-  // u^n = mv/rho + dt/2 F^{n-1} (src/lb.c:464-466); F^n for Guo (src/forcing.c:1423-1435)
-  A ux, uy, uz, Fx = A(0), Fy = A(0), Fz = A(0);
-  if (F & K_FORCING) {
-    A px, py, pz;
-    const A tp = THERM ? P.tprev[idx] : A(0);
-    const A sp = SCAL ? P.sprev[idx] : A(0);
-    cell_force(P, x, y, z, idx, tp, sp, P.hit_prev, (F & K_TWOWAY) ? P.dprev : nullptr, px, py, pz);
-    ux = mx / rho + P.hdt * px;
-    uy = my / rho + P.hdt * py;
-    uz = mz / rho + P.hdt * pz;
-    cell_force(P, x, y, z, idx, tt, ss, P.hit_cur, (F & K_TWOWAY) ? P.dcur : nullptr, Fx, Fy, Fz);
-  } else {
-    ux = mx / rho;
-    uy = my / rho;
-    uz = mz / rho;
-  }
-  if constexpr (THERM) P.tprev[idx] = tt;
-  if constexpr (SCAL) P.sprev[idx] = ss;
-
-  const A u2 = ux * ux + uy * uy + uz * uz;
-  A invtau = P.invtau[0];
-  if (F & K_LES) {
-    const A tl = les_tau(P, x, y, z);
-    P.tau_les[idx] = tl;
-    invtau = A(1) / tl;
-  }
-
-  // fluid: BGK + Guo, in place
-#pragma unroll
-  for (int q = 0; q < Q; q++) {
-    A cu;
-    switch (q) {  // resolved at compile time after unrolling
-#define CH4_CU(Q_) \
-  case Q_: cu = cdot<Q_>(ux, uy, uz); break;
-      CH4_CU(0) CH4_CU(1) CH4_CU(2) CH4_CU(3) CH4_CU(4) CH4_CU(5) CH4_CU(6) CH4_CU(7) CH4_CU(8) CH4_CU(9)
-      CH4_CU(10) CH4_CU(11) CH4_CU(12) CH4_CU(13) CH4_CU(14) CH4_CU(15) CH4_CU(16) CH4_CU(17) CH4_CU(18)
-#undef CH4_CU
-      default: cu = A(0);
-    }
-    const A feq = rho * P.w[q] * (A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * u2);
-    A r = f[q];
-    r += -invtau * (f[q] - feq);
-    if (F & K_FORCING) {
-      A dx, dy, dz;
-      switch (q) {
-#define CH4_D(Q_)                                               \
-  case Q_:                                                      \
-    dx = guo_d<cx(Q_)>(ux, cu, P.invcs2, P.invcs4);             \
-    dy = guo_d<cy(Q_)>(uy, cu, P.invcs2, P.invcs4);             \
-    dz = guo_d<cz(Q_)>(uz, cu, P.invcs2, P.invcs4);             \
-    break;
-        CH4_D(0) CH4_D(1) CH4_D(2) CH4_D(3) CH4_D(4) CH4_D(5) CH4_D(6) CH4_D(7) CH4_D(8) CH4_D(9)
-        CH4_D(10) CH4_D(11) CH4_D(12) CH4_D(13) CH4_D(14) CH4_D(15) CH4_D(16) CH4_D(17) CH4_D(18)
-#undef CH4_D
-        default: dx = dy = dz = A(0);
-      }
-      r += P.facw[q] * rho * Fx * dx;
-      r += P.facw[q] * rho * Fy * dy;
-      r += P.facw[q] * rho * Fz * dz;
-    }
-    f[q] = r;
-  }
-  push_set<S, A, 0>(P, x, y, z, idx, f, (F & K_FWALL) ? 1 : 0, (F & K_FSLIP_P) != 0, (F & K_FSLIP_M) != 0, A(0), A(0));
-
-  // temperature / scalar: BGK with the fluid velocity (+ plain source), value walls
-  if constexpr (THERM) {
-    const A it = P.invtau[1];
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-      A cu;
-      switch (q) {
-#define CH4_CU(Q_) \
-  case Q_: cu = cdot<Q_>(ux, uy, uz); break;
-        CH4_CU(0) CH4_CU(1) CH4_CU(2) CH4_CU(3) CH4_CU(4) CH4_CU(5) CH4_CU(6) CH4_CU(7) CH4_CU(8) CH4_CU(9)
-        CH4_CU(10) CH4_CU(11) CH4_CU(12) CH4_CU(13) CH4_CU(14) CH4_CU(15) CH4_CU(16) CH4_CU(17) CH4_CU(18)
-#undef CH4_CU
-        default: cu = A(0);
-      }
-      const A geq = tt * P.w[q] * (A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * u2);
-      A r = g[q];
-      r += -it * (g[q] - geq);
-      g[q] = r;
-    }
-    A fac_top = A(0), fac_bot = A(0);
-    if (F & K_TWALL) {  // src/boundary_conditions.c:966-1081
-      A T_wall = P.T_top;
-      if (F & K_TFLUX_P) T_wall = A(0.5) * P.grad_T_top + tt + P.T_ref;
-      fac_top = (F & K_TNOFLUX_P) ? A(0) : A(2) * ((T_wall - P.T_ref) - tt);
-      T_wall = P.T_bot;
-      if (F & K_TFLUX_M) T_wall = A(-0.5) * P.grad_T_bot + tt + P.T_ref;
-      fac_bot = (F & K_TNOFLUX_M) ? A(0) : A(2) * ((T_wall - P.T_ref) - tt);
-    }
-    push_set<S, A, 1>(P, x, y, z, idx, g, (F & K_TWALL) ? 2 : 0, false, false, fac_top, fac_bot);
-  }
-  if constexpr (SCAL) {
-    const A is = P.invtau[2];
-#pragma unroll
-    for (int q = 0; q < Q; q++) {
-      A cu;
-      switch (q) {
-#define CH4_CU(Q_) \
-  case Q_: cu = cdot<Q_>(ux, uy, uz); break;
-        CH4_CU(0) CH4_CU(1) CH4_CU(2) CH4_CU(3) CH4_CU(4) CH4_CU(5) CH4_CU(6) CH4_CU(7) CH4_CU(8) CH4_CU(9)
-        CH4_CU(10) CH4_CU(11) CH4_CU(12) CH4_CU(13) CH4_CU(14) CH4_CU(15) CH4_CU(16) CH4_CU(17) CH4_CU(18)
-#undef CH4_CU
-        default: cu = A(0);
-      }
-      const A heq = ss * P.w[q] * (A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * u2);
-      A r = h[q];
-      r += -is * (h[q] - heq);
-      h[q] = r;
-    }
-    A fac_top = A(0), fac_bot = A(0);
-    if (F & K_SWALL) {  // src/boundary_conditions.c:1249-1380
-      fac_top = A(2) * ((P.S_top - P.S_ref) - ss);
-      fac_bot = A(2) * ((P.S_bot - P.S_ref) - ss);
-    }
-    push_set<S, A, 2>(P, x, y, z, idx, h, (F & K_SWALL) ? 2 : 0, false, false, fac_top, fac_bot);
-  }
-}
+#include "lb_step.cuh"
 
 // t^{n-1} := m(g^0), s^{n-1} := m(h^0) at initialisation (src/main.c:24-48)
 template <typename S, typename A, bool THERM, bool SCAL>

@@ -1,0 +1,234 @@
+// The fused step kernel (included by lb_kernels.cuh inside namespace ch4).
+//
+// One launch = one iteration of the reference loop for the populations: BGK
+// collision (src/fluid.c:1033-1226) with the equilibrium of src/lb.c:382-415,
+// the build_forcing terms (src/forcing.c:360-707), Guo forcing
+// (src/forcing.c:1423-1435), the wall rules of src/boundary_conditions.c:419-1524
+// and streaming (src/lb.c:544-584), for p, g and h.  Each population is read once
+// and written once.
+//
+// EXACT (the FP64 instantiation) keeps every operation of the reference in its
+// order, so the result is bit-identical.  The FP32 instantiation evaluates the
+// same quantities with fewer instructions (reciprocal density, the equilibrium
+// polynomial in Horner form, the Guo term as (c.F - u.F)/cs^2 + (c.u)(c.F)/cs^4);
+// its error against FP64 is reported, not zero.
+
+template <typename S, typename A, int set>
+__device__ __forceinline__ void load_set(const StepParams<A>& P, long long idx, A* f) {
+  const S* in = static_cast<const S*>(P.fin[set]);
+#pragma unroll
+  for (int q = 0; q < Q; q++) f[q] = Codec<S, A>::load(in, (long long)q * P.N + idx, P.w[q], P.shift[set]);
+}
+
+// Linear-index deltas to the neighbour at c = -1 / +1 along each axis, with the
+// periodic wrap folded in (computed once per cell instead of once per direction).
+struct Nbr {
+  int xm, xp, ym, yp, zm, zp;
+};
+
+__device__ __forceinline__ Nbr neighbours(int x, int y, int z, int NX, int NY, int NZ) {
+  const int sxy = NX * NY;
+  Nbr n;
+  n.xm = x == 0 ? NX - 1 : -1;
+  n.xp = x == NX - 1 ? -(NX - 1) : 1;
+  n.ym = y == 0 ? (NY - 1) * NX : -NX;
+  n.yp = y == NY - 1 ? -(NY - 1) * NX : NX;
+  n.zm = z == 0 ? (NZ - 1) * sxy : -sxy;
+  n.zp = z == NZ - 1 ? -(NZ - 1) * sxy : sxy;
+  return n;
+}
+
+template <int q, bool WITH_Y>
+__device__ __forceinline__ int nbr_delta(const Nbr& n) {
+  int d = 0;
+  if constexpr (cx(q) < 0) d += n.xm;
+  if constexpr (cx(q) > 0) d += n.xp;
+  if constexpr (WITH_Y && cy(q) < 0) d += n.ym;
+  if constexpr (WITH_Y && cy(q) > 0) d += n.yp;
+  if constexpr (cz(q) < 0) d += n.zm;
+  if constexpr (cz(q) > 0) d += n.zp;
+  return d;
+}
+
+// push one set; wallmode: 0 periodic in y, 1 fluid walls, 2 value walls (T or S).
+// top/bot: this cell is the last/first interior row of a walled set (uniform per block).
+template <typename S, typename A, int set, int q>
+__device__ __forceinline__ void push_one(const StepParams<A>& P, S* out, int idx, const Nbr& nb, const A* post,
+                                         int wallmode, bool top, bool bot, bool slip_top, bool slip_bot, A fac_top,
+                                         A fac_bot) {
+  const long long N = P.N;
+  const float sh = P.shift[set];
+  const bool hits_wall = (cy(q) > 0 && top) || (cy(q) < 0 && bot);
+  if (cy(q) != 0 && wallmode != 0 && hits_wall) {
+    if (wallmode == 1) {
+      const bool slip = cy(q) > 0 ? slip_top : slip_bot;
+      if (slip) {  // specular reflection, src/boundary_conditions.c:753,786
+        constexpr int r = qinv_y(q);
+        Codec<S, A>::store(out, (long long)r * N + (idx + nbr_delta<q, false>(nb)), post[q], P.w[r], sh);
+      } else {  // halfway bounce-back, src/boundary_conditions.c:775,798
+        constexpr int r = qinv(q);
+        Codec<S, A>::store(out, (long long)r * N + idx, post[q], P.w[r], sh);
+      }
+    } else {  // fixed value / flux wall: rhs(x).p[inv q] + w[inv q]*fac, src/boundary_conditions.c:1019-1027
+      constexpr int r = qinv(q);
+      const A fac = cy(q) > 0 ? fac_top : fac_bot;
+      Codec<S, A>::store(out, (long long)r * N + idx, post[r] + P.w[r] * fac, P.w[r], sh);
+    }
+  } else {
+    Codec<S, A>::store(out, (long long)q * N + (idx + nbr_delta<q, true>(nb)), post[q], P.w[q], sh);
+  }
+}
+
+template <typename S, typename A, int set>
+__device__ __forceinline__ void push_set(const StepParams<A>& P, int idx, const Nbr& nb, const A* post, int wallmode,
+                                         bool top, bool bot, bool slip_top, bool slip_bot, A fac_top, A fac_bot) {
+  S* out = static_cast<S*>(P.fout[set]);
+#define CH4_PUSH(Q_) push_one<S, A, set, Q_>(P, out, idx, nb, post, wallmode, top, bot, slip_top, slip_bot, fac_top, fac_bot);
+  CH4_PUSH(0) CH4_PUSH(1) CH4_PUSH(2) CH4_PUSH(3) CH4_PUSH(4) CH4_PUSH(5) CH4_PUSH(6) CH4_PUSH(7) CH4_PUSH(8)
+  CH4_PUSH(9) CH4_PUSH(10) CH4_PUSH(11) CH4_PUSH(12) CH4_PUSH(13) CH4_PUSH(14) CH4_PUSH(15) CH4_PUSH(16)
+  CH4_PUSH(17) CH4_PUSH(18)
+#undef CH4_PUSH
+}
+
+// Per-cell quantities shared by the collision of every direction.
+template <typename A>
+struct CellState {
+  A rho, ux, uy, uz, u2, tt, ss;
+  A Fx, Fy, Fz;
+  A invtau, it, is;
+  A base, uF;  // FP32 form: 1 - u2/(2 cs^2), u.F
+};
+
+// Collision of direction q for all enabled sets, in place.
+template <int q, bool EXACT, bool THERM, bool SCAL, typename A>
+__device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellState<A>& c, bool forcing, A* f, A* g,
+                                            A* h) {
+  const A cu = cdot<q>(c.ux, c.uy, c.uz);
+  if constexpr (EXACT) {
+    // equilibrium polynomial of src/lb.c:408, identical for p, g and h
+    const A poly = A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * c.u2;
+    const A feq = c.rho * P.w[q] * poly;
+    A r = f[q];
+    r += -c.invtau * (f[q] - feq);
+    if (forcing) {
+      const A dx = guo_d<cx(q)>(c.ux, cu, P.invcs2, P.invcs4);
+      const A dy = guo_d<cy(q)>(c.uy, cu, P.invcs2, P.invcs4);
+      const A dz = guo_d<cz(q)>(c.uz, cu, P.invcs2, P.invcs4);
+      r += P.facw[q] * c.rho * c.Fx * dx;
+      r += P.facw[q] * c.rho * c.Fy * dy;
+      r += P.facw[q] * c.rho * c.Fz * dz;
+    }
+    f[q] = r;
+    if constexpr (THERM) {
+      const A geq = c.tt * P.w[q] * poly;
+      A s = g[q];
+      s += -c.it * (g[q] - geq);
+      g[q] = s;
+    }
+    if constexpr (SCAL) {
+      const A heq = c.ss * P.w[q] * poly;
+      A s = h[q];
+      s += -c.is * (h[q] - heq);
+      h[q] = s;
+    }
+  } else {
+    const A poly = c.base + cu * (P.invcs2 + P.invtwocs4 * cu);
+    const A feq = (c.rho * P.w[q]) * poly;
+    A r = f[q] + c.invtau * (feq - f[q]);
+    if (forcing) {
+      const A cF = cdot<q>(c.Fx, c.Fy, c.Fz);
+      const A gt = (cF - c.uF) * P.invcs2 + (cu * cF) * P.invcs4;
+      r += (P.facw[q] * c.rho) * gt;
+    }
+    f[q] = r;
+    if constexpr (THERM) g[q] += c.it * ((c.tt * P.w[q]) * poly - g[q]);
+    if constexpr (SCAL) h[q] += c.is * ((c.ss * P.w[q]) * poly - h[q]);
+  }
+}
+
+template <typename S, typename A, bool THERM, bool SCAL>
+__global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
+  constexpr bool EXACT = sizeof(A) == 8;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int z = blockIdx.z;
+  if (x >= P.NX) return;
+  const int idx = (z * P.NY + y) * P.NX + x;
+  const uint32_t F = P.feat;
+  const bool forcing = (F & K_FORCING) != 0;
+
+  A f[Q], g[Q], h[Q];
+  load_set<S, A, 0>(P, idx, f);
+  if constexpr (THERM) load_set<S, A, 1>(P, idx, g);
+  if constexpr (SCAL) load_set<S, A, 2>(P, idx, h);
+
+  CellState<A> c;
+  c.rho = mom0(f);
+  const A mx = momx(f), my = momy(f), mz = momz(f);
+  c.tt = THERM ? mom0(g) : A(0);
+  c.ss = SCAL ? mom0(h) : A(0);
+
+  // u^n = mv/rho + dt/2 F^{n-1} (src/lb.c:464-466); F^n for Guo (src/forcing.c:1423-1435)
+  A px = A(0), py = A(0), pz = A(0);
+  c.Fx = c.Fy = c.Fz = A(0);
+  if (forcing) {
+    const A tp = THERM ? P.tprev[idx] : A(0);
+    const A sp = SCAL ? P.sprev[idx] : A(0);
+    cell_force(P, x, y, z, idx, tp, sp, P.hit_prev, (F & K_TWOWAY) ? P.dprev : nullptr, px, py, pz);
+    cell_force(P, x, y, z, idx, c.tt, c.ss, P.hit_cur, (F & K_TWOWAY) ? P.dcur : nullptr, c.Fx, c.Fy, c.Fz);
+  }
+  if constexpr (EXACT) {
+    c.ux = mx / c.rho + P.hdt * px;
+    c.uy = my / c.rho + P.hdt * py;
+    c.uz = mz / c.rho + P.hdt * pz;
+  } else {
+    const A ir = A(1) / c.rho;
+    c.ux = mx * ir + P.hdt * px;
+    c.uy = my * ir + P.hdt * py;
+    c.uz = mz * ir + P.hdt * pz;
+  }
+  if constexpr (THERM) P.tprev[idx] = c.tt;
+  if constexpr (SCAL) P.sprev[idx] = c.ss;
+
+  c.u2 = c.ux * c.ux + c.uy * c.uy + c.uz * c.uz;
+  c.invtau = P.invtau[0];
+  if (F & K_LES) {
+    const A tl = les_tau(P, x, y, z);
+    P.tau_les[idx] = tl;
+    c.invtau = A(1) / tl;
+  }
+  c.it = P.invtau[1];
+  c.is = P.invtau[2];
+  c.base = A(1) - P.invtwocs2 * c.u2;
+  c.uF = c.ux * c.Fx + c.uy * c.Fy + c.uz * c.Fz;
+
+#define CH4_COL(Q_) collide_one<Q_, EXACT, THERM, SCAL>(P, c, forcing, f, g, h);
+  CH4_COL(0) CH4_COL(1) CH4_COL(2) CH4_COL(3) CH4_COL(4) CH4_COL(5) CH4_COL(6) CH4_COL(7) CH4_COL(8) CH4_COL(9)
+  CH4_COL(10) CH4_COL(11) CH4_COL(12) CH4_COL(13) CH4_COL(14) CH4_COL(15) CH4_COL(16) CH4_COL(17) CH4_COL(18)
+#undef CH4_COL
+
+  const Nbr nb = neighbours(x, y, z, P.NX, P.NY, P.NZ);
+  const bool toprow = y == P.NY - 1, botrow = y == 0;
+  push_set<S, A, 0>(P, idx, nb, f, (F & K_FWALL) ? 1 : 0, toprow, botrow, (F & K_FSLIP_P) != 0,
+                    (F & K_FSLIP_M) != 0, A(0), A(0));
+  if constexpr (THERM) {
+    A fac_top = A(0), fac_bot = A(0);
+    if (F & K_TWALL) {  // src/boundary_conditions.c:966-1081
+      A T_wall = P.T_top;
+      if (F & K_TFLUX_P) T_wall = A(0.5) * P.grad_T_top + c.tt + P.T_ref;
+      fac_top = (F & K_TNOFLUX_P) ? A(0) : A(2) * ((T_wall - P.T_ref) - c.tt);
+      T_wall = P.T_bot;
+      if (F & K_TFLUX_M) T_wall = A(-0.5) * P.grad_T_bot + c.tt + P.T_ref;
+      fac_bot = (F & K_TNOFLUX_M) ? A(0) : A(2) * ((T_wall - P.T_ref) - c.tt);
+    }
+    push_set<S, A, 1>(P, idx, nb, g, (F & K_TWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
+  }
+  if constexpr (SCAL) {
+    A fac_top = A(0), fac_bot = A(0);
+    if (F & K_SWALL) {  // src/boundary_conditions.c:1249-1380
+      fac_top = A(2) * ((P.S_top - P.S_ref) - c.ss);
+      fac_bot = A(2) * ((P.S_bot - P.S_ref) - c.ss);
+    }
+    push_set<S, A, 2>(P, idx, nb, h, (F & K_SWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
+  }
+}
