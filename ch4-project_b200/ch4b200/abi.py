@@ -71,6 +71,7 @@ class Config(C.Structure):
         ("time_dt_lagr_factor", C.c_double),
         ("particle_number", C.c_int),
         ("seed", C.c_uint64),
+        ("resume", C.c_int),
     ]
 
 

@@ -593,13 +593,13 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
     double* dst;
     bool needed;
   };
-  double NX, NY, NZ, particle_number = 0;
+  double NX, NY, NZ, particle_number = 0, resume = 0;
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
   const bool grav = forcing && (fl & (CH4_F_TEMPERATURE_BUOYANCY | CH4_F_SCALAR_BUOYANCY));
   std::vector<K> keys = {
-      {"NX", &NX, true}, {"NY", &NY, true}, {"NZ", &NZ, true}, {"SX", &cfg->SX, true}, {"SY", &cfg->SY, true},
+      {"resume", &resume, true}, {"NX", &NX, true}, {"NY", &NY, true}, {"NZ", &NZ, true}, {"SX", &cfg->SX, true}, {"SY", &cfg->SY, true},
       {"SZ", &cfg->SZ, true}, {"time_dt", &cfg->time_dt, true}, {"tau_u", &cfg->tau_u, true},
       {"Amp_x", &cfg->Amp_x, forcing}, {"Amp_y", &cfg->Amp_y, forcing}, {"Amp_z", &cfg->Amp_z, forcing},
       {"gravity_x", &cfg->gravity_x, grav}, {"gravity_y", &cfg->gravity_y, grav}, {"gravity_z", &cfg->gravity_z, grav},
@@ -626,6 +626,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   cfg->NY = (int)NY;
   cfg->NZ = (int)NZ;
   cfg->particle_number = (int)particle_number;
+  cfg->resume = (int)resume;
   // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
   cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
   cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;

@@ -109,6 +109,10 @@ typedef struct {
   int particle_number;
   /* drand48 seed of the host RNG (HIT phases), src/parallel.c:237-240 */
   uint64_t seed;
+  /* param.in `resume`: the run continues earlier state, so the first step is
+   * not treated as the start (src/lagrange.c:3190 itime==1 && resume==0,
+   * src/main.c:124-128 two-way coupling from the first step) */
+  int resume;
 } ch4_config;
 
 /* One Lagrangian particle (the fields of point_particle, src/typedef.h:391-481,

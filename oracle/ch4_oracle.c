@@ -60,6 +60,9 @@ struct ch4o_state {
   /* particles */
   int npart;
   ch4_particle *part;
+  double *pvol, *pdr; /* per-particle volume (4/3 pi r^3) and rho_p/rho_f */
+  /* two-way deposit of this and the previous step, velocity field for the particles */
+  double *dcur, *dprev, *uf;
 };
 
 /* ---- host RNG: drand48 stream (src/random.c:4-16 with SYSTEM_RANDOM48) ---- */
@@ -122,7 +125,8 @@ static void hit_tables(ch4o_state *s, double phi[NK][3], double *tab) {
 }
 
 /* per-cell force of build_forcing's grid loop, src/forcing.c:360-707 */
-static void cell_force(const ch4o_state *s, int i, int j, int k, double t, double sc, const double *hit, double F[3]) {
+static void cell_force(const ch4o_state *s, int i, int j, int k, double t, double sc, const double *hit,
+                       const double *dep, double F[3]) {
   const ch4_config *c = &s->cfg;
   double fx = 0.0, fy = 0.0, fz = 0.0;
   if (c->flags & CH4_F_FORCING_POISEUILLE) { /* src/forcing.c:365-370 */
@@ -165,6 +169,12 @@ static void cell_force(const ch4o_state *s, int i, int j, int k, double t, doubl
     fx += fac * c->gravity_x;
     fy += fac * c->gravity_y;
     fz += fac * c->gravity_z;
+  }
+  if (dep) { /* force += force_twoway, src/lagrange_feedback.c:245-254 */
+    size_t idx = ((size_t)k * (size_t)s->NY + (size_t)j) * (size_t)s->NX + (size_t)i;
+    fx += dep[3 * idx];
+    fy += dep[3 * idx + 1];
+    fz += dep[3 * idx + 2];
   }
   F[0] = fx;
   F[1] = fy;
@@ -236,7 +246,8 @@ static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k)
 }
 
 /* hydro fields of src/lb.c:420-539 from the current populations and F^{n-1} */
-static void hydro(const ch4o_state *s, const double *hit, double *dens, double *u, double *t, double *sc) {
+static void hydro(const ch4o_state *s, const double *hit, const double *dep, double *dens, double *u, double *t,
+                  double *sc) {
   const int NX = s->NX, NY = s->NY, NZ = s->NZ;
   const size_t N = s->N;
   const double hdt = 0.5 * s->cfg.time_dt;
@@ -246,7 +257,7 @@ static void hydro(const ch4o_state *s, const double *hit, double *dens, double *
         size_t idx = cidx(s, i, j, k);
         double a[NPOP], F[3];
         double tprev = s->tprev ? s->tprev[idx] : 0.0, sprev = s->sprev ? s->sprev[idx] : 0.0;
-        cell_force(s, i, j, k, tprev, sprev, hit, F);
+        cell_force(s, i, j, k, tprev, sprev, hit, dep, F);
         if (!(s->cfg.flags & CH4_F_LB_FLUID_FORCING)) F[0] = F[1] = F[2] = 0.0;
         load_cell(s->f[0], N, idx, a);
         double rho = mom0(a);
@@ -265,6 +276,272 @@ static void hydro(const ch4o_state *s, const double *hit, double *dens, double *
           sc[idx] = mom0(a);
         }
       }
+}
+
+
+/* ---- Lagrangian particles (periodic box with LAGRANGE_WRAP) --------------- */
+
+/* wrap(x,s) of src/typedef.h:378 */
+static inline double wrapd(double x, double S) { return (x) - floor((x) / S) * S; }
+static inline int pwrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+/* u component a at interior coordinates (i,j,k) in [-1, N]: the halo is the
+ * periodic copy made by boundary_conditions_hydro (src/boundary_conditions.c:2786) */
+static inline double uat(const ch4o_state *s, const double *u, int a, int i, int j, int k) {
+  return u[3 * cidx(s, pwrap(i, s->NX), pwrap(j, s->NY), pwrap(k, s->NZ)) + a];
+}
+
+/* d u_a / d x_b at a cell of the particle stencil (gradient_vector with LAGRANGE,
+ * src/gradients.c:78-95): centred inside, and on the first halo layer the one-sided
+ * 2nd-order stencil of LAGRANGE_INTERPOLATION_FIX (src/gradients.c:358-420) */
+static double grad_at(const ch4o_state *s, const double *u, int a, int b, int i, int j, int k) {
+  const int n = b == 0 ? s->NX : b == 1 ? s->NY : s->NZ;
+  const int c = b == 0 ? i : b == 1 ? j : k;
+  const int di = b == 0, dj = b == 1, dk = b == 2;
+  const double h1 = 1.0, h2 = 1.0;
+  if (c == -1) {
+    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
+    return a0 * uat(s, u, a, i, j, k) + a1 * uat(s, u, a, i + di, j + dj, k + dk) +
+           a2 * uat(s, u, a, i + 2 * di, j + 2 * dj, k + 2 * dk);
+  }
+  if (c == n) {
+    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
+    return a0 * uat(s, u, a, i, j, k) + a1 * uat(s, u, a, i - di, j - dj, k - dk) +
+           a2 * uat(s, u, a, i - 2 * di, j - 2 * dj, k - 2 * dk);
+  }
+  return (uat(s, u, a, i + di, j + dj, k + dk) - uat(s, u, a, i - di, j - dj, k - dk)) / 2.0;
+}
+
+/* cell of the stencil and the six distances (src/lagrange.c:1231-1287) */
+typedef struct {
+  int im, jm, km;
+  double dxm, dxp, dym, dyp, dzm, dzp;
+  double vol[8]; /* ip_jp_kp, im_jp_kp, ip_jm_kp, ip_jp_km, im_jm_kp, ip_jm_km, im_jp_km, im_jm_km */
+} stencil_t;
+
+static void stencil(const ch4o_state *s, const ch4_particle *p, stencil_t *t) {
+  double px = wrapd(p->x, s->cfg.SX), py = wrapd(p->y, s->cfg.SY), pz = wrapd(p->z, s->cfg.SZ);
+  /* center_V[i] <= x < center_V[i+1] with center_V = index + 0.5 */
+  t->im = (int)floor(px - 0.5);
+  t->jm = (int)floor(py - 0.5);
+  t->km = (int)floor(pz - 0.5);
+  t->dxm = px - ((double)t->im + 0.5);
+  t->dxp = ((double)(t->im + 1) + 0.5) - px;
+  t->dym = py - ((double)t->jm + 0.5);
+  t->dyp = ((double)(t->jm + 1) + 0.5) - py;
+  t->dzm = pz - ((double)t->km + 0.5);
+  t->dzp = ((double)(t->km + 1) + 0.5) - pz;
+  t->vol[0] = t->dxp * t->dyp * t->dzp;
+  t->vol[1] = t->dxm * t->dyp * t->dzp;
+  t->vol[2] = t->dxp * t->dym * t->dzp;
+  t->vol[3] = t->dxp * t->dyp * t->dzm;
+  t->vol[4] = t->dxm * t->dym * t->dzp;
+  t->vol[5] = t->dxp * t->dym * t->dzm;
+  t->vol[6] = t->dxm * t->dyp * t->dzm;
+  t->vol[7] = t->dxm * t->dym * t->dzm;
+}
+
+/* corner order of the trilinear sums: (im,jm,km) (ip,jm,km) (im,jp,km) (im,jm,kp)
+ * (ip,jp,km) (im,jp,kp) (ip,jm,kp) (ip,jp,kp), paired with vol[0..7] */
+static const int CORNER[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}, {1, 1, 1}};
+
+/* interpolate_vector_at_particles(u,'u'), src/lagrange.c:1211-1439 */
+static void interp_particle(const ch4o_state *s, const double *u, ch4_particle *p) {
+  stencil_t t;
+  stencil(s, p, &t);
+  double v[3];
+  for (int a = 0; a < 3; a++) {
+    double acc = 0.0;
+    for (int c = 0; c < 8; c++) {
+      double term = uat(s, u, a, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2]) * t.vol[c];
+      acc = c == 0 ? term : acc + term;
+    }
+    v[a] = acc;
+  }
+  p->ux = v[0];
+  p->uy = v[1];
+  p->uz = v[2];
+  if (s->cfg.flags & CH4_F_LAGRANGE_GRADIENT) {
+    double gr[3][3];
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) {
+        double acc = 0.0;
+        for (int c = 0; c < 8; c++) {
+          double term =
+              grad_at(s, u, a, b, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2]) * t.vol[c];
+          acc = c == 0 ? term : acc + term;
+        }
+        gr[a][b] = acc;
+      }
+    p->dx_ux = gr[0][0];
+    p->dy_ux = gr[0][1];
+    p->dz_ux = gr[0][2];
+    p->dx_uy = gr[1][0];
+    p->dy_uy = gr[1][1];
+    p->dz_uy = gr[1][2];
+    p->dx_uz = gr[2][0];
+    p->dy_uz = gr[2][1];
+    p->dz_uz = gr[2][2];
+  }
+}
+
+/* move_particles for point particles, src/lagrange.c:2934-3470 (tracers
+ * tau_drag == 0, Eulerian probes tau_drag < 0, Stokes drag + added mass) */
+static void move_particle(const ch4o_state *s, ch4_particle *p, int first, double dtl) {
+  if (p->tau_drag < 0.0) {
+    p->vx = p->ux;
+    p->vy = p->uy;
+    p->vz = p->uz;
+  }
+  if (p->tau_drag == 0.0) {
+    p->vx = p->ux;
+    p->vy = p->uy;
+    p->vz = p->uz;
+    if (first) {
+      p->vx_old = p->vx;
+      p->vy_old = p->vy;
+      p->vz_old = p->vz;
+    }
+    p->ax = (p->vx - p->vx_old) / dtl;
+    p->ay = (p->vy - p->vy_old) / dtl;
+    p->az = (p->vz - p->vz_old) / dtl;
+    if (first) {
+      p->x += dtl * p->vx;
+      p->y += dtl * p->vy;
+      p->z += dtl * p->vz;
+    } else {
+      p->x += dtl * 0.5 * (3.0 * p->vx - p->vx_old);
+      p->y += dtl * 0.5 * (3.0 * p->vy - p->vy_old);
+      p->z += dtl * 0.5 * (3.0 * p->vz - p->vz_old);
+    }
+    p->vx_old = p->vx;
+    p->vy_old = p->vy;
+    p->vz_old = p->vz;
+    p->ux_old = p->ux;
+    p->uy_old = p->uy;
+    p->uz_old = p->uz;
+  }
+  if (p->tau_drag > 0.0) {
+    double invtau = 1.0 / p->tau_drag;
+    p->ax = (p->ux - p->vx) * invtau;
+    p->ay = (p->uy - p->vy) * invtau;
+    p->az = (p->uz - p->vz) * invtau;
+    if ((s->cfg.flags & CH4_F_LAGRANGE_ADDEDMASS) && p->beta_coeff != 0.0) {
+      if (first) {
+        p->ux_old = p->ux;
+        p->uy_old = p->uy;
+        p->uz_old = p->uz;
+      }
+      double Dx = (p->ux - p->ux_old) / dtl + (p->ux - p->vx) * p->dx_ux + (p->uy - p->vy) * p->dy_ux +
+                  (p->uz - p->vz) * p->dz_ux;
+      double Dy = (p->uy - p->uy_old) / dtl + (p->ux - p->vx) * p->dx_uy + (p->uy - p->vy) * p->dy_uy +
+                  (p->uz - p->vz) * p->dz_uy;
+      double Dz = (p->uz - p->uz_old) / dtl + (p->ux - p->vx) * p->dx_uz + (p->uy - p->vy) * p->dy_uz +
+                  (p->uz - p->vz) * p->dz_uz;
+      p->ax += Dx * p->beta_coeff;
+      p->ay += Dy * p->beta_coeff;
+      p->az += Dz * p->beta_coeff;
+      p->Dt_ux = Dx;
+      p->Dt_uy = Dy;
+      p->Dt_uz = Dz;
+    }
+    if (first) {
+      p->x += dtl * p->vx;
+      p->y += dtl * p->vy;
+      p->z += dtl * p->vz;
+    } else {
+      p->x += dtl * 0.5 * (3.0 * p->vx - p->vx_old);
+      p->y += dtl * 0.5 * (3.0 * p->vy - p->vy_old);
+      p->z += dtl * 0.5 * (3.0 * p->vz - p->vz_old);
+    }
+    p->vx_old = p->vx;
+    p->vy_old = p->vy;
+    p->vz_old = p->vz;
+    p->ux_old = p->ux;
+    p->uy_old = p->uy;
+    p->uz_old = p->uz;
+    if (first) {
+      p->vx += dtl * p->ax;
+      p->vy += dtl * p->ay;
+      p->vz += dtl * p->az;
+    } else {
+      p->vx += dtl * 0.5 * (3.0 * p->ax - p->ax_old);
+      p->vy += dtl * 0.5 * (3.0 * p->ay - p->ay_old);
+      p->vz += dtl * 0.5 * (3.0 * p->az - p->az_old);
+    }
+    p->ax_old = p->ax;
+    p->ay_old = p->ay;
+    p->az_old = p->az;
+  }
+}
+
+/* sendrecv_particles on one rank (src/lagrange.c:4028-4221): LAGRANGE_WRAP puts
+ * every coordinate back in [0,S); a particle whose wrapped coordinate rounds to S
+ * counts as leaving and is re-appended after the others (stable order). */
+static void wrap_particles(ch4o_state *s) {
+  const double SX = s->cfg.SX, SY = s->cfg.SY, SZ = s->cfg.SZ;
+  int n = s->npart, nthere = 0;
+  ch4_particle *tmp = (ch4_particle *)malloc(sizeof(ch4_particle) * (size_t)(n > 0 ? n : 1));
+  double *tv = (double *)malloc(sizeof(double) * 2 * (size_t)(n > 0 ? n : 1));
+  int *there = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  int nhere = 0;
+  for (int i = 0; i < n; i++) {
+    ch4_particle *p = &s->part[i];
+    double wx = wrapd(p->x, SX), wy = wrapd(p->y, SY), wz = wrapd(p->z, SZ);
+    p->x = wrapd(p->x, SX);
+    p->z = wrapd(p->z, SZ);
+    p->y = wrapd(p->y, SY);
+    if (wx >= 0.0 && wx < SX && wy >= 0.0 && wy < SY && wz >= 0.0 && wz < SZ) {
+      tmp[nhere] = *p;
+      tv[2 * nhere] = s->pvol[i];
+      tv[2 * nhere + 1] = s->pdr[i];
+      nhere++;
+    } else {
+      there[nthere++] = i;
+    }
+  }
+  if (nthere) {
+    for (int t = 0; t < nthere; t++) {
+      tmp[nhere + t] = s->part[there[t]];
+      tv[2 * (nhere + t)] = s->pvol[there[t]];
+      tv[2 * (nhere + t) + 1] = s->pdr[there[t]];
+    }
+    memcpy(s->part, tmp, sizeof(ch4_particle) * (size_t)n);
+    for (int i = 0; i < n; i++) {
+      s->pvol[i] = tv[2 * i];
+      s->pdr[i] = tv[2 * i + 1];
+    }
+  }
+  free(tmp);
+  free(tv);
+  free(there);
+}
+
+/* add_particle_feedbacks, trilinear + LAGRANGE_TWOWAY_MOMENTUM without gravity
+ * (src/lagrange_feedback.c:11-256).  Deposits landing on halo cells are dropped,
+ * as the reference's border fold adds interior values into the halo and never
+ * the reverse (src/lagrange_feedback.c:525-835).  Particles of zero or undefined
+ * volume (tracers, beta = 0, probes) add nothing. */
+static void deposit(const ch4o_state *s, double *D) {
+  memset(D, 0, sizeof(double) * 3 * s->N);
+  for (int ip = 0; ip < s->npart; ip++) {
+    const ch4_particle *p = &s->part[ip];
+    const double fac = s->pvol[ip], dr = s->pdr[ip];
+    if (!(fac > 0.0) || p->beta_coeff == 0.0) continue;
+    stencil_t t;
+    stencil(s, p, &t);
+    const double gx = 0.0, gy = 0.0, gz = 0.0;
+    double fp[3];
+    fp[0] = p->Dt_ux - gx + dr * (gx - p->ax);
+    fp[1] = p->Dt_uy - gy + dr * (gy - p->ay);
+    fp[2] = p->Dt_uz - gz + dr * (gz - p->az);
+    for (int a = 0; a < 3; a++)
+      for (int c = 0; c < 8; c++) {
+        int i = t.im + CORNER[c][0], j = t.jm + CORNER[c][1], k = t.km + CORNER[c][2];
+        if (i < 0 || i >= s->NX || j < 0 || j >= s->NY || k < 0 || k >= s->NZ) continue;
+        D[3 * cidx(s, i, j, k) + a] += fac * fp[a] * t.vol[c];
+      }
+  }
 }
 
 /* one step of src/main.c:67-161 */
@@ -286,11 +563,23 @@ static void one_step(ch4o_state *s) {
     hit_tables(s, s->phi_cur, s->hit_cur);
   }
 
+  /* two-way coupling: deposit of the particles moved in the previous step
+   * (src/main.c:122-128: from the second step on unless resuming) */
+  if (c->flags & CH4_F_LAGRANGE_TWOWAY) {
+    double *tmp = s->dprev;
+    s->dprev = s->dcur;
+    s->dcur = tmp;
+    if (c->resume || s->itime > 1)
+      deposit(s, s->dcur);
+    else
+      memset(s->dcur, 0, sizeof(double) * 3 * N);
+  }
+
   /* u^n field (needed by LES gradients, src/fluid.c:1056-1075) */
   double *uarr = NULL;
   if (c->flags & CH4_F_FLUID_LES) {
     uarr = (double *)malloc(sizeof(double) * 3 * N);
-    hydro(s, s->hit_prev, NULL, uarr, NULL, NULL);
+    hydro(s, s->hit_prev, s->dprev, NULL, uarr, NULL, NULL);
   }
 
   const double invtau_u = 1.0 / c->tau_u;
@@ -316,8 +605,9 @@ static void one_step(ch4o_state *s) {
         }
         double Fp[3] = {0, 0, 0}, Fc[3] = {0, 0, 0};
         if (forcing) {
-          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_prev, Fp);
-          cell_force(s, i, j, k, tt, ss, s->hit_cur, Fc);
+          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_prev,
+                     s->dprev, Fp);
+          cell_force(s, i, j, k, tt, ss, s->hit_cur, s->dcur, Fc);
         }
         double ux = mx / rho + hdt * Fp[0];
         double uy = my / rho + hdt * Fp[1];
@@ -425,6 +715,19 @@ static void one_step(ch4o_state *s) {
     s->fn[set] = tmp;
   }
   free(uarr);
+
+  /* Lagrangian sub-steps, src/main.c:164-185: u^{n+1} with dt/2 F^n, then
+   * interpolate + move + wrap time_dt_lagr_factor times */
+  if (c->flags & CH4_F_LAGRANGE) {
+    hydro(s, s->hit_cur, s->dcur, NULL, s->uf, NULL, NULL);
+    const double dtl = c->time_dt / c->time_dt_lagr_factor;
+    const int first = (s->itime == 1 && c->resume == 0);
+    for (int sub = 0; sub < (int)c->time_dt_lagr_factor; sub++) {
+      for (int ip = 0; ip < s->npart; ip++) interp_particle(s, s->uf, &s->part[ip]);
+      for (int ip = 0; ip < s->npart; ip++) move_particle(s, &s->part[ip], first, dtl);
+      wrap_particles(s);
+    }
+  }
 }
 
 int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
@@ -458,6 +761,11 @@ int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
   if (s->nsets_on[1]) s->tprev = (double *)calloc(s->N, sizeof(double));
   if (s->nsets_on[2]) s->sprev = (double *)calloc(s->N, sizeof(double));
   s->force = (double *)calloc(3 * s->N, sizeof(double));
+  if (cfg->flags & CH4_F_LAGRANGE_TWOWAY) {
+    s->dcur = (double *)calloc(3 * s->N, sizeof(double));
+    s->dprev = (double *)calloc(3 * s->N, sizeof(double));
+  }
+  if (cfg->flags & CH4_F_LAGRANGE) s->uf = (double *)calloc(3 * s->N, sizeof(double));
   s->tau_les = (double *)calloc(s->N, sizeof(double));
   /* constant force tables */
   const double LX = cfg->SX, LY = cfg->SY, nu = cfg->nu;
@@ -515,6 +823,11 @@ int ch4o_destroy(ch4o_state *s) {
   free(s->hit_prev);
   free(s->hit_cur);
   free(s->part);
+  free(s->pvol);
+  free(s->pdr);
+  free(s->dcur);
+  free(s->dprev);
+  free(s->uf);
   free(s);
   return CH4_OK;
 }
@@ -594,7 +907,7 @@ int ch4o_initialize(ch4o_state *s) {
         size_t idx = cidx(s, i, j, k);
         double F[3] = {0, 0, 0};
         if (s->cfg.flags & CH4_F_LB_FLUID_FORCING)
-          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_cur, F);
+          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_cur, NULL, F);
         s->force[3 * idx] = F[0];
         s->force[3 * idx + 1] = F[1];
         s->force[3 * idx + 2] = F[2];
@@ -624,7 +937,7 @@ int ch4o_get_fields(ch4o_state *s, double *dens, double *u, double *t, double *s
   double *d0 = (double *)malloc(sizeof(double) * N), *u0 = (double *)malloc(sizeof(double) * 3 * N);
   double *t0 = (double *)calloc(N, sizeof(double)), *s0 = (double *)calloc(N, sizeof(double));
   /* between steps the kept temperature is t^n and the latest phases those of F^n */
-  hydro(s, s->hit_cur, d0, u0, t0, s0);
+  hydro(s, s->hit_cur, s->dcur, d0, u0, t0, s0);
   if (dens) scatter_field(s, d0, 1, dens, brd);
   if (u) scatter_field(s, u0, 3, u, brd);
   if (t) scatter_field(s, t0, 1, t, brd);
@@ -642,9 +955,22 @@ int ch4o_get_force(ch4o_state *s, double *force, int brd) {
 }
 
 int ch4o_set_particles(ch4o_state *s, const ch4_particle *parts, int n) {
+  if (n < 0 || (n > 0 && !parts)) return CH4_ERR_ARG;
   free(s->part);
-  s->part = (ch4_particle *)malloc(sizeof(ch4_particle) * (size_t)(n > 0 ? n : 1));
+  free(s->pvol);
+  free(s->pdr);
+  size_t m = (size_t)(n > 0 ? n : 1);
+  s->part = (ch4_particle *)malloc(sizeof(ch4_particle) * m);
+  s->pvol = (double *)malloc(sizeof(double) * m);
+  s->pdr = (double *)malloc(sizeof(double) * m);
   memcpy(s->part, parts, sizeof(ch4_particle) * (size_t)n);
+  for (int i = 0; i < n; i++) {
+    /* src/lagrange_feedback.c:84-90 */
+    double beta = parts[i].beta_coeff, tau = parts[i].tau_drag;
+    s->pdr[i] = (3.0 - beta) / (2.0 * beta);
+    double squared_radius = 3.0 * s->cfg.nu * beta * tau;
+    s->pvol[i] = (4. / 3.) * 3.14159265359 * pow(squared_radius, 3. / 2.);
+  }
   s->npart = n;
   return CH4_OK;
 }

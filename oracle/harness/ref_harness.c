@@ -150,8 +150,14 @@ static void dump_state(void) {
 }
 
 int main(int argc, char **argv) {
+#ifdef LAGRANGE
+  if (argc >= 2 && strcmp(argv[1], "layout") == 0) { /* only report the particle record layout */
+    write_part_layout();
+    return 0;
+  }
+#endif
   if (argc < 3) {
-    fprintf(stderr, "usage: %s <nsteps> <seed>\n", argv[0]);
+    fprintf(stderr, "usage: %s <nsteps> <seed> | layout\n", argv[0]);
     return 1;
   }
   int nsteps = atoi(argv[1]);

@@ -42,6 +42,8 @@ FLAGSETS = {
                "LB_SCALAR_BC_Y"],
     "les": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
             "LB_FLUID_BC_Y", "LB_FLUID_LES"],
+    "particles": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                  "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
 }
 # non-flag configuration implied by a flag set (define.h variants of one setting)
 FLAGSET_EXTRA = {"walls2": {"t0_kind": abi.T0_REF}}
@@ -85,13 +87,17 @@ PARAM_KEYS = ["resume", "resume_u", "resume_t", "resume_s", "NX", "NY", "NZ", "S
               "tau_u", "Amp_x", "Amp_y", "Amp_z", "gravity_x", "gravity_y", "gravity_z",
               "tau_t", "T_bot", "T_top", "T_ref", "grad_T_bot", "grad_T_top", "beta_t", "beta2_t",
               "tau_s", "S_bot", "S_top", "S_ref", "beta_s",
-              "time_dt_lagr_factor", "time_dump_lagr", "particle_number"]
+              "time_dt_lagr_factor", "time_dump_lagr", "particle_number",
+              "tau_drag_types", "tau_drag_min", "tau_drag_max",
+              "beta_coeff_types", "beta_coeff_min", "beta_coeff_max"]
 
 
 def write_param_in(path, cfg, nsteps=1):
-    vals = {"resume": 0, "resume_u": 0, "resume_t": 0, "resume_s": 0,
+    vals = {"resume": int(cfg.resume), "resume_u": 0, "resume_t": 0, "resume_s": 0,
             "time_start": 0.0, "time_end": float(nsteps), "time_dump_field": 1e12,
-            "time_dump_diagn": 1e12, "time_dump_lagr": 1e12}
+            "time_dump_diagn": 1e12, "time_dump_lagr": 1e12,
+            "tau_drag_types": 1, "tau_drag_min": 1.0, "tau_drag_max": 1.0,
+            "beta_coeff_types": 1, "beta_coeff_min": 1.0, "beta_coeff_max": 1.0}
     with open(path, "w") as f:
         for k in PARAM_KEYS:
             v = vals[k] if k in vals else getattr(cfg, k)
@@ -103,7 +109,37 @@ def aos_from_soa(f_soa, NX, NY, NZ):
     return np.ascontiguousarray(f_soa.reshape(NPOP, NZ, NY, NX).transpose(1, 2, 3, 0))
 
 
-def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None):
+def part_layout(flagset):
+    """field -> double offset of the reference's point_particle record for a flag set."""
+    tmp = tempfile.mkdtemp(prefix="ch4lay_")
+    subprocess.run([ref_binary(flagset), "layout"], cwd=tmp, check=True, capture_output=True)
+    lay = {}
+    with open(os.path.join(tmp, "part_layout.txt")) as f:
+        for line in f:
+            k, v = line.split()
+            lay[k] = int(v)
+    return lay
+
+
+def particles_to_ref(parts, lay):
+    """ch4_particle array -> reference point_particle records (float64 [n, size])."""
+    a = np.zeros((len(parts), lay["size"]))
+    for name, off in lay.items():
+        if name != "size":
+            a[:, off] = [getattr(p, name) for p in parts]
+    return a
+
+
+def particles_from_ref(arr, lay):
+    """reference records -> dict of field -> array (fields of the record only)."""
+    return {name: arr[:, off].copy() for name, off in lay.items() if name != "size"}
+
+
+def particles_as_dict(parts):
+    return {n: np.array([getattr(p, n) for p in parts]) for n in abi.PARTICLE_FIELDS}
+
+
+def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None, parts=None):
     """Run the compiled reference on injected populations.
 
     pops: dict which -> AoS array [NZ][NY][NX][NPOP] (interior cells).
@@ -118,6 +154,10 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None)
         np.ascontiguousarray(arr, dtype=np.float64).tofile(os.path.join(tmp, "in_%s.bin" % which))
     if phi is not None:
         np.ascontiguousarray(phi, dtype=np.float64).tofile(os.path.join(tmp, "in_phi.bin"))
+    lay = None
+    if parts is not None:
+        lay = part_layout(flagset)
+        particles_to_ref(parts, lay).tofile(os.path.join(tmp, "in_part.bin"))
     seed = int(cfg.seed) if seed is None else seed
     r = subprocess.run([exe, str(nsteps), str(seed)], cwd=tmp, capture_output=True, text=True)
     if r.returncode != 0:
@@ -131,6 +171,9 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None)
         fn = os.path.join(tmp, "out_%s.bin" % name)
         if os.path.exists(fn):
             out[name] = np.fromfile(fn, dtype=np.float64).reshape(shape)
+    if lay is not None:
+        arr = np.fromfile(os.path.join(tmp, "out_part.bin"), dtype=np.float64).reshape(-1, lay["size"])
+        out["part"] = particles_from_ref(arr, lay)
     with open(os.path.join(tmp, "timing.json")) as f:
         out["timing"] = json.load(f)
     return out

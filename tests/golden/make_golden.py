@@ -17,16 +17,19 @@ sys.path.insert(0, os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"))
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "ch4-project_b200"))
 import oracle as O  # noqa: E402
-from lbcases import CASES, make_case  # noqa: E402
+from lbcases import CASES, make_case, pop_items  # noqa: E402
 
 NSTEPS = 12
 SEED = 7
 
 for name in sorted(CASES):
     flagset, cfg, state = make_case(name, seed=SEED)
-    ref = O.run_reference(flagset, cfg, NSTEPS, state)
+    ref = O.run_reference(flagset, cfg, NSTEPS, dict(pop_items(state)), parts=state.get("part"))
     out = {"seed": SEED, "nsteps": NSTEPS}
-    for k, v in state.items():
+    if "part" in ref:
+        for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux"):
+            out["out_part_" + f] = ref["part"][f]
+    for k, v in pop_items(state):
         out["in_sha256_" + k] = hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()
         out["out_" + k] = ref[k]
     for k in ("u", "t", "s", "phi"):

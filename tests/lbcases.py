@@ -41,7 +41,28 @@ CASES = {
                                S_bot=0.2, S_top=0.7, S_ref=0.1, beta_s=0.3, gravity_y=2e-3, gravity_x=1e-3)),
     "les": dict(flagset="les", NX=8, NY=9, NZ=6,
                 params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "particles": dict(flagset="particles", NX=10, NY=8, NZ=7, npart=300,
+                      params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=6,
+                                  time_dt_lagr_factor=2.0, particle_number=300)),
 }
+
+
+def make_particles(rng, n, NX, NY, NZ):
+    """Tracers and Stokes particles (beta in {1, 3}, tau_drag in {0.5, 2, 5}), uniform
+    random positions (a few exactly on cell centres and faces), at rest."""
+    from ch4b200 import abi
+    parts = (abi.Particle * n)()
+    taus = [0.0, 0.5, 2.0, 5.0]
+    betas = [1.0, 3.0]
+    for i in range(n):
+        p = parts[i]
+        p.name = float(i)
+        p.tau_drag = taus[i % len(taus)]
+        p.beta_coeff = betas[(i // len(taus)) % len(betas)]
+        p.x, p.y, p.z = rng.random() * NX, rng.random() * NY, rng.random() * NZ
+        if i % 50 == 7:  # on a cell centre / on the domain face
+            p.x, p.y, p.z = 0.5 + (i % NX), 0.0, float(NZ) - 0.5
+    return parts
 
 
 def make_case(name, seed=0, storage=0, **over):
@@ -57,18 +78,28 @@ def make_case(name, seed=0, storage=0, **over):
         state["g"] = rb_temperature_pops(rng, c["NX"], c["NY"], c["NZ"], cfg.T_bot, cfg.T_top, 1e-2)
     if "LB_SCALAR" in flags:
         state["h"] = pops(rng, c["NX"], c["NY"], c["NZ"], 0.3, 1e-1)
+    if "LAGRANGE" in flags:
+        state["part"] = make_particles(rng, c["npart"], c["NX"], c["NY"], c["NZ"])
     return c["flagset"], cfg, state
+
+
+def pop_items(state):
+    return [(k, v) for k, v in state.items() if k in ("p", "g", "h")]
 
 
 def run_restatement(cfg, state, nsteps, phi=None):
     r = O.Restatement(cfg)
-    for k, v in state.items():
+    for k, v in pop_items(state):
         r.set_pop(k, v)
+    if "part" in state:
+        r.set_particles(state["part"])
     if phi is not None:
         r.set_hit_phases(phi)
     r.initialize()
     r.step(nsteps)
-    out = {k: r.get_pop(k) for k in state}
+    out = {k: r.get_pop(k) for k, _ in pop_items(state)}
+    if "part" in state:
+        out["part"] = O.particles_as_dict(r.get_particles(len(state["part"])))
     out.update(r.fields())
     out["force"] = r.force()
     if cfg.flags & O.abi.FLAGS["LB_FLUID_FORCING_HIT"]:

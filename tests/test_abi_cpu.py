@@ -33,7 +33,7 @@ def test_config_default():
 def test_read_param_semantics(tmp_path):
     p = tmp_path / "param.in"
     # first number after a key wins; extra numbers are consumed as junk pairs
-    p.write_text("NX 16\nNY 8\nNZ 4\nSX 16\nSY 8\nSZ 4\ntime_dt 1.0\n"
+    p.write_text("resume 0\nNX 16\nNY 8\nNZ 4\nSX 16\nSY 8\nSZ 4\ntime_dt 1.0\n"
                  "tau_u 0.6 0.51 0.52 0.53 0.54\nAmp_x 1.e-2\nAmp_y 0\nAmp_z 0\n")
     c = ch4b200.default_config()
     c.flags = abi.flags_of(["LB_FLUID", "LB_FLUID_FORCING"])
@@ -46,7 +46,7 @@ def test_read_param_semantics(tmp_path):
 
 def test_read_param_missing_key(tmp_path):
     p = tmp_path / "param.in"
-    p.write_text("NX 16\nNY 8\n")
+    p.write_text("resume 0\nNX 16\nNY 8\n")
     c = ch4b200.default_config()
     with pytest.raises(ch4b200.CH4Error) as e:
         ch4b200.read_param(c, str(p))

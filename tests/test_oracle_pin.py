@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from lbcases import CASES, make_case, run_restatement
+from lbcases import CASES, make_case, pop_items, run_restatement
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -22,17 +22,20 @@ def _assert_same(a, b, what):
 
 
 @pytest.mark.parametrize("name,nsteps", [("kolmogorov", 20), ("rb", 20), ("hit", 15), ("walls2", 20),
-                                          ("scalar", 20), ("les", 20)])
+                                          ("scalar", 20), ("les", 20), ("particles", 8)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
         pytest.skip("reference build oracle/_ref/%s missing" % flagset)
-    ref = O.run_reference(flagset, cfg, nsteps, state)
+    ref = O.run_reference(flagset, cfg, nsteps, dict(pop_items(state)), parts=state.get("part"))
     mine = run_restatement(cfg, state, nsteps)
     if "phi" in ref:
         _assert_same(mine["phi"], ref["phi"], "HIT phases")
-    for k in state:
+    for k, _ in pop_items(state):
         _assert_same(mine[k], ref[k], "%s populations" % k)
+    if "part" in ref:
+        for f, v in ref["part"].items():
+            _assert_same(mine["part"][f], v, "particle field " + f)
     _assert_same(mine["u"], ref["u"], "u")
     _assert_same(mine["dens"], ref["dens"], "dens")
     if "t" in ref:
@@ -62,12 +65,27 @@ def test_restatement_matches_golden_fixture(name):
     g = np.load(path)
     flagset, cfg, state = make_case(name, seed=int(g["seed"]))
     import hashlib
-    for k in state:
-        h = hashlib.sha256(np.ascontiguousarray(state[k]).tobytes()).hexdigest()
+    for k, v in pop_items(state):
+        h = hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()
         assert h == str(g["in_sha256_" + k]), "case generator changed for %s" % k
     mine = run_restatement(cfg, state, int(g["nsteps"]))
-    for k in state:
+    for k, _ in pop_items(state):
         _assert_same(mine[k], g["out_" + k], k)
+    for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux"):
+        if "out_part_" + f in g.files:
+            _assert_same(mine["part"][f], g["out_part_" + f], "particle " + f)
     for k in ("u", "t", "s", "phi"):
         if "out_" + k in g.files:
             _assert_same(mine[k], g["out_" + k], k)
+
+
+def test_two_way_deposit_is_active():
+    """The particle case really feeds momentum back: its force field differs from
+    the same flow without the deposit (HIT forcing only)."""
+    _, cfg, state = make_case("particles", seed=3)
+    with_dep = run_restatement(cfg, state, 4)
+    from ch4b200 import abi
+    cfg2 = make_case("particles", seed=3)[1]
+    cfg2.flags &= ~(abi.FLAGS["LAGRANGE_TWOWAY"] | abi.FLAGS["LAGRANGE_TWOWAY_MOMENTUM"])
+    no_dep = run_restatement(cfg2, state, 4)
+    assert np.abs(with_dep["force"] - no_dep["force"]).max() > 1e-12
