@@ -51,7 +51,9 @@ const uint64_t SUPPORTED =
     CH4_F_LB_TEMPERATURE | CH4_F_TEMPERATURE_BUOYANCY | CH4_F_LB_SCALAR | CH4_F_SCALAR_BUOYANCY | CH4_F_FLUID_BC_Y |
     CH4_F_FLUID_BC_Y_P_SLIP | CH4_F_FLUID_BC_Y_M_SLIP | CH4_F_TEMPERATURE_BC_Y | CH4_F_TEMPERATURE_BC_Y_P_FLUX |
     CH4_F_TEMPERATURE_BC_Y_M_FLUX | CH4_F_TEMPERATURE_BC_Y_P_NOFLUX | CH4_F_TEMPERATURE_BC_Y_M_NOFLUX |
-    CH4_F_SCALAR_BC_Y | CH4_F_FLUID_LES | CH4_F_TEMPERATURE_FORCING;
+    CH4_F_SCALAR_BC_Y | CH4_F_FLUID_LES | CH4_F_TEMPERATURE_FORCING | CH4_F_LAGRANGE | CH4_F_LAGRANGE_WRAP |
+    CH4_F_LAGRANGE_GRADIENT | CH4_F_LAGRANGE_ADDEDMASS | CH4_F_LAGRANGE_TWOWAY | CH4_F_LAGRANGE_TWOWAY_MOMENTUM |
+    CH4_F_LAGRANGE_GRADIENT_BRD2;
 
 }  // namespace
 
@@ -66,6 +68,9 @@ struct EngineBase {
   virtual ch4_status initialize() = 0;
   virtual ch4_status step(int n) = 0;
   virtual ch4_status fields(double* dens, double* u, double* t, double* s, double* force, int brd) = 0;
+  virtual ch4_status averages(ch4_averages* out) = 0;
+  virtual ch4_status set_particles(const ch4_particle* parts, int n) = 0;
+  virtual ch4_status get_particles(ch4_particle* parts, int n) = 0;
   virtual size_t device_bytes() const = 0;
 };
 
@@ -168,6 +173,20 @@ struct Engine : EngineBase {
   static constexpr int CHUNK = 256;
   StepParams<A> P{};
   LaunchShape shape{};
+  // Lagrangian particles
+  int np = 0;
+  double* pf = nullptr;   // [PF_TOTAL][np]
+  A* upart = nullptr;     // u^{n+1} for the interpolation, 3 planes
+  A* dbuf[2] = {nullptr, nullptr};  // two-way deposit of this / previous step
+  int dcur_i = 0;
+  unsigned int *key = nullptr, *key2 = nullptr;
+  int *order = nullptr, *order2 = nullptr;
+  double* rec = nullptr;
+  int *cstart = nullptr, *cend = nullptr;
+  void* cubtmp = nullptr;
+  size_t cubbytes = 0;
+  bool lagr() const { return (c.flags & CH4_F_LAGRANGE) != 0; }
+  bool twoway() const { return (c.flags & CH4_F_LAGRANGE_TWOWAY) != 0; }
 
   Engine(ch4_handle* h) : H(h), c(h->cfg) {
     N = (long long)c.NX * c.NY * c.NZ;
@@ -194,6 +213,156 @@ struct Engine : EngineBase {
     if (staging_h) cudaFreeHost(staging_h);
     if (hit_h) cudaFreeHost(hit_h);
     if (hit_ev) cudaEventDestroy(hit_ev);
+    free_particles();
+    cudaFree(upart);
+    cudaFree(dbuf[0]);
+    cudaFree(dbuf[1]);
+    cudaFree(cstart);
+    cudaFree(cend);
+  }
+
+  void free_particles() {
+    cudaFree(pf);
+    cudaFree(key);
+    cudaFree(key2);
+    cudaFree(order);
+    cudaFree(order2);
+    cudaFree(rec);
+    cudaFree(cubtmp);
+    pf = nullptr;
+    key = key2 = nullptr;
+    order = order2 = nullptr;
+    rec = nullptr;
+    cubtmp = nullptr;
+    cubbytes = 0;
+    np = 0;
+  }
+
+  size_t nhome() const { return (size_t)(c.NX + 1) * (c.NY + 1) * (c.NZ + 1); }
+
+  PartParams<A> part_params() {
+    PartParams<A> Q{};
+    Q.NX = c.NX;
+    Q.NY = c.NY;
+    Q.NZ = c.NZ;
+    Q.N = N;
+    Q.np = np;
+    Q.SX = c.SX;
+    Q.SY = c.SY;
+    Q.SZ = c.SZ;
+    Q.dtl = c.time_dt / c.time_dt_lagr_factor;
+    Q.gradient = (c.flags & CH4_F_LAGRANGE_GRADIENT) != 0;
+    Q.addedmass = (c.flags & CH4_F_LAGRANGE_ADDEDMASS) != 0;
+    Q.pf = pf;
+    Q.u = upart;
+    Q.key = key;
+    Q.order = order;
+    Q.rec = rec;
+    Q.cell_start = cstart;
+    Q.cell_end = cend;
+    Q.dep = dbuf[dcur_i];
+    return Q;
+  }
+
+  // dump_averages (src/output.c:63-~720): hydro fields in FP64, deterministic sums, normalisation
+  ch4_status averages(ch4_averages* out) override {
+    bind_pops(cur);
+    const size_t n1 = (size_t)N;
+    const int nblocks = (int)std::min<long long>(4 * 148, (N + AVG_BLOCK - 1) / AVG_BLOCK);
+    double* d = nullptr;
+    ch4_status st;
+    const size_t total = 6 * n1 + (size_t)nblocks * NAVG * 2 + NAVG;
+    if ((st = H->cuda(cudaMalloc(&d, total * sizeof(double)), "averages scratch"))) return st;
+    double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *part = d + 6 * n1;
+    double* res = part + (size_t)nblocks * NAVG * 2;
+    const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
+    st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, dd, du, nsets_on[1] ? dt : nullptr,
+                              nsets_on[2] ? ds : nullptr, nullptr, nullptr, H->stream),
+                 "hydro");
+    AvgParams Q{};
+    Q.NX = c.NX;
+    Q.NY = c.NY;
+    Q.NZ = c.NZ;
+    Q.N = N;
+    Q.dens = dd;
+    Q.u = du;
+    Q.t = nsets_on[1] ? dt : nullptr;
+    Q.s = nsets_on[2] ? ds : nullptr;
+    Q.fwall = (c.flags & CH4_F_FLUID_BC_Y) != 0;
+    Q.twall = (c.flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+    Q.nu = c.nu;
+    Q.kappa = c.kappa;
+    Q.partial = part;
+    double h[NAVG];
+    if (!st) st = H->cuda(launch_averages(Q, nblocks, res, H->stream), "averages");
+    if (!st) st = H->cuda(cudaMemcpyAsync(h, res, sizeof h, cudaMemcpyDeviceToHost, H->stream), "averages down");
+    if (!st) st = H->cuda(cudaStreamSynchronize(H->stream), "averages sync");
+    cudaFree(d);
+    if (st) return st;
+    const double norm = 1.0 / (c.SX * c.SY * c.SZ);  // src/output.c:498-579
+    for (int q = 0; q < 18; q++) h[q] *= norm;
+    for (int q = 18; q < 21; q++) h[q] *= norm / (c.kappa * c.deltaT / c.SY);
+    h[21] *= norm;
+    h[22] *= norm;
+    std::memcpy(out, h, sizeof h);
+    return CH4_OK;
+  }
+
+  ch4_status set_particles(const ch4_particle* parts, int n) override {
+    if (!lagr()) return H->fail(CH4_ERR_ARG, "particles need the LAGRANGE flag");
+    if (n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "bad particle array");
+    ch4_status st;
+    if ((st = H->cuda(cudaStreamSynchronize(H->stream), "sync"))) return st;
+    if (n != np) {
+      free_particles();
+      if (n > 0) {
+        if (cudaMalloc(&pf, sizeof(double) * PF_TOTAL * (size_t)n) != cudaSuccess)
+          return H->fail(CH4_ERR_NOMEM, "particle state");
+        if (twoway()) {
+          bool ok = cudaMalloc(&key, sizeof(unsigned) * n) == cudaSuccess &&
+                    cudaMalloc(&key2, sizeof(unsigned) * n) == cudaSuccess &&
+                    cudaMalloc(&order, sizeof(int) * n) == cudaSuccess &&
+                    cudaMalloc(&order2, sizeof(int) * n) == cudaSuccess &&
+                    cudaMalloc(&rec, sizeof(double) * 9 * (size_t)n) == cudaSuccess;
+          if (!ok) return H->fail(CH4_ERR_NOMEM, "deposit buffers");
+          np = n;
+          PartParams<A> Q = part_params();
+          size_t bytes = 0;
+          if ((st = H->cuda(launch_deposit(Q, key2, order2, nullptr, bytes, H->stream), "sort size"))) return st;
+          cubbytes = bytes;
+          if (cudaMalloc(&cubtmp, bytes ? bytes : 16) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "sort scratch");
+        }
+      }
+      np = n;
+    }
+    if (n == 0) return CH4_OK;
+    // AoS -> SoA with the two per-particle deposit constants (src/lagrange_feedback.c:84-90, host libm)
+    std::vector<double> h((size_t)PF_TOTAL * n);
+    const double* raw = reinterpret_cast<const double*>(parts);
+    for (int i = 0; i < n; i++) {
+      for (int f = 0; f < PF_FIELDS; f++) h[(size_t)f * n + i] = raw[(size_t)i * PF_FIELDS + f];
+      double beta = parts[i].beta_coeff, tau = parts[i].tau_drag;
+      h[(size_t)PF_DR * n + i] = (3.0 - beta) / (2.0 * beta);
+      double squared_radius = 3.0 * c.nu * beta * tau;
+      h[(size_t)PF_VOL * n + i] = (4. / 3.) * 3.14159265359 * std::pow(squared_radius, 3. / 2.);
+    }
+    if ((st = H->cuda(cudaMemcpy(pf, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice), "particles up")))
+      return st;
+    return CH4_OK;
+  }
+
+  ch4_status get_particles(ch4_particle* parts, int n) override {
+    if (n > np || n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "asked for %d of %d particles", n, np);
+    if (n == 0) return CH4_OK;
+    std::vector<double> h((size_t)PF_TOTAL * np);
+    ch4_status st;
+    if ((st = H->cuda(cudaStreamSynchronize(H->stream), "sync"))) return st;
+    if ((st = H->cuda(cudaMemcpy(h.data(), pf, sizeof(double) * h.size(), cudaMemcpyDeviceToHost), "particles down")))
+      return st;
+    double* raw = reinterpret_cast<double*>(parts);
+    for (int i = 0; i < n; i++)
+      for (int f = 0; f < PF_FIELDS; f++) raw[(size_t)i * PF_FIELDS + f] = h[(size_t)f * np + i];
+    return CH4_OK;
   }
 
   int L() const { return c.NX + c.NY + c.NZ; }
@@ -221,6 +390,16 @@ struct Engine : EngineBase {
     }
     if (nsets_on[1] && cudaMalloc(&tprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tprev");
     if (nsets_on[2] && cudaMalloc(&sprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "sprev");
+    if (lagr() && cudaMalloc(&upart, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u for particles");
+    if (twoway()) {
+      for (int b = 0; b < 2; b++) {
+        if (cudaMalloc(&dbuf[b], 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "deposit");
+        if (cudaMemset(dbuf[b], 0, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "deposit memset");
+      }
+      if (cudaMalloc(&cstart, sizeof(int) * nhome()) != cudaSuccess ||
+          cudaMalloc(&cend, sizeof(int) * nhome()) != cudaSuccess)
+        return H->fail(CH4_ERR_NOMEM, "home-cell ranges");
+    }
     if (c.flags & CH4_F_FLUID_LES) {
       if (cudaMalloc(&ules, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
       if (cudaMalloc(&tau_les, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tau_les");
@@ -479,14 +658,41 @@ struct Engine : EngineBase {
         if ((st = H->cuda(cudaEventRecord(hit_ev, H->stream), "hit event"))) return st;
       }
       for (int k = 0; k < m; k++) {
+        const int n_step = H->itime + 1;  // the reference's itime during this step
         bind_pops(cur);
         P.hit_prev = hit ? hit_ring + (size_t)k * slot : nullptr;
         P.hit_cur = hit ? hit_ring + (size_t)(k + 1) * slot : nullptr;
+        if (twoway()) {
+          // deposit of the particles moved in the previous step (src/main.c:122-128)
+          dcur_i ^= 1;
+          P.dcur = dbuf[dcur_i];
+          P.dprev = dbuf[dcur_i ^ 1];
+          P.feat |= K_TWOWAY;
+          if (c.resume || n_step > 1) {
+            PartParams<A> Q = part_params();
+            size_t bytes = cubbytes;
+            if ((st = H->cuda(launch_deposit(Q, key2, order2, cubtmp, bytes, H->stream), "deposit"))) return st;
+          } else if ((st = H->cuda(cudaMemsetAsync(dbuf[dcur_i], 0, 3 * N * sizeof(A), H->stream), "deposit zero"))) {
+            return st;
+          }
+        }
         if (c.flags & CH4_F_FLUID_LES)
           if ((st = les_u())) return st;
         if ((st = H->cuda(launch_step(P, shape, H->stream), "lb_step"))) return st;
         cur ^= 1;
         H->itime++;
+        if (lagr()) {
+          // u^{n+1} with dt/2 F^n, then the Lagrangian sub-steps (src/main.c:164-185)
+          bind_pops(cur);
+          if ((st = H->cuda(launch_hydro(P, shape, P.hit_cur, twoway() ? P.dcur : nullptr, nullptr, nullptr, nullptr,
+                                         nullptr, nullptr, upart, H->stream),
+                            "particle u")))
+            return st;
+          PartParams<A> Q = part_params();
+          Q.first = (n_step == 1 && c.resume == 0);
+          for (int sub = 0; sub < (int)c.time_dt_lagr_factor; sub++)
+            if ((st = H->cuda(launch_particle_substep(Q, H->stream), "particle substep"))) return st;
+        }
       }
       if (hit && (st = H->cuda(cudaMemcpyAsync(hit_last, hit_ring + (size_t)m * slot, slot * sizeof(A),
                                                cudaMemcpyDeviceToDevice, H->stream),
@@ -506,7 +712,7 @@ struct Engine : EngineBase {
     if ((st = H->cuda(cudaMalloc(&d, 9 * n1 * sizeof(double)), "fields scratch"))) return st;
     double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *dfo = d + 6 * n1;
     const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
-    st = H->cuda(launch_hydro(P, shape, hit, nullptr, dd, du, nsets_on[1] ? dt : nullptr, nsets_on[2] ? ds : nullptr,
+    st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, dd, du, nsets_on[1] ? dt : nullptr, nsets_on[2] ? ds : nullptr,
                               dfo, nullptr, H->stream),
                  "hydro");
     std::vector<double> hbuf(9 * n1);
@@ -755,6 +961,14 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
   if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
     return why = "walls need NY >= 3", CH4_ERR_ARG;
   if (!(c->tau_u > 0.5)) return why = "tau_u must exceed 0.5", CH4_ERR_ARG;
+  if (c->flags & CH4_F_LAGRANGE) {
+    if (c->flags & (CH4_F_FLUID_BC_Y | CH4_F_LB_TEMPERATURE | CH4_F_LB_SCALAR))
+      return why = "particles are implemented for the periodic fluid-only box", CH4_ERR_UNSUPPORTED;
+    if (!(c->flags & CH4_F_LAGRANGE_WRAP)) return why = "particles need LAGRANGE_WRAP", CH4_ERR_UNSUPPORTED;
+    if ((c->flags & CH4_F_LAGRANGE_TWOWAY) && !(c->flags & CH4_F_LAGRANGE_TWOWAY_MOMENTUM))
+      return why = "LAGRANGE_TWOWAY is implemented with LAGRANGE_TWOWAY_MOMENTUM", CH4_ERR_UNSUPPORTED;
+    if (!(c->time_dt_lagr_factor >= 1.0)) return why = "time_dt_lagr_factor must be >= 1", CH4_ERR_ARG;
+  }
   return CH4_OK;
 }
 
@@ -850,14 +1064,14 @@ ch4_status ch4_get_hit_phases(ch4_handle* h, double* phi) {
   return CH4_OK;
 }
 
-ch4_status ch4_set_particles(ch4_handle* h, const ch4_particle*, int) {
+ch4_status ch4_set_particles(ch4_handle* h, const ch4_particle* parts, int n) {
   if (!h) return CH4_ERR_ARG;
-  return h->fail(CH4_ERR_UNSUPPORTED, "particles are not enabled in this build");
+  return h->eng->set_particles(parts, n);
 }
 
-ch4_status ch4_get_particles(ch4_handle* h, ch4_particle*, int) {
+ch4_status ch4_get_particles(ch4_handle* h, ch4_particle* parts, int n) {
   if (!h) return CH4_ERR_ARG;
-  return h->fail(CH4_ERR_UNSUPPORTED, "particles are not enabled in this build");
+  return h->eng->get_particles(parts, n);
 }
 
 ch4_status ch4_initialize(ch4_handle* h) {
@@ -896,7 +1110,8 @@ ch4_status ch4_get_force(ch4_handle* h, double* force, int brd) {
 
 ch4_status ch4_averages_get(ch4_handle* h, ch4_averages* out) {
   if (!h || !out) return CH4_ERR_ARG;
-  return h->fail(CH4_ERR_UNSUPPORTED, "averages not built yet");
+  static_assert(sizeof(ch4_averages) == NAVG * sizeof(double), "averages layout");
+  return h->eng->averages(out);
 }
 
 ch4_status ch4_get_itime(const ch4_handle* h, int* itime) {

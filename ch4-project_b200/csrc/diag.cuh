@@ -1,0 +1,148 @@
+// Global averages of dump_averages (src/output.c:63-~720) as a deterministic FP64
+// device reduction.  Each per-cell contribution is the reference's expression;
+// the sum runs in double-double (TwoSum error-free transformations) over a fixed
+// cell -> thread -> block assignment and a fixed tree, so the result does not
+// depend on scheduling and is more accurate than the reference's sequential sum.
+#pragma once
+#include <cstdint>
+
+namespace ch4 {
+
+constexpr int NAVG = 23;  // fields of ch4_averages, same order
+constexpr int AVG_BLOCK = 256;
+
+struct AvgParams {
+  int NX, NY, NZ;
+  long long N;
+  const double* dens;  // FP64 planes from the hydro kernel
+  const double* u;     // 3 planes
+  const double* t;     // may be null
+  const double* s;     // may be null
+  int fwall, twall;    // one-sided y gradients for u / for t
+  double nu, kappa;
+  double* partial;     // [gridDim.x][NAVG][2]
+};
+
+#ifdef __CUDACC__
+
+struct DD {
+  double hi, lo;
+};
+
+__device__ __forceinline__ DD dd_add(DD a, double b) {
+  // TwoSum(a.hi, b) then fold the low parts
+  const double s = a.hi + b;
+  const double bb = s - a.hi;
+  const double err = (a.hi - (s - bb)) + (b - bb);
+  const double lo = a.lo + err;
+  const double hi = s + lo;
+  return {hi, lo - (hi - s)};
+}
+
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+  DD r = dd_add(a, b.hi);
+  return dd_add(r, b.lo);
+}
+
+__device__ __forceinline__ double gfield(const AvgParams& P, const double* f, int i, int j, int k, int b, bool walls) {
+  const int NX = P.NX, NY = P.NY, NZ = P.NZ;
+  auto at = [&](int ii, int jj, int kk) { return f[((long long)kk * NY + jj) * NX + ii]; };
+  if (b == 0) return (at(i + 1 == NX ? 0 : i + 1, j, k) - at(i == 0 ? NX - 1 : i - 1, j, k)) / 2.0;
+  if (b == 2) return (at(i, j, k + 1 == NZ ? 0 : k + 1) - at(i, j, k == 0 ? NZ - 1 : k - 1)) / 2.0;
+  if (walls && j == 0) return -1.5 * at(i, 0, k) + 2.0 * at(i, 1, k) + -0.5 * at(i, 2, k);
+  if (walls && j == NY - 1) return 1.5 * at(i, NY - 1, k) + -2.0 * at(i, NY - 2, k) + 0.5 * at(i, NY - 3, k);
+  return (at(i, j + 1 == NY ? 0 : j + 1, k) - at(i, j == 0 ? NY - 1 : j - 1, k)) / 2.0;
+}
+
+// per-cell contributions in ch4_averages order (unit cell volume)
+__device__ __forceinline__ void cell_terms(const AvgParams& P, long long c, double* v) {
+  const int i = (int)(c % P.NX), j = (int)((c / P.NX) % P.NY), k = (int)(c / ((long long)P.NX * P.NY));
+  const long long N = P.N;
+  const double ux = P.u[c], uy = P.u[N + c], uz = P.u[2 * N + c];
+  v[0] = P.dens[c];
+  v[1] = ux;
+  v[2] = uy;
+  v[3] = uz;
+  v[4] = ux * ux;
+  v[5] = uy * uy;
+  v[6] = uz * uz;
+  v[7] = 0.5 * (ux * ux + uy * uy + uz * uz);
+  double g[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) g[a][b] = gfield(P, P.u + a * N, i, j, k, b, P.fwall != 0);
+  const double xx = g[0][0], xy = g[0][1], xz = g[0][2], yx = g[1][0], yy = g[1][1], yz = g[1][2], zx = g[2][0],
+               zy = g[2][1], zz = g[2][2];
+  v[8] = ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) + (yx + xy) * (yx + xy) +
+          (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) + (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) +
+          (zz + zz) * (zz + zz)) *
+         0.5 * P.nu;
+  for (int q = 9; q < NAVG; q++) v[q] = 0.0;
+  if (P.t) {
+    const double t = P.t[c];
+    const double gx = gfield(P, P.t, i, j, k, 0, P.twall != 0), gy = gfield(P, P.t, i, j, k, 1, P.twall != 0),
+                 gz = gfield(P, P.t, i, j, k, 2, P.twall != 0);
+    v[9] = t;
+    v[10] = t * t;
+    v[11] = P.kappa * (gx * gx + gy * gy + gz * gz);
+    v[12] = gx;
+    v[13] = gy;
+    v[14] = gz;
+    v[15] = ux * t;
+    v[16] = uy * t;
+    v[17] = uz * t;
+    v[18] = -P.kappa * gx + ux * t;
+    v[19] = -P.kappa * gy + uy * t;
+    v[20] = -P.kappa * gz + uz * t;
+  }
+  if (P.s) {
+    v[21] = P.s[c];
+    v[22] = P.s[c] * P.s[c];
+  }
+}
+
+// pass 1: every block reduces a fixed contiguous range of cells
+static __global__ void __launch_bounds__(AVG_BLOCK) averages_partial_kernel(const AvgParams P) {
+  __shared__ double sh_hi[AVG_BLOCK], sh_lo[AVG_BLOCK];
+  const long long per_block = (P.N + gridDim.x - 1) / gridDim.x;
+  const long long c0 = (long long)blockIdx.x * per_block;
+  const long long c1 = c0 + per_block < P.N ? c0 + per_block : P.N;
+  DD acc[NAVG];
+  for (int q = 0; q < NAVG; q++) acc[q] = {0.0, 0.0};
+  double v[NAVG];
+  for (long long c = c0 + threadIdx.x; c < c1; c += AVG_BLOCK) {
+    cell_terms(P, c, v);
+    for (int q = 0; q < NAVG; q++) acc[q] = dd_add(acc[q], v[q]);
+  }
+  for (int q = 0; q < NAVG; q++) {
+    sh_hi[threadIdx.x] = acc[q].hi;
+    sh_lo[threadIdx.x] = acc[q].lo;
+    __syncthreads();
+    for (int w = AVG_BLOCK / 2; w > 0; w >>= 1) {
+      if ((int)threadIdx.x < w) {
+        DD a = {sh_hi[threadIdx.x], sh_lo[threadIdx.x]};
+        DD b = {sh_hi[threadIdx.x + w], sh_lo[threadIdx.x + w]};
+        a = dd_add(a, b);
+        sh_hi[threadIdx.x] = a.hi;
+        sh_lo[threadIdx.x] = a.lo;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      P.partial[((long long)blockIdx.x * NAVG + q) * 2] = sh_hi[0];
+      P.partial[((long long)blockIdx.x * NAVG + q) * 2 + 1] = sh_lo[0];
+    }
+    __syncthreads();
+  }
+}
+
+// pass 2: one thread per quantity sums the block partials in block order
+static __global__ void averages_final_kernel(const double* partial, int nblocks, double* out) {
+  const int q = threadIdx.x;
+  if (q >= NAVG) return;
+  DD acc = {0.0, 0.0};
+  for (int b = 0; b < nblocks; b++) acc = dd_add(acc, DD{partial[((long long)b * NAVG + q) * 2], partial[((long long)b * NAVG + q) * 2 + 1]});
+  out[q] = acc.hi + acc.lo;
+}
+
+#endif  // __CUDACC__
+}  // namespace ch4

@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "lattice.cuh"
+#include "particles.cuh"
+#include "diag.cuh"
 
 namespace ch4 {
 
@@ -31,6 +33,19 @@ cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape s, int se
                               int nz, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
                               int nz, cudaStream_t st);
+
+// Lagrangian particles: one sub-step (interpolate + move + wrap)
+cudaError_t launch_particle_substep(const PartParams<double>& P, cudaStream_t st);
+cudaError_t launch_particle_substep(const PartParams<float>& P, cudaStream_t st);
+// two-way deposit into P.dep; `tmp`/`tmp_bytes` is CUB scratch (query with tmp == nullptr),
+// key2/order2 are the sort's output buffers
+cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
+                           cudaStream_t st);
+cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
+                           cudaStream_t st);
+
+// dump_averages sums (FP64, deterministic); out_dev receives NAVG raw sums
+cudaError_t launch_averages(const AvgParams& P, int nblocks, double* out_dev, cudaStream_t st);
 
 // block shape of the fused step kernel
 constexpr int STEP_BLOCK_X = 128;

@@ -1,5 +1,7 @@
 // FP32-arithmetic instantiation of the lattice-Boltzmann kernels with FP32 or
 // FP16-deviation population storage (the reduced-precision forms).
+#include <cub/cub.cuh>
+
 #include "launch.h"
 #include "lb_kernels.cuh"
 #include "lb_launch.inc"
@@ -25,5 +27,10 @@ cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set
                               int nz, cudaStream_t st) {
   return s.storage == 2 ? s2a_t<__half, float>(P, set, soa, aos, z0, nz, st)
                         : s2a_t<float, float>(P, set, soa, aos, z0, nz, st);
+}
+cudaError_t launch_particle_substep(const PartParams<float>& P, cudaStream_t st) { return part_substep_t<float>(P, st); }
+cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
+                           cudaStream_t st) {
+  return deposit_t<float>(P, key2, order2, tmp, tmp_bytes, st);
 }
 }  // namespace ch4

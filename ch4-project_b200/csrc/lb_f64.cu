@@ -1,6 +1,8 @@
 // FP64 instantiation of the lattice-Boltzmann kernels (the drop-in path).
 // Built with -fmad=false: every multiply and add rounds separately, as in the
 // reference's x86-64 build, so results are bit-identical to the reference.
+#include <cub/cub.cuh>
+
 #include "launch.h"
 #include "lb_kernels.cuh"
 #include "lb_launch.inc"
@@ -23,5 +25,17 @@ cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape, int set,
 cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape, int set, const void* soa, double* aos, int z0,
                               int nz, cudaStream_t st) {
   return s2a_t<double, double>(P, set, soa, aos, z0, nz, st);
+}
+cudaError_t launch_averages(const AvgParams& P, int nblocks, double* out_dev, cudaStream_t st) {
+  averages_partial_kernel<<<nblocks, AVG_BLOCK, 0, st>>>(P);
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
+  averages_final_kernel<<<1, 32, 0, st>>>(P.partial, nblocks, out_dev);
+  return cudaGetLastError();
+}
+cudaError_t launch_particle_substep(const PartParams<double>& P, cudaStream_t st) { return part_substep_t<double>(P, st); }
+cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
+                           cudaStream_t st) {
+  return deposit_t<double>(P, key2, order2, tmp, tmp_bytes, st);
 }
 }  // namespace ch4

@@ -1,0 +1,363 @@
+// Lagrangian point particles on the device (periodic box, LAGRANGE_WRAP).
+//
+// State: FP64 structure-of-arrays, one plane per field of ch4_particle (same
+// field order as the C struct) plus two per-particle constants of the deposit.
+// One launch of particle_substep_kernel is one Lagrangian sub-step of the
+// reference (src/main.c:167-183): interpolate_vector_at_particles
+// (src/lagrange.c:1211-1439), move_particles (src/lagrange.c:2934-3470) and the
+// wrap of sendrecv_particles (src/lagrange.c:4028-4221), fused per particle.
+//
+// Two-way momentum deposit (src/lagrange_feedback.c:11-256) as a deterministic
+// gather: particles are stably radix-sorted by their home cell (the lower corner
+// of the trilinear stencil, shifted by +1 so that the halo row -1 is index 0);
+// every lattice cell then merges the (up to 8) home-cell lists around it in
+// particle-index order, which is exactly the order in which the reference's
+// particle loop adds to that cell.  Deposits on halo cells are dropped as in the
+// reference's border fold (src/lagrange_feedback.c:525-835).
+#pragma once
+#include <cstddef>
+
+#include "../../include/ch4.h"
+#include "lattice.cuh"
+
+namespace ch4 {
+
+#define CH4_PF(name) ((int)(offsetof(ch4_particle, name) / sizeof(double)))
+constexpr int PF_FIELDS = (int)(sizeof(ch4_particle) / sizeof(double));
+constexpr int PF_VOL = PF_FIELDS;      // (4/3) pi r^3 with r^2 = 3 nu beta tau_drag
+constexpr int PF_DR = PF_FIELDS + 1;   // rho_p / rho_f = (3 - beta) / (2 beta)
+constexpr int PF_TOTAL = PF_FIELDS + 2;
+
+template <typename A>
+struct PartParams {
+  int NX, NY, NZ;
+  long long N;
+  int np;
+  double SX, SY, SZ, dtl;
+  int first;      // itime == 1 && resume == 0 (src/lagrange.c:3190)
+  int gradient;   // LAGRANGE_GRADIENT
+  int addedmass;  // LAGRANGE_ADDEDMASS
+  double* pf;     // [PF_TOTAL][np]
+  const A* u;     // 3 SoA planes of u^{n+1}
+  // deposit
+  unsigned int* key;     // home cell per particle (sorted in place by the caller)
+  int* order;            // particle index per sorted slot
+  double* rec;           // [9][np] per particle: fac*fp (3), dxm dxp dym dyp dzm dzp
+  int* cell_start;       // [(NX+1)(NY+1)(NZ+1)]
+  int* cell_end;
+  A* dep;                // 3 SoA planes, output
+};
+
+#ifdef __CUDACC__
+
+__device__ __forceinline__ double pwrapd(double x, double S) { return (x) - floor((x) / S) * S; }
+__device__ __forceinline__ int pwrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+template <typename A>
+__device__ __forceinline__ double u_at(const PartParams<A>& P, int a, int i, int j, int k) {
+  const long long c = ((long long)pwrapi(k, P.NZ) * P.NY + pwrapi(j, P.NY)) * P.NX + pwrapi(i, P.NX);
+  return (double)P.u[a * P.N + c];
+}
+
+// d u_a / d x_b on a stencil cell: centred inside, one-sided 2nd order on the
+// first halo layer (LAGRANGE_INTERPOLATION_FIX, src/gradients.c:358-420)
+template <typename A>
+__device__ double grad_at(const PartParams<A>& P, int a, int b, int i, int j, int k) {
+  const int n = b == 0 ? P.NX : b == 1 ? P.NY : P.NZ;
+  const int c = b == 0 ? i : b == 1 ? j : k;
+  const int di = b == 0, dj = b == 1, dk = b == 2;
+  if (c == -1)
+    return -1.5 * u_at(P, a, i, j, k) + 2.0 * u_at(P, a, i + di, j + dj, k + dk) +
+           -0.5 * u_at(P, a, i + 2 * di, j + 2 * dj, k + 2 * dk);
+  if (c == n)
+    return 1.5 * u_at(P, a, i, j, k) + -2.0 * u_at(P, a, i - di, j - dj, k - dk) +
+           0.5 * u_at(P, a, i - 2 * di, j - 2 * dj, k - 2 * dk);
+  return (u_at(P, a, i + di, j + dj, k + dk) - u_at(P, a, i - di, j - dj, k - dk)) / 2.0;
+}
+
+struct Stencil {
+  int im, jm, km;
+  double dxm, dxp, dym, dyp, dzm, dzp;
+  double vol[8];
+};
+
+// cell search of src/lagrange.c:1253-1264 on the unit grid (center_V = index + 0.5)
+__device__ __forceinline__ void make_stencil(double px, double py, double pz, Stencil& t) {
+  t.im = (int)floor(px - 0.5);
+  t.jm = (int)floor(py - 0.5);
+  t.km = (int)floor(pz - 0.5);
+  t.dxm = px - ((double)t.im + 0.5);
+  t.dxp = ((double)(t.im + 1) + 0.5) - px;
+  t.dym = py - ((double)t.jm + 0.5);
+  t.dyp = ((double)(t.jm + 1) + 0.5) - py;
+  t.dzm = pz - ((double)t.km + 0.5);
+  t.dzp = ((double)(t.km + 1) + 0.5) - pz;
+  t.vol[0] = t.dxp * t.dyp * t.dzp;
+  t.vol[1] = t.dxm * t.dyp * t.dzp;
+  t.vol[2] = t.dxp * t.dym * t.dzp;
+  t.vol[3] = t.dxp * t.dyp * t.dzm;
+  t.vol[4] = t.dxm * t.dym * t.dzp;
+  t.vol[5] = t.dxp * t.dym * t.dzm;
+  t.vol[6] = t.dxm * t.dyp * t.dzm;
+  t.vol[7] = t.dxm * t.dym * t.dzm;
+}
+
+// corner order of the reference's trilinear sums, paired with vol[0..7]
+__device__ __forceinline__ void corner(int c, int& di, int& dj, int& dk) {
+  di = (c == 1 || c == 4 || c == 6 || c == 7);
+  dj = (c == 2 || c == 4 || c == 5 || c == 7);
+  dk = (c == 3 || c == 5 || c == 6 || c == 7);
+}
+
+// One Lagrangian sub-step for one particle: interpolate, move, wrap.
+template <typename A>
+__global__ void particle_substep_kernel(const PartParams<A> P) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= P.np) return;
+  double* pf = P.pf;
+  const int np = P.np;
+#define F(name) pf[(long long)CH4_PF(name) * np + ip]
+  // ---- interpolate_vector_at_particles
+  Stencil t;
+  make_stencil(pwrapd(F(x), P.SX), pwrapd(F(y), P.SY), pwrapd(F(z), P.SZ), t);
+  double v[3];
+  for (int a = 0; a < 3; a++) {
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      int di, dj, dk;
+      corner(c, di, dj, dk);
+      const double term = u_at(P, a, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
+      acc = c == 0 ? term : acc + term;
+    }
+    v[a] = acc;
+  }
+  double ux = v[0], uy = v[1], uz = v[2];
+  F(ux) = ux;
+  F(uy) = uy;
+  F(uz) = uz;
+  if (P.gradient) {
+    double gr[9];
+    for (int ab = 0; ab < 9; ab++) {
+      const int a = ab / 3, b = ab % 3;
+      double acc = 0.0;
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        int di, dj, dk;
+        corner(c, di, dj, dk);
+        const double term = grad_at(P, a, b, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
+        acc = c == 0 ? term : acc + term;
+      }
+      gr[ab] = acc;
+    }
+    F(dx_ux) = gr[0];
+    F(dy_ux) = gr[1];
+    F(dz_ux) = gr[2];
+    F(dx_uy) = gr[3];
+    F(dy_uy) = gr[4];
+    F(dz_uy) = gr[5];
+    F(dx_uz) = gr[6];
+    F(dy_uz) = gr[7];
+    F(dz_uz) = gr[8];
+  }
+  // ---- move_particles (src/lagrange.c:3040-3440)
+  const double dtl = P.dtl;
+  const bool first = P.first != 0;
+  const double tau = F(tau_drag);
+  if (tau < 0.0) {  // Eulerian probe
+    F(vx) = ux;
+    F(vy) = uy;
+    F(vz) = uz;
+  }
+  if (tau == 0.0) {  // tracer
+    double vx = ux, vy = uy, vz = uz;
+    double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
+    if (first) {
+      vxo = vx;
+      vyo = vy;
+      vzo = vz;
+    }
+    F(ax) = (vx - vxo) / dtl;
+    F(ay) = (vy - vyo) / dtl;
+    F(az) = (vz - vzo) / dtl;
+    if (first) {
+      F(x) += dtl * vx;
+      F(y) += dtl * vy;
+      F(z) += dtl * vz;
+    } else {
+      F(x) += dtl * 0.5 * (3.0 * vx - vxo);
+      F(y) += dtl * 0.5 * (3.0 * vy - vyo);
+      F(z) += dtl * 0.5 * (3.0 * vz - vzo);
+    }
+    F(vx) = vx;
+    F(vy) = vy;
+    F(vz) = vz;
+    F(vx_old) = vx;
+    F(vy_old) = vy;
+    F(vz_old) = vz;
+    F(ux_old) = ux;
+    F(uy_old) = uy;
+    F(uz_old) = uz;
+  }
+  if (tau > 0.0) {  // Stokes drag (+ added mass)
+    const double invtau = 1.0 / tau;
+    double vx = F(vx), vy = F(vy), vz = F(vz);
+    double ax = (ux - vx) * invtau, ay = (uy - vy) * invtau, az = (uz - vz) * invtau;
+    const double beta = F(beta_coeff);
+    double uxo = F(ux_old), uyo = F(uy_old), uzo = F(uz_old);
+    if (P.addedmass && beta != 0.0) {
+      if (first) {
+        uxo = ux;
+        uyo = uy;
+        uzo = uz;
+      }
+      const double Dx = (ux - uxo) / dtl + (ux - vx) * F(dx_ux) + (uy - vy) * F(dy_ux) + (uz - vz) * F(dz_ux);
+      const double Dy = (uy - uyo) / dtl + (ux - vx) * F(dx_uy) + (uy - vy) * F(dy_uy) + (uz - vz) * F(dz_uy);
+      const double Dz = (uz - uzo) / dtl + (ux - vx) * F(dx_uz) + (uy - vy) * F(dy_uz) + (uz - vz) * F(dz_uz);
+      ax += Dx * beta;
+      ay += Dy * beta;
+      az += Dz * beta;
+      F(Dt_ux) = Dx;
+      F(Dt_uy) = Dy;
+      F(Dt_uz) = Dz;
+    }
+    const double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
+    if (first) {
+      F(x) += dtl * vx;
+      F(y) += dtl * vy;
+      F(z) += dtl * vz;
+    } else {
+      F(x) += dtl * 0.5 * (3.0 * vx - vxo);
+      F(y) += dtl * 0.5 * (3.0 * vy - vyo);
+      F(z) += dtl * 0.5 * (3.0 * vz - vzo);
+    }
+    F(vx_old) = vx;
+    F(vy_old) = vy;
+    F(vz_old) = vz;
+    F(ux_old) = ux;
+    F(uy_old) = uy;
+    F(uz_old) = uz;
+    if (first) {
+      vx += dtl * ax;
+      vy += dtl * ay;
+      vz += dtl * az;
+    } else {
+      vx += dtl * 0.5 * (3.0 * ax - F(ax_old));
+      vy += dtl * 0.5 * (3.0 * ay - F(ay_old));
+      vz += dtl * 0.5 * (3.0 * az - F(az_old));
+    }
+    F(vx) = vx;
+    F(vy) = vy;
+    F(vz) = vz;
+    F(ax) = ax;
+    F(ay) = ay;
+    F(az) = az;
+    F(ax_old) = ax;
+    F(ay_old) = ay;
+    F(az_old) = az;
+  }
+  // ---- LAGRANGE_WRAP of sendrecv_particles
+  F(x) = pwrapd(F(x), P.SX);
+  F(z) = pwrapd(F(z), P.SZ);
+  F(y) = pwrapd(F(y), P.SY);
+#undef F
+}
+
+// Deposit record and home-cell key of every particle (src/lagrange_feedback.c:34-118).
+template <typename A>
+__global__ void deposit_prepare_kernel(const PartParams<A> P) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= P.np) return;
+  const double* pf = P.pf;
+  const int np = P.np;
+#define F(name) pf[(long long)CH4_PF(name) * np + ip]
+  Stencil t;
+  make_stencil(pwrapd(F(x), P.SX), pwrapd(F(y), P.SY), pwrapd(F(z), P.SZ), t);
+  const double fac = pf[(long long)PF_VOL * np + ip], dr = pf[(long long)PF_DR * np + ip];
+  const bool live = (fac > 0.0) && F(beta_coeff) != 0.0;
+  const double gx = 0.0, gy = 0.0, gz = 0.0;
+  double* r = P.rec;
+  r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
+  r[1LL * np + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;
+  r[2LL * np + ip] = live ? fac * (F(Dt_uz) - gz + dr * (gz - F(az))) : 0.0;
+  r[3LL * np + ip] = t.dxm;
+  r[4LL * np + ip] = t.dxp;
+  r[5LL * np + ip] = t.dym;
+  r[6LL * np + ip] = t.dyp;
+  r[7LL * np + ip] = t.dzm;
+  r[8LL * np + ip] = t.dzp;
+  // particles that deposit nothing get a key past the last cell and are never merged
+  const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km + 1);
+  const unsigned int nh = (unsigned)(P.NX + 1) * (unsigned)(P.NY + 1) * (unsigned)(P.NZ + 1);
+  P.key[ip] = live ? (hz * (unsigned)(P.NY + 1) + hy) * (unsigned)(P.NX + 1) + hx : nh;
+  P.order[ip] = ip;
+#undef F
+}
+
+// [start, end) of every home cell in the sorted key array
+static __global__ void cell_range_kernel(const unsigned int* key, int n, unsigned int nh, int* start, int* end) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned int k = key[i];
+  if (k >= nh) return;
+  if (i == 0 || key[i - 1] != k) start[k] = i;
+  if (i == n - 1 || key[i + 1] != k) end[k] = i + 1;
+}
+
+// Gather of the deposit on one interior cell: merge the particles of the 8 home
+// cells in particle-index order and accumulate fac*fp*vol as the reference does.
+template <typename A>
+__global__ void deposit_gather_kernel(const PartParams<A> P) {
+  const long long cidx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (cidx >= P.N) return;
+  const int i = (int)(cidx % P.NX);
+  const int j = (int)((cidx / P.NX) % P.NY);
+  const int k = (int)(cidx / ((long long)P.NX * P.NY));
+  const int HX = P.NX + 1, HY = P.NY + 1;
+  int pos[8], endp[8];
+  int any = 0;
+#pragma unroll
+  for (int h = 0; h < 8; h++) {
+    const int di = h & 1, dj = (h >> 1) & 1, dk = (h >> 2) & 1;
+    // home (i+di, j+dj, k+dk) in shifted coordinates holds particles with im = i+di-1
+    const long long home = ((long long)(k + dk) * HY + (j + dj)) * HX + (i + di);
+    pos[h] = P.cell_start[home];
+    endp[h] = P.cell_end[home];
+    any |= endp[h] > pos[h];
+  }
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (any) {
+    const int np = P.np;
+    for (;;) {
+      int best = -1, bidx = 0x7fffffff;
+#pragma unroll
+      for (int h = 0; h < 8; h++)
+        if (pos[h] < endp[h]) {
+          const int pidx = P.order[pos[h]];
+          if (pidx < bidx) {
+            bidx = pidx;
+            best = h;
+          }
+        }
+      if (best < 0) break;
+      const int slot = pos[best]++;
+      const int di = best & 1, dj = (best >> 1) & 1, dk = (best >> 2) & 1;
+      // this cell is the particle's ip corner when di == 0 (weight dxm), im corner when di == 1 (dxp)
+      const double* r = P.rec;
+      const int s0 = P.order[slot];
+      const double wx = di ? r[4LL * np + s0] : r[3LL * np + s0];
+      const double wy = dj ? r[6LL * np + s0] : r[5LL * np + s0];
+      const double wz = dk ? r[8LL * np + s0] : r[7LL * np + s0];
+      const double vol = wx * wy * wz;
+      acc[0] += r[0LL * np + s0] * vol;
+      acc[1] += r[1LL * np + s0] * vol;
+      acc[2] += r[2LL * np + s0] * vol;
+    }
+  }
+  P.dep[cidx] = (A)acc[0];
+  P.dep[P.N + cidx] = (A)acc[1];
+  P.dep[2 * P.N + cidx] = (A)acc[2];
+}
+
+#endif  // __CUDACC__
+}  // namespace ch4

@@ -981,8 +981,118 @@ int ch4o_get_particles(ch4o_state *s, ch4_particle *parts, int n) {
   return CH4_OK;
 }
 
+/* gradient_vector / gradient_scalar of one field component at an interior cell
+ * (src/gradients.c:78-240, 505-620): centred with periodic halos, one-sided 2nd
+ * order at y walls when `walls` */
+static double grad_field(const ch4o_state *s, const double *f, int ncomp, int a, int b, int i, int j, int k,
+                         int walls) {
+  const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+#define FV(ii, jj, kk) f[cidx(s, (ii), (jj), (kk)) * ncomp + a]
+  if (b == 0) return (FV((i + 1) % NX, j, k) - FV((i + NX - 1) % NX, j, k)) / 2.0;
+  if (b == 2) return (FV(i, j, (k + 1) % NZ) - FV(i, j, (k + NZ - 1) % NZ)) / 2.0;
+  const double h1 = 1.0, h2 = 1.0;
+  if (walls && j == 0) {
+    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
+    return a0 * FV(i, 0, k) + a1 * FV(i, 1, k) + a2 * FV(i, 2, k);
+  }
+  if (walls && j == NY - 1) {
+    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
+    return a0 * FV(i, NY - 1, k) + a1 * FV(i, NY - 2, k) + a2 * FV(i, NY - 3, k);
+  }
+  return (FV(i, (j + 1) % NY, k) - FV(i, (j + NY - 1) % NY, k)) / 2.0;
+#undef FV
+}
+
+/* dump_averages global sums, src/output.c:63-~720, in the reference's loop order
+ * (x outermost, z innermost) with unit cell volume, normalised as src/output.c:498-707 */
 int ch4o_averages_get(ch4o_state *s, ch4_averages *out) {
-  memset(out, 0, sizeof(*out));
-  (void)s;
-  return CH4_ERR_UNSUPPORTED;
+  const ch4_config *c = &s->cfg;
+  const size_t N = s->N;
+  double *dens = (double *)malloc(sizeof(double) * N), *u = (double *)malloc(sizeof(double) * 3 * N);
+  double *t = (double *)calloc(N, sizeof(double)), *sc = (double *)calloc(N, sizeof(double));
+  hydro(s, s->hit_cur, s->dcur, dens, u, t, sc);
+  const int fw = (c->flags & CH4_F_FLUID_BC_Y) != 0;
+  const int tw = (c->flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+  ch4_averages o;
+  memset(&o, 0, sizeof(o));
+  const double vol = 1.0;
+  for (int i = 0; i < s->NX; i++)
+    for (int j = 0; j < s->NY; j++)
+      for (int k = 0; k < s->NZ; k++) {
+        size_t id = cidx(s, i, j, k);
+        double ux = u[3 * id], uy = u[3 * id + 1], uz = u[3 * id + 2];
+        o.ux += ux * vol;
+        o.uy += uy * vol;
+        o.uz += uz * vol;
+        o.ux2 += ux * ux * vol;
+        o.uy2 += uy * uy * vol;
+        o.uz2 += uz * uz * vol;
+        o.rho += dens[id] * vol;
+        o.ene += 0.5 * (ux * ux + uy * uy + uz * uz) * vol;
+        double g[3][3];
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++) g[a][b] = grad_field(s, u, 3, a, b, i, j, k, fw);
+        double xx = g[0][0], xy = g[0][1], xz = g[0][2], yx = g[1][0], yy = g[1][1], yz = g[1][2], zx = g[2][0],
+               zy = g[2][1], zz = g[2][2];
+        o.eps += ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) + (yx + xy) * (yx + xy) +
+                  (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) + (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) +
+                  (zz + zz) * (zz + zz)) *
+                 0.5 * c->nu * vol;
+        if (s->nsets_on[1]) {
+          double gx = grad_field(s, t, 1, 0, 0, i, j, k, tw), gy = grad_field(s, t, 1, 0, 1, i, j, k, tw),
+                 gz = grad_field(s, t, 1, 0, 2, i, j, k, tw);
+          double dxt = gx * vol, dyt = gy * vol, dzt = gz * vol;
+          o.dxt += dxt;
+          o.dyt += dyt;
+          o.dzt += dzt;
+          double uxt = ux * t[id] * vol, uyt = uy * t[id] * vol, uzt = uz * t[id] * vol;
+          o.uxt += uxt;
+          o.uyt += uyt;
+          o.uzt += uzt;
+          o.nux += (-c->kappa * dxt + uxt);
+          o.nuy += (-c->kappa * dyt + uyt);
+          o.nuz += (-c->kappa * dzt + uzt);
+          o.t += t[id] * vol;
+          o.t2 += t[id] * t[id] * vol;
+          o.epst += c->kappa * (gx * gx + gy * gy + gz * gz) * vol;
+        }
+        if (s->nsets_on[2]) {
+          o.s += sc[id] * vol;
+          o.s2 += sc[id] * sc[id] * vol;
+        }
+      }
+  double norm = 1.0 / (c->SX * c->SY * c->SZ);
+  o.ene *= norm;
+  o.rho *= norm;
+  o.ux *= norm;
+  o.uy *= norm;
+  o.uz *= norm;
+  o.ux2 *= norm;
+  o.uy2 *= norm;
+  o.uz2 *= norm;
+  o.eps *= norm;
+  if (s->nsets_on[1]) {
+    o.t *= norm;
+    o.t2 *= norm;
+    o.epst *= norm;
+    o.dxt *= norm;
+    o.dyt *= norm;
+    o.dzt *= norm;
+    o.uxt *= norm;
+    o.uyt *= norm;
+    o.uzt *= norm;
+    o.nux *= norm / (c->kappa * c->deltaT / c->SY);
+    o.nuy *= norm / (c->kappa * c->deltaT / c->SY);
+    o.nuz *= norm / (c->kappa * c->deltaT / c->SY);
+  }
+  if (s->nsets_on[2]) {
+    o.s *= norm;
+    o.s2 *= norm;
+  }
+  *out = o;
+  free(dens);
+  free(u);
+  free(t);
+  free(sc);
+  return CH4_OK;
 }

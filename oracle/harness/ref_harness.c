@@ -339,6 +339,24 @@ int main(int argc, char **argv) {
   double t_stop = MPI_Wtime();
 
   dump_state();
+  /* global averages of dump_averages (src/output.c:63) at the final state */
+  {
+    property.time_dump_diagn = property.time_dt;
+    dump_averages();
+    FILE *fp = fopen("out_avg.txt", "w");
+#define A(name) fprintf(fp, "%s %.17g\n", #name, (double)out_all.name)
+#ifdef LB_FLUID
+    A(rho); A(ux); A(uy); A(uz); A(ux2); A(uy2); A(uz2); A(ene); A(eps);
+#endif
+#ifdef LB_TEMPERATURE
+    A(t); A(t2); A(epst); A(dxt); A(dyt); A(dzt); A(uxt); A(uyt); A(uzt); A(nux); A(nuy); A(nuz);
+#endif
+#ifdef LB_SCALAR
+    A(s); A(s2);
+#endif
+#undef A
+    fclose(fp);
+  }
   {
     FILE *fp = fopen("timing.json", "w");
     double sec = t_stop - t_start;

@@ -174,6 +174,10 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None,
     if lay is not None:
         arr = np.fromfile(os.path.join(tmp, "out_part.bin"), dtype=np.float64).reshape(-1, lay["size"])
         out["part"] = particles_from_ref(arr, lay)
+    avg = os.path.join(tmp, "out_avg.txt")
+    if os.path.exists(avg):
+        with open(avg) as f:
+            out["avg"] = {k: float(v) for k, v in (line.split() for line in f)}
     with open(os.path.join(tmp, "timing.json")) as f:
         out["timing"] = json.load(f)
     return out
@@ -278,6 +282,11 @@ class Restatement:
 
     def set_particles(self, parts):
         self._check(self.lib().ch4o_set_particles(self.h, parts, len(parts)), "set_particles")
+
+    def averages(self):
+        a = abi.Averages()
+        self._check(self.lib().ch4o_averages_get(self.h, C.byref(a)), "averages")
+        return {n: getattr(a, n) for n in abi.AVERAGE_FIELDS}
 
     def get_particles(self, n):
         arr = (abi.Particle * n)()

@@ -102,6 +102,7 @@ def run_restatement(cfg, state, nsteps, phi=None):
         out["part"] = O.particles_as_dict(r.get_particles(len(state["part"])))
     out.update(r.fields())
     out["force"] = r.force()
+    out["avg"] = r.averages()
     if cfg.flags & O.abi.FLAGS["LB_FLUID_FORCING_HIT"]:
         out["phi"] = r.get_hit_phases()
     r.close()

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from lbcases import make_case, run_restatement
+from lbcases import make_case, pop_items, run_restatement
 
 pytestmark = pytest.mark.gpu
 
@@ -21,15 +21,20 @@ import ch4b200  # noqa: E402
 
 def run_gpu(cfg, state, nsteps, phi=None):
     with ch4b200.Simulation(cfg) as sim:
-        for k, v in state.items():
+        for k, v in pop_items(state):
             sim.set_pop(k, v)
+        if "part" in state:
+            sim.set_particles(state["part"])
         if phi is not None:
             sim.set_hit_phases(phi)
         sim.initialize()
         sim.step(nsteps)
-        out = {k: sim.get_pop(k) for k in state}
+        out = {k: sim.get_pop(k) for k, _ in pop_items(state)}
+        if "part" in state:
+            out["part"] = O.particles_as_dict(sim.get_particles(len(state["part"])))
         out.update(sim.fields())
         out["force"] = sim.force()
+        out["avg"] = sim.averages()
         out["itime"] = sim.itime
         out["phi"] = sim.get_hit_phases()
     return out
@@ -40,13 +45,17 @@ def rel_l2(a, b):
 
 
 @pytest.mark.parametrize("name,nsteps", [("kolmogorov", 25), ("rb", 25), ("hit", 20), ("walls2", 25),
-                                          ("scalar", 25), ("les", 25)])
+                                          ("scalar", 25), ("les", 25), ("particles", 12)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):
     _, cfg, state = make_case(name, seed=11)
     ref = run_restatement(cfg, state, nsteps)
     gpu = run_gpu(cfg, state, nsteps)
     assert gpu["itime"] == nsteps
-    for k in state:
+    if "part" in state:
+        for f in ref["part"]:
+            assert np.array_equal(gpu["part"][f], ref["part"][f]), "particle %s: max |d| %g" % (
+                f, np.abs(gpu["part"][f] - ref["part"][f]).max())
+    for k, _ in pop_items(state):
         assert np.array_equal(gpu[k], ref[k]), "%s: max |d| %g" % (k, np.abs(gpu[k] - ref[k]).max())
     for k in ("u", "dens", "force"):
         assert np.array_equal(gpu[k], ref[k]), k
@@ -58,14 +67,17 @@ def test_fp64_bit_identical_to_oracle(name, nsteps):
         assert np.array_equal(gpu["phi"], ref["phi"])
 
 
-@pytest.mark.parametrize("name", ["kolmogorov", "rb", "hit", "walls2", "scalar", "les"])
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "hit", "walls2", "scalar", "les", "particles"])
 def test_fp64_matches_compiled_reference(name):
     flagset, cfg, state = make_case(name, seed=5)
     if not O.ref_available(flagset):
         pytest.skip("reference build missing")
-    ref = O.run_reference(flagset, cfg, 30, state)
+    ref = O.run_reference(flagset, cfg, 30, dict(pop_items(state)), parts=state.get("part"))
     gpu = run_gpu(cfg, state, 30)
-    for k in state:
+    if "part" in ref:
+        for f, v in ref["part"].items():
+            assert np.array_equal(gpu["part"][f], v), "particle " + f
+    for k, _ in pop_items(state):
         assert np.array_equal(gpu[k], ref[k]), k
     assert np.array_equal(gpu["u"], ref["u"])
 
@@ -103,3 +115,26 @@ def test_larger_lattice_bit_identical():
     gpu = run_gpu(cfg, state, 120)
     assert np.array_equal(gpu["p"], ref["p"])
     assert np.array_equal(gpu["g"], ref["g"])
+
+
+def test_particles_fp32_fluid_close_to_fp64():
+    """FP32 lattice arithmetic (FP64 particle state): positions after 30 steps
+    within 1e-9 relative L2 of the FP64 oracle."""
+    _, cfg64, state = make_case("particles", seed=4)
+    _, cfg, _ = make_case("particles", seed=4, storage=1)
+    ref = run_restatement(cfg64, state, 30)
+    gpu = run_gpu(cfg, state, 30)
+    pos = lambda d: np.stack([d["part"][k] for k in ("x", "y", "z")])
+    assert rel_l2(pos(gpu), pos(ref)) < 1e-9
+
+
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "walls2", "scalar", "particles"])
+def test_fp64_averages_match_oracle(name):
+    """Global sums of dump_averages: the device's double-double reduction against the
+    oracle's sequential FP64 sum -- within 1e-12 relative (1e-18 absolute for means
+    that cancel to ~0)."""
+    _, cfg, state = make_case(name, seed=13)
+    ref = run_restatement(cfg, state, 15)
+    gpu = run_gpu(cfg, state, 15)
+    for k, v in ref["avg"].items():
+        assert abs(gpu["avg"][k] - v) <= 1e-12 * abs(v) + 1e-18, "%s: %r vs %r" % (k, gpu["avg"][k], v)

@@ -36,6 +36,9 @@ def test_restatement_matches_compiled_reference(name, nsteps):
     if "part" in ref:
         for f, v in ref["part"].items():
             _assert_same(mine["part"][f], v, "particle field " + f)
+    # global averages of dump_averages, same summation order -> identical
+    for k, v in ref["avg"].items():
+        assert mine["avg"][k] == v, "average %s: %r vs %r" % (k, mine["avg"][k], v)
     _assert_same(mine["u"], ref["u"], "u")
     _assert_same(mine["dens"], ref["dens"], "dens")
     if "t" in ref:
