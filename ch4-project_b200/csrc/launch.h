@@ -5,6 +5,7 @@
 #include "lattice.cuh"
 #include "particles.cuh"
 #include "diag.cuh"
+#include "ensemble.cuh"
 
 namespace ch4 {
 
@@ -46,6 +47,12 @@ cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* 
 
 // dump_averages sums (FP64, deterministic); out_dev receives NAVG raw sums
 cudaError_t launch_averages(const AvgParams& P, int nblocks, double* out_dev, cudaStream_t st);
+
+// one ensemble step over a tile list (FP32 arithmetic, storage 1 = f32, 2 = f16)
+cudaError_t launch_ensemble_step(const StepParams<float>* params, const EnsTile* tiles, int ntiles, int* counter,
+                                 LaunchShape s, int grid, int block, cudaStream_t st);
+// resident CTAs per SM of the ensemble kernel for a block size
+int ensemble_blocks_per_sm(LaunchShape s, int block);
 
 // block shape of the fused step kernel
 constexpr int STEP_BLOCK_X = 128;

@@ -5,6 +5,7 @@
 #include "launch.h"
 #include "lb_kernels.cuh"
 #include "lb_launch.inc"
+#include "ensemble_kernel.cuh"
 
 namespace ch4 {
 cudaError_t launch_step(const StepParams<float>& P, LaunchShape s, cudaStream_t st) {
@@ -32,5 +33,42 @@ cudaError_t launch_particle_substep(const PartParams<float>& P, cudaStream_t st)
 cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
                            cudaStream_t st) {
   return deposit_t<float>(P, key2, order2, tmp, tmp_bytes, st);
+}
+template <typename S, bool T, bool H>
+static cudaError_t ens_t(const StepParams<float>* params, const EnsTile* tiles, int ntiles, int* counter, int grid,
+                         int block, cudaStream_t st) {
+  ensemble_step_kernel<S, float, T, H><<<grid, block, 0, st>>>(params, tiles, ntiles, counter);
+  return cudaGetLastError();
+}
+template <typename S>
+static cudaError_t ens_s(const StepParams<float>* params, const EnsTile* tiles, int ntiles, int* counter,
+                         LaunchShape s, int grid, int block, cudaStream_t st) {
+  if (s.therm && s.scal) return ens_t<S, true, true>(params, tiles, ntiles, counter, grid, block, st);
+  if (s.therm) return ens_t<S, true, false>(params, tiles, ntiles, counter, grid, block, st);
+  if (s.scal) return ens_t<S, false, true>(params, tiles, ntiles, counter, grid, block, st);
+  return ens_t<S, false, false>(params, tiles, ntiles, counter, grid, block, st);
+}
+cudaError_t launch_ensemble_step(const StepParams<float>* params, const EnsTile* tiles, int ntiles, int* counter,
+                                 LaunchShape s, int grid, int block, cudaStream_t st) {
+  return s.storage == 2 ? ens_s<__half>(params, tiles, ntiles, counter, s, grid, block, st)
+                        : ens_s<float>(params, tiles, ntiles, counter, s, grid, block, st);
+}
+template <typename S, bool T, bool H>
+static int occ_t(int block) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ensemble_step_kernel<S, float, T, H>, block, 0);
+  return n;
+}
+int ensemble_blocks_per_sm(LaunchShape s, int block) {
+  if (s.storage == 2) {
+    if (s.therm && s.scal) return occ_t<__half, true, true>(block);
+    if (s.therm) return occ_t<__half, true, false>(block);
+    if (s.scal) return occ_t<__half, false, true>(block);
+    return occ_t<__half, false, false>(block);
+  }
+  if (s.therm && s.scal) return occ_t<float, true, true>(block);
+  if (s.therm) return occ_t<float, true, false>(block);
+  if (s.scal) return occ_t<float, false, true>(block);
+  return occ_t<float, false, false>(block);
 }
 }  // namespace ch4

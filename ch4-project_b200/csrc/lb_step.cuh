@@ -146,13 +146,10 @@ __device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellSt
   }
 }
 
+// The step for one cell (x, y, z) of the lattice described by P.
 template <typename S, typename A, bool THERM, bool SCAL>
-__global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
+__device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, int z) {
   constexpr bool EXACT = sizeof(A) == 8;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  const int z = blockIdx.z;
-  if (x >= P.NX) return;
   const int idx = (z * P.NY + y) * P.NX + x;
   const uint32_t F = P.feat;
   const bool forcing = (F & K_FORCING) != 0;
@@ -231,4 +228,11 @@ __global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
     }
     push_set<S, A, 2>(P, idx, nb, h, (F & K_SWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
   }
+}
+
+template <typename S, typename A, bool THERM, bool SCAL>
+__global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= P.NX) return;
+  lb_cell<S, A, THERM, SCAL>(P, x, blockIdx.y, blockIdx.z);
 }
