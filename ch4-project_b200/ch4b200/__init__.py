@@ -58,6 +58,25 @@ def lib():
         L.ch4_averages_get.argtypes = [P, C.POINTER(Averages)]
         L.ch4_get_itime.argtypes = [P, C.POINTER(C.c_int)]
         L.ch4_get_stream.argtypes = [P, C.POINTER(C.c_void_p)]
+        I = C.POINTER(C.c_int)
+        L.ch4_ensemble_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(P)]
+        L.ch4_ensemble_destroy.argtypes = [P]
+        L.ch4_ensemble_last_error.argtypes = [P]
+        L.ch4_ensemble_last_error.restype = C.c_char_p
+        L.ch4_ensemble_add.argtypes = [P, C.POINTER(Config), I]
+        L.ch4_ensemble_remove.argtypes = [P, C.c_int]
+        L.ch4_ensemble_set_pop.argtypes = [P, C.c_int, C.c_char, D, C.c_int]
+        L.ch4_ensemble_get_pop.argtypes = [P, C.c_int, C.c_char, D, C.c_int]
+        L.ch4_ensemble_initialize.argtypes = [P, C.c_int]
+        L.ch4_ensemble_step.argtypes = [P, C.c_int]
+        L.ch4_ensemble_synchronize.argtypes = [P]
+        L.ch4_ensemble_get_fields.argtypes = [P, C.c_int, D, D, D, D, C.c_int]
+        L.ch4_ensemble_averages.argtypes = [P, C.c_int, C.POINTER(Averages)]
+        L.ch4_ensemble_itime.argtypes = [P, C.c_int, I]
+        L.ch4_ensemble_slot_bytes.argtypes = [C.POINTER(Config), C.c_int, C.POINTER(C.c_size_t)]
+        L.ch4_ensemble_bytes_in_use.argtypes = [P, C.POINTER(C.c_size_t)]
+        L.ch4_ensemble_tune.argtypes = [P, I, I]
+        L.ch4_ensemble_set_shape.argtypes = [P, C.c_int, C.c_int]
         _lib = L
     return _lib
 
@@ -205,3 +224,104 @@ class Simulation:
         v = C.c_int()
         self._check(lib().ch4_get_itime(self.h, C.byref(v)), "get_itime")
         return v.value
+
+
+class Ensemble:
+    """Many independent lattices advanced together (ch4_ensemble_* of include/ch4.h)."""
+
+    def __init__(self, storage=abi.STORE_F32, budget_bytes=0):
+        self.h = C.c_void_p()
+        rc = lib().ch4_ensemble_create(storage, budget_bytes, C.byref(self.h))
+        if rc:
+            raise CH4Error(rc, "ch4_ensemble_create")
+        self.cfgs = {}
+
+    def close(self):
+        if self.h:
+            lib().ch4_ensemble_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc:
+            raise CH4Error(rc, "%s: %s" % (what, lib().ch4_ensemble_last_error(self.h).decode()))
+
+    def add(self, cfg):
+        slot = C.c_int()
+        self._check(lib().ch4_ensemble_add(self.h, C.byref(cfg), C.byref(slot)), "add")
+        self.cfgs[slot.value] = cfg
+        return slot.value
+
+    def remove(self, slot):
+        self._check(lib().ch4_ensemble_remove(self.h, slot), "remove")
+        self.cfgs.pop(slot, None)
+
+    def set_pop(self, slot, which, aos, brd=0):
+        a = np.ascontiguousarray(aos, dtype=np.float64)
+        self._check(lib().ch4_ensemble_set_pop(self.h, slot, which.encode(), _dp(a), brd), "set_pop")
+
+    def get_pop(self, slot, which, brd=0):
+        c = self.cfgs[slot]
+        a = np.empty((c.NZ + 2 * brd, c.NY + 2 * brd, c.NX + 2 * brd, NPOP))
+        self._check(lib().ch4_ensemble_get_pop(self.h, slot, which.encode(), _dp(a), brd), "get_pop")
+        return a
+
+    def initialize(self, slot):
+        self._check(lib().ch4_ensemble_initialize(self.h, slot), "initialize")
+
+    def step(self, n=1):
+        self._check(lib().ch4_ensemble_step(self.h, n), "step")
+
+    def synchronize(self):
+        self._check(lib().ch4_ensemble_synchronize(self.h), "synchronize")
+
+    def fields(self, slot):
+        c = self.cfgs[slot]
+        dens = np.empty((c.NZ, c.NY, c.NX))
+        u = np.empty((c.NZ, c.NY, c.NX, 3))
+        t = np.empty((c.NZ, c.NY, c.NX))
+        s = np.empty((c.NZ, c.NY, c.NX))
+        self._check(lib().ch4_ensemble_get_fields(self.h, slot, _dp(dens), _dp(u), _dp(t), _dp(s), 0), "fields")
+        return {"dens": dens, "u": u, "t": t, "s": s}
+
+    def averages(self, slot):
+        a = Averages()
+        self._check(lib().ch4_ensemble_averages(self.h, slot, C.byref(a)), "averages")
+        return {n: getattr(a, n) for n in abi.AVERAGE_FIELDS}
+
+    def itime(self, slot):
+        v = C.c_int()
+        self._check(lib().ch4_ensemble_itime(self.h, slot, C.byref(v)), "itime")
+        return v.value
+
+    def bytes_in_use(self):
+        v = C.c_size_t()
+        self._check(lib().ch4_ensemble_bytes_in_use(self.h, C.byref(v)), "bytes_in_use")
+        return v.value
+
+    def tune(self):
+        b, r = C.c_int(), C.c_int()
+        self._check(lib().ch4_ensemble_tune(self.h, C.byref(b), C.byref(r)), "tune")
+        return b.value, r.value
+
+    def set_shape(self, block, rows):
+        self._check(lib().ch4_ensemble_set_shape(self.h, block, rows), "set_shape")
+
+
+def ensemble_slot_bytes(cfg, storage):
+    v = C.c_size_t()
+    rc = lib().ch4_ensemble_slot_bytes(C.byref(cfg), storage, C.byref(v))
+    if rc:
+        raise CH4Error(rc, "slot_bytes")
+    return v.value

@@ -151,6 +151,88 @@ struct StorageOf<float> {
   static size_t bytes(int storage) { return storage == CH4_STORE_F16 ? 2 : 4; }
 };
 
+// Parameter block of one lattice from its configuration (host FP64 -> arithmetic type A).
+template <typename A>
+void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, const double* hit_fac, long long N,
+                  const int* nsets_on) {
+  P.NX = c.NX;
+  P.NY = c.NY;
+  P.NZ = c.NZ;
+  P.N = N;
+  uint32_t F = 0;
+  const uint64_t fl = c.flags;
+  if (fl & CH4_F_LB_FLUID_FORCING) {
+    F |= K_FORCING;
+    if (fl & CH4_F_FORCING_KOLMOGOROV) F |= K_KOLMO;
+    if (fl & CH4_F_FORCING_POISEUILLE) F |= K_POIS;
+    if (fl & CH4_F_FORCING_HIT) F |= K_HIT;
+    if (fl & CH4_F_TEMPERATURE_BUOYANCY) F |= K_BUOY;
+    if (fl & CH4_F_SCALAR_BUOYANCY) F |= K_SBUOY;
+    if (c.beta2_t != 0.0) F |= K_BETA2;
+  }
+  if (fl & CH4_F_FLUID_BC_Y) F |= K_FWALL;
+  if (fl & CH4_F_FLUID_BC_Y_P_SLIP) F |= K_FSLIP_P;
+  if (fl & CH4_F_FLUID_BC_Y_M_SLIP) F |= K_FSLIP_M;
+  if (fl & CH4_F_TEMPERATURE_BC_Y) F |= K_TWALL;
+  if (fl & CH4_F_TEMPERATURE_BC_Y_P_FLUX) F |= K_TFLUX_P;
+  if (fl & CH4_F_TEMPERATURE_BC_Y_M_FLUX) F |= K_TFLUX_M;
+  if (fl & CH4_F_TEMPERATURE_BC_Y_P_NOFLUX) F |= K_TNOFLUX_P;
+  if (fl & CH4_F_TEMPERATURE_BC_Y_M_NOFLUX) F |= K_TNOFLUX_M;
+  if (fl & CH4_F_SCALAR_BC_Y) F |= K_SWALL;
+  if (fl & CH4_F_FLUID_LES) F |= K_LES;
+  P.feat = F;
+  for (int q = 0; q < NPOP; q++) P.w[q] = (A)lat.w[q];
+  const double invtau = 1.0 / c.tau_u;
+  const double fac = (1.0 - 0.5 * c.time_dt * invtau);  // src/forcing.c:1289
+  for (int q = 0; q < NPOP; q++) P.facw[q] = (A)(fac * lat.w[q]);
+  P.invcs2 = (A)lat.invcs2;
+  P.invcs4 = (A)lat.invcs4;
+  P.invtwocs2 = (A)lat.invtwocs2;
+  P.invtwocs4 = (A)lat.invtwocs4;
+  P.invtau[0] = (A)invtau;
+  P.invtau[1] = (A)(nsets_on[1] ? 1.0 / c.tau_t : 0.0);
+  P.invtau[2] = (A)(nsets_on[2] ? 1.0 / c.tau_s : 0.0);
+  P.hdt = (A)(0.5 * c.time_dt);
+  P.nu = (A)c.nu;
+  P.csmag2 = (A)std::pow(c.C_smag * 1.0, 2.0);
+  const double LX = c.SX, LY = c.SY, nu = c.nu;
+  P.pois[0] = (A)(2.0 * c.Amp_x * ((4. * nu) * std::pow(LY, -2.0)));
+  P.pois[1] = (A)(2.0 * c.Amp_y * ((4. * nu) * std::pow(LX, -2.0)));
+  P.pois[2] = (A)(2.0 * c.Amp_z * ((4. * nu) * std::pow(LY, -2.0)));
+  for (int ii = 0; ii < NK; ii++) {
+    P.hitamp[ii][0] = (A)(hit_fac[ii] * c.Amp_x);
+    P.hitamp[ii][1] = (A)(hit_fac[ii] * c.Amp_y);
+    P.hitamp[ii][2] = (A)(hit_fac[ii] * c.Amp_z);
+  }
+  double T0;
+  switch (c.t0_kind) {
+    case CH4_T0_REF: T0 = c.T_ref; break;
+    case CH4_T0_TOP: T0 = c.T_top; break;
+    case CH4_T0_BOT: T0 = c.T_bot; break;
+    default: T0 = 0.5 * (c.T_bot + c.T_top);
+  }
+  P.T0 = (A)T0;
+  P.beta_t = (A)c.beta_t;
+  P.beta2_t = (A)c.beta2_t;
+  P.S0 = (A)(0.5 * (c.S_bot + c.S_top));
+  P.beta_s = (A)c.beta_s;
+  P.grav[0] = (A)c.gravity_x;
+  P.grav[1] = (A)c.gravity_y;
+  P.grav[2] = (A)c.gravity_z;
+  P.T_top = (A)c.T_top;
+  P.T_bot = (A)c.T_bot;
+  P.T_ref = (A)c.T_ref;
+  P.grad_T_top = (A)c.grad_T_top;
+  P.grad_T_bot = (A)c.grad_T_bot;
+  P.S_top = (A)c.S_top;
+  P.S_bot = (A)c.S_bot;
+  P.S_ref = (A)c.S_ref;
+  // F16 storage shifts: rho0 = 1 for p, the buoyancy reference for g, S0 for h
+  P.shift[0] = 1.0f;
+  P.shift[1] = (float)T0;
+  P.shift[2] = (float)(0.5 * (c.S_bot + c.S_top));
+}
+
 template <typename A>
 struct Engine : EngineBase {
   ch4_handle* H;
@@ -452,83 +534,7 @@ struct Engine : EngineBase {
   }
 
   void fill_params() {
-    const Lattice& lat = H->lat;
-    P.NX = c.NX;
-    P.NY = c.NY;
-    P.NZ = c.NZ;
-    P.N = N;
-    uint32_t F = 0;
-    const uint64_t fl = c.flags;
-    if (fl & CH4_F_LB_FLUID_FORCING) {
-      F |= K_FORCING;
-      if (fl & CH4_F_FORCING_KOLMOGOROV) F |= K_KOLMO;
-      if (fl & CH4_F_FORCING_POISEUILLE) F |= K_POIS;
-      if (fl & CH4_F_FORCING_HIT) F |= K_HIT;
-      if (fl & CH4_F_TEMPERATURE_BUOYANCY) F |= K_BUOY;
-      if (fl & CH4_F_SCALAR_BUOYANCY) F |= K_SBUOY;
-      if (c.beta2_t != 0.0) F |= K_BETA2;
-    }
-    if (fl & CH4_F_FLUID_BC_Y) F |= K_FWALL;
-    if (fl & CH4_F_FLUID_BC_Y_P_SLIP) F |= K_FSLIP_P;
-    if (fl & CH4_F_FLUID_BC_Y_M_SLIP) F |= K_FSLIP_M;
-    if (fl & CH4_F_TEMPERATURE_BC_Y) F |= K_TWALL;
-    if (fl & CH4_F_TEMPERATURE_BC_Y_P_FLUX) F |= K_TFLUX_P;
-    if (fl & CH4_F_TEMPERATURE_BC_Y_M_FLUX) F |= K_TFLUX_M;
-    if (fl & CH4_F_TEMPERATURE_BC_Y_P_NOFLUX) F |= K_TNOFLUX_P;
-    if (fl & CH4_F_TEMPERATURE_BC_Y_M_NOFLUX) F |= K_TNOFLUX_M;
-    if (fl & CH4_F_SCALAR_BC_Y) F |= K_SWALL;
-    if (fl & CH4_F_FLUID_LES) F |= K_LES;
-    P.feat = F;
-    for (int q = 0; q < NPOP; q++) P.w[q] = (A)lat.w[q];
-    const double invtau = 1.0 / c.tau_u;
-    const double fac = (1.0 - 0.5 * c.time_dt * invtau);  // src/forcing.c:1289
-    for (int q = 0; q < NPOP; q++) P.facw[q] = (A)(fac * lat.w[q]);
-    P.invcs2 = (A)lat.invcs2;
-    P.invcs4 = (A)lat.invcs4;
-    P.invtwocs2 = (A)lat.invtwocs2;
-    P.invtwocs4 = (A)lat.invtwocs4;
-    P.invtau[0] = (A)invtau;
-    P.invtau[1] = (A)(nsets_on[1] ? 1.0 / c.tau_t : 0.0);
-    P.invtau[2] = (A)(nsets_on[2] ? 1.0 / c.tau_s : 0.0);
-    P.hdt = (A)(0.5 * c.time_dt);
-    P.nu = (A)c.nu;
-    P.csmag2 = (A)std::pow(c.C_smag * 1.0, 2.0);
-    const double LX = c.SX, LY = c.SY, nu = c.nu;
-    P.pois[0] = (A)(2.0 * c.Amp_x * ((4. * nu) * std::pow(LY, -2.0)));
-    P.pois[1] = (A)(2.0 * c.Amp_y * ((4. * nu) * std::pow(LX, -2.0)));
-    P.pois[2] = (A)(2.0 * c.Amp_z * ((4. * nu) * std::pow(LY, -2.0)));
-    for (int ii = 0; ii < NK; ii++) {
-      P.hitamp[ii][0] = (A)(H->hit_fac[ii] * c.Amp_x);
-      P.hitamp[ii][1] = (A)(H->hit_fac[ii] * c.Amp_y);
-      P.hitamp[ii][2] = (A)(H->hit_fac[ii] * c.Amp_z);
-    }
-    double T0;
-    switch (c.t0_kind) {
-      case CH4_T0_REF: T0 = c.T_ref; break;
-      case CH4_T0_TOP: T0 = c.T_top; break;
-      case CH4_T0_BOT: T0 = c.T_bot; break;
-      default: T0 = 0.5 * (c.T_bot + c.T_top);
-    }
-    P.T0 = (A)T0;
-    P.beta_t = (A)c.beta_t;
-    P.beta2_t = (A)c.beta2_t;
-    P.S0 = (A)(0.5 * (c.S_bot + c.S_top));
-    P.beta_s = (A)c.beta_s;
-    P.grav[0] = (A)c.gravity_x;
-    P.grav[1] = (A)c.gravity_y;
-    P.grav[2] = (A)c.gravity_z;
-    P.T_top = (A)c.T_top;
-    P.T_bot = (A)c.T_bot;
-    P.T_ref = (A)c.T_ref;
-    P.grad_T_top = (A)c.grad_T_top;
-    P.grad_T_bot = (A)c.grad_T_bot;
-    P.S_top = (A)c.S_top;
-    P.S_bot = (A)c.S_bot;
-    P.S_ref = (A)c.S_ref;
-    // F16 storage shifts: rho0 = 1 for p, the buoyancy reference for g, S0 for h
-    P.shift[0] = 1.0f;
-    P.shift[1] = (float)T0;
-    P.shift[2] = (float)(0.5 * (c.S_bot + c.S_top));
+    build_params<A>(P, c, H->lat, H->hit_fac, N, nsets_on);
     P.tprev = tprev;
     P.sprev = sprev;
     P.ules = ules;
@@ -1117,6 +1123,605 @@ ch4_status ch4_averages_get(ch4_handle* h, ch4_averages* out) {
 ch4_status ch4_get_itime(const ch4_handle* h, int* itime) {
   if (!h || !itime) return CH4_ERR_ARG;
   *itime = h->itime;
+  return CH4_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched ensemble: many independent lattices advanced by one persistent
+// work-queue launch per step (ensemble_kernel.cuh), K steps per CUDA graph.
+
+namespace {
+
+struct Slot {
+  bool used = false, initialized = false;
+  ch4_config cfg{};
+  long long N = 0;
+  int nsets_on[3] = {1, 0, 0};
+  void* f[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+  float *tprev = nullptr, *sprev = nullptr;
+  float* kol = nullptr;
+  int cur = 0;
+  int itime = 0;
+  size_t bytes = 0;
+  StepParams<float> P{};  // constants; population pointers are set per parity
+};
+
+size_t slot_bytes(const ch4_config& c, int storage) {
+  const size_t N = (size_t)c.NX * c.NY * c.NZ;
+  const size_t sb = storage == CH4_STORE_F16 ? 2 : 4;
+  int sets = 1 + ((c.flags & CH4_F_LB_TEMPERATURE) != 0) + ((c.flags & CH4_F_LB_SCALAR) != 0);
+  size_t b = (size_t)sets * 2 * NPOP * N * sb;
+  if (c.flags & CH4_F_LB_TEMPERATURE) b += N * 4;
+  if (c.flags & CH4_F_LB_SCALAR) b += N * 4;
+  b += (size_t)(2 * c.NY + c.NX) * 4;
+  return b;
+}
+
+// AoS FP64 (halo width brd) <-> SoA device storage of one set, through a temporary staging buffer
+ch4_status move_pop(const StepParams<float>& P, LaunchShape shape, int set, void* soa, double* host, int brd, bool up,
+                    cudaStream_t st, std::string& err) {
+  const int NX = P.NX, NY = P.NY, NZ = P.NZ;
+  const size_t row = (size_t)NX * NPOP, plane = row * NY;
+  const int nzc = (int)std::max<size_t>(1, std::min<size_t>((size_t)NZ, (32u << 20) / (plane * sizeof(double))));
+  double* dstage = nullptr;
+  std::vector<double> hstage(plane * nzc);
+  auto fail = [&](const char* what, cudaError_t e) {
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    if (dstage) cudaFree(dstage);
+    return CH4_ERR_CUDA;
+  };
+  cudaError_t e = cudaMalloc(&dstage, plane * nzc * sizeof(double));
+  if (e) return fail("staging", e);
+  const size_t PX = NX + 2 * brd, PY = NY + 2 * brd;
+  for (int z0 = 0; z0 < NZ; z0 += nzc) {
+    const int nz = std::min(nzc, NZ - z0);
+    if (up) {
+      for (int zl = 0; zl < nz; zl++)
+        for (int y = 0; y < NY; y++)
+          std::memcpy(hstage.data() + ((size_t)zl * NY + y) * row,
+                      host + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, row * sizeof(double));
+      if ((e = cudaMemcpyAsync(dstage, hstage.data(), plane * nz * sizeof(double), cudaMemcpyHostToDevice, st)))
+        return fail("upload", e);
+      if ((e = launch_aos_to_soa(P, shape, set, dstage, soa, z0, nz, st))) return fail("aos_to_soa", e);
+      if ((e = cudaStreamSynchronize(st))) return fail("upload sync", e);
+    } else {
+      if ((e = launch_soa_to_aos(P, shape, set, soa, dstage, z0, nz, st))) return fail("soa_to_aos", e);
+      if ((e = cudaMemcpyAsync(hstage.data(), dstage, plane * nz * sizeof(double), cudaMemcpyDeviceToHost, st)))
+        return fail("download", e);
+      if ((e = cudaStreamSynchronize(st))) return fail("download sync", e);
+      for (int zl = 0; zl < nz; zl++)
+        for (int y = 0; y < NY; y++)
+          std::memcpy(host + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
+                      hstage.data() + ((size_t)zl * NY + y) * row, row * sizeof(double));
+    }
+  }
+  cudaFree(dstage);
+  return CH4_OK;
+}
+
+}  // namespace
+
+struct ch4_ensemble {
+  int storage = CH4_STORE_F32;
+  size_t budget = 0, used = 0;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  Lattice lat;
+  double hit_fac[NK] = {0, 0, 0, 0, 0, 0};
+  std::vector<Slot> slots;
+  LaunchShape shape{};
+  bool shape_known = false;
+  int block = 256, rows = 2, num_sms = 148;
+  StepParams<float>* d_params[2] = {nullptr, nullptr};
+  int params_cap = 0;
+  EnsTile* d_tiles = nullptr;
+  int tiles_cap = 0, ntiles = 0;
+  int* d_counter = nullptr;
+  static constexpr int KMAX = 100;
+  bool dirty = true;
+  cudaGraphExec_t gexec = nullptr;
+  int g_len = 0;
+
+  ch4_status fail(ch4_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return s;
+  }
+  ch4_status cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return CH4_OK;
+    return fail(CH4_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  }
+  int grid() const {
+    int per = ensemble_blocks_per_sm(shape, block);
+    return std::max(1, per) * num_sms;
+  }
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+    g_len = 0;
+  }
+  StepParams<float> params_of(const Slot& s, int parity) const {
+    StepParams<float> P = s.P;
+    const int in = s.cur ^ parity;
+    for (int k = 0; k < 3; k++) {
+      P.fin[k] = s.f[k][in];
+      P.fout[k] = s.f[k][in ^ 1];
+    }
+    return P;
+  }
+};
+
+namespace {
+
+// tile list (largest first) and both parity parameter arrays of the active slots
+ch4_status ens_rebuild(ch4_ensemble* E) {
+  std::vector<EnsTile> tiles;
+  for (int i = 0; i < (int)E->slots.size(); i++) {
+    const Slot& s = E->slots[i];
+    if (!s.used || !s.initialized) continue;
+    for (int y0 = 0; y0 < s.cfg.NY; y0 += E->rows) tiles.push_back({i, y0, std::min(E->rows, s.cfg.NY - y0), 0});
+  }
+  std::stable_sort(tiles.begin(), tiles.end(), [&](const EnsTile& a, const EnsTile& b) {
+    const Slot &sa = E->slots[a.slot], &sb = E->slots[b.slot];
+    return (long long)sa.cfg.NX * a.ny * sa.cfg.NZ > (long long)sb.cfg.NX * b.ny * sb.cfg.NZ;
+  });
+  ch4_status st;
+  if ((int)tiles.size() > E->tiles_cap) {
+    cudaFree(E->d_tiles);
+    E->tiles_cap = (int)tiles.size() * 2 + 16;
+    if ((st = E->cuda(cudaMalloc(&E->d_tiles, sizeof(EnsTile) * E->tiles_cap), "tiles"))) return st;
+  }
+  E->ntiles = (int)tiles.size();
+  if (E->ntiles &&
+      (st = E->cuda(cudaMemcpyAsync(E->d_tiles, tiles.data(), sizeof(EnsTile) * tiles.size(), cudaMemcpyHostToDevice,
+                                    E->stream),
+                    "tiles up")))
+    return st;
+  if ((int)E->slots.size() > E->params_cap) {
+    cudaFree(E->d_params[0]);
+    cudaFree(E->d_params[1]);
+    E->params_cap = (int)E->slots.size() * 2 + 16;
+    for (int p = 0; p < 2; p++)
+      if ((st = E->cuda(cudaMalloc(&E->d_params[p], sizeof(StepParams<float>) * E->params_cap), "params"))) return st;
+  }
+  for (int p = 0; p < 2; p++) {
+    std::vector<StepParams<float>> h(E->slots.size());
+    for (size_t i = 0; i < E->slots.size(); i++)
+      if (E->slots[i].used) h[i] = E->params_of(E->slots[i], p);
+    if (!h.empty() && (st = E->cuda(cudaMemcpyAsync(E->d_params[p], h.data(), sizeof(StepParams<float>) * h.size(),
+                                                    cudaMemcpyHostToDevice, E->stream),
+                                    "params up")))
+      return st;
+  }
+  if ((st = E->cuda(cudaStreamSynchronize(E->stream), "rebuild sync"))) return st;
+  E->dirty = false;
+  return CH4_OK;
+}
+
+ch4_status ens_graph(ch4_ensemble* E, int K) {
+  if (E->gexec && E->g_len == K) return CH4_OK;
+  E->drop_graph();
+  ch4_status st;
+  cudaGraph_t g = nullptr;
+  if ((st = E->cuda(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal), "capture"))) return st;
+  cudaError_t e = cudaMemsetAsync(E->d_counter, 0, sizeof(int) * K, E->stream);
+  const int grid = E->grid();
+  for (int k = 0; k < K && e == cudaSuccess; k++)
+    e = launch_ensemble_step(E->d_params[k & 1], E->d_tiles, E->ntiles, E->d_counter + k, E->shape, grid, E->block,
+                             E->stream);
+  cudaError_t e2 = cudaStreamEndCapture(E->stream, &g);
+  if (e) return E->cuda(e, "capture launch");
+  if ((st = E->cuda(e2, "end capture"))) return st;
+  e = cudaGraphInstantiate(&E->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if ((st = E->cuda(e, "instantiate"))) return st;
+  E->g_len = K;
+  return CH4_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ch4_status ch4_ensemble_slot_bytes(const ch4_config* cfg, int storage, size_t* bytes) {
+  if (!cfg || !bytes) return CH4_ERR_ARG;
+  *bytes = slot_bytes(*cfg, storage);
+  return CH4_OK;
+}
+
+ch4_status ch4_ensemble_create(int storage, size_t budget, ch4_ensemble** out) {
+  if (!out || (storage != CH4_STORE_F32 && storage != CH4_STORE_F16)) return CH4_ERR_ARG;
+  *out = nullptr;
+  auto* E = new ch4_ensemble();
+  E->storage = storage;
+  int dev = 0;
+  cudaDeviceProp prop{};
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    delete E;
+    return CH4_ERR_CUDA;
+  }
+  E->num_sms = prop.multiProcessorCount;
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  E->budget = budget ? budget : (size_t)(0.9 * (double)fr);
+  if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&E->d_counter, sizeof(int) * ch4_ensemble::KMAX) != cudaSuccess) {
+    delete E;
+    return CH4_ERR_CUDA;
+  }
+  *out = E;
+  return CH4_OK;
+}
+
+static void free_slot(Slot& s) {
+  for (auto& a : s.f)
+    for (auto& b : a) {
+      cudaFree(b);
+      b = nullptr;
+    }
+  cudaFree(s.tprev);
+  cudaFree(s.sprev);
+  cudaFree(s.kol);
+  s.tprev = s.sprev = s.kol = nullptr;
+  s.used = s.initialized = false;
+}
+
+ch4_status ch4_ensemble_destroy(ch4_ensemble* E) {
+  if (!E) return CH4_OK;
+  cudaStreamSynchronize(E->stream);
+  E->drop_graph();
+  for (auto& s : E->slots) free_slot(s);
+  cudaFree(E->d_params[0]);
+  cudaFree(E->d_params[1]);
+  cudaFree(E->d_tiles);
+  cudaFree(E->d_counter);
+  cudaStreamDestroy(E->stream);
+  delete E;
+  return CH4_OK;
+}
+
+const char* ch4_ensemble_last_error(const ch4_ensemble* E) { return E ? E->err.c_str() : "null ensemble"; }
+
+ch4_status ch4_ensemble_add(ch4_ensemble* E, const ch4_config* cfg, int* slot) {
+  if (!E || !cfg || !slot) return CH4_ERR_ARG;
+  std::string why;
+  ch4_status st = validate(cfg, why);
+  if (st) return E->fail(st, "%s", why.c_str());
+  if (cfg->flags & (CH4_F_FORCING_HIT | CH4_F_FLUID_LES | CH4_F_LAGRANGE))
+    return E->fail(CH4_ERR_UNSUPPORTED, "ensemble slots run without HIT forcing, LES or particles");
+  LaunchShape sh{(cfg->flags & CH4_F_LB_TEMPERATURE) != 0, (cfg->flags & CH4_F_LB_SCALAR) != 0, E->storage};
+  bool any = false;
+  for (auto& s : E->slots) any |= s.used;
+  if (any && (sh.therm != E->shape.therm || sh.scal != E->shape.scal))
+    return E->fail(CH4_ERR_ARG, "every slot of an ensemble must have the same population sets");
+  const size_t need = slot_bytes(*cfg, E->storage);
+  if (E->used + need > E->budget)
+    return E->fail(CH4_ERR_NOMEM, "slot needs %zu bytes, %zu of %zu in use", need, E->used, E->budget);
+  int id = -1;
+  for (int i = 0; i < (int)E->slots.size(); i++)
+    if (!E->slots[i].used) {
+      id = i;
+      break;
+    }
+  if (id < 0) {
+    id = (int)E->slots.size();
+    E->slots.emplace_back();
+  }
+  Slot& s = E->slots[id];
+  s = Slot{};
+  s.cfg = *cfg;
+  s.cfg.storage = E->storage;
+  s.N = (long long)cfg->NX * cfg->NY * cfg->NZ;
+  s.nsets_on[1] = sh.therm;
+  s.nsets_on[2] = sh.scal;
+  const size_t sb = E->storage == CH4_STORE_F16 ? 2 : 4;
+  bool ok = true;
+  for (int k = 0; k < 3 && ok; k++)
+    if (s.nsets_on[k])
+      for (int b = 0; b < 2 && ok; b++) ok = cudaMalloc(&s.f[k][b], (size_t)NPOP * s.N * sb) == cudaSuccess;
+  if (ok && sh.therm) ok = cudaMalloc(&s.tprev, s.N * sizeof(float)) == cudaSuccess;
+  if (ok && sh.scal) ok = cudaMalloc(&s.sprev, s.N * sizeof(float)) == cudaSuccess;
+  const int nk = 2 * cfg->NY + cfg->NX;
+  if (ok) ok = cudaMalloc(&s.kol, nk * sizeof(float)) == cudaSuccess;
+  if (!ok) {
+    free_slot(s);
+    return E->fail(CH4_ERR_NOMEM, "device allocation of slot %d failed", id);
+  }
+  s.used = true;
+  s.bytes = need;
+  E->used += need;
+  E->shape = sh;
+  build_params<float>(s.P, s.cfg, E->lat, E->hit_fac, s.N, s.nsets_on);
+  s.P.tprev = s.tprev;
+  s.P.sprev = s.sprev;
+  s.P.kol = s.kol;
+  s.P.ules = nullptr;
+  s.P.tau_les = nullptr;
+  s.P.hit_prev = s.P.hit_cur = nullptr;
+  s.P.dcur = s.P.dprev = nullptr;
+  {  // Kolmogorov tables (src/forcing.c:390-400)
+    std::vector<float> t(nk);
+    const double LX = cfg->SX, LY = cfg->SY, nu = cfg->nu, kn = 1.0;
+    double fnx = nu * std::pow(2 * 3.14159265359 / LX, 2.0), fny = nu * std::pow(2 * 3.14159265359 / LY, 2.0);
+    for (int j = 0; j < cfg->NY; j++) {
+      double y = (double)j + 0.5;
+      t[j] = (float)(cfg->Amp_x * fny * std::sin(kn * 2 * 3.14159265359 * y / LY));
+      t[cfg->NY + cfg->NX + j] = (float)(cfg->Amp_z * fny * std::sin(kn * 2 * 3.14159265359 * y / LY));
+    }
+    for (int i = 0; i < cfg->NX; i++)
+      t[cfg->NY + i] = (float)(cfg->Amp_y * fnx * std::sin(kn * 2 * 3.14159265359 * ((double)i + 0.5) / LX));
+    if ((st = E->cuda(cudaMemcpy(s.kol, t.data(), nk * sizeof(float), cudaMemcpyHostToDevice), "kol"))) return st;
+  }
+  // rest state p = w, g = h = 0
+  std::vector<double> rest((size_t)s.N * NPOP);
+  for (size_t i = 0; i < rest.size(); i++) rest[i] = E->lat.w[i % NPOP];
+  StepParams<float> P = E->params_of(s, 0);
+  if ((st = move_pop(P, E->shape, 0, s.f[0][s.cur], rest.data(), 0, true, E->stream, E->err))) return st;
+  std::fill(rest.begin(), rest.end(), 0.0);
+  for (int k = 1; k < 3; k++)
+    if (s.nsets_on[k] && (st = move_pop(P, E->shape, k, s.f[k][s.cur], rest.data(), 0, true, E->stream, E->err)))
+      return st;
+  *slot = id;
+  E->dirty = true;
+  E->drop_graph();
+  return CH4_OK;
+}
+
+static Slot* ens_slot(ch4_ensemble* E, int slot) {
+  if (!E || slot < 0 || slot >= (int)E->slots.size() || !E->slots[slot].used) return nullptr;
+  return &E->slots[slot];
+}
+
+ch4_status ch4_ensemble_remove(ch4_ensemble* E, int slot) {
+  Slot* s = ens_slot(E, slot);
+  if (!s) return CH4_ERR_ARG;
+  cudaStreamSynchronize(E->stream);
+  E->used -= s->bytes;
+  free_slot(*s);
+  E->dirty = true;
+  E->drop_graph();
+  return CH4_OK;
+}
+
+ch4_status ch4_ensemble_set_pop(ch4_ensemble* E, int slot, char which, const double* aos, int brd) {
+  Slot* s = ens_slot(E, slot);
+  int set = set_of(which);
+  if (!s || set < 0 || !s->nsets_on[set] || !aos || brd < 0) return CH4_ERR_ARG;
+  cudaStreamSynchronize(E->stream);
+  s->initialized = false;
+  E->dirty = true;
+  E->drop_graph();
+  return move_pop(E->params_of(*s, 0), E->shape, set, s->f[set][s->cur], const_cast<double*>(aos), brd, true,
+                  E->stream, E->err);
+}
+
+ch4_status ch4_ensemble_get_pop(ch4_ensemble* E, int slot, char which, double* aos, int brd) {
+  Slot* s = ens_slot(E, slot);
+  int set = set_of(which);
+  if (!s || set < 0 || !s->nsets_on[set] || !aos || brd < 0) return CH4_ERR_ARG;
+  cudaStreamSynchronize(E->stream);
+  return move_pop(E->params_of(*s, 0), E->shape, set, s->f[set][s->cur], aos, brd, false, E->stream, E->err);
+}
+
+ch4_status ch4_ensemble_initialize(ch4_ensemble* E, int slot) {
+  Slot* s = ens_slot(E, slot);
+  if (!s) return CH4_ERR_ARG;
+  ch4_status st;
+  if (s->nsets_on[1] || s->nsets_on[2])
+    if ((st = E->cuda(launch_init_prev(E->params_of(*s, 0), E->shape, E->stream), "init_prev"))) return st;
+  if ((st = E->cuda(cudaStreamSynchronize(E->stream), "initialize"))) return st;
+  s->initialized = true;
+  E->dirty = true;
+  E->drop_graph();
+  return CH4_OK;
+}
+
+ch4_status ch4_ensemble_step(ch4_ensemble* E, int nsteps) {
+  if (!E || nsteps < 0) return CH4_ERR_ARG;
+  ch4_status st;
+  if (E->dirty) {
+    E->drop_graph();
+    if ((st = ens_rebuild(E))) return st;
+  }
+  if (E->ntiles == 0) return CH4_OK;
+  while (nsteps > 0) {
+    const int K = std::min(nsteps, (int)ch4_ensemble::KMAX);
+    if ((st = ens_graph(E, K))) return st;
+    if ((st = E->cuda(cudaGraphLaunch(E->gexec, E->stream), "graph launch"))) return st;
+    for (auto& s : E->slots)
+      if (s.used && s.initialized) {
+        s.itime += K;
+        s.cur ^= (K & 1);
+      }
+    if (K & 1) {  // every slot changed parity: refresh the parameter arrays the graph reads
+      if ((st = ens_rebuild(E))) return st;
+    }
+    nsteps -= K;
+  }
+  return CH4_OK;
+}
+
+ch4_status ch4_ensemble_synchronize(ch4_ensemble* E) {
+  if (!E) return CH4_ERR_ARG;
+  return E->cuda(cudaStreamSynchronize(E->stream), "synchronize");
+}
+
+ch4_status ch4_ensemble_itime(const ch4_ensemble* E, int slot, int* itime) {
+  if (!E || !itime || slot < 0 || slot >= (int)E->slots.size() || !E->slots[slot].used) return CH4_ERR_ARG;
+  *itime = E->slots[slot].itime;
+  return CH4_OK;
+}
+
+ch4_status ch4_ensemble_bytes_in_use(const ch4_ensemble* E, size_t* bytes) {
+  if (!E || !bytes) return CH4_ERR_ARG;
+  *bytes = E->used;
+  return CH4_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+ch4_status ch4_ensemble_get_fields(ch4_ensemble* E, int slot, double* dens, double* u, double* t, double* sc,
+                                   int brd) {
+  Slot* s = ens_slot(E, slot);
+  if (!s || brd < 0) return CH4_ERR_ARG;
+  const size_t n1 = (size_t)s->N;
+  double* d = nullptr;
+  ch4_status st;
+  if ((st = E->cuda(cudaMalloc(&d, 6 * n1 * sizeof(double)), "fields scratch"))) return st;
+  st = E->cuda(launch_hydro(E->params_of(*s, 0), E->shape, nullptr, nullptr, d, d + n1, s->nsets_on[1] ? d + 4 * n1 : nullptr,
+                            s->nsets_on[2] ? d + 5 * n1 : nullptr, nullptr, nullptr, E->stream),
+               "hydro");
+  std::vector<double> h(6 * n1, 0.0);
+  if (!st) st = E->cuda(cudaMemcpyAsync(h.data(), d, 6 * n1 * sizeof(double), cudaMemcpyDeviceToHost, E->stream), "down");
+  if (!st) st = E->cuda(cudaStreamSynchronize(E->stream), "sync");
+  cudaFree(d);
+  if (st) return st;
+  const ch4_config& c = s->cfg;
+  const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
+  for (int z = 0; z < c.NZ; z++)
+    for (int y = 0; y < c.NY; y++)
+      for (int x = 0; x < c.NX; x++) {
+        size_t i = ((size_t)z * c.NY + y) * c.NX + x, o = ((size_t)(z + brd) * PY + (y + brd)) * PX + (x + brd);
+        if (dens) dens[o] = h[i];
+        if (u)
+          for (int a = 0; a < 3; a++) u[3 * o + a] = h[(1 + a) * n1 + i];
+        if (t) t[o] = h[4 * n1 + i];
+        if (sc) sc[o] = h[5 * n1 + i];
+      }
+  return CH4_OK;
+}
+
+ch4_status ch4_ensemble_averages(ch4_ensemble* E, int slot, ch4_averages* out) {
+  Slot* s = ens_slot(E, slot);
+  if (!s || !out) return CH4_ERR_ARG;
+  const ch4_config& c = s->cfg;
+  const size_t n1 = (size_t)s->N;
+  const int nblocks = (int)std::min<long long>(4 * 148, (s->N + AVG_BLOCK - 1) / AVG_BLOCK);
+  double* d = nullptr;
+  ch4_status st;
+  const size_t total = 6 * n1 + (size_t)nblocks * NAVG * 2 + NAVG;
+  if ((st = E->cuda(cudaMalloc(&d, total * sizeof(double)), "averages scratch"))) return st;
+  double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *part = d + 6 * n1;
+  double* res = part + (size_t)nblocks * NAVG * 2;
+  st = E->cuda(launch_hydro(E->params_of(*s, 0), E->shape, nullptr, nullptr, dd, du, s->nsets_on[1] ? dt : nullptr,
+                            s->nsets_on[2] ? ds : nullptr, nullptr, nullptr, E->stream),
+               "hydro");
+  AvgParams Q{};
+  Q.NX = c.NX;
+  Q.NY = c.NY;
+  Q.NZ = c.NZ;
+  Q.N = s->N;
+  Q.dens = dd;
+  Q.u = du;
+  Q.t = s->nsets_on[1] ? dt : nullptr;
+  Q.s = s->nsets_on[2] ? ds : nullptr;
+  Q.fwall = (c.flags & CH4_F_FLUID_BC_Y) != 0;
+  Q.twall = (c.flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+  Q.nu = c.nu;
+  Q.kappa = c.kappa;
+  Q.partial = part;
+  double h[NAVG];
+  if (!st) st = E->cuda(launch_averages(Q, nblocks, res, E->stream), "averages");
+  if (!st) st = E->cuda(cudaMemcpyAsync(h, res, sizeof h, cudaMemcpyDeviceToHost, E->stream), "averages down");
+  if (!st) st = E->cuda(cudaStreamSynchronize(E->stream), "averages sync");
+  cudaFree(d);
+  if (st) return st;
+  const double norm = 1.0 / (c.SX * c.SY * c.SZ);  // src/output.c:498-579
+  for (int q = 0; q < 18; q++) h[q] *= norm;
+  for (int q = 18; q < 21; q++) h[q] *= norm / (c.kappa * c.deltaT / c.SY);
+  h[21] *= norm;
+  h[22] *= norm;
+  std::memcpy(out, h, sizeof h);
+  return CH4_OK;
+}
+
+ch4_status ch4_ensemble_set_shape(ch4_ensemble* E, int block, int rows) {
+  if (!E || block < 64 || block > 1024 || (block % 32) || rows < 1) return CH4_ERR_ARG;
+  E->block = block;
+  E->rows = rows;
+  E->dirty = true;
+  E->drop_graph();
+  return CH4_OK;
+}
+
+// Project autotuner: one launch per candidate (block, rows) from the current state
+// into the scratch buffers, best of 3 timings; t^{n-1} fields are saved and restored,
+// so the simulation state is unchanged.
+ch4_status ch4_ensemble_tune(ch4_ensemble* E, int* block_out, int* rows_out) {
+  if (!E) return CH4_ERR_ARG;
+  ch4_status st;
+  std::vector<std::pair<float*, size_t>> saved;  // (backup, index into slots*2+which)
+  std::vector<float*> backups;
+  cudaStreamSynchronize(E->stream);
+  for (auto& s : E->slots) {
+    if (!s.used || !s.initialized) continue;
+    for (float* src : {s.tprev, s.sprev}) {
+      if (!src) continue;
+      float* b = nullptr;
+      if ((st = E->cuda(cudaMalloc(&b, s.N * sizeof(float)), "tune backup"))) return st;
+      cudaMemcpyAsync(b, src, s.N * sizeof(float), cudaMemcpyDeviceToDevice, E->stream);
+      backups.push_back(b);
+    }
+  }
+  const int blocks[] = {128, 256, 512};
+  const int rowsv[] = {1, 2, 4, 8};
+  float best = 1e30f;
+  int bb = E->block, br = E->rows;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int b : blocks)
+    for (int r : rowsv) {
+      E->block = b;
+      E->rows = r;
+      if ((st = ens_rebuild(E))) return st;
+      if (E->ntiles == 0) continue;
+      float t_best = 1e30f;
+      for (int rep = 0; rep < 4; rep++) {
+        cudaMemsetAsync(E->d_counter, 0, sizeof(int), E->stream);
+        cudaEventRecord(e0, E->stream);
+        if ((st = E->cuda(launch_ensemble_step(E->d_params[0], E->d_tiles, E->ntiles, E->d_counter, E->shape,
+                                               E->grid(), E->block, E->stream),
+                          "tune launch")))
+          return st;
+        cudaEventRecord(e1, E->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) t_best = std::min(t_best, ms);
+      }
+      if (t_best < best) {
+        best = t_best;
+        bb = b;
+        br = r;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  size_t k = 0;
+  for (auto& s : E->slots) {
+    if (!s.used || !s.initialized) continue;
+    for (float* dst : {s.tprev, s.sprev}) {
+      if (!dst) continue;
+      cudaMemcpyAsync(dst, backups[k++], s.N * sizeof(float), cudaMemcpyDeviceToDevice, E->stream);
+    }
+  }
+  if ((st = E->cuda(cudaStreamSynchronize(E->stream), "tune restore"))) return st;
+  for (float* b : backups) cudaFree(b);
+  E->block = bb;
+  E->rows = br;
+  E->dirty = true;
+  E->drop_graph();
+  if (block_out) *block_out = bb;
+  if (rows_out) *rows_out = br;
   return CH4_OK;
 }
 

@@ -220,6 +220,44 @@ ch4_status ch4_averages_get(ch4_handle *h, ch4_averages *out);
 /* Steps done so far (the reference's itime). */
 ch4_status ch4_get_itime(const ch4_handle *h, int *itime);
 
+
+/* --- batched ensemble (no reference counterpart: the reference runs one lattice
+ *     per MPI job; this runs many independent lattices in one device launch) --- */
+
+typedef struct ch4_ensemble ch4_ensemble;
+
+/* storage: CH4_STORE_F32 or CH4_STORE_F16 (FP32 arithmetic).  device_budget_bytes
+ * caps the population/state memory of all slots (0 = 90% of free device memory);
+ * a slot that does not fit is refused with CH4_ERR_NOMEM (admission control). */
+ch4_status ch4_ensemble_create(int storage, size_t device_budget_bytes, ch4_ensemble **out);
+ch4_status ch4_ensemble_destroy(ch4_ensemble *e);
+const char *ch4_ensemble_last_error(const ch4_ensemble *e);
+
+/* Add one lattice (same implemented flags as ch4_create, without HIT forcing, LES or
+ * particles; every slot of an ensemble must have the same population sets).  Starts
+ * at rest like ch4_create.  *slot receives its id. */
+ch4_status ch4_ensemble_add(ch4_ensemble *e, const ch4_config *cfg, int *slot);
+ch4_status ch4_ensemble_remove(ch4_ensemble *e, int slot);
+ch4_status ch4_ensemble_set_pop(ch4_ensemble *e, int slot, char which, const double *aos, int brd);
+ch4_status ch4_ensemble_get_pop(ch4_ensemble *e, int slot, char which, double *aos, int brd);
+/* src/main.c:24-48 for one slot (after its populations are set) */
+ch4_status ch4_ensemble_initialize(ch4_ensemble *e, int slot);
+/* Advance every active, initialised slot by nsteps (CUDA-graph-captured blocks of
+ * one persistent work-queue launch per step).  Asynchronous. */
+ch4_status ch4_ensemble_step(ch4_ensemble *e, int nsteps);
+ch4_status ch4_ensemble_synchronize(ch4_ensemble *e);
+ch4_status ch4_ensemble_get_fields(ch4_ensemble *e, int slot, double *dens, double *u, double *t, double *s, int brd);
+ch4_status ch4_ensemble_averages(ch4_ensemble *e, int slot, ch4_averages *out);
+ch4_status ch4_ensemble_itime(const ch4_ensemble *e, int slot, int *itime);
+/* Device bytes a slot with this configuration would take, and bytes in use. */
+ch4_status ch4_ensemble_slot_bytes(const ch4_config *cfg, int storage, size_t *bytes);
+ch4_status ch4_ensemble_bytes_in_use(const ch4_ensemble *e, size_t *bytes);
+/* Time the work-queue launch for each candidate block size and tile height on the
+ * current slots and keep the fastest (state is left unchanged); reports the choice. */
+ch4_status ch4_ensemble_tune(ch4_ensemble *e, int *block, int *rows_per_tile);
+/* Fix the launch shape instead of tuning (block 64..1024, rows >= 1). */
+ch4_status ch4_ensemble_set_shape(ch4_ensemble *e, int block, int rows_per_tile);
+
 #ifdef __cplusplus
 }
 #endif
