@@ -151,6 +151,21 @@ struct StorageOf<float> {
   static size_t bytes(int storage) { return storage == CH4_STORE_F16 ? 2 : 4; }
 };
 
+// Normalisation of the dump_averages sums, src/output.c:498-579 (the temperature
+// block only when the lattice has a temperature field).
+void normalize_averages(const ch4_config& c, const int* nsets_on, double* h) {
+  const double norm = 1.0 / (c.SX * c.SY * c.SZ);
+  for (int q = 0; q < 9; q++) h[q] *= norm;
+  if (nsets_on[1]) {
+    for (int q = 9; q < 18; q++) h[q] *= norm;
+    for (int q = 18; q < 21; q++) h[q] *= norm / (c.kappa * c.deltaT / c.SY);
+  }
+  if (nsets_on[2]) {
+    h[21] *= norm;
+    h[22] *= norm;
+  }
+}
+
 // Parameter block of one lattice from its configuration (host FP64 -> arithmetic type A).
 template <typename A>
 void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, const double* hit_fac, long long N,
@@ -381,11 +396,7 @@ struct Engine : EngineBase {
     if (!st) st = H->cuda(cudaStreamSynchronize(H->stream), "averages sync");
     cudaFree(d);
     if (st) return st;
-    const double norm = 1.0 / (c.SX * c.SY * c.SZ);  // src/output.c:498-579
-    for (int q = 0; q < 18; q++) h[q] *= norm;
-    for (int q = 18; q < 21; q++) h[q] *= norm / (c.kappa * c.deltaT / c.SY);
-    h[21] *= norm;
-    h[22] *= norm;
+    normalize_averages(c, nsets_on, h);
     std::memcpy(out, h, sizeof h);
     return CH4_OK;
   }
@@ -1634,17 +1645,13 @@ ch4_status ch4_ensemble_averages(ch4_ensemble* E, int slot, ch4_averages* out) {
   if (!st) st = E->cuda(cudaStreamSynchronize(E->stream), "averages sync");
   cudaFree(d);
   if (st) return st;
-  const double norm = 1.0 / (c.SX * c.SY * c.SZ);  // src/output.c:498-579
-  for (int q = 0; q < 18; q++) h[q] *= norm;
-  for (int q = 18; q < 21; q++) h[q] *= norm / (c.kappa * c.deltaT / c.SY);
-  h[21] *= norm;
-  h[22] *= norm;
+  normalize_averages(c, s->nsets_on, h);
   std::memcpy(out, h, sizeof h);
   return CH4_OK;
 }
 
 ch4_status ch4_ensemble_set_shape(ch4_ensemble* E, int block, int rows) {
-  if (!E || block < 64 || block > 1024 || (block % 32) || rows < 1) return CH4_ERR_ARG;
+  if (!E || block < 32 || block > 256 || (block % 32) || rows < 1) return CH4_ERR_ARG;
   E->block = block;
   E->rows = rows;
   E->dirty = true;
@@ -1658,7 +1665,6 @@ ch4_status ch4_ensemble_set_shape(ch4_ensemble* E, int block, int rows) {
 ch4_status ch4_ensemble_tune(ch4_ensemble* E, int* block_out, int* rows_out) {
   if (!E) return CH4_ERR_ARG;
   ch4_status st;
-  std::vector<std::pair<float*, size_t>> saved;  // (backup, index into slots*2+which)
   std::vector<float*> backups;
   cudaStreamSynchronize(E->stream);
   for (auto& s : E->slots) {
@@ -1671,7 +1677,7 @@ ch4_status ch4_ensemble_tune(ch4_ensemble* E, int* block_out, int* rows_out) {
       backups.push_back(b);
     }
   }
-  const int blocks[] = {128, 256, 512};
+  const int blocks[] = {64, 128, 256};  // the kernel is built for at most 256 threads
   const int rowsv[] = {1, 2, 4, 8};
   float best = 1e30f;
   int bb = E->block, br = E->rows;

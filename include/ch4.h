@@ -255,7 +255,7 @@ ch4_status ch4_ensemble_bytes_in_use(const ch4_ensemble *e, size_t *bytes);
 /* Time the work-queue launch for each candidate block size and tile height on the
  * current slots and keep the fastest (state is left unchanged); reports the choice. */
 ch4_status ch4_ensemble_tune(ch4_ensemble *e, int *block, int *rows_per_tile);
-/* Fix the launch shape instead of tuning (block 64..1024, rows >= 1). */
+/* Fix the launch shape instead of tuning (block 32..256 in steps of 32, rows >= 1). */
 ch4_status ch4_ensemble_set_shape(ch4_ensemble *e, int block, int rows_per_tile);
 
 #ifdef __cplusplus

@@ -93,7 +93,8 @@ def test_ensemble_fp32_close_to_fp64_oracle():
         cfg64 = O.make_config(cfg.NX, cfg.NY, cfg.NZ, RB_FLAGS, tau_u=cfg.tau_u, tau_t=cfg.tau_t, beta_t=1.0,
                               gravity_y=cfg.gravity_y, T_bot=1.0, T_top=0.0, T_ref=0.5)
         ref = run_restatement(cfg64, st, 60)
-        assert np.linalg.norm(m["t"] - ref["t"]) / np.linalg.norm(ref["t"]) < 1e-6
+        # FP32 arithmetic and storage: T within 1e-5 relative L2 after 60 steps
+        assert np.linalg.norm(m["t"] - ref["t"]) / np.linalg.norm(ref["t"]) < 1e-5
         # Nusselt number (dump_averages nuy) within 1e-4 relative
         assert abs(m["avg"]["nuy"] - ref["avg"]["nuy"]) <= 1e-4 * abs(ref["avg"]["nuy"])
 

@@ -119,13 +119,13 @@ def test_larger_lattice_bit_identical():
 
 def test_particles_fp32_fluid_close_to_fp64():
     """FP32 lattice arithmetic (FP64 particle state): positions after 30 steps
-    within 1e-9 relative L2 of the FP64 oracle."""
+    within 1e-6 relative L2 of the FP64 oracle."""
     _, cfg64, state = make_case("particles", seed=4)
     _, cfg, _ = make_case("particles", seed=4, storage=1)
     ref = run_restatement(cfg64, state, 30)
     gpu = run_gpu(cfg, state, 30)
     pos = lambda d: np.stack([d["part"][k] for k in ("x", "y", "z")])
-    assert rel_l2(pos(gpu), pos(ref)) < 1e-9
+    assert rel_l2(pos(gpu), pos(ref)) < 1e-6
 
 
 @pytest.mark.parametrize("name", ["kolmogorov", "rb", "walls2", "scalar", "particles"])
