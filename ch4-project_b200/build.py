@@ -40,6 +40,7 @@ def build(verbose=False):
     units = [
         ("lb_f64.cu", ["-fmad=false"]),
         ("lb_f32.cu", []),
+        ("noalloc.cu", ["-fmad=false"]),
     ]
     for src, extra in units:
         s = os.path.join(CSRC, src)

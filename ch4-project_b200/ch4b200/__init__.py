@@ -77,6 +77,9 @@ def lib():
         L.ch4_ensemble_bytes_in_use.argtypes = [P, C.POINTER(C.c_size_t)]
         L.ch4_ensemble_tune.argtypes = [P, I, I]
         L.ch4_ensemble_set_shape.argtypes = [P, C.c_int, C.c_int]
+        V = C.c_void_p
+        L.ch4_averages_noalloc.argtypes = [V, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                           C.c_double, V, V]
         _lib = L
     return _lib
 
@@ -325,3 +328,17 @@ def ensemble_slot_bytes(cfg, storage):
     if rc:
         raise CH4Error(rc, "slot_bytes")
     return v.value
+
+
+NOALLOC_MAX_CELLS = 2048 * 65536  # CH4_NOALLOC_MAX_BLOCKS * CH4_NOALLOC_CELLS_PER_BLOCK
+
+
+def averages_noalloc(dens, u, t, s, NX, NY, NZ, fluid_walls, scalar_walls, nu, kappa, sums, stream=0):
+    """ch4_averages_noalloc: raw dump_averages sums of FP64 device fields (device
+    addresses as integers) into `sums` (23 device doubles); allocates nothing.
+    For callers that cannot call cudaMalloc (a diagnostic inside a stream-ordered
+    time loop, or a fully reserved device-memory budget)."""
+    rc = lib().ch4_averages_noalloc(dens, u, t, s, NX, NY, NZ, int(fluid_walls), int(scalar_walls), nu, kappa,
+                                    sums, stream)
+    if rc:
+        raise CH4Error(rc, "ch4_averages_noalloc")

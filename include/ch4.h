@@ -258,6 +258,28 @@ ch4_status ch4_ensemble_tune(ch4_ensemble *e, int *block, int *rows_per_tile);
 /* Fix the launch shape instead of tuning (block 32..256 in steps of 32, rows >= 1). */
 ch4_status ch4_ensemble_set_shape(ch4_ensemble *e, int block, int rows_per_tile);
 
+/* --- global averages without any allocation ------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * a diagnostic run inside a stream-ordered time loop (allocation would
+ * synchronise the device) or inside a fixed device-memory budget already
+ * reserved in full.  The caller passes device pointers to the FP64 hydrodynamic
+ * fields (dens, u as 3 planes of NX*NY*NZ, optional t and s; x fastest) and to
+ * `sums` (CH4_NOALLOC_SUMS doubles, device memory), and receives the raw sums of
+ * dump_averages in ch4_averages field order (before the normalisation of
+ * src/output.c:498-579).  The reduction's scratch is a file-scope device array of
+ * CH4_NOALLOC_MAX_BLOCKS block partials (754 KB, held by every GPU that loads the
+ * library until exit); lattices above CH4_NOALLOC_MAX_BLOCKS *
+ * CH4_NOALLOC_CELLS_PER_BLOCK cells are refused with CH4_ERR_ARG.  The first call
+ * on a device looks up that array's device address (make it before any stream
+ * capture); all calls share the array, so calls that overlap on the GPU race.
+ * Asynchronous on `stream` (a cudaStream_t, NULL = default stream). */
+#define CH4_NOALLOC_MAX_BLOCKS 2048
+#define CH4_NOALLOC_CELLS_PER_BLOCK 65536
+#define CH4_NOALLOC_SUMS 23
+ch4_status ch4_averages_noalloc(const double *dens, const double *u, const double *t, const double *s, int NX, int NY,
+                                int NZ, int fluid_walls, int scalar_walls, double nu, double kappa, double *sums,
+                                void *stream);
+
 #ifdef __cplusplus
 }
 #endif
