@@ -196,6 +196,237 @@ def run_reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# other workloads (not the driver's default line)
+
+def _event_time(stream_handle, fn):
+    import torch
+    st = torch.cuda.ExternalStream(stream_handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    fn()
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3
+
+
+def bench_ensemble(args):
+    """512 independent quasi-2D Rayleigh-Benard cells (NZ = 1) of log-uniform sizes
+    64x64 .. 512x256 and Ra in [1e5, 1e8], Pr = 1, advanced together.  Throughput as
+    solves/hour for S steps per solve, against the plain FP64 path run one case at a
+    time (per-case step time fitted as a + b*cells on a sample).  Accuracy on the same
+    sample: Nusselt number averaged over steps [S/2, S] (every 500 steps), ensemble
+    against FP64, relative error."""
+    import math
+    import torch
+    import ch4b200
+    from ch4b200 import abi
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(4)
+    S = args.steps_per_solve
+    every = 500
+    storage = {"f32": abi.STORE_F32, "f16": abi.STORE_F16}.get(args.storage, abi.STORE_F16)
+    cases = []
+    for i in range(args.cases):
+        nx = int(round(math.exp(rng.uniform(math.log(64), math.log(512)))))
+        ny = int(round(math.exp(rng.uniform(math.log(64), math.log(256)))))
+        ra = math.exp(rng.uniform(math.log(1e5), math.log(1e8)))
+        cases.append((nx, ny, ra))
+    sample = sorted(int(i) for i in rng.choice(len(cases), size=min(args.sample, len(cases)), replace=False))
+
+    def cfg_of(nx, ny, ra, st):
+        c = ch4b200.default_config()
+        c.NX, c.NY, c.NZ = nx, ny, 1
+        c.SX, c.SY, c.SZ = float(nx), float(ny), 1.0
+        c.flags = abi.flags_of(["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
+                                "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y"])
+        c.storage = st
+        bg = 0.05 ** 2 / ny
+        nu = (bg * ny ** 3 / ra) ** 0.5
+        c.tau_u = c.tau_t = 0.5 + 3 * nu
+        c.beta_t, c.gravity_y, c.T_bot, c.T_top, c.T_ref = 1.0, bg, 1.0, 0.0, 0.5
+        c.nu = (c.tau_u - 0.5) / 3.0
+        c.kappa = (c.tau_t - 0.5) / 3.0
+        c.deltaT = 1.0
+        return c
+
+    w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+
+    def state_of(i, nx, ny):
+        r = np.random.default_rng(100 + i)
+        y = (np.arange(ny) + 0.5) / ny
+        T = (1.0 - y)[None, :, None] + 1e-3 * (2 * r.random((1, ny, nx)) - 1)
+        return np.ascontiguousarray(np.broadcast_to(w, (1, ny, nx, 19))), np.ascontiguousarray(T[..., None] * w)
+
+    ens = ch4b200.Ensemble(storage)
+    slots = []
+    cells = 0
+    for i, (nx, ny, ra) in enumerate(cases):
+        s = ens.add(cfg_of(nx, ny, ra, storage))
+        p0, g0 = state_of(i, nx, ny)
+        ens.set_pop(s, "p", p0)
+        ens.set_pop(s, "g", g0)
+        ens.initialize(s)
+        slots.append(s)
+        cells += nx * ny
+    block, rows = ens.tune()
+    ens.step(100)
+    ens.synchronize()
+    K = args.steps
+    t_step = _event_time(ens.stream_handle, lambda: ens.step(K)) / K
+    solves_h = len(cases) * 3600.0 / (S * t_step)
+    # the rest of the solve, sampling Nu of the sampled cases over [S/2, S]
+    done = 100 + K
+    nu_ens = {i: [] for i in sample}
+    while done < S:
+        target = min(S, (done // every + 1) * every)
+        ens.step(target - done)
+        done = target
+        if done >= S // 2:
+            for i in sample:
+                nu_ens[i].append(ens.averages(slots[i])["nuy"])
+    ens.close()
+    # plain FP64, one case at a time, on the sample
+    xs, ts, errs, nus = [], [], [], []
+    for i in sample:
+        nx, ny, ra = cases[i]
+        p0, g0 = state_of(i, nx, ny)
+        with ch4b200.Simulation(cfg_of(nx, ny, ra, abi.STORE_F64)) as sim:
+            sim.set_pop("p", p0)
+            sim.set_pop("g", g0)
+            sim.initialize()
+            sim.step(20)
+            sim.synchronize()
+            t = _event_time(sim.stream_handle, lambda: sim.step(100))
+            d, nu64 = 120, []
+            while d < S:
+                target = min(S, (d // every + 1) * every)
+                sim.step(target - d)
+                d = target
+                if d >= S // 2:
+                    nu64.append(sim.averages()["nuy"])
+        xs.append(nx * ny)
+        ts.append(t / 100)
+        m64, m32 = float(np.mean(nu64)), float(np.mean(nu_ens[i]))
+        nus.append(m64)
+        errs.append(abs(m32 - m64) / abs(m64))
+    a, b = np.polyfit(np.array(xs, float), np.array(ts), 1)[::-1]
+    t64 = sum(max(a + b * nx * ny, min(ts)) for nx, ny, _ in cases)
+    solves_h64 = 3600.0 * len(cases) / (S * t64)
+    st_name = "f16" if storage == abi.STORE_F16 else "f32"
+    print(json.dumps({
+        "metric": "ensemble solves/hour", "value": solves_h, "unit": "solves/h", "n_gpus": 1, "steps": K,
+        "higher_is_better": True, "dtype": "f32 (%s storage)" % st_name, "data": "synthetic",
+        "config": {"workload": "ensemble_%d_quasi2d_rayleigh_benard" % len(cases), "cells_total": cells,
+                   "steps_per_solve": S, "tile_block": block, "tile_rows": rows, "graph_block_steps": 100,
+                   "storage": st_name},
+        "ensemble_ms_per_step": t_step * 1e3, "ensemble_mlups": cells / t_step / 1e6,
+        "fp64_one_at_a_time": {"solves_per_hour": solves_h64, "fit_seconds_per_step": [a, b],
+                               "sample_cases": len(sample)},
+        "speedup_vs_fp64_one_at_a_time": solves_h / solves_h64,
+        "nusselt_vs_fp64": {"window": [S // 2, S], "every": every, "cases": len(errs),
+                            "rel_error_median": float(np.median(errs)), "rel_error_max": float(np.max(errs)),
+                            "nu_fp64_range": [float(min(nus)), float(max(nus))]},
+    }))
+    return 0
+
+
+def bench_serve(args):
+    """Poisson request stream (20/s) of Kolmogorov and Rayleigh-Benard cubes, half with
+    LES (C_s 0.17) and 1e4-1e5 tracers; step counts log-uniform in [500, 20000] times
+    --step-scale.  p50/p99 latency and aggregate MLUPS against the FP64 path serving the
+    same requests one at a time."""
+    import copy
+    import torch
+    from ch4b200 import abi, serve
+    torch.cuda.set_device(0)
+    reqs = serve.make_requests(args.requests, rate=20.0, step_scale=args.step_scale)
+    work = sum(r.cells * r.steps for r in reqs)
+    for r in reqs:  # requests arrive with their initial state: build them outside both timed runs
+        serve.request_state(r)
+        serve.request_particles(r)
+    srv = serve.Server(abi.STORE_F32, block=100)
+    t0 = time.perf_counter()
+    done = srv.run(copy.deepcopy(reqs))
+    makespan = time.perf_counter() - t0
+    lat = np.array([r.latency for r in done])
+    base = serve.serve_fp64_one_at_a_time(copy.deepcopy(reqs))
+    lat64 = np.array([r.latency for r in base])
+    span64 = max(r.finished for r in base) - min(r.arrival for r in base)
+    print(json.dumps({
+        "metric": "served p50/p99 latency and aggregate MLUPS", "value": work / makespan / 1e6, "unit": "MLUPS",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "served_stream", "requests": len(reqs), "rate_per_s": 20.0,
+                   "sizes": [32, 64, 96, 128, 192], "steps": "log-uniform [500,20000] x %g" % args.step_scale,
+                   "les_fraction": 0.5, "block_steps": 100},
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)), "makespan_s": makespan,
+        "fp64_one_at_a_time": {"p50_s": float(np.percentile(lat64, 50)), "p99_s": float(np.percentile(lat64, 99)),
+                               "mlups": work / span64 / 1e6},
+    }))
+    return 0
+
+
+TAU_ETA = 10.0  # Kolmogorov time in steps that sets tau_p = St * tau_eta
+
+
+def bench_hit_particles(args):
+    """Forced HIT 256^3 (FP32), 1e6 particles: tracers and Stokes particles with added
+    mass, beta in {0, 1, 3} x St in {0.1, 1, 5} with tau_p = St * 10 steps, except that
+    the bubbles (beta = 3) stop at St = 2: at St = 5 their radius sqrt(3 nu beta tau_p)
+    is 1.22 cells and the explicit two-way deposit diverges within ~20 steps (the FP64
+    oracle shows the same).  Trilinear interpolation with gradients, two-way momentum
+    deposit.  MLUPS and particle updates per second."""
+    import torch
+    import ch4b200
+    from ch4b200 import abi
+    torch.cuda.set_device(0)
+    n = args.hit_size
+    npart = args.particles
+    c = ch4b200.default_config()
+    c.NX = c.NY = c.NZ = n
+    c.SX = c.SY = c.SZ = float(n)
+    c.flags = abi.flags_of(["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                            "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY",
+                            "LAGRANGE_TWOWAY_MOMENTUM"])
+    c.storage = {"f64": abi.STORE_F64, "f16": abi.STORE_F16}.get(args.storage, abi.STORE_F32)
+    c.tau_u = 0.51
+    c.nu = (c.tau_u - 0.5) / 3.0
+    c.Amp_x = c.Amp_y = c.Amp_z = 5e-6
+    c.time_dt_lagr_factor = 1.0
+    c.seed = 11
+    rng = np.random.default_rng(5)
+    # one record of 43 doubles per particle (name, tau_drag, beta_coeff, x, y, z, ...), at rest;
+    # kinds cycle over tracers and the 9 (St, beta) Stokes classes
+    rec = np.zeros((npart, len(abi.Particle._fields_)))
+    rec[:, 0] = np.arange(npart)
+    rec[:, 3:6] = rng.random((npart, 3)) * n
+    kind = np.arange(npart) % 10
+    stokes = kind > 0
+    beta = np.array([0.0, 1.0, 3.0])[(kind[stokes] - 1) % 3]
+    st = np.array([0.1, 1.0, 5.0])[(kind[stokes] - 1) // 3]
+    st = np.where(beta == 3.0, np.minimum(st, 2.0), st)
+    rec[stokes, 2] = beta
+    rec[stokes, 1] = st * TAU_ETA
+    parts = (abi.Particle * npart).from_buffer(rec)
+    with ch4b200.Simulation(c) as sim:
+        sim.set_particles(parts)
+        sim.initialize()
+        sim.step(max(3, args.warmup))
+        sim.synchronize()
+        sec = _event_time(sim.stream_handle, lambda: sim.step(args.steps))
+        f = sim.fields()
+    cells = n ** 3
+    print(json.dumps({
+        "metric": "MLUPS and particle updates/s", "value": cells * args.steps / sec / 1e6, "unit": "MLUPS",
+        "particles_per_s": npart * args.steps / sec, "n_gpus": 1, "steps": args.steps,
+        "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True, "dtype": args.storage,
+        "data": "synthetic", "config": {"workload": "hit_%d3_particles_%d_twoway" % (n, npart), "tau_eta_steps": TAU_ETA,
+                                        "classes": "tracers + beta{0,1,3} x St{0.1,1,5}, bubbles St<=2"},
+        "finite": bool(np.isfinite(f["u"]).all()),
+    }))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,7 +437,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--lattice", default=None, help="NX,NY,NZ override (profiling runs on a smaller case)")
+    ap.add_argument("--workload", default="rb", choices=["rb", "ensemble", "serve", "hit_particles"])
+    ap.add_argument("--cases", type=int, default=512)
+    ap.add_argument("--steps-per-solve", type=int, default=20000)
+    ap.add_argument("--sample", type=int, default=16)
+    ap.add_argument("--compare-steps", type=int, default=2000)
+    ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--step-scale", type=float, default=0.05)
+    ap.add_argument("--hit-size", type=int, default=256)
+    ap.add_argument("--particles", type=int, default=1000000)
     args = ap.parse_args()
+    if args.workload == "ensemble":
+        return bench_ensemble(args)
+    if args.workload == "serve":
+        return bench_serve(args)
+    if args.workload == "hit_particles":
+        return bench_hit_particles(args)
     if args.lattice:
         global NX, NY, NZ
         NX, NY, NZ = (int(v) for v in args.lattice.split(","))

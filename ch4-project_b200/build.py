@@ -46,8 +46,10 @@ def build(verbose=False):
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if newer([s] + headers, o):
-            run([NVCC] + ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + extra
-                + ["-c", s, "-o", o])
+            r = run([NVCC] + ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + extra
+                    + ["-c", s, "-o", o])
+            with open(o + ".ptxas.txt", "w") as f:  # registers, spills and shared memory per kernel
+                f.write(r.stdout + r.stderr)
         objs.append(o)
     for src in ["ch4_host.cpp"]:
         s = os.path.join(CSRC, src)

@@ -15,7 +15,7 @@ from . import abi
 from .abi import NPOP, Config, Particle, Averages, FLAGS, flags_of  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libch4b200.so")
+LIB_PATH = os.environ.get("CH4B200_LIB") or os.path.join(HERE, "libch4b200.so")  # override: another build of the library
 
 _lib = None
 
@@ -77,6 +77,9 @@ def lib():
         L.ch4_ensemble_bytes_in_use.argtypes = [P, C.POINTER(C.c_size_t)]
         L.ch4_ensemble_tune.argtypes = [P, I, I]
         L.ch4_ensemble_set_shape.argtypes = [P, C.c_int, C.c_int]
+        L.ch4_ensemble_get_stream.argtypes = [P, C.POINTER(C.c_void_p)]
+        L.ch4_initial_populations.argtypes = [C.POINTER(Config), D, D, D, D]
+        L.ch4_initial_conditions.argtypes = [P]
         V = C.c_void_p
         L.ch4_averages_noalloc.argtypes = [V, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                            C.c_double, V, V]
@@ -118,6 +121,24 @@ def read_parameter(path, key):
     if rc:
         raise CH4Error(rc, "%s not found in %s" % (key, path))
     return v.value
+
+
+def initial_populations(cfg):
+    """ch4_initial_populations: the reference's initial fields for the *_INITIAL_*
+    flags of cfg (host only).  Returns {"p", "g", "h": AoS (NZ, NY, NX, 19) float64,
+    "phi": (6, 3) HIT phases drawn after them}."""
+    shape = (cfg.NZ, cfg.NY, cfg.NX, abi.NPOP)
+    out = {"p": np.zeros(shape)}
+    if cfg.flags & abi.FLAGS["LB_TEMPERATURE"]:
+        out["g"] = np.zeros(shape)
+    if cfg.flags & abi.FLAGS["LB_SCALAR"]:
+        out["h"] = np.zeros(shape)
+    phi = np.zeros((abi.NK, 3))
+    rc = lib().ch4_initial_populations(C.byref(cfg), _dp(out["p"]), _dp(out.get("g")), _dp(out.get("h")), _dp(phi))
+    if rc:
+        raise CH4Error(rc, "ch4_initial_populations")
+    out["phi"] = phi
+    return out
 
 
 def device_bytes(cfg):
@@ -185,6 +206,10 @@ class Simulation:
         arr = (Particle * n)()
         self._check(lib().ch4_get_particles(self.h, arr, n), "get_particles")
         return arr
+
+    def initial_conditions(self):
+        """ch4_initial_conditions: the reference's initial fields and HIT phases."""
+        self._check(lib().ch4_initial_conditions(self.h), "initial_conditions")
 
     def initialize(self):
         self._check(lib().ch4_initialize(self.h), "initialize")
@@ -317,6 +342,13 @@ class Ensemble:
         b, r = C.c_int(), C.c_int()
         self._check(lib().ch4_ensemble_tune(self.h, C.byref(b), C.byref(r)), "tune")
         return b.value, r.value
+
+    @property
+    def stream_handle(self):
+        """cudaStream_t of the ensemble as an integer (for torch.cuda.ExternalStream)."""
+        v = C.c_void_p()
+        self._check(lib().ch4_ensemble_get_stream(self.h, C.byref(v)), "get_stream")
+        return v.value or 0
 
     def set_shape(self, block, rows):
         self._check(lib().ch4_ensemble_set_shape(self.h, block, rows), "set_shape")

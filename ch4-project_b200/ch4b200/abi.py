@@ -46,7 +46,30 @@ FLAGS = {
     "LB_TEMPERATURE_FORCING": 1 << 25,
     "LAGRANGE_WRAP": 1 << 26,
     "LAGRANGE_GRADIENT_BRD2": 1 << 27,
+    # initial fields (ch4_initial_conditions)
+    "LB_FLUID_INITIAL_KOLMOGOROV": 1 << 28,
+    "LB_FLUID_INITIAL_POISEUILLE": 1 << 29,
+    "LB_FLUID_INITIAL_PERTURBATION": 1 << 30,
+    "LB_FLUID_INITIAL_ADD_NOISE": 1 << 31,
+    "LB_FLUID_INITIAL_UNIT_DENSITY": 1 << 32,
+    "LB_INITIAL_BAROMETRIC": 1 << 33,
+    "LB_FLUID_INITIAL_VORTICES": 1 << 34,
+    "LB_FLUID_INITIAL_CELLULAR": 1 << 35,
+    "LB_TEMPERATURE_INITIAL_LINEAR": 1 << 36,
+    "LB_TEMPERATURE_INITIAL_CONSTANT": 1 << 37,
+    "LB_TEMPERATURE_INITIAL_CONSTANT_MEAN": 1 << 38,
+    "LB_TEMPERATURE_INITIAL_CONSTANT_BOT": 1 << 39,
+    "LB_TEMPERATURE_INITIAL_CONSTANT_TOP": 1 << 40,
+    "LB_TEMPERATURE_INITIAL_ADD_PERTURBATION": 1 << 41,
+    "LB_TEMPERATURE_INITIAL_ADD_NOISE": 1 << 42,
+    "LB_SCALAR_INITIAL_LINEAR": 1 << 43,
+    "LB_SCALAR_INITIAL_ADD_PERTURBATION": 1 << 44,
+    "LB_SCALAR_INITIAL_CONSTANT": 1 << 45,
+    "LB_SCALAR_INITIAL_CONSTANT_MEAN": 1 << 46,
+    "LB_SCALAR_INITIAL_CONSTANT_BOT": 1 << 47,
+    "LB_SCALAR_INITIAL_CONSTANT_TOP": 1 << 48,
 }
+INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 
 
 class Config(C.Structure):
@@ -72,6 +95,7 @@ class Config(C.Structure):
         ("particle_number", C.c_int),
         ("seed", C.c_uint64),
         ("resume", C.c_int),
+        ("noise_u", C.c_double), ("noise_t", C.c_double),
     ]
 
 

@@ -32,13 +32,14 @@ const double VK[NK][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1},
 // lattice constants of design_lb (src/lb.c:139-160, 368-377), host FP64
 struct Lattice {
   double w[NPOP];
-  double invcs2, invcs4, invtwocs2, invtwocs4;
+  double cs2, invcs2, invcs4, invtwocs2, invtwocs4;
   Lattice() {
     w[0] = 1. / 3.;
     for (int q = 1; q <= 6; q++) w[q] = 1. / 18.;
     for (int q = 7; q < NPOP; q++) w[q] = 1. / 36.;
     double cs = 1.0 / std::sqrt(3.0);
-    double cs2 = std::pow(cs, 2.0), cs4 = std::pow(cs, 4.0);
+    cs2 = std::pow(cs, 2.0);
+    double cs4 = std::pow(cs, 4.0);
     invcs2 = 1.0 / cs2;
     invcs4 = 1.0 / cs4;
     invtwocs2 = 1.0 / (2.0 * cs2);
@@ -53,7 +54,169 @@ const uint64_t SUPPORTED =
     CH4_F_TEMPERATURE_BC_Y_M_FLUX | CH4_F_TEMPERATURE_BC_Y_P_NOFLUX | CH4_F_TEMPERATURE_BC_Y_M_NOFLUX |
     CH4_F_SCALAR_BC_Y | CH4_F_FLUID_LES | CH4_F_TEMPERATURE_FORCING | CH4_F_LAGRANGE | CH4_F_LAGRANGE_WRAP |
     CH4_F_LAGRANGE_GRADIENT | CH4_F_LAGRANGE_ADDEDMASS | CH4_F_LAGRANGE_TWOWAY | CH4_F_LAGRANGE_TWOWAY_MOMENTUM |
-    CH4_F_LAGRANGE_GRADIENT_BRD2;
+    CH4_F_LAGRANGE_GRADIENT_BRD2 | CH4_F_FLUID_INITIAL_KOLMOGOROV | CH4_F_FLUID_INITIAL_POISEUILLE |
+    CH4_F_FLUID_INITIAL_PERTURBATION | CH4_F_FLUID_INITIAL_ADD_NOISE | CH4_F_FLUID_INITIAL_UNIT_DENSITY |
+    CH4_F_INITIAL_BAROMETRIC | CH4_F_FLUID_INITIAL_VORTICES | CH4_F_FLUID_INITIAL_CELLULAR |
+    CH4_F_TEMPERATURE_INITIAL_LINEAR | CH4_F_TEMPERATURE_INITIAL_CONSTANT | CH4_F_TEMPERATURE_INITIAL_CONSTANT_MEAN |
+    CH4_F_TEMPERATURE_INITIAL_CONSTANT_BOT | CH4_F_TEMPERATURE_INITIAL_CONSTANT_TOP |
+    CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION | CH4_F_TEMPERATURE_INITIAL_ADD_NOISE | CH4_F_SCALAR_INITIAL_LINEAR |
+    CH4_F_SCALAR_INITIAL_ADD_PERTURBATION | CH4_F_SCALAR_INITIAL_CONSTANT | CH4_F_SCALAR_INITIAL_CONSTANT_MEAN |
+    CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER;
+
+// drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
+inline double myrand48(unsigned short st[3]) { return erand48(st); }
+
+// srand48(seed): the state the reference's stream starts from (src/parallel.c:238-240)
+inline void seed48_state(uint64_t seed, unsigned short st[3]) {
+  st[0] = 0x330E;
+  st[1] = (unsigned short)(seed & 0xFFFF);
+  st[2] = (unsigned short)((seed >> 16) & 0xFFFF);
+}
+
+// The reference's two_pi is the text `2*3.14159265359`: kn*two_pi*y/L is ((kn*2)*pi)*y/L.
+inline double twopi_times(double a) { return a * 2 * 3.14159265359; }
+
+// initial_conditions (src/initial_conditions.c:3-500) for the supported flags, on
+// the host in FP64 with the reference's loop order (k, j, i), operation order and
+// drand48 draws.  Cell centres are index + 0.5 (GRID_REGULAR with S = N).
+ch4_status initial_fields(const ch4_config& c, const Lattice& lat, unsigned short rng[3], double* p, double* g,
+                          double* hs) {
+  const uint64_t F = c.flags;
+  const int NX = c.NX, NY = c.NY, NZ = c.NZ;
+  auto cell = [&](int i, int j, int k) { return ((size_t)k * NY + j) * NX + i; };
+  auto has = [&](uint64_t b) { return (F & b) != 0; };
+  double cxd[NPOP], cyd[NPOP], czd[NPOP];
+  for (int q = 0; q < NPOP; q++) {
+    cxd[q] = (double)cx(q);
+    cyd[q] = (double)cy(q);
+    czd[q] = (double)cz(q);
+  }
+  if (p) {
+    for (int k = 0; k < NZ; k++)
+      for (int j = 0; j < NY; j++)
+        for (int i = 0; i < NX; i++) {
+          double* f = p + cell(i, j, k) * NPOP;
+          const double x = (double)i + 0.5, y = (double)j + 0.5;
+          for (int pp = 0; pp < NPOP; pp++) f[pp] = lat.w[pp];  // 45
+          if (has(CH4_F_TEMPERATURE_BUOYANCY) && has(CH4_F_INITIAL_BAROMETRIC)) {  // 72-88
+            const double L = c.SY;
+            for (int pp = 0; pp < NPOP; pp++)
+              f[pp] = lat.w[pp] *
+                      (std::exp(c.beta_t * c.gravity_y * y * (0.5 * c.deltaT - 0.5 * (c.deltaT / L) * y) / lat.cs2));
+          }
+          if (has(CH4_F_FLUID_INITIAL_VORTICES)) {  // 99-110
+            const double fn = 0.0001, kn = 10.0, LY = c.SY, LX = c.SX;
+            for (int pp = 0; pp < NPOP; pp++)
+              f[pp] += 3.0 * fn * lat.w[pp] *
+                       (cyd[pp] * std::sin(twopi_times(0.5 * kn) * x / LX) - cxd[pp] * std::cos(twopi_times(kn) * y / LY));
+          }
+          if (has(CH4_F_FLUID_INITIAL_KOLMOGOROV)) {  // 112-122
+            const double fn = 0.01, kn = 1.0, L = c.SY;
+            for (int pp = 0; pp < NPOP; pp++) f[pp] += 3.0 * lat.w[pp] * cxd[pp] * fn * std::sin(twopi_times(kn) * y / L);
+          }
+          if (has(CH4_F_FLUID_INITIAL_CELLULAR)) {  // 124-145
+            const double kn = 0.5, fn = c.Amp_x, LX = c.SX, LY = c.SY;
+            for (int pp = 0; pp < NPOP; pp++)
+              f[pp] += 3.0 * fn * lat.w[pp] *
+                       (cxd[pp] * (-std::sin(twopi_times(2. * kn) * x / LX) * std::cos(twopi_times(kn) * y / LY)) +
+                        cyd[pp] * (std::cos(twopi_times(2. * kn) * x / LX) * std::sin(twopi_times(kn) * y / LY)));
+          }
+          if (has(CH4_F_FLUID_INITIAL_POISEUILLE)) {  // 170-180
+            const double L = c.SY, fn = -c.Amp_x * 4.0 * std::pow(L, -2.0);
+            for (int pp = 0; pp < NPOP; pp++) f[pp] += 3.0 * lat.w[pp] * cxd[pp] * fn * y * (y - L);
+          }
+          if (has(CH4_F_FLUID_INITIAL_PERTURBATION)) {  // 226-231: three draws per direction, x then y then z
+            const double fn = 0.2 * c.Amp_x;
+            for (int pp = 0; pp < NPOP; pp++) {
+              const double rx = 2.0 * myrand48(rng) - 1.0;
+              const double ry = 2.0 * myrand48(rng) - 1.0;
+              const double rz = 2.0 * myrand48(rng) - 1.0;
+              f[pp] += 3.0 * fn * lat.w[pp] * (rx * cxd[pp] + ry * cyd[pp] + rz * czd[pp]);
+            }
+          }
+          if (has(CH4_F_FLUID_INITIAL_ADD_NOISE)) {  // 233-242: one draw per cell, its sign only
+            const double val = 2.0 * myrand48(rng) - 1.0;
+            const double sgn = (double)((val > 0) - (val < 0));
+            for (int pp = 0; pp < NPOP; pp++) f[pp] += 6.0 * lat.w[pp] * c.noise_u * cxd[pp] * sgn;
+          }
+        }
+    if (has(CH4_F_FLUID_INITIAL_UNIT_DENSITY)) {  // 256-279: global density 1
+      double norm = 0.0;
+      for (int k = 0; k < NZ; k++)
+        for (int j = 0; j < NY; j++)
+          for (int i = 0; i < NX; i++)
+            for (int pp = 0; pp < NPOP; pp++) norm += p[cell(i, j, k) * NPOP + pp];
+      double norm_all = norm;
+      norm_all /= (double)NX * (double)NY * (double)NZ;
+      for (int k = 0; k < NZ; k++)
+        for (int j = 0; j < NY; j++)
+          for (int i = 0; i < NX; i++)
+            for (int pp = 0; pp < NPOP; pp++) p[cell(i, j, k) * NPOP + pp] /= norm_all;
+    }
+  }
+  if (g && has(CH4_F_LB_TEMPERATURE)) {
+    for (int k = 0; k < NZ; k++)
+      for (int j = 0; j < NY; j++)
+        for (int i = 0; i < NX; i++) {
+          const double x = (double)i + 0.5, y = (double)j + 0.5, z = (double)k + 0.5;
+          double t = 0.0;
+          if (has(CH4_F_TEMPERATURE_INITIAL_LINEAR)) {  // 303-308
+            const double L = c.SY;
+            t = ((c.T_bot - c.T_ref) - (c.deltaT / L) * y);
+          }
+          if (has(CH4_F_TEMPERATURE_INITIAL_CONSTANT)) {  // 336-348
+            if (has(CH4_F_TEMPERATURE_INITIAL_CONSTANT_MEAN)) t = 0.5 * (c.T_top + c.T_bot);
+            if (has(CH4_F_TEMPERATURE_INITIAL_CONSTANT_BOT)) t = c.T_bot;
+            if (has(CH4_F_TEMPERATURE_INITIAL_CONSTANT_TOP)) t = c.T_top;
+          }
+          if (has(CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION)) {  // 411-420
+            const double val = 1.e-3;
+            if (NZ == 1) {
+              if (x < c.SX / 2) t += val;
+              else t -= val;
+            } else {
+              if (x < c.SX / 2 && z < c.SZ / 2) t += val;
+              else t -= val / 4.0;
+            }
+          }
+          if (has(CH4_F_TEMPERATURE_INITIAL_ADD_NOISE)) {  // 421-424
+            const double val = c.noise_t;
+            t += val * (2.0 * myrand48(rng) - 1.0);
+          }
+          double* f = g + cell(i, j, k) * NPOP;
+          for (int pp = 0; pp < NPOP; pp++) f[pp] = lat.w[pp] * t;  // 486-487
+        }
+  }
+  if (hs && has(CH4_F_LB_SCALAR)) {
+    for (int k = 0; k < NZ; k++)
+      for (int j = 0; j < NY; j++)
+        for (int i = 0; i < NX; i++) {
+          const double x = (double)i + 0.5, y = (double)j + 0.5, z = (double)k + 0.5;
+          double sv = 0.0;
+          if (has(CH4_F_SCALAR_INITIAL_LINEAR)) {  // 547-552
+            const double L = c.SY;
+            sv = ((c.S_bot - c.S_ref) - (c.deltaS / L) * y);
+          }
+          if (has(CH4_F_SCALAR_INITIAL_ADD_PERTURBATION)) {  // 554-560
+            if (NZ == 1) {
+              if (x < c.SX / 2) sv += 1.e-2;
+              else sv -= 1.e-2;
+            } else {
+              if (x < c.SX / 2 && z < c.SZ / 2) sv += 1.e-1;
+              else sv -= 0.25e-1;
+            }
+          }
+          if (has(CH4_F_SCALAR_INITIAL_CONSTANT)) {  // 562-575
+            if (has(CH4_F_SCALAR_INITIAL_CONSTANT_MEAN)) sv = 0.5 * (c.S_top + c.S_bot);
+            if (has(CH4_F_SCALAR_INITIAL_CONSTANT_BOT)) sv = c.S_bot;
+            if (has(CH4_F_SCALAR_INITIAL_CONSTANT_TOP)) sv = c.S_top;
+          }
+          double* f = hs + cell(i, j, k) * NPOP;
+          for (int pp = 0; pp < NPOP; pp++) f[pp] = lat.w[pp] * sv;  // 591-592
+        }
+  }
+  return CH4_OK;
+}
 
 }  // namespace
 
@@ -72,6 +235,8 @@ struct EngineBase {
   virtual ch4_status set_particles(const ch4_particle* parts, int n) = 0;
   virtual ch4_status get_particles(ch4_particle* parts, int n) = 0;
   virtual size_t device_bytes() const = 0;
+  // after a stream synchronisation: errors the kernels recorded on the device
+  virtual ch4_status check() { return CH4_OK; }
 };
 
 struct ch4_handle {
@@ -280,6 +445,7 @@ struct Engine : EngineBase {
   int *order = nullptr, *order2 = nullptr;
   double* rec = nullptr;
   int *cstart = nullptr, *cend = nullptr;
+  int* pstatus = nullptr;  // particle position check of the kernels (sticky until set_particles)
   void* cubtmp = nullptr;
   size_t cubbytes = 0;
   bool lagr() const { return (c.flags & CH4_F_LAGRANGE) != 0; }
@@ -316,6 +482,7 @@ struct Engine : EngineBase {
     cudaFree(dbuf[1]);
     cudaFree(cstart);
     cudaFree(cend);
+    cudaFree(pstatus);
   }
 
   void free_particles() {
@@ -358,6 +525,7 @@ struct Engine : EngineBase {
     Q.cell_start = cstart;
     Q.cell_end = cend;
     Q.dep = dbuf[dcur_i];
+    Q.status = pstatus;
     return Q;
   }
 
@@ -428,7 +596,11 @@ struct Engine : EngineBase {
       }
       np = n;
     }
+    if ((st = H->cuda(cudaMemset(pstatus, 0, sizeof(int)), "particle status"))) return st;
     if (n == 0) return CH4_OK;
+    for (int i = 0; i < n; i++)
+      if (!std::isfinite(parts[i].x) || !std::isfinite(parts[i].y) || !std::isfinite(parts[i].z))
+        return H->fail(CH4_ERR_ARG, "particle %d has a non-finite position", i);
     // AoS -> SoA with the two per-particle deposit constants (src/lagrange_feedback.c:84-90, host libm)
     std::vector<double> h((size_t)PF_TOTAL * n);
     const double* raw = reinterpret_cast<const double*>(parts);
@@ -441,6 +613,18 @@ struct Engine : EngineBase {
     }
     if ((st = H->cuda(cudaMemcpy(pf, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice), "particles up")))
       return st;
+    return CH4_OK;
+  }
+
+  ch4_status check() override {
+    if (!pstatus) return CH4_OK;
+    int flag = 0;
+    ch4_status st;
+    if ((st = H->cuda(cudaMemcpy(&flag, pstatus, sizeof(int), cudaMemcpyDeviceToHost), "particle status"))) return st;
+    if (flag)
+      return H->fail(CH4_ERR_NUMERIC,
+                     "a particle position left the box or became non-finite (the coupled particle-fluid "
+                     "integration diverged); the particle state is no longer meaningful");
     return CH4_OK;
   }
 
@@ -484,6 +668,10 @@ struct Engine : EngineBase {
     if (nsets_on[1] && cudaMalloc(&tprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tprev");
     if (nsets_on[2] && cudaMalloc(&sprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "sprev");
     if (lagr() && cudaMalloc(&upart, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u for particles");
+    if (lagr()) {
+      if (cudaMalloc(&pstatus, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "particle status");
+      if (cudaMemset(pstatus, 0, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "particle status");
+    }
     if (twoway()) {
       for (int b = 0; b < 2; b++) {
         if (cudaMalloc(&dbuf[b], 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "deposit");
@@ -834,6 +1022,8 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
       {"beta_s", &cfg->beta_s, S && (fl & CH4_F_SCALAR_BUOYANCY)},
       {"time_dt_lagr_factor", &cfg->time_dt_lagr_factor, (fl & CH4_F_LAGRANGE) != 0},
       {"particle_number", &particle_number, (fl & CH4_F_LAGRANGE) != 0},
+      {"noise_u", &cfg->noise_u, (fl & CH4_F_FLUID_INITIAL_ADD_NOISE) != 0},  // src/parameters.c:216-220
+      {"noise_t", &cfg->noise_t, T && (fl & CH4_F_TEMPERATURE_INITIAL_ADD_NOISE)},  // src/parameters.c:347-351
   };
   for (auto& k : keys) {
     if (!k.needed) continue;
@@ -914,6 +1104,27 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_TEMPERATURE_FORCING", CH4_F_TEMPERATURE_FORCING},
       {"LAGRANGE_WRAP", CH4_F_LAGRANGE_WRAP},
       {"LAGRANGE_GRADIENT_BRD2", CH4_F_LAGRANGE_GRADIENT_BRD2},
+      {"LB_FLUID_INITIAL_KOLMOGOROV", CH4_F_FLUID_INITIAL_KOLMOGOROV},
+      {"LB_FLUID_INITIAL_POISEUILLE", CH4_F_FLUID_INITIAL_POISEUILLE},
+      {"LB_FLUID_INITIAL_PERTURBATION", CH4_F_FLUID_INITIAL_PERTURBATION},
+      {"LB_FLUID_INITIAL_ADD_NOISE", CH4_F_FLUID_INITIAL_ADD_NOISE},
+      {"LB_FLUID_INITIAL_UNIT_DENSITY", CH4_F_FLUID_INITIAL_UNIT_DENSITY},
+      {"LB_INITIAL_BAROMETRIC", CH4_F_INITIAL_BAROMETRIC},
+      {"LB_FLUID_INITIAL_VORTICES", CH4_F_FLUID_INITIAL_VORTICES},
+      {"LB_FLUID_INITIAL_CELLULAR", CH4_F_FLUID_INITIAL_CELLULAR},
+      {"LB_TEMPERATURE_INITIAL_LINEAR", CH4_F_TEMPERATURE_INITIAL_LINEAR},
+      {"LB_TEMPERATURE_INITIAL_CONSTANT", CH4_F_TEMPERATURE_INITIAL_CONSTANT},
+      {"LB_TEMPERATURE_INITIAL_CONSTANT_MEAN", CH4_F_TEMPERATURE_INITIAL_CONSTANT_MEAN},
+      {"LB_TEMPERATURE_INITIAL_CONSTANT_BOT", CH4_F_TEMPERATURE_INITIAL_CONSTANT_BOT},
+      {"LB_TEMPERATURE_INITIAL_CONSTANT_TOP", CH4_F_TEMPERATURE_INITIAL_CONSTANT_TOP},
+      {"LB_TEMPERATURE_INITIAL_ADD_PERTURBATION", CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION},
+      {"LB_TEMPERATURE_INITIAL_ADD_NOISE", CH4_F_TEMPERATURE_INITIAL_ADD_NOISE},
+      {"LB_SCALAR_INITIAL_LINEAR", CH4_F_SCALAR_INITIAL_LINEAR},
+      {"LB_SCALAR_INITIAL_ADD_PERTURBATION", CH4_F_SCALAR_INITIAL_ADD_PERTURBATION},
+      {"LB_SCALAR_INITIAL_CONSTANT", CH4_F_SCALAR_INITIAL_CONSTANT},
+      {"LB_SCALAR_INITIAL_CONSTANT_MEAN", CH4_F_SCALAR_INITIAL_CONSTANT_MEAN},
+      {"LB_SCALAR_INITIAL_CONSTANT_BOT", CH4_F_SCALAR_INITIAL_CONSTANT_BOT},
+      {"LB_SCALAR_INITIAL_CONSTANT_TOP", CH4_F_SCALAR_INITIAL_CONSTANT_TOP},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -948,7 +1159,11 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       }
     for (const char* nn : neutral)
       if (name == nn) known = true;
-    if (!known && (name.rfind("DEBUG", 0) == 0 || name.find("_INITIAL_") != std::string::npos)) known = true;
+    if (!known && name.rfind("DEBUG", 0) == 0) known = true;
+    if (!known && name.find("_INITIAL_") != std::string::npos) {  // initial state the library does not build
+      flags |= CH4_F_INITIAL_OTHER;
+      known = true;
+    }
     if (!known) {
       put_bad(bad, bad_len, name);
       return CH4_ERR_UNSUPPORTED;
@@ -1013,9 +1228,7 @@ ch4_status ch4_create(const ch4_config* cfg, ch4_handle** out) {
   auto* h = new ch4_handle();
   h->cfg = *cfg;
   // srand48(seed) state (src/parallel.c:238-240 with a fixed seed)
-  h->rng[0] = 0x330E;
-  h->rng[1] = (unsigned short)(cfg->seed & 0xFFFF);
-  h->rng[2] = (unsigned short)((cfg->seed >> 16) & 0xFFFF);
+  seed48_state(cfg->seed, h->rng);
   std::memset(h->phi, 0, sizeof h->phi);
   for (int ii = 0; ii < NK; ii++) {
     double vk2 = VK[ii][0] * VK[ii][0] + VK[ii][1] * VK[ii][1] + VK[ii][2] * VK[ii][2];
@@ -1098,6 +1311,52 @@ ch4_status ch4_initialize(ch4_handle* h) {
   return st;
 }
 
+// HIT phases of initialization_forcing (src/initial_conditions.c:863-870): 18 draws
+static void draw_phases(unsigned short rng[3], double phi[NK][3]) {
+  for (int ii = 0; ii < NK; ii++)
+    for (int a = 0; a < 3; a++) phi[ii][a] = myrand48(rng);
+}
+
+ch4_status ch4_initial_populations(const ch4_config* cfg, double* p, double* g, double* hs, double* phi) {
+  if (!cfg || cfg->NX < 1 || cfg->NY < 1 || cfg->NZ < 1) return CH4_ERR_ARG;
+  if (cfg->flags & CH4_F_INITIAL_OTHER) return CH4_ERR_UNSUPPORTED;
+  unsigned short rng[3];
+  seed48_state(cfg->seed, rng);
+  static const Lattice lat;
+  ch4_status st = initial_fields(*cfg, lat, rng, p, g, hs);
+  if (st) return st;
+  if (phi) {
+    double ph[NK][3] = {};
+    if (cfg->flags & CH4_F_FORCING_HIT) draw_phases(rng, ph);
+    std::memcpy(phi, ph, sizeof ph);
+  }
+  return CH4_OK;
+}
+
+ch4_status ch4_initial_conditions(ch4_handle* h) {
+  if (!h) return CH4_ERR_ARG;
+  if (h->initialized) return h->fail(CH4_ERR_STATE, "ch4_initial_conditions after ch4_initialize");
+  const ch4_config& c = h->cfg;
+  if (c.flags & CH4_F_INITIAL_OTHER)
+    return h->fail(CH4_ERR_UNSUPPORTED, "define.h asks for an initial state the library does not build");
+  const size_t n = (size_t)c.NX * c.NY * c.NZ * NPOP;
+  std::vector<double> p(n), g, hs;
+  if (c.flags & CH4_F_LB_TEMPERATURE) g.resize(n);
+  if (c.flags & CH4_F_LB_SCALAR) hs.resize(n);
+  unsigned short rng[3];
+  seed48_state(c.seed, rng);
+  ch4_status st = initial_fields(c, h->lat, rng, p.data(), g.empty() ? nullptr : g.data(),
+                                 hs.empty() ? nullptr : hs.data());
+  if (st) return h->fail(st, "initial fields");
+  if ((st = h->eng->set_pop(0, p.data(), 0))) return st;
+  if (!g.empty() && (st = h->eng->set_pop(1, g.data(), 0))) return st;
+  if (!hs.empty() && (st = h->eng->set_pop(2, hs.data(), 0))) return st;
+  std::memset(h->phi, 0, sizeof h->phi);
+  if (c.flags & CH4_F_FORCING_HIT) draw_phases(rng, h->phi);
+  std::memcpy(h->rng, rng, sizeof rng);
+  return CH4_OK;
+}
+
 ch4_status ch4_step(ch4_handle* h, int nsteps) {
   if (!h || nsteps < 0) return CH4_ERR_ARG;
   if (!h->initialized) return h->fail(CH4_ERR_STATE, "ch4_step before ch4_initialize");
@@ -1106,7 +1365,8 @@ ch4_status ch4_step(ch4_handle* h, int nsteps) {
 
 ch4_status ch4_synchronize(ch4_handle* h) {
   if (!h) return CH4_ERR_ARG;
-  return h->cuda(cudaStreamSynchronize(h->stream), "synchronize");
+  ch4_status st = h->cuda(cudaStreamSynchronize(h->stream), "synchronize");
+  return st ? st : h->eng->check();
 }
 
 ch4_status ch4_get_stream(ch4_handle* h, void** stream) {
@@ -1561,6 +1821,12 @@ ch4_status ch4_ensemble_step(ch4_ensemble* E, int nsteps) {
 ch4_status ch4_ensemble_synchronize(ch4_ensemble* E) {
   if (!E) return CH4_ERR_ARG;
   return E->cuda(cudaStreamSynchronize(E->stream), "synchronize");
+}
+
+ch4_status ch4_ensemble_get_stream(ch4_ensemble* E, void** stream) {
+  if (!E || !stream) return CH4_ERR_ARG;
+  *stream = static_cast<void*>(E->stream);
+  return CH4_OK;
 }
 
 ch4_status ch4_ensemble_itime(const ch4_ensemble* E, int slot, int* itime) {

@@ -46,6 +46,7 @@ struct PartParams {
   int* cell_start;       // [(NX+1)(NY+1)(NZ+1)]
   int* cell_end;
   A* dep;                // 3 SoA planes, output
+  int* status;           // set to 1 when a particle position is outside [0, S] or not finite
 };
 
 #ifdef __CUDACC__
@@ -80,6 +81,24 @@ struct Stencil {
   double dxm, dxp, dym, dyp, dzm, dzp;
   double vol[8];
 };
+
+// Wrapped position of a particle, checked: a position outside [0, S] on any axis
+// (non-finite, or too large for one wrap to bring back, as after a numerical
+// blow-up) is reported through P.status and replaced by the origin, so that every
+// stencil index stays inside the lattice whatever the particle state holds.
+template <typename A>
+__device__ __forceinline__ bool wrapped_position(const PartParams<A>& P, double x, double y, double z, double& px,
+                                                 double& py, double& pz) {
+  px = pwrapd(x, P.SX);
+  py = pwrapd(y, P.SY);
+  pz = pwrapd(z, P.SZ);
+  const bool ok = px >= 0.0 && px <= P.SX && py >= 0.0 && py <= P.SY && pz >= 0.0 && pz <= P.SZ;
+  if (!ok) {
+    atomicOr(P.status, 1);
+    px = py = pz = 0.0;
+  }
+  return ok;
+}
 
 // cell search of src/lagrange.c:1253-1264 on the unit grid (center_V = index + 0.5)
 __device__ __forceinline__ void make_stencil(double px, double py, double pz, Stencil& t) {
@@ -119,7 +138,9 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
 #define F(name) pf[(long long)CH4_PF(name) * np + ip]
   // ---- interpolate_vector_at_particles
   Stencil t;
-  make_stencil(pwrapd(F(x), P.SX), pwrapd(F(y), P.SY), pwrapd(F(z), P.SZ), t);
+  double px, py, pz;
+  wrapped_position(P, F(x), F(y), F(z), px, py, pz);
+  make_stencil(px, py, pz, t);
   double v[3];
   for (int a = 0; a < 3; a++) {
     double acc = 0.0;
@@ -272,9 +293,11 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   const int np = P.np;
 #define F(name) pf[(long long)CH4_PF(name) * np + ip]
   Stencil t;
-  make_stencil(pwrapd(F(x), P.SX), pwrapd(F(y), P.SY), pwrapd(F(z), P.SZ), t);
+  double px, py, pz;
+  const bool inside = wrapped_position(P, F(x), F(y), F(z), px, py, pz);
+  make_stencil(px, py, pz, t);
   const double fac = pf[(long long)PF_VOL * np + ip], dr = pf[(long long)PF_DR * np + ip];
-  const bool live = (fac > 0.0) && F(beta_coeff) != 0.0;
+  const bool live = inside && (fac > 0.0) && F(beta_coeff) != 0.0;
   const double gx = 0.0, gy = 0.0, gz = 0.0;
   double* r = P.rec;
   r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;

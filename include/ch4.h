@@ -69,7 +69,32 @@ enum {
   CH4_F_LAGRANGE_TWOWAY_MOMENTUM = 1ull << 24,
   CH4_F_TEMPERATURE_FORCING = 1ull << 25,  /* t_source (plain source term), src/forcing.c:769,1475 */
   CH4_F_LAGRANGE_WRAP = 1ull << 26,
-  CH4_F_LAGRANGE_GRADIENT_BRD2 = 1ull << 27
+  CH4_F_LAGRANGE_GRADIENT_BRD2 = 1ull << 27,
+  /* initial fields of ch4_initial_conditions (src/initial_conditions.c:3-500) */
+  CH4_F_FLUID_INITIAL_KOLMOGOROV = 1ull << 28,          /* 112-122 */
+  CH4_F_FLUID_INITIAL_POISEUILLE = 1ull << 29,          /* 147-158 */
+  CH4_F_FLUID_INITIAL_PERTURBATION = 1ull << 30,        /* 226-231, drand48 */
+  CH4_F_FLUID_INITIAL_ADD_NOISE = 1ull << 31,           /* 233-242, drand48, param noise_u */
+  CH4_F_FLUID_INITIAL_UNIT_DENSITY = 1ull << 32,        /* 256-279 */
+  CH4_F_INITIAL_BAROMETRIC = 1ull << 33,                /* 77-88, with LB_TEMPERATURE_BUOYANCY */
+  CH4_F_FLUID_INITIAL_VORTICES = 1ull << 34,            /* 98-110 */
+  CH4_F_FLUID_INITIAL_CELLULAR = 1ull << 35,            /* 124-145 */
+  CH4_F_TEMPERATURE_INITIAL_LINEAR = 1ull << 36,        /* 303-308 */
+  CH4_F_TEMPERATURE_INITIAL_CONSTANT = 1ull << 37,      /* 336-349, with one of the three below */
+  CH4_F_TEMPERATURE_INITIAL_CONSTANT_MEAN = 1ull << 38,
+  CH4_F_TEMPERATURE_INITIAL_CONSTANT_BOT = 1ull << 39,
+  CH4_F_TEMPERATURE_INITIAL_CONSTANT_TOP = 1ull << 40,
+  CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION = 1ull << 41,  /* 411-420 */
+  CH4_F_TEMPERATURE_INITIAL_ADD_NOISE = 1ull << 42,     /* 421-424, drand48, param noise_t */
+  CH4_F_SCALAR_INITIAL_LINEAR = 1ull << 43,             /* 583-589 */
+  CH4_F_SCALAR_INITIAL_ADD_PERTURBATION = 1ull << 44,
+  CH4_F_SCALAR_INITIAL_CONSTANT = 1ull << 45,
+  CH4_F_SCALAR_INITIAL_CONSTANT_MEAN = 1ull << 46,
+  CH4_F_SCALAR_INITIAL_CONSTANT_BOT = 1ull << 47,
+  CH4_F_SCALAR_INITIAL_CONSTANT_TOP = 1ull << 48,
+  /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
+   * (the caller can still set the populations itself) */
+  CH4_F_INITIAL_OTHER = 1ull << 63
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
@@ -113,6 +138,8 @@ typedef struct {
    * not treated as the start (src/lagrange.c:3190 itime==1 && resume==0,
    * src/main.c:124-128 two-way coupling from the first step) */
   int resume;
+  /* amplitudes of LB_FLUID_INITIAL_ADD_NOISE / LB_TEMPERATURE_INITIAL_ADD_NOISE */
+  double noise_u, noise_t;
 } ch4_config;
 
 /* One Lagrangian particle (the fields of point_particle, src/typedef.h:391-481,
@@ -184,9 +211,23 @@ ch4_status ch4_get_pop(ch4_handle *h, char which, double *aos, int brd);
 ch4_status ch4_set_hit_phases(ch4_handle *h, const double *phi);
 ch4_status ch4_get_hit_phases(ch4_handle *h, double *phi);
 
-/* Particles (src/lagrange.c:72 initial_conditions_particles / part.h5). */
+/* Particles (src/lagrange.c:72 initial_conditions_particles / part.h5).
+ * Non-finite positions are refused (CH4_ERR_ARG). */
 ch4_status ch4_set_particles(ch4_handle *h, const ch4_particle *parts, int n);
 ch4_status ch4_get_particles(ch4_handle *h, ch4_particle *parts, int n);
+
+/* Initial fields of initial_conditions (src/initial_conditions.c:3-500) for the
+ * CH4_F_*_INITIAL_* flags, computed on the host: p, g, h as AoS [NZ][NY][NX][19]
+ * (no halo; a pointer may be NULL when its set is off), and the HIT phases that
+ * initialization_forcing draws next (phi[6*3], may be NULL).  The drand48 stream
+ * is consumed in the reference's order (the noise draws, then the phases).
+ * Host only: needs no device.  CH4_ERR_UNSUPPORTED for CH4_F_INITIAL_OTHER. */
+ch4_status ch4_initial_populations(const ch4_config *cfg, double *p, double *g, double *h, double *phi);
+
+/* The same applied to a handle, before ch4_initialize: uploads p, g, h and sets
+ * the HIT phases and the host random stream as after src/main.c:22-23
+ * (initial_conditions, initialization_forcing). */
+ch4_status ch4_initial_conditions(ch4_handle *h);
 
 /* --- the time step ---------------------------------------------------------- */
 
@@ -199,7 +240,9 @@ ch4_status ch4_initialize(ch4_handle *h);
  * particle sub-steps.  Asynchronous with respect to the host. */
 ch4_status ch4_step(ch4_handle *h, int nsteps);
 
-/* Wait for the handle's stream. */
+/* Wait for the handle's stream.  CH4_ERR_NUMERIC when a particle position has
+ * left the box or become non-finite since ch4_set_particles (a diverged run: the
+ * kernels keep every access inside the lattice and record it instead). */
 ch4_status ch4_synchronize(ch4_handle *h);
 
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own
@@ -246,6 +289,9 @@ ch4_status ch4_ensemble_initialize(ch4_ensemble *e, int slot);
  * one persistent work-queue launch per step).  Asynchronous. */
 ch4_status ch4_ensemble_step(ch4_ensemble *e, int nsteps);
 ch4_status ch4_ensemble_synchronize(ch4_ensemble *e);
+/* The ensemble's CUDA stream (cudaStream_t) for the caller's own events; no
+ * reference counterpart. */
+ch4_status ch4_ensemble_get_stream(ch4_ensemble *e, void **stream);
 ch4_status ch4_ensemble_get_fields(ch4_ensemble *e, int slot, double *dens, double *u, double *t, double *s, int brd);
 ch4_status ch4_ensemble_averages(ch4_ensemble *e, int slot, ch4_averages *out);
 ch4_status ch4_ensemble_itime(const ch4_ensemble *e, int slot, int *itime);

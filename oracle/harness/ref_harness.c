@@ -15,6 +15,8 @@
  *                                  build_forcing call, i.e. after
  *                                  initialization_forcing, src/initial_conditions.c:822)
  *   in_part.bin                    npart*SIZE_OF_POINT_PARTICLE doubles
+ * out_phi0.bin: the HIT phases right after initialization_forcing (before the
+ *   first build_forcing walks them).
  * Outputs after <nsteps> steps (same layouts):
  *   out_p.bin out_g.bin out_h.bin out_u.bin (3 per cell) out_dens.bin out_t.bin
  *   out_s.bin out_force.bin (3 per cell) out_phi.bin out_part.bin
@@ -108,6 +110,17 @@ static void write_part_layout(void) {
 }
 #endif
 
+#ifdef LB_FLUID_FORCING_HIT
+static void write_phases(const char *name) {
+  FILE *fp = fopen(name, "wb");
+  for (int ii = 0; ii < nk; ii++) {
+    double v[3] = {(double)phi_u[ii].x, (double)phi_u[ii].y, (double)phi_u[ii].z};
+    fwrite(v, sizeof(double), 3, fp);
+  }
+  fclose(fp);
+}
+#endif
+
 static void dump_state(void) {
 #ifdef LB_FLUID
   write_pop("out_p.bin", p);
@@ -117,14 +130,7 @@ static void dump_state(void) {
   write_vector("out_force.bin", force);
 #endif
 #ifdef LB_FLUID_FORCING_HIT
-  {
-    FILE *fp = fopen("out_phi.bin", "wb");
-    for (int ii = 0; ii < nk; ii++) {
-      double v[3] = {(double)phi_u[ii].x, (double)phi_u[ii].y, (double)phi_u[ii].z};
-      fwrite(v, sizeof(double), 3, fp);
-    }
-    fclose(fp);
-  }
+  write_phases("out_phi.bin");
 #endif
 #endif
 #ifdef LB_TEMPERATURE
@@ -214,6 +220,7 @@ int main(int argc, char **argv) {
       }
       fclose(fp);
     }
+    write_phases("out_phi0.bin"); /* as initialization_forcing left them (or injected) */
   }
 #endif
 

@@ -44,6 +44,16 @@ FLAGSETS = {
             "LB_FLUID_BC_Y", "LB_FLUID_LES"],
     "particles": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                   "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    "init_rb": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+                "LB_TEMPERATURE_BC_Y", "LB_SCALAR", "LB_SCALAR_BC_Y", "LB_INITIAL_BAROMETRIC",
+                "LB_FLUID_INITIAL_PERTURBATION", "LB_FLUID_INITIAL_ADD_NOISE", "LB_FLUID_INITIAL_UNIT_DENSITY",
+                "LB_TEMPERATURE_INITIAL_LINEAR", "LB_TEMPERATURE_INITIAL_ADD_PERTURBATION",
+                "LB_TEMPERATURE_INITIAL_ADD_NOISE", "LB_SCALAR_INITIAL_LINEAR", "LB_SCALAR_INITIAL_ADD_PERTURBATION"],
+    "init_hit": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE", "LB_SCALAR",
+                 "LB_FLUID_INITIAL_VORTICES", "LB_FLUID_INITIAL_KOLMOGOROV", "LB_FLUID_INITIAL_CELLULAR",
+                 "LB_FLUID_INITIAL_POISEUILLE", "LB_FLUID_INITIAL_PERTURBATION", "LB_TEMPERATURE_INITIAL_CONSTANT",
+                 "LB_TEMPERATURE_INITIAL_CONSTANT_MEAN", "LB_TEMPERATURE_INITIAL_ADD_NOISE",
+                 "LB_SCALAR_INITIAL_CONSTANT", "LB_SCALAR_INITIAL_CONSTANT_TOP"],
 }
 # non-flag configuration implied by a flag set (define.h variants of one setting)
 FLAGSET_EXTRA = {"walls2": {"t0_kind": abi.T0_REF}}
@@ -89,7 +99,7 @@ PARAM_KEYS = ["resume", "resume_u", "resume_t", "resume_s", "NX", "NY", "NZ", "S
               "tau_s", "S_bot", "S_top", "S_ref", "beta_s",
               "time_dt_lagr_factor", "time_dump_lagr", "particle_number",
               "tau_drag_types", "tau_drag_min", "tau_drag_max",
-              "beta_coeff_types", "beta_coeff_min", "beta_coeff_max"]
+              "beta_coeff_types", "beta_coeff_min", "beta_coeff_max", "noise_u", "noise_t"]
 
 
 def write_param_in(path, cfg, nsteps=1):
@@ -166,7 +176,7 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None,
     out = {}
     shapes = {"p": (NZ, NY, NX, NPOP), "g": (NZ, NY, NX, NPOP), "h": (NZ, NY, NX, NPOP),
               "u": (NZ, NY, NX, 3), "force": (NZ, NY, NX, 3), "dens": (NZ, NY, NX),
-              "t": (NZ, NY, NX), "s": (NZ, NY, NX), "phi": (abi.NK, 3)}
+              "t": (NZ, NY, NX), "s": (NZ, NY, NX), "phi": (abi.NK, 3), "phi0": (abi.NK, 3)}
     for name, shape in shapes.items():
         fn = os.path.join(tmp, "out_%s.bin" % name)
         if os.path.exists(fn):

@@ -95,8 +95,11 @@ def test_ensemble_fp32_close_to_fp64_oracle():
         ref = run_restatement(cfg64, st, 60)
         # FP32 arithmetic and storage: T within 1e-5 relative L2 after 60 steps
         assert np.linalg.norm(m["t"] - ref["t"]) / np.linalg.norm(ref["t"]) < 1e-5
-        # Nusselt number (dump_averages nuy) within 1e-4 relative
-        assert abs(m["avg"]["nuy"] - ref["avg"]["nuy"]) <= 1e-4 * abs(ref["avg"]["nuy"])
+        # Nusselt number (dump_averages nuy = <u_y T - kappa dT/dy> / (kappa dT / H)): the FP32
+        # velocity carries about one unit roundoff (2^-24) of error, which the division by the
+        # small conductive flux kappa*dT/H (1e-4 .. 5e-4 here) amplifies; allow 4 unit roundoffs
+        flux = cfg64.kappa * (cfg64.T_bot - cfg64.T_top) / cfg64.SY
+        assert abs(m["avg"]["nuy"] - ref["avg"]["nuy"]) <= 4 * 2.0 ** -24 / flux
 
 
 def test_tuner_keeps_state():
