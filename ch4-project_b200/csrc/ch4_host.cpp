@@ -439,6 +439,7 @@ struct Engine : EngineBase {
   int np = 0;
   double* pf = nullptr;   // [PF_TOTAL][np]
   A* upart = nullptr;     // u^{n+1} for the interpolation, 3 planes
+  A* tpart = nullptr;     // t^{n+1} for the interpolation (LB_TEMPERATURE)
   A* dbuf[2] = {nullptr, nullptr};  // two-way deposit of this / previous step
   int dcur_i = 0;
   unsigned int *key = nullptr, *key2 = nullptr;
@@ -478,6 +479,7 @@ struct Engine : EngineBase {
     if (hit_ev) cudaEventDestroy(hit_ev);
     free_particles();
     cudaFree(upart);
+    cudaFree(tpart);
     cudaFree(dbuf[0]);
     cudaFree(dbuf[1]);
     cudaFree(cstart);
@@ -519,6 +521,7 @@ struct Engine : EngineBase {
     Q.addedmass = (c.flags & CH4_F_LAGRANGE_ADDEDMASS) != 0;
     Q.pf = pf;
     Q.u = upart;
+    Q.t = tpart;
     Q.key = key;
     Q.order = order;
     Q.rec = rec;
@@ -668,6 +671,8 @@ struct Engine : EngineBase {
     if (nsets_on[1] && cudaMalloc(&tprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tprev");
     if (nsets_on[2] && cudaMalloc(&sprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "sprev");
     if (lagr() && cudaMalloc(&upart, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u for particles");
+    if (lagr() && nsets_on[1] && cudaMalloc(&tpart, N * sizeof(A)) != cudaSuccess)
+      return H->fail(CH4_ERR_NOMEM, "t for particles");
     if (lagr()) {
       if (cudaMalloc(&pstatus, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "particle status");
       if (cudaMemset(pstatus, 0, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "particle status");
@@ -890,7 +895,7 @@ struct Engine : EngineBase {
           // u^{n+1} with dt/2 F^n, then the Lagrangian sub-steps (src/main.c:164-185)
           bind_pops(cur);
           if ((st = H->cuda(launch_hydro(P, shape, P.hit_cur, twoway() ? P.dcur : nullptr, nullptr, nullptr, nullptr,
-                                         nullptr, nullptr, upart, H->stream),
+                                         nullptr, nullptr, upart, H->stream, tpart),
                             "particle u")))
             return st;
           PartParams<A> Q = part_params();
@@ -1194,8 +1199,9 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
     return why = "walls need NY >= 3", CH4_ERR_ARG;
   if (!(c->tau_u > 0.5)) return why = "tau_u must exceed 0.5", CH4_ERR_ARG;
   if (c->flags & CH4_F_LAGRANGE) {
-    if (c->flags & (CH4_F_FLUID_BC_Y | CH4_F_LB_TEMPERATURE | CH4_F_LB_SCALAR))
-      return why = "particles are implemented for the periodic fluid-only box", CH4_ERR_UNSUPPORTED;
+    if (c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_LB_SCALAR))
+      return why = "particles are implemented for the periodic box (fluid, optionally temperature)",
+             CH4_ERR_UNSUPPORTED;
     if (!(c->flags & CH4_F_LAGRANGE_WRAP)) return why = "particles need LAGRANGE_WRAP", CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_LAGRANGE_TWOWAY) && !(c->flags & CH4_F_LAGRANGE_TWOWAY_MOMENTUM))
       return why = "LAGRANGE_TWOWAY is implemented with LAGRANGE_TWOWAY_MOMENTUM", CH4_ERR_UNSUPPORTED;

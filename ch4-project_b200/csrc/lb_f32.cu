@@ -15,9 +15,10 @@ cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStre
   return s.storage == 2 ? init_prev_t<__half, float>(P, s, st) : init_prev_t<float, float>(P, s, st);
 }
 cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep, double* dens,
-                         double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st) {
-  return s.storage == 2 ? hydro_t<__half, float>(P, s, hit, dep, dens, u, t, sc, force, u_arith, st)
-                        : hydro_t<float, float>(P, s, hit, dep, dens, u, t, sc, force, u_arith, st);
+                         double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
+                         float* t_arith) {
+  return s.storage == 2 ? hydro_t<__half, float>(P, s, hit, dep, dens, u, t, sc, force, u_arith, t_arith, st)
+                        : hydro_t<float, float>(P, s, hit, dep, dens, u, t, sc, force, u_arith, t_arith, st);
 }
 cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st) {

@@ -15,8 +15,9 @@ cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStr
   return init_prev_t<double, double>(P, s, st);
 }
 cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep, double* dens,
-                         double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st) {
-  return hydro_t<double, double>(P, s, hit, dep, dens, u, t, sc, force, u_arith, st);
+                         double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st,
+                         double* t_arith) {
+  return hydro_t<double, double>(P, s, hit, dep, dens, u, t, sc, force, u_arith, t_arith, st);
 }
 cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st) {

@@ -186,10 +186,11 @@ __global__ void init_prev_kernel(const StepParams<A> P) {
 
 // hydro_fields (src/lb.c:420-539): dens, u (with dt/2 of the force built from the
 // kept temperature and the given phase table), t, s -- all as FP64 SoA planes.
-// Also the force field itself when `force` is non-null.
+// Also the force field itself when `force` is non-null, and u and t in the
+// arithmetic precision for the particle interpolation (u_arith, t_arith).
 template <typename S, typename A, bool THERM, bool SCAL>
 __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, double* dens, double* u, double* t,
-                             double* s, double* force, A* u_arith) {
+                             double* s, double* force, A* u_arith, A* t_arith) {
   const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (idx >= P.N) return;
   const int x = (int)(idx % P.NX);
@@ -224,10 +225,12 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
     force[2 * P.N + idx] = (double)Fz;
   }
   if constexpr (THERM) {
-    if (t) {
+    if (t || t_arith) {
       A g[Q];
       load_set<S, A, 1>(P, idx, g);
-      t[idx] = (double)mom0(g);
+      const A tt = mom0(g);
+      if (t) t[idx] = (double)tt;
+      if (t_arith) t_arith[idx] = tt;
     }
   }
   if constexpr (SCAL) {

@@ -39,6 +39,7 @@ struct PartParams {
   int addedmass;  // LAGRANGE_ADDEDMASS
   double* pf;     // [PF_TOTAL][np]
   const A* u;     // 3 SoA planes of u^{n+1}
+  const A* t;     // t^{n+1} = m(g^{n+1}) with LB_TEMPERATURE, else null
   // deposit
   unsigned int* key;     // home cell per particle (sorted in place by the caller)
   int* order;            // particle index per sorted slot
@@ -74,6 +75,26 @@ __device__ double grad_at(const PartParams<A>& P, int a, int b, int i, int j, in
     return 1.5 * u_at(P, a, i, j, k) + -2.0 * u_at(P, a, i - di, j - dj, k - dk) +
            0.5 * u_at(P, a, i - 2 * di, j - 2 * dj, k - 2 * dk);
   return (u_at(P, a, i + di, j + dj, k + dk) - u_at(P, a, i - di, j - dj, k - dk)) / 2.0;
+}
+
+template <typename A>
+__device__ __forceinline__ double t_at(const PartParams<A>& P, int i, int j, int k) {
+  const long long c = ((long long)pwrapi(k, P.NZ) * P.NY + pwrapi(j, P.NY)) * P.NX + pwrapi(i, P.NX);
+  return (double)P.t[c];
+}
+
+// d t / d x_b on a stencil cell, gradient_scalar with LAGRANGE_INTERPOLATION_FIX
+// (src/gradients.c:505-520, 731-800): the same rule as grad_at
+template <typename A>
+__device__ double tgrad_at(const PartParams<A>& P, int b, int i, int j, int k) {
+  const int n = b == 0 ? P.NX : b == 1 ? P.NY : P.NZ;
+  const int c = b == 0 ? i : b == 1 ? j : k;
+  const int di = b == 0, dj = b == 1, dk = b == 2;
+  if (c == -1)
+    return -1.5 * t_at(P, i, j, k) + 2.0 * t_at(P, i + di, j + dj, k + dk) + -0.5 * t_at(P, i + 2 * di, j + 2 * dj, k + 2 * dk);
+  if (c == n)
+    return 1.5 * t_at(P, i, j, k) + -2.0 * t_at(P, i - di, j - dj, k - dk) + 0.5 * t_at(P, i - 2 * di, j - 2 * dj, k - 2 * dk);
+  return (t_at(P, i + di, j + dj, k + dk) - t_at(P, i - di, j - dj, k - dk)) / 2.0;
 }
 
 struct Stencil {
@@ -181,9 +202,49 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     F(dy_uz) = gr[7];
     F(dz_uz) = gr[8];
   }
+  // ---- interpolate_scalar_at_particles(t, 't') (src/lagrange.c:1442-1593)
+  if (P.t) {
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      int di, dj, dk;
+      corner(c, di, dj, dk);
+      const double term = t_at(P, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
+      acc = c == 0 ? term : acc + term;
+    }
+    F(t) = acc;
+    if (P.gradient) {
+      double gt[3];
+      for (int b = 0; b < 3; b++) {
+        double g = 0.0;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+          int di, dj, dk;
+          corner(c, di, dj, dk);
+          const double term = tgrad_at(P, b, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
+          g = c == 0 ? term : g + term;
+        }
+        gt[b] = g;
+      }
+      F(dx_t) = gt[0];
+      F(dy_t) = gt[1];
+      F(dz_t) = gt[2];
+    }
+  }
   // ---- move_particles (src/lagrange.c:3040-3440)
   const double dtl = P.dtl;
   const bool first = P.first != 0;
+  if (P.t) {  // time derivatives of t along the path, src/lagrange.c:2997-3010
+    if (first) {
+      F(t_old) = F(t);
+    } else {
+      const double tnow = F(t);
+      F(dt_t) = (tnow - F(t_old)) / dtl;
+      F(t_old) = tnow;
+      if (P.gradient)
+        F(Dt_t) = F(dt_t) + (ux - F(vx)) * F(dx_t) + (uy - F(vy)) * F(dy_t) + (uz - F(vz)) * F(dz_t);
+    }
+  }
   const double tau = F(tau_drag);
   if (tau < 0.0) {  // Eulerian probe
     F(vx) = ux;

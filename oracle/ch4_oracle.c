@@ -62,7 +62,7 @@ struct ch4o_state {
   ch4_particle *part;
   double *pvol, *pdr; /* per-particle volume (4/3 pi r^3) and rho_p/rho_f */
   /* two-way deposit of this and the previous step, velocity field for the particles */
-  double *dcur, *dprev, *uf;
+  double *dcur, *dprev, *uf, *tf;
 };
 
 /* ---- host RNG: drand48 stream (src/random.c:4-16 with SYSTEM_RANDOM48) ---- */
@@ -312,6 +312,30 @@ static double grad_at(const ch4o_state *s, const double *u, int a, int b, int i,
   return (uat(s, u, a, i + di, j + dj, k + dk) - uat(s, u, a, i - di, j - dj, k - dk)) / 2.0;
 }
 
+/* scalar field at interior coordinates in [-1, N] (periodic halo) */
+static inline double tat(const ch4o_state *s, const double *t, int i, int j, int k) {
+  return t[cidx(s, pwrap(i, s->NX), pwrap(j, s->NY), pwrap(k, s->NZ))];
+}
+
+/* d t / d x_b at a cell of the particle stencil: gradient_scalar with LAGRANGE
+ * (src/gradients.c:505-520) and LAGRANGE_INTERPOLATION_FIX, SECOND_ORDER_GRAD on the
+ * first halo layer of a box without temperature walls (src/gradients.c:731-800) */
+static double tgrad_at(const ch4o_state *s, const double *t, int b, int i, int j, int k) {
+  const int n = b == 0 ? s->NX : b == 1 ? s->NY : s->NZ;
+  const int c = b == 0 ? i : b == 1 ? j : k;
+  const int di = b == 0, dj = b == 1, dk = b == 2;
+  const double h1 = 1.0, h2 = 1.0;
+  if (c == -1) {
+    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
+    return a0 * tat(s, t, i, j, k) + a1 * tat(s, t, i + di, j + dj, k + dk) + a2 * tat(s, t, i + 2 * di, j + 2 * dj, k + 2 * dk);
+  }
+  if (c == n) {
+    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
+    return a0 * tat(s, t, i, j, k) + a1 * tat(s, t, i - di, j - dj, k - dk) + a2 * tat(s, t, i - 2 * di, j - 2 * dj, k - 2 * dk);
+  }
+  return (tat(s, t, i + di, j + dj, k + dk) - tat(s, t, i - di, j - dj, k - dk)) / 2.0;
+}
+
 /* cell of the stencil and the six distances (src/lagrange.c:1231-1287) */
 typedef struct {
   int im, jm, km;
@@ -385,9 +409,45 @@ static void interp_particle(const ch4o_state *s, const double *u, ch4_particle *
   }
 }
 
+/* interpolate_scalar_at_particles(t, 't'), src/lagrange.c:1442-1593 */
+static void interp_particle_t(const ch4o_state *s, const double *tf, ch4_particle *p) {
+  stencil_t t;
+  stencil(s, p, &t);
+  double acc = 0.0;
+  for (int c = 0; c < 8; c++) {
+    double term = tat(s, tf, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2]) * t.vol[c];
+    acc = c == 0 ? term : acc + term;
+  }
+  p->t = acc;
+  if (s->cfg.flags & CH4_F_LAGRANGE_GRADIENT) {
+    double g[3];
+    for (int b = 0; b < 3; b++) {
+      double a = 0.0;
+      for (int c = 0; c < 8; c++) {
+        double term = tgrad_at(s, tf, b, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2]) * t.vol[c];
+        a = c == 0 ? term : a + term;
+      }
+      g[b] = a;
+    }
+    p->dx_t = g[0];
+    p->dy_t = g[1];
+    p->dz_t = g[2];
+  }
+}
+
 /* move_particles for point particles, src/lagrange.c:2934-3470 (tracers
  * tau_drag == 0, Eulerian probes tau_drag < 0, Stokes drag + added mass) */
 static void move_particle(const ch4o_state *s, ch4_particle *p, int first, double dtl) {
+  if (s->tf) { /* time derivatives of t along the path, src/lagrange.c:2997-3010 */
+    if (first) {
+      p->t_old = p->t;
+    } else {
+      p->dt_t = (p->t - p->t_old) / dtl;
+      p->t_old = p->t;
+      if (s->cfg.flags & CH4_F_LAGRANGE_GRADIENT)
+        p->Dt_t = p->dt_t + (p->ux - p->vx) * p->dx_t + (p->uy - p->vy) * p->dy_t + (p->uz - p->vz) * p->dz_t;
+    }
+  }
   if (p->tau_drag < 0.0) {
     p->vx = p->ux;
     p->vy = p->uy;
@@ -719,11 +779,13 @@ static void one_step(ch4o_state *s) {
   /* Lagrangian sub-steps, src/main.c:164-185: u^{n+1} with dt/2 F^n, then
    * interpolate + move + wrap time_dt_lagr_factor times */
   if (c->flags & CH4_F_LAGRANGE) {
-    hydro(s, s->hit_cur, s->dcur, NULL, s->uf, NULL, NULL);
+    hydro(s, s->hit_cur, s->dcur, NULL, s->uf, s->tf, NULL);
     const double dtl = c->time_dt / c->time_dt_lagr_factor;
     const int first = (s->itime == 1 && c->resume == 0);
     for (int sub = 0; sub < (int)c->time_dt_lagr_factor; sub++) {
       for (int ip = 0; ip < s->npart; ip++) interp_particle(s, s->uf, &s->part[ip]);
+      if (s->tf)
+        for (int ip = 0; ip < s->npart; ip++) interp_particle_t(s, s->tf, &s->part[ip]);
       for (int ip = 0; ip < s->npart; ip++) move_particle(s, &s->part[ip], first, dtl);
       wrap_particles(s);
     }
@@ -766,6 +828,8 @@ int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
     s->dprev = (double *)calloc(3 * s->N, sizeof(double));
   }
   if (cfg->flags & CH4_F_LAGRANGE) s->uf = (double *)calloc(3 * s->N, sizeof(double));
+  if ((cfg->flags & CH4_F_LAGRANGE) && (cfg->flags & CH4_F_LB_TEMPERATURE))
+    s->tf = (double *)calloc(s->N, sizeof(double));
   s->tau_les = (double *)calloc(s->N, sizeof(double));
   /* constant force tables */
   const double LX = cfg->SX, LY = cfg->SY, nu = cfg->nu;
@@ -828,6 +892,7 @@ int ch4o_destroy(ch4o_state *s) {
   free(s->dcur);
   free(s->dprev);
   free(s->uf);
+  free(s->tf);
   free(s);
   return CH4_OK;
 }

@@ -1,6 +1,6 @@
 """Generate tests/golden/<case>.npz from the reference solver compiled by oracle/Makefile.
 
-Run here, where the reference sources exist:  python tests/golden/make_golden.py
+Run here, where the reference sources exist:  python tests/golden/make_golden.py [case ...]
 Each fixture holds the seeded inputs (in_*), the step count and the reference's
 outputs (out_*) after that many steps; tests/test_oracle_pin.py checks the oracle
 restatement against them.
@@ -22,12 +22,13 @@ from lbcases import CASES, make_case, pop_items  # noqa: E402
 NSTEPS = 12
 SEED = 7
 
-for name in sorted(CASES):
+for name in sys.argv[1:] or sorted(CASES):
     flagset, cfg, state = make_case(name, seed=SEED)
     ref = O.run_reference(flagset, cfg, NSTEPS, dict(pop_items(state)), parts=state.get("part"))
     out = {"seed": SEED, "nsteps": NSTEPS}
     if "part" in ref:
-        for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux"):
+        temperature = ("t", "dt_t", "Dt_t", "dx_t") if "t" in ref["part"] else ()
+        for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux") + temperature:
             out["out_part_" + f] = ref["part"][f]
     for k, v in pop_items(state):
         out["in_sha256_" + k] = hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()

@@ -44,6 +44,10 @@ CASES = {
     "particles": dict(flagset="particles", NX=10, NY=8, NZ=7, npart=300,
                       params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=6,
                                   time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_t": dict(flagset="particles_t", NX=9, NY=8, NZ=7, npart=250,
+                        params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=5,
+                                    T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
+                                    time_dt_lagr_factor=2.0, particle_number=250)),
 }
 
 

@@ -22,7 +22,8 @@ def _assert_same(a, b, what):
 
 
 @pytest.mark.parametrize("name,nsteps", [("kolmogorov", 20), ("rb", 20), ("hit", 15), ("walls2", 20),
-                                          ("scalar", 20), ("les", 20), ("particles", 8)])
+                                          ("scalar", 20), ("les", 20), ("particles", 8),
+                                          ("particles_t", 8)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
@@ -74,7 +75,7 @@ def test_restatement_matches_golden_fixture(name):
     mine = run_restatement(cfg, state, int(g["nsteps"]))
     for k, _ in pop_items(state):
         _assert_same(mine[k], g["out_" + k], k)
-    for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux"):
+    for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux", "t", "dt_t", "Dt_t", "dx_t"):
         if "out_part_" + f in g.files:
             _assert_same(mine["part"][f], g["out_part_" + f], "particle " + f)
     for k in ("u", "t", "s", "phi"):
