@@ -275,19 +275,25 @@ def bench_ensemble(args):
     K = args.steps
     t_step = _event_time(ens.stream_handle, lambda: ens.step(K)) / K
     solves_h = len(cases) * 3600.0 / (S * t_step)
-    # the rest of the solve, sampling Nu of the sampled cases over [S/2, S]
+    # the rest of the solve: T fields of the sampled cases at the short horizon, then Nu over [S/2, S]
     done = 100 + K
     nu_ens = {i: [] for i in sample}
-    while done < S:
-        target = min(S, (done // every + 1) * every)
+    t_ens = {}
+    marks = sorted({min(S, args.short_horizon)} | set(range(every, S + 1, every)))
+    for target in marks:
+        if target <= done:
+            continue
         ens.step(target - done)
         done = target
-        if done >= S // 2:
+        if done == args.short_horizon:
+            for i in sample:
+                t_ens[i] = ens.fields(slots[i])["t"]
+        if done >= S // 2 and done % every == 0:
             for i in sample:
                 nu_ens[i].append(ens.averages(slots[i])["nuy"])
     ens.close()
     # plain FP64, one case at a time, on the sample
-    xs, ts, errs, nus = [], [], [], []
+    xs, ts, errs, nus, terrs, per_case = [], [], [], [], [], []
     for i in sample:
         nx, ny, ra = cases[i]
         p0, g0 = state_of(i, nx, ny)
@@ -299,17 +305,23 @@ def bench_ensemble(args):
             sim.synchronize()
             t = _event_time(sim.stream_handle, lambda: sim.step(100))
             d, nu64 = 120, []
-            while d < S:
-                target = min(S, (d // every + 1) * every)
+            for target in marks:
+                if target <= d:
+                    continue
                 sim.step(target - d)
                 d = target
-                if d >= S // 2:
+                if d == args.short_horizon and i in t_ens:
+                    t64 = sim.fields()["t"]
+                    terrs.append(float(np.linalg.norm(t_ens[i] - t64) / np.linalg.norm(t64)))
+                if d >= S // 2 and d % every == 0:
                     nu64.append(sim.averages()["nuy"])
         xs.append(nx * ny)
         ts.append(t / 100)
         m64, m32 = float(np.mean(nu64)), float(np.mean(nu_ens[i]))
         nus.append(m64)
         errs.append(abs(m32 - m64) / abs(m64))
+        per_case.append({"NX": nx, "NY": ny, "Ra": float("%.4g" % ra), "nu_fp64": round(m64, 5), "nu": round(m32, 5),
+                         "t_rel_l2_at_short_horizon": float("%.3g" % terrs[-1]) if terrs else None})
     a, b = np.polyfit(np.array(xs, float), np.array(ts), 1)[::-1]
     t64 = sum(max(a + b * nx * ny, min(ts)) for nx, ny, _ in cases)
     solves_h64 = 3600.0 * len(cases) / (S * t64)
@@ -327,6 +339,9 @@ def bench_ensemble(args):
         "nusselt_vs_fp64": {"window": [S // 2, S], "every": every, "cases": len(errs),
                             "rel_error_median": float(np.median(errs)), "rel_error_max": float(np.max(errs)),
                             "nu_fp64_range": [float(min(nus)), float(max(nus))]},
+        "t_field_vs_fp64": {"after_steps": args.short_horizon, "rel_l2_median": float(np.median(terrs)),
+                            "rel_l2_max": float(np.max(terrs))},
+        "sample": per_case,
     }))
     return 0
 
@@ -441,9 +456,9 @@ def main():
     ap.add_argument("--cases", type=int, default=512)
     ap.add_argument("--steps-per-solve", type=int, default=20000)
     ap.add_argument("--sample", type=int, default=16)
-    ap.add_argument("--compare-steps", type=int, default=2000)
+    ap.add_argument("--short-horizon", type=int, default=2000)
     ap.add_argument("--requests", type=int, default=24)
-    ap.add_argument("--step-scale", type=float, default=0.05)
+    ap.add_argument("--step-scale", type=float, default=1.0)
     ap.add_argument("--hit-size", type=int, default=256)
     ap.add_argument("--particles", type=int, default=1000000)
     args = ap.parse_args()

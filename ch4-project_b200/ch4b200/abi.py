@@ -68,6 +68,7 @@ FLAGS = {
     "LB_SCALAR_INITIAL_CONSTANT_MEAN": 1 << 46,
     "LB_SCALAR_INITIAL_CONSTANT_BOT": 1 << 47,
     "LB_SCALAR_INITIAL_CONSTANT_TOP": 1 << 48,
+    "LB_FLUID_FORCING_CONSTANT_POWER": 1 << 49,
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 

@@ -61,7 +61,8 @@ const uint64_t SUPPORTED =
     CH4_F_TEMPERATURE_INITIAL_CONSTANT_BOT | CH4_F_TEMPERATURE_INITIAL_CONSTANT_TOP |
     CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION | CH4_F_TEMPERATURE_INITIAL_ADD_NOISE | CH4_F_SCALAR_INITIAL_LINEAR |
     CH4_F_SCALAR_INITIAL_ADD_PERTURBATION | CH4_F_SCALAR_INITIAL_CONSTANT | CH4_F_SCALAR_INITIAL_CONSTANT_MEAN |
-    CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER;
+    CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
+    CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -349,6 +350,8 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
     if (fl & CH4_F_TEMPERATURE_BUOYANCY) F |= K_BUOY;
     if (fl & CH4_F_SCALAR_BUOYANCY) F |= K_SBUOY;
     if (c.beta2_t != 0.0) F |= K_BETA2;
+    if (fl & CH4_F_FORCING_NOZEROMODE) F |= K_NOZERO;
+    if (fl & CH4_F_FORCING_CONSTANT_POWER) F |= K_CPOWER;
   }
   if (fl & CH4_F_FLUID_BC_Y) F |= K_FWALL;
   if (fl & CH4_F_FLUID_BC_Y_P_SLIP) F |= K_FSLIP_P;
@@ -361,6 +364,7 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   if (fl & CH4_F_SCALAR_BC_Y) F |= K_SWALL;
   if (fl & CH4_F_FLUID_LES) F |= K_LES;
   P.feat = F;
+  P.fm_prev = P.fm_cur = nullptr;
   for (int q = 0; q < NPOP; q++) P.w[q] = (A)lat.w[q];
   const double invtau = 1.0 / c.tau_u;
   const double fac = (1.0 - 0.5 * c.time_dt * invtau);  // src/forcing.c:1289
@@ -447,6 +451,13 @@ struct Engine : EngineBase {
   double* rec = nullptr;
   int *cstart = nullptr, *cend = nullptr;
   int* pstatus = nullptr;  // particle position check of the kernels (sticky until set_particles)
+  // global force corrections (NOZEROMODE / CONSTANT_POWER): two slots of 6, the
+  // last step's (fm_i) and the one being built; reduction scratch
+  A* fmbuf = nullptr;
+  double* fmpart = nullptr;
+  int fm_nblocks = 0, fm_i = 0;
+  bool fmoments() const { return (c.flags & (CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER)) != 0; }
+  const A* fm_last() const { return fmbuf ? fmbuf + 6 * fm_i : nullptr; }
   void* cubtmp = nullptr;
   size_t cubbytes = 0;
   bool lagr() const { return (c.flags & CH4_F_LAGRANGE) != 0; }
@@ -485,6 +496,8 @@ struct Engine : EngineBase {
     cudaFree(cstart);
     cudaFree(cend);
     cudaFree(pstatus);
+    cudaFree(fmbuf);
+    cudaFree(fmpart);
   }
 
   void free_particles() {
@@ -544,7 +557,7 @@ struct Engine : EngineBase {
     double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *part = d + 6 * n1;
     double* res = part + (size_t)nblocks * NAVG * 2;
     const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
-    st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, dd, du, nsets_on[1] ? dt : nullptr,
+    st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, fm_last(), dd, du, nsets_on[1] ? dt : nullptr,
                               nsets_on[2] ? ds : nullptr, nullptr, nullptr, H->stream),
                  "hydro");
     AvgParams Q{};
@@ -686,6 +699,15 @@ struct Engine : EngineBase {
           cudaMalloc(&cend, sizeof(int) * nhome()) != cudaSuccess)
         return H->fail(CH4_ERR_NOMEM, "home-cell ranges");
     }
+    if (fmoments()) {
+      fm_nblocks = (int)std::min<long long>(4 * 148, (N + FM_BLOCK - 1) / FM_BLOCK);
+      const A init[12] = {A(0), A(0), A(0), A(1), A(1), A(1), A(0), A(0), A(0), A(1), A(1), A(1)};
+      if (cudaMalloc(&fmbuf, sizeof init) != cudaSuccess ||
+          cudaMalloc(&fmpart, sizeof(double) * FM_SUMS * 2 * (size_t)fm_nblocks) != cudaSuccess)
+        return H->fail(CH4_ERR_NOMEM, "force corrections");
+      if (cudaMemcpy(fmbuf, init, sizeof init, cudaMemcpyHostToDevice) != cudaSuccess)
+        return H->fail(CH4_ERR_CUDA, "force corrections");
+    }
     if (c.flags & CH4_F_FLUID_LES) {
       if (cudaMalloc(&ules, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
       if (cudaMalloc(&tau_les, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tau_les");
@@ -745,6 +767,7 @@ struct Engine : EngineBase {
     P.tau_les = tau_les;
     P.kol = kol;
     P.dcur = P.dprev = nullptr;
+    P.fm_prev = P.fm_cur = fmbuf;  // both slots hold {0, 1} until the first correction
   }
 
   void bind_pops(int in) {
@@ -834,13 +857,24 @@ struct Engine : EngineBase {
         return st;
       if ((st = H->cuda(cudaEventRecord(hit_ev, H->stream), "hit event"))) return st;
     }
+    if (fmoments()) {  // corrections of the initial build_forcing (u = mv/rho: its force array is still zero)
+      fm_i = 0;
+      if ((st = force_moments(hit_last, 0, fmbuf))) return st;
+    }
     return H->cuda(cudaStreamSynchronize(H->stream), "initialize");
+  }
+
+  ch4_status force_moments(const A* hit_cur, int with_prev, A* out) {
+    const double amp[3] = {c.Amp_x, c.Amp_y, c.Amp_z};
+    const double norm = 1.0 / ((double)c.NX * (double)c.NY * (double)c.NZ);  // src/forcing.c:1139
+    return H->cuda(launch_force_moments(P, shape, hit_cur, with_prev, fmpart, fm_nblocks, norm, amp, out, H->stream),
+                   "force corrections");
   }
 
   ch4_status les_u() {
     // u^n with dt/2 F^{n-1}: prev tables are P.hit_prev
-    return H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, nullptr, nullptr, nullptr, nullptr, nullptr, ules,
-                                H->stream),
+    return H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                ules, H->stream),
                    "les u");
   }
 
@@ -886,15 +920,22 @@ struct Engine : EngineBase {
             return st;
           }
         }
+        if (fmoments()) {
+          // this step's corrections, from t^n, its tables and (CONSTANT_POWER) u^n
+          P.fm_prev = fmbuf + 6 * fm_i;
+          P.fm_cur = fmbuf + 6 * (fm_i ^ 1);
+          if ((st = force_moments(P.hit_cur, 1, fmbuf + 6 * (fm_i ^ 1)))) return st;
+        }
         if (c.flags & CH4_F_FLUID_LES)
           if ((st = les_u())) return st;
         if ((st = H->cuda(launch_step(P, shape, H->stream), "lb_step"))) return st;
+        if (fmoments()) fm_i ^= 1;
         cur ^= 1;
         H->itime++;
         if (lagr()) {
           // u^{n+1} with dt/2 F^n, then the Lagrangian sub-steps (src/main.c:164-185)
           bind_pops(cur);
-          if ((st = H->cuda(launch_hydro(P, shape, P.hit_cur, twoway() ? P.dcur : nullptr, nullptr, nullptr, nullptr,
+          if ((st = H->cuda(launch_hydro(P, shape, P.hit_cur, twoway() ? P.dcur : nullptr, fm_last(), nullptr, nullptr, nullptr,
                                          nullptr, nullptr, upart, H->stream, tpart),
                             "particle u")))
             return st;
@@ -922,7 +963,7 @@ struct Engine : EngineBase {
     if ((st = H->cuda(cudaMalloc(&d, 9 * n1 * sizeof(double)), "fields scratch"))) return st;
     double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *dfo = d + 6 * n1;
     const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
-    st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, dd, du, nsets_on[1] ? dt : nullptr, nsets_on[2] ? ds : nullptr,
+    st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, fm_last(), dd, du, nsets_on[1] ? dt : nullptr, nsets_on[2] ? ds : nullptr,
                               dfo, nullptr, H->stream),
                  "hydro");
     std::vector<double> hbuf(9 * n1);
@@ -1130,6 +1171,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_SCALAR_INITIAL_CONSTANT_MEAN", CH4_F_SCALAR_INITIAL_CONSTANT_MEAN},
       {"LB_SCALAR_INITIAL_CONSTANT_BOT", CH4_F_SCALAR_INITIAL_CONSTANT_BOT},
       {"LB_SCALAR_INITIAL_CONSTANT_TOP", CH4_F_SCALAR_INITIAL_CONSTANT_TOP},
+      {"LB_FLUID_FORCING_CONSTANT_POWER", CH4_F_FORCING_CONSTANT_POWER},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -1670,8 +1712,10 @@ ch4_status ch4_ensemble_add(ch4_ensemble* E, const ch4_config* cfg, int* slot) {
   std::string why;
   ch4_status st = validate(cfg, why);
   if (st) return E->fail(st, "%s", why.c_str());
-  if (cfg->flags & (CH4_F_FORCING_HIT | CH4_F_FLUID_LES | CH4_F_LAGRANGE))
-    return E->fail(CH4_ERR_UNSUPPORTED, "ensemble slots run without HIT forcing, LES or particles");
+  if (cfg->flags & (CH4_F_FORCING_HIT | CH4_F_FLUID_LES | CH4_F_LAGRANGE | CH4_F_FORCING_NOZEROMODE |
+                    CH4_F_FORCING_CONSTANT_POWER))
+    return E->fail(CH4_ERR_UNSUPPORTED,
+                   "ensemble slots run without HIT forcing, LES, particles or global force corrections");
   LaunchShape sh{(cfg->flags & CH4_F_LB_TEMPERATURE) != 0, (cfg->flags & CH4_F_LB_SCALAR) != 0, E->storage};
   bool any = false;
   for (auto& s : E->slots) any |= s.used;
@@ -1859,7 +1903,7 @@ ch4_status ch4_ensemble_get_fields(ch4_ensemble* E, int slot, double* dens, doub
   double* d = nullptr;
   ch4_status st;
   if ((st = E->cuda(cudaMalloc(&d, 6 * n1 * sizeof(double)), "fields scratch"))) return st;
-  st = E->cuda(launch_hydro(E->params_of(*s, 0), E->shape, nullptr, nullptr, d, d + n1, s->nsets_on[1] ? d + 4 * n1 : nullptr,
+  st = E->cuda(launch_hydro(E->params_of(*s, 0), E->shape, nullptr, nullptr, nullptr, d, d + n1, s->nsets_on[1] ? d + 4 * n1 : nullptr,
                             s->nsets_on[2] ? d + 5 * n1 : nullptr, nullptr, nullptr, E->stream),
                "hydro");
   std::vector<double> h(6 * n1, 0.0);
@@ -1894,7 +1938,7 @@ ch4_status ch4_ensemble_averages(ch4_ensemble* E, int slot, ch4_averages* out) {
   if ((st = E->cuda(cudaMalloc(&d, total * sizeof(double)), "averages scratch"))) return st;
   double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *part = d + 6 * n1;
   double* res = part + (size_t)nblocks * NAVG * 2;
-  st = E->cuda(launch_hydro(E->params_of(*s, 0), E->shape, nullptr, nullptr, dd, du, s->nsets_on[1] ? dt : nullptr,
+  st = E->cuda(launch_hydro(E->params_of(*s, 0), E->shape, nullptr, nullptr, nullptr, dd, du, s->nsets_on[1] ? dt : nullptr,
                             s->nsets_on[2] ? ds : nullptr, nullptr, nullptr, E->stream),
                "hydro");
   AvgParams Q{};

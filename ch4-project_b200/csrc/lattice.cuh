@@ -12,6 +12,8 @@ namespace ch4 {
 
 constexpr int Q = 19;
 constexpr int NK = 6;  // HIT forcing modes, src/initial_conditions.c:841-849
+constexpr int FM_SUMS = 9;     // sums of the global force corrections: F, F*u, u per component
+constexpr int FM_BLOCK = 256;  // threads per block of that reduction
 
 __host__ __device__ constexpr int cx(int q) {
   return q == 1 || q == 7 || q == 8 || q == 11 || q == 13 ? 1 : (q == 2 || q == 9 || q == 10 || q == 12 || q == 14 ? -1 : 0);
@@ -51,7 +53,9 @@ enum : uint32_t {
   K_LES = 1u << 15,
   K_TWOWAY = 1u << 16,
   K_BETA2 = 1u << 17,
-  K_TSRC = 1u << 18
+  K_TSRC = 1u << 18,
+  K_NOZERO = 1u << 19,  // LB_FLUID_FORCING_NOZEROMODE: subtract the mean force
+  K_CPOWER = 1u << 20   // LB_FLUID_FORCING_CONSTANT_POWER: scale to a fixed mean power
 };
 
 template <typename A>
@@ -71,6 +75,10 @@ struct StepParams {
   // two-way coupling deposit of this and the previous step (3 SoA planes each)
   const A* dcur;
   const A* dprev;
+  // global force corrections {f0x, f0y, f0z, coeffx, coeffy, coeffz} of the previous
+  // and current step (NOZEROMODE / CONSTANT_POWER), device arrays of 6
+  const A* fm_prev;
+  const A* fm_cur;
   // constants (host-computed in FP64, then cast)
   A w[Q];
   A facw[Q];  // (1 - dt/(2 tau_u)) * w_q, the Guo prefactor of src/forcing.c:1289,1432

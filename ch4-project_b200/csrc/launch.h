@@ -21,12 +21,22 @@ cudaError_t launch_step(const StepParams<float>& P, LaunchShape s, cudaStream_t 
 cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStream_t st);
 cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStream_t st);
 // hydro fields / force (FP64 outputs), optional arithmetic-precision u planes and t plane
-cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep, double* dens,
+cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep,
+                         const double* fm, double* dens,
                          double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st,
                          double* t_arith = nullptr);
-cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep, double* dens,
+cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep,
+                         const float* fm, double* dens,
                          double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
                          float* t_arith = nullptr);
+// global force corrections (NOZEROMODE / CONSTANT_POWER) of one step into fm[6];
+// partial holds nblocks * 9 * 2 doubles
+cudaError_t launch_force_moments(const StepParams<double>& P, LaunchShape s, const double* hit_cur, int with_prev,
+                                 double* partial, int nblocks, double norm, const double* amp, double* fm,
+                                 cudaStream_t st);
+cudaError_t launch_force_moments(const StepParams<float>& P, LaunchShape s, const float* hit_cur, int with_prev,
+                                 double* partial, int nblocks, double norm, const double* amp, float* fm,
+                                 cudaStream_t st);
 // compact AoS chunk <-> SoA storage for one population set
 cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st);

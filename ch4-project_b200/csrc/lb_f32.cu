@@ -14,11 +14,18 @@ cudaError_t launch_step(const StepParams<float>& P, LaunchShape s, cudaStream_t 
 cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStream_t st) {
   return s.storage == 2 ? init_prev_t<__half, float>(P, s, st) : init_prev_t<float, float>(P, s, st);
 }
-cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep, double* dens,
+cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep, const float* fm,
+                         double* dens,
                          double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
                          float* t_arith) {
-  return s.storage == 2 ? hydro_t<__half, float>(P, s, hit, dep, dens, u, t, sc, force, u_arith, t_arith, st)
-                        : hydro_t<float, float>(P, s, hit, dep, dens, u, t, sc, force, u_arith, t_arith, st);
+  return s.storage == 2 ? hydro_t<__half, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, t_arith, st)
+                        : hydro_t<float, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, t_arith, st);
+}
+cudaError_t launch_force_moments(const StepParams<float>& P, LaunchShape s, const float* hit_cur, int with_prev,
+                                 double* partial, int nblocks, double norm, const double* amp, float* fm,
+                                 cudaStream_t st) {
+  return s.storage == 2 ? force_moments_t<__half, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st)
+                        : force_moments_t<float, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st);
 }
 cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st) {

@@ -14,10 +14,16 @@ cudaError_t launch_step(const StepParams<double>& P, LaunchShape s, cudaStream_t
 cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStream_t st) {
   return init_prev_t<double, double>(P, s, st);
 }
-cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep, double* dens,
+cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep, const double* fm,
+                         double* dens,
                          double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st,
                          double* t_arith) {
-  return hydro_t<double, double>(P, s, hit, dep, dens, u, t, sc, force, u_arith, t_arith, st);
+  return hydro_t<double, double>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, t_arith, st);
+}
+cudaError_t launch_force_moments(const StepParams<double>& P, LaunchShape s, const double* hit_cur, int with_prev,
+                                 double* partial, int nblocks, double norm, const double* amp, double* fm,
+                                 cudaStream_t st) {
+  return force_moments_t<double, double>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st);
 }
 cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st) {

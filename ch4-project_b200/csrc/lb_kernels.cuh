@@ -19,6 +19,7 @@
 // compiled with FMA contraction off, which makes it bit-identical to the
 // reference CPU build.
 #pragma once
+#include "diag.cuh"
 #include "lattice.cuh"
 
 namespace ch4 {
@@ -78,7 +79,7 @@ __device__ __forceinline__ A momz(const A* a) {
 // two-way deposit (src/lagrange_feedback.c:245-254), in the reference's order.
 template <typename A>
 __device__ __forceinline__ void cell_force(const StepParams<A>& P, int x, int y, int z, long long idx, A t, A s,
-                                           const A* hit, const A* dep, A& fx, A& fy, A& fz) {
+                                           const A* hit, const A* dep, const A* fm, A& fx, A& fy, A& fz) {
   fx = A(0);
   fy = A(0);
   fz = A(0);
@@ -117,6 +118,18 @@ __device__ __forceinline__ void cell_force(const StepParams<A>& P, int x, int y,
     fx += fac * P.grav[0];
     fy += fac * P.grav[1];
     fz += fac * P.grav[2];
+  }
+  if (fm) {  // global corrections after the grid loop, src/forcing.c:1123-1190
+    if (F & K_NOZERO) {
+      fx -= fm[0];
+      fy -= fm[1];
+      fz -= fm[2];
+    }
+    if (F & K_CPOWER) {
+      fx *= fm[3];
+      fy *= fm[4];
+      fz *= fm[5];
+    }
   }
   if (dep) {
     fx += dep[idx];
@@ -189,8 +202,8 @@ __global__ void init_prev_kernel(const StepParams<A> P) {
 // Also the force field itself when `force` is non-null, and u and t in the
 // arithmetic precision for the particle interpolation (u_arith, t_arith).
 template <typename S, typename A, bool THERM, bool SCAL>
-__global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, double* dens, double* u, double* t,
-                             double* s, double* force, A* u_arith, A* t_arith) {
+__global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, const A* fm, double* dens, double* u,
+                             double* t, double* s, double* force, A* u_arith, A* t_arith) {
   const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (idx >= P.N) return;
   const int x = (int)(idx % P.NX);
@@ -203,7 +216,7 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
   if (P.feat & K_FORCING) {
     const A tp = THERM ? P.tprev[idx] : A(0);
     const A sp = SCAL ? P.sprev[idx] : A(0);
-    cell_force(P, x, y, z, idx, tp, sp, hit, dep, Fx, Fy, Fz);
+    cell_force(P, x, y, z, idx, tp, sp, hit, dep, fm, Fx, Fy, Fz);
   }
   const A ux = momx(f) / rho + P.hdt * Fx;
   const A uy = momy(f) / rho + P.hdt * Fy;
@@ -265,5 +278,7 @@ __global__ void soa_to_aos_kernel(const S* soa, double* aos, int NX, int NY, int
   const long long c = t / Q;
   aos[t] = (double)Codec<S, A>::load(soa, (long long)q * N + (long long)z0 * NX * NY + c, P.w[q], P.shift[set]);
 }
+
+#include "force_moments.cuh"
 
 }  // namespace ch4

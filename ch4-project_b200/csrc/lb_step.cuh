@@ -171,8 +171,8 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
   if (forcing) {
     const A tp = THERM ? P.tprev[idx] : A(0);
     const A sp = SCAL ? P.sprev[idx] : A(0);
-    cell_force(P, x, y, z, idx, tp, sp, P.hit_prev, (F & K_TWOWAY) ? P.dprev : nullptr, px, py, pz);
-    cell_force(P, x, y, z, idx, c.tt, c.ss, P.hit_cur, (F & K_TWOWAY) ? P.dcur : nullptr, c.Fx, c.Fy, c.Fz);
+    cell_force(P, x, y, z, idx, tp, sp, P.hit_prev, (F & K_TWOWAY) ? P.dprev : nullptr, P.fm_prev, px, py, pz);
+    cell_force(P, x, y, z, idx, c.tt, c.ss, P.hit_cur, (F & K_TWOWAY) ? P.dcur : nullptr, P.fm_cur, c.Fx, c.Fy, c.Fz);
   }
   if constexpr (EXACT) {
     c.ux = mx / c.rho + P.hdt * px;

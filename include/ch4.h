@@ -92,6 +92,7 @@ enum {
   CH4_F_SCALAR_INITIAL_CONSTANT_MEAN = 1ull << 46,
   CH4_F_SCALAR_INITIAL_CONSTANT_BOT = 1ull << 47,
   CH4_F_SCALAR_INITIAL_CONSTANT_TOP = 1ull << 48,
+  CH4_F_FORCING_CONSTANT_POWER = 1ull << 49,  /* src/forcing.c:1154-1190 */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63

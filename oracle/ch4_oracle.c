@@ -63,6 +63,9 @@ struct ch4o_state {
   double *pvol, *pdr; /* per-particle volume (4/3 pi r^3) and rho_p/rho_f */
   /* two-way deposit of this and the previous step, velocity field for the particles */
   double *dcur, *dprev, *uf, *tf;
+  /* build_forcing's global corrections of the previous and current step:
+   * mean force f0 (NOZEROMODE) and per-component power coefficients (CONSTANT_POWER) */
+  double fm_prev[6], fm_cur[6];
 };
 
 /* ---- host RNG: drand48 stream (src/random.c:4-16 with SYSTEM_RANDOM48) ---- */
@@ -126,7 +129,7 @@ static void hit_tables(ch4o_state *s, double phi[NK][3], double *tab) {
 
 /* per-cell force of build_forcing's grid loop, src/forcing.c:360-707 */
 static void cell_force(const ch4o_state *s, int i, int j, int k, double t, double sc, const double *hit,
-                       const double *dep, double F[3]) {
+                       const double *dep, const double *fm, double F[3]) {
   const ch4_config *c = &s->cfg;
   double fx = 0.0, fy = 0.0, fz = 0.0;
   if (c->flags & CH4_F_FORCING_POISEUILLE) { /* src/forcing.c:365-370 */
@@ -169,6 +172,18 @@ static void cell_force(const ch4o_state *s, int i, int j, int k, double t, doubl
     fx += fac * c->gravity_x;
     fy += fac * c->gravity_y;
     fz += fac * c->gravity_z;
+  }
+  if (fm) { /* after the grid loop: src/forcing.c:1123-1152, 1154-1190 */
+    if (c->flags & CH4_F_FORCING_NOZEROMODE) {
+      fx -= fm[0];
+      fy -= fm[1];
+      fz -= fm[2];
+    }
+    if (c->flags & CH4_F_FORCING_CONSTANT_POWER) {
+      fx *= fm[3];
+      fy *= fm[4];
+      fz *= fm[5];
+    }
   }
   if (dep) { /* force += force_twoway, src/lagrange_feedback.c:245-254 */
     size_t idx = ((size_t)k * (size_t)s->NY + (size_t)j) * (size_t)s->NX + (size_t)i;
@@ -246,8 +261,8 @@ static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k)
 }
 
 /* hydro fields of src/lb.c:420-539 from the current populations and F^{n-1} */
-static void hydro(const ch4o_state *s, const double *hit, const double *dep, double *dens, double *u, double *t,
-                  double *sc) {
+static void hydro(const ch4o_state *s, const double *hit, const double *dep, const double *fm, double *dens, double *u,
+                  double *t, double *sc) {
   const int NX = s->NX, NY = s->NY, NZ = s->NZ;
   const size_t N = s->N;
   const double hdt = 0.5 * s->cfg.time_dt;
@@ -257,7 +272,7 @@ static void hydro(const ch4o_state *s, const double *hit, const double *dep, dou
         size_t idx = cidx(s, i, j, k);
         double a[NPOP], F[3];
         double tprev = s->tprev ? s->tprev[idx] : 0.0, sprev = s->sprev ? s->sprev[idx] : 0.0;
-        cell_force(s, i, j, k, tprev, sprev, hit, dep, F);
+        cell_force(s, i, j, k, tprev, sprev, hit, dep, fm, F);
         if (!(s->cfg.flags & CH4_F_LB_FLUID_FORCING)) F[0] = F[1] = F[2] = 0.0;
         load_cell(s->f[0], N, idx, a);
         double rho = mom0(a);
@@ -604,6 +619,82 @@ static void deposit(const ch4o_state *s, double *D) {
   }
 }
 
+/* The global corrections of build_forcing (src/forcing.c:1123-1190) for the force
+ * built from the current populations and the table `hit`: NOZEROMODE subtracts the
+ * mean force, CONSTANT_POWER then scales component a by Amp_a / <F.u>, with u the
+ * velocity field the reference holds at that moment (`u`, or mv/rho before the first
+ * build_forcing, while its force array is still zero).  Both sums run over k, j, i
+ * in the reference's order.  fm = {f0x, f0y, f0z, coeffx, coeffy, coeffz}. */
+static void force_moments(const ch4o_state *s, const double *hit, const double *u, double fm[6]) {
+  const ch4_config *c = &s->cfg;
+  const size_t N = s->N;
+  double f0[3] = {0.0, 0.0, 0.0}, pw[3] = {0.0, 0.0, 0.0};
+  const double norm = 1.0 / ((double)c->NX * (double)c->NY * (double)c->NZ);
+  const int nozero = (c->flags & CH4_F_FORCING_NOZEROMODE) != 0;
+  const int cpower = (c->flags & CH4_F_FORCING_CONSTANT_POWER) != 0;
+  double *F = (double *)malloc(sizeof(double) * 3 * N);
+  for (int k = 0; k < s->NZ; k++)
+    for (int j = 0; j < s->NY; j++)
+      for (int i = 0; i < s->NX; i++) {
+        size_t idx = cidx(s, i, j, k);
+        double a[NPOP], tt = 0.0, ss = 0.0;
+        if (s->nsets_on[1]) {
+          load_cell(s->f[1], N, idx, a);
+          tt = mom0(a);
+        }
+        if (s->nsets_on[2]) {
+          load_cell(s->f[2], N, idx, a);
+          ss = mom0(a);
+        }
+        cell_force(s, i, j, k, tt, ss, hit, NULL, NULL, F + 3 * idx);
+      }
+  fm[0] = fm[1] = fm[2] = 0.0;
+  fm[3] = fm[4] = fm[5] = 1.0;
+  if (nozero) {
+    for (int k = 0; k < s->NZ; k++)
+      for (int j = 0; j < s->NY; j++)
+        for (int i = 0; i < s->NX; i++) {
+          size_t idx = cidx(s, i, j, k);
+          f0[0] += F[3 * idx];
+          f0[1] += F[3 * idx + 1];
+          f0[2] += F[3 * idx + 2];
+        }
+    for (int a = 0; a < 3; a++) fm[a] = f0[a] * norm;
+  }
+  if (cpower) {
+    for (int k = 0; k < s->NZ; k++)
+      for (int j = 0; j < s->NY; j++)
+        for (int i = 0; i < s->NX; i++) {
+          size_t idx = cidx(s, i, j, k);
+          double uu[3];
+          if (u) {
+            uu[0] = u[3 * idx];
+            uu[1] = u[3 * idx + 1];
+            uu[2] = u[3 * idx + 2];
+          } else {
+            double a[NPOP];
+            load_cell(s->f[0], N, idx, a);
+            double rho = mom0(a);
+            uu[0] = momx(a) / rho + 0.5 * c->time_dt * 0.0;
+            uu[1] = momy(a) / rho + 0.5 * c->time_dt * 0.0;
+            uu[2] = momz(a) / rho + 0.5 * c->time_dt * 0.0;
+          }
+          for (int a = 0; a < 3; a++) {
+            double fa = F[3 * idx + a];
+            if (nozero) fa -= fm[a];
+            pw[a] += fa * uu[a];
+          }
+        }
+    double fac = (pw[0] + pw[1] + pw[2]) * norm;
+    if (fac != 0.0) {
+      fm[3] = c->Amp_x / fac;
+      fm[4] = c->Amp_y / fac;
+      fm[5] = c->Amp_z / fac;
+    }
+  }
+  free(F);
+}
+
 /* one step of src/main.c:67-161 */
 static void one_step(ch4o_state *s) {
   const ch4_config *c = &s->cfg;
@@ -635,11 +726,23 @@ static void one_step(ch4o_state *s) {
       memset(s->dcur, 0, sizeof(double) * 3 * N);
   }
 
+  /* global corrections of this step's build_forcing, with u^n of the previous one */
+  memcpy(s->fm_prev, s->fm_cur, sizeof(s->fm_cur));
+  if (c->flags & (CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER)) {
+    double *un = NULL;
+    if (c->flags & CH4_F_FORCING_CONSTANT_POWER) {
+      un = (double *)malloc(sizeof(double) * 3 * N);
+      hydro(s, s->hit_prev, s->dprev, s->fm_prev, NULL, un, NULL, NULL);
+    }
+    force_moments(s, s->hit_cur, un, s->fm_cur);
+    free(un);
+  }
+
   /* u^n field (needed by LES gradients, src/fluid.c:1056-1075) */
   double *uarr = NULL;
   if (c->flags & CH4_F_FLUID_LES) {
     uarr = (double *)malloc(sizeof(double) * 3 * N);
-    hydro(s, s->hit_prev, s->dprev, NULL, uarr, NULL, NULL);
+    hydro(s, s->hit_prev, s->dprev, s->fm_prev, NULL, uarr, NULL, NULL);
   }
 
   const double invtau_u = 1.0 / c->tau_u;
@@ -666,8 +769,8 @@ static void one_step(ch4o_state *s) {
         double Fp[3] = {0, 0, 0}, Fc[3] = {0, 0, 0};
         if (forcing) {
           cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_prev,
-                     s->dprev, Fp);
-          cell_force(s, i, j, k, tt, ss, s->hit_cur, s->dcur, Fc);
+                     s->dprev, s->fm_prev, Fp);
+          cell_force(s, i, j, k, tt, ss, s->hit_cur, s->dcur, s->fm_cur, Fc);
         }
         double ux = mx / rho + hdt * Fp[0];
         double uy = my / rho + hdt * Fp[1];
@@ -779,7 +882,7 @@ static void one_step(ch4o_state *s) {
   /* Lagrangian sub-steps, src/main.c:164-185: u^{n+1} with dt/2 F^n, then
    * interpolate + move + wrap time_dt_lagr_factor times */
   if (c->flags & CH4_F_LAGRANGE) {
-    hydro(s, s->hit_cur, s->dcur, NULL, s->uf, s->tf, NULL);
+    hydro(s, s->hit_cur, s->dcur, s->fm_cur, NULL, s->uf, s->tf, NULL);
     const double dtl = c->time_dt / c->time_dt_lagr_factor;
     const int first = (s->itime == 1 && c->resume == 0);
     for (int sub = 0; sub < (int)c->time_dt_lagr_factor; sub++) {
@@ -796,6 +899,8 @@ int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
   if (!cfg || !out || cfg->NX <= 0 || cfg->NY <= 0 || cfg->NZ <= 0) return CH4_ERR_ARG;
   ch4o_state *s = (ch4o_state *)calloc(1, sizeof(ch4o_state));
   s->cfg = *cfg;
+  s->fm_cur[3] = s->fm_cur[4] = s->fm_cur[5] = 1.0;
+  s->fm_prev[3] = s->fm_prev[4] = s->fm_prev[5] = 1.0;
   s->NX = cfg->NX;
   s->NY = cfg->NY;
   s->NZ = cfg->NZ;
@@ -965,6 +1070,9 @@ int ch4o_initialize(ch4o_state *s) {
     memcpy(s->hit_prev, s->hit_cur, sizeof(double) * NK * (s->NX + s->NY + s->NZ));
     memcpy(s->phi_prev, s->phi_cur, sizeof(s->phi_cur));
   }
+  /* global corrections of the initial build_forcing */
+  if (s->cfg.flags & (CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER))
+    force_moments(s, s->hit_cur, NULL, s->fm_cur);
   /* force field of the initial build_forcing */
   for (int k = 0; k < s->NZ; k++)
     for (int j = 0; j < s->NY; j++)
@@ -972,7 +1080,8 @@ int ch4o_initialize(ch4o_state *s) {
         size_t idx = cidx(s, i, j, k);
         double F[3] = {0, 0, 0};
         if (s->cfg.flags & CH4_F_LB_FLUID_FORCING)
-          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_cur, NULL, F);
+          cell_force(s, i, j, k, s->tprev ? s->tprev[idx] : 0.0, s->sprev ? s->sprev[idx] : 0.0, s->hit_cur, NULL,
+                     s->fm_cur, F);
         s->force[3 * idx] = F[0];
         s->force[3 * idx + 1] = F[1];
         s->force[3 * idx + 2] = F[2];
@@ -1002,7 +1111,7 @@ int ch4o_get_fields(ch4o_state *s, double *dens, double *u, double *t, double *s
   double *d0 = (double *)malloc(sizeof(double) * N), *u0 = (double *)malloc(sizeof(double) * 3 * N);
   double *t0 = (double *)calloc(N, sizeof(double)), *s0 = (double *)calloc(N, sizeof(double));
   /* between steps the kept temperature is t^n and the latest phases those of F^n */
-  hydro(s, s->hit_cur, s->dcur, d0, u0, t0, s0);
+  hydro(s, s->hit_cur, s->dcur, s->fm_cur, d0, u0, t0, s0);
   if (dens) scatter_field(s, d0, 1, dens, brd);
   if (u) scatter_field(s, u0, 3, u, brd);
   if (t) scatter_field(s, t0, 1, t, brd);
@@ -1075,7 +1184,7 @@ int ch4o_averages_get(ch4o_state *s, ch4_averages *out) {
   const size_t N = s->N;
   double *dens = (double *)malloc(sizeof(double) * N), *u = (double *)malloc(sizeof(double) * 3 * N);
   double *t = (double *)calloc(N, sizeof(double)), *sc = (double *)calloc(N, sizeof(double));
-  hydro(s, s->hit_cur, s->dcur, dens, u, t, sc);
+  hydro(s, s->hit_cur, s->dcur, s->fm_cur, dens, u, t, sc);
   const int fw = (c->flags & CH4_F_FLUID_BC_Y) != 0;
   const int tw = (c->flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
   ch4_averages o;

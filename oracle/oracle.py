@@ -47,6 +47,10 @@ FLAGSETS = {
     "particles_t": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE",
                     "LB_TEMPERATURE_BUOYANCY", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
                     "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    "nozero": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
+               "LB_FLUID_FORCING_NOZEROMODE", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY"],
+    "cpower": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_FLUID_FORCING_NOZEROMODE",
+               "LB_FLUID_FORCING_CONSTANT_POWER"],
     "init_rb": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
                 "LB_TEMPERATURE_BC_Y", "LB_SCALAR", "LB_SCALAR_BC_Y", "LB_INITIAL_BAROMETRIC",
                 "LB_FLUID_INITIAL_PERTURBATION", "LB_FLUID_INITIAL_ADD_NOISE", "LB_FLUID_INITIAL_UNIT_DENSITY",

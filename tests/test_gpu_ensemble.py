@@ -41,9 +41,9 @@ CASES = [(16, 12, 1, 1e4, 1), (40, 20, 1, 3e4, 2), (24, 16, 3, 1e5, 3), (64, 24,
          (33, 17, 1, 8e4, 6)]
 
 
-def run_ensemble(cases, nsteps, shape=None, tune=False):
+def run_ensemble(cases, nsteps, shape=None, tune=False, storage=abi.STORE_F32):
     out = []
-    with ch4b200.Ensemble(abi.STORE_F32) as ens:
+    with ch4b200.Ensemble(storage) as ens:
         slots = []
         for cfg, st in cases:
             s = ens.add(cfg)
@@ -139,3 +139,28 @@ def test_ensemble_rejects_hit_and_mixed_sets():
         kol = O.make_config(8, 8, 8, ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV"], tau_u=0.6)
         with pytest.raises(ch4b200.CH4Error):
             ens.add(kol)
+
+
+def test_fp16_ensemble_matches_single_lattice_fp16_and_fp64_bounds():
+    """FP16-deviation storage in the ensemble: the same per-cell arithmetic as the
+    single-lattice FP16 path -- a last-place FP32 difference can flip the rounding of a
+    stored half, so agreement is within two FP16 ulps (2^-9 relative) of the largest
+    stored deviation f - w*shift -- and the FP16 error bound of the single-lattice
+    parity tests against the FP64 oracle (T within 2e-2 relative L2)."""
+    cases = [rb_case(*c, storage=abi.STORE_F16) for c in CASES[:3]]
+    mix = run_ensemble(cases, 30, storage=abi.STORE_F16)
+    for (cfg, st), m in zip(cases, mix):
+        with ch4b200.Simulation(cfg) as sim:
+            sim.set_pop("p", st["p"])
+            sim.set_pop("g", st["g"])
+            sim.initialize()
+            sim.step(30)
+            p, g = sim.get_pop("p"), sim.get_pop("g")
+        dev_p = np.abs(p - W * 1.0).max()
+        dev_g = np.abs(g - W * 0.5).max()
+        assert np.abs(m["p"] - p).max() <= 2.0 ** -9 * dev_p
+        assert np.abs(m["g"] - g).max() <= 2.0 ** -9 * dev_g
+        cfg64 = O.make_config(cfg.NX, cfg.NY, cfg.NZ, RB_FLAGS, tau_u=cfg.tau_u, tau_t=cfg.tau_t, beta_t=1.0,
+                              gravity_y=cfg.gravity_y, T_bot=1.0, T_top=0.0, T_ref=0.5)
+        ref = run_restatement(cfg64, st, 30)
+        assert np.linalg.norm(m["t"] - ref["t"]) / np.linalg.norm(ref["t"]) < 2e-2
