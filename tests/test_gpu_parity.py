@@ -168,4 +168,5 @@ def test_fp32_global_force_corrections_close_to_fp64():
     ref = run_restatement(cfg64, state, 40)
     gpu = run_gpu(cfg, state, 40)
     assert rel_l2(gpu["u"], ref["u"]) < 1e-3
-    assert rel_l2(gpu["t"], ref["t"]) < 1e-6
+    # FP32 T (~0.5) after 40 steps: a few unit roundoffs (2^-24) per step accumulate
+    assert rel_l2(gpu["t"], ref["t"]) < 3e-6

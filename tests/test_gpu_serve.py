@@ -26,8 +26,9 @@ def small_requests():
     ]
 
 
-def test_each_request_same_alone_and_in_the_mix():
-    mix = Server(abi.STORE_F32, budget_bytes=8 << 30, block=32).run(small_requests())
+@pytest.mark.parametrize("cells_in_flight", [None, 20000])
+def test_each_request_same_alone_and_in_the_mix(cells_in_flight):
+    mix = Server(abi.STORE_F32, budget_bytes=8 << 30, block=32, cells_in_flight=cells_in_flight).run(small_requests())
     for req in mix:
         assert req.finished is not None and req.latency >= 0
         alone = Server(abi.STORE_F32, budget_bytes=8 << 30, block=32).run(
@@ -45,4 +46,12 @@ def test_admission_by_memory_budget_queues_requests():
     assert all(r.finished is not None for r in done)
     # at most two fit at a time: the third is admitted only after one of the first two finished
     order = sorted(done, key=lambda r: r.admitted)
+    assert order[2].admitted >= min(order[0].finished, order[1].finished)
+
+
+def test_cells_in_flight_limits_concurrency():
+    reqs = [Request(i, "kolmogorov", 24, 40, arrival=0.0) for i in range(4)]  # 13,824 cells each
+    done = Server(abi.STORE_F32, budget_bytes=8 << 30, block=16, cells_in_flight=30000).run(reqs)
+    order = sorted(done, key=lambda r: r.admitted)
+    # two fit under the cap: the third waits for one of the first two
     assert order[2].admitted >= min(order[0].finished, order[1].finished)
