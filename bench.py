@@ -17,6 +17,7 @@ max over ranks.  Prints ONE JSON line on rank 0.
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -147,23 +148,46 @@ def ncu_traffic(storage):
         return None
 
 
-def cpu_reference_run(steps, workdir=None):
-    """Time the reference solver's own CPU build (oracle/_ref/rb, single rank) on the
-    full lattice from its rest state; returns MLUPS and the sample description."""
+def cpu_reference_run(steps, procs=None):
+    """Time the reference solver's own CPU build (oracle/_ref/rb) on the host cores.
+
+    The build links the single-rank MPI stand-in, so the reference's domain
+    decomposition is reproduced by running one single-rank process per core on its own
+    box of the lattice (x and z split, y walls kept whole), all at once: the MPI run
+    without its halo exchange, i.e. an upper bound on the MPI build's throughput.
+    Returns (MLUPS of the whole lattice, cores, sample description)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
     exe = O.ref_binary("rb")
     if not os.path.exists(exe):
-        return None, "oracle/_ref/rb/ch4ref not built"
-    cfg = O.make_config(NX, NY, NZ, O.FLAGSETS["rb"], **rb_params())
-    tmp = workdir or tempfile.mkdtemp(prefix="ch4cpu_")
-    O.write_param_in(os.path.join(tmp, "param.in"), cfg, steps)
-    r = subprocess.run([exe, str(steps), "1"], cwd=tmp, capture_output=True, text=True)
-    if r.returncode != 0:
-        return None, "reference run failed: " + r.stderr[-300:]
-    with open(os.path.join(tmp, "timing.json")) as f:
-        t = json.load(f)
-    return t["mlups"], "%d step(s) of the full 256x256x128 lattice from the rest state, 1 MPI rank" % steps
+        return None, 0, "oracle/_ref/rb/ch4ref not built"
+    cores = procs or len(os.sched_getaffinity(0))
+    px = pz = 1
+    while px * pz * 2 <= cores and (NX // (px * 2) >= 8 or NZ // (pz * 2) >= 8):
+        if NX // (px * 2) >= 8 and (px <= pz or NZ // (pz * 2) < 8):
+            px *= 2
+        else:
+            pz *= 2
+    nx, nz = NX // px, NZ // pz
+    cfg = O.make_config(nx, NY, nz, O.FLAGSETS["rb"], **rb_params())
+    runs = []
+    for r in range(px * pz):
+        tmp = tempfile.mkdtemp(prefix="ch4cpu_")
+        O.write_param_in(os.path.join(tmp, "param.in"), cfg, steps)
+        runs.append((tmp, subprocess.Popen([exe, str(steps), str(1 + r)], cwd=tmp, stdout=subprocess.DEVNULL,
+                                           stderr=subprocess.PIPE, text=True)))
+    secs = []
+    for tmp, pr in runs:
+        _, err = pr.communicate()
+        if pr.returncode != 0:
+            return None, 0, "reference run failed: " + err[-300:]
+        with open(os.path.join(tmp, "timing.json")) as f:
+            secs.append(json.load(f)["seconds"])
+        shutil.rmtree(tmp, ignore_errors=True)  # the harness also dumps the final state there
+    mlups = NX * NY * NZ * steps / max(secs) / 1e6
+    return mlups, px * pz, ("%d step(s) of the 256x256x128 lattice as %d concurrent single-rank reference processes "
+                            "on %dx%dx%d boxes (x and z split, one per core): the MPI decomposition without its "
+                            "halo exchange" % (steps, px * pz, nx, NY, nz))
 
 
 def dist_setup():
@@ -173,14 +197,19 @@ def dist_setup():
     return world, rank, local
 
 
+def cpu_sample_steps():
+    """Steps for ~15 s of reference CPU work on all usable cores (2.4 MLUPS per core measured)."""
+    cores = len(os.sched_getaffinity(0))
+    return int(min(100, max(2, round(15.0 * 2.4e6 * cores / (NX * NY * NZ)))))
+
+
 def run_reference_arm(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    k = max(1, min(args.steps, 6))
     if args.warmup > 0:
         cpu_reference_run(1)
-    mlups, sample = cpu_reference_run(k)
+    mlups, cores, sample = cpu_reference_run(cpu_sample_steps())
     if mlups is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return 0
@@ -189,7 +218,7 @@ def run_reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": NX * NY * NZ / mlups / 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "lattice": [NX, NY, NZ], "Ra": RA, "Pr": PR},
-        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": 1, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -287,13 +316,13 @@ def bench_ensemble(args):
         done = target
         if done == args.short_horizon:
             for i in sample:
-                t_ens[i] = ens.fields(slots[i])["t"]
+                t_ens[i] = (ens.fields(slots[i])["t"], ens.averages(slots[i]))
         if done >= S // 2 and done % every == 0:
             for i in sample:
                 nu_ens[i].append(ens.averages(slots[i])["nuy"])
     ens.close()
     # plain FP64, one case at a time, on the sample
-    xs, ts, errs, nus, terrs, per_case = [], [], [], [], [], []
+    xs, ts, errs, nus, terrs, per_case, short_nu, short_ke = [], [], [], [], [], [], [], []
     for i in sample:
         nx, ny, ra = cases[i]
         p0, g0 = state_of(i, nx, ny)
@@ -311,8 +340,11 @@ def bench_ensemble(args):
                 sim.step(target - d)
                 d = target
                 if d == args.short_horizon and i in t_ens:
-                    t64 = sim.fields()["t"]
-                    terrs.append(float(np.linalg.norm(t_ens[i] - t64) / np.linalg.norm(t64)))
+                    t64, a64 = sim.fields()["t"], sim.averages()
+                    te, ae = t_ens[i]
+                    terrs.append(float(np.linalg.norm(te - t64) / np.linalg.norm(t64)))
+                    short_nu.append(abs(ae["nuy"] - a64["nuy"]) / abs(a64["nuy"]))
+                    short_ke.append(abs(ae["ene"] - a64["ene"]) / abs(a64["ene"]))
                 if d >= S // 2 and d % every == 0:
                     nu64.append(sim.averages()["nuy"])
         xs.append(nx * ny)
@@ -341,6 +373,11 @@ def bench_ensemble(args):
                             "nu_fp64_range": [float(min(nus)), float(max(nus))]},
         "t_field_vs_fp64": {"after_steps": args.short_horizon, "rel_l2_median": float(np.median(terrs)),
                             "rel_l2_max": float(np.max(terrs))},
+        "nusselt_and_kinetic_energy_vs_fp64": {"after_steps": args.short_horizon,
+                                               "nu_rel_error_max": float(np.max(short_nu)),
+                                               "ke_rel_error_max": float(np.max(short_ke)),
+                                               "nu_rel_error_median": float(np.median(short_nu)),
+                                               "ke_rel_error_median": float(np.median(short_ke))},
         "sample": per_case,
     }))
     return 0
@@ -553,11 +590,8 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        mlups, sample = cpu_reference_run(2)
-        if mlups is not None:
-            cpu = {"value": mlups, "unit": "MLUPS", "cores": 1, "kind": "reference", "sample": sample}
-        else:
-            cpu = {"value": None, "unit": "MLUPS", "cores": 1, "kind": "reference", "sample": sample}
+        mlups, cores, sample = cpu_reference_run(cpu_sample_steps())
+        cpu = {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": "reference", "sample": sample}
 
     if rank == 0:
         line = {
