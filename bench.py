@@ -354,6 +354,34 @@ def bench_ensemble(args):
         errs.append(abs(m32 - m64) / abs(m64))
         per_case.append({"NX": nx, "NY": ny, "Ra": float("%.4g" % ra), "nu_fp64": round(m64, 5), "nu": round(m32, 5),
                          "t_rel_l2_at_short_horizon": float("%.3g" % terrs[-1]) if terrs else None})
+    # steady laminar cells, where FP32 and FP64 can be compared at the end of the run:
+    # 32x16 cells at Ra 3e3 - 1e4, many thermal diffusion times (H^2 / kappa = 17 k - 32 k steps)
+    lam = [(32, 16, float(ra)) for ra in np.geomspace(3e3, 1e4, args.laminar_cases)]
+    lam_ens = ch4b200.Ensemble(storage)
+    lam_slots = []
+    for i, (nx, ny, ra) in enumerate(lam):
+        sl = lam_ens.add(cfg_of(nx, ny, ra, storage))
+        p0, g0 = state_of(1000 + i, nx, ny)
+        lam_ens.set_pop(sl, "p", p0)
+        lam_ens.set_pop(sl, "g", g0)
+        lam_ens.initialize(sl)
+        lam_slots.append(sl)
+    lam_ens.step(args.laminar_steps)
+    lam_ens.synchronize()
+    lam_err_nu, lam_err_ke, lam_nu = [], [], []
+    for i, ((nx, ny, ra), sl) in enumerate(zip(lam, lam_slots)):
+        a32 = lam_ens.averages(sl)
+        p0, g0 = state_of(1000 + i, nx, ny)
+        with ch4b200.Simulation(cfg_of(nx, ny, ra, abi.STORE_F64)) as sim:
+            sim.set_pop("p", p0)
+            sim.set_pop("g", g0)
+            sim.initialize()
+            sim.step(args.laminar_steps)
+            a64 = sim.averages()
+        lam_nu.append(round(a64["nuy"], 6))
+        lam_err_nu.append(abs(a32["nuy"] - a64["nuy"]) / abs(a64["nuy"]))
+        lam_err_ke.append(abs(a32["ene"] - a64["ene"]) / abs(a64["ene"]))
+    lam_ens.close()
     a, b = np.polyfit(np.array(xs, float), np.array(ts), 1)[::-1]
     t64 = sum(max(a + b * nx * ny, min(ts)) for nx, ny, _ in cases)
     solves_h64 = 3600.0 * len(cases) / (S * t64)
@@ -378,6 +406,10 @@ def bench_ensemble(args):
                                                "ke_rel_error_max": float(np.max(short_ke)),
                                                "nu_rel_error_median": float(np.median(short_nu)),
                                                "ke_rel_error_median": float(np.median(short_ke))},
+        "steady_laminar_vs_fp64": {"cases": len(lam), "lattice": [32, 16], "Ra": [3e3, 1e4],
+                                   "steps": args.laminar_steps, "nu_fp64": lam_nu,
+                                   "nu_rel_error_max": float(max(lam_err_nu)),
+                                   "ke_rel_error_max": float(max(lam_err_ke))},
         "sample": per_case,
     }))
     return 0
@@ -500,6 +532,8 @@ def main():
     ap.add_argument("--steps-per-solve", type=int, default=20000)
     ap.add_argument("--sample", type=int, default=16)
     ap.add_argument("--short-horizon", type=int, default=2000)
+    ap.add_argument("--laminar-cases", type=int, default=8)
+    ap.add_argument("--laminar-steps", type=int, default=200000)
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--cells-in-flight", type=int, default=8 << 20)
     ap.add_argument("--step-scale", type=float, default=1.0)

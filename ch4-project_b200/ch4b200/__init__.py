@@ -80,6 +80,8 @@ def lib():
         L.ch4_ensemble_get_stream.argtypes = [P, C.POINTER(C.c_void_p)]
         L.ch4_initial_populations.argtypes = [C.POINTER(Config), D, D, D, D]
         L.ch4_initial_conditions.argtypes = [P]
+        L.ch4_diagnostics.argtypes = [P, D, D, D, D]
+        L.ch4_dump_averages.argtypes = [P, C.c_char_p, C.c_double, C.c_int]
         V = C.c_void_p
         L.ch4_averages_noalloc.argtypes = [V, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                            C.c_double, V, V]
@@ -239,6 +241,25 @@ class Simulation:
         a = Averages()
         self._check(lib().ch4_averages_get(self.h, C.byref(a)), "averages")
         return {n: getattr(a, n) for n in abi.AVERAGE_FIELDS}
+
+    def diagnostics(self, rulers=True):
+        """ch4_diagnostics: dump_averages' volume averages ({field: value}) and, with
+        rulers, the per-plane averages along x, y, z as {field: array over the planes}."""
+        c = self.cfg
+        nf = len(abi.DIAG_FIELDS)
+        g = np.zeros(nf)
+        rs = [np.zeros((n, nf)) for n in (c.NX, c.NY, c.NZ)] if rulers else [None] * 3
+        self._check(lib().ch4_diagnostics(self.h, _dp(g), *[_dp(r) for r in rs]), "diagnostics")
+        out = {"global": dict(zip(abi.DIAG_FIELDS, g))}
+        if rulers:
+            for axis, r in zip("xyz", rs):
+                out[axis] = {f: r[:, q].copy() for q, f in enumerate(abi.DIAG_FIELDS)}
+        return out
+
+    def dump_averages(self, directory, time_now, irun):
+        """ch4_dump_averages: the reference's dump_averages ASCII files in `directory`."""
+        self._check(lib().ch4_dump_averages(self.h, str(directory).encode(), float(time_now), int(irun)),
+                    "dump_averages")
 
     @property
     def stream_handle(self):

@@ -69,6 +69,7 @@ FLAGS = {
     "LB_SCALAR_INITIAL_CONSTANT_BOT": 1 << 47,
     "LB_SCALAR_INITIAL_CONSTANT_TOP": 1 << 48,
     "LB_FLUID_FORCING_CONSTANT_POWER": 1 << 49,
+    "OUTPUT_DIAGN_APPEND": 1 << 50,
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 
@@ -115,6 +116,11 @@ PARTICLE_FIELDS = [
 class Particle(C.Structure):
     _fields_ = [(n, C.c_double) for n in PARTICLE_FIELDS]
 
+
+# fields of ch4_diag (the `output` record of dump_averages), same order
+DIAG_FIELDS = ["x", "y", "z", "ux", "uy", "uz", "ux2", "uy2", "uz2", "rho", "rho2", "ene", "eps",
+               "t", "t2", "epst", "dxt", "dyt", "dzt", "uxt", "uyt", "uzt", "nux", "nuy", "nuz", "lb",
+               "s", "s2", "epss", "dxs", "dys", "dzs", "uxs", "uys", "uzs", "nusx", "nusy", "nusz"]
 
 AVERAGE_FIELDS = ["rho", "ux", "uy", "uz", "ux2", "uy2", "uz2", "ene", "eps",
                   "t", "t2", "epst", "dxt", "dyt", "dzt", "uxt", "uyt", "uzt", "nux", "nuy", "nuz",

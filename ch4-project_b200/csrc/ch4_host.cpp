@@ -62,7 +62,7 @@ const uint64_t SUPPORTED =
     CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION | CH4_F_TEMPERATURE_INITIAL_ADD_NOISE | CH4_F_SCALAR_INITIAL_LINEAR |
     CH4_F_SCALAR_INITIAL_ADD_PERTURBATION | CH4_F_SCALAR_INITIAL_CONSTANT | CH4_F_SCALAR_INITIAL_CONSTANT_MEAN |
     CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
-    CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER;
+    CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -233,6 +233,9 @@ struct EngineBase {
   virtual ch4_status step(int n) = 0;
   virtual ch4_status fields(double* dens, double* u, double* t, double* s, double* force, int brd) = 0;
   virtual ch4_status averages(ch4_averages* out) = 0;
+  // raw (unnormalised) dump_averages sums: global [NDIAG] and, for each non-null
+  // ruler, [bins][NDIAG] along x, y, z
+  virtual ch4_status diag_sums(double* glob, double* rx, double* ry, double* rz) = 0;
   virtual ch4_status set_particles(const ch4_particle* parts, int n) = 0;
   virtual ch4_status get_particles(ch4_particle* parts, int n) = 0;
   virtual size_t device_bytes() const = 0;
@@ -252,6 +255,8 @@ struct ch4_handle {
   int itime = 0;
   bool initialized = false;
   Lattice lat;
+  // running rulers of ch4_dump_averages (ruler_*_running, src/output.c:765-768)
+  std::vector<double> run[3];
 
   ch4_status fail(ch4_status s, const char* fmt, ...) {
     char buf[512];
@@ -329,6 +334,15 @@ void normalize_averages(const ch4_config& c, const int* nsets_on, double* h) {
   if (nsets_on[2]) {
     h[21] *= norm;
     h[22] *= norm;
+  }
+}
+
+// plane pointers of set s from its base pointers (N cells, `bytes` per stored value)
+template <typename A>
+void set_planes(StepParams<A>& P, int s, long long N, size_t bytes) {
+  for (int q = 0; q < NPOP; q++) {
+    P.fin_q[s][q] = P.fin[s] ? static_cast<const char*>(P.fin[s]) + (size_t)q * N * bytes : nullptr;
+    P.fout_q[s][q] = P.fout[s] ? static_cast<char*>(P.fout[s]) + (size_t)q * N * bytes : nullptr;
   }
 }
 
@@ -585,6 +599,54 @@ struct Engine : EngineBase {
     return CH4_OK;
   }
 
+  ch4_status diag_sums(double* glob, double* rx, double* ry, double* rz) override {
+    bind_pops(cur);
+    const size_t n1 = (size_t)N;
+    const int nblocks = (int)std::min<long long>(4 * 148, (N + DIAG_BLOCK - 1) / DIAG_BLOCK);
+    const size_t nbins = (size_t)c.NX + c.NY + c.NZ;
+    double* d = nullptr;
+    ch4_status st;
+    const size_t total = 6 * n1 + (size_t)nblocks * NDIAG + NDIAG + nbins * NDIAG;
+    if ((st = H->cuda(cudaMalloc(&d, total * sizeof(double)), "diagnostics scratch"))) return st;
+    double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *part = d + 6 * n1;
+    double* res = part + (size_t)nblocks * NDIAG;
+    double* rul = res + NDIAG;  // x | y | z rulers
+    const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
+    st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, fm_last(), dd, du,
+                              nsets_on[1] ? dt : nullptr, nsets_on[2] ? ds : nullptr, nullptr, nullptr, H->stream),
+                 "hydro");
+    AvgParams Q{};
+    Q.NX = c.NX;
+    Q.NY = c.NY;
+    Q.NZ = c.NZ;
+    Q.N = N;
+    Q.dens = dd;
+    Q.u = du;
+    Q.t = nsets_on[1] ? dt : nullptr;
+    Q.s = nsets_on[2] ? ds : nullptr;
+    Q.fwall = (c.flags & CH4_F_FLUID_BC_Y) != 0;
+    Q.twall = (c.flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+    Q.nu = c.nu;
+    Q.kappa = c.kappa;
+    Q.chi = c.chi;
+    double* outs[3] = {rx, ry, rz};
+    const int bins[3] = {c.NX, c.NY, c.NZ};
+    double* dst[3] = {rul, rul + (size_t)c.NX * NDIAG, rul + (size_t)(c.NX + c.NY) * NDIAG};
+    if (!st) st = H->cuda(launch_diag(Q, -1, nblocks, part, res, H->stream), "diagnostics");
+    for (int a = 0; a < 3 && !st; a++)
+      if (outs[a]) st = H->cuda(launch_diag(Q, a, bins[a], nullptr, dst[a], H->stream), "rulers");
+    if (!st && glob)
+      st = H->cuda(cudaMemcpyAsync(glob, res, NDIAG * sizeof(double), cudaMemcpyDeviceToHost, H->stream), "down");
+    for (int a = 0; a < 3 && !st; a++)
+      if (outs[a])
+        st = H->cuda(cudaMemcpyAsync(outs[a], dst[a], (size_t)bins[a] * NDIAG * sizeof(double), cudaMemcpyDeviceToHost,
+                                     H->stream),
+                     "rulers down");
+    if (!st) st = H->cuda(cudaStreamSynchronize(H->stream), "diagnostics sync");
+    cudaFree(d);
+    return st;
+  }
+
   ch4_status set_particles(const ch4_particle* parts, int n) override {
     if (!lagr()) return H->fail(CH4_ERR_ARG, "particles need the LAGRANGE flag");
     if (n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "bad particle array");
@@ -774,6 +836,7 @@ struct Engine : EngineBase {
     for (int s = 0; s < 3; s++) {
       P.fin[s] = f[s][in];
       P.fout[s] = f[s][in ^ 1];
+      set_planes(P, s, N, sbytes);
     }
   }
 
@@ -1172,6 +1235,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_SCALAR_INITIAL_CONSTANT_BOT", CH4_F_SCALAR_INITIAL_CONSTANT_BOT},
       {"LB_SCALAR_INITIAL_CONSTANT_TOP", CH4_F_SCALAR_INITIAL_CONSTANT_TOP},
       {"LB_FLUID_FORCING_CONSTANT_POWER", CH4_F_FORCING_CONSTANT_POWER},
+      {"OUTPUT_DIAGN_APPEND", CH4_F_OUTPUT_DIAGN_APPEND},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -1179,7 +1243,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
                                   "METHOD_FORCING_GUO", "LB_FLUID_FORCING_GRAVITY", "LB_FLUID_BC", "LB_TEMPERATURE_BC",
                                   "LB_SCALAR_BC", "SYSTEM_RANDOM48", "SYSTEM_TIMING", "TIMING", "NEW_SENDRECV",
                                   "OUTPUT_H5", "OUTPUT_H5_GRID", "OUTPUT_H5_TIMESTAMP_REAL", "OUTPUT_AT_START",
-                                  "OUTPUT_ASCII", "OUTPUT_DIAGN_APPEND", "VERBOSE", "LB_TEMPERATURE_BUOYANCY_T0_REF",
+                                  "OUTPUT_ASCII", "VERBOSE", "LB_TEMPERATURE_BUOYANCY_T0_REF",
                                   "LB_TEMPERATURE_BUOYANCY_T0_TOP", "LB_TEMPERATURE_BUOYANCY_T0_BOT", "LB_FLUID_LES_OUTPUT"};
   uint64_t flags = 0;
   int t0 = CH4_T0_MEAN;
@@ -1405,6 +1469,153 @@ ch4_status ch4_initial_conditions(ch4_handle* h) {
   return CH4_OK;
 }
 
+// ---- dump_averages in full ------------------------------------------------
+namespace {
+enum DiagField {
+  DX, DY, DZ, DUX, DUY, DUZ, DUX2, DUY2, DUZ2, DRHO, DRHO2, DENE, DEPS,
+  DT, DT2, DEPST, DDXT, DDYT, DDZT, DUXT, DUYT, DUZT, DNUX, DNUY, DNUZ, DLB,
+  DS, DS2, DEPSS, DDXS, DDYS, DDZS, DUXS, DUYS, DUZS, DNUSX, DNUSY, DNUSZ
+};
+static_assert(sizeof(ch4_diag) == NDIAG * sizeof(double), "ch4_diag layout");
+
+// Normalisation of src/output.c:495-760 for the volume averages (axis < 0) or one
+// ruler bin along axis 0/1/2, with the reference's factors as written.
+void normalize_diag(const ch4_config& c, bool therm, bool scal, double* v, int axis) {
+  double norm;
+  if (axis < 0) {
+    norm = 1.0 / (c.SX * c.SY * c.SZ);
+  } else if (axis == 0) {
+    v[DX] *= 1.0 / (double)(c.NY * c.NZ);
+    norm = 1.0 / (c.SY * c.SZ);
+  } else if (axis == 1) {
+    v[DY] *= 1.0 / (double)(c.NX * c.NZ);
+    norm = 1.0 / (c.SX * c.SZ);
+  } else {
+    v[DZ] *= 1.0 / (double)(c.NX * c.NY);
+    norm = 1.0 / (c.SX * c.SY);
+  }
+  for (int f : {DENE, DRHO, DUX, DUY, DUZ, DUX2, DUY2, DUZ2, DEPS, DRHO2}) v[f] *= norm;
+  // temperature and scalar blocks: their z rulers use 1/(SY*SZ) (src/output.c:631,745)
+  const double tnorm = axis < 0 ? 1.0 / (c.SX * c.SY * c.SZ) : axis == 1 ? 1.0 / (c.SX * c.SZ) : 1.0 / (c.SY * c.SZ);
+  if (therm) {
+    for (int f = DT; f <= DUZT; f++) v[f] *= tnorm;
+    for (int f = DNUX; f <= DNUZ; f++) v[f] *= tnorm / (c.kappa * c.deltaT / c.SY);
+    v[DLB] = (c.flags & CH4_F_TEMPERATURE_BUOYANCY)
+                 ? std::pow(v[DEPS], 5. / 4.) * std::pow(v[DEPST], -3. / 4.) * std::pow(c.gravity_y * c.beta_t, -3. / 2.)
+                 : 0.0;
+  }
+  if (scal) {
+    for (int f = DS; f <= DUZS; f++) v[f] *= tnorm;
+    for (int f = DNUSX; f <= DNUSZ; f++) v[f] *= tnorm / (c.chi * c.deltaS / c.SY);
+  }
+}
+
+ch4_status diagnostics(ch4_handle* h, double* g, double* r[3]) {
+  const ch4_config& c = h->cfg;
+  ch4_status st = h->eng->diag_sums(g, r[0], r[1], r[2]);
+  if (st) return st;
+  const bool therm = (c.flags & CH4_F_LB_TEMPERATURE) != 0, scal = (c.flags & CH4_F_LB_SCALAR) != 0;
+  if (g) normalize_diag(c, therm, scal, g, -1);
+  const int bins[3] = {c.NX, c.NY, c.NZ};
+  for (int a = 0; a < 3; a++)
+    if (r[a])
+      for (int b = 0; b < bins[a]; b++) normalize_diag(c, therm, scal, r[a] + (size_t)b * NDIAG, a);
+  return CH4_OK;
+}
+
+FILE* open_in(const char* dir, const char* name, const char* mode) {
+  std::string path = dir && *dir ? std::string(dir) + "/" + name : std::string(name);
+  return std::fopen(path.c_str(), mode);
+}
+
+// rows of one ruler file: the coordinate of the axis, then the given fields, each / div
+bool write_ruler(const char* dir, const char* name, const char* mode, const double* r, int bins, int axis,
+                 const std::vector<int>& fields, double div) {
+  FILE* f = open_in(dir, name, mode);
+  if (!f) return false;
+  for (int b = 0; b < bins; b++) {
+    const double* v = r + (size_t)b * NDIAG;
+    std::fprintf(f, "%e", v[axis] / div);
+    for (int q : fields) std::fprintf(f, " %e", v[q] / div);
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
+  return true;
+}
+}  // namespace
+
+ch4_status ch4_diagnostics(ch4_handle* h, ch4_diag* global, ch4_diag* ruler_x, ch4_diag* ruler_y, ch4_diag* ruler_z) {
+  if (!h) return CH4_ERR_ARG;
+  double* r[3] = {reinterpret_cast<double*>(ruler_x), reinterpret_cast<double*>(ruler_y),
+                  reinterpret_cast<double*>(ruler_z)};
+  return diagnostics(h, reinterpret_cast<double*>(global), r);
+}
+
+ch4_status ch4_dump_averages(ch4_handle* h, const char* dir, double time_now, int irun) {
+  if (!h || irun < 1) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  const int bins[3] = {c.NX, c.NY, c.NZ};
+  std::vector<double> g(NDIAG), r[3];
+  double* rp[3];
+  for (int a = 0; a < 3; a++) {
+    r[a].assign((size_t)bins[a] * NDIAG, 0.0);
+    rp[a] = r[a].data();
+  }
+  ch4_status st = diagnostics(h, g.data(), rp);
+  if (st) return st;
+  for (int a = 0; a < 3; a++) {  // add_output(ruler_*_running, ruler_*), src/output.c:765-768
+    if (h->run[a].size() != r[a].size()) h->run[a].assign(r[a].size(), 0.0);
+    for (size_t i = 0; i < r[a].size(); i++) h->run[a][i] += r[a][i];
+  }
+  const char* mode = (c.flags & CH4_F_OUTPUT_DIAGN_APPEND) ? "a" : "w";
+  const double ir = (double)irun;
+  static const char* axes[3] = {"x", "y", "z"};
+  auto block = [&](const char* stem, const std::vector<int>& glob_fields, const std::vector<int>& ruler_fields) {
+    FILE* f = open_in(dir, (std::string(stem) + ".dat").c_str(), "a");
+    if (!f) return false;
+    std::fprintf(f, "%e", time_now);
+    for (int q : glob_fields) std::fprintf(f, " %e", g[q]);
+    std::fprintf(f, "\n");
+    std::fclose(f);
+    for (int a = 0; a < 3; a++)
+      if (!write_ruler(dir, (std::string(stem) + "_" + axes[a] + ".dat").c_str(), mode, r[a].data(), bins[a], a,
+                       ruler_fields, 1.0))
+        return false;
+    for (int a = 0; a < 3; a++)
+      if (!write_ruler(dir, (std::string(stem) + "_" + axes[a] + "_run.dat").c_str(), mode, h->run[a].data(), bins[a],
+                       a, ruler_fields, ir))
+        return false;
+    return true;
+  };
+  // src/output.c:772-830
+  const std::vector<int> fl = {DENE, DRHO, DUX, DUY, DUZ, DUX2, DUY2, DUZ2, DEPS, DRHO2};
+  if (!block("velocity_averages", fl, fl)) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
+  if (c.flags & CH4_F_FORCING_HIT) {  // src/output.c:832-858
+    const double nu = c.nu, eps = g[DEPS];
+    const double u_prime =
+        std::sqrt(((g[DUX2] - g[DUX] * g[DUX]) + (g[DUY2] - g[DUY] * g[DUY]) + (g[DUZ2] - g[DUZ] * g[DUZ])) / 3.0);
+    const double lambda = std::sqrt(15.0 * nu * u_prime * u_prime / eps);
+    const double Re_lambda = lambda * u_prime / nu;
+    const double lk = std::pow(std::pow(nu, 3.0) / eps, 0.25), tk = std::pow(nu / eps, 0.5),
+                 vk = std::pow(nu * eps, 0.25);
+    const double k_turb = 1.5 * std::pow(u_prime, 2.0);
+    const double lL = std::pow(u_prime, 3.0) / eps, tL = k_turb / eps, vL = u_prime;
+    FILE* f = open_in(dir, "velocity_turbulence.dat", "a");
+    if (!f) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
+    std::fprintf(f, "%e %e %e %e %e %e %e %e %e\n", time_now, Re_lambda, lambda, lk, tk, vk, lL, tL, vL);
+    std::fclose(f);
+  }
+  if (c.flags & CH4_F_LB_TEMPERATURE) {  // src/output.c:862-935
+    const std::vector<int> ft = {DT, DT2, DEPST, DDXT, DDYT, DDZT, DUXT, DUYT, DUZT, DNUX, DNUY, DNUZ, DLB};
+    if (!block("temperature_averages", ft, ft)) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
+  }
+  if (c.flags & CH4_F_LB_SCALAR) {  // src/output.c:1034-1096
+    const std::vector<int> fs = {DS, DS2, DEPSS, DDXS, DDYS, DDZS, DUXS, DUYS, DUZS, DNUSX, DNUSY, DNUSZ};
+    if (!block("scalar_averages", fs, fs)) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
+  }
+  return CH4_OK;
+}
+
 ch4_status ch4_step(ch4_handle* h, int nsteps) {
   if (!h || nsteps < 0) return CH4_ERR_ARG;
   if (!h->initialized) return h->fail(CH4_ERR_STATE, "ch4_step before ch4_initialize");
@@ -1571,6 +1782,7 @@ struct ch4_ensemble {
     for (int k = 0; k < 3; k++) {
       P.fin[k] = s.f[k][in];
       P.fout[k] = s.f[k][in ^ 1];
+      set_planes(P, k, s.N, storage == CH4_STORE_F16 ? 2 : 4);
     }
     return P;
   }

@@ -9,6 +9,8 @@
 namespace ch4 {
 
 constexpr int NAVG = 23;  // fields of ch4_averages, same order
+constexpr int NDIAG = 38;  // fields of ch4_diag, same order
+constexpr int DIAG_BLOCK = 256;
 constexpr int AVG_BLOCK = 256;
 
 struct AvgParams {
@@ -18,8 +20,8 @@ struct AvgParams {
   const double* u;     // 3 planes
   const double* t;     // may be null
   const double* s;     // may be null
-  int fwall, twall;    // one-sided y gradients for u / for t
-  double nu, kappa;
+  int fwall, twall;    // one-sided y gradients for u / for t and s
+  double nu, kappa, chi;
   double* partial;     // [gridDim.x][NAVG][2]
 };
 
@@ -142,6 +144,126 @@ static __global__ void averages_final_kernel(const double* partial, int nblocks,
   DD acc = {0.0, 0.0};
   for (int b = 0; b < nblocks; b++) acc = dd_add(acc, DD{partial[((long long)b * NAVG + q) * 2], partial[((long long)b * NAVG + q) * 2 + 1]});
   out[q] = acc.hi + acc.lo;
+}
+
+// All per-cell terms of dump_averages (src/output.c:188-480) in ch4_diag order, on
+// the unit grid of GRID_REGULAR with S = N (cell volume 1, centres at index + 0.5):
+// x y z | ux uy uz ux2 uy2 uz2 rho rho2 ene eps | t t2 epst dxt dyt dzt uxt uyt uzt nux
+// nuy nuz lb | s s2 epss dxs dys dzs uxs uys uzs nusx nusy nusz.  The gradients of t
+// and s are one-sided at the y walls when either set has walls, as gradient_scalar's
+// compile-time test (src/gradients.c:505-620).
+__device__ __forceinline__ void cell_terms_full(const AvgParams& P, long long c, double* v) {
+  const int i = (int)(c % P.NX), j = (int)((c / P.NX) % P.NY), k = (int)(c / ((long long)P.NX * P.NY));
+  const long long N = P.N;
+  const double ux = P.u[c], uy = P.u[N + c], uz = P.u[2 * N + c], rho = P.dens[c];
+  v[0] = (double)i + 0.5;
+  v[1] = (double)j + 0.5;
+  v[2] = (double)k + 0.5;
+  v[3] = ux;
+  v[4] = uy;
+  v[5] = uz;
+  v[6] = ux * ux;
+  v[7] = uy * uy;
+  v[8] = uz * uz;
+  v[9] = rho;
+  v[10] = rho * rho;
+  v[11] = 0.5 * (ux * ux + uy * uy + uz * uz);
+  double g[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) g[a][b] = gfield(P, P.u + a * N, i, j, k, b, P.fwall != 0);
+  const double xx = g[0][0], xy = g[0][1], xz = g[0][2], yx = g[1][0], yy = g[1][1], yz = g[1][2], zx = g[2][0],
+               zy = g[2][1], zz = g[2][2];
+  v[12] = ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) + (yx + xy) * (yx + xy) +
+           (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) + (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) +
+           (zz + zz) * (zz + zz)) *
+          0.5 * P.nu;
+  for (int q = 13; q < NDIAG; q++) v[q] = 0.0;
+  if (P.t) {
+    const double t = P.t[c];
+    const double gx = gfield(P, P.t, i, j, k, 0, P.twall != 0), gy = gfield(P, P.t, i, j, k, 1, P.twall != 0),
+                 gz = gfield(P, P.t, i, j, k, 2, P.twall != 0);
+    v[13] = t;
+    v[14] = t * t;
+    v[15] = P.kappa * (gx * gx + gy * gy + gz * gz);
+    v[16] = gx;
+    v[17] = gy;
+    v[18] = gz;
+    v[19] = ux * t;
+    v[20] = uy * t;
+    v[21] = uz * t;
+    v[22] = -P.kappa * gx + ux * t;
+    v[23] = -P.kappa * gy + uy * t;
+    v[24] = -P.kappa * gz + uz * t;
+    // v[25] (lb) is 0 per cell; it is formed from the normalised sums
+  }
+  if (P.s) {
+    const double sv = P.s[c];
+    const double gx = gfield(P, P.s, i, j, k, 0, P.twall != 0), gy = gfield(P, P.s, i, j, k, 1, P.twall != 0),
+                 gz = gfield(P, P.s, i, j, k, 2, P.twall != 0);
+    v[26] = sv;
+    v[27] = sv * sv;
+    v[28] = P.chi * (gx * gx + gy * gy + gz * gz);
+    v[29] = gx;
+    v[30] = gy;
+    v[31] = gz;
+    v[32] = ux * sv;
+    v[33] = uy * sv;
+    v[34] = uz * sv;
+    v[35] = -P.chi * gx + ux * sv;
+    v[36] = -P.chi * gy + uy * sv;
+    v[37] = -P.chi * gz + uz * sv;
+  }
+}
+
+// The k-th cell of reduction block b: axis < 0 -- block b owns a contiguous range of
+// cells (global sums); axis 0/1/2 -- block b owns the plane x = b / y = b / z = b
+// (the rulers of dump_averages), walked in a fixed order.
+__device__ __forceinline__ long long diag_cell(const AvgParams& P, int axis, int b, long long k) {
+  if (axis == 0) return ((k / P.NY) * P.NY + (k % P.NY)) * (long long)P.NX + b;
+  if (axis == 1) return ((k / P.NX) * P.NY + b) * (long long)P.NX + (k % P.NX);
+  return (long long)b * P.NX * P.NY + k;
+}
+
+// Sums of the NDIAG terms per block, plain FP64 in a fixed order (thread-strided,
+// then a fixed tree): out[blockIdx.x][q].  The per-block count is n (global: N split
+// into gridDim.x ranges; rulers: the cells of one plane).
+static __global__ void __launch_bounds__(DIAG_BLOCK) diag_sums_kernel(const AvgParams P, int axis, double* out) {
+  __shared__ double sh[DIAG_BLOCK];
+  long long c0 = 0, n;
+  if (axis < 0) {
+    const long long per_block = (P.N + gridDim.x - 1) / gridDim.x;
+    c0 = (long long)blockIdx.x * per_block;
+    n = c0 + per_block < P.N ? per_block : (P.N > c0 ? P.N - c0 : 0);
+  } else {
+    n = axis == 0 ? (long long)P.NY * P.NZ : axis == 1 ? (long long)P.NX * P.NZ : (long long)P.NX * P.NY;
+  }
+  double acc[NDIAG];
+  for (int q = 0; q < NDIAG; q++) acc[q] = 0.0;
+  double v[NDIAG];
+  for (long long k = threadIdx.x; k < n; k += DIAG_BLOCK) {
+    const long long c = axis < 0 ? c0 + k : diag_cell(P, axis, blockIdx.x, k);
+    cell_terms_full(P, c, v);
+    for (int q = 0; q < NDIAG; q++) acc[q] += v[q];
+  }
+  for (int q = 0; q < NDIAG; q++) {
+    sh[threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int w = DIAG_BLOCK / 2; w > 0; w >>= 1) {
+      if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[(long long)blockIdx.x * NDIAG + q] = sh[0];
+    __syncthreads();
+  }
+}
+
+// global sums: one thread per quantity adds the block sums in block order
+static __global__ void diag_final_kernel(const double* partial, int nblocks, double* out) {
+  const int q = threadIdx.x;
+  if (q >= NDIAG) return;
+  double a = 0.0;
+  for (int b = 0; b < nblocks; b++) a += partial[(long long)b * NDIAG + q];
+  out[q] = a;
 }
 
 #endif  // __CUDACC__

@@ -26,11 +26,22 @@ __global__ void __launch_bounds__(256) ensemble_step_kernel(const StepParams<A>*
     __syncthreads();
     const int NX = sp.NX, rows = tl.ny, NZ = sp.NZ;
     const int ncell = NX * rows * NZ;
+    // cell i = x + NX * (r + rows * z), advanced by blockDim.x without dividing per cell
+    const int dx = (int)blockDim.x % NX, drow = (int)blockDim.x / NX;
+    int x = (int)threadIdx.x % NX, row = (int)threadIdx.x / NX;  // row = r + rows * z
+    int r = row % rows, z = row / rows;
     for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
-      const int x = i % NX;
-      const int r = (i / NX) % rows;
-      const int z = i / (NX * rows);
       lb_cell<S, A, THERM, SCAL>(sp, x, tl.y0 + r, z);
+      x += dx;
+      r += drow;
+      if (x >= NX) {
+        x -= NX;
+        r += 1;
+      }
+      if (r >= rows) {
+        z += r / rows;
+        r %= rows;
+      }
     }
     __syncthreads();  // sp and tile_id are reused by the next tile
   }

@@ -66,6 +66,10 @@ struct StepParams {
   // populations (storage type erased; cast in the kernel)
   const void* fin[3];
   void* fout[3];
+  // plane q of each set (fin[s] + q*N elements), filled by the host with fin/fout: an
+  // access is then one wide multiply-add of the cell index onto a parameter
+  const void* fin_q[3][Q];
+  void* fout_q[3][Q];
   // previous-step temperature / scalar (t^{n-1}), read and overwritten in place
   A* tprev;
   A* sprev;

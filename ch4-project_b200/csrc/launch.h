@@ -59,6 +59,9 @@ cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* 
 
 // dump_averages sums (FP64, deterministic); out_dev receives NAVG raw sums
 cudaError_t launch_averages(const AvgParams& P, int nblocks, double* out_dev, cudaStream_t st);
+// all dump_averages terms: global sums (axis < 0: nblocks partials into partial, then
+// out[NDIAG]) or the per-plane rulers along axis 0/1/2 (out[nbins][NDIAG])
+cudaError_t launch_diag(const AvgParams& P, int axis, int nblocks, double* partial, double* out, cudaStream_t st);
 
 // one ensemble step over a tile list (FP32 arithmetic, storage 1 = f32, 2 = f16)
 cudaError_t launch_ensemble_step(const StepParams<float>* params, const EnsTile* tiles, int ntiles, int* counter,

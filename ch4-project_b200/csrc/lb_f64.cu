@@ -40,6 +40,17 @@ cudaError_t launch_averages(const AvgParams& P, int nblocks, double* out_dev, cu
   averages_final_kernel<<<1, 32, 0, st>>>(P.partial, nblocks, out_dev);
   return cudaGetLastError();
 }
+cudaError_t launch_diag(const AvgParams& P, int axis, int nblocks, double* partial, double* out, cudaStream_t st) {
+  if (axis >= 0) {
+    diag_sums_kernel<<<nblocks, DIAG_BLOCK, 0, st>>>(P, axis, out);
+    return cudaGetLastError();
+  }
+  diag_sums_kernel<<<nblocks, DIAG_BLOCK, 0, st>>>(P, -1, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
+  diag_final_kernel<<<1, 64, 0, st>>>(partial, nblocks, out);
+  return cudaGetLastError();
+}
 cudaError_t launch_particle_substep(const PartParams<double>& P, cudaStream_t st) { return part_substep_t<double>(P, st); }
 cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
                            cudaStream_t st) {

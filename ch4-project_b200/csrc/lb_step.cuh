@@ -15,9 +15,9 @@
 
 template <typename S, typename A, int set>
 __device__ __forceinline__ void load_set(const StepParams<A>& P, long long idx, A* f) {
-  const S* in = static_cast<const S*>(P.fin[set]);
 #pragma unroll
-  for (int q = 0; q < Q; q++) f[q] = Codec<S, A>::load(in, (long long)q * P.N + idx, P.w[q], P.shift[set]);
+  for (int q = 0; q < Q; q++)
+    f[q] = Codec<S, A>::load(static_cast<const S*>(P.fin_q[set][q]), idx, P.w[q], P.shift[set]);
 }
 
 // Linear-index deltas to the neighbour at c = -1 / +1 along each axis, with the
@@ -52,38 +52,38 @@ __device__ __forceinline__ int nbr_delta(const Nbr& n) {
 
 // push one set; wallmode: 0 periodic in y, 1 fluid walls, 2 value walls (T or S).
 // top/bot: this cell is the last/first interior row of a walled set (uniform per block).
-template <typename S, typename A, int set, int q>
-__device__ __forceinline__ void push_one(const StepParams<A>& P, S* out, int idx, const Nbr& nb, const A* post,
-                                         int wallmode, bool top, bool bot, bool slip_top, bool slip_bot, A fac_top,
-                                         A fac_bot) {
-  const long long N = P.N;
+// WALLS = false is the form for rows that touch no wall: every value streams to x + c_q.
+template <typename S, typename A, int set, int q, bool WALLS>
+__device__ __forceinline__ void push_one(const StepParams<A>& P, int idx, const Nbr& nb, const A* post, int wallmode,
+                                         bool top, bool bot, bool slip_top, bool slip_bot, A fac_top, A fac_bot) {
   const float sh = P.shift[set];
-  const bool hits_wall = (cy(q) > 0 && top) || (cy(q) < 0 && bot);
-  if (cy(q) != 0 && wallmode != 0 && hits_wall) {
-    if (wallmode == 1) {
-      const bool slip = cy(q) > 0 ? slip_top : slip_bot;
-      if (slip) {  // specular reflection, src/boundary_conditions.c:753,786
-        constexpr int r = qinv_y(q);
-        Codec<S, A>::store(out, (long long)r * N + (idx + nbr_delta<q, false>(nb)), post[q], P.w[r], sh);
-      } else {  // halfway bounce-back, src/boundary_conditions.c:775,798
+  if constexpr (WALLS) {
+    const bool hits_wall = (cy(q) > 0 && top) || (cy(q) < 0 && bot);
+    if (cy(q) != 0 && wallmode != 0 && hits_wall) {
+      if (wallmode == 1) {
+        const bool slip = cy(q) > 0 ? slip_top : slip_bot;
+        if (slip) {  // specular reflection, src/boundary_conditions.c:753,786
+          constexpr int r = qinv_y(q);
+          Codec<S, A>::store(static_cast<S*>(P.fout_q[set][r]), idx + nbr_delta<q, false>(nb), post[q], P.w[r], sh);
+        } else {  // halfway bounce-back, src/boundary_conditions.c:775,798
+          constexpr int r = qinv(q);
+          Codec<S, A>::store(static_cast<S*>(P.fout_q[set][r]), idx, post[q], P.w[r], sh);
+        }
+      } else {  // fixed value / flux wall: rhs(x).p[inv q] + w[inv q]*fac, src/boundary_conditions.c:1019-1027
         constexpr int r = qinv(q);
-        Codec<S, A>::store(out, (long long)r * N + idx, post[q], P.w[r], sh);
+        const A fac = cy(q) > 0 ? fac_top : fac_bot;
+        Codec<S, A>::store(static_cast<S*>(P.fout_q[set][r]), idx, post[r] + P.w[r] * fac, P.w[r], sh);
       }
-    } else {  // fixed value / flux wall: rhs(x).p[inv q] + w[inv q]*fac, src/boundary_conditions.c:1019-1027
-      constexpr int r = qinv(q);
-      const A fac = cy(q) > 0 ? fac_top : fac_bot;
-      Codec<S, A>::store(out, (long long)r * N + idx, post[r] + P.w[r] * fac, P.w[r], sh);
+      return;
     }
-  } else {
-    Codec<S, A>::store(out, (long long)q * N + (idx + nbr_delta<q, true>(nb)), post[q], P.w[q], sh);
   }
+  Codec<S, A>::store(static_cast<S*>(P.fout_q[set][q]), idx + nbr_delta<q, true>(nb), post[q], P.w[q], sh);
 }
 
-template <typename S, typename A, int set>
+template <typename S, typename A, int set, bool WALLS>
 __device__ __forceinline__ void push_set(const StepParams<A>& P, int idx, const Nbr& nb, const A* post, int wallmode,
                                          bool top, bool bot, bool slip_top, bool slip_bot, A fac_top, A fac_bot) {
-  S* out = static_cast<S*>(P.fout[set]);
-#define CH4_PUSH(Q_) push_one<S, A, set, Q_>(P, out, idx, nb, post, wallmode, top, bot, slip_top, slip_bot, fac_top, fac_bot);
+#define CH4_PUSH(Q_) push_one<S, A, set, Q_, WALLS>(P, idx, nb, post, wallmode, top, bot, slip_top, slip_bot, fac_top, fac_bot);
   CH4_PUSH(0) CH4_PUSH(1) CH4_PUSH(2) CH4_PUSH(3) CH4_PUSH(4) CH4_PUSH(5) CH4_PUSH(6) CH4_PUSH(7) CH4_PUSH(8)
   CH4_PUSH(9) CH4_PUSH(10) CH4_PUSH(11) CH4_PUSH(12) CH4_PUSH(13) CH4_PUSH(14) CH4_PUSH(15) CH4_PUSH(16)
   CH4_PUSH(17) CH4_PUSH(18)
@@ -206,8 +206,16 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
 
   const Nbr nb = neighbours(x, y, z, P.NX, P.NY, P.NZ);
   const bool toprow = y == P.NY - 1, botrow = y == 0;
-  push_set<S, A, 0>(P, idx, nb, f, (F & K_FWALL) ? 1 : 0, toprow, botrow, (F & K_FSLIP_P) != 0,
-                    (F & K_FSLIP_M) != 0, A(0), A(0));
+#ifndef CH4_NO_WALL_SPLIT
+  if (!(toprow || botrow)) {  // uniform per block: rows that touch no wall stream every value
+    push_set<S, A, 0, false>(P, idx, nb, f, 0, false, false, false, false, A(0), A(0));
+    if constexpr (THERM) push_set<S, A, 1, false>(P, idx, nb, g, 0, false, false, false, false, A(0), A(0));
+    if constexpr (SCAL) push_set<S, A, 2, false>(P, idx, nb, h, 0, false, false, false, false, A(0), A(0));
+    return;
+  }
+#endif
+  push_set<S, A, 0, true>(P, idx, nb, f, (F & K_FWALL) ? 1 : 0, toprow, botrow, (F & K_FSLIP_P) != 0,
+                          (F & K_FSLIP_M) != 0, A(0), A(0));
   if constexpr (THERM) {
     A fac_top = A(0), fac_bot = A(0);
     if (F & K_TWALL) {  // src/boundary_conditions.c:966-1081
@@ -218,7 +226,7 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
       if (F & K_TFLUX_M) T_wall = A(-0.5) * P.grad_T_bot + c.tt + P.T_ref;
       fac_bot = (F & K_TNOFLUX_M) ? A(0) : A(2) * ((T_wall - P.T_ref) - c.tt);
     }
-    push_set<S, A, 1>(P, idx, nb, g, (F & K_TWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
+    push_set<S, A, 1, true>(P, idx, nb, g, (F & K_TWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
   }
   if constexpr (SCAL) {
     A fac_top = A(0), fac_bot = A(0);
@@ -226,7 +234,7 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
       fac_top = A(2) * ((P.S_top - P.S_ref) - c.ss);
       fac_bot = A(2) * ((P.S_bot - P.S_ref) - c.ss);
     }
-    push_set<S, A, 2>(P, idx, nb, h, (F & K_SWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
+    push_set<S, A, 2, true>(P, idx, nb, h, (F & K_SWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
   }
 }
 

@@ -93,6 +93,7 @@ enum {
   CH4_F_SCALAR_INITIAL_CONSTANT_BOT = 1ull << 47,
   CH4_F_SCALAR_INITIAL_CONSTANT_TOP = 1ull << 48,
   CH4_F_FORCING_CONSTANT_POWER = 1ull << 49,  /* src/forcing.c:1154-1190 */
+  CH4_F_OUTPUT_DIAGN_APPEND = 1ull << 50,     /* ruler files appended, src/output.c:780-830 */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63
@@ -216,6 +217,35 @@ ch4_status ch4_get_hit_phases(ch4_handle *h, double *phi);
  * Non-finite positions are refused (CH4_ERR_ARG). */
 ch4_status ch4_set_particles(ch4_handle *h, const ch4_particle *parts, int n);
 ch4_status ch4_get_particles(ch4_handle *h, ch4_particle *parts, int n);
+
+/* --- dump_averages in full: volume averages, per-plane rulers, ASCII files -- */
+
+/* One record of dump_averages (the `output` fields it prints, src/output.c:63-1100):
+ * cell-centre coordinate, fluid, temperature and scalar statistics. */
+#define CH4_DIAG_FIELDS 38
+typedef struct {
+  double x, y, z;
+  double ux, uy, uz, ux2, uy2, uz2, rho, rho2, ene, eps;
+  double t, t2, epst, dxt, dyt, dzt, uxt, uyt, uzt, nux, nuy, nuz, lb;
+  double s, s2, epss, dxs, dys, dzs, uxs, uys, uzs, nusx, nusy, nusz;
+} ch4_diag;
+
+/* The volume averages (`out_all`) and, for each non-NULL array, the per-plane
+ * averages along x, y and z (`ruler_x[NX]`, `ruler_y[NY]`, `ruler_z[NZ]`) at the
+ * current state, normalised as src/output.c:495-760 does (including its use of
+ * 1/(SY*SZ) for the temperature and scalar z rulers).  Sums in FP64 on the device in
+ * a fixed order: they agree with the reference's sequential sums to rounding. */
+ch4_status ch4_diagnostics(ch4_handle *h, ch4_diag *global, ch4_diag *ruler_x, ch4_diag *ruler_y,
+                           ch4_diag *ruler_z);
+
+/* One diagnostic dump as dump_averages writes it (src/output.c:760-1100), into the
+ * directory `dir`: appends a line to velocity_averages.dat (and temperature_ /
+ * scalar_averages.dat, velocity_turbulence.dat with HIT forcing), writes -- appends
+ * with CH4_F_OUTPUT_DIAGN_APPEND -- the *_x/_y/_z.dat rulers and the *_run.dat
+ * running rulers.  The running rulers accumulate over the calls on this handle and
+ * are printed divided by `irun`, the reference's dump count (itime * time_dt /
+ * time_dump_diagn, plus one with OUTPUT_AT_START). */
+ch4_status ch4_dump_averages(ch4_handle *h, const char *dir, double time_now, int irun);
 
 /* Initial fields of initial_conditions (src/initial_conditions.c:3-500) for the
  * CH4_F_*_INITIAL_* flags, computed on the host: p, g, h as AoS [NZ][NY][NX][19]

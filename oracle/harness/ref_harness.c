@@ -15,6 +15,8 @@
  *                                  build_forcing call, i.e. after
  *                                  initialization_forcing, src/initial_conditions.c:822)
  *   in_part.bin                    npart*SIZE_OF_POINT_PARTICLE doubles
+ * out_diag.txt: every record of the final dump_averages (volume averages and the
+ *   x / y / z rulers) at full precision; its *.dat files stay beside it.
  * out_phi0.bin: the HIT phases right after initialization_forcing (before the
  *   first build_forcing walks them).
  * Outputs after <nsteps> steps (same layouts):
@@ -120,6 +122,21 @@ static void write_phases(const char *name) {
   fclose(fp);
 }
 #endif
+
+/* one `output` record of dump_averages at full precision: "<scope> <index> <field> <value>" */
+static void write_record(FILE *fp, const char *scope, int i, const output *o) {
+#define F(name) fprintf(fp, "%s %d %s %.17g\n", scope, i, #name, (double)o->name)
+#ifdef LB_FLUID
+  F(x); F(y); F(z); F(ux); F(uy); F(uz); F(ux2); F(uy2); F(uz2); F(rho); F(ene); F(eps); F(rho2);
+#endif
+#ifdef LB_TEMPERATURE
+  F(t); F(t2); F(epst); F(dxt); F(dyt); F(dzt); F(uxt); F(uyt); F(uzt); F(nux); F(nuy); F(nuz); F(lb);
+#endif
+#ifdef LB_SCALAR
+  F(s); F(s2); F(epss); F(dxs); F(dys); F(dzs); F(uxs); F(uys); F(uzs); F(nusx); F(nusy); F(nusz);
+#endif
+#undef F
+}
 
 static void dump_state(void) {
 #ifdef LB_FLUID
@@ -362,6 +379,14 @@ int main(int argc, char **argv) {
     A(s); A(s2);
 #endif
 #undef A
+    fclose(fp);
+    /* the same dump in full: volume averages and the x / y / z rulers (its *.dat files
+       are left in the working directory too) */
+    fp = fopen("out_diag.txt", "w");
+    write_record(fp, "global", 0, &out_all);
+    for (int i = 0; i < NX; i++) write_record(fp, "x", i, &ruler_x[i]);
+    for (int j = 0; j < NY; j++) write_record(fp, "y", j, &ruler_y[j]);
+    for (int k = 0; k < NZ; k++) write_record(fp, "z", k, &ruler_z[k]);
     fclose(fp);
   }
   {

@@ -56,6 +56,10 @@ FLAGSETS = {
                 "LB_FLUID_INITIAL_PERTURBATION", "LB_FLUID_INITIAL_ADD_NOISE", "LB_FLUID_INITIAL_UNIT_DENSITY",
                 "LB_TEMPERATURE_INITIAL_LINEAR", "LB_TEMPERATURE_INITIAL_ADD_PERTURBATION",
                 "LB_TEMPERATURE_INITIAL_ADD_NOISE", "LB_SCALAR_INITIAL_LINEAR", "LB_SCALAR_INITIAL_ADD_PERTURBATION"],
+    "init_const": ["LB_FLUID", "LB_TEMPERATURE", "LB_SCALAR", "LB_TEMPERATURE_INITIAL_CONSTANT",
+                   "LB_TEMPERATURE_INITIAL_CONSTANT_BOT", "LB_SCALAR_INITIAL_CONSTANT", "LB_SCALAR_INITIAL_CONSTANT_MEAN"],
+    "init_const2": ["LB_FLUID", "LB_TEMPERATURE", "LB_SCALAR", "LB_TEMPERATURE_INITIAL_CONSTANT",
+                    "LB_TEMPERATURE_INITIAL_CONSTANT_TOP", "LB_SCALAR_INITIAL_CONSTANT", "LB_SCALAR_INITIAL_CONSTANT_BOT"],
     "init_hit": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE", "LB_SCALAR",
                  "LB_FLUID_INITIAL_VORTICES", "LB_FLUID_INITIAL_KOLMOGOROV", "LB_FLUID_INITIAL_CELLULAR",
                  "LB_FLUID_INITIAL_POISEUILLE", "LB_FLUID_INITIAL_PERTURBATION", "LB_TEMPERATURE_INITIAL_CONSTANT",
@@ -188,6 +192,16 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None,
         fn = os.path.join(tmp, "out_%s.bin" % name)
         if os.path.exists(fn):
             out[name] = np.fromfile(fn, dtype=np.float64).reshape(shape)
+    fn = os.path.join(tmp, "out_diag.txt")
+    if os.path.exists(fn):
+        diag = {}
+        with open(fn) as f:
+            for line in f:
+                scope, i, field, v = line.split()
+                diag[(scope, int(i), field)] = float(v)
+        out["diag"] = diag
+        out["dat"] = {name: open(os.path.join(tmp, name)).read() for name in sorted(os.listdir(tmp))
+                      if name.endswith(".dat")}
     if lay is not None:
         arr = np.fromfile(os.path.join(tmp, "out_part.bin"), dtype=np.float64).reshape(-1, lay["size"])
         out["part"] = particles_from_ref(arr, lay)

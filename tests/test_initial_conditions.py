@@ -3,7 +3,7 @@ initialization_forcing (src/initial_conditions.c:3-592, 822-870) for the support
 *_INITIAL_* flags, bit-identical to the reference compiled from its own sources
 (oracle/_ref/init_rb, oracle/_ref/init_hit), which runs 0 steps with no injected state.
 
-The flag sets cover every supported flag, the drand48 order across the fluid,
+The five flag sets cover every supported flag, the drand48 order across the fluid,
 temperature and phase draws, and both branches of the NZ == 1 perturbation rule.
 """
 import numpy as np
@@ -17,7 +17,8 @@ from ch4b200 import abi
 PARAMS = dict(tau_u=0.6, tau_t=0.7, tau_s=0.8, Amp_x=2e-3, Amp_y=1e-3, Amp_z=5e-4, gravity_y=1e-4, beta_t=1.0,
               T_bot=1.0, T_top=0.0, T_ref=0.5, S_bot=0.3, S_top=-0.2, S_ref=0.0, noise_u=1e-3, noise_t=2e-3)
 
-CASES = [("init_rb", 12, 10, 6, 7), ("init_rb", 12, 10, 1, 8), ("init_hit", 9, 8, 7, 9)]
+CASES = [("init_rb", 12, 10, 6, 7), ("init_rb", 12, 10, 1, 8), ("init_hit", 9, 8, 7, 9), ("init_const", 6, 5, 4, 3),
+         ("init_const2", 6, 5, 4, 4)]
 
 
 def need_ref(flagset):
