@@ -304,6 +304,12 @@ def bench_ensemble(args):
     K = args.steps
     t_step = _event_time(ens.stream_handle, lambda: ens.step(K)) / K
     solves_h = len(cases) * 3600.0 / (S * t_step)
+    if args.throughput_only:  # tuning runs: the timed ensemble step alone
+        ens.close()
+        print(json.dumps({"metric": "ensemble solves/hour", "value": solves_h, "unit": "solves/h",
+                          "ensemble_mlups": cells / t_step / 1e6, "tile_block": block, "tile_rows": rows,
+                          "throughput_only": True}))
+        return 0
     # the rest of the solve: T fields of the sampled cases at the short horizon, then Nu over [S/2, S]
     done = 100 + K
     nu_ens = {i: [] for i in sample}
@@ -533,6 +539,7 @@ def main():
     ap.add_argument("--sample", type=int, default=16)
     ap.add_argument("--short-horizon", type=int, default=2000)
     ap.add_argument("--laminar-cases", type=int, default=8)
+    ap.add_argument("--throughput-only", action="store_true")
     ap.add_argument("--laminar-steps", type=int, default=200000)
     ap.add_argument("--requests", type=int, default=24)
     ap.add_argument("--cells-in-flight", type=int, default=8 << 20)

@@ -82,6 +82,7 @@ def lib():
         L.ch4_initial_conditions.argtypes = [P]
         L.ch4_diagnostics.argtypes = [P, D, D, D, D]
         L.ch4_dump_averages.argtypes = [P, C.c_char_p, C.c_double, C.c_int]
+        L.ch4_dump_fields_ascii.argtypes = [P, C.c_char_p, C.c_int]
         V = C.c_void_p
         L.ch4_averages_noalloc.argtypes = [V, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                            C.c_double, V, V]
@@ -260,6 +261,10 @@ class Simulation:
         """ch4_dump_averages: the reference's dump_averages ASCII files in `directory`."""
         self._check(lib().ch4_dump_averages(self.h, str(directory).encode(), float(time_now), int(irun)),
                     "dump_averages")
+
+    def dump_fields_ascii(self, directory, itime):
+        """ch4_dump_fields_ascii: the OUTPUT_ASCII vel/temp/scal.<itime> files in `directory`."""
+        self._check(lib().ch4_dump_fields_ascii(self.h, str(directory).encode(), int(itime)), "dump_fields_ascii")
 
     @property
     def stream_handle(self):

@@ -70,6 +70,7 @@ FLAGS = {
     "LB_SCALAR_INITIAL_CONSTANT_TOP": 1 << 48,
     "LB_FLUID_FORCING_CONSTANT_POWER": 1 << 49,
     "OUTPUT_DIAGN_APPEND": 1 << 50,
+    "LAGRANGE_GRAVITY": 1 << 51,
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 

@@ -62,7 +62,7 @@ const uint64_t SUPPORTED =
     CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION | CH4_F_TEMPERATURE_INITIAL_ADD_NOISE | CH4_F_SCALAR_INITIAL_LINEAR |
     CH4_F_SCALAR_INITIAL_ADD_PERTURBATION | CH4_F_SCALAR_INITIAL_CONSTANT | CH4_F_SCALAR_INITIAL_CONSTANT_MEAN |
     CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
-    CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND;
+    CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND | CH4_F_LAGRANGE_GRAVITY;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -546,6 +546,10 @@ struct Engine : EngineBase {
     Q.dtl = c.time_dt / c.time_dt_lagr_factor;
     Q.gradient = (c.flags & CH4_F_LAGRANGE_GRADIENT) != 0;
     Q.addedmass = (c.flags & CH4_F_LAGRANGE_ADDEDMASS) != 0;
+    Q.gravity = (c.flags & CH4_F_LAGRANGE_GRAVITY) != 0;
+    Q.g[0] = c.gravity_x;
+    Q.g[1] = c.gravity_y;
+    Q.g[2] = c.gravity_z;
     Q.pf = pf;
     Q.u = upart;
     Q.t = tpart;
@@ -1117,7 +1121,8 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
-  const bool grav = forcing && (fl & (CH4_F_TEMPERATURE_BUOYANCY | CH4_F_SCALAR_BUOYANCY));
+  const bool grav = (forcing && (fl & (CH4_F_TEMPERATURE_BUOYANCY | CH4_F_SCALAR_BUOYANCY))) ||
+                    (fl & CH4_F_LAGRANGE_GRAVITY);
   std::vector<K> keys = {
       {"resume", &resume, true}, {"NX", &NX, true}, {"NY", &NY, true}, {"NZ", &NZ, true}, {"SX", &cfg->SX, true}, {"SY", &cfg->SY, true},
       {"SZ", &cfg->SZ, true}, {"time_dt", &cfg->time_dt, true}, {"tau_u", &cfg->tau_u, true},
@@ -1236,6 +1241,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_SCALAR_INITIAL_CONSTANT_TOP", CH4_F_SCALAR_INITIAL_CONSTANT_TOP},
       {"LB_FLUID_FORCING_CONSTANT_POWER", CH4_F_FORCING_CONSTANT_POWER},
       {"OUTPUT_DIAGN_APPEND", CH4_F_OUTPUT_DIAGN_APPEND},
+      {"LAGRANGE_GRAVITY", CH4_F_LAGRANGE_GRAVITY},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -1614,6 +1620,45 @@ ch4_status ch4_dump_averages(ch4_handle* h, const char* dir, double time_now, in
     if (!block("scalar_averages", fs, fs)) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
   }
   return CH4_OK;
+}
+
+ch4_status ch4_dump_fields_ascii(ch4_handle* h, const char* dir, int itime) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  const size_t n = (size_t)c.NX * c.NY * c.NZ;
+  std::vector<double> dens(n), u(3 * n), t, s;
+  if (c.flags & CH4_F_LB_TEMPERATURE) t.resize(n);
+  if (c.flags & CH4_F_LB_SCALAR) s.resize(n);
+  ch4_status st = h->eng->fields(dens.data(), u.data(), t.empty() ? nullptr : t.data(), s.empty() ? nullptr : s.data(),
+                                 nullptr, 0);
+  if (st) return st;
+  auto dump = [&](const char* stem, int ncol, auto&& row) {
+    char name[64];
+    std::snprintf(name, sizeof name, "%s.%d", stem, itime);
+    FILE* f = open_in(dir, name, "w");
+    if (!f) return false;
+    for (int k = 0; k < c.NZ; k++) {
+      for (int j = 0; j < c.NY; j++) {
+        for (int i = 0; i < c.NX; i++) {
+          const size_t idx = ((size_t)k * c.NY + j) * c.NX + i;
+          std::fprintf(f, "%e %e %e", (double)i + 0.5, (double)j + 0.5, (double)k + 0.5);
+          row(f, idx);
+          std::fprintf(f, "\n");
+        }
+        std::fprintf(f, "\n");
+      }
+      std::fprintf(f, "\n");
+    }
+    std::fclose(f);
+    (void)ncol;
+    return true;
+  };
+  bool ok = dump("vel", 7, [&](FILE* f, size_t idx) {
+    std::fprintf(f, " %e %e %e %e", u[3 * idx], u[3 * idx + 1], u[3 * idx + 2], dens[idx]);
+  });
+  if (ok && !t.empty()) ok = dump("temp", 4, [&](FILE* f, size_t idx) { std::fprintf(f, " %e", t[idx]); });
+  if (ok && !s.empty()) ok = dump("scal", 4, [&](FILE* f, size_t idx) { std::fprintf(f, " %e", s[idx]); });
+  return ok ? CH4_OK : h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
 }
 
 ch4_status ch4_step(ch4_handle* h, int nsteps) {
@@ -2206,7 +2251,7 @@ ch4_status ch4_ensemble_tune(ch4_ensemble* E, int* block_out, int* rows_out) {
     }
   }
   const int blocks[] = {64, 128, 256};  // the kernel is built for at most 256 threads
-  const int rowsv[] = {1, 2, 4, 8};
+  const int rowsv[] = {1, 2, 4, 8, 16, 32};
   float best = 1e30f;
   int bb = E->block, br = E->rows;
   cudaEvent_t e0, e1;

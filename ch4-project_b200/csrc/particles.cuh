@@ -37,6 +37,8 @@ struct PartParams {
   int first;      // itime == 1 && resume == 0 (src/lagrange.c:3190)
   int gradient;   // LAGRANGE_GRADIENT
   int addedmass;  // LAGRANGE_ADDEDMASS
+  int gravity;    // LAGRANGE_GRAVITY
+  double g[3];    // gravity_x, gravity_y, gravity_z
   double* pf;     // [PF_TOTAL][np]
   const A* u;     // 3 SoA planes of u^{n+1}
   const A* t;     // t^{n+1} = m(g^{n+1}) with LB_TEMPERATURE, else null
@@ -285,9 +287,19 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     const double invtau = 1.0 / tau;
     double vx = F(vx), vy = F(vy), vz = F(vz);
     double ax = (ux - vx) * invtau, ay = (uy - vy) * invtau, az = (uz - vz) * invtau;
+    if (P.gravity) {  // -g, src/lagrange.c:3312-3323
+      ax -= P.g[0];
+      ay -= P.g[1];
+      az -= P.g[2];
+    }
     const double beta = F(beta_coeff);
     double uxo = F(ux_old), uyo = F(uy_old), uzo = F(uz_old);
     if (P.addedmass && beta != 0.0) {
+      if (P.gravity) {  // -(-beta) g, src/lagrange.c:3330-3339
+        ax -= (-beta) * P.g[0];
+        ay -= (-beta) * P.g[1];
+        az -= (-beta) * P.g[2];
+      }
       if (first) {
         uxo = ux;
         uyo = uy;
@@ -359,7 +371,8 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   make_stencil(px, py, pz, t);
   const double fac = pf[(long long)PF_VOL * np + ip], dr = pf[(long long)PF_DR * np + ip];
   const bool live = inside && (fac > 0.0) && F(beta_coeff) != 0.0;
-  const double gx = 0.0, gy = 0.0, gz = 0.0;
+  // gravity_vector of src/lagrange_feedback.c:95-103 (y points down)
+  const double gx = P.gravity ? P.g[0] : 0.0, gy = P.gravity ? -P.g[1] : 0.0, gz = P.gravity ? P.g[2] : 0.0;
   double* r = P.rec;
   r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
   r[1LL * np + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;

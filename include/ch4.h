@@ -94,6 +94,7 @@ enum {
   CH4_F_SCALAR_INITIAL_CONSTANT_TOP = 1ull << 48,
   CH4_F_FORCING_CONSTANT_POWER = 1ull << 49,  /* src/forcing.c:1154-1190 */
   CH4_F_OUTPUT_DIAGN_APPEND = 1ull << 50,     /* ruler files appended, src/output.c:780-830 */
+  CH4_F_LAGRANGE_GRAVITY = 1ull << 51,        /* -g on inertial particles, src/lagrange.c:3312-3339 */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63
@@ -246,6 +247,12 @@ ch4_status ch4_diagnostics(ch4_handle *h, ch4_diag *global, ch4_diag *ruler_x, c
  * are printed divided by `irun`, the reference's dump count (itime * time_dt /
  * time_dump_diagn, plus one with OUTPUT_AT_START). */
 ch4_status ch4_dump_averages(ch4_handle *h, const char *dir, double time_now, int irun);
+
+/* The OUTPUT_ASCII field dumps of dump_averages (src/output.c:1107-1200): dir/vel.<itime>
+ * (x y z ux uy uz rho per cell), dir/temp.<itime> and dir/scal.<itime> (x y z value),
+ * cells in the reference's k, j, i order with a blank line after every row and plane.
+ * The reference writes them into RUN/ (OutDir). */
+ch4_status ch4_dump_fields_ascii(ch4_handle *h, const char *dir, int itime);
 
 /* Initial fields of initial_conditions (src/initial_conditions.c:3-500) for the
  * CH4_F_*_INITIAL_* flags, computed on the host: p, g, h as AoS [NZ][NY][NX][19]

@@ -501,7 +501,17 @@ static void move_particle(const ch4o_state *s, ch4_particle *p, int first, doubl
     p->ax = (p->ux - p->vx) * invtau;
     p->ay = (p->uy - p->vy) * invtau;
     p->az = (p->uz - p->vz) * invtau;
+    if (s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) { /* -g, src/lagrange.c:3312-3323 */
+      p->ax -= s->cfg.gravity_x;
+      p->ay -= s->cfg.gravity_y;
+      p->az -= s->cfg.gravity_z;
+    }
     if ((s->cfg.flags & CH4_F_LAGRANGE_ADDEDMASS) && p->beta_coeff != 0.0) {
+      if (s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) { /* -(-beta) g, src/lagrange.c:3330-3339 */
+        p->ax -= (-(p->beta_coeff)) * s->cfg.gravity_x;
+        p->ay -= (-(p->beta_coeff)) * s->cfg.gravity_y;
+        p->az -= (-(p->beta_coeff)) * s->cfg.gravity_z;
+      }
       if (first) {
         p->ux_old = p->ux;
         p->uy_old = p->uy;
@@ -605,7 +615,10 @@ static void deposit(const ch4o_state *s, double *D) {
     if (!(fac > 0.0) || p->beta_coeff == 0.0) continue;
     stencil_t t;
     stencil(s, p, &t);
-    const double gx = 0.0, gy = 0.0, gz = 0.0;
+    /* gravity_vector of src/lagrange_feedback.c:95-103: y points down */
+    const int grav = (s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) != 0;
+    const double gx = grav ? s->cfg.gravity_x : 0.0, gy = grav ? -s->cfg.gravity_y : 0.0,
+                 gz = grav ? s->cfg.gravity_z : 0.0;
     double fp[3];
     fp[0] = p->Dt_ux - gx + dr * (gx - p->ax);
     fp[1] = p->Dt_uy - gy + dr * (gy - p->ay);

@@ -44,6 +44,9 @@ FLAGSETS = {
             "LB_FLUID_BC_Y", "LB_FLUID_LES"],
     "particles": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                   "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    "particles_g": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                    "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                    "LAGRANGE_GRAVITY"],
     "particles_t": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE",
                     "LB_TEMPERATURE_BUOYANCY", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
                     "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
@@ -51,6 +54,8 @@ FLAGSETS = {
                "LB_FLUID_FORCING_NOZEROMODE", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY"],
     "cpower": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_FLUID_FORCING_NOZEROMODE",
                "LB_FLUID_FORCING_CONSTANT_POWER"],
+    "ascii": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+              "LB_TEMPERATURE_BC_Y"],
     "init_rb": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
                 "LB_TEMPERATURE_BC_Y", "LB_SCALAR", "LB_SCALAR_BC_Y", "LB_INITIAL_BAROMETRIC",
                 "LB_FLUID_INITIAL_PERTURBATION", "LB_FLUID_INITIAL_ADD_NOISE", "LB_FLUID_INITIAL_UNIT_DENSITY",
@@ -113,12 +118,13 @@ PARAM_KEYS = ["resume", "resume_u", "resume_t", "resume_s", "NX", "NY", "NZ", "S
               "beta_coeff_types", "beta_coeff_min", "beta_coeff_max", "noise_u", "noise_t"]
 
 
-def write_param_in(path, cfg, nsteps=1):
+def write_param_in(path, cfg, nsteps=1, overrides=None):
     vals = {"resume": int(cfg.resume), "resume_u": 0, "resume_t": 0, "resume_s": 0,
             "time_start": 0.0, "time_end": float(nsteps), "time_dump_field": 1e12,
             "time_dump_diagn": 1e12, "time_dump_lagr": 1e12,
             "tau_drag_types": 1, "tau_drag_min": 1.0, "tau_drag_max": 1.0,
             "beta_coeff_types": 1, "beta_coeff_min": 1.0, "beta_coeff_max": 1.0}
+    vals.update(overrides or {})
     with open(path, "w") as f:
         for k in PARAM_KEYS:
             v = vals[k] if k in vals else getattr(cfg, k)
@@ -160,7 +166,7 @@ def particles_as_dict(parts):
     return {n: np.array([getattr(p, n) for p in parts]) for n in abi.PARTICLE_FIELDS}
 
 
-def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None, parts=None):
+def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None, parts=None, params=None):
     """Run the compiled reference on injected populations.
 
     pops: dict which -> AoS array [NZ][NY][NX][NPOP] (interior cells).
@@ -170,7 +176,7 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None,
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     tmp = workdir or tempfile.mkdtemp(prefix="ch4ref_")
-    write_param_in(os.path.join(tmp, "param.in"), cfg, nsteps)
+    write_param_in(os.path.join(tmp, "param.in"), cfg, nsteps, params)
     for which, arr in pops.items():
         np.ascontiguousarray(arr, dtype=np.float64).tofile(os.path.join(tmp, "in_%s.bin" % which))
     if phi is not None:
@@ -202,6 +208,9 @@ def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None,
         out["diag"] = diag
         out["dat"] = {name: open(os.path.join(tmp, name)).read() for name in sorted(os.listdir(tmp))
                       if name.endswith(".dat")}
+    run_dir = os.path.join(tmp, "RUN")
+    if os.path.isdir(run_dir):  # OutDir files (OUTPUT_ASCII field dumps)
+        out["run"] = {name: open(os.path.join(run_dir, name)).read() for name in sorted(os.listdir(run_dir))}
     if lay is not None:
         arr = np.fromfile(os.path.join(tmp, "out_part.bin"), dtype=np.float64).reshape(-1, lay["size"])
         out["part"] = particles_from_ref(arr, lay)

@@ -85,3 +85,23 @@ def test_running_rulers_average_over_calls(tmp_path):
     assert run.shape == (cfg.NY, 14)
     assert np.allclose(run[:, 1], 0.5 * (r1["t"] + r2["t"]), rtol=2e-6, atol=1e-12)
     assert len(np.loadtxt(tmp_path / "velocity_averages.dat", ndmin=2)) == 2
+
+
+def test_ascii_field_dumps_identical_to_reference(tmp_path):
+    """OUTPUT_ASCII (flag set "ascii" = "rb" + OUTPUT_ASCII, time_dump_field = time_dt): the
+    FP64 fields are bit-identical to the reference, so vel.<itime> and temp.<itime> are the
+    same text byte for byte."""
+    _, cfg, state = make_case("rb", seed=25)
+    if not O.ref_available("ascii"):
+        pytest.skip("reference build missing")
+    nsteps = 9
+    ref = O.run_reference("ascii", cfg, nsteps, dict(pop_items(state)), params={"time_dump_field": 1.0})
+    with ch4b200.Simulation(cfg) as sim:
+        for k, v in pop_items(state):
+            sim.set_pop(k, v)
+        sim.initialize()
+        sim.step(nsteps)
+        sim.dump_fields_ascii(tmp_path, nsteps)
+    assert sorted(ref["run"]) == ["temp.%d" % nsteps, "vel.%d" % nsteps]
+    for name, text in ref["run"].items():
+        assert (tmp_path / name).read_text() == text, name
