@@ -17,6 +17,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/ch4.h"
@@ -27,6 +28,20 @@ using namespace ch4;
 namespace {
 
 constexpr int NPOP = Q;
+
+// body(i0, i1) over [0, n), split across up to 8 host threads (one thread when n is
+// below 2 * grain).  Host<->pinned copies run at a few GB/s per thread; the first
+// touch of a freshly allocated caller array faults its pages in the same threads.
+template <class F>
+void host_parallel(size_t n, size_t grain, F&& body) {
+  const size_t hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const size_t nt = std::min(hw, std::max<size_t>(1, n / std::max<size_t>(1, grain)));
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < nt; t++) pool.emplace_back([&body, n, nt, t] { body(n * t / nt, n * (t + 1) / nt); });
+  body(0, n / nt);
+  for (auto& th : pool) th.join();
+}
+
 const double VK[NK][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}};
 
 // lattice constants of design_lb (src/lb.c:139-160, 368-377), host FP64
@@ -447,6 +462,10 @@ struct Engine : EngineBase {
   A *hit_last = nullptr;  // tables of the latest phases (those of F^n)
   double* staging_d = nullptr;  // device AoS chunk
   double* staging_h = nullptr;  // pinned host chunk
+  // second pair: the host fills one pinned chunk while the other is copied and converted
+  double* staging_d2 = nullptr;
+  double* staging_h2 = nullptr;
+  cudaEvent_t up_ev[2] = {nullptr, nullptr};
   A* hit_h = nullptr;           // pinned host phase tables
   cudaEvent_t hit_ev = nullptr;
   size_t chunk_planes = 0;
@@ -500,6 +519,10 @@ struct Engine : EngineBase {
     cudaFree(hit_last);
     cudaFree(staging_d);
     if (staging_h) cudaFreeHost(staging_h);
+    cudaFree(staging_d2);
+    if (staging_h2) cudaFreeHost(staging_h2);
+    for (cudaEvent_t e : up_ev)
+      if (e) cudaEventDestroy(e);
     if (hit_h) cudaFreeHost(hit_h);
     if (hit_ev) cudaEventDestroy(hit_ev);
     free_particles();
@@ -791,6 +814,13 @@ struct Engine : EngineBase {
     chunk_planes = std::max<size_t>(1, std::min<size_t>((size_t)c.NZ, (64u << 20) / plane));
     if (cudaMalloc(&staging_d, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "staging");
     if (cudaMallocHost(&staging_h, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "pinned staging");
+    if (chunk_planes < (size_t)c.NZ) {  // more than one chunk: double-buffer the upload
+      if (cudaMalloc(&staging_d2, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "staging");
+      if (cudaMallocHost(&staging_h2, chunk_planes * plane) != cudaSuccess)
+        return H->fail(CH4_ERR_NOMEM, "pinned staging");
+    }
+    for (cudaEvent_t& e : up_ev)
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "event");
     fill_params();
     // rest state p = w (src/initial_conditions.c:45), g = h = 0
     std::vector<double> rest((size_t)c.NX * c.NY * NPOP * chunk_planes);
@@ -845,31 +875,46 @@ struct Engine : EngineBase {
   }
 
   // AoS (halo-padded by brd) -> device SoA; `repeat` uploads the same chunk to every slab
+  // Reference-layout AoS (with `brd` halo) -> device SoA, in z-slab chunks through
+  // pinned staging.  With two staging pairs the host copies chunk k+1 (rows split over
+  // host threads) while chunk k is transferred and converted.
   ch4_status upload_chunks(int set, const double* aos, int brd, bool repeat) {
     const size_t row = (size_t)c.NX * NPOP;
     const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
     bind_pops(cur);
+    double* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
+    double* db[2] = {staging_d, staging_d2 ? staging_d2 : staging_d};
+    int b = 0;
+    ch4_status st;
     for (int z0 = 0; z0 < c.NZ; z0 += (int)chunk_planes) {
       int nz = std::min<int>((int)chunk_planes, c.NZ - z0);
       const double* src;
       if (repeat) {
         src = aos;
       } else {
-        for (int zl = 0; zl < nz; zl++)
-          for (int y = 0; y < c.NY; y++)
-            std::memcpy(staging_h + ((size_t)zl * c.NY + y) * row,
-                        aos + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, row * sizeof(double));
-        src = staging_h;
+        // the copy out of hb[b] two chunks ago must be finished before it is refilled
+        if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "upload wait"))) return st;
+        double* dst = hb[b];
+        host_parallel((size_t)nz * c.NY, 64, [&](size_t r0, size_t r1) {
+          for (size_t r = r0; r < r1; r++) {
+            const size_t zl = r / c.NY, y = r % c.NY;
+            std::memcpy(dst + r * row, aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
+                        row * sizeof(double));
+          }
+        });
+        src = dst;
       }
-      ch4_status st = H->cuda(cudaMemcpyAsync(staging_d, src, (size_t)nz * c.NY * row * sizeof(double),
-                                              cudaMemcpyHostToDevice, H->stream),
-                              "upload");
-      if (st) return st;
-      if ((st = H->cuda(launch_aos_to_soa(P, shape, set, staging_d, f[set][cur], z0, nz, H->stream), "aos_to_soa")))
+      if ((st = H->cuda(cudaMemcpyAsync(db[b], src, (size_t)nz * c.NY * row * sizeof(double), cudaMemcpyHostToDevice,
+                                        H->stream),
+                        "upload")))
         return st;
-      if ((st = H->cuda(cudaStreamSynchronize(H->stream), "upload sync"))) return st;
+      if ((st = H->cuda(launch_aos_to_soa(P, shape, set, db[b], f[set][cur], z0, nz, H->stream), "aos_to_soa")))
+        return st;
+      if ((st = H->cuda(cudaEventRecord(up_ev[b], H->stream), "upload event"))) return st;
+      if (repeat && (st = H->cuda(cudaStreamSynchronize(H->stream), "upload sync"))) return st;
+      if (staging_h2) b ^= 1;
     }
-    return CH4_OK;
+    return H->cuda(cudaStreamSynchronize(H->stream), "upload sync");
   }
 
   ch4_status set_pop(int set, const double* aos, int brd) override {
@@ -883,20 +928,37 @@ struct Engine : EngineBase {
     const size_t row = (size_t)c.NX * NPOP;
     const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
     bind_pops(cur);
-    for (int z0 = 0; z0 < c.NZ; z0 += (int)chunk_planes) {
-      int nz = std::min<int>((int)chunk_planes, c.NZ - z0);
-      ch4_status st;
-      if ((st = H->cuda(launch_soa_to_aos(P, shape, set, f[set][cur], staging_d, z0, nz, H->stream), "soa_to_aos")))
-        return st;
-      if ((st = H->cuda(cudaMemcpyAsync(staging_h, staging_d, (size_t)nz * c.NY * row * sizeof(double),
+    // chunk k+1 is converted and transferred while the host threads unpack chunk k
+    double* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
+    double* db[2] = {staging_d, staging_d2 ? staging_d2 : staging_d};
+    const int nchunks = (int)((c.NZ + chunk_planes - 1) / chunk_planes);
+    const int depth = staging_h2 ? 2 : 1;
+    ch4_status st;
+    auto issue = [&](int k) -> ch4_status {
+      const int z0 = k * (int)chunk_planes, nz = std::min<int>((int)chunk_planes, c.NZ - z0), b = k & 1;
+      ch4_status s2;
+      if ((s2 = H->cuda(launch_soa_to_aos(P, shape, set, f[set][cur], db[b], z0, nz, H->stream), "soa_to_aos")))
+        return s2;
+      if ((s2 = H->cuda(cudaMemcpyAsync(hb[b], db[b], (size_t)nz * c.NY * row * sizeof(double),
                                         cudaMemcpyDeviceToHost, H->stream),
                         "download")))
-        return st;
-      if ((st = H->cuda(cudaStreamSynchronize(H->stream), "download sync"))) return st;
-      for (int zl = 0; zl < nz; zl++)
-        for (int y = 0; y < c.NY; y++)
-          std::memcpy(aos + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
-                      staging_h + ((size_t)zl * c.NY + y) * row, row * sizeof(double));
+        return s2;
+      return H->cuda(cudaEventRecord(up_ev[b], H->stream), "download event");
+    };
+    for (int k = 0; k < std::min(depth, nchunks); k++)
+      if ((st = issue(k))) return st;
+    for (int k = 0; k < nchunks; k++) {
+      const int z0 = k * (int)chunk_planes, nz = std::min<int>((int)chunk_planes, c.NZ - z0), b = k & 1;
+      if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "download sync"))) return st;
+      const double* srcb = hb[b];
+      host_parallel((size_t)nz * c.NY, 64, [&](size_t r0, size_t r1) {
+        for (size_t r = r0; r < r1; r++) {
+          const size_t zl = r / c.NY, y = r % c.NY;
+          std::memcpy(aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, srcb + r * row,
+                      row * sizeof(double));
+        }
+      });
+      if (k + depth < nchunks && (st = issue(k + depth))) return st;
     }
     return CH4_OK;
   }
@@ -1021,11 +1083,67 @@ struct Engine : EngineBase {
     return CH4_OK;
   }
 
+  // device array -> caller's host array through the two pinned staging buffers: chunk
+  // k+1 is in flight while host threads copy chunk k out
+  ch4_status download_bounce(const double* dsrc, double* hdst, size_t count) {
+    const size_t cap = chunk_planes * (size_t)c.NX * c.NY * NPOP;
+    double* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
+    const size_t nchunks = (count + cap - 1) / cap;
+    const size_t depth = staging_h2 ? 2 : 1;
+    ch4_status st;
+    auto issue = [&](size_t k) {
+      const size_t b = depth == 2 ? (k & 1) : 0, len = std::min(cap, count - k * cap);
+      ch4_status s2 = H->cuda(
+          cudaMemcpyAsync(hb[b], dsrc + k * cap, len * sizeof(double), cudaMemcpyDeviceToHost, H->stream), "download");
+      return s2 ? s2 : H->cuda(cudaEventRecord(up_ev[b], H->stream), "download event");
+    };
+    for (size_t k = 0; k < std::min(depth, nchunks); k++)
+      if ((st = issue(k))) return st;
+    for (size_t k = 0; k < nchunks; k++) {
+      const size_t b = depth == 2 ? (k & 1) : 0, len = std::min(cap, count - k * cap);
+      if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "download sync"))) return st;
+      const double* srcb = hb[b];
+      double* out = hdst + k * cap;
+      host_parallel(len, 1 << 16, [&](size_t i0, size_t i1) {
+        std::memcpy(out + i0, srcb + i0, (i1 - i0) * sizeof(double));
+      });
+      if (k + depth < nchunks && (st = issue(k + depth))) return st;
+    }
+    return CH4_OK;
+  }
+
   ch4_status fields(double* dens, double* u, double* t, double* s, double* force, int brd) override {
     bind_pops(cur);
     ch4_status st;
     double* d = nullptr;
     const size_t n1 = (size_t)N;
+    if (brd == 0) {
+      // only the requested fields, straight into the caller's arrays; vectors are
+      // interleaved on the device
+      if ((st = H->cuda(cudaMalloc(&d, 12 * n1 * sizeof(double)), "fields scratch"))) return st;
+      double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *dfo = d + 6 * n1, *vec = d + 9 * n1;
+      const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
+      st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, fm_last(), dens ? dd : nullptr,
+                                u ? du : nullptr, t && nsets_on[1] ? dt : nullptr, s && nsets_on[2] ? ds : nullptr,
+                                force ? dfo : nullptr, nullptr, H->stream),
+                   "hydro");
+      if (!st && dens) st = download_bounce(dd, dens, n1);
+      if (!st && u && !(st = H->cuda(launch_interleave3(du, vec, (long long)n1, H->stream), "interleave")))
+        st = download_bounce(vec, u, 3 * n1);
+      if (!st && t) {
+        if (nsets_on[1]) st = download_bounce(dt, t, n1);
+        else std::fill(t, t + n1, 0.0);
+      }
+      if (!st && s) {
+        if (nsets_on[2]) st = download_bounce(ds, s, n1);
+        else std::fill(s, s + n1, 0.0);
+      }
+      if (!st && force && !(st = H->cuda(launch_interleave3(dfo, vec, (long long)n1, H->stream), "interleave")))
+        st = download_bounce(vec, force, 3 * n1);
+      cudaStreamSynchronize(H->stream);
+      cudaFree(d);
+      return st;
+    }
     // scratch planes: dens | u (3) | t | s | force (3)
     if ((st = H->cuda(cudaMalloc(&d, 9 * n1 * sizeof(double)), "fields scratch"))) return st;
     double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *dfo = d + 6 * n1;

@@ -46,6 +46,8 @@ cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape s, int se
                               int nz, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
                               int nz, cudaStream_t st);
+// vec[3 i + a] = planes[a n + i], a = 0..2 (planar vector field -> interleaved)
+cudaError_t launch_interleave3(const double* planes, double* vec, long long n, cudaStream_t st);
 
 // Lagrangian particles: one sub-step (interpolate + move + wrap)
 cudaError_t launch_particle_substep(const PartParams<double>& P, cudaStream_t st);

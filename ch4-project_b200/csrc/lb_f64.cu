@@ -8,6 +8,23 @@
 #include "lb_launch.inc"
 
 namespace ch4 {
+namespace {
+__global__ void interleave3_kernel(const double* __restrict__ planes, double* __restrict__ vec, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = planes[i], b = planes[n + i], c = planes[2 * n + i];
+  vec[3 * i] = a;
+  vec[3 * i + 1] = b;
+  vec[3 * i + 2] = c;
+}
+}  // namespace
+
+cudaError_t launch_interleave3(const double* planes, double* vec, long long n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  interleave3_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(planes, vec, n);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_step(const StepParams<double>& P, LaunchShape s, cudaStream_t st) {
   return step_t<double, double>(P, s, st);
 }
