@@ -474,7 +474,14 @@ struct Engine : EngineBase {
   LaunchShape shape{};
   // Lagrangian particles
   int np = 0;
-  double* pf = nullptr;   // [PF_TOTAL][np]
+  double* pf = nullptr;   // [PF_TOTAL][np], by state slot (kept in home-cell order)
+  int* pid = nullptr;     // caller's particle index of every state slot
+  double* pf_alt = nullptr;
+  int* pid_alt = nullptr;
+  int since_reorder = 0;
+  // re-sort of the state slots by home cell every REORDER_EVERY steps (a particle
+  // moves well under a cell in that time, so the order stays close to sorted)
+  static constexpr int REORDER_EVERY = 4;
   A* upart = nullptr;     // u^{n+1} for the interpolation, 3 planes
   A* tpart = nullptr;     // t^{n+1} for the interpolation (LB_TEMPERATURE)
   A* dbuf[2] = {nullptr, nullptr};  // two-way deposit of this / previous step
@@ -482,6 +489,8 @@ struct Engine : EngineBase {
   unsigned int *key = nullptr, *key2 = nullptr;
   int *order = nullptr, *order2 = nullptr;
   double* rec = nullptr;
+  double* srec = nullptr;
+  int* spid = nullptr;
   int *cstart = nullptr, *cend = nullptr;
   int* pstatus = nullptr;  // particle position check of the kernels (sticky until set_particles)
   // global force corrections (NOZEROMODE / CONSTANT_POWER): two slots of 6, the
@@ -539,11 +548,20 @@ struct Engine : EngineBase {
 
   void free_particles() {
     cudaFree(pf);
+    cudaFree(pf_alt);
+    cudaFree(pid);
+    cudaFree(pid_alt);
+    pf_alt = nullptr;
+    pid = pid_alt = nullptr;
     cudaFree(key);
     cudaFree(key2);
     cudaFree(order);
     cudaFree(order2);
     cudaFree(rec);
+    cudaFree(srec);
+    cudaFree(spid);
+    srec = nullptr;
+    spid = nullptr;
     cudaFree(cubtmp);
     pf = nullptr;
     key = key2 = nullptr;
@@ -574,11 +592,16 @@ struct Engine : EngineBase {
     Q.g[1] = c.gravity_y;
     Q.g[2] = c.gravity_z;
     Q.pf = pf;
+    Q.pid = pid;
+    Q.pf_alt = pf_alt;
+    Q.pid_alt = pid_alt;
     Q.u = upart;
     Q.t = tpart;
     Q.key = key;
     Q.order = order;
     Q.rec = rec;
+    Q.srec = srec;
+    Q.spid = spid;
     Q.cell_start = cstart;
     Q.cell_end = cend;
     Q.dep = dbuf[dcur_i];
@@ -682,15 +705,20 @@ struct Engine : EngineBase {
     if (n != np) {
       free_particles();
       if (n > 0) {
-        if (cudaMalloc(&pf, sizeof(double) * PF_TOTAL * (size_t)n) != cudaSuccess)
+        if (cudaMalloc(&pf, sizeof(double) * PF_TOTAL * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&pf_alt, sizeof(double) * PF_TOTAL * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&pid, sizeof(int) * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&pid_alt, sizeof(int) * (size_t)n) != cudaSuccess)
           return H->fail(CH4_ERR_NOMEM, "particle state");
-        if (twoway()) {
+        {
           bool ok = cudaMalloc(&key, sizeof(unsigned) * n) == cudaSuccess &&
                     cudaMalloc(&key2, sizeof(unsigned) * n) == cudaSuccess &&
                     cudaMalloc(&order, sizeof(int) * n) == cudaSuccess &&
                     cudaMalloc(&order2, sizeof(int) * n) == cudaSuccess &&
-                    cudaMalloc(&rec, sizeof(double) * 9 * (size_t)n) == cudaSuccess;
-          if (!ok) return H->fail(CH4_ERR_NOMEM, "deposit buffers");
+                    (!twoway() || (cudaMalloc(&rec, sizeof(double) * 9 * (size_t)n) == cudaSuccess &&
+                                   cudaMalloc(&srec, sizeof(double) * 9 * (size_t)n) == cudaSuccess &&
+                                   cudaMalloc(&spid, sizeof(int) * (size_t)n) == cudaSuccess));
+          if (!ok) return H->fail(CH4_ERR_NOMEM, "sort buffers");
           np = n;
           PartParams<A> Q = part_params();
           size_t bytes = 0;
@@ -718,6 +746,21 @@ struct Engine : EngineBase {
     }
     if ((st = H->cuda(cudaMemcpy(pf, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice), "particles up")))
       return st;
+    std::vector<int> ids(n);
+    for (int i = 0; i < n; i++) ids[i] = i;
+    since_reorder = REORDER_EVERY;  // sort at the first opportunity
+    return H->cuda(cudaMemcpy(pid, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "particle ids up");
+  }
+
+  // slot order <- order2 (sorted by home cell); with sort, compute and sort the keys here
+  ch4_status reorder_particles(int sort) {
+    PartParams<A> Q = part_params();
+    size_t bytes = cubbytes;
+    ch4_status st = H->cuda(launch_particle_reorder(Q, key2, order2, cubtmp, bytes, sort, H->stream), "reorder");
+    if (st) return st;
+    std::swap(pf, pf_alt);
+    std::swap(pid, pid_alt);
+    since_reorder = 0;
     return CH4_OK;
   }
 
@@ -737,13 +780,20 @@ struct Engine : EngineBase {
     if (n > np || n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "asked for %d of %d particles", n, np);
     if (n == 0) return CH4_OK;
     std::vector<double> h((size_t)PF_TOTAL * np);
+    std::vector<int> ids(np);
     ch4_status st;
     if ((st = H->cuda(cudaStreamSynchronize(H->stream), "sync"))) return st;
     if ((st = H->cuda(cudaMemcpy(h.data(), pf, sizeof(double) * h.size(), cudaMemcpyDeviceToHost), "particles down")))
       return st;
+    if ((st = H->cuda(cudaMemcpy(ids.data(), pid, sizeof(int) * np, cudaMemcpyDeviceToHost), "particle ids down")))
+      return st;
     double* raw = reinterpret_cast<double*>(parts);
-    for (int i = 0; i < n; i++)
-      for (int f = 0; f < PF_FIELDS; f++) raw[(size_t)i * PF_FIELDS + f] = h[(size_t)f * np + i];
+    for (int s = 0; s < np; s++) {
+      const int i = ids[s];  // the caller's index of state slot s
+      if (i < 0 || i >= np) return H->fail(CH4_ERR_CUDA, "particle index table corrupted");
+      if (i < n)
+        for (int f = 0; f < PF_FIELDS; f++) raw[(size_t)i * PF_FIELDS + f] = h[(size_t)f * np + s];
+    }
     return CH4_OK;
   }
 
@@ -1045,10 +1095,14 @@ struct Engine : EngineBase {
             PartParams<A> Q = part_params();
             size_t bytes = cubbytes;
             if ((st = H->cuda(launch_deposit(Q, key2, order2, cubtmp, bytes, H->stream), "deposit"))) return st;
+            // the deposit's sort already holds the slots in home-cell order
+            if (np > 0 && ++since_reorder >= REORDER_EVERY && (st = reorder_particles(0))) return st;
           } else if ((st = H->cuda(cudaMemsetAsync(dbuf[dcur_i], 0, 3 * N * sizeof(A), H->stream), "deposit zero"))) {
             return st;
           }
         }
+        if (lagr() && !twoway() && np > 0 && ++since_reorder >= REORDER_EVERY && (st = reorder_particles(1)))
+          return st;
         if (fmoments()) {
           // this step's corrections, from t^n, its tables and (CONSTANT_POWER) u^n
           P.fm_prev = fmbuf + 6 * fm_i;

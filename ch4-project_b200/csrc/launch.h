@@ -49,6 +49,12 @@ cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set
 // vec[3 i + a] = planes[a n + i], a = 0..2 (planar vector field -> interleaved)
 cudaError_t launch_interleave3(const double* planes, double* vec, long long n, cudaStream_t st);
 
+// Lagrangian particles: state slot i <- slot order2[i] into P.pf_alt / P.pid_alt (with
+// sort != 0 the home-cell keys are computed and radix-sorted into key2 / order2 first)
+cudaError_t launch_particle_reorder(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp,
+                                    size_t& tmp_bytes, int sort, cudaStream_t st);
+cudaError_t launch_particle_reorder(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp,
+                                    size_t& tmp_bytes, int sort, cudaStream_t st);
 // Lagrangian particles: one sub-step (interpolate + move + wrap)
 cudaError_t launch_particle_substep(const PartParams<double>& P, cudaStream_t st);
 cudaError_t launch_particle_substep(const PartParams<float>& P, cudaStream_t st);

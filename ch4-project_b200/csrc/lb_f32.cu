@@ -38,6 +38,10 @@ cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set
                         : s2a_t<float, float>(P, set, soa, aos, z0, nz, st);
 }
 cudaError_t launch_particle_substep(const PartParams<float>& P, cudaStream_t st) { return part_substep_t<float>(P, st); }
+cudaError_t launch_particle_reorder(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp,
+                                    size_t& tmp_bytes, int sort, cudaStream_t st) {
+  return reorder_t<float>(P, key2, order2, tmp, tmp_bytes, sort, st);
+}
 cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
                            cudaStream_t st) {
   return deposit_t<float>(P, key2, order2, tmp, tmp_bytes, st);

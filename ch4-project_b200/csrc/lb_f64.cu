@@ -69,6 +69,10 @@ cudaError_t launch_diag(const AvgParams& P, int axis, int nblocks, double* parti
   return cudaGetLastError();
 }
 cudaError_t launch_particle_substep(const PartParams<double>& P, cudaStream_t st) { return part_substep_t<double>(P, st); }
+cudaError_t launch_particle_reorder(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp,
+                                    size_t& tmp_bytes, int sort, cudaStream_t st) {
+  return reorder_t<double>(P, key2, order2, tmp, tmp_bytes, sort, st);
+}
 cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
                            cudaStream_t st) {
   return deposit_t<double>(P, key2, order2, tmp, tmp_bytes, st);

@@ -14,6 +14,13 @@
 // particle-index order, which is exactly the order in which the reference's
 // particle loop adds to that cell.  Deposits on halo cells are dropped as in the
 // reference's border fold (src/lagrange_feedback.c:525-835).
+//
+// Spatial order: the state slots are kept sorted by home cell (re-sorted every few
+// steps), so that the particles of one warp read neighbouring lattice rows in the
+// interpolation and neighbouring records in the gather.  pid[slot] is the particle's
+// index in the caller's array: the sort input is laid out in that index order, so
+// each home-cell list stays in particle-index order whatever the slot order, and
+// every per-cell sum keeps the reference's order.
 #pragma once
 #include <cstddef>
 
@@ -39,13 +46,19 @@ struct PartParams {
   int addedmass;  // LAGRANGE_ADDEDMASS
   int gravity;    // LAGRANGE_GRAVITY
   double g[3];    // gravity_x, gravity_y, gravity_z
-  double* pf;     // [PF_TOTAL][np]
+  double* pf;     // [PF_TOTAL][np] by state slot
+  const int* pid; // particle index of each slot
+  double* pf_alt; // reorder target of pf / pid
+  int* pid_alt;
   const A* u;     // 3 SoA planes of u^{n+1}
   const A* t;     // t^{n+1} = m(g^{n+1}) with LB_TEMPERATURE, else null
   // deposit
-  unsigned int* key;     // home cell per particle (sorted in place by the caller)
-  int* order;            // particle index per sorted slot
-  double* rec;           // [9][np] per particle: fac*fp (3), dxm dxp dym dyp dzm dzp
+  unsigned int* key;     // sort keys, by particle index: home cell (+ nh when it deposits nothing)
+  int* order;            // sort values, by particle index: the state slot; after the sort, the
+                         // state slot of every sorted position
+  double* rec;           // [9][np] per state slot: fac*fp (3), dxm dxp dym dyp dzm dzp
+  double* srec;          // [9][np] the same by sorted position (depositing particles only)
+  int* spid;             // particle index by sorted position
   int* cell_start;       // [(NX+1)(NY+1)(NZ+1)]
   int* cell_end;
   A* dep;                // 3 SoA planes, output
@@ -55,49 +68,6 @@ struct PartParams {
 #ifdef __CUDACC__
 
 __device__ __forceinline__ double pwrapd(double x, double S) { return (x) - floor((x) / S) * S; }
-__device__ __forceinline__ int pwrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
-
-template <typename A>
-__device__ __forceinline__ double u_at(const PartParams<A>& P, int a, int i, int j, int k) {
-  const long long c = ((long long)pwrapi(k, P.NZ) * P.NY + pwrapi(j, P.NY)) * P.NX + pwrapi(i, P.NX);
-  return (double)P.u[a * P.N + c];
-}
-
-// d u_a / d x_b on a stencil cell: centred inside, one-sided 2nd order on the
-// first halo layer (LAGRANGE_INTERPOLATION_FIX, src/gradients.c:358-420)
-template <typename A>
-__device__ double grad_at(const PartParams<A>& P, int a, int b, int i, int j, int k) {
-  const int n = b == 0 ? P.NX : b == 1 ? P.NY : P.NZ;
-  const int c = b == 0 ? i : b == 1 ? j : k;
-  const int di = b == 0, dj = b == 1, dk = b == 2;
-  if (c == -1)
-    return -1.5 * u_at(P, a, i, j, k) + 2.0 * u_at(P, a, i + di, j + dj, k + dk) +
-           -0.5 * u_at(P, a, i + 2 * di, j + 2 * dj, k + 2 * dk);
-  if (c == n)
-    return 1.5 * u_at(P, a, i, j, k) + -2.0 * u_at(P, a, i - di, j - dj, k - dk) +
-           0.5 * u_at(P, a, i - 2 * di, j - 2 * dj, k - 2 * dk);
-  return (u_at(P, a, i + di, j + dj, k + dk) - u_at(P, a, i - di, j - dj, k - dk)) / 2.0;
-}
-
-template <typename A>
-__device__ __forceinline__ double t_at(const PartParams<A>& P, int i, int j, int k) {
-  const long long c = ((long long)pwrapi(k, P.NZ) * P.NY + pwrapi(j, P.NY)) * P.NX + pwrapi(i, P.NX);
-  return (double)P.t[c];
-}
-
-// d t / d x_b on a stencil cell, gradient_scalar with LAGRANGE_INTERPOLATION_FIX
-// (src/gradients.c:505-520, 731-800): the same rule as grad_at
-template <typename A>
-__device__ double tgrad_at(const PartParams<A>& P, int b, int i, int j, int k) {
-  const int n = b == 0 ? P.NX : b == 1 ? P.NY : P.NZ;
-  const int c = b == 0 ? i : b == 1 ? j : k;
-  const int di = b == 0, dj = b == 1, dk = b == 2;
-  if (c == -1)
-    return -1.5 * t_at(P, i, j, k) + 2.0 * t_at(P, i + di, j + dj, k + dk) + -0.5 * t_at(P, i + 2 * di, j + 2 * dj, k + 2 * dk);
-  if (c == n)
-    return 1.5 * t_at(P, i, j, k) + -2.0 * t_at(P, i - di, j - dj, k - dk) + 0.5 * t_at(P, i - 2 * di, j - 2 * dj, k - 2 * dk);
-  return (t_at(P, i + di, j + dj, k + dk) - t_at(P, i - di, j - dj, k - dk)) / 2.0;
-}
 
 struct Stencil {
   int im, jm, km;
@@ -151,6 +121,81 @@ __device__ __forceinline__ void corner(int c, int& di, int& dj, int& dk) {
   dk = (c == 3 || c == 5 || c == 6 || c == 7);
 }
 
+// Wrapped offsets of the 4x4x4 neighbourhood (lower stencil corner - 1 ... + 2 on
+// each axis) that the trilinear value and gradient of a particle read.
+struct PNbr {
+  long long zo[4];
+  int yo[4], xo[4];
+};
+
+__device__ __forceinline__ int pmod(int i, int n) {
+  const int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+// Trilinear value (and with GRAD the gradient) of one lattice field at a particle,
+// `lo`/`hi` flagging a stencil whose lower corner is the halo layer -1 / whose upper
+// corner is the halo layer n on each axis.  Per corner the gradient is centred,
+// (u(c+1) - u(c-1)) / 2, or one-sided of second order on those halo layers
+// (LAGRANGE_INTERPOLATION_FIX, src/gradients.c:358-420 for vectors, 731-800 for
+// scalars); the eight corners are summed in the reference's order with the weights
+// of make_stencil (src/lagrange.c:1266-1439).  The 32 lattice values used (the 8
+// corners and their 24 face neighbours) are loaded once, up front.
+template <bool GRAD, typename A>
+__device__ __forceinline__ void interp_field(const A* __restrict__ f, const PNbr& o, const double* vol, const bool* lo,
+                                             const bool* hi, double& val, double* grad) {
+  A b[4][4][4];
+#pragma unroll
+  for (int z = 0; z < 4; z++)
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++) {
+        const int inner = (x == 1 || x == 2) + (y == 1 || y == 2) + (z == 1 || z == 2);
+        if (inner == 3 || (GRAD && inner == 2)) b[z][y][x] = f[o.zo[z] + o.yo[y] + o.xo[x]];
+      }
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    int di, dj, dk;
+    corner(c, di, dj, dk);
+    const double term = (double)b[1 + dk][1 + dj][1 + di] * vol[c];
+    acc = c == 0 ? term : acc + term;
+  }
+  val = acc;
+  if constexpr (GRAD) {
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+      double g = 0.0;
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        int di, dj, dk;
+        corner(c, di, dj, dk);
+        const int x = 1 + di, y = 1 + dj, z = 1 + dk;
+        const int d = ax == 0 ? di : ax == 1 ? dj : dk;  // 0: lower corner, 1: upper corner
+        // value at offset s along ax from the corner (indices clamped so that every
+        // unrolled form is in range; the branches below use only in-range offsets)
+        auto at = [&](int s) -> double {
+          const int xx = ax == 0 ? min(max(x + s, 0), 3) : x;
+          const int yy = ax == 1 ? min(max(y + s, 0), 3) : y;
+          const int zz = ax == 2 ? min(max(z + s, 0), 3) : z;
+          return (double)b[zz][yy][xx];
+        };
+        double gc;
+        if (d == 0 && lo[ax])
+          gc = -1.5 * at(0) + 2.0 * at(1) + -0.5 * at(2);
+        else if (d == 1 && hi[ax])
+          gc = 1.5 * at(0) + -2.0 * at(-1) + 0.5 * at(-2);
+        else
+          gc = (at(1) - at(-1)) / 2.0;
+        const double term = gc * vol[c];
+        g = c == 0 ? term : g + term;
+      }
+      grad[ax] = g;
+    }
+  }
+}
+
 // One Lagrangian sub-step for one particle: interpolate, move, wrap.
 template <typename A>
 __global__ void particle_substep_kernel(const PartParams<A> P) {
@@ -159,41 +204,34 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
   double* pf = P.pf;
   const int np = P.np;
 #define F(name) pf[(long long)CH4_PF(name) * np + ip]
-  // ---- interpolate_vector_at_particles
+  // ---- interpolate_vector_at_particles, interpolate_scalar_at_particles(t, 't')
+  //      (src/lagrange.c:1211-1439, 1442-1593)
   Stencil t;
   double px, py, pz;
   wrapped_position(P, F(x), F(y), F(z), px, py, pz);
   make_stencil(px, py, pz, t);
-  double v[3];
-  for (int a = 0; a < 3; a++) {
-    double acc = 0.0;
+  PNbr o;
 #pragma unroll
-    for (int c = 0; c < 8; c++) {
-      int di, dj, dk;
-      corner(c, di, dj, dk);
-      const double term = u_at(P, a, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
-      acc = c == 0 ? term : acc + term;
-    }
-    v[a] = acc;
+  for (int q = 0; q < 4; q++) {
+    o.xo[q] = pmod(t.im - 1 + q, P.NX);
+    o.yo[q] = pmod(t.jm - 1 + q, P.NY) * P.NX;
+    o.zo[q] = (long long)pmod(t.km - 1 + q, P.NZ) * P.NX * P.NY;
+  }
+  const bool lo[3] = {t.im == -1, t.jm == -1, t.km == -1};
+  const bool hi[3] = {t.im + 1 == P.NX, t.jm + 1 == P.NY, t.km + 1 == P.NZ};
+  double v[3], gr[9];
+  if (P.gradient) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) interp_field<true>(P.u + a * P.N, o, t.vol, lo, hi, v[a], gr + 3 * a);
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; a++) interp_field<false>(P.u + a * P.N, o, t.vol, lo, hi, v[a], gr + 3 * a);
   }
   double ux = v[0], uy = v[1], uz = v[2];
   F(ux) = ux;
   F(uy) = uy;
   F(uz) = uz;
   if (P.gradient) {
-    double gr[9];
-    for (int ab = 0; ab < 9; ab++) {
-      const int a = ab / 3, b = ab % 3;
-      double acc = 0.0;
-#pragma unroll
-      for (int c = 0; c < 8; c++) {
-        int di, dj, dk;
-        corner(c, di, dj, dk);
-        const double term = grad_at(P, a, b, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
-        acc = c == 0 ? term : acc + term;
-      }
-      gr[ab] = acc;
-    }
     F(dx_ux) = gr[0];
     F(dy_ux) = gr[1];
     F(dz_ux) = gr[2];
@@ -204,33 +242,17 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     F(dy_uz) = gr[7];
     F(dz_uz) = gr[8];
   }
-  // ---- interpolate_scalar_at_particles(t, 't') (src/lagrange.c:1442-1593)
   if (P.t) {
-    double acc = 0.0;
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      int di, dj, dk;
-      corner(c, di, dj, dk);
-      const double term = t_at(P, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
-      acc = c == 0 ? term : acc + term;
-    }
-    F(t) = acc;
+    double tv, gt[3];
     if (P.gradient) {
-      double gt[3];
-      for (int b = 0; b < 3; b++) {
-        double g = 0.0;
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-          int di, dj, dk;
-          corner(c, di, dj, dk);
-          const double term = tgrad_at(P, b, t.im + di, t.jm + dj, t.km + dk) * t.vol[c];
-          g = c == 0 ? term : g + term;
-        }
-        gt[b] = g;
-      }
+      interp_field<true>(P.t, o, t.vol, lo, hi, tv, gt);
+      F(t) = tv;
       F(dx_t) = gt[0];
       F(dy_t) = gt[1];
       F(dz_t) = gt[2];
+    } else {
+      interp_field<false>(P.t, o, t.vol, lo, hi, tv, gt);
+      F(t) = tv;
     }
   }
   // ---- move_particles (src/lagrange.c:3040-3440)
@@ -370,6 +392,7 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   const bool inside = wrapped_position(P, F(x), F(y), F(z), px, py, pz);
   make_stencil(px, py, pz, t);
   const double fac = pf[(long long)PF_VOL * np + ip], dr = pf[(long long)PF_DR * np + ip];
+  const int o = P.pid[ip];
   const bool live = inside && (fac > 0.0) && F(beta_coeff) != 0.0;
   // gravity_vector of src/lagrange_feedback.c:95-103 (y points down)
   const double gx = P.gravity ? P.g[0] : 0.0, gy = P.gravity ? -P.g[1] : 0.0, gz = P.gravity ? P.g[2] : 0.0;
@@ -383,26 +406,66 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   r[6LL * np + ip] = t.dyp;
   r[7LL * np + ip] = t.dzm;
   r[8LL * np + ip] = t.dzp;
-  // particles that deposit nothing get a key past the last cell and are never merged
+  // particles that deposit nothing sort after every home cell (still in spatial
+  // order among themselves) and are never merged
   const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km + 1);
   const unsigned int nh = (unsigned)(P.NX + 1) * (unsigned)(P.NY + 1) * (unsigned)(P.NZ + 1);
-  P.key[ip] = live ? (hz * (unsigned)(P.NY + 1) + hy) * (unsigned)(P.NX + 1) + hx : nh;
-  P.order[ip] = ip;
+  P.key[o] = (live ? 0u : nh) + (hz * (unsigned)(P.NY + 1) + hy) * (unsigned)(P.NX + 1) + hx;
+  P.order[o] = ip;
 #undef F
 }
 
-// [start, end) of every home cell in the sorted key array
-static __global__ void cell_range_kernel(const unsigned int* key, int n, unsigned int nh, int* start, int* end) {
+// Home-cell key of every particle for a reorder without a deposit (one-way coupling).
+template <typename A>
+__global__ void particle_key_kernel(const PartParams<A> P) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= P.np) return;
+  const double* pf = P.pf;
+  const long long np = P.np;
+  double px, py, pz;
+  wrapped_position(P, pf[CH4_PF(x) * np + ip], pf[CH4_PF(y) * np + ip], pf[CH4_PF(z) * np + ip], px, py, pz);
+  Stencil t;
+  make_stencil(px, py, pz, t);
+  const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km + 1);
+  const int o = P.pid[ip];
+  P.key[o] = (hz * (unsigned)(P.NY + 1) + hy) * (unsigned)(P.NX + 1) + hx;
+  P.order[o] = ip;
+}
+
+// slot i of (pf_alt, pid_alt) <- slot src[i] of (pf, pid)
+template <typename A>
+__global__ void particle_permute_kernel(const PartParams<A> P, const int* __restrict__ src) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.np) return;
+  const long long np = P.np;
+  const int s = src[i];
+  P.pid_alt[i] = P.pid[s];
+#pragma unroll 5
+  for (int f = 0; f < PF_TOTAL; f++) P.pf_alt[f * np + i] = P.pf[f * np + s];
+}
+
+// [start, end) of every home cell in the sorted key array, and the records and
+// particle indices copied into sorted order (the gather then reads each home list
+// as one contiguous run)
+template <typename A>
+__global__ void cell_range_kernel(const PartParams<A> P, const unsigned int* key, const int* slot_of, unsigned int nh) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = P.np;
   if (i >= n) return;
   const unsigned int k = key[i];
   if (k >= nh) return;
-  if (i == 0 || key[i - 1] != k) start[k] = i;
-  if (i == n - 1 || key[i + 1] != k) end[k] = i + 1;
+  if (i == 0 || key[i - 1] != k) P.cell_start[k] = i;
+  if (i == n - 1 || key[i + 1] != k) P.cell_end[k] = i + 1;
+  const int s = slot_of[i];
+  P.spid[i] = P.pid[s];
+#pragma unroll
+  for (int f = 0; f < 9; f++) P.srec[(long long)f * n + i] = P.rec[(long long)f * n + s];
 }
 
 // Gather of the deposit on one interior cell: merge the particles of the 8 home
 // cells in particle-index order and accumulate fac*fp*vol as the reference does.
+// The list heads stay in registers (every index into pos/endp/head is a constant
+// after unrolling): one dependent load per merged particle.
 template <typename A>
 __global__ void deposit_gather_kernel(const PartParams<A> P) {
   const long long cidx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -412,7 +475,7 @@ __global__ void deposit_gather_kernel(const PartParams<A> P) {
   const int k = (int)(cidx / ((long long)P.NX * P.NY));
   const int HX = P.NX + 1, HY = P.NY + 1;
   int pos[8], endp[8];
-  int any = 0;
+  bool any = false;
 #pragma unroll
   for (int h = 0; h < 8; h++) {
     const int di = h & 1, dj = (h >> 1) & 1, dk = (h >> 2) & 1;
@@ -422,38 +485,45 @@ __global__ void deposit_gather_kernel(const PartParams<A> P) {
     endp[h] = P.cell_end[home];
     any |= endp[h] > pos[h];
   }
-  double acc[3] = {0.0, 0.0, 0.0};
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
   if (any) {
-    const int np = P.np;
+    const long long np = P.np;
+    const int* __restrict__ spid = P.spid;
+    const double* __restrict__ r = P.srec;
+    constexpr int NONE = 0x7fffffff;
+    int head[8];
+#pragma unroll
+    for (int h = 0; h < 8; h++) head[h] = pos[h] < endp[h] ? spid[pos[h]] : NONE;
     for (;;) {
-      int best = -1, bidx = 0x7fffffff;
+      int best = 0, bv = head[0];
+#pragma unroll
+      for (int h = 1; h < 8; h++)
+        if (head[h] < bv) {
+          bv = head[h];
+          best = h;
+        }
+      if (bv == NONE) break;
+      int slot = 0;
 #pragma unroll
       for (int h = 0; h < 8; h++)
-        if (pos[h] < endp[h]) {
-          const int pidx = P.order[pos[h]];
-          if (pidx < bidx) {
-            bidx = pidx;
-            best = h;
-          }
+        if (h == best) {
+          slot = pos[h]++;
+          head[h] = pos[h] < endp[h] ? spid[pos[h]] : NONE;
         }
-      if (best < 0) break;
-      const int slot = pos[best]++;
       const int di = best & 1, dj = (best >> 1) & 1, dk = (best >> 2) & 1;
       // this cell is the particle's ip corner when di == 0 (weight dxm), im corner when di == 1 (dxp)
-      const double* r = P.rec;
-      const int s0 = P.order[slot];
-      const double wx = di ? r[4LL * np + s0] : r[3LL * np + s0];
-      const double wy = dj ? r[6LL * np + s0] : r[5LL * np + s0];
-      const double wz = dk ? r[8LL * np + s0] : r[7LL * np + s0];
+      const double wx = r[(3 + di) * np + slot];
+      const double wy = r[(5 + dj) * np + slot];
+      const double wz = r[(7 + dk) * np + slot];
       const double vol = wx * wy * wz;
-      acc[0] += r[0LL * np + s0] * vol;
-      acc[1] += r[1LL * np + s0] * vol;
-      acc[2] += r[2LL * np + s0] * vol;
+      acc0 += r[slot] * vol;
+      acc1 += r[np + slot] * vol;
+      acc2 += r[2 * np + slot] * vol;
     }
   }
-  P.dep[cidx] = (A)acc[0];
-  P.dep[P.N + cidx] = (A)acc[1];
-  P.dep[2 * P.N + cidx] = (A)acc[2];
+  P.dep[cidx] = (A)acc0;
+  P.dep[P.N + cidx] = (A)acc1;
+  P.dep[2 * P.N + cidx] = (A)acc2;
 }
 
 #endif  // __CUDACC__

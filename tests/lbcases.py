@@ -49,6 +49,9 @@ CASES = {
                                T_ref=0.5, beta_t=0.3, gravity_y=2e-3, gravity_x=1e-3)),
     "cpower": dict(flagset="cpower", NX=8, NY=7, NZ=6,
                    params=dict(tau_u=0.57, Amp_x=1e-9, Amp_y=8e-10, Amp_z=5e-10, seed=3)),
+    "particles_1w": dict(flagset="particles_1w", NX=10, NY=8, NZ=7, npart=300,
+                         params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=8,
+                                     time_dt_lagr_factor=2.0, particle_number=300)),
     "particles_g": dict(flagset="particles_g", NX=10, NY=8, NZ=7, npart=300,
                         params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=7, gravity_x=2e-5,
                                     gravity_y=1e-4, gravity_z=-3e-5, time_dt_lagr_factor=2.0, particle_number=300)),
