@@ -398,6 +398,7 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   const double invtau = 1.0 / c.tau_u;
   const double fac = (1.0 - 0.5 * c.time_dt * invtau);  // src/forcing.c:1289
   for (int q = 0; q < NPOP; q++) P.facw[q] = (A)(fac * lat.w[q]);
+  P.gfac = (A)fac;
   P.invcs2 = (A)lat.invcs2;
   P.invcs4 = (A)lat.invcs4;
   P.invtwocs2 = (A)lat.invtwocs2;
@@ -1013,11 +1014,40 @@ struct Engine : EngineBase {
     return CH4_OK;
   }
 
-  // host phase tables -> device slot
+  // host phase tables -> device slot.  FP64: the per-mode sin tables, summed on the
+  // device in the reference's order.  FP32: the mode sums folded per force component
+  // and coordinate in FP64 (two blocks of L: [Syx | Sxy | Sxz] and [Szx | Szy | Syz],
+  // S_ab(c) = sum over modes of amp_a * table_b(c)), so that a cell's force needs
+  // six loads instead of eighteen loads and thirty-six operations.
   void tables_to(A* dst_h) {
     std::vector<double> t((size_t)NK * L());
     H->hit_tables(t.data());
-    for (size_t i = 0; i < t.size(); i++) dst_h[i] = (A)t[i];
+    if (sizeof(A) == 8) {
+      for (size_t i = 0; i < t.size(); i++) dst_h[i] = (A)t[i];
+      return;
+    }
+    const int NX = c.NX, NY = c.NY, NZ = c.NZ, Ln = L();
+    const double amp[3] = {c.Amp_x, c.Amp_y, c.Amp_z};
+    auto fold = [&](int comp, int axis, int i) {  // sum over modes of amp_comp * table_axis(i)
+      const int off = axis == 0 ? 0 : axis == 1 ? NX : NX + NY;
+      double s = 0.0;
+      for (int ii = 0; ii < NK; ii++) s += (H->hit_fac[ii] * amp[comp]) * t[(size_t)ii * Ln + off + i];
+      return s;
+    };
+    A* b0 = dst_h;
+    A* b1 = dst_h + Ln;
+    for (int i = 0; i < NX; i++) {
+      b0[i] = (A)fold(1, 0, i);
+      b1[i] = (A)fold(2, 0, i);
+    }
+    for (int j = 0; j < NY; j++) {
+      b0[NX + j] = (A)fold(0, 1, j);
+      b1[NX + j] = (A)fold(2, 1, j);
+    }
+    for (int k = 0; k < NZ; k++) {
+      b0[NX + NY + k] = (A)fold(0, 2, k);
+      b1[NX + NY + k] = (A)fold(1, 2, k);
+    }
   }
 
   ch4_status initialize() override {

@@ -86,6 +86,7 @@ struct StepParams {
   // constants (host-computed in FP64, then cast)
   A w[Q];
   A facw[Q];  // (1 - dt/(2 tau_u)) * w_q, the Guo prefactor of src/forcing.c:1289,1432
+  A gfac;     // 1 - dt/(2 tau_u)
   A invcs2, invcs4, invtwocs2, invtwocs4;
   A invtau[3];
   A hdt;  // 0.5*time_dt

@@ -96,6 +96,13 @@ __device__ __forceinline__ void cell_force(const StepParams<A>& P, int x, int y,
   }
   if (F & K_HIT) {
     const int L = P.NX + P.NY + P.NZ;
+    if constexpr (sizeof(A) == 4) {
+      // FP32 form: the mode sums folded per axis on the host (Engine::tables_to),
+      // F_x = Sxy[y] + Sxz[z], F_y = Syx[x] + Syz[z], F_z = Szy[y] + Szx[x]
+      fx += hit[P.NX + y] + hit[P.NX + P.NY + z];
+      fy += hit[x] + hit[L + P.NX + P.NY + z];
+      fz += hit[L + P.NX + y] + hit[L + x];
+    } else
 #pragma unroll
     for (int ii = 0; ii < NK; ii++) {
       const A ax = hit[ii * L + x], ay = hit[ii * L + P.NX + y], az = hit[ii * L + P.NX + P.NY + z];
@@ -204,11 +211,11 @@ __global__ void init_prev_kernel(const StepParams<A> P) {
 template <typename S, typename A, bool THERM, bool SCAL>
 __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, const A* fm, double* dens, double* u,
                              double* t, double* s, double* force, A* u_arith, A* t_arith) {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (idx >= P.N) return;
-  const int x = (int)(idx % P.NX);
-  const int y = (int)((idx / P.NX) % P.NY);
-  const int z = (int)(idx / ((long long)P.NX * P.NY));
+  // grid (x blocks, NY, NZ): no index division
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= P.NX) return;
+  const int y = blockIdx.y, z = blockIdx.z;
+  const long long idx = ((long long)z * P.NY + y) * P.NX + x;
   A f[Q];
   load_set<S, A, 0>(P, idx, f);
   const A rho = mom0(f);

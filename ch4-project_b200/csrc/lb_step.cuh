@@ -114,6 +114,8 @@ struct CellState {
   A Fx, Fy, Fz;
   A invtau, it, is;
   A base, uF;  // FP32 form: 1 - u2/(2 cs^2), u.F
+  // FP32 forced fluid update, f' = (1 - om) f + rho w_q (a0 + c.a + (c.u)(c.b)/cs^4)
+  A a0, ax, ay, az, bx, by, bz, omf, rw[3];
 };
 
 // Collision of direction q for all enabled sets, in place.
@@ -150,14 +152,21 @@ __device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellSt
     }
   } else {
     const A poly = c.base + cu * (P.invcs2 + P.invtwocs4 * cu);
-    const A feq = (c.rho * P.w[q]) * poly;
-    A r = f[q] + c.invtau * (feq - f[q]);
     if (forcing) {
-      const A cF = cdot<q>(c.Fx, c.Fy, c.Fz);
-      const A gt = (cF - c.uF) * P.invcs2 + (cu * cF) * P.invcs4;
-      r += (P.facw[q] * c.rho) * gt;
+      // BGK + Guo in one polynomial: om feq + (1 - dt/2tau) w rho ((c - u).F/cs^2 + (c.u)(c.F)/cs^4)
+      // = rho w (a0 + c.a + (c.u)(c.b)/cs^4), a0 = om (1 - u^2/2cs^2) - k u.F/cs^2,
+      // a = (om u + k F)/cs^2, b = om u/2 + k F (k = 1 - dt/2tau)
+      constexpr int wc = q == 0 ? 0 : (q <= 6 ? 1 : 2);
+      const A ca = cdot<q>(c.ax, c.ay, c.az);
+      const A cb = cdot<q>(c.bx, c.by, c.bz);
+      // explicit fma / round-to-nearest products: every kernel that inlines this
+      // (single lattice and ensemble) rounds the same way
+      const A s = fmaf(__fmul_rn(cu, cb), P.invcs4, c.a0 + ca);
+      f[q] = fmaf(c.rw[wc], s, __fmul_rn(c.omf, f[q]));
+    } else {
+      const A feq = (c.rho * P.w[q]) * poly;
+      f[q] = f[q] + c.invtau * (feq - f[q]);
     }
-    f[q] = r;
     if constexpr (THERM) g[q] += c.it * ((c.tt * P.w[q]) * poly - g[q]);
     if constexpr (SCAL) h[q] += c.is * ((c.ss * P.w[q]) * poly - h[q]);
   }
@@ -215,6 +224,23 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
   c.is = P.invtau[2];
   c.base = A(1) - P.invtwocs2 * c.u2;
   c.uF = c.ux * c.Fx + c.uy * c.Fy + c.uz * c.Fz;
+  if constexpr (!EXACT) {
+    if (forcing) {
+      const A om = c.invtau, k = P.gfac, hom = __fmul_rn(A(0.5), om);
+      const A kFx = __fmul_rn(k, c.Fx), kFy = __fmul_rn(k, c.Fy), kFz = __fmul_rn(k, c.Fz);
+      c.a0 = fmaf(-__fmul_rn(k, c.uF), P.invcs2, __fmul_rn(om, c.base));
+      c.ax = __fmul_rn(fmaf(om, c.ux, kFx), P.invcs2);
+      c.ay = __fmul_rn(fmaf(om, c.uy, kFy), P.invcs2);
+      c.az = __fmul_rn(fmaf(om, c.uz, kFz), P.invcs2);
+      c.bx = fmaf(hom, c.ux, kFx);
+      c.by = fmaf(hom, c.uy, kFy);
+      c.bz = fmaf(hom, c.uz, kFz);
+      c.omf = A(1) - om;
+      c.rw[0] = __fmul_rn(c.rho, P.w[0]);
+      c.rw[1] = __fmul_rn(c.rho, P.w[1]);
+      c.rw[2] = __fmul_rn(c.rho, P.w[7]);
+    }
+  }
 
 #define CH4_COL(Q_) collide_one<Q_, EXACT, THERM, SCAL>(P, c, forcing, f, g, h);
   CH4_COL(0) CH4_COL(1) CH4_COL(2) CH4_COL(3) CH4_COL(4) CH4_COL(5) CH4_COL(6) CH4_COL(7) CH4_COL(8) CH4_COL(9)

@@ -196,19 +196,29 @@ __device__ __forceinline__ void interp_field(const A* __restrict__ f, const PNbr
   }
 }
 
-// One Lagrangian sub-step for one particle: interpolate, move, wrap.
+// One Lagrangian sub-step for one particle: interpolate, move, wrap.  The state the
+// step reads is loaded once, up front (independent loads), and every result is
+// stored once at the end; the arithmetic is the reference's, expression for
+// expression.
 template <typename A>
 __global__ void particle_substep_kernel(const PartParams<A> P) {
   const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= P.np) return;
   double* pf = P.pf;
-  const int np = P.np;
-#define F(name) pf[(long long)CH4_PF(name) * np + ip]
+  const long long np = P.np;
+#define F(name) pf[CH4_PF(name) * np + ip]
+  const double x0 = F(x), y0 = F(y), z0 = F(z);
+  const double vx0 = F(vx), vy0 = F(vy), vz0 = F(vz);
+  const double vxo0 = F(vx_old), vyo0 = F(vy_old), vzo0 = F(vz_old);
+  const double uxo0 = F(ux_old), uyo0 = F(uy_old), uzo0 = F(uz_old);
+  const double axo0 = F(ax_old), ayo0 = F(ay_old), azo0 = F(az_old);
+  const double tau = F(tau_drag), beta = F(beta_coeff);
+  const double told0 = P.t ? F(t_old) : 0.0;
   // ---- interpolate_vector_at_particles, interpolate_scalar_at_particles(t, 't')
   //      (src/lagrange.c:1211-1439, 1442-1593)
   Stencil t;
   double px, py, pz;
-  wrapped_position(P, F(x), F(y), F(z), px, py, pz);
+  wrapped_position(P, x0, y0, z0, px, py, pz);
   make_stencil(px, py, pz, t);
   PNbr o;
 #pragma unroll
@@ -226,8 +236,18 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
   } else {
 #pragma unroll
     for (int a = 0; a < 3; a++) interp_field<false>(P.u + a * P.N, o, t.vol, lo, hi, v[a], gr + 3 * a);
+    // without LAGRANGE_GRADIENT the added-mass term reads the stored gradients
+    gr[0] = F(dx_ux);
+    gr[1] = F(dy_ux);
+    gr[2] = F(dz_ux);
+    gr[3] = F(dx_uy);
+    gr[4] = F(dy_uy);
+    gr[5] = F(dz_uy);
+    gr[6] = F(dx_uz);
+    gr[7] = F(dy_uz);
+    gr[8] = F(dz_uz);
   }
-  double ux = v[0], uy = v[1], uz = v[2];
+  const double ux = v[0], uy = v[1], uz = v[2];
   F(ux) = ux;
   F(uy) = uy;
   F(uz) = uz;
@@ -242,42 +262,39 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     F(dy_uz) = gr[7];
     F(dz_uz) = gr[8];
   }
+  // ---- move_particles (src/lagrange.c:3040-3440)
+  const double dtl = P.dtl;
+  const bool first = P.first != 0;
   if (P.t) {
     double tv, gt[3];
     if (P.gradient) {
       interp_field<true>(P.t, o, t.vol, lo, hi, tv, gt);
-      F(t) = tv;
       F(dx_t) = gt[0];
       F(dy_t) = gt[1];
       F(dz_t) = gt[2];
     } else {
       interp_field<false>(P.t, o, t.vol, lo, hi, tv, gt);
-      F(t) = tv;
     }
-  }
-  // ---- move_particles (src/lagrange.c:3040-3440)
-  const double dtl = P.dtl;
-  const bool first = P.first != 0;
-  if (P.t) {  // time derivatives of t along the path, src/lagrange.c:2997-3010
+    F(t) = tv;
+    // time derivatives of t along the path, src/lagrange.c:2997-3010
     if (first) {
-      F(t_old) = F(t);
+      F(t_old) = tv;
     } else {
-      const double tnow = F(t);
-      F(dt_t) = (tnow - F(t_old)) / dtl;
-      F(t_old) = tnow;
-      if (P.gradient)
-        F(Dt_t) = F(dt_t) + (ux - F(vx)) * F(dx_t) + (uy - F(vy)) * F(dy_t) + (uz - F(vz)) * F(dz_t);
+      const double dt_t = (tv - told0) / dtl;
+      F(dt_t) = dt_t;
+      F(t_old) = tv;
+      if (P.gradient) F(Dt_t) = dt_t + (ux - vx0) * gt[0] + (uy - vy0) * gt[1] + (uz - vz0) * gt[2];
     }
   }
-  const double tau = F(tau_drag);
+  double xn = x0, yn = y0, zn = z0;
   if (tau < 0.0) {  // Eulerian probe
     F(vx) = ux;
     F(vy) = uy;
     F(vz) = uz;
   }
   if (tau == 0.0) {  // tracer
-    double vx = ux, vy = uy, vz = uz;
-    double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
+    const double vx = ux, vy = uy, vz = uz;
+    double vxo = vxo0, vyo = vyo0, vzo = vzo0;
     if (first) {
       vxo = vx;
       vyo = vy;
@@ -287,13 +304,13 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     F(ay) = (vy - vyo) / dtl;
     F(az) = (vz - vzo) / dtl;
     if (first) {
-      F(x) += dtl * vx;
-      F(y) += dtl * vy;
-      F(z) += dtl * vz;
+      xn = x0 + dtl * vx;
+      yn = y0 + dtl * vy;
+      zn = z0 + dtl * vz;
     } else {
-      F(x) += dtl * 0.5 * (3.0 * vx - vxo);
-      F(y) += dtl * 0.5 * (3.0 * vy - vyo);
-      F(z) += dtl * 0.5 * (3.0 * vz - vzo);
+      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo);
+      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo);
+      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo);
     }
     F(vx) = vx;
     F(vy) = vy;
@@ -307,15 +324,14 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
   }
   if (tau > 0.0) {  // Stokes drag (+ added mass)
     const double invtau = 1.0 / tau;
-    double vx = F(vx), vy = F(vy), vz = F(vz);
+    double vx = vx0, vy = vy0, vz = vz0;
     double ax = (ux - vx) * invtau, ay = (uy - vy) * invtau, az = (uz - vz) * invtau;
     if (P.gravity) {  // -g, src/lagrange.c:3312-3323
       ax -= P.g[0];
       ay -= P.g[1];
       az -= P.g[2];
     }
-    const double beta = F(beta_coeff);
-    double uxo = F(ux_old), uyo = F(uy_old), uzo = F(uz_old);
+    double uxo = uxo0, uyo = uyo0, uzo = uzo0;
     if (P.addedmass && beta != 0.0) {
       if (P.gravity) {  // -(-beta) g, src/lagrange.c:3330-3339
         ax -= (-beta) * P.g[0];
@@ -327,9 +343,9 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
         uyo = uy;
         uzo = uz;
       }
-      const double Dx = (ux - uxo) / dtl + (ux - vx) * F(dx_ux) + (uy - vy) * F(dy_ux) + (uz - vz) * F(dz_ux);
-      const double Dy = (uy - uyo) / dtl + (ux - vx) * F(dx_uy) + (uy - vy) * F(dy_uy) + (uz - vz) * F(dz_uy);
-      const double Dz = (uz - uzo) / dtl + (ux - vx) * F(dx_uz) + (uy - vy) * F(dy_uz) + (uz - vz) * F(dz_uz);
+      const double Dx = (ux - uxo) / dtl + (ux - vx) * gr[0] + (uy - vy) * gr[1] + (uz - vz) * gr[2];
+      const double Dy = (uy - uyo) / dtl + (ux - vx) * gr[3] + (uy - vy) * gr[4] + (uz - vz) * gr[5];
+      const double Dz = (uz - uzo) / dtl + (ux - vx) * gr[6] + (uy - vy) * gr[7] + (uz - vz) * gr[8];
       ax += Dx * beta;
       ay += Dy * beta;
       az += Dz * beta;
@@ -337,15 +353,14 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
       F(Dt_uy) = Dy;
       F(Dt_uz) = Dz;
     }
-    const double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
     if (first) {
-      F(x) += dtl * vx;
-      F(y) += dtl * vy;
-      F(z) += dtl * vz;
+      xn = x0 + dtl * vx;
+      yn = y0 + dtl * vy;
+      zn = z0 + dtl * vz;
     } else {
-      F(x) += dtl * 0.5 * (3.0 * vx - vxo);
-      F(y) += dtl * 0.5 * (3.0 * vy - vyo);
-      F(z) += dtl * 0.5 * (3.0 * vz - vzo);
+      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo0);
+      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo0);
+      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo0);
     }
     F(vx_old) = vx;
     F(vy_old) = vy;
@@ -358,9 +373,9 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
       vy += dtl * ay;
       vz += dtl * az;
     } else {
-      vx += dtl * 0.5 * (3.0 * ax - F(ax_old));
-      vy += dtl * 0.5 * (3.0 * ay - F(ay_old));
-      vz += dtl * 0.5 * (3.0 * az - F(az_old));
+      vx += dtl * 0.5 * (3.0 * ax - axo0);
+      vy += dtl * 0.5 * (3.0 * ay - ayo0);
+      vz += dtl * 0.5 * (3.0 * az - azo0);
     }
     F(vx) = vx;
     F(vy) = vy;
@@ -373,9 +388,9 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     F(az_old) = az;
   }
   // ---- LAGRANGE_WRAP of sendrecv_particles
-  F(x) = pwrapd(F(x), P.SX);
-  F(z) = pwrapd(F(z), P.SZ);
-  F(y) = pwrapd(F(y), P.SY);
+  F(x) = pwrapd(xn, P.SX);
+  F(z) = pwrapd(zn, P.SZ);
+  F(y) = pwrapd(yn, P.SY);
 #undef F
 }
 
@@ -468,11 +483,11 @@ __global__ void cell_range_kernel(const PartParams<A> P, const unsigned int* key
 // after unrolling): one dependent load per merged particle.
 template <typename A>
 __global__ void deposit_gather_kernel(const PartParams<A> P) {
-  const long long cidx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (cidx >= P.N) return;
-  const int i = (int)(cidx % P.NX);
-  const int j = (int)((cidx / P.NX) % P.NY);
-  const int k = (int)(cidx / ((long long)P.NX * P.NY));
+  // grid (x blocks, NY, NZ): no index division
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.NX) return;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
   const int HX = P.NX + 1, HY = P.NY + 1;
   int pos[8], endp[8];
   bool any = false;

@@ -89,7 +89,7 @@ def test_fp64_matches_compiled_reference(name):
 # of rho within 1e-5, of T within 1e-6 (40 steps).
 # FP16 deviations (11-bit mantissa): u within 0.2, rho within 1e-3, T within 2e-2.
 @pytest.mark.parametrize("storage,tol_u,tol_rho,tol_t", [(1, 1e-3, 1e-5, 1e-6), (2, 0.2, 1e-3, 2e-2)])
-@pytest.mark.parametrize("name", ["kolmogorov", "rb", "scalar"])
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "scalar", "hit"])
 def test_reduced_precision_error_bounds(name, storage, tol_u, tol_rho, tol_t):
     _, cfg64, state = make_case(name, seed=2)
     _, cfg, _ = make_case(name, seed=2, storage=storage)
