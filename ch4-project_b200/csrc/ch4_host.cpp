@@ -873,18 +873,16 @@ struct Engine : EngineBase {
     for (cudaEvent_t& e : up_ev)
       if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "event");
     fill_params();
-    // rest state p = w (src/initial_conditions.c:45), g = h = 0
-    std::vector<double> rest((size_t)c.NX * c.NY * NPOP * chunk_planes);
-    for (size_t i = 0; i < rest.size(); i++) rest[i] = H->lat.w[i % NPOP];
-    ch4_status st = upload_chunks(0, rest.data(), 0, true);
+    // rest state p = w (src/initial_conditions.c:45), g = h = 0: one z-slab chunk of it is
+    // built in the pinned staging buffer, copied once, and converted into every chunk
+    const size_t rest_n = (size_t)c.NX * c.NY * NPOP * chunk_planes;
+    for (size_t i = 0; i < rest_n; i++) staging_h[i] = H->lat.w[i % NPOP];
+    ch4_status st = fill_repeated(0);
     if (st) return st;
-    if (nsets_on[1]) {
-      std::fill(rest.begin(), rest.end(), 0.0);
-      if ((st = upload_chunks(1, rest.data(), 0, true))) return st;
-    }
-    if (nsets_on[2]) {
-      std::fill(rest.begin(), rest.end(), 0.0);
-      if ((st = upload_chunks(2, rest.data(), 0, true))) return st;
+    if (nsets_on[1] || nsets_on[2]) {
+      std::fill(staging_h, staging_h + rest_n, 0.0);
+      if (nsets_on[1] && (st = fill_repeated(1))) return st;
+      if (nsets_on[2] && (st = fill_repeated(2))) return st;
     }
     // Kolmogorov tables (src/forcing.c:390-400), host libm
     {
@@ -929,7 +927,19 @@ struct Engine : EngineBase {
   // Reference-layout AoS (with `brd` halo) -> device SoA, in z-slab chunks through
   // pinned staging.  With two staging pairs the host copies chunk k+1 (rows split over
   // host threads) while chunk k is transferred and converted.
-  ch4_status upload_chunks(int set, const double* aos, int brd, bool repeat) {
+  // every z-slab chunk of a set <- the AoS chunk held in staging_h
+  ch4_status fill_repeated(int set) {
+    const size_t bytes = (size_t)c.NX * c.NY * NPOP * chunk_planes * sizeof(double);
+    bind_pops(cur);
+    ch4_status st = H->cuda(cudaMemcpyAsync(staging_d, staging_h, bytes, cudaMemcpyHostToDevice, H->stream), "fill");
+    for (int z0 = 0; z0 < c.NZ && !st; z0 += (int)chunk_planes) {
+      const int nz = std::min<int>((int)chunk_planes, c.NZ - z0);
+      st = H->cuda(launch_aos_to_soa(P, shape, set, staging_d, f[set][cur], z0, nz, H->stream), "aos_to_soa");
+    }
+    return st ? st : H->cuda(cudaStreamSynchronize(H->stream), "fill sync");
+  }
+
+  ch4_status upload_chunks(int set, const double* aos, int brd) {
     const size_t row = (size_t)c.NX * NPOP;
     const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
     bind_pops(cur);
@@ -939,30 +949,23 @@ struct Engine : EngineBase {
     ch4_status st;
     for (int z0 = 0; z0 < c.NZ; z0 += (int)chunk_planes) {
       int nz = std::min<int>((int)chunk_planes, c.NZ - z0);
-      const double* src;
-      if (repeat) {
-        src = aos;
-      } else {
-        // the copy out of hb[b] two chunks ago must be finished before it is refilled
-        if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "upload wait"))) return st;
-        double* dst = hb[b];
-        host_parallel((size_t)nz * c.NY, 64, [&](size_t r0, size_t r1) {
-          for (size_t r = r0; r < r1; r++) {
-            const size_t zl = r / c.NY, y = r % c.NY;
-            std::memcpy(dst + r * row, aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
-                        row * sizeof(double));
-          }
-        });
-        src = dst;
-      }
-      if ((st = H->cuda(cudaMemcpyAsync(db[b], src, (size_t)nz * c.NY * row * sizeof(double), cudaMemcpyHostToDevice,
+      // the copy out of hb[b] two chunks ago must be finished before it is refilled
+      if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "upload wait"))) return st;
+      double* dst = hb[b];
+      host_parallel((size_t)nz * c.NY, 64, [&](size_t r0, size_t r1) {
+        for (size_t r = r0; r < r1; r++) {
+          const size_t zl = r / c.NY, y = r % c.NY;
+          std::memcpy(dst + r * row, aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
+                      row * sizeof(double));
+        }
+      });
+      if ((st = H->cuda(cudaMemcpyAsync(db[b], dst, (size_t)nz * c.NY * row * sizeof(double), cudaMemcpyHostToDevice,
                                         H->stream),
                         "upload")))
         return st;
       if ((st = H->cuda(launch_aos_to_soa(P, shape, set, db[b], f[set][cur], z0, nz, H->stream), "aos_to_soa")))
         return st;
       if ((st = H->cuda(cudaEventRecord(up_ev[b], H->stream), "upload event"))) return st;
-      if (repeat && (st = H->cuda(cudaStreamSynchronize(H->stream), "upload sync"))) return st;
       if (staging_h2) b ^= 1;
     }
     return H->cuda(cudaStreamSynchronize(H->stream), "upload sync");
@@ -971,7 +974,7 @@ struct Engine : EngineBase {
   ch4_status set_pop(int set, const double* aos, int brd) override {
     if (!nsets_on[set]) return H->fail(CH4_ERR_ARG, "population set %d is not enabled", set);
     H->initialized = false;
-    return upload_chunks(set, aos, brd, false);
+    return upload_chunks(set, aos, brd);
   }
 
   ch4_status get_pop(int set, double* aos, int brd) override {
