@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -41,6 +42,51 @@ void host_parallel(size_t n, size_t grain, F&& body) {
   body(0, n / nt);
   for (auto& th : pool) th.join();
 }
+
+// Process-wide cache of pinned host buffers.  Page-locking a 64 MB staging buffer
+// takes tens of milliseconds; buffers a closed handle released serve the next handle
+// of the same shape (up to 512 MB cached; the rest is freed at once).
+struct PinnedPool {
+  static void* get(size_t bytes) {
+    {
+      std::lock_guard<std::mutex> g(mu());
+      auto& L = list();
+      for (size_t i = 0; i < L.size(); i++)
+        if (L[i].first == bytes) {
+          void* p = L[i].second;
+          L.erase(L.begin() + (long)i);
+          cached() -= bytes;
+          return p;
+        }
+    }
+    void* p = nullptr;
+    return cudaMallocHost(&p, bytes) == cudaSuccess ? p : nullptr;
+  }
+  static void put(void* p, size_t bytes) {
+    if (!p) return;
+    std::lock_guard<std::mutex> g(mu());
+    if (cached() + bytes > (512ull << 20)) {
+      cudaFreeHost(p);
+      return;
+    }
+    list().push_back({bytes, p});
+    cached() += bytes;
+  }
+
+ private:
+  static std::mutex& mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::vector<std::pair<size_t, void*>>& list() {
+    static std::vector<std::pair<size_t, void*>> l;
+    return l;
+  }
+  static size_t& cached() {
+    static size_t c = 0;
+    return c;
+  }
+};
 
 const double VK[NK][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}};
 
@@ -466,6 +512,7 @@ struct Engine : EngineBase {
   // second pair: the host fills one pinned chunk while the other is copied and converted
   double* staging_d2 = nullptr;
   double* staging_h2 = nullptr;
+  size_t staging_bytes = 0, hit_h_bytes = 0;
   cudaEvent_t up_ev[2] = {nullptr, nullptr};
   A* hit_h = nullptr;           // pinned host phase tables
   cudaEvent_t hit_ev = nullptr;
@@ -492,7 +539,9 @@ struct Engine : EngineBase {
   double* rec = nullptr;
   double* srec = nullptr;
   int* spid = nullptr;
-  int *cstart = nullptr, *cend = nullptr;
+  int2* crng = nullptr;   // {start, end} per home cell
+  int* busy = nullptr;    // cells for the deposit merge pass, and their count
+  int* busy_n = nullptr;
   int* pstatus = nullptr;  // particle position check of the kernels (sticky until set_particles)
   // global force corrections (NOZEROMODE / CONSTANT_POWER): two slots of 6, the
   // last step's (fm_i) and the one being built; reduction scratch
@@ -528,20 +577,21 @@ struct Engine : EngineBase {
     cudaFree(hit_ring);
     cudaFree(hit_last);
     cudaFree(staging_d);
-    if (staging_h) cudaFreeHost(staging_h);
+    PinnedPool::put(staging_h, staging_bytes);
     cudaFree(staging_d2);
-    if (staging_h2) cudaFreeHost(staging_h2);
+    PinnedPool::put(staging_h2, staging_bytes);
     for (cudaEvent_t e : up_ev)
       if (e) cudaEventDestroy(e);
-    if (hit_h) cudaFreeHost(hit_h);
+    PinnedPool::put(hit_h, hit_h_bytes);
     if (hit_ev) cudaEventDestroy(hit_ev);
     free_particles();
     cudaFree(upart);
     cudaFree(tpart);
     cudaFree(dbuf[0]);
     cudaFree(dbuf[1]);
-    cudaFree(cstart);
-    cudaFree(cend);
+    cudaFree(crng);
+    cudaFree(busy);
+    cudaFree(busy_n);
     cudaFree(pstatus);
     cudaFree(fmbuf);
     cudaFree(fmpart);
@@ -603,8 +653,9 @@ struct Engine : EngineBase {
     Q.rec = rec;
     Q.srec = srec;
     Q.spid = spid;
-    Q.cell_start = cstart;
-    Q.cell_end = cend;
+    Q.cell_rng = crng;
+    Q.busy = busy;
+    Q.busy_n = busy_n;
     Q.dep = dbuf[dcur_i];
     Q.status = pstatus;
     return Q;
@@ -835,8 +886,8 @@ struct Engine : EngineBase {
         if (cudaMalloc(&dbuf[b], 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "deposit");
         if (cudaMemset(dbuf[b], 0, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "deposit memset");
       }
-      if (cudaMalloc(&cstart, sizeof(int) * nhome()) != cudaSuccess ||
-          cudaMalloc(&cend, sizeof(int) * nhome()) != cudaSuccess)
+      if (cudaMalloc(&crng, sizeof(int2) * nhome()) != cudaSuccess || cudaMalloc(&busy, sizeof(int) * N) != cudaSuccess ||
+          cudaMalloc(&busy_n, sizeof(int)) != cudaSuccess)
         return H->fail(CH4_ERR_NOMEM, "home-cell ranges");
     }
     if (fmoments()) {
@@ -857,17 +908,19 @@ struct Engine : EngineBase {
     if (cudaMalloc(&hit_ring, (size_t)(CHUNK + 1) * NK * L() * sizeof(A)) != cudaSuccess)
       return H->fail(CH4_ERR_NOMEM, "hit ring");
     if (cudaMalloc(&hit_last, (size_t)NK * L() * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "hit last");
-    if (cudaMallocHost(&hit_h, (size_t)(CHUNK + 1) * NK * L() * sizeof(A)) != cudaSuccess)
-      return H->fail(CH4_ERR_NOMEM, "pinned hit tables");
+    hit_h_bytes = (size_t)(CHUNK + 1) * NK * L() * sizeof(A);
+    if (!(hit_h = static_cast<A*>(PinnedPool::get(hit_h_bytes)))) return H->fail(CH4_ERR_NOMEM, "pinned hit tables");
     if (cudaEventCreateWithFlags(&hit_ev, cudaEventDisableTiming) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "event");
     // staging for AoS exchange: a few z-planes at a time (<= 64 MiB)
     const size_t plane = (size_t)c.NX * c.NY * NPOP * sizeof(double);
     chunk_planes = std::max<size_t>(1, std::min<size_t>((size_t)c.NZ, (64u << 20) / plane));
     if (cudaMalloc(&staging_d, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "staging");
-    if (cudaMallocHost(&staging_h, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "pinned staging");
+    staging_bytes = chunk_planes * plane;
+    if (!(staging_h = static_cast<double*>(PinnedPool::get(staging_bytes))))
+      return H->fail(CH4_ERR_NOMEM, "pinned staging");
     if (chunk_planes < (size_t)c.NZ) {  // more than one chunk: double-buffer the upload
       if (cudaMalloc(&staging_d2, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "staging");
-      if (cudaMallocHost(&staging_h2, chunk_planes * plane) != cudaSuccess)
+      if (!(staging_h2 = static_cast<double*>(PinnedPool::get(staging_bytes))))
         return H->fail(CH4_ERR_NOMEM, "pinned staging");
     }
     for (cudaEvent_t& e : up_ev)
