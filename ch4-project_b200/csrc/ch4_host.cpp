@@ -540,8 +540,8 @@ struct Engine : EngineBase {
   double* srec = nullptr;
   int* spid = nullptr;
   int2* crng = nullptr;   // {start, end} per home cell
-  int* busy = nullptr;    // cells for the deposit merge pass, and their count
-  int* busy_n = nullptr;
+  int* busy = nullptr;    // cells for the deposit merge pass, per gather block
+  int *bcount = nullptr, *boff = nullptr;
   int* pstatus = nullptr;  // particle position check of the kernels (sticky until set_particles)
   // global force corrections (NOZEROMODE / CONSTANT_POWER): two slots of 6, the
   // last step's (fm_i) and the one being built; reduction scratch
@@ -591,7 +591,8 @@ struct Engine : EngineBase {
     cudaFree(dbuf[1]);
     cudaFree(crng);
     cudaFree(busy);
-    cudaFree(busy_n);
+    cudaFree(bcount);
+    cudaFree(boff);
     cudaFree(pstatus);
     cudaFree(fmbuf);
     cudaFree(fmpart);
@@ -655,7 +656,8 @@ struct Engine : EngineBase {
     Q.spid = spid;
     Q.cell_rng = crng;
     Q.busy = busy;
-    Q.busy_n = busy_n;
+    Q.bcount = bcount;
+    Q.boff = boff;
     Q.dep = dbuf[dcur_i];
     Q.status = pstatus;
     return Q;
@@ -886,8 +888,10 @@ struct Engine : EngineBase {
         if (cudaMalloc(&dbuf[b], 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "deposit");
         if (cudaMemset(dbuf[b], 0, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "deposit memset");
       }
-      if (cudaMalloc(&crng, sizeof(int2) * nhome()) != cudaSuccess || cudaMalloc(&busy, sizeof(int) * N) != cudaSuccess ||
-          cudaMalloc(&busy_n, sizeof(int)) != cudaSuccess)
+      const size_t nreg = (size_t)((c.NX + GATHER_BLOCK - 1) / GATHER_BLOCK) * c.NY * c.NZ;
+      if (cudaMalloc(&crng, sizeof(int2) * nhome()) != cudaSuccess ||
+          cudaMalloc(&busy, sizeof(int) * nreg * GATHER_BLOCK) != cudaSuccess ||
+          cudaMalloc(&bcount, sizeof(int) * nreg) != cudaSuccess || cudaMalloc(&boff, sizeof(int) * nreg) != cudaSuccess)
         return H->fail(CH4_ERR_NOMEM, "home-cell ranges");
     }
     if (fmoments()) {

@@ -34,6 +34,7 @@ constexpr int PF_FIELDS = (int)(sizeof(ch4_particle) / sizeof(double));
 constexpr int PF_VOL = PF_FIELDS;      // (4/3) pi r^3 with r^2 = 3 nu beta tau_drag
 constexpr int PF_DR = PF_FIELDS + 1;   // rho_p / rho_f = (3 - beta) / (2 beta)
 constexpr int PF_TOTAL = PF_FIELDS + 2;
+constexpr int GATHER_BLOCK = 128;  // threads (cells along x) per block of the first deposit pass
 
 template <typename A>
 struct PartParams {
@@ -60,8 +61,12 @@ struct PartParams {
   double* srec;          // [9][np] the same by sorted position (depositing particles only)
   int* spid;             // particle index by sorted position
   int2* cell_rng;        // [(NX+1)(NY+1)(NZ+1)] {start, end} of every home cell's sorted run
-  int* busy;             // [N] cells whose 8 home cells hold two or more depositing particles
-  int* busy_n;           // their count (device); cell indices fit int: lattices are < 2^31 cells
+  // cells whose 8 home cells hold two or more depositing particles, listed per block of
+  // the first gather pass (region b = busy[b*GATHER_BLOCK ...], bcount[b] entries),
+  // boff = exclusive prefix sum of bcount; cell indices fit int (lattices are < 2^31 cells)
+  int* busy;
+  int* bcount;
+  int* boff;
   A* dep;                // 3 SoA planes, output
   int* status;           // set to 1 when a particle position is outside [0, S] or not finite
 };
@@ -197,29 +202,34 @@ __device__ __forceinline__ void interp_field(const A* __restrict__ f, const PNbr
   }
 }
 
-// One Lagrangian sub-step for one particle: interpolate, move, wrap.  The state the
-// step reads is loaded once, up front (independent loads), and every result is
-// stored once at the end; the arithmetic is the reference's, expression for
-// expression.
+// One Lagrangian sub-step, one particle per quad of lanes: lane a = 0, 1, 2 owns
+// component a (interpolation of u_a and its gradient row, the move along axis a),
+// lane 3 the temperature (interpolation of t and its gradient, the t_old / dt_t /
+// Dt_t bookkeeping).  The couplings between components -- the stencil's position,
+// (u_b - v_b) in the added-mass derivative and in Dt_t -- go through quad shuffles,
+// so every expression is the reference's, operand for operand.  Four lanes per
+// particle cut the registers per thread to a third and quadruple the loads in flight.
 template <typename A>
 __global__ void particle_substep_kernel(const PartParams<A> P) {
-  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ip >= P.np) return;
+  const long long gtid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int ip = (int)(gtid >> 2), a = (int)(gtid & 3);
+  if (ip >= P.np) return;  // whole quads leave together
+  const unsigned qm = 0xFu << (threadIdx.x & 28);
   double* pf = P.pf;
   const long long np = P.np;
-#define F(name) pf[CH4_PF(name) * np + ip]
-  const double x0 = F(x), y0 = F(y), z0 = F(z);
-  const double vx0 = F(vx), vy0 = F(vy), vz0 = F(vz);
-  const double vxo0 = F(vx_old), vyo0 = F(vy_old), vzo0 = F(vz_old);
-  const double uxo0 = F(ux_old), uyo0 = F(uy_old), uzo0 = F(uz_old);
-  const double axo0 = F(ax_old), ayo0 = F(ay_old), azo0 = F(az_old);
-  const double tau = F(tau_drag), beta = F(beta_coeff);
-  const double told0 = P.t ? F(t_old) : 0.0;
-  // ---- interpolate_vector_at_particles, interpolate_scalar_at_particles(t, 't')
-  //      (src/lagrange.c:1211-1439, 1442-1593)
+#define FA(name, k) pf[(CH4_PF(name) + (k)) * np + ip]
+  const bool comp = a < 3;
+  const int c = comp ? a : 0;  // component index for the loads of lane 3 (unused values)
+  const double x0a = FA(x, c);
+  const double px0 = __shfl_sync(qm, x0a, 0, 4), py0 = __shfl_sync(qm, x0a, 1, 4), pz0 = __shfl_sync(qm, x0a, 2, 4);
+  const double v0 = FA(vx, c), vo0 = FA(vx_old, c), uo0 = FA(ux_old, c), ao0 = FA(ax_old, c);
+  const double tau = FA(tau_drag, 0), beta = FA(beta_coeff, 0);
+  const double told0 = (!comp && P.t) ? FA(t_old, 0) : 0.0;
+  // ---- interpolate_vector_at_particles (lanes 0-2), interpolate_scalar_at_particles(t, 't')
+  //      (lane 3) (src/lagrange.c:1211-1439, 1442-1593)
   Stencil t;
   double px, py, pz;
-  wrapped_position(P, x0, y0, z0, px, py, pz);
+  wrapped_position(P, px0, py0, pz0, px, py, pz);
   make_stencil(px, py, pz, t);
   PNbr o;
 #pragma unroll
@@ -230,169 +240,86 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
   }
   const bool lo[3] = {t.im == -1, t.jm == -1, t.km == -1};
   const bool hi[3] = {t.im + 1 == P.NX, t.jm + 1 == P.NY, t.km + 1 == P.NZ};
-  double v[3], gr[9];
-  if (P.gradient) {
-#pragma unroll
-    for (int a = 0; a < 3; a++) interp_field<true>(P.u + a * P.N, o, t.vol, lo, hi, v[a], gr + 3 * a);
-  } else {
-#pragma unroll
-    for (int a = 0; a < 3; a++) interp_field<false>(P.u + a * P.N, o, t.vol, lo, hi, v[a], gr + 3 * a);
-    // without LAGRANGE_GRADIENT the added-mass term reads the stored gradients
-    gr[0] = F(dx_ux);
-    gr[1] = F(dy_ux);
-    gr[2] = F(dz_ux);
-    gr[3] = F(dx_uy);
-    gr[4] = F(dy_uy);
-    gr[5] = F(dz_uy);
-    gr[6] = F(dx_uz);
-    gr[7] = F(dy_uz);
-    gr[8] = F(dz_uz);
+  double val = 0.0, g[3] = {0.0, 0.0, 0.0};
+  if (comp || P.t) {
+    const A* field = comp ? P.u + a * P.N : P.t;
+    if (P.gradient) interp_field<true>(field, o, t.vol, lo, hi, val, g);
+    else interp_field<false>(field, o, t.vol, lo, hi, val, g);
   }
-  const double ux = v[0], uy = v[1], uz = v[2];
-  F(ux) = ux;
-  F(uy) = uy;
-  F(uz) = uz;
-  if (P.gradient) {
-    F(dx_ux) = gr[0];
-    F(dy_ux) = gr[1];
-    F(dz_ux) = gr[2];
-    F(dx_uy) = gr[3];
-    F(dy_uy) = gr[4];
-    F(dz_uy) = gr[5];
-    F(dx_uz) = gr[6];
-    F(dy_uz) = gr[7];
-    F(dz_uz) = gr[8];
+  if (comp && !P.gradient) {  // the added-mass term then reads the stored gradient row
+    g[0] = FA(dx_ux, 3 * a);
+    g[1] = FA(dx_ux, 3 * a + 1);
+    g[2] = FA(dx_ux, 3 * a + 2);
   }
-  // ---- move_particles (src/lagrange.c:3040-3440)
+  const double ux = __shfl_sync(qm, val, 0, 4), uy = __shfl_sync(qm, val, 1, 4), uz = __shfl_sync(qm, val, 2, 4);
+  const double vx0 = __shfl_sync(qm, v0, 0, 4), vy0 = __shfl_sync(qm, v0, 1, 4), vz0 = __shfl_sync(qm, v0, 2, 4);
   const double dtl = P.dtl;
   const bool first = P.first != 0;
-  if (P.t) {
-    double tv, gt[3];
-    if (P.gradient) {
-      interp_field<true>(P.t, o, t.vol, lo, hi, tv, gt);
-      F(dx_t) = gt[0];
-      F(dy_t) = gt[1];
-      F(dz_t) = gt[2];
-    } else {
-      interp_field<false>(P.t, o, t.vol, lo, hi, tv, gt);
+  if (!comp) {
+    // ---- temperature along the path, src/lagrange.c:2997-3010
+    if (P.t) {
+      FA(t, 0) = val;
+      if (P.gradient) {
+        FA(dx_t, 0) = g[0];
+        FA(dx_t, 1) = g[1];
+        FA(dx_t, 2) = g[2];
+      }
+      if (first) {
+        FA(t_old, 0) = val;
+      } else {
+        const double dt_t = (val - told0) / dtl;
+        FA(dt_t, 0) = dt_t;
+        FA(t_old, 0) = val;
+        if (P.gradient) FA(Dt_t, 0) = dt_t + (ux - vx0) * g[0] + (uy - vy0) * g[1] + (uz - vz0) * g[2];
+      }
     }
-    F(t) = tv;
-    // time derivatives of t along the path, src/lagrange.c:2997-3010
-    if (first) {
-      F(t_old) = tv;
-    } else {
-      const double dt_t = (tv - told0) / dtl;
-      F(dt_t) = dt_t;
-      F(t_old) = tv;
-      if (P.gradient) F(Dt_t) = dt_t + (ux - vx0) * gt[0] + (uy - vy0) * gt[1] + (uz - vz0) * gt[2];
-    }
+    return;
   }
-  double xn = x0, yn = y0, zn = z0;
-  if (tau < 0.0) {  // Eulerian probe
-    F(vx) = ux;
-    F(vy) = uy;
-    F(vz) = uz;
+  // ---- move_particles (src/lagrange.c:3040-3440), component a
+  const double u = val;
+  FA(ux, a) = u;
+  if (P.gradient) {
+    FA(dx_ux, 3 * a) = g[0];
+    FA(dx_ux, 3 * a + 1) = g[1];
+    FA(dx_ux, 3 * a + 2) = g[2];
   }
-  if (tau == 0.0) {  // tracer
-    const double vx = ux, vy = uy, vz = uz;
-    double vxo = vxo0, vyo = vyo0, vzo = vzo0;
-    if (first) {
-      vxo = vx;
-      vyo = vy;
-      vzo = vz;
-    }
-    F(ax) = (vx - vxo) / dtl;
-    F(ay) = (vy - vyo) / dtl;
-    F(az) = (vz - vzo) / dtl;
-    if (first) {
-      xn = x0 + dtl * vx;
-      yn = y0 + dtl * vy;
-      zn = z0 + dtl * vz;
-    } else {
-      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo);
-      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo);
-      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo);
-    }
-    F(vx) = vx;
-    F(vy) = vy;
-    F(vz) = vz;
-    F(vx_old) = vx;
-    F(vy_old) = vy;
-    F(vz_old) = vz;
-    F(ux_old) = ux;
-    F(uy_old) = uy;
-    F(uz_old) = uz;
+  double xn = x0a;
+  if (tau < 0.0) FA(vx, a) = u;  // Eulerian probe
+  if (tau == 0.0) {              // tracer
+    const double v = u;
+    const double vo = first ? v : vo0;
+    FA(ax, a) = (v - vo) / dtl;
+    if (first) xn = x0a + dtl * v;
+    else xn = x0a + dtl * 0.5 * (3.0 * v - vo);
+    FA(vx, a) = v;
+    FA(vx_old, a) = v;
+    FA(ux_old, a) = u;
   }
   if (tau > 0.0) {  // Stokes drag (+ added mass)
     const double invtau = 1.0 / tau;
-    double vx = vx0, vy = vy0, vz = vz0;
-    double ax = (ux - vx) * invtau, ay = (uy - vy) * invtau, az = (uz - vz) * invtau;
-    if (P.gravity) {  // -g, src/lagrange.c:3312-3323
-      ax -= P.g[0];
-      ay -= P.g[1];
-      az -= P.g[2];
-    }
-    double uxo = uxo0, uyo = uyo0, uzo = uzo0;
+    double v = v0;
+    double acc = (u - v) * invtau;
+    if (P.gravity) acc -= P.g[a];  // -g, src/lagrange.c:3312-3323
     if (P.addedmass && beta != 0.0) {
-      if (P.gravity) {  // -(-beta) g, src/lagrange.c:3330-3339
-        ax -= (-beta) * P.g[0];
-        ay -= (-beta) * P.g[1];
-        az -= (-beta) * P.g[2];
-      }
-      if (first) {
-        uxo = ux;
-        uyo = uy;
-        uzo = uz;
-      }
-      const double Dx = (ux - uxo) / dtl + (ux - vx) * gr[0] + (uy - vy) * gr[1] + (uz - vz) * gr[2];
-      const double Dy = (uy - uyo) / dtl + (ux - vx) * gr[3] + (uy - vy) * gr[4] + (uz - vz) * gr[5];
-      const double Dz = (uz - uzo) / dtl + (ux - vx) * gr[6] + (uy - vy) * gr[7] + (uz - vz) * gr[8];
-      ax += Dx * beta;
-      ay += Dy * beta;
-      az += Dz * beta;
-      F(Dt_ux) = Dx;
-      F(Dt_uy) = Dy;
-      F(Dt_uz) = Dz;
+      if (P.gravity) acc -= (-beta) * P.g[a];  // -(-beta) g, src/lagrange.c:3330-3339
+      const double uo = first ? u : uo0;
+      const double D = (u - uo) / dtl + (ux - vx0) * g[0] + (uy - vy0) * g[1] + (uz - vz0) * g[2];
+      acc += D * beta;
+      FA(Dt_ux, a) = D;
     }
-    if (first) {
-      xn = x0 + dtl * vx;
-      yn = y0 + dtl * vy;
-      zn = z0 + dtl * vz;
-    } else {
-      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo0);
-      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo0);
-      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo0);
-    }
-    F(vx_old) = vx;
-    F(vy_old) = vy;
-    F(vz_old) = vz;
-    F(ux_old) = ux;
-    F(uy_old) = uy;
-    F(uz_old) = uz;
-    if (first) {
-      vx += dtl * ax;
-      vy += dtl * ay;
-      vz += dtl * az;
-    } else {
-      vx += dtl * 0.5 * (3.0 * ax - axo0);
-      vy += dtl * 0.5 * (3.0 * ay - ayo0);
-      vz += dtl * 0.5 * (3.0 * az - azo0);
-    }
-    F(vx) = vx;
-    F(vy) = vy;
-    F(vz) = vz;
-    F(ax) = ax;
-    F(ay) = ay;
-    F(az) = az;
-    F(ax_old) = ax;
-    F(ay_old) = ay;
-    F(az_old) = az;
+    if (first) xn = x0a + dtl * v;
+    else xn = x0a + dtl * 0.5 * (3.0 * v - vo0);
+    FA(vx_old, a) = v;
+    FA(ux_old, a) = u;
+    if (first) v += dtl * acc;
+    else v += dtl * 0.5 * (3.0 * acc - ao0);
+    FA(vx, a) = v;
+    FA(ax, a) = acc;
+    FA(ax_old, a) = acc;
   }
   // ---- LAGRANGE_WRAP of sendrecv_particles
-  F(x) = pwrapd(xn, P.SX);
-  F(z) = pwrapd(zn, P.SZ);
-  F(y) = pwrapd(yn, P.SY);
-#undef F
+  FA(x, a) = pwrapd(xn, a == 0 ? P.SX : a == 1 ? P.SY : P.SZ);
+#undef FA
 }
 
 // Deposit record and home-cell key of every particle (src/lagrange_feedback.c:34-118).
@@ -531,45 +458,61 @@ __device__ __forceinline__ void deposit_merge(const int* __restrict__ spid, cons
 // Deposit on every lattice cell, first pass: cells whose 8 home cells hold no
 // depositing particle get 0, those holding one get its contribution directly; the
 // others (two or more, a few per cent of the cells at 0.04 depositing particles per
-// cell) are appended to P.busy for deposit_busy_kernel, so that no warp runs the merge
-// loop for the sake of a single lane.
+// cell) are listed in the block's region of P.busy for deposit_busy_kernel, so that no
+// warp runs the merge loop for the sake of a single lane.  The list is built with a
+// shared-memory counter: no global atomics (one address taking a few per cent of 16 M
+// cells' appends serialised the whole pass).
 template <typename A>
-__global__ void deposit_gather_kernel(const PartParams<A> P) {
+__global__ void __launch_bounds__(GATHER_BLOCK) deposit_gather_kernel(const PartParams<A> P) {
   // grid (x blocks, NY, NZ): no index division
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.NX) return;
+  __shared__ int s_n;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  const int i = blockIdx.x * GATHER_BLOCK + threadIdx.x;
   const int j = blockIdx.y, k = blockIdx.z;
-  const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
-  const int HX = P.NX + 1, HY = P.NY + 1;
-  int m = 0, best = 0, slot = 0;
+  const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (i < P.NX) {
+    const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
+    const int HX = P.NX + 1, HY = P.NY + 1;
+    int m = 0, best = 0, slot = 0;
 #pragma unroll
-  for (int h = 0; h < 8; h++) {
-    const int2 rg = P.cell_rng[home_of(i, j, k, h, HX, HY)];
-    const int cnt = rg.y - rg.x;
-    if (cnt > 0) {
-      best = h;
-      slot = rg.x;
+    for (int h = 0; h < 8; h++) {
+      const int2 rg = P.cell_rng[home_of(i, j, k, h, HX, HY)];
+      const int cnt = rg.y - rg.x;
+      if (cnt > 0) {
+        best = h;
+        slot = rg.x;
+      }
+      m += cnt;
     }
-    m += cnt;
+    if (m >= 2) {
+      P.busy[(long long)bid * GATHER_BLOCK + atomicAdd(&s_n, 1)] = (int)cidx;  // the merge writes this cell
+    } else {
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+      if (m == 1) deposit_add(P.srec, P.np, slot, best, acc0, acc1, acc2);
+      P.dep[cidx] = (A)acc0;
+      P.dep[P.N + cidx] = (A)acc1;
+      P.dep[2 * P.N + cidx] = (A)acc2;
+    }
   }
-  if (m >= 2) {
-    P.busy[atomicAdd(P.busy_n, 1)] = (int)cidx;  // the merge writes this cell
-    return;
-  }
-  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-  if (m == 1) deposit_add(P.srec, P.np, slot, best, acc0, acc1, acc2);
-  P.dep[cidx] = (A)acc0;
-  P.dep[P.N + cidx] = (A)acc1;
-  P.dep[2 * P.N + cidx] = (A)acc2;
+  __syncthreads();
+  if (threadIdx.x == 0) P.bcount[bid] = s_n;
 }
 
-// Second pass: the merge on the listed cells (grid-stride over the device count).
+// Second pass: the merge on the listed cells, dense over all regions (grid-stride;
+// entry t lies in the last region whose prefix offset is <= t).
 template <typename A>
-__global__ void deposit_busy_kernel(const PartParams<A> P) {
-  const int n = *P.busy_n;
+__global__ void deposit_busy_kernel(const PartParams<A> P, int nregions) {
+  const int total = P.boff[nregions - 1] + P.bcount[nregions - 1];
   const int HX = P.NX + 1, HY = P.NY + 1;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int cidx = P.busy[t];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nregions - 1;
+    while (lo < hi) {  // largest r with boff[r] <= t
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.boff[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const int cidx = P.busy[(long long)lo * GATHER_BLOCK + (t - P.boff[lo])];
     const int i = cidx % P.NX, j = (cidx / P.NX) % P.NY, k = cidx / (P.NX * P.NY);
     int pos[8], endp[8];
 #pragma unroll
