@@ -530,8 +530,7 @@ struct Engine : EngineBase {
   // re-sort of the state slots by home cell every REORDER_EVERY steps (a particle
   // moves well under a cell in that time, so the order stays close to sorted)
   static constexpr int REORDER_EVERY = 4;
-  A* upart = nullptr;     // u^{n+1} for the interpolation, 3 planes
-  A* tpart = nullptr;     // t^{n+1} for the interpolation (LB_TEMPERATURE)
+  A* upart = nullptr;     // (u_x, u_y, u_z, t)^{n+1} per cell for the interpolation
   A* dbuf[2] = {nullptr, nullptr};  // two-way deposit of this / previous step
   int dcur_i = 0;
   unsigned int *key = nullptr, *key2 = nullptr;
@@ -541,7 +540,7 @@ struct Engine : EngineBase {
   int* spid = nullptr;
   int2* crng = nullptr;   // {start, end} per home cell
   int* busy = nullptr;    // cells for the deposit merge pass, per gather block
-  int *bcount = nullptr, *boff = nullptr;
+  int *bcount = nullptr, *boff = nullptr, *dense = nullptr;
   int* pstatus = nullptr;  // particle position check of the kernels (sticky until set_particles)
   // global force corrections (NOZEROMODE / CONSTANT_POWER): two slots of 6, the
   // last step's (fm_i) and the one being built; reduction scratch
@@ -586,13 +585,13 @@ struct Engine : EngineBase {
     if (hit_ev) cudaEventDestroy(hit_ev);
     free_particles();
     cudaFree(upart);
-    cudaFree(tpart);
     cudaFree(dbuf[0]);
     cudaFree(dbuf[1]);
     cudaFree(crng);
     cudaFree(busy);
     cudaFree(bcount);
     cudaFree(boff);
+    cudaFree(dense);
     cudaFree(pstatus);
     cudaFree(fmbuf);
     cudaFree(fmpart);
@@ -647,8 +646,8 @@ struct Engine : EngineBase {
     Q.pid = pid;
     Q.pf_alt = pf_alt;
     Q.pid_alt = pid_alt;
-    Q.u = upart;
-    Q.t = tpart;
+    Q.ut4 = upart;
+    Q.has_t = nsets_on[1];
     Q.key = key;
     Q.order = order;
     Q.rec = rec;
@@ -658,6 +657,7 @@ struct Engine : EngineBase {
     Q.busy = busy;
     Q.bcount = bcount;
     Q.boff = boff;
+    Q.dense = dense;
     Q.dep = dbuf[dcur_i];
     Q.status = pstatus;
     return Q;
@@ -876,9 +876,7 @@ struct Engine : EngineBase {
     }
     if (nsets_on[1] && cudaMalloc(&tprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tprev");
     if (nsets_on[2] && cudaMalloc(&sprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "sprev");
-    if (lagr() && cudaMalloc(&upart, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u for particles");
-    if (lagr() && nsets_on[1] && cudaMalloc(&tpart, N * sizeof(A)) != cudaSuccess)
-      return H->fail(CH4_ERR_NOMEM, "t for particles");
+    if (lagr() && cudaMalloc(&upart, 4 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u for particles");
     if (lagr()) {
       if (cudaMalloc(&pstatus, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "particle status");
       if (cudaMemset(pstatus, 0, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "particle status");
@@ -891,6 +889,7 @@ struct Engine : EngineBase {
       const size_t nreg = (size_t)((c.NX + GATHER_BLOCK - 1) / GATHER_BLOCK) * c.NY * c.NZ;
       if (cudaMalloc(&crng, sizeof(int2) * nhome()) != cudaSuccess ||
           cudaMalloc(&busy, sizeof(int) * nreg * GATHER_BLOCK) != cudaSuccess ||
+          cudaMalloc(&dense, sizeof(int) * nreg * GATHER_BLOCK) != cudaSuccess ||
           cudaMalloc(&bcount, sizeof(int) * nreg) != cudaSuccess || cudaMalloc(&boff, sizeof(int) * nreg) != cudaSuccess)
         return H->fail(CH4_ERR_NOMEM, "home-cell ranges");
     }
@@ -1209,7 +1208,7 @@ struct Engine : EngineBase {
           // u^{n+1} with dt/2 F^n, then the Lagrangian sub-steps (src/main.c:164-185)
           bind_pops(cur);
           if ((st = H->cuda(launch_hydro(P, shape, P.hit_cur, twoway() ? P.dcur : nullptr, fm_last(), nullptr, nullptr, nullptr,
-                                         nullptr, nullptr, upart, H->stream, tpart),
+                                         nullptr, nullptr, nullptr, H->stream, upart),
                             "particle u")))
             return st;
           PartParams<A> Q = part_params();

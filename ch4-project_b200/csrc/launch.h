@@ -20,15 +20,16 @@ cudaError_t launch_step(const StepParams<float>& P, LaunchShape s, cudaStream_t 
 // t^{n-1} := m(g), s^{n-1} := m(h)
 cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStream_t st);
 cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStream_t st);
-// hydro fields / force (FP64 outputs), optional arithmetic-precision u planes and t plane
+// hydro fields / force (FP64 outputs), optional arithmetic-precision u planes (u_arith)
+// and (u_x, u_y, u_z, t) per cell for the particles (ut4)
 cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep,
                          const double* fm, double* dens,
                          double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st,
-                         double* t_arith = nullptr);
+                         double* ut4 = nullptr);
 cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep,
                          const float* fm, double* dens,
                          double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
-                         float* t_arith = nullptr);
+                         float* ut4 = nullptr);
 // global force corrections (NOZEROMODE / CONSTANT_POWER) of one step into fm[6];
 // partial holds nblocks * 9 * 2 doubles
 cudaError_t launch_force_moments(const StepParams<double>& P, LaunchShape s, const double* hit_cur, int with_prev,

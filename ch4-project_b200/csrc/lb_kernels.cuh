@@ -207,10 +207,23 @@ __global__ void init_prev_kernel(const StepParams<A> P) {
 // hydro_fields (src/lb.c:420-539): dens, u (with dt/2 of the force built from the
 // kept temperature and the given phase table), t, s -- all as FP64 SoA planes.
 // Also the force field itself when `force` is non-null, and u and t in the
-// arithmetic precision for the particle interpolation (u_arith, t_arith).
+// arithmetic precision: u_arith (3 planes, LES) and ut4 ((u_x, u_y, u_z, t) per cell,
+// the particle interpolation; t = 0 without a temperature set).
+template <typename A>
+__device__ __forceinline__ void store_ut4(A* ut4, long long idx, A a, A b, A c, A d);
+template <>
+__device__ __forceinline__ void store_ut4<float>(float* ut4, long long idx, float a, float b, float c, float d) {
+  reinterpret_cast<float4*>(ut4)[idx] = make_float4(a, b, c, d);
+}
+template <>
+__device__ __forceinline__ void store_ut4<double>(double* ut4, long long idx, double a, double b, double c, double d) {
+  reinterpret_cast<double2*>(ut4)[2 * idx] = make_double2(a, b);
+  reinterpret_cast<double2*>(ut4)[2 * idx + 1] = make_double2(c, d);
+}
+
 template <typename S, typename A, bool THERM, bool SCAL>
 __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, const A* fm, double* dens, double* u,
-                             double* t, double* s, double* force, A* u_arith, A* t_arith) {
+                             double* t, double* s, double* force, A* u_arith, A* ut4) {
   // grid (x blocks, NY, NZ): no index division
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
@@ -244,15 +257,17 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
     force[P.N + idx] = (double)Fy;
     force[2 * P.N + idx] = (double)Fz;
   }
+  A tt4 = A(0);
   if constexpr (THERM) {
-    if (t || t_arith) {
+    if (t || ut4) {
       A g[Q];
       load_set<S, A, 1>(P, idx, g);
       const A tt = mom0(g);
       if (t) t[idx] = (double)tt;
-      if (t_arith) t_arith[idx] = tt;
+      tt4 = tt;
     }
   }
+  if (ut4) store_ut4<A>(ut4, idx, ux, uy, uz, tt4);
   if constexpr (SCAL) {
     if (s) {
       A h[Q];

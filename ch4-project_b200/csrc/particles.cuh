@@ -51,8 +51,8 @@ struct PartParams {
   const int* pid; // particle index of each slot
   double* pf_alt; // reorder target of pf / pid
   int* pid_alt;
-  const A* u;     // 3 SoA planes of u^{n+1}
-  const A* t;     // t^{n+1} = m(g^{n+1}) with LB_TEMPERATURE, else null
+  const A* ut4;   // u^{n+1} and t^{n+1} = m(g^{n+1}) per cell, (ux, uy, uz, t) (t = 0 without LB_TEMPERATURE)
+  int has_t;      // LB_TEMPERATURE: interpolate t too
   // deposit
   unsigned int* key;     // sort keys, by particle index: home cell (+ nh when it deposits nothing)
   int* order;            // sort values, by particle index: the state slot; after the sort, the
@@ -67,6 +67,7 @@ struct PartParams {
   int* busy;
   int* bcount;
   int* boff;
+  int* dense;            // the listed cells, compacted in region order
   A* dep;                // 3 SoA planes, output
   int* status;           // set to 1 when a particle position is outside [0, S] or not finite
 };
@@ -134,32 +135,25 @@ struct PNbr {
   int yo[4], xo[4];
 };
 
+// periodic index for i in [-2, n + 1] (the neighbourhood of a stencil): one wrap
+// suffices for n >= 2; a lattice one cell wide maps everything to 0
 __device__ __forceinline__ int pmod(int i, int n) {
-  const int r = i % n;
-  return r < 0 ? r + n : r;
+  if (n == 1) return 0;
+  return i < 0 ? i + n : (i >= n ? i - n : i);
 }
 
-// Trilinear value (and with GRAD the gradient) of one lattice field at a particle,
-// `lo`/`hi` flagging a stencil whose lower corner is the halo layer -1 / whose upper
-// corner is the halo layer n on each axis.  Per corner the gradient is centred,
+// Trilinear value (and with GRAD the gradient) of one lattice field at a particle from
+// its neighbourhood block b[z][y][x] (lower stencil corner at block index 1 on each
+// axis), `lo`/`hi` flagging a stencil whose lower corner is the halo layer -1 / whose
+// upper corner is the halo layer n on each axis.  Per corner the gradient is centred,
 // (u(c+1) - u(c-1)) / 2, or one-sided of second order on those halo layers
 // (LAGRANGE_INTERPOLATION_FIX, src/gradients.c:358-420 for vectors, 731-800 for
-// scalars); the eight corners are summed in the reference's order with the weights
-// of make_stencil (src/lagrange.c:1266-1439).  The 32 lattice values used (the 8
-// corners and their 24 face neighbours) are loaded once, up front.
+// scalars); the eight corners are summed in the reference's order with the weights of
+// make_stencil (src/lagrange.c:1266-1439).  Only the 8 corners and, with GRAD, their 24
+// face neighbours are read.
 template <bool GRAD, typename A>
-__device__ __forceinline__ void interp_field(const A* __restrict__ f, const PNbr& o, const double* vol, const bool* lo,
-                                             const bool* hi, double& val, double* grad) {
-  A b[4][4][4];
-#pragma unroll
-  for (int z = 0; z < 4; z++)
-#pragma unroll
-    for (int y = 0; y < 4; y++)
-#pragma unroll
-      for (int x = 0; x < 4; x++) {
-        const int inner = (x == 1 || x == 2) + (y == 1 || y == 2) + (z == 1 || z == 2);
-        if (inner == 3 || (GRAD && inner == 2)) b[z][y][x] = f[o.zo[z] + o.yo[y] + o.xo[x]];
-      }
+__device__ __forceinline__ void interp_block(const A (&b)[4][4][4], const double* vol, const bool* lo, const bool* hi,
+                                             double& val, double* grad) {
   double acc = 0.0;
 #pragma unroll
   for (int c = 0; c < 8; c++) {
@@ -202,34 +196,78 @@ __device__ __forceinline__ void interp_field(const A* __restrict__ f, const PNbr
   }
 }
 
-// One Lagrangian sub-step, one particle per quad of lanes: lane a = 0, 1, 2 owns
-// component a (interpolation of u_a and its gradient row, the move along axis a),
-// lane 3 the temperature (interpolation of t and its gradient, the t_old / dt_t /
-// Dt_t bookkeeping).  The couplings between components -- the stencil's position,
-// (u_b - v_b) in the added-mass derivative and in Dt_t -- go through quad shuffles,
-// so every expression is the reference's, operand for operand.  Four lanes per
-// particle cut the registers per thread to a third and quadruple the loads in flight.
+// block entries an interpolation reads: the 8 corners, and with GRAD their face neighbours
+template <bool GRAD>
+__device__ __forceinline__ constexpr bool block_used(int x, int y, int z) {
+  const int inner = (x == 1 || x == 2) + (y == 1 || y == 2) + (z == 1 || z == 2);
+  return inner == 3 || (GRAD && inner == 2);
+}
+
+// Value (and gradient) of the fields of ut4 at a particle: FP32 cells are read as one
+// 16-byte vector (u_x, u_y, u_z, t); FP64 cells field by field.
+template <bool GRAD>
+__device__ __forceinline__ void interp_cells(const float* __restrict__ ut4, int nf, const PNbr& o, const double* vol,
+                                             const bool* lo, const bool* hi, double* val, double* grad) {
+  float b[4][4][4][4];  // [field][z][y][x]
+#pragma unroll
+  for (int z = 0; z < 4; z++)
+#pragma unroll
+    for (int y = 0; y < 4; y++)
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+        if (block_used<GRAD>(x, y, z)) {
+          const float4 v = reinterpret_cast<const float4*>(ut4)[o.zo[z] + o.yo[y] + o.xo[x]];
+          b[0][z][y][x] = v.x;
+          b[1][z][y][x] = v.y;
+          b[2][z][y][x] = v.z;
+          b[3][z][y][x] = v.w;
+        }
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+    if (a < nf) interp_block<GRAD>(b[a], vol, lo, hi, val[a], grad + 3 * a);
+}
+
+template <bool GRAD>
+__device__ __forceinline__ void interp_cells(const double* __restrict__ ut4, int nf, const PNbr& o, const double* vol,
+                                             const bool* lo, const bool* hi, double* val, double* grad) {
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    if (a >= nf) break;
+    double b[4][4][4];
+#pragma unroll
+    for (int z = 0; z < 4; z++)
+#pragma unroll
+      for (int y = 0; y < 4; y++)
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+          if (block_used<GRAD>(x, y, z)) b[z][y][x] = ut4[4 * (o.zo[z] + o.yo[y] + o.xo[x]) + a];
+    interp_block<GRAD>(b, vol, lo, hi, val[a], grad + 3 * a);
+  }
+}
+
+// One Lagrangian sub-step for one particle: interpolate, move, wrap.  The state the
+// step reads is loaded once, up front (independent loads), and every result is
+// stored once at the end; the arithmetic is the reference's, expression for
+// expression.
 template <typename A>
 __global__ void particle_substep_kernel(const PartParams<A> P) {
-  const long long gtid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int ip = (int)(gtid >> 2), a = (int)(gtid & 3);
-  if (ip >= P.np) return;  // whole quads leave together
-  const unsigned qm = 0xFu << (threadIdx.x & 28);
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= P.np) return;
   double* pf = P.pf;
   const long long np = P.np;
-#define FA(name, k) pf[(CH4_PF(name) + (k)) * np + ip]
-  const bool comp = a < 3;
-  const int c = comp ? a : 0;  // component index for the loads of lane 3 (unused values)
-  const double x0a = FA(x, c);
-  const double px0 = __shfl_sync(qm, x0a, 0, 4), py0 = __shfl_sync(qm, x0a, 1, 4), pz0 = __shfl_sync(qm, x0a, 2, 4);
-  const double v0 = FA(vx, c), vo0 = FA(vx_old, c), uo0 = FA(ux_old, c), ao0 = FA(ax_old, c);
-  const double tau = FA(tau_drag, 0), beta = FA(beta_coeff, 0);
-  const double told0 = (!comp && P.t) ? FA(t_old, 0) : 0.0;
-  // ---- interpolate_vector_at_particles (lanes 0-2), interpolate_scalar_at_particles(t, 't')
-  //      (lane 3) (src/lagrange.c:1211-1439, 1442-1593)
+#define F(name) pf[CH4_PF(name) * np + ip]
+  const double x0 = F(x), y0 = F(y), z0 = F(z);
+  const double vx0 = F(vx), vy0 = F(vy), vz0 = F(vz);
+  const double vxo0 = F(vx_old), vyo0 = F(vy_old), vzo0 = F(vz_old);
+  const double uxo0 = F(ux_old), uyo0 = F(uy_old), uzo0 = F(uz_old);
+  const double axo0 = F(ax_old), ayo0 = F(ay_old), azo0 = F(az_old);
+  const double tau = F(tau_drag), beta = F(beta_coeff);
+  const double told0 = P.has_t ? F(t_old) : 0.0;
+  // ---- interpolate_vector_at_particles, interpolate_scalar_at_particles(t, 't')
+  //      (src/lagrange.c:1211-1439, 1442-1593)
   Stencil t;
   double px, py, pz;
-  wrapped_position(P, px0, py0, pz0, px, py, pz);
+  wrapped_position(P, x0, y0, z0, px, py, pz);
   make_stencil(px, py, pz, t);
   PNbr o;
 #pragma unroll
@@ -240,86 +278,166 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
   }
   const bool lo[3] = {t.im == -1, t.jm == -1, t.km == -1};
   const bool hi[3] = {t.im + 1 == P.NX, t.jm + 1 == P.NY, t.km + 1 == P.NZ};
-  double val = 0.0, g[3] = {0.0, 0.0, 0.0};
-  if (comp || P.t) {
-    const A* field = comp ? P.u + a * P.N : P.t;
-    if (P.gradient) interp_field<true>(field, o, t.vol, lo, hi, val, g);
-    else interp_field<false>(field, o, t.vol, lo, hi, val, g);
+  double v[4], gr[12];  // u_x, u_y, u_z, t and their gradient rows
+  const int nf = P.has_t ? 4 : 3;
+  if (P.gradient) {
+    interp_cells<true>(P.ut4, nf, o, t.vol, lo, hi, v, gr);
+  } else {
+    interp_cells<false>(P.ut4, nf, o, t.vol, lo, hi, v, gr);
+    // without LAGRANGE_GRADIENT the added-mass term reads the stored gradients
+    gr[0] = F(dx_ux);
+    gr[1] = F(dy_ux);
+    gr[2] = F(dz_ux);
+    gr[3] = F(dx_uy);
+    gr[4] = F(dy_uy);
+    gr[5] = F(dz_uy);
+    gr[6] = F(dx_uz);
+    gr[7] = F(dy_uz);
+    gr[8] = F(dz_uz);
   }
-  if (comp && !P.gradient) {  // the added-mass term then reads the stored gradient row
-    g[0] = FA(dx_ux, 3 * a);
-    g[1] = FA(dx_ux, 3 * a + 1);
-    g[2] = FA(dx_ux, 3 * a + 2);
+  const double ux = v[0], uy = v[1], uz = v[2];
+  F(ux) = ux;
+  F(uy) = uy;
+  F(uz) = uz;
+  if (P.gradient) {
+    F(dx_ux) = gr[0];
+    F(dy_ux) = gr[1];
+    F(dz_ux) = gr[2];
+    F(dx_uy) = gr[3];
+    F(dy_uy) = gr[4];
+    F(dz_uy) = gr[5];
+    F(dx_uz) = gr[6];
+    F(dy_uz) = gr[7];
+    F(dz_uz) = gr[8];
   }
-  const double ux = __shfl_sync(qm, val, 0, 4), uy = __shfl_sync(qm, val, 1, 4), uz = __shfl_sync(qm, val, 2, 4);
-  const double vx0 = __shfl_sync(qm, v0, 0, 4), vy0 = __shfl_sync(qm, v0, 1, 4), vz0 = __shfl_sync(qm, v0, 2, 4);
+  // ---- move_particles (src/lagrange.c:3040-3440)
   const double dtl = P.dtl;
   const bool first = P.first != 0;
-  if (!comp) {
-    // ---- temperature along the path, src/lagrange.c:2997-3010
-    if (P.t) {
-      FA(t, 0) = val;
-      if (P.gradient) {
-        FA(dx_t, 0) = g[0];
-        FA(dx_t, 1) = g[1];
-        FA(dx_t, 2) = g[2];
-      }
-      if (first) {
-        FA(t_old, 0) = val;
-      } else {
-        const double dt_t = (val - told0) / dtl;
-        FA(dt_t, 0) = dt_t;
-        FA(t_old, 0) = val;
-        if (P.gradient) FA(Dt_t, 0) = dt_t + (ux - vx0) * g[0] + (uy - vy0) * g[1] + (uz - vz0) * g[2];
-      }
+  if (P.has_t) {
+    const double tv = v[3];
+    const double* gt = gr + 9;
+    if (P.gradient) {
+      F(dx_t) = gt[0];
+      F(dy_t) = gt[1];
+      F(dz_t) = gt[2];
     }
-    return;
+    F(t) = tv;
+    // time derivatives of t along the path, src/lagrange.c:2997-3010
+    if (first) {
+      F(t_old) = tv;
+    } else {
+      const double dt_t = (tv - told0) / dtl;
+      F(dt_t) = dt_t;
+      F(t_old) = tv;
+      if (P.gradient) F(Dt_t) = dt_t + (ux - vx0) * gt[0] + (uy - vy0) * gt[1] + (uz - vz0) * gt[2];
+    }
   }
-  // ---- move_particles (src/lagrange.c:3040-3440), component a
-  const double u = val;
-  FA(ux, a) = u;
-  if (P.gradient) {
-    FA(dx_ux, 3 * a) = g[0];
-    FA(dx_ux, 3 * a + 1) = g[1];
-    FA(dx_ux, 3 * a + 2) = g[2];
+  double xn = x0, yn = y0, zn = z0;
+  if (tau < 0.0) {  // Eulerian probe
+    F(vx) = ux;
+    F(vy) = uy;
+    F(vz) = uz;
   }
-  double xn = x0a;
-  if (tau < 0.0) FA(vx, a) = u;  // Eulerian probe
-  if (tau == 0.0) {              // tracer
-    const double v = u;
-    const double vo = first ? v : vo0;
-    FA(ax, a) = (v - vo) / dtl;
-    if (first) xn = x0a + dtl * v;
-    else xn = x0a + dtl * 0.5 * (3.0 * v - vo);
-    FA(vx, a) = v;
-    FA(vx_old, a) = v;
-    FA(ux_old, a) = u;
+  if (tau == 0.0) {  // tracer
+    const double vx = ux, vy = uy, vz = uz;
+    double vxo = vxo0, vyo = vyo0, vzo = vzo0;
+    if (first) {
+      vxo = vx;
+      vyo = vy;
+      vzo = vz;
+    }
+    F(ax) = (vx - vxo) / dtl;
+    F(ay) = (vy - vyo) / dtl;
+    F(az) = (vz - vzo) / dtl;
+    if (first) {
+      xn = x0 + dtl * vx;
+      yn = y0 + dtl * vy;
+      zn = z0 + dtl * vz;
+    } else {
+      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo);
+      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo);
+      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo);
+    }
+    F(vx) = vx;
+    F(vy) = vy;
+    F(vz) = vz;
+    F(vx_old) = vx;
+    F(vy_old) = vy;
+    F(vz_old) = vz;
+    F(ux_old) = ux;
+    F(uy_old) = uy;
+    F(uz_old) = uz;
   }
   if (tau > 0.0) {  // Stokes drag (+ added mass)
     const double invtau = 1.0 / tau;
-    double v = v0;
-    double acc = (u - v) * invtau;
-    if (P.gravity) acc -= P.g[a];  // -g, src/lagrange.c:3312-3323
-    if (P.addedmass && beta != 0.0) {
-      if (P.gravity) acc -= (-beta) * P.g[a];  // -(-beta) g, src/lagrange.c:3330-3339
-      const double uo = first ? u : uo0;
-      const double D = (u - uo) / dtl + (ux - vx0) * g[0] + (uy - vy0) * g[1] + (uz - vz0) * g[2];
-      acc += D * beta;
-      FA(Dt_ux, a) = D;
+    double vx = vx0, vy = vy0, vz = vz0;
+    double ax = (ux - vx) * invtau, ay = (uy - vy) * invtau, az = (uz - vz) * invtau;
+    if (P.gravity) {  // -g, src/lagrange.c:3312-3323
+      ax -= P.g[0];
+      ay -= P.g[1];
+      az -= P.g[2];
     }
-    if (first) xn = x0a + dtl * v;
-    else xn = x0a + dtl * 0.5 * (3.0 * v - vo0);
-    FA(vx_old, a) = v;
-    FA(ux_old, a) = u;
-    if (first) v += dtl * acc;
-    else v += dtl * 0.5 * (3.0 * acc - ao0);
-    FA(vx, a) = v;
-    FA(ax, a) = acc;
-    FA(ax_old, a) = acc;
+    double uxo = uxo0, uyo = uyo0, uzo = uzo0;
+    if (P.addedmass && beta != 0.0) {
+      if (P.gravity) {  // -(-beta) g, src/lagrange.c:3330-3339
+        ax -= (-beta) * P.g[0];
+        ay -= (-beta) * P.g[1];
+        az -= (-beta) * P.g[2];
+      }
+      if (first) {
+        uxo = ux;
+        uyo = uy;
+        uzo = uz;
+      }
+      const double Dx = (ux - uxo) / dtl + (ux - vx) * gr[0] + (uy - vy) * gr[1] + (uz - vz) * gr[2];
+      const double Dy = (uy - uyo) / dtl + (ux - vx) * gr[3] + (uy - vy) * gr[4] + (uz - vz) * gr[5];
+      const double Dz = (uz - uzo) / dtl + (ux - vx) * gr[6] + (uy - vy) * gr[7] + (uz - vz) * gr[8];
+      ax += Dx * beta;
+      ay += Dy * beta;
+      az += Dz * beta;
+      F(Dt_ux) = Dx;
+      F(Dt_uy) = Dy;
+      F(Dt_uz) = Dz;
+    }
+    if (first) {
+      xn = x0 + dtl * vx;
+      yn = y0 + dtl * vy;
+      zn = z0 + dtl * vz;
+    } else {
+      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo0);
+      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo0);
+      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo0);
+    }
+    F(vx_old) = vx;
+    F(vy_old) = vy;
+    F(vz_old) = vz;
+    F(ux_old) = ux;
+    F(uy_old) = uy;
+    F(uz_old) = uz;
+    if (first) {
+      vx += dtl * ax;
+      vy += dtl * ay;
+      vz += dtl * az;
+    } else {
+      vx += dtl * 0.5 * (3.0 * ax - axo0);
+      vy += dtl * 0.5 * (3.0 * ay - ayo0);
+      vz += dtl * 0.5 * (3.0 * az - azo0);
+    }
+    F(vx) = vx;
+    F(vy) = vy;
+    F(vz) = vz;
+    F(ax) = ax;
+    F(ay) = ay;
+    F(az) = az;
+    F(ax_old) = ax;
+    F(ay_old) = ay;
+    F(az_old) = az;
   }
   // ---- LAGRANGE_WRAP of sendrecv_particles
-  FA(x, a) = pwrapd(xn, a == 0 ? P.SX : a == 1 ? P.SY : P.SZ);
-#undef FA
+  F(x) = pwrapd(xn, P.SX);
+  F(z) = pwrapd(zn, P.SZ);
+  F(y) = pwrapd(yn, P.SY);
+#undef F
 }
 
 // Deposit record and home-cell key of every particle (src/lagrange_feedback.c:34-118).
@@ -499,20 +617,22 @@ __global__ void __launch_bounds__(GATHER_BLOCK) deposit_gather_kernel(const Part
   if (threadIdx.x == 0) P.bcount[bid] = s_n;
 }
 
-// Second pass: the merge on the listed cells, dense over all regions (grid-stride;
-// entry t lies in the last region whose prefix offset is <= t).
+// The listed cells of every region, compacted to P.dense[boff[r] ...].
+template <typename A>
+__global__ void deposit_compact_kernel(const PartParams<A> P, int nregions) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nregions) return;
+  const int n = P.bcount[r], o = P.boff[r];
+  for (int t = 0; t < n; t++) P.dense[o + t] = P.busy[(long long)r * GATHER_BLOCK + t];
+}
+
+// Second pass: the merge on the listed cells (grid-stride over the compacted list).
 template <typename A>
 __global__ void deposit_busy_kernel(const PartParams<A> P, int nregions) {
   const int total = P.boff[nregions - 1] + P.bcount[nregions - 1];
   const int HX = P.NX + 1, HY = P.NY + 1;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    int lo = 0, hi = nregions - 1;
-    while (lo < hi) {  // largest r with boff[r] <= t
-      const int mid = (lo + hi + 1) >> 1;
-      if (P.boff[mid] <= t) lo = mid;
-      else hi = mid - 1;
-    }
-    const int cidx = P.busy[(long long)lo * GATHER_BLOCK + (t - P.boff[lo])];
+    const int cidx = P.dense[t];
     const int i = cidx % P.NX, j = (cidx / P.NX) % P.NY, k = cidx / (P.NX * P.NY);
     int pos[8], endp[8];
 #pragma unroll
