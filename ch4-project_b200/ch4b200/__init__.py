@@ -83,6 +83,8 @@ def lib():
         L.ch4_diagnostics.argtypes = [P, D, D, D, D]
         L.ch4_dump_averages.argtypes = [P, C.c_char_p, C.c_double, C.c_int]
         L.ch4_dump_fields_ascii.argtypes = [P, C.c_char_p, C.c_int]
+        L.ch4_particle_averages.argtypes = [P, D]
+        L.ch4_dump_particle_averages.argtypes = [P, C.c_char_p, C.c_double]
         V = C.c_void_p
         L.ch4_averages_noalloc.argtypes = [V, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                            C.c_double, V, V]
@@ -261,6 +263,19 @@ class Simulation:
         """ch4_dump_averages: the reference's dump_averages ASCII files in `directory`."""
         self._check(lib().ch4_dump_averages(self.h, str(directory).encode(), float(time_now), int(irun)),
                     "dump_averages")
+
+    def particle_averages(self):
+        """ch4_particle_averages: dump_particle_averages' means per particle type, as
+        {field: array over the cfg.particle_types types} (field "count" included)."""
+        nt = max(1, self.cfg.particle_types)
+        a = np.zeros((nt, len(abi.PART_AVG_FIELDS)))
+        self._check(lib().ch4_particle_averages(self.h, _dp(a)), "particle_averages")
+        return {f: a[:, q].copy() for q, f in enumerate(abi.PART_AVG_FIELDS)}
+
+    def dump_particle_averages(self, directory, time_now):
+        """ch4_dump_particle_averages: appends the types' lines to directory/particle_averages.dat."""
+        self._check(lib().ch4_dump_particle_averages(self.h, str(directory).encode(), float(time_now)),
+                    "dump_particle_averages")
 
     def dump_fields_ascii(self, directory, itime):
         """ch4_dump_fields_ascii: the OUTPUT_ASCII vel/temp/scal.<itime> files in `directory`."""

@@ -71,6 +71,7 @@ FLAGS = {
     "LB_FLUID_FORCING_CONSTANT_POWER": 1 << 49,
     "OUTPUT_DIAGN_APPEND": 1 << 50,
     "LAGRANGE_GRAVITY": 1 << 51,
+    "LAGRANGE_OUTPUT_FLUID_AVERAGES": 1 << 52,
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 
@@ -99,6 +100,7 @@ class Config(C.Structure):
         ("seed", C.c_uint64),
         ("resume", C.c_int),
         ("noise_u", C.c_double), ("noise_t", C.c_double),
+        ("particle_types", C.c_int),
     ]
 
 
@@ -122,6 +124,12 @@ class Particle(C.Structure):
 DIAG_FIELDS = ["x", "y", "z", "ux", "uy", "uz", "ux2", "uy2", "uz2", "rho", "rho2", "ene", "eps",
                "t", "t2", "epst", "dxt", "dyt", "dzt", "uxt", "uyt", "uzt", "nux", "nuy", "nuz", "lb",
                "s", "s2", "epss", "dxs", "dys", "dzs", "uxs", "uys", "uzs", "nusx", "nusy", "nusz"]
+
+# fields of ch4_part_avg (dump_particle_averages, per particle type), same order
+PART_AVG_FIELDS = ["count", "vx", "vy", "vz", "vx2", "vy2", "vz2", "vx4", "vy4", "vz4",
+                   "ax", "ay", "az", "ax2", "ay2", "az2", "ax4", "ay4", "az4",
+                   "t", "t2", "t4", "dt_t", "dt_t2",
+                   "ux", "uy", "uz", "ux2", "uy2", "uz2", "ux4", "uy4", "uz4"]
 
 AVERAGE_FIELDS = ["rho", "ux", "uy", "uz", "ux2", "uy2", "uz2", "ene", "eps",
                   "t", "t2", "epst", "dxt", "dyt", "dzt", "uxt", "uyt", "uzt", "nux", "nuy", "nuz",

@@ -123,7 +123,8 @@ const uint64_t SUPPORTED =
     CH4_F_TEMPERATURE_INITIAL_ADD_PERTURBATION | CH4_F_TEMPERATURE_INITIAL_ADD_NOISE | CH4_F_SCALAR_INITIAL_LINEAR |
     CH4_F_SCALAR_INITIAL_ADD_PERTURBATION | CH4_F_SCALAR_INITIAL_CONSTANT | CH4_F_SCALAR_INITIAL_CONSTANT_MEAN |
     CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
-    CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND | CH4_F_LAGRANGE_GRAVITY;
+    CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND | CH4_F_LAGRANGE_GRAVITY |
+    CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -302,6 +303,8 @@ struct EngineBase {
   virtual size_t device_bytes() const = 0;
   // after a stream synchronisation: errors the kernels recorded on the device
   virtual ch4_status check() { return CH4_OK; }
+  // Lagrangian averages per particle type, out[types][CH4_PART_AVG_FIELDS]
+  virtual ch4_status particle_averages(int types, double* out) = 0;
 };
 
 struct ch4_handle {
@@ -830,6 +833,23 @@ struct Engine : EngineBase {
     return CH4_OK;
   }
 
+  ch4_status particle_averages(int types, double* out) override {
+    if (np <= 0) return H->fail(CH4_ERR_ARG, "no particles");
+    if (types < 1) return H->fail(CH4_ERR_ARG, "particle_types must be >= 1");
+    const int nblk = (int)std::min<long long>(4 * 148, ((long long)np + 127) / 128);
+    double* d = nullptr;
+    const size_t part_n = (size_t)types * 3 * nblk * 11 * 2, out_n = (size_t)types * CH4_PART_AVG_FIELDS;
+    ch4_status st = H->cuda(cudaMalloc(&d, (part_n + out_n) * sizeof(double)), "particle averages scratch");
+    if (st) return st;
+    st = H->cuda(launch_particle_averages(pf, np, types, d, nblk, d + part_n, H->stream), "particle averages");
+    if (!st)
+      st = H->cuda(cudaMemcpyAsync(out, d + part_n, out_n * sizeof(double), cudaMemcpyDeviceToHost, H->stream),
+                   "particle averages down");
+    if (!st) st = H->cuda(cudaStreamSynchronize(H->stream), "particle averages sync");
+    cudaFree(d);
+    return st;
+  }
+
   ch4_status get_particles(ch4_particle* parts, int n) override {
     if (n > np || n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "asked for %d of %d particles", n, np);
     if (n == 0) return CH4_OK;
@@ -1337,6 +1357,7 @@ ch4_status ch4_config_default(ch4_config* cfg) {
   cfg->time_dt = 1.0;
   cfg->tau_u = cfg->tau_t = cfg->tau_s = 1.0;
   cfg->C_smag = 0.18;  // src/les.c:10
+  cfg->particle_types = 1;
   cfg->time_dt_lagr_factor = 1.0;
   cfg->seed = 1;
   return CH4_OK;
@@ -1378,7 +1399,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
     double* dst;
     bool needed;
   };
-  double NX, NY, NZ, particle_number = 0, resume = 0;
+  double NX, NY, NZ, particle_number = 0, resume = 0, tau_drag_types = 1, beta_coeff_types = 1;
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
@@ -1397,6 +1418,10 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
       {"beta_s", &cfg->beta_s, S && (fl & CH4_F_SCALAR_BUOYANCY)},
       {"time_dt_lagr_factor", &cfg->time_dt_lagr_factor, (fl & CH4_F_LAGRANGE) != 0},
       {"particle_number", &particle_number, (fl & CH4_F_LAGRANGE) != 0},
+      // particle types of the Lagrangian averages, src/parameters.c:556-586
+      {"tau_drag_types", &tau_drag_types, (fl & CH4_F_LAGRANGE) != 0},
+      {"beta_coeff_types", &beta_coeff_types,
+       (fl & CH4_F_LAGRANGE) && (fl & CH4_F_LAGRANGE_GRADIENT) && (fl & CH4_F_LAGRANGE_ADDEDMASS)},
       {"noise_u", &cfg->noise_u, (fl & CH4_F_FLUID_INITIAL_ADD_NOISE) != 0},  // src/parameters.c:216-220
       {"noise_t", &cfg->noise_t, T && (fl & CH4_F_TEMPERATURE_INITIAL_ADD_NOISE)},  // src/parameters.c:347-351
   };
@@ -1415,6 +1440,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   cfg->NZ = (int)NZ;
   cfg->particle_number = (int)particle_number;
   cfg->resume = (int)resume;
+  cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types;
   // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
   cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
   cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;
@@ -1503,6 +1529,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_FLUID_FORCING_CONSTANT_POWER", CH4_F_FORCING_CONSTANT_POWER},
       {"OUTPUT_DIAGN_APPEND", CH4_F_OUTPUT_DIAGN_APPEND},
       {"LAGRANGE_GRAVITY", CH4_F_LAGRANGE_GRAVITY},
+      {"LAGRANGE_OUTPUT_FLUID_AVERAGES", CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -1880,6 +1907,36 @@ ch4_status ch4_dump_averages(ch4_handle* h, const char* dir, double time_now, in
     const std::vector<int> fs = {DS, DS2, DEPSS, DDXS, DDYS, DDZS, DUXS, DUYS, DUZS, DNUSX, DNUSY, DNUSZ};
     if (!block("scalar_averages", fs, fs)) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
   }
+  return CH4_OK;
+}
+
+ch4_status ch4_particle_averages(ch4_handle* h, ch4_part_avg* out) {
+  if (!h || !out) return CH4_ERR_ARG;
+  if (!(h->cfg.flags & CH4_F_LAGRANGE)) return h->fail(CH4_ERR_ARG, "particle averages need LAGRANGE");
+  return h->eng->particle_averages(h->cfg.particle_types, reinterpret_cast<double*>(out));
+}
+
+// dump_particle_averages' file (src/lagrange.c:2880-2922): per type one line
+ch4_status ch4_dump_particle_averages(ch4_handle* h, const char* dir, double time_now) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  if (c.particle_types < 1) return h->fail(CH4_ERR_ARG, "particle_types must be >= 1");
+  std::vector<ch4_part_avg> a((size_t)c.particle_types);
+  ch4_status st = ch4_particle_averages(h, a.data());
+  if (st) return st;
+  FILE* f = open_in(dir, "particle_averages.dat", "a");
+  if (!f) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
+  for (int type = 0; type < c.particle_types; type++) {
+    const ch4_part_avg& o = a[(size_t)type];
+    std::fprintf(f, "%e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e ", time_now, (double)type, o.vx, o.vy,
+                 o.vz, o.vx2, o.vy2, o.vz2, o.vx4, o.vy4, o.vz4, o.ax, o.ay, o.az, o.ax2, o.ay2, o.az2, o.ax4, o.ay4,
+                 o.az4);
+    if (c.flags & CH4_F_LB_TEMPERATURE) std::fprintf(f, "%e %e %e %e %e ", o.t, o.t2, o.t4, o.dt_t, o.dt_t2);
+    if (c.flags & CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES)
+      std::fprintf(f, "%e %e %e %e %e %e %e %e %e ", o.ux, o.uy, o.uz, o.ux2, o.uy2, o.uz2, o.ux4, o.uy4, o.uz4);
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
   return CH4_OK;
 }
 

@@ -66,6 +66,11 @@ cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int*
 cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
                            cudaStream_t st);
 
+// Lagrangian averages per particle type (dump_particle_averages): partial holds
+// types * 3 * nblk * 11 * 2 doubles, out_dev receives [types][CH4_PART_AVG_FIELDS]
+cudaError_t launch_particle_averages(const double* pf, int np, int types, double* partial, int nblk, double* out_dev,
+                                     cudaStream_t st);
+
 // dump_averages sums (FP64, deterministic); out_dev receives NAVG raw sums
 cudaError_t launch_averages(const AvgParams& P, int nblocks, double* out_dev, cudaStream_t st);
 // all dump_averages terms: global sums (axis < 0: nblocks partials into partial, then

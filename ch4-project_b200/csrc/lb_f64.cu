@@ -6,6 +6,7 @@
 #include "launch.h"
 #include "lb_kernels.cuh"
 #include "lb_launch.inc"
+#include "part_avg.cuh"
 
 namespace ch4 {
 namespace {
@@ -49,6 +50,14 @@ cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape, int set,
 cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape, int set, const void* soa, double* aos, int z0,
                               int nz, cudaStream_t st) {
   return s2a_t<double, double>(P, set, soa, aos, z0, nz, st);
+}
+cudaError_t launch_particle_averages(const double* pf, int np, int types, double* partial, int nblk, double* out_dev,
+                                     cudaStream_t st) {
+  part_avg_partial_kernel<<<dim3(nblk, types, 3), PAVG_BLOCK, 0, st>>>(pf, np, types, partial);
+  cudaError_t e = cudaGetLastError();
+  if (e) return e;
+  part_avg_final_kernel<<<types, 64, 0, st>>>(partial, nblk, out_dev);
+  return cudaGetLastError();
 }
 cudaError_t launch_averages(const AvgParams& P, int nblocks, double* out_dev, cudaStream_t st) {
   averages_partial_kernel<<<nblocks, AVG_BLOCK, 0, st>>>(P);

@@ -95,6 +95,7 @@ enum {
   CH4_F_FORCING_CONSTANT_POWER = 1ull << 49,  /* src/forcing.c:1154-1190 */
   CH4_F_OUTPUT_DIAGN_APPEND = 1ull << 50,     /* ruler files appended, src/output.c:780-830 */
   CH4_F_LAGRANGE_GRAVITY = 1ull << 51,        /* -g on inertial particles, src/lagrange.c:3312-3339 */
+  CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES = 1ull << 52, /* u at the particles in particle_averages.dat */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63
@@ -143,6 +144,10 @@ typedef struct {
   int resume;
   /* amplitudes of LB_FLUID_INITIAL_ADD_NOISE / LB_TEMPERATURE_INITIAL_ADD_NOISE */
   double noise_u, noise_t;
+  /* number of particle types of the Lagrangian averages, a particle's type being
+   * (int)name % particle_types: tau_drag_types x beta_coeff_types (the latter with
+   * LAGRANGE_GRADIENT and LAGRANGE_ADDEDMASS), src/parameters.c:556-586 */
+  int particle_types;
 } ch4_config;
 
 /* One Lagrangian particle (the fields of point_particle, src/typedef.h:391-481,
@@ -247,6 +252,31 @@ ch4_status ch4_diagnostics(ch4_handle *h, ch4_diag *global, ch4_diag *ruler_x, c
  * are printed divided by `irun`, the reference's dump count (itime * time_dt /
  * time_dump_diagn, plus one with OUTPUT_AT_START). */
 ch4_status ch4_dump_averages(ch4_handle *h, const char *dir, double time_now, int irun);
+
+/* --- Lagrangian averages per particle type (dump_particle_averages) ------------ */
+
+/* Per type: the particle count, then the means of v, v^2, v^4, a, a^2, a^4 (per
+ * component), of t, t^2, t^4, dt_t, dt_t^2 (meaningful with LB_TEMPERATURE) and of the
+ * fluid velocity at the particle u, u^2, u^4 (src/lagrange.c:2598-2931). */
+#define CH4_PART_AVG_FIELDS 33
+typedef struct {
+  double count;
+  double vx, vy, vz, vx2, vy2, vz2, vx4, vy4, vz4;
+  double ax, ay, az, ax2, ay2, az2, ax4, ay4, az4;
+  double t, t2, t4, dt_t, dt_t2;
+  double ux, uy, uz, ux2, uy2, uz2, ux4, uy4, uz4;
+} ch4_part_avg;
+
+/* The averages of every particle type (out[cfg.particle_types]) at the current state.
+ * Sums in double-double on the device over a fixed order: they agree with the
+ * reference's sequential FP64 sums to rounding.  No particles: CH4_ERR_ARG. */
+ch4_status ch4_particle_averages(ch4_handle *h, ch4_part_avg *out);
+
+/* One dump of dump_particle_averages into dir/particle_averages.dat (appended): per
+ * type a line of time_now, type, the v and a means, the temperature means with
+ * LB_TEMPERATURE and the fluid-velocity means with LAGRANGE_OUTPUT_FLUID_AVERAGES, in the
+ * reference's "%e " format. */
+ch4_status ch4_dump_particle_averages(ch4_handle *h, const char *dir, double time_now);
 
 /* The OUTPUT_ASCII field dumps of dump_averages (src/output.c:1107-1200): dir/vel.<itime>
  * (x y z ux uy uz rho per cell), dir/temp.<itime> and dir/scal.<itime> (x y z value),

@@ -16,7 +16,8 @@
  *                                  initialization_forcing, src/initial_conditions.c:822)
  *   in_part.bin                    npart*SIZE_OF_POINT_PARTICLE doubles
  * out_diag.txt: every record of the final dump_averages (volume averages and the
- *   x / y / z rulers) at full precision; its *.dat files stay beside it.
+ *   x / y / z rulers) at full precision; its *.dat files stay beside it, with
+ *   particle_averages.dat of a final dump_particle_averages when LAGRANGE is on.
  * out_phi0.bin: the HIT phases right after initialization_forcing (before the
  *   first build_forcing walks them).
  * Outputs after <nsteps> steps (same layouts):
@@ -389,6 +390,10 @@ int main(int argc, char **argv) {
     for (int k = 0; k < NZ; k++) write_record(fp, "z", k, &ruler_z[k]);
     fclose(fp);
   }
+#ifdef LAGRANGE
+  /* the Lagrangian averages of the final state (appends particle_averages.dat) */
+  dump_particle_averages();
+#endif
   {
     FILE *fp = fopen("timing.json", "w");
     double sec = t_stop - t_start;

@@ -46,6 +46,9 @@ FLAGSETS = {
                   "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
     "particles_1w": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS"],
+    "particles_fa": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                     "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                     "LAGRANGE_OUTPUT_FLUID_AVERAGES"],
     "particles_g": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                     "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
                     "LAGRANGE_GRAVITY"],
@@ -98,6 +101,7 @@ def make_config(NX, NY, NZ, flags, storage=abi.STORE_F64, **kw):
     c.tau_s = 1.0
     c.C_smag = 0.18
     c.time_dt_lagr_factor = 1.0
+    c.particle_types = 1
     c.seed = 1
     for k, v in kw.items():
         setattr(c, k, v)
@@ -124,7 +128,7 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
     vals = {"resume": int(cfg.resume), "resume_u": 0, "resume_t": 0, "resume_s": 0,
             "time_start": 0.0, "time_end": float(nsteps), "time_dump_field": 1e12,
             "time_dump_diagn": 1e12, "time_dump_lagr": 1e12,
-            "tau_drag_types": 1, "tau_drag_min": 1.0, "tau_drag_max": 1.0,
+            "tau_drag_types": max(1, int(cfg.particle_types)), "tau_drag_min": 1.0, "tau_drag_max": 1.0,
             "beta_coeff_types": 1, "beta_coeff_min": 1.0, "beta_coeff_max": 1.0}
     vals.update(overrides or {})
     with open(path, "w") as f:
@@ -166,6 +170,58 @@ def particles_from_ref(arr, lay):
 
 def particles_as_dict(parts):
     return {n: np.array([getattr(p, n) for p in parts]) for n in abi.PARTICLE_FIELDS}
+
+
+def particle_averages(part, types):
+    """dump_particle_averages (src/lagrange.c:2598-2931) restated: per type
+    ((int)name % types) the count and the sums, in particle order, of v, v*v,
+    pow(v, 4.0), a, ..., t, t*t, pow(t, 4.0), dt_t, dt_t*dt_t, u, u*u, pow(u, 4.0), each
+    multiplied by 1/count.  `part`: dict of particle field -> array (particles_as_dict).
+    Returns [types][abi.PART_AVG_FIELDS] as nested lists of Python floats."""
+    import math
+    n = len(part["name"])
+    fields = abi.PART_AVG_FIELDS
+    sums = [[0.0] * len(fields) for _ in range(types)]
+    for ip in range(n):
+        ty = int(part["name"][ip]) % types
+        s = sums[ty]
+        s[0] += 1.0
+        k = 1
+        for base in ("v", "a"):
+            vals = [float(part[base + c][ip]) for c in "xyz"]
+            for x in vals:
+                s[k] += x
+                k += 1
+            for x in vals:
+                s[k] += x * x
+                k += 1
+            for x in vals:
+                s[k] += math.pow(x, 4.0)
+                k += 1
+        # without LB_TEMPERATURE the record has no t fields: those sums stay unused
+        t = float(part["t"][ip]) if "t" in part else 0.0
+        dt = float(part["dt_t"][ip]) if "dt_t" in part else 0.0
+        s[19] += t
+        s[20] += t * t
+        s[21] += math.pow(t, 4.0)
+        s[22] += dt
+        s[23] += dt * dt
+        k = 24
+        vals = [float(part["u" + c][ip]) if "u" + c in part else 0.0 for c in "xyz"]
+        for x in vals:
+            s[k] += x
+            k += 1
+        for x in vals:
+            s[k] += x * x
+            k += 1
+        for x in vals:
+            s[k] += math.pow(x, 4.0)
+            k += 1
+    out = []
+    for ty in range(types):
+        norm = 1.0 / sums[ty][0] if sums[ty][0] else float("inf")
+        out.append([sums[ty][0]] + [v * norm for v in sums[ty][1:]])
+    return out
 
 
 def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None, parts=None, params=None):
