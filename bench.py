@@ -572,14 +572,29 @@ def main():
     cfg = make_cfg(args.storage)
     p0, g0 = initial_state(1234 + rank)
     cells = NX * NY * NZ
+    # N > 1: one lattice NX x NY x (N*NZ), a z-slab of NX x NY x NZ per GPU, the slab
+    # faces exchanged over NCCL after every step (weak scaling)
+    slab_mode = world > 1
+    if slab_mode:
+        from ch4b200 import slab as slabmod
+        gcfg = make_cfg(args.storage)
+        gcfg.NZ = NZ * world
+        gcfg.SZ = float(NZ * world)
+
+    def new_sim():
+        if slab_mode:
+            s = slabmod.Slab(gcfg, rank * NZ, NZ)
+            return s.sim, (lambda n: s.step(n, rank, world))
+        s = ch4b200.Simulation(cfg)
+        return s, s.step
 
     # ---- device-resident timing --------------------------------------------
-    sim = ch4b200.Simulation(cfg)
+    sim, run = new_sim()
     sim.set_pop("p", p0)
     sim.set_pop("g", g0)
     sim.initialize()
     stream = torch.cuda.ExternalStream(sim.stream_handle)
-    sim.step(W)
+    run(W)
     sim.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -587,7 +602,7 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         ev0.record(stream)
-        sim.step(K)
+        run(K)
         ev1.record(stream)
         ev1.synchronize()
     torch.cuda.synchronize()
@@ -609,12 +624,15 @@ def main():
     e2e = None
     if not args.no_e2e:
         torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
         t0 = time.perf_counter()
-        with ch4b200.Simulation(cfg) as s2:
+        s2, run2 = new_sim()
+        with s2:
             s2.set_pop("p", p0)
             s2.set_pop("g", g0)
             s2.initialize()
-            s2.step(K)
+            run2(K)
             f2 = s2.fields()
         t1 = time.perf_counter()
         sec = t1 - t0
@@ -639,17 +657,18 @@ def main():
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"f32": "f32", "f16": "f32 (f16 storage)", "f64": "f64"}[args.storage], "data": "synthetic",
-            "config": {"workload": WORKLOAD, "lattice": [NX, NY, NZ], "Ra": RA, "Pr": PR,
+            "config": {"workload": WORKLOAD, "lattice": [NX, NY, NZ * world], "lattice_per_gpu": [NX, NY, NZ],
+                       "Ra": RA, "Pr": PR,
                        "storage": args.storage, "l2": "inputs larger than L2 (%.2f GB of populations)" %
                        (2 * 19 * cells * {"f64": 8, "f32": 4, "f16": 2}[args.storage] / 1e9),
-                       "parallelism": "replicas%d" % world},
+                       "parallelism": "zslab%d" % world if slab_mode else "single"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": ncu_traffic(args.storage),
                          "bytes_per_cell": BYTES_PER_CELL[args.storage], "kernel": "lb_step_kernel"},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": K,
+            "gpu_launches": K * (3 if slab_mode else 1),  # lb_step (+ halo pack and unpack per step)
             "clocks": clk.summary(),
             "finite": finite,
         }

@@ -101,6 +101,7 @@ class Config(C.Structure):
         ("resume", C.c_int),
         ("noise_u", C.c_double), ("noise_t", C.c_double),
         ("particle_types", C.c_int),
+        ("nz_global", C.c_int), ("z_offset", C.c_int),
     ]
 
 

@@ -1,0 +1,128 @@
+"""One lattice as z-slabs, one handle per GPU (ch4_halo_pack / ch4_halo_unpack).
+
+Each slab holds NZ_local planes of a lattice NZ planes deep (ch4_config.nz_global,
+z_offset).  Its step streams the populations leaving through the z faces periodically
+onto its own opposite face; after every step the slabs swap those values: every slab
+sends the 5 c_z = -1 directions of its top plane to the slab below and the 5 c_z = +1
+directions of its bottom plane to the slab above (SZ * NX*NY values per set and
+face), and writes what it receives into the same places.  The x and y directions,
+y walls and forcing are plane-local, so the decomposition reproduces the single
+lattice bit for bit (HIT tables run over the whole lattice's z).
+
+The transfer is the caller's plumbing: `exchange` pairs the four point-to-point
+transfers of one step over a torch.distributed process group (NCCL between GPUs,
+gloo on CPU); `step_local` runs several slabs of one process, each unpacking straight
+from its neighbours' send buffers.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import Simulation, lib
+from . import abi
+
+
+def bounds(nz, nslabs):
+    """(z_offset, planes) of each slab: an even split, the first nz % nslabs one plane deeper."""
+    if not 1 <= nslabs <= nz:
+        raise ValueError("need 1 <= slabs <= NZ")
+    q, r = divmod(nz, nslabs)
+    out, z = [], 0
+    for i in range(nslabs):
+        n = q + (1 if i < r else 0)
+        out.append((z, n))
+        z += n
+    return out
+
+
+def slab_config(cfg, z0, nz):
+    """The configuration of planes z0 .. z0+nz-1 of the whole-lattice configuration cfg."""
+    c = abi.Config()
+    C.pointer(c)[0] = cfg
+    c.nz_global = cfg.NZ
+    c.z_offset = z0
+    c.NZ = nz
+    return c
+
+
+def neighbours(rank, world):
+    """(below, above): the ranks holding the slabs under and over this one (periodic in z)."""
+    return (rank - 1) % world, (rank + 1) % world
+
+
+def exchange(send_down, send_up, recv_up, recv_down, rank, world, group=None):
+    """One step's face exchange over torch.distributed: send_down -> the slab below (its
+    recv_up), send_up -> the slab above (its recv_down).  With one rank the slab is its
+    own neighbour (the periodic lattice).  The four transfers are issued as one batch in
+    the same order on every rank, so a pair of ranks that are each other's neighbour on
+    both sides (two slabs) still matches them one to one."""
+    import torch.distributed as dist
+    if world == 1:
+        recv_up.copy_(send_down)
+        recv_down.copy_(send_up)
+        return
+    below, above = neighbours(rank, world)
+    ops = [dist.P2POp(dist.isend, send_down, below, group), dist.P2POp(dist.irecv, recv_up, above, group),
+           dist.P2POp(dist.isend, send_up, above, group), dist.P2POp(dist.irecv, recv_down, below, group)]
+    for w in dist.batch_isend_irecv(ops):
+        w.wait()
+
+
+class Slab:
+    """A Simulation holding planes z0 .. z0+nz-1 of the lattice `cfg`, with its four
+    face buffers as device tensors."""
+
+    def __init__(self, cfg, z0, nz, device=None):
+        import torch
+        self.z0, self.nz = z0, nz
+        self.sim = Simulation(slab_config(cfg, z0, nz))
+        n = C.c_size_t()
+        self.sim._check(lib().ch4_halo_bytes(self.sim.h, C.byref(n)), "halo_bytes")
+        dev = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.send_down, self.send_up, self.recv_up, self.recv_down = (
+            torch.empty(n.value, dtype=torch.uint8, device=dev) for _ in range(4))
+
+    def set_pop(self, which, aos_whole):
+        """Populations of the whole lattice, AoS [NZ][NY][NX][19]: this slab's planes."""
+        self.sim.set_pop(which, np.ascontiguousarray(aos_whole[self.z0:self.z0 + self.nz]))
+
+    def pack(self):
+        self.sim._check(lib().ch4_halo_pack(self.sim.h, C.c_void_p(self.send_down.data_ptr()),
+                                            C.c_void_p(self.send_up.data_ptr())), "halo_pack")
+
+    def unpack(self, from_up=None, from_down=None):
+        fu = self.recv_up if from_up is None else from_up
+        fd = self.recv_down if from_down is None else from_down
+        self.sim._check(lib().ch4_halo_unpack(self.sim.h, C.c_void_p(fu.data_ptr()), C.c_void_p(fd.data_ptr())),
+                        "halo_unpack")
+
+    def step(self, n, rank, world, group=None):
+        """n steps of a slab of a multi-rank lattice: step, pack, exchange on the
+        handle's stream, unpack."""
+        import torch
+        stream = torch.cuda.ExternalStream(self.sim.stream_handle)
+        for _ in range(n):
+            self.sim.step(1)
+            self.pack()
+            with torch.cuda.stream(stream):
+                exchange(self.send_down, self.send_up, self.recv_up, self.recv_down, rank, world, group)
+            self.unpack()
+
+    def close(self):
+        self.sim.close()
+
+
+def step_local(slabs, n):
+    """n steps of the slabs of one process (in z order): every slab unpacks straight
+    from its neighbours' send buffers once all have packed."""
+    m = len(slabs)
+    for _ in range(n):
+        for s in slabs:
+            s.sim.step(1)
+            s.pack()
+        for s in slabs:
+            s.sim.synchronize()
+        for i, s in enumerate(slabs):
+            s.unpack(from_up=slabs[(i + 1) % m].send_down, from_down=slabs[(i - 1) % m].send_up)
+        for s in slabs:
+            s.sim.synchronize()

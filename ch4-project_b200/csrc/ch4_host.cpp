@@ -305,6 +305,10 @@ struct EngineBase {
   virtual ch4_status check() { return CH4_OK; }
   // Lagrangian averages per particle type, out[types][CH4_PART_AVG_FIELDS]
   virtual ch4_status particle_averages(int types, double* out) = 0;
+  // z-slab faces: bytes of one face buffer; pack (a = send_down, b = send_up) or unpack
+  // (a = from_up, b = from_down)
+  virtual size_t halo_bytes() const = 0;
+  virtual ch4_status halo(bool pack, void* a, void* b) = 0;
 };
 
 struct ch4_handle {
@@ -361,14 +365,16 @@ struct ch4_handle {
       }
   }
   // sin tables of src/forcing.c:582-584 for the current phases
+  // planes of the whole lattice along z (a z-slab handle holds NZ of them)
+  int nz_all() const { return cfg.nz_global > 0 ? cfg.nz_global : cfg.NZ; }
   void hit_tables(double* tab) const {
     const double LX = cfg.SX, LY = cfg.SY, LZ = cfg.SZ;
-    const int L = cfg.NX + cfg.NY + cfg.NZ;
+    const int NZg = nz_all(), L = cfg.NX + cfg.NY + NZg;
     for (int ii = 0; ii < NK; ii++) {
       double *ax = tab + ii * L, *ay = ax + cfg.NX, *az = ay + cfg.NY;
       for (int i = 0; i < cfg.NX; i++) ax[i] = std::sin(2 * 3.14159265359 * (VK[ii][0] * ((double)i + 0.5) / LX + phi[ii][0]));
       for (int j = 0; j < cfg.NY; j++) ay[j] = std::sin(2 * 3.14159265359 * (VK[ii][1] * ((double)j + 0.5) / LY + phi[ii][1]));
-      for (int k = 0; k < cfg.NZ; k++) az[k] = std::sin(2 * 3.14159265359 * (VK[ii][2] * ((double)k + 0.5) / LZ + phi[ii][2]));
+      for (int k = 0; k < NZg; k++) az[k] = std::sin(2 * 3.14159265359 * (VK[ii][2] * ((double)k + 0.5) / LZ + phi[ii][2]));
     }
   }
 };
@@ -418,6 +424,8 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.NY = c.NY;
   P.NZ = c.NZ;
   P.N = N;
+  P.zoff = c.nz_global > 0 ? c.z_offset : 0;
+  P.Lhit = c.NX + c.NY + (c.nz_global > 0 ? c.nz_global : c.NZ);
   uint32_t F = 0;
   const uint64_t fl = c.flags;
   if (fl & CH4_F_LB_FLUID_FORCING) {
@@ -833,6 +841,50 @@ struct Engine : EngineBase {
     return CH4_OK;
   }
 
+  size_t halo_bytes() const override {
+    int ns = 0;
+    for (int s = 0; s < 3; s++) ns += nsets_on[s];
+    return (size_t)ns * 5 * c.NX * c.NY * sbytes;
+  }
+
+  // The 5 directions leaving through the bottom (c_z = -1) and the top (c_z = +1).  On
+  // a wall row a direction pointing away from the wall (c_y = -1 on the top row, +1 on
+  // the bottom row) has no source row: the cell's own wall rule writes it (bounce-back,
+  // or the fixed-value rule of a temperature/scalar wall), not a stream from across the
+  // face, so that row stays out of the exchange (a slip wall streams it: exchanged).
+  ch4_status halo(bool pack, void* a, void* b) override {
+    const size_t row = (size_t)c.NX * sbytes, plane = row * c.NY, top = (size_t)(c.NZ - 1) * plane;
+    const uint32_t F = P.feat;
+    const bool local_top[3] = {(F & K_FWALL) && !(F & K_FSLIP_P), (F & K_TWALL) != 0, (F & K_SWALL) != 0};
+    const bool local_bot[3] = {(F & K_FWALL) && !(F & K_FSLIP_M), (F & K_TWALL) != 0, (F & K_SWALL) != 0};
+    HaloCopy hc{};
+    int slot = 0;
+    for (int s = 0; s < 3; s++) {
+      if (!nsets_on[s]) continue;
+      char* base = static_cast<char*>(f[s][cur]);
+      int kd = 0, ku = 0;
+      for (int q = 0; q < NPOP; q++) {
+        if (cz(q) == 0) continue;
+        char* qplane = base + (size_t)q * N * sbytes;
+        // c_z = -1: the top plane holds the values sent down; c_z = +1: the bottom plane those sent up
+        char* face = cz(q) < 0 ? qplane + top : qplane;
+        char* buf = static_cast<char*>(cz(q) < 0 ? a : b) + ((size_t)slot * 5 + (cz(q) < 0 ? kd++ : ku++)) * plane;
+        size_t off = 0, bytes = plane;
+        if (cy(q) < 0 && local_top[s]) bytes -= row;  // rows 0 .. NY-2
+        if (cy(q) > 0 && local_bot[s]) {              // rows 1 .. NY-1
+          off = row;
+          bytes -= row;
+        }
+        hc.src[hc.n] = (pack ? face : buf) + off;
+        hc.dst[hc.n] = (pack ? buf : face) + off;
+        hc.bytes[hc.n] = bytes;
+        hc.n++;
+      }
+      slot++;
+    }
+    return H->cuda(launch_halo_copy(hc, H->stream), pack ? "halo pack" : "halo unpack");
+  }
+
   ch4_status particle_averages(int types, double* out) override {
     if (np <= 0) return H->fail(CH4_ERR_ARG, "no particles");
     if (types < 1) return H->fail(CH4_ERR_ARG, "particle_types must be >= 1");
@@ -871,7 +923,7 @@ struct Engine : EngineBase {
     return CH4_OK;
   }
 
-  int L() const { return c.NX + c.NY + c.NZ; }
+  int L() const { return c.NX + c.NY + H->nz_all(); }  // HIT table row: the whole lattice's z
 
   size_t device_bytes() const override {
     size_t b = 0;
@@ -1105,7 +1157,7 @@ struct Engine : EngineBase {
       for (size_t i = 0; i < t.size(); i++) dst_h[i] = (A)t[i];
       return;
     }
-    const int NX = c.NX, NY = c.NY, NZ = c.NZ, Ln = L();
+    const int NX = c.NX, NY = c.NY, NZ = H->nz_all(), Ln = L();
     const double amp[3] = {c.Amp_x, c.Amp_y, c.Amp_z};
     auto fold = [&](int comp, int axis, int i) {  // sum over modes of amp_comp * table_axis(i)
       const int off = axis == 0 ? 0 : axis == 1 ? NX : NX + NY;
@@ -1593,8 +1645,17 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
   if (c->NY > 65535 || c->NZ > 65535) return why = "NY and NZ must be <= 65535 (launch grid)", CH4_ERR_ARG;
   if (c->flags & ~SUPPORTED) return why = "flag outside the implemented hot path", CH4_ERR_UNSUPPORTED;
   if (c->storage < 0 || c->storage > 2) return why = "unknown storage", CH4_ERR_ARG;
-  if (c->time_dt != 1.0 || c->SX != c->NX || c->SY != c->NY || c->SZ != c->NZ)
+  const int nz_all = c->nz_global > 0 ? c->nz_global : c->NZ;
+  if (c->time_dt != 1.0 || c->SX != c->NX || c->SY != c->NY || c->SZ != nz_all)
     return why = "streaming requires time_dt = 1 and S = N (src/parameters.c:135)", CH4_ERR_UNSUPPORTED;
+  if (c->nz_global > 0) {
+    if (c->z_offset < 0 || c->z_offset + c->NZ > c->nz_global) return why = "z-slab outside the lattice", CH4_ERR_ARG;
+    if (c->nz_global > 65535) return why = "nz_global must be <= 65535", CH4_ERR_ARG;
+    // z-slabs exchange populations only: no z-halo of u (LES), no global sums inside
+    // the step (force corrections), no particle migration
+    if (c->flags & (CH4_F_FLUID_LES | CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_LAGRANGE))
+      return why = "z-slab handles run without LES, global force corrections and particles", CH4_ERR_UNSUPPORTED;
+  }
   if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
     return why = "walls need NY >= 3", CH4_ERR_ARG;
   if (!(c->tau_u > 0.5)) return why = "tau_u must exceed 0.5", CH4_ERR_ARG;
@@ -1726,6 +1787,9 @@ static void draw_phases(unsigned short rng[3], double phi[NK][3]) {
 ch4_status ch4_initial_populations(const ch4_config* cfg, double* p, double* g, double* hs, double* phi) {
   if (!cfg || cfg->NX < 1 || cfg->NY < 1 || cfg->NZ < 1) return CH4_ERR_ARG;
   if (cfg->flags & CH4_F_INITIAL_OTHER) return CH4_ERR_UNSUPPORTED;
+  // the drand48 draws run over the whole lattice: build it with a whole-lattice
+  // configuration and give each z-slab its planes
+  if (cfg->nz_global > 0) return CH4_ERR_UNSUPPORTED;
   unsigned short rng[3];
   seed48_state(cfg->seed, rng);
   static const Lattice lat;
@@ -1743,6 +1807,8 @@ ch4_status ch4_initial_conditions(ch4_handle* h) {
   if (!h) return CH4_ERR_ARG;
   if (h->initialized) return h->fail(CH4_ERR_STATE, "ch4_initial_conditions after ch4_initialize");
   const ch4_config& c = h->cfg;
+  if (c.nz_global > 0)
+    return h->fail(CH4_ERR_UNSUPPORTED, "a z-slab takes its planes of the whole lattice's initial state (ch4_set_pop)");
   if (c.flags & CH4_F_INITIAL_OTHER)
     return h->fail(CH4_ERR_UNSUPPORTED, "define.h asks for an initial state the library does not build");
   const size_t n = (size_t)c.NX * c.NY * c.NZ * NPOP;
@@ -1908,6 +1974,22 @@ ch4_status ch4_dump_averages(ch4_handle* h, const char* dir, double time_now, in
     if (!block("scalar_averages", fs, fs)) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
   }
   return CH4_OK;
+}
+
+ch4_status ch4_halo_bytes(ch4_handle* h, size_t* bytes) {
+  if (!h || !bytes) return CH4_ERR_ARG;
+  *bytes = h->eng->halo_bytes();
+  return CH4_OK;
+}
+
+ch4_status ch4_halo_pack(ch4_handle* h, void* send_down, void* send_up) {
+  if (!h || !send_down || !send_up) return CH4_ERR_ARG;
+  return h->eng->halo(true, send_down, send_up);
+}
+
+ch4_status ch4_halo_unpack(ch4_handle* h, const void* from_up, const void* from_down) {
+  if (!h || !from_up || !from_down) return CH4_ERR_ARG;
+  return h->eng->halo(false, const_cast<void*>(from_up), const_cast<void*>(from_down));
 }
 
 ch4_status ch4_particle_averages(ch4_handle* h, ch4_part_avg* out) {

@@ -62,6 +62,8 @@ template <typename A>
 struct StepParams {
   int NX, NY, NZ;
   long long N;  // cells
+  int zoff;     // global z of plane 0 (z-slab of a larger lattice), else 0
+  int Lhit;     // NX + NY + global NZ: length of one HIT table row
   uint32_t feat;
   // populations (storage type erased; cast in the kernel)
   const void* fin[3];

@@ -47,6 +47,16 @@ cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape s, int se
                               int nz, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
                               int nz, cudaStream_t st);
+// copies of up to 30 device regions (z-slab face exchange), in 4-byte words when every
+// region's size and addresses allow it, else in 2-byte words
+struct HaloCopy {
+  const void* src[30];
+  void* dst[30];
+  size_t bytes[30];
+  int n;
+};
+cudaError_t launch_halo_copy(const HaloCopy& H, cudaStream_t st);
+
 // vec[3 i + a] = planes[a n + i], a = 0..2 (planar vector field -> interleaved)
 cudaError_t launch_interleave3(const double* planes, double* vec, long long n, cudaStream_t st);
 

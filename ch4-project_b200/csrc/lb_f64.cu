@@ -20,6 +20,31 @@ __global__ void interleave3_kernel(const double* __restrict__ planes, double* __
 }
 }  // namespace
 
+template <typename W>
+__global__ void halo_copy_kernel(const HaloCopy H) {
+  const W* s = static_cast<const W*>(H.src[blockIdx.y]);
+  W* d = static_cast<W*>(H.dst[blockIdx.y]);
+  const size_t n = H.bytes[blockIdx.y] / sizeof(W);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) d[i] = s[i];
+}
+
+cudaError_t launch_halo_copy(const HaloCopy& H, cudaStream_t st) {
+  if (H.n <= 0) return cudaSuccess;
+  bool w4 = true;
+  size_t most = 0;
+  for (int r = 0; r < H.n; r++) {
+    w4 = w4 && H.bytes[r] % 4 == 0 && reinterpret_cast<uintptr_t>(H.src[r]) % 4 == 0 &&
+         reinterpret_cast<uintptr_t>(H.dst[r]) % 4 == 0;
+    most = std::max(most, H.bytes[r]);
+  }
+  const size_t words = most / (w4 ? 4 : 2);
+  if (words == 0) return cudaSuccess;
+  const unsigned bx = (unsigned)std::min<size_t>(64, (words + 255) / 256);
+  if (w4) halo_copy_kernel<uint32_t><<<dim3(bx, H.n), 256, 0, st>>>(H);
+  else halo_copy_kernel<uint16_t><<<dim3(bx, H.n), 256, 0, st>>>(H);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_interleave3(const double* planes, double* vec, long long n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   interleave3_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(planes, vec, n);

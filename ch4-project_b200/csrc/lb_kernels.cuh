@@ -95,17 +95,18 @@ __device__ __forceinline__ void cell_force(const StepParams<A>& P, int x, int y,
     fz += P.kol[P.NY + P.NX + y];
   }
   if (F & K_HIT) {
-    const int L = P.NX + P.NY + P.NZ;
+    const int L = P.Lhit;
+    const int zg = z + P.zoff;  // tables run over the whole lattice's z
     if constexpr (sizeof(A) == 4) {
       // FP32 form: the mode sums folded per axis on the host (Engine::tables_to),
       // F_x = Sxy[y] + Sxz[z], F_y = Syx[x] + Syz[z], F_z = Szy[y] + Szx[x]
-      fx += hit[P.NX + y] + hit[P.NX + P.NY + z];
-      fy += hit[x] + hit[L + P.NX + P.NY + z];
+      fx += hit[P.NX + y] + hit[P.NX + P.NY + zg];
+      fy += hit[x] + hit[L + P.NX + P.NY + zg];
       fz += hit[L + P.NX + y] + hit[L + x];
     } else
 #pragma unroll
     for (int ii = 0; ii < NK; ii++) {
-      const A ax = hit[ii * L + x], ay = hit[ii * L + P.NX + y], az = hit[ii * L + P.NX + P.NY + z];
+      const A ax = hit[ii * L + x], ay = hit[ii * L + P.NX + y], az = hit[ii * L + P.NX + P.NY + zg];
       fx += P.hitamp[ii][0] * (ay + az);
       fy += P.hitamp[ii][1] * (ax + az);
       fz += P.hitamp[ii][2] * (ay + ax);

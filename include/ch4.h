@@ -148,6 +148,11 @@ typedef struct {
    * (int)name % particle_types: tau_drag_types x beta_coeff_types (the latter with
    * LAGRANGE_GRADIENT and LAGRANGE_ADDEDMASS), src/parameters.c:556-586 */
   int particle_types;
+  /* z-slab of a larger lattice (the multi-GPU decomposition): this handle holds planes
+   * z_offset .. z_offset + NZ - 1 of a lattice nz_global planes deep (SZ = nz_global),
+   * and the caller exchanges the populations crossing the slab faces after every step
+   * (ch4_halo_pack / ch4_halo_unpack).  nz_global = 0: the handle is the whole lattice. */
+  int nz_global, z_offset;
 } ch4_config;
 
 /* One Lagrangian particle (the fields of point_particle, src/typedef.h:391-481,
@@ -252,6 +257,24 @@ ch4_status ch4_diagnostics(ch4_handle *h, ch4_diag *global, ch4_diag *ruler_x, c
  * are printed divided by `irun`, the reference's dump count (itime * time_dt /
  * time_dump_diagn, plus one with OUTPUT_AT_START). */
 ch4_status ch4_dump_averages(ch4_handle *h, const char *dir, double time_now, int irun);
+
+/* --- z-slab decomposition (one handle per GPU, slabs stacked along z) ----------- */
+
+/* Bytes of one face buffer: per enabled population set the 5 directions with c_z = -1
+ * (or +1), one NX*NY plane each, in the stored type. */
+ch4_status ch4_halo_bytes(ch4_handle *h, size_t *bytes);
+
+/* After ch4_step(h, 1).  The step streams the populations that leave the slab
+ * periodically onto its own opposite face, so after it the top plane holds, in its
+ * c_z = -1 directions, what this slab sends to the slab below, and the bottom plane, in
+ * its c_z = +1 directions, what it sends to the slab above.  pack copies them into the
+ * device buffers send_down / send_up; unpack writes what the slab above sent down into
+ * the top plane and what the slab below sent up into the bottom plane.  Both run on the
+ * handle's stream (the caller's transfer between them must be ordered on it, e.g. NCCL
+ * on that stream).  With one slab, from_up = send_down and from_down = send_up give the
+ * periodic lattice back. */
+ch4_status ch4_halo_pack(ch4_handle *h, void *send_down, void *send_up);
+ch4_status ch4_halo_unpack(ch4_handle *h, const void *from_up, const void *from_down);
 
 /* --- Lagrangian averages per particle type (dump_particle_averages) ------------ */
 

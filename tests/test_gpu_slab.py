@@ -1,0 +1,75 @@
+"""z-slab decomposition (ch4_halo_pack / ch4_halo_unpack, ch4b200.slab) on one GPU:
+the lattice cut into slabs along z, each a handle of its own, exchanging the face
+populations after every step, reproduces the single-lattice run bit for bit (FP64 and
+FP32: every cell does the same arithmetic; HIT tables run over the whole lattice's z).
+The slabs of one process unpack straight from their neighbours' send buffers; the
+multi-rank exchange over torch.distributed is covered on CPU (tests/test_slab_exchange.py).
+"""
+import numpy as np
+import pytest
+
+from lbcases import make_case, pop_items
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import ch4b200  # noqa: E402
+from ch4b200 import slab  # noqa: E402
+
+
+def whole(cfg, state, nsteps):
+    with ch4b200.Simulation(cfg) as sim:
+        for k, v in pop_items(state):
+            sim.set_pop(k, v)
+        sim.initialize()
+        sim.step(nsteps)
+        out = {k: sim.get_pop(k) for k, _ in pop_items(state)}
+        out.update(sim.fields())
+    return out
+
+
+def slabbed(cfg, state, nsteps, nslabs):
+    slabs = [slab.Slab(cfg, z0, nz) for z0, nz in slab.bounds(cfg.NZ, nslabs)]
+    try:
+        for s in slabs:
+            for k, v in pop_items(state):
+                s.set_pop(k, v)
+            s.sim.initialize()
+        slab.step_local(slabs, nsteps)
+        out = {k: np.concatenate([s.sim.get_pop(k) for s in slabs]) for k, _ in pop_items(state)}
+        f = [s.sim.fields() for s in slabs]
+        out.update({k: np.concatenate([x[k] for x in f]) for k in f[0]})
+    finally:
+        for s in slabs:
+            s.close()
+    return out
+
+
+@pytest.mark.parametrize("name,storage,nslabs", [("rb", 0, 2), ("hit", 0, 3), ("kolmogorov", 0, 2),
+                                                 ("scalar", 0, 3), ("rb", 1, 3), ("hit", 1, 2), ("walls2", 0, 2)])
+def test_slabs_reproduce_the_single_lattice(name, storage, nslabs):
+    _, cfg, state = make_case(name, seed=41, storage=storage)
+    nsteps = 9
+    a = whole(cfg, state, nsteps)
+    b = slabbed(cfg, state, nsteps, nslabs)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_one_rank_exchange_is_the_periodic_lattice():
+    """Slab.step with world = 1: the exchange hands each face back to the same slab."""
+    _, cfg, state = make_case("hit", seed=42)
+    a = whole(cfg, state, 6)
+    s = slab.Slab(cfg, 0, cfg.NZ)
+    try:
+        for k, v in pop_items(state):
+            s.set_pop(k, v)
+        s.sim.initialize()
+        s.step(6, 0, 1)
+        for k, _ in pop_items(state):
+            assert np.array_equal(s.sim.get_pop(k), a[k]), k
+    finally:
+        s.close()
