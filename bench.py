@@ -532,6 +532,7 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "f16", "f64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--zslab", action="store_true", help="run the z-slab path (face exchange every step) at N = 1 too")
     ap.add_argument("--lattice", default=None, help="NX,NY,NZ override (profiling runs on a smaller case)")
     ap.add_argument("--workload", default="rb", choices=["rb", "ensemble", "serve", "hit_particles"])
     ap.add_argument("--cases", type=int, default=512)
@@ -574,7 +575,7 @@ def main():
     cells = NX * NY * NZ
     # N > 1: one lattice NX x NY x (N*NZ), a z-slab of NX x NY x NZ per GPU, the slab
     # faces exchanged over NCCL after every step (weak scaling)
-    slab_mode = world > 1
+    slab_mode = world > 1 or args.zslab
     if slab_mode:
         from ch4b200 import slab as slabmod
         gcfg = make_cfg(args.storage)
