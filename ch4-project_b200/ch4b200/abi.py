@@ -72,6 +72,7 @@ FLAGS = {
     "OUTPUT_DIAGN_APPEND": 1 << 50,
     "LAGRANGE_GRAVITY": 1 << 51,
     "LAGRANGE_OUTPUT_FLUID_AVERAGES": 1 << 52,
+    "METHOD_TRT": 1 << 53,
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 

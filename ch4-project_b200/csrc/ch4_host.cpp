@@ -124,7 +124,7 @@ const uint64_t SUPPORTED =
     CH4_F_SCALAR_INITIAL_ADD_PERTURBATION | CH4_F_SCALAR_INITIAL_CONSTANT | CH4_F_SCALAR_INITIAL_CONSTANT_MEAN |
     CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
     CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND | CH4_F_LAGRANGE_GRAVITY |
-    CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES;
+    CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES | CH4_F_METHOD_TRT;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -449,11 +449,16 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   if (fl & CH4_F_TEMPERATURE_BC_Y_M_NOFLUX) F |= K_TNOFLUX_M;
   if (fl & CH4_F_SCALAR_BC_Y) F |= K_SWALL;
   if (fl & CH4_F_FLUID_LES) F |= K_LES;
+  if (fl & CH4_F_METHOD_TRT) F |= K_TRT;
   P.feat = F;
   P.fm_prev = P.fm_cur = nullptr;
   for (int q = 0; q < NPOP; q++) P.w[q] = (A)lat.w[q];
   const double invtau = 1.0 / c.tau_u;
-  const double fac = (1.0 - 0.5 * c.time_dt * invtau);  // src/forcing.c:1289
+  // METHOD_TRT: the antisymmetric rate of src/fluid.c:1141-1143 (magic gamma 1/4); the
+  // Guo prefactor then uses it (src/forcing.c:1279-1284)
+  auto trt_minus = [](double w) { return (4. - 2. * w) / (2. + (4. * 0.25 - 1.) * w); };
+  const bool trt = (fl & CH4_F_METHOD_TRT) != 0;
+  const double fac = (1.0 - 0.5 * c.time_dt * (trt ? trt_minus(invtau) : invtau));  // src/forcing.c:1289
   for (int q = 0; q < NPOP; q++) P.facw[q] = (A)(fac * lat.w[q]);
   P.gfac = (A)fac;
   P.invcs2 = (A)lat.invcs2;
@@ -463,6 +468,9 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.invtau[0] = (A)invtau;
   P.invtau[1] = (A)(nsets_on[1] ? 1.0 / c.tau_t : 0.0);
   P.invtau[2] = (A)(nsets_on[2] ? 1.0 / c.tau_s : 0.0);
+  P.invtau_m[0] = (A)trt_minus(invtau);
+  P.invtau_m[1] = (A)(nsets_on[1] ? trt_minus(1.0 / c.tau_t) : 0.0);
+  P.invtau_m[2] = (A)(nsets_on[2] ? trt_minus(1.0 / c.tau_s) : 0.0);
   P.hdt = (A)(0.5 * c.time_dt);
   P.nu = (A)c.nu;
   P.csmag2 = (A)std::pow(c.C_smag * 1.0, 2.0);
@@ -1582,6 +1590,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"OUTPUT_DIAGN_APPEND", CH4_F_OUTPUT_DIAGN_APPEND},
       {"LAGRANGE_GRAVITY", CH4_F_LAGRANGE_GRAVITY},
       {"LAGRANGE_OUTPUT_FLUID_AVERAGES", CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES},
+      {"METHOD_TRT", CH4_F_METHOD_TRT},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2370,9 +2379,11 @@ ch4_status ch4_ensemble_add(ch4_ensemble* E, const ch4_config* cfg, int* slot) {
   ch4_status st = validate(cfg, why);
   if (st) return E->fail(st, "%s", why.c_str());
   if (cfg->flags & (CH4_F_FORCING_HIT | CH4_F_FLUID_LES | CH4_F_LAGRANGE | CH4_F_FORCING_NOZEROMODE |
-                    CH4_F_FORCING_CONSTANT_POWER))
+                    CH4_F_FORCING_CONSTANT_POWER | CH4_F_METHOD_TRT) ||
+      cfg->nz_global > 0)
     return E->fail(CH4_ERR_UNSUPPORTED,
-                   "ensemble slots run without HIT forcing, LES, particles or global force corrections");
+                   "ensemble slots run without HIT forcing, LES, particles, global force corrections, TRT "
+                   "or z-slabs");
   LaunchShape sh{(cfg->flags & CH4_F_LB_TEMPERATURE) != 0, (cfg->flags & CH4_F_LB_SCALAR) != 0, E->storage};
   bool any = false;
   for (auto& s : E->slots) any |= s.used;

@@ -55,7 +55,8 @@ enum : uint32_t {
   K_BETA2 = 1u << 17,
   K_TSRC = 1u << 18,
   K_NOZERO = 1u << 19,  // LB_FLUID_FORCING_NOZEROMODE: subtract the mean force
-  K_CPOWER = 1u << 20   // LB_FLUID_FORCING_CONSTANT_POWER: scale to a fixed mean power
+  K_CPOWER = 1u << 20,  // LB_FLUID_FORCING_CONSTANT_POWER: scale to a fixed mean power
+  K_TRT = 1u << 21      // METHOD_TRT: two-relaxation-time collision
 };
 
 template <typename A>
@@ -91,6 +92,7 @@ struct StepParams {
   A gfac;     // 1 - dt/(2 tau_u)
   A invcs2, invcs4, invtwocs2, invtwocs4;
   A invtau[3];
+  A invtau_m[3];  // METHOD_TRT: (4 - 2/tau) / (2 + (4 gamma - 1)/tau), gamma = 1/4, per set
   A hdt;  // 0.5*time_dt
   A nu, csmag2;  // LES: nu and pow(C_smag*1, 2)
   // storage shift (rho0 for p, T0 for g, S0 for h) used by the F16 codec

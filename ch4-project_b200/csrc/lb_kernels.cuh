@@ -48,12 +48,40 @@ __device__ __forceinline__ A cdot(A ux, A uy, A uz) {
   return r;
 }
 
+// cdot<q> for a q known only after unrolling (constant-folds the same way)
+template <typename A>
+__device__ __forceinline__ A cdot_rt(int q, A ux, A uy, A uz) {
+  const int a = cx(q), b = cy(q), c = cz(q);
+  A r = A(0);
+  bool have = false;
+  if (a != 0) {
+    r = a > 0 ? ux : -ux;
+    have = true;
+  }
+  if (b != 0) {
+    const A t = b > 0 ? uy : -uy;
+    r = have ? r + t : t;
+    have = true;
+  }
+  if (c != 0) {
+    const A t = c > 0 ? uz : -uz;
+    r = have ? r + t : t;
+  }
+  return r;
+}
+
 // (c - u) * invcs2 + c * cu * invcs4 for one component (src/forcing.c:1427-1429)
 template <int cc, typename A>
 __device__ __forceinline__ A guo_d(A u, A cu, A invcs2, A invcs4) {
   if constexpr (cc == 0) return (-u) * invcs2;
   else if constexpr (cc > 0) return (A(1) - u) * invcs2 + cu * invcs4;
   else return (A(-1) - u) * invcs2 + (-cu) * invcs4;
+}
+template <typename A>
+__device__ __forceinline__ A guo_d_rt(int cc, A u, A cu, A invcs2, A invcs4) {
+  if (cc == 0) return (-u) * invcs2;
+  if (cc > 0) return (A(1) - u) * invcs2 + cu * invcs4;
+  return (A(-1) - u) * invcs2 + (-cu) * invcs4;
 }
 
 // m(), mvx(), mvy(), mvz() of src/typedef.h:286-291, fixed left-to-right order

@@ -177,8 +177,70 @@ __device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellSt
   }
 }
 
+// Two-relaxation-time collision of METHOD_TRT (src/fluid.c:1140-1160) of one set, in
+// place: per direction the symmetric part (f_q + f_-q)/2 relaxes towards that of the
+// equilibrium with wm, the antisymmetric part (f_q - f_-q)/2 with w.  The reference picks
+// the rates by which_pop == 'f', a name no set is called with ('p', 'g', 'h'), so every
+// set takes this form, as here.  Operations in the reference's order.
+template <typename A>
+__device__ __forceinline__ void trt_set(A* f, const A* eq, A w, A wm) {
+  A out[Q];
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const int qb = qinv(q);
+    const A fp = A(0.5) * (f[q] + f[qb]), fm = A(0.5) * (f[q] - f[qb]);
+    const A ep = A(0.5) * (eq[q] + eq[qb]), em = A(0.5) * (eq[q] - eq[qb]);
+    const A fcoll = -wm * (fp - ep) - w * (fm - em);
+    out[q] = f[q] + fcoll;
+  }
+#pragma unroll
+  for (int q = 0; q < Q; q++) f[q] = out[q];
+}
+
+// METHOD_TRT collision of all enabled sets, then Guo's forcing of the fluid
+template <bool EXACT, bool THERM, bool SCAL, typename A>
+__device__ __forceinline__ void collide_trt(const StepParams<A>& P, const CellState<A>& c, bool forcing, A wm, A* f,
+                                            A* g, A* h) {
+  A poly[Q], eq[Q];
+#pragma unroll
+  for (int q = 0; q < Q; q++) {
+    const A cu = cdot_rt(q, c.ux, c.uy, c.uz);
+    poly[q] = EXACT ? A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * c.u2
+                    : c.base + cu * (P.invcs2 + P.invtwocs4 * cu);
+    eq[q] = EXACT ? c.rho * P.w[q] * poly[q] : (c.rho * P.w[q]) * poly[q];
+  }
+  trt_set(f, eq, c.invtau, wm);
+  if (forcing) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      const A cu = cdot_rt(q, c.ux, c.uy, c.uz);
+      if constexpr (EXACT) {  // src/forcing.c:1423-1435, three separate additions
+        const A dx = guo_d_rt(cx(q), c.ux, cu, P.invcs2, P.invcs4);
+        const A dy = guo_d_rt(cy(q), c.uy, cu, P.invcs2, P.invcs4);
+        const A dz = guo_d_rt(cz(q), c.uz, cu, P.invcs2, P.invcs4);
+        f[q] += P.facw[q] * c.rho * c.Fx * dx;
+        f[q] += P.facw[q] * c.rho * c.Fy * dy;
+        f[q] += P.facw[q] * c.rho * c.Fz * dz;
+      } else {
+        const A cF = cdot_rt(q, c.Fx, c.Fy, c.Fz);
+        f[q] += (P.facw[q] * c.rho) * ((cF - c.uF) * P.invcs2 + (cu * cF) * P.invcs4);
+      }
+    }
+  }
+  if constexpr (THERM) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) eq[q] = EXACT ? c.tt * P.w[q] * poly[q] : (c.tt * P.w[q]) * poly[q];
+    trt_set(g, eq, c.it, P.invtau_m[1]);
+  }
+  if constexpr (SCAL) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) eq[q] = EXACT ? c.ss * P.w[q] * poly[q] : (c.ss * P.w[q]) * poly[q];
+    trt_set(h, eq, c.is, P.invtau_m[2]);
+  }
+}
+
 // The step for one cell (x, y, z) of the lattice described by P.
-template <typename S, typename A, bool THERM, bool SCAL>
+template <typename S, typename A, bool THERM, bool SCAL, bool TRT = false>
 __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, int z) {
   constexpr bool EXACT = sizeof(A) == 8;
   const int idx = (z * P.NY + y) * P.NX + x;
@@ -252,7 +314,12 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
   CH4_COL(0, FO) CH4_COL(1, FO) CH4_COL(2, FO) CH4_COL(3, FO) CH4_COL(4, FO) CH4_COL(5, FO) CH4_COL(6, FO)          \
   CH4_COL(7, FO) CH4_COL(8, FO) CH4_COL(9, FO) CH4_COL(10, FO) CH4_COL(11, FO) CH4_COL(12, FO) CH4_COL(13, FO)     \
   CH4_COL(14, FO) CH4_COL(15, FO) CH4_COL(16, FO) CH4_COL(17, FO) CH4_COL(18, FO)
-  if constexpr (sizeof(S) == 4) {
+  if constexpr (TRT) {
+    // the antisymmetric rate from the cell's own rate (LES) or the set's
+    const A wm = (F & K_LES) ? (A(4) - A(2) * c.invtau) / (A(2) + (A(4) * A(0.25) - A(1)) * c.invtau)
+                             : P.invtau_m[0];
+    collide_trt<EXACT, THERM, SCAL>(P, c, forcing, wm, f, g, h);
+  } else if constexpr (sizeof(S) == 4) {
     if (forcing) {
       CH4_COLS(1)
     } else {
@@ -298,9 +365,9 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
   }
 }
 
-template <typename S, typename A, bool THERM, bool SCAL>
+template <typename S, typename A, bool THERM, bool SCAL, bool TRT = false>
 __global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
-  lb_cell<S, A, THERM, SCAL>(P, x, blockIdx.y, blockIdx.z);
+  lb_cell<S, A, THERM, SCAL, TRT>(P, x, blockIdx.y, blockIdx.z);
 }

@@ -96,6 +96,7 @@ enum {
   CH4_F_OUTPUT_DIAGN_APPEND = 1ull << 50,     /* ruler files appended, src/output.c:780-830 */
   CH4_F_LAGRANGE_GRAVITY = 1ull << 51,        /* -g on inertial particles, src/lagrange.c:3312-3339 */
   CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES = 1ull << 52, /* u at the particles in particle_averages.dat */
+  CH4_F_METHOD_TRT = 1ull << 53,              /* two-relaxation-time collision, src/fluid.c:1140-1160 */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63

@@ -709,6 +709,18 @@ static void force_moments(const ch4o_state *s, const double *hit, const double *
 }
 
 /* one step of src/main.c:67-161 */
+/* METHOD_TRT (src/fluid.c:1140-1160): the antisymmetric rate (magic gamma 1/4) and the
+ * collision term of direction q: the symmetric part relaxes with wm, the antisymmetric
+ * part with w.  The reference selects the rates by which_pop == 'f', a name no set is
+ * called with, so every set takes this form. */
+static double trt_minus(double w) { return (4. - 2. * w) / (2. + (4. * 0.25 - 1.) * w); }
+static double trt_coll(const double *f, const double *eq, int q, double w, double wm) {
+  int qb = INV[q];
+  double fp = 0.5 * (f[q] + f[qb]), fm = 0.5 * (f[q] - f[qb]);
+  double ep = 0.5 * (eq[q] + eq[qb]), em = 0.5 * (eq[q] - eq[qb]);
+  return -wm * (fp - ep) - w * (fm - em);
+}
+
 static void one_step(ch4o_state *s) {
   const ch4_config *c = &s->cfg;
   const int NX = s->NX, NY = s->NY, NZ = s->NZ;
@@ -759,7 +771,9 @@ static void one_step(ch4o_state *s) {
   }
 
   const double invtau_u = 1.0 / c->tau_u;
-  const double fac_guo = (1.0 - 0.5 * c->time_dt * invtau_u); /* src/forcing.c:1289 */
+  const int trt = (c->flags & CH4_F_METHOD_TRT) != 0;
+  /* METHOD_TRT: the Guo prefactor takes the antisymmetric rate, src/forcing.c:1279-1284 */
+  const double fac_guo = (1.0 - 0.5 * c->time_dt * (trt ? trt_minus(invtau_u) : invtau_u)); /* src/forcing.c:1289 */
   const double invtau_set[3] = {invtau_u, s->nsets_on[1] ? 1.0 / c->tau_t : 0.0, s->nsets_on[2] ? 1.0 / c->tau_s : 0.0};
 
   for (int k = 0; k < NZ; k++)
@@ -800,12 +814,23 @@ static void one_step(ch4o_state *s) {
           invtau = 1.0 / tl;
         }
         double post[3][NPOP];
-        /* fluid: BGK (src/fluid.c:1163,1218) + Guo (src/forcing.c:1423-1435) */
+        double feqs[3][NPOP];
         for (int q = 0; q < NPOP; q++) {
           double cu = (CX[q] * ux + CY[q] * uy + CZ[q] * uz);
-          double feq = rho * s->w[q] * (1.0 + s->invcs2 * cu + s->invtwocs4 * cu * cu - s->invtwocs2 * u2);
+          double poly = (1.0 + s->invcs2 * cu + s->invtwocs4 * cu * cu - s->invtwocs2 * u2);
+          feqs[0][q] = rho * s->w[q] * poly;
+          feqs[1][q] = tt * s->w[q] * poly;
+          feqs[2][q] = ss * s->w[q] * poly;
+        }
+        /* fluid: BGK (src/fluid.c:1163,1218) or TRT (1140-1160) + Guo (src/forcing.c:1423-1435) */
+        for (int q = 0; q < NPOP; q++) {
+          double cu = (CX[q] * ux + CY[q] * uy + CZ[q] * uz);
+          double feq = feqs[0][q];
           double r = a[q];
-          r += -invtau * (a[q] - feq);
+          if (trt)
+            r += trt_coll(a, feqs[0], q, invtau, trt_minus(invtau));
+          else
+            r += -invtau * (a[q] - feq);
           if (forcing) {
             double dx = (CX[q] - ux) * s->invcs2 + CX[q] * cu * s->invcs4;
             double dy = (CY[q] - uy) * s->invcs2 + CY[q] * cu * s->invcs4;
@@ -820,12 +845,13 @@ static void one_step(ch4o_state *s) {
         for (int set = 1; set < 3; set++) {
           if (!s->nsets_on[set]) continue;
           const double *b = set == 1 ? ga : ha;
-          double m0 = set == 1 ? tt : ss;
           for (int q = 0; q < NPOP; q++) {
-            double cu = (CX[q] * ux + CY[q] * uy + CZ[q] * uz);
-            double feq = m0 * s->w[q] * (1.0 + s->invcs2 * cu + s->invtwocs4 * cu * cu - s->invtwocs2 * u2);
+            double feq = feqs[set][q];
             double r = b[q];
-            r += -invtau_set[set] * (b[q] - feq);
+            if (trt)
+              r += trt_coll(b, feqs[set], q, invtau_set[set], trt_minus(invtau_set[set]));
+            else
+              r += -invtau_set[set] * (b[q] - feq);
             post[set][q] = r;
           }
         }

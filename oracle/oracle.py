@@ -46,6 +46,10 @@ FLAGSETS = {
                   "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
     "particles_1w": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS"],
+    "trt": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+            "LB_TEMPERATURE_BC_Y", "METHOD_TRT"],
+    "trt_les": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
+                "LB_FLUID_BC_Y", "LB_FLUID_LES", "METHOD_TRT"],
     "particles_fa": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
                      "LAGRANGE_OUTPUT_FLUID_AVERAGES"],

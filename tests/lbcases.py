@@ -41,6 +41,11 @@ CASES = {
                                S_bot=0.2, S_top=0.7, S_ref=0.1, beta_s=0.3, gravity_y=2e-3, gravity_x=1e-3)),
     "les": dict(flagset="les", NX=8, NY=9, NZ=6,
                 params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "trt": dict(flagset="trt", NX=8, NY=7, NZ=5,
+                params=dict(tau_u=0.62, tau_t=0.7, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
+                            gravity_y=1e-3, gravity_x=2e-4)),
+    "trt_les": dict(flagset="trt_les", NX=8, NY=9, NZ=6,
+                    params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
     "particles": dict(flagset="particles", NX=10, NY=8, NZ=7, npart=300,
                       params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=6,
                                   time_dt_lagr_factor=2.0, particle_number=300)),

@@ -46,7 +46,8 @@ def rel_l2(a, b):
 
 @pytest.mark.parametrize("name,nsteps", [("kolmogorov", 25), ("rb", 25), ("hit", 20), ("walls2", 25),
                                           ("scalar", 25), ("les", 25), ("particles", 12),
-                                          ("particles_t", 12), ("particles_g", 12), ("particles_1w", 12)])
+                                          ("particles_t", 12), ("particles_g", 12), ("particles_1w", 12),
+                                          ("trt", 25), ("trt_les", 25)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):
     _, cfg, state = make_case(name, seed=11)
     ref = run_restatement(cfg, state, nsteps)
@@ -69,7 +70,7 @@ def test_fp64_bit_identical_to_oracle(name, nsteps):
 
 
 @pytest.mark.parametrize("name", ["kolmogorov", "rb", "hit", "walls2", "scalar", "les", "particles",
-                                  "particles_t", "particles_g"])
+                                  "particles_t", "particles_g", "trt", "trt_les"])
 def test_fp64_matches_compiled_reference(name):
     flagset, cfg, state = make_case(name, seed=5)
     if not O.ref_available(flagset):
@@ -89,7 +90,7 @@ def test_fp64_matches_compiled_reference(name):
 # of rho within 1e-5, of T within 1e-6 (40 steps).
 # FP16 deviations (11-bit mantissa): u within 0.2, rho within 1e-3, T within 2e-2.
 @pytest.mark.parametrize("storage,tol_u,tol_rho,tol_t", [(1, 1e-3, 1e-5, 1e-6), (2, 0.2, 1e-3, 2e-2)])
-@pytest.mark.parametrize("name", ["kolmogorov", "rb", "scalar", "hit"])
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "scalar", "hit", "trt"])
 def test_reduced_precision_error_bounds(name, storage, tol_u, tol_rho, tol_t):
     _, cfg64, state = make_case(name, seed=2)
     _, cfg, _ = make_case(name, seed=2, storage=storage)
