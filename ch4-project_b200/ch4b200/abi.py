@@ -73,6 +73,11 @@ FLAGS = {
     "LAGRANGE_GRAVITY": 1 << 51,
     "LAGRANGE_OUTPUT_FLUID_AVERAGES": 1 << 52,
     "METHOD_TRT": 1 << 53,
+    "LB_FLUID_LES_VANDRIEST": 1 << 54,
+    "LB_TEMPERATURE_LES": 1 << 55,
+    "LB_SCALAR_LES": 1 << 56,
+    "LB_FLUID_LES_WALE": 1 << 57,
+    "LB_FLUID_LES_LOCAL_STRAIN": 1 << 58,
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 

@@ -124,7 +124,8 @@ const uint64_t SUPPORTED =
     CH4_F_SCALAR_INITIAL_ADD_PERTURBATION | CH4_F_SCALAR_INITIAL_CONSTANT | CH4_F_SCALAR_INITIAL_CONSTANT_MEAN |
     CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
     CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND | CH4_F_LAGRANGE_GRAVITY |
-    CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES | CH4_F_METHOD_TRT;
+    CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES | CH4_F_METHOD_TRT | CH4_F_FLUID_LES_VANDRIEST | CH4_F_TEMPERATURE_LES |
+    CH4_F_SCALAR_LES | CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -450,6 +451,11 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   if (fl & CH4_F_SCALAR_BC_Y) F |= K_SWALL;
   if (fl & CH4_F_FLUID_LES) F |= K_LES;
   if (fl & CH4_F_METHOD_TRT) F |= K_TRT;
+  if (fl & CH4_F_FLUID_LES_VANDRIEST) F |= K_VANDRIEST;
+  if (fl & CH4_F_TEMPERATURE_LES) F |= K_TLES;
+  if (fl & CH4_F_SCALAR_LES) F |= K_SLES;
+  if (fl & CH4_F_FLUID_LES_WALE) F |= K_WALE;
+  if (fl & CH4_F_FLUID_LES_LOCAL_STRAIN) F |= K_LSTRAIN;
   P.feat = F;
   P.fm_prev = P.fm_cur = nullptr;
   for (int q = 0; q < NPOP; q++) P.w[q] = (A)lat.w[q];
@@ -474,6 +480,12 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.hdt = (A)(0.5 * c.time_dt);
   P.nu = (A)c.nu;
   P.csmag2 = (A)std::pow(c.C_smag * 1.0, 2.0);
+  P.kappa = (A)c.kappa;
+  P.chi = (A)c.chi;
+  P.tau_u = (A)c.tau_u;
+  P.cs2 = (A)lat.cs2;
+  P.les_first = 0;
+  P.csmag2_y = nullptr;
   const double LX = c.SX, LY = c.SY, nu = c.nu;
   P.pois[0] = (A)(2.0 * c.Amp_x * ((4. * nu) * std::pow(LY, -2.0)));
   P.pois[1] = (A)(2.0 * c.Amp_y * ((4. * nu) * std::pow(LX, -2.0)));
@@ -524,6 +536,7 @@ struct Engine : EngineBase {
   A *tprev = nullptr, *sprev = nullptr;
   A *kol = nullptr;
   A *ules = nullptr, *tau_les = nullptr;
+  A* vd = nullptr;  // LB_FLUID_LES_VANDRIEST: pow(C_smag(y), 2) per row
   A *hit_ring = nullptr;  // (CHUNK+1) phase-table slots
   A *hit_last = nullptr;  // tables of the latest phases (those of F^n)
   double* staging_d = nullptr;  // device AoS chunk
@@ -592,6 +605,7 @@ struct Engine : EngineBase {
     cudaFree(kol);
     cudaFree(ules);
     cudaFree(tau_les);
+    cudaFree(vd);
     cudaFree(hit_ring);
     cudaFree(hit_last);
     cudaFree(staging_d);
@@ -985,6 +999,20 @@ struct Engine : EngineBase {
     if (c.flags & CH4_F_FLUID_LES) {
       if (cudaMalloc(&ules, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
       if (cudaMalloc(&tau_les, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tau_les");
+      if (c.flags & CH4_F_FLUID_LES_VANDRIEST) {
+        // C_smag(y) of src/les.c:136-142: the test is on the row index with the LES halo
+        // (BRD = 2, src/typedef.h:317), the distance on the cell centre y = j + 0.5
+        std::vector<A> t(c.NY);
+        for (int j = 0; j < c.NY; j++) {
+          const double yc = (double)j + 0.5, jp = (double)(j + 2);
+          const double C = jp < (c.SY / 2.0) ? c.C_smag * (1.0 - std::exp((-(c.Amp_x * yc) / c.nu) / 26.0))
+                                             : c.C_smag * (1.0 - std::exp((-(c.Amp_x * ((c.SY - yc))) / c.nu) / 26.0));
+          t[j] = (A)std::pow(C * 1.0, 2.0);
+        }
+        if (cudaMalloc(&vd, c.NY * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "van Driest table");
+        if (cudaMemcpy(vd, t.data(), c.NY * sizeof(A), cudaMemcpyHostToDevice) != cudaSuccess)
+          return H->fail(CH4_ERR_CUDA, "van Driest table");
+      }
     }
     const int nk = 2 * c.NY + c.NX;
     if (cudaMalloc(&kol, nk * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "kol");
@@ -1047,6 +1075,7 @@ struct Engine : EngineBase {
     P.ules = ules;
     P.tau_les = tau_les;
     P.kol = kol;
+    P.csmag2_y = vd;
     P.dcur = P.dprev = nullptr;
     P.fm_prev = P.fm_cur = fmbuf;  // both slots hold {0, 1} until the first correction
   }
@@ -1059,10 +1088,6 @@ struct Engine : EngineBase {
     }
   }
 
-  // AoS (halo-padded by brd) -> device SoA; `repeat` uploads the same chunk to every slab
-  // Reference-layout AoS (with `brd` halo) -> device SoA, in z-slab chunks through
-  // pinned staging.  With two staging pairs the host copies chunk k+1 (rows split over
-  // host threads) while chunk k is transferred and converted.
   // every z-slab chunk of a set <- the AoS chunk held in staging_h
   ch4_status fill_repeated(int set) {
     const size_t bytes = (size_t)c.NX * c.NY * NPOP * chunk_planes * sizeof(double);
@@ -1075,6 +1100,9 @@ struct Engine : EngineBase {
     return st ? st : H->cuda(cudaStreamSynchronize(H->stream), "fill sync");
   }
 
+  // Reference-layout AoS (with `brd` halo) -> device SoA, in z-slab chunks through
+  // pinned staging.  With two staging pairs the host copies chunk k+1 (rows split over
+  // host threads) while chunk k is transferred and converted.
   ch4_status upload_chunks(int set, const double* aos, int brd) {
     const size_t row = (size_t)c.NX * NPOP;
     const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
@@ -1253,6 +1281,7 @@ struct Engine : EngineBase {
         const int n_step = H->itime + 1;  // the reference's itime during this step
         bind_pops(cur);
         P.hit_prev = hit ? hit_ring + (size_t)k * slot : nullptr;
+        P.les_first = H->itime == 0;  // LOCAL_STRAIN: no previous LES time yet
         P.hit_cur = hit ? hit_ring + (size_t)(k + 1) * slot : nullptr;
         if (twoway()) {
           // deposit of the particles moved in the previous step (src/main.c:122-128)
@@ -1591,6 +1620,11 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_GRAVITY", CH4_F_LAGRANGE_GRAVITY},
       {"LAGRANGE_OUTPUT_FLUID_AVERAGES", CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES},
       {"METHOD_TRT", CH4_F_METHOD_TRT},
+      {"LB_FLUID_LES_VANDRIEST", CH4_F_FLUID_LES_VANDRIEST},
+      {"LB_TEMPERATURE_LES", CH4_F_TEMPERATURE_LES},
+      {"LB_SCALAR_LES", CH4_F_SCALAR_LES},
+      {"LB_FLUID_LES_WALE", CH4_F_FLUID_LES_WALE},
+      {"LB_FLUID_LES_LOCAL_STRAIN", CH4_F_FLUID_LES_LOCAL_STRAIN},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -1668,6 +1702,24 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
   if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
     return why = "walls need NY >= 3", CH4_ERR_ARG;
   if (!(c->tau_u > 0.5)) return why = "tau_u must exceed 0.5", CH4_ERR_ARG;
+  {
+    const uint64_t les_variants = CH4_F_FLUID_LES_VANDRIEST | CH4_F_TEMPERATURE_LES | CH4_F_SCALAR_LES |
+                                  CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN;
+    if ((c->flags & les_variants) && !(c->flags & CH4_F_FLUID_LES))
+      return why = "LES variants need LB_FLUID_LES", CH4_ERR_UNSUPPORTED;
+    if ((c->flags & CH4_F_TEMPERATURE_LES) && !(c->flags & CH4_F_LB_TEMPERATURE))
+      return why = "LB_TEMPERATURE_LES needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
+    if ((c->flags & CH4_F_SCALAR_LES) && !(c->flags & CH4_F_LB_SCALAR))
+      return why = "LB_SCALAR_LES needs LB_SCALAR", CH4_ERR_UNSUPPORTED;
+    // the reference's scalar LES time calls tau_u_les a second time, which with LOCAL_STRAIN
+    // reads the LES time the fluid's call has just stored: not reproduced
+    if ((c->flags & CH4_F_SCALAR_LES) && (c->flags & CH4_F_FLUID_LES_LOCAL_STRAIN))
+      return why = "LB_SCALAR_LES with LB_FLUID_LES_LOCAL_STRAIN is not supported", CH4_ERR_UNSUPPORTED;
+    // the reference's WALE reads the finite-difference gradient, which LOCAL_STRAIN never computes
+    if ((c->flags & CH4_F_FLUID_LES_WALE) && (c->flags & CH4_F_FLUID_LES_LOCAL_STRAIN))
+      return why = "LB_FLUID_LES_WALE with LB_FLUID_LES_LOCAL_STRAIN reads an unset gradient in the reference",
+             CH4_ERR_UNSUPPORTED;
+  }
   if (c->flags & CH4_F_LAGRANGE) {
     if (c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_LB_SCALAR))
       return why = "particles are implemented for the periodic box (fluid, optionally temperature)",

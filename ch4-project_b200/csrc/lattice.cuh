@@ -56,7 +56,12 @@ enum : uint32_t {
   K_TSRC = 1u << 18,
   K_NOZERO = 1u << 19,  // LB_FLUID_FORCING_NOZEROMODE: subtract the mean force
   K_CPOWER = 1u << 20,  // LB_FLUID_FORCING_CONSTANT_POWER: scale to a fixed mean power
-  K_TRT = 1u << 21      // METHOD_TRT: two-relaxation-time collision
+  K_TRT = 1u << 21,     // METHOD_TRT: two-relaxation-time collision
+  K_VANDRIEST = 1u << 22,  // LB_FLUID_LES_VANDRIEST: C_smag damped towards the y walls (table per row)
+  K_TLES = 1u << 23,       // LB_TEMPERATURE_LES: thermal relaxation time from the LES one
+  K_SLES = 1u << 24,       // LB_SCALAR_LES: scalar relaxation time from the LES one
+  K_WALE = 1u << 25,       // LB_FLUID_LES_WALE: WALE eddy viscosity
+  K_LSTRAIN = 1u << 26     // LB_FLUID_LES_LOCAL_STRAIN: |S| from the populations' stress tensor
 };
 
 template <typename A>
@@ -95,6 +100,9 @@ struct StepParams {
   A invtau_m[3];  // METHOD_TRT: (4 - 2/tau) / (2 + (4 gamma - 1)/tau), gamma = 1/4, per set
   A hdt;  // 0.5*time_dt
   A nu, csmag2;  // LES: nu and pow(C_smag*1, 2)
+  const A* csmag2_y;  // LB_FLUID_LES_VANDRIEST: pow(C_smag(y)*1, 2) per row
+  A kappa, chi, tau_u, cs2;  // LES of the temperature / scalar, LOCAL_STRAIN (cs2 = pow(cs, 2))
+  int les_first;      // first step of the run: LOCAL_STRAIN takes tau_u as the previous LES time
   // storage shift (rho0 for p, T0 for g, S0 for h) used by the F16 codec
   float shift[3];
   // forcing

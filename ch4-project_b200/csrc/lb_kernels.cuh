@@ -178,39 +178,100 @@ __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >=
 
 // Smagorinsky relaxation time of src/les.c:5-269 (centred differences of
 // src/gradients.c:78-~240, one-sided 2nd order at the y walls)
-template <typename A>
-__device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z) {
+// Eddy-viscosity relaxation time of tau_u_les (src/les.c:5-269) for one cell:
+// Smagorinsky with |S| from centred differences of u^n (src/gradients.c:78-~240, one-sided
+// 2nd order at the y walls) or, with LB_FLUID_LES_LOCAL_STRAIN, from the populations'
+// stress tensor; C_smag per row with LB_FLUID_LES_VANDRIEST; WALE with LB_FLUID_LES_WALE.
+// f, rho, ux..u2: the cell's populations and the collision's rho, u^n, |u|^2.
+template <bool EXACT, typename A>
+__device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z, long long idx, const A* f, A rho,
+                                     A ux, A uy, A uz, A u2) {
   const int NX = P.NX, NY = P.NY, NZ = P.NZ;
   const long long N = P.N;
-  const A* u = P.ules;
-  auto at = [&](int a, int i, int j, int k) { return u[a * N + ((long long)k * NY + j) * NX + i]; };
-  A g[3][3];
-  const int xp = wrap(x + 1, NX), xm = wrap(x - 1, NX), zp = wrap(z + 1, NZ), zm = wrap(z - 1, NZ);
+  const uint32_t F = P.feat;
+  A s_norm;
+  A xx = A(0), xy = A(0), xz = A(0), yx = A(0), yy = A(0), yz = A(0), zx = A(0), zy = A(0), zz = A(0);
+  if (F & K_LSTRAIN) {
+    // stress_tensor (src/gradients.c:42-66) as the reference has it: zz takes xz, zx stays 0
+    A S[6] = {A(0), A(0), A(0), A(0), A(0), A(0)};  // xx yy zz xy xz yz
 #pragma unroll
-  for (int a = 0; a < 3; a++) {
-    g[a][0] = (at(a, xp, y, z) - at(a, xm, y, z)) / A(2);
-    g[a][2] = (at(a, x, y, zp) - at(a, x, y, zm)) / A(2);
-  }
-  const bool walls = (P.feat & K_FWALL) != 0;
-  if (walls && y == 0) {
-#pragma unroll
-    for (int a = 0; a < 3; a++) g[a][1] = A(-1.5) * at(a, x, 0, z) + A(2) * at(a, x, 1, z) + A(-0.5) * at(a, x, 2, z);
-  } else if (walls && y == NY - 1) {
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-      g[a][1] = A(1.5) * at(a, x, NY - 1, z) + A(-2) * at(a, x, NY - 2, z) + A(0.5) * at(a, x, NY - 3, z);
+    for (int q = 0; q < Q; q++) {
+      const A cu = cdot_rt(q, ux, uy, uz);
+      const A poly = EXACT ? A(1) + P.invcs2 * cu + P.invtwocs4 * cu * cu - P.invtwocs2 * u2
+                           : (A(1) - P.invtwocs2 * u2) + cu * (P.invcs2 + P.invtwocs4 * cu);
+      const A d = f[q] - rho * P.w[q] * poly;
+      const int a = cx(q), b = cy(q), c = cz(q);
+      if (a != 0) S[0] += d;            // c_x c_x = 1
+      if (b != 0) S[1] += d;
+      if (c != 0) S[2] += d;
+      if (a * b != 0) S[3] += A(a * b) * d;
+      if (a * c != 0) S[4] += A(a * c) * d;
+      if (b * c != 0) S[5] += A(b * c) * d;
+    }
+    const A QQxx = S[0], QQyy = S[1], QQxy = S[3], QQxz = S[4], QQyz = S[5];
+    const A QQzz = QQxz, QQyx = QQxy, QQzy = QQyz, QQzx = A(0);
+    // the previous step's LES time (tau_u on the first step), src/les.c:23-26
+    const A tprev = P.les_first ? P.tau_u : P.tau_les[idx];
+    const A fac = A(-1) / (A(2) * P.cs2 * rho * tprev * A(1));
+    s_norm = fabs(fac) * sqrt(A(2) * (QQxx * QQxx + QQxy * QQxy + QQxz * QQxz + QQyx * QQyx + QQyy * QQyy +
+                                      QQyz * QQyz + QQzx * QQzx + QQzy * QQzy + QQzz * QQzz));
   } else {
-    const int yp = wrap(y + 1, NY), ym = wrap(y - 1, NY);
+    const A* u = P.ules;
+    auto at = [&](int a, int i, int j, int k) { return u[a * N + ((long long)k * NY + j) * NX + i]; };
+    A g[3][3];
+    const int xp = wrap(x + 1, NX), xm = wrap(x - 1, NX), zp = wrap(z + 1, NZ), zm = wrap(z - 1, NZ);
 #pragma unroll
-    for (int a = 0; a < 3; a++) g[a][1] = (at(a, x, yp, z) - at(a, x, ym, z)) / A(2);
+    for (int a = 0; a < 3; a++) {
+      g[a][0] = (at(a, xp, y, z) - at(a, xm, y, z)) / A(2);
+      g[a][2] = (at(a, x, y, zp) - at(a, x, y, zm)) / A(2);
+    }
+    const bool walls = (F & K_FWALL) != 0;
+    if (walls && y == 0) {
+#pragma unroll
+      for (int a = 0; a < 3; a++) g[a][1] = A(-1.5) * at(a, x, 0, z) + A(2) * at(a, x, 1, z) + A(-0.5) * at(a, x, 2, z);
+    } else if (walls && y == NY - 1) {
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        g[a][1] = A(1.5) * at(a, x, NY - 1, z) + A(-2) * at(a, x, NY - 2, z) + A(0.5) * at(a, x, NY - 3, z);
+    } else {
+      const int yp = wrap(y + 1, NY), ym = wrap(y - 1, NY);
+#pragma unroll
+      for (int a = 0; a < 3; a++) g[a][1] = (at(a, x, yp, z) - at(a, x, ym, z)) / A(2);
+    }
+    xx = g[0][0], xy = g[0][1], xz = g[0][2];
+    yx = g[1][0], yy = g[1][1], yz = g[1][2];
+    zx = g[2][0], zy = g[2][1], zz = g[2][2];
+    s_norm = sqrt(A(0.5) * ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) +
+                            (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
+                            (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
   }
-  const A xx = g[0][0], xy = g[0][1], xz = g[0][2];
-  const A yx = g[1][0], yy = g[1][1], yz = g[1][2];
-  const A zx = g[2][0], zy = g[2][1], zz = g[2][2];
-  const A s_norm = sqrt(A(0.5) * ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) +
-                                  (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
-                                  (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
-  const A nu_les = s_norm * P.csmag2;
+  A nu_les = s_norm * ((F & K_VANDRIEST) ? P.csmag2_y[y] : P.csmag2);
+  if (F & K_WALE) {  // Nicoud & Ducros 1999, src/les.c:182-248 (C_wale = 0.5)
+    const A Sxx = xx, Syy = yy, Szz = zz;
+    const A Sxy = A(0.5) * (xy + yx), Sxz = A(0.5) * (xz + zx), Szy = A(0.5) * (zy + yz);
+    const A Syx = Sxy, Szx = Sxz, Syz = Szy;
+    const A Wxx = A(0), Wyy = A(0), Wzz = A(0);
+    const A Wxy = A(0.5) * (xy - yx), Wxz = A(0.5) * (xz - zx), Wyz = A(0.5) * (zy - yz);
+    const A Wyx = -Wxy, Wzx = -Wxz, Wzy = -Wyz;
+    const A iso = Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Syx * Syx + Syy * Syy + Syz * Syz + Szx * Szx + Szy * Szy +
+                  Szz * Szz - Wxx * Wxx - Wxy * Wxy - Wxz * Wxz - Wyx * Wyx - Wyy * Wyy - Wyz * Wyz - Wzx * Wzx -
+                  Wzy * Wzy - Wzz * Wzz;
+    const A Jxx = Sxx * Sxx + Sxy * Syx + Sxz * Szx + Wxx * Wxx + Wxy * Wyx + Wxz * Wzx - iso / A(3);
+    const A Jxy = Sxx * Sxy + Sxy * Syy + Sxz * Szy + Wxx * Wxy + Wxy * Wyy + Wxz * Wzy;
+    const A Jxz = Sxx * Sxz + Sxy * Syz + Sxz * Szz + Wxx * Wxz + Wxy * Wyz + Wxz * Wzz;
+    const A Jyx = Syx * Sxx + Syy * Syx + Syz * Szx + Wyx * Wxx + Wyy * Wyx + Wyz * Wzx;
+    const A Jyy = Syx * Sxy + Syy * Syy + Syz * Szy + Wyx * Wxy + Wyy * Wyy + Wyz * Wzy - iso / A(3);
+    const A Jyz = Syx * Sxz + Syy * Syz + Syz * Szz + Wyx * Wxz + Wyy * Wyz + Wyz * Wzz;
+    const A Jzx = Szx * Sxx + Szy * Syx + Szz * Szx + Wzx * Wxx + Wzy * Wyx + Wzz * Wzx;
+    const A Jzy = Szx * Sxy + Szy * Syy + Szz * Szy + Wzx * Wxy + Wzy * Wyy + Wzz * Wzy;
+    const A Jzz = Szx * Sxz + Szy * Syz + Szz * Szz + Wzx * Wxz + Wzy * Wyz + Wzz * Wzz - iso / A(3);
+    const A s_norm2 = s_norm * s_norm / A(2);  // pow(s_norm, 2.0) / 2.0
+    const A j_norm2 = Jxx * Jxx + Jxy * Jxy + Jxz * Jxz + Jyx * Jyx + Jyy * Jyy + Jyz * Jyz + Jzx * Jzx + Jzy * Jzy +
+                      Jzz * Jzz;
+    // the device pow: within an ulp or two of the reference's libm
+    const A op = pow(j_norm2, A(1.5)) / (pow(s_norm2, A(2.5)) + pow(j_norm2, A(1.25)));
+    nu_les = op * A(0.25);  // pow(C_wale * 1, 2.0)
+  }
   return A(3) * (nu_les + P.nu) + A(0.5);
 }
 

@@ -177,6 +177,12 @@ __device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellSt
   }
 }
 
+// METHOD_TRT's antisymmetric rate from a rate w (src/fluid.c:1141-1143, magic gamma 1/4)
+template <typename A>
+__device__ __forceinline__ A trt_minus(A w) {
+  return (A(4) - A(2) * w) / (A(2) + (A(4) * A(0.25) - A(1)) * w);
+}
+
 // Two-relaxation-time collision of METHOD_TRT (src/fluid.c:1140-1160) of one set, in
 // place: per direction the symmetric part (f_q + f_-q)/2 relaxes towards that of the
 // equilibrium with wm, the antisymmetric part (f_q - f_-q)/2 with w.  The reference picks
@@ -230,18 +236,23 @@ __device__ __forceinline__ void collide_trt(const StepParams<A>& P, const CellSt
   if constexpr (THERM) {
 #pragma unroll
     for (int q = 0; q < Q; q++) eq[q] = EXACT ? c.tt * P.w[q] * poly[q] : (c.tt * P.w[q]) * poly[q];
-    trt_set(g, eq, c.it, P.invtau_m[1]);
+    trt_set(g, eq, c.it, (P.feat & K_TLES) ? trt_minus(c.it) : P.invtau_m[1]);
   }
   if constexpr (SCAL) {
 #pragma unroll
     for (int q = 0; q < Q; q++) eq[q] = EXACT ? c.ss * P.w[q] * poly[q] : (c.ss * P.w[q]) * poly[q];
-    trt_set(h, eq, c.is, P.invtau_m[2]);
+    trt_set(h, eq, c.is, (P.feat & K_SLES) ? trt_minus(c.is) : P.invtau_m[2]);
   }
 }
 
 // The step for one cell (x, y, z) of the lattice described by P.
-template <typename S, typename A, bool THERM, bool SCAL, bool TRT = false>
+// Kernel variants (separate instantiations, so that the plain BGK kernels keep their
+// registers): bit 0 METHOD_TRT, bit 1 LES (eddy-viscosity relaxation times).
+constexpr int V_TRT = 1, V_LES = 2;
+
+template <typename S, typename A, bool THERM, bool SCAL, int V = 0>
 __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, int z) {
+  constexpr bool TRT = (V & V_TRT) != 0, LES = (V & V_LES) != 0;
   constexpr bool EXACT = sizeof(A) == 8;
   const int idx = (z * P.NY + y) * P.NX + x;
   const uint32_t F = P.feat;
@@ -282,13 +293,16 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
 
   c.u2 = c.ux * c.ux + c.uy * c.uy + c.uz * c.uz;
   c.invtau = P.invtau[0];
-  if (F & K_LES) {
-    const A tl = les_tau(P, x, y, z);
-    P.tau_les[idx] = tl;
-    c.invtau = A(1) / tl;
-  }
   c.it = P.invtau[1];
   c.is = P.invtau[2];
+  if constexpr (LES) {
+    const A tl = les_tau<EXACT>(P, x, y, z, idx, f, c.rho, c.ux, c.uy, c.uz, c.u2);
+    P.tau_les[idx] = tl;
+    c.invtau = A(1) / tl;
+    // tau_t_les / tau_s_les (src/les.c:273-326, turbulent Prandtl and Schmidt numbers 1)
+    if (THERM && (F & K_TLES)) c.it = A(1) / (A(3) * (P.kappa + (tl - A(0.5) - A(3) * P.nu) / (A(3) * A(1))) + A(0.5));
+    if (SCAL && (F & K_SLES)) c.is = A(1) / (A(3) * (P.chi + (tl - A(0.5) - A(3) * P.nu) / (A(3) * A(1))) + A(0.5));
+  }
   c.base = A(1) - P.invtwocs2 * c.u2;
   c.uF = c.ux * c.Fx + c.uy * c.Fy + c.uz * c.Fz;
   if constexpr (!EXACT) {
@@ -316,8 +330,7 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
   CH4_COL(14, FO) CH4_COL(15, FO) CH4_COL(16, FO) CH4_COL(17, FO) CH4_COL(18, FO)
   if constexpr (TRT) {
     // the antisymmetric rate from the cell's own rate (LES) or the set's
-    const A wm = (F & K_LES) ? (A(4) - A(2) * c.invtau) / (A(2) + (A(4) * A(0.25) - A(1)) * c.invtau)
-                             : P.invtau_m[0];
+    const A wm = LES ? trt_minus(c.invtau) : P.invtau_m[0];
     collide_trt<EXACT, THERM, SCAL>(P, c, forcing, wm, f, g, h);
   } else if constexpr (sizeof(S) == 4) {
     if (forcing) {
@@ -365,9 +378,20 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
   }
 }
 
-template <typename S, typename A, bool THERM, bool SCAL, bool TRT = false>
+template <typename S, typename A, bool THERM, bool SCAL, int V = 0>
 __global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
-  lb_cell<S, A, THERM, SCAL, TRT>(P, x, blockIdx.y, blockIdx.z);
+  lb_cell<S, A, THERM, SCAL, V>(P, x, blockIdx.y, blockIdx.z);
+}
+
+// The FP64 BGK step with two population sets, held to 128 registers (four 128-thread
+// blocks per SM): the allocation at which it runs at the HBM roofline; left to itself the
+// compiler may take a few more and lose a block per SM (-13 % measured).  (A minimum-blocks
+// hint on the other forms raises their registers instead; they keep the plain bound.)
+template <typename S, typename A, bool THERM, bool SCAL>
+__global__ void __launch_bounds__(128, 4) lb_step_kernel_cap128(const StepParams<A> P) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= P.NX) return;
+  lb_cell<S, A, THERM, SCAL, 0>(P, x, blockIdx.y, blockIdx.z);
 }

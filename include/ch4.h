@@ -97,6 +97,12 @@ enum {
   CH4_F_LAGRANGE_GRAVITY = 1ull << 51,        /* -g on inertial particles, src/lagrange.c:3312-3339 */
   CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES = 1ull << 52, /* u at the particles in particle_averages.dat */
   CH4_F_METHOD_TRT = 1ull << 53,              /* two-relaxation-time collision, src/fluid.c:1140-1160 */
+  /* LES variants, src/les.c:5-326 */
+  CH4_F_FLUID_LES_VANDRIEST = 1ull << 54,     /* C_smag damped towards the y walls */
+  CH4_F_TEMPERATURE_LES = 1ull << 55,         /* thermal relaxation time from the LES one */
+  CH4_F_SCALAR_LES = 1ull << 56,              /* scalar relaxation time from the LES one */
+  CH4_F_FLUID_LES_WALE = 1ull << 57,          /* WALE eddy viscosity */
+  CH4_F_FLUID_LES_LOCAL_STRAIN = 1ull << 58,  /* |S| from the populations' stress tensor */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63

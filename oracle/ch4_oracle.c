@@ -41,7 +41,7 @@ struct ch4o_state {
   int NX, NY, NZ;
   size_t N;
   double w[NPOP];
-  double invcs2, invcs4, invtwocs2, invtwocs4;
+  double cs2, invcs2, invcs4, invtwocs2, invtwocs4;
   double *f[3], *fn[3]; /* 0: p, 1: g, 2: h */
   int nsets_on[3];
   double *tprev, *sprev; /* t^{n-1}, s^{n-1} */
@@ -221,9 +221,50 @@ static void load_cell(const double *f, size_t N, size_t idx, double *a) {
 
 /* |S| Smagorinsky relaxation time, src/les.c:5-269 with centred differences
  * of src/gradients.c:78-~240 (one-sided 2nd order at walls) */
-static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k) {
+/* tau_u_les (src/les.c:5-269).  Variants: |S| from the populations' stress tensor
+ * (LB_FLUID_LES_LOCAL_STRAIN, src/gradients.c:42-66 as written: zz takes xz, zx stays 0,
+ * with the previous step's LES time, tau_u on the first step); C_smag per row
+ * (LB_FLUID_LES_VANDRIEST, the test on the row index with the LES halo BRD = 2); WALE
+ * (LB_FLUID_LES_WALE).  f, rho, u_*, u2: the cell's populations and the collision's
+ * rho, u^n and |u|^2; tau_prev: the cell's LES time of the previous step. */
+/* C_smag of LB_FLUID_LES_VANDRIEST at row j (src/les.c:136-142): the test uses the row
+ * index with the LES halo (j + BRD, BRD = 2), the distance the cell centre j + 0.5 */
+static double vandriest(const ch4o_state *s, int j) {
+  const ch4_config *c = &s->cfg;
+  double yc = (double)j + 0.5;
+  if ((j + 2) < (c->SY / 2.0)) return c->C_smag * (1.0 - exp((-(c->Amp_x * yc) / c->nu) / 26.0));
+  return c->C_smag * (1.0 - exp((-(c->Amp_x * ((c->SY - yc))) / c->nu) / 26.0));
+}
+
+static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k, const double *f, double rho,
+                      double ux, double uy, double uz, double u2, double tau_prev) {
   const int NX = s->NX, NY = s->NY, NZ = s->NZ;
-  const int walls = (s->cfg.flags & CH4_F_FLUID_BC_Y) != 0;
+  const uint64_t fl = s->cfg.flags;
+  const int walls = (fl & CH4_F_FLUID_BC_Y) != 0;
+  if (fl & CH4_F_FLUID_LES_LOCAL_STRAIN) {
+    double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Sxz = 0, Syz = 0;
+    for (int pp = 0; pp < NPOP; pp++) {
+      double cu = (CX[pp] * ux + CY[pp] * uy + CZ[pp] * uz);
+      double feq = rho * s->w[pp] * (1.0 + s->invcs2 * cu + s->invtwocs4 * cu * cu - s->invtwocs2 * u2);
+      double d = f[pp] - feq;
+      Sxx += CX[pp] * CX[pp] * d;
+      Syy += CY[pp] * CY[pp] * d;
+      Szz += CZ[pp] * CZ[pp] * d;
+      Sxy += CX[pp] * CY[pp] * d;
+      Sxz += CX[pp] * CZ[pp] * d;
+      Syz += CY[pp] * CZ[pp] * d;
+    }
+    double Syx = Sxy, Szy = Syz, Szx = 0.0;
+    Szz = Sxz;
+    double tprev = s->itime == 1 ? s->cfg.tau_u : tau_prev;
+    double fac = -1.0 / (2 * s->cs2 * rho * tprev * s->cfg.time_dt);
+    double s_norm = fabs(fac) * sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Syx * Syx + Syy * Syy + Syz * Syz +
+                                            Szx * Szx + Szy * Szy + Szz * Szz));
+    double C_smag = s->cfg.C_smag;
+    if (fl & CH4_F_FLUID_LES_VANDRIEST) C_smag = vandriest(s, j);
+    double nu_les = s_norm * pow(C_smag * 1.0, 2.0);
+    return 3.0 * (nu_les + s->cfg.nu) + 0.5;
+  }
   double g[3][3]; /* g[a][b] = d u_a / d x_b  (tens.ab with a=component) */
   int ip = (i + 1) % NX, im = (i + NX - 1) % NX;
   int kp = (k + 1) % NZ, km = (k + NZ - 1) % NZ;
@@ -256,7 +297,35 @@ static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k)
                               (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
                               (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
   double vol = 1.0; /* (dx*dy*dz)^(1/3) on the unit lattice */
-  double nu_les = s_norm * pow(s->cfg.C_smag * vol, 2.0);
+  double C_smag = s->cfg.C_smag;
+  if (fl & CH4_F_FLUID_LES_VANDRIEST) C_smag = vandriest(s, j);
+  double nu_les = s_norm * pow(C_smag * vol, 2.0);
+  if (fl & CH4_F_FLUID_LES_WALE) { /* src/les.c:182-248 */
+    double SSxx = xx, SSyy = yy, SSzz = zz;
+    double SSxy = 0.5 * (xy + yx), SSxz = 0.5 * (xz + zx), SSzy = 0.5 * (zy + yz);
+    double SSyx = SSxy, SSzx = SSxz, SSyz = SSzy;
+    double WWxx = 0.0, WWyy = 0.0, WWzz = 0.0;
+    double WWxy = 0.5 * (xy - yx), WWxz = 0.5 * (xz - zx), WWyz = 0.5 * (zy - yz);
+    double WWyx = -WWxy, WWzx = -WWxz, WWzy = -WWyz;
+    double iso = SSxx * SSxx + SSxy * SSxy + SSxz * SSxz + SSyx * SSyx + SSyy * SSyy + SSyz * SSyz + SSzx * SSzx +
+                 SSzy * SSzy + SSzz * SSzz - WWxx * WWxx - WWxy * WWxy - WWxz * WWxz - WWyx * WWyx - WWyy * WWyy -
+                 WWyz * WWyz - WWzx * WWzx - WWzy * WWzy - WWzz * WWzz;
+    double Jxx = SSxx * SSxx + SSxy * SSyx + SSxz * SSzx + WWxx * WWxx + WWxy * WWyx + WWxz * WWzx - iso / 3.0;
+    double Jxy = SSxx * SSxy + SSxy * SSyy + SSxz * SSzy + WWxx * WWxy + WWxy * WWyy + WWxz * WWzy;
+    double Jxz = SSxx * SSxz + SSxy * SSyz + SSxz * SSzz + WWxx * WWxz + WWxy * WWyz + WWxz * WWzz;
+    double Jyx = SSyx * SSxx + SSyy * SSyx + SSyz * SSzx + WWyx * WWxx + WWyy * WWyx + WWyz * WWzx;
+    double Jyy = SSyx * SSxy + SSyy * SSyy + SSyz * SSzy + WWyx * WWxy + WWyy * WWyy + WWyz * WWzy - iso / 3.0;
+    double Jyz = SSyx * SSxz + SSyy * SSyz + SSyz * SSzz + WWyx * WWxz + WWyy * WWyz + WWyz * WWzz;
+    double Jzx = SSzx * SSxx + SSzy * SSyx + SSzz * SSzx + WWzx * WWxx + WWzy * WWyx + WWzz * WWzx;
+    double Jzy = SSzx * SSxy + SSzy * SSyy + SSzz * SSzy + WWzx * WWxy + WWzy * WWyy + WWzz * WWzy;
+    double Jzz = SSzx * SSxz + SSzy * SSyz + SSzz * SSzz + WWzx * WWxz + WWzy * WWyz + WWzz * WWzz - iso / 3.0;
+    double s_norm2 = pow(s_norm, 2.0) / 2.0;
+    double j_norm2 = Jxx * Jxx + Jxy * Jxy + Jxz * Jxz + Jyx * Jyx + Jyy * Jyy + Jyz * Jyz + Jzx * Jzx + Jzy * Jzy +
+                     Jzz * Jzz;
+    double op_wale = pow(j_norm2, 1.5) / (pow(s_norm2, 2.5) + pow(j_norm2, 1.25));
+    double C_wale = 0.5;
+    nu_les = op_wale * pow(C_wale * vol, 2.0);
+  }
   return 3.0 * (nu_les + s->cfg.nu) + 0.5;
 }
 
@@ -808,10 +877,16 @@ static void one_step(ch4o_state *s) {
         double u2 = (ux * ux + uy * uy + uz * uz);
 
         double invtau = invtau_u;
+        double invtau_cell[3] = {invtau_set[0], invtau_set[1], invtau_set[2]};
         if (c->flags & CH4_F_FLUID_LES) {
-          double tl = les_tau(s, uarr, i, j, k);
+          double tl = les_tau(s, uarr, i, j, k, a, rho, ux, uy, uz, u2, s->tau_les[idx]);
           s->tau_les[idx] = tl;
           invtau = 1.0 / tl;
+          /* tau_t_les / tau_s_les (src/les.c:273-326), turbulent Prandtl and Schmidt 1 */
+          if (c->flags & CH4_F_TEMPERATURE_LES)
+            invtau_cell[1] = 1.0 / (3.0 * (c->kappa + (tl - 0.5 - 3 * c->nu) / (3 * 1.0)) + 0.5);
+          if (c->flags & CH4_F_SCALAR_LES)
+            invtau_cell[2] = 1.0 / (3.0 * (c->chi + (tl - 0.5 - 3 * c->nu) / (3 * 1.0)) + 0.5);
         }
         double post[3][NPOP];
         double feqs[3][NPOP];
@@ -849,9 +924,9 @@ static void one_step(ch4o_state *s) {
             double feq = feqs[set][q];
             double r = b[q];
             if (trt)
-              r += trt_coll(b, feqs[set], q, invtau_set[set], trt_minus(invtau_set[set]));
+              r += trt_coll(b, feqs[set], q, invtau_cell[set], trt_minus(invtau_cell[set]));
             else
-              r += -invtau_set[set] * (b[q] - feq);
+              r += -invtau_cell[set] * (b[q] - feq);
             post[set][q] = r;
           }
         }
@@ -950,6 +1025,7 @@ int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
   for (int q = 7; q < NPOP; q++) s->w[q] = 1. / 36.;
   double cs = 1.0 / sqrt(3.0);
   double cs2 = pow(cs, 2.0), cs4 = pow(cs, 4.0);
+  s->cs2 = cs2;
   s->invcs2 = 1.0 / cs2;
   s->invcs4 = 1.0 / cs4;
   s->invtwocs2 = 1.0 / (2.0 * cs2);

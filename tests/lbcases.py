@@ -41,6 +41,15 @@ CASES = {
                                S_bot=0.2, S_top=0.7, S_ref=0.1, beta_s=0.3, gravity_y=2e-3, gravity_x=1e-3)),
     "les": dict(flagset="les", NX=8, NY=9, NZ=6,
                 params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "les_vd": dict(flagset="les_vd", NX=8, NY=12, NZ=6,
+                   params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "les_ls": dict(flagset="les_ls", NX=8, NY=9, NZ=6,
+                   params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "les_wale": dict(flagset="les_wale", NX=8, NY=9, NZ=6,
+                     params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "les_ts": dict(flagset="les_ts", NX=6, NY=8, NZ=5,
+                   params=dict(tau_u=0.53, tau_t=0.56, tau_s=0.58, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2,
+                               S_bot=0.2, S_top=0.7, S_ref=0.1, beta_s=0.3, gravity_y=2e-3, gravity_x=1e-3)),
     "trt": dict(flagset="trt", NX=8, NY=7, NZ=5,
                 params=dict(tau_u=0.62, tau_t=0.7, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
                             gravity_y=1e-3, gravity_x=2e-4)),
