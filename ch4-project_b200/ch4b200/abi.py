@@ -78,6 +78,7 @@ FLAGS = {
     "LB_SCALAR_LES": 1 << 56,
     "LB_FLUID_LES_WALE": 1 << 57,
     "LB_FLUID_LES_LOCAL_STRAIN": 1 << 58,
+    "LAGRANGE_TWOWAY_TRICUBIC": 1 << 59,
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 

@@ -125,7 +125,7 @@ const uint64_t SUPPORTED =
     CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
     CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND | CH4_F_LAGRANGE_GRAVITY |
     CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES | CH4_F_METHOD_TRT | CH4_F_FLUID_LES_VANDRIEST | CH4_F_TEMPERATURE_LES |
-    CH4_F_SCALAR_LES | CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN;
+    CH4_F_SCALAR_LES | CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN | CH4_F_LAGRANGE_TWOWAY_TRICUBIC;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -657,6 +657,7 @@ struct Engine : EngineBase {
   }
 
   size_t nhome() const { return (size_t)(c.NX + 1) * (c.NY + 1) * (c.NZ + 1); }
+  int nrec() const { return (c.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) ? 15 : 9; }
 
   PartParams<A> part_params() {
     PartParams<A> Q{};
@@ -683,6 +684,8 @@ struct Engine : EngineBase {
     Q.has_t = nsets_on[1];
     Q.key = key;
     Q.order = order;
+    Q.tricubic = (c.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) != 0;
+    Q.nrec = Q.tricubic ? 15 : 9;
     Q.rec = rec;
     Q.srec = srec;
     Q.spid = spid;
@@ -802,8 +805,8 @@ struct Engine : EngineBase {
                     cudaMalloc(&key2, sizeof(unsigned) * n) == cudaSuccess &&
                     cudaMalloc(&order, sizeof(int) * n) == cudaSuccess &&
                     cudaMalloc(&order2, sizeof(int) * n) == cudaSuccess &&
-                    (!twoway() || (cudaMalloc(&rec, sizeof(double) * 9 * (size_t)n) == cudaSuccess &&
-                                   cudaMalloc(&srec, sizeof(double) * 9 * (size_t)n) == cudaSuccess &&
+                    (!twoway() || (cudaMalloc(&rec, sizeof(double) * nrec() * (size_t)n) == cudaSuccess &&
+                                   cudaMalloc(&srec, sizeof(double) * nrec() * (size_t)n) == cudaSuccess &&
                                    cudaMalloc(&spid, sizeof(int) * (size_t)n) == cudaSuccess));
           if (!ok) return H->fail(CH4_ERR_NOMEM, "sort buffers");
           np = n;
@@ -1625,6 +1628,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_SCALAR_LES", CH4_F_SCALAR_LES},
       {"LB_FLUID_LES_WALE", CH4_F_FLUID_LES_WALE},
       {"LB_FLUID_LES_LOCAL_STRAIN", CH4_F_FLUID_LES_LOCAL_STRAIN},
+      {"LAGRANGE_TWOWAY_TRICUBIC", CH4_F_LAGRANGE_TWOWAY_TRICUBIC},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -1727,6 +1731,8 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
     if (!(c->flags & CH4_F_LAGRANGE_WRAP)) return why = "particles need LAGRANGE_WRAP", CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_LAGRANGE_TWOWAY) && !(c->flags & CH4_F_LAGRANGE_TWOWAY_MOMENTUM))
       return why = "LAGRANGE_TWOWAY is implemented with LAGRANGE_TWOWAY_MOMENTUM", CH4_ERR_UNSUPPORTED;
+    if ((c->flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) && !(c->flags & CH4_F_LAGRANGE_TWOWAY))
+      return why = "LAGRANGE_TWOWAY_TRICUBIC needs LAGRANGE_TWOWAY", CH4_ERR_UNSUPPORTED;
     if (!(c->time_dt_lagr_factor >= 1.0)) return why = "time_dt_lagr_factor must be >= 1", CH4_ERR_ARG;
   }
   return CH4_OK;

@@ -57,8 +57,11 @@ struct PartParams {
   unsigned int* key;     // sort keys, by particle index: home cell (+ nh when it deposits nothing)
   int* order;            // sort values, by particle index: the state slot; after the sort, the
                          // state slot of every sorted position
-  double* rec;           // [9][np] per state slot: fac*fp (3), dxm dxp dym dyp dzm dzp
-  double* srec;          // [9][np] the same by sorted position (depositing particles only)
+  int tricubic;          // LAGRANGE_TWOWAY_TRICUBIC: 64-cell cubic deposit
+  int nrec;              // fields of a record: 9 (trilinear) or 15 (tricubic)
+  double* rec;           // [nrec][np] per state slot: fac*fp (3), then dxm dxp dym dyp dzm dzp
+                         // (trilinear) or the cubic weights wx[4] wy[4] wz[4] (tricubic)
+  double* srec;          // [nrec][np] the same by sorted position (depositing particles only)
   int* spid;             // particle index by sorted position
   int2* cell_rng;        // [(NX+1)(NY+1)(NZ+1)] {start, end} of every home cell's sorted run
   // cells whose 8 home cells hold two or more depositing particles, listed per block of
@@ -440,6 +443,14 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
 #undef F
 }
 
+// Keys cubic kernel of the tricubic deposit (src/lagrange_feedback.c:839-848)
+__device__ __forceinline__ double cubic_weight(double x) {
+  x = fabs(x);
+  if (x <= 1.0) return (1.5 * x - 2.5) * x * x + 1.0;
+  if (x < 2.0) return ((-0.5 * x + 2.5) * x - 4.0) * x + 2.0;
+  return 0.0;
+}
+
 // Deposit record and home-cell key of every particle (src/lagrange_feedback.c:34-118).
 template <typename A>
 __global__ void deposit_prepare_kernel(const PartParams<A> P) {
@@ -461,12 +472,21 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
   r[1LL * np + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;
   r[2LL * np + ip] = live ? fac * (F(Dt_uz) - gz + dr * (gz - F(az))) : 0.0;
-  r[3LL * np + ip] = t.dxm;
-  r[4LL * np + ip] = t.dxp;
-  r[5LL * np + ip] = t.dym;
-  r[6LL * np + ip] = t.dyp;
-  r[7LL * np + ip] = t.dzm;
-  r[8LL * np + ip] = t.dzp;
+  if (P.tricubic) {  // cubic weights of the offsets -1 .. 2, src/lagrange_feedback.c:51-60
+#pragma unroll
+    for (int n = -1; n <= 2; n++) {
+      r[(4LL + n) * np + ip] = cubic_weight(t.dxm - (double)n);
+      r[(8LL + n) * np + ip] = cubic_weight(t.dym - (double)n);
+      r[(12LL + n) * np + ip] = cubic_weight(t.dzm - (double)n);
+    }
+  } else {
+    r[3LL * np + ip] = t.dxm;
+    r[4LL * np + ip] = t.dxp;
+    r[5LL * np + ip] = t.dym;
+    r[6LL * np + ip] = t.dyp;
+    r[7LL * np + ip] = t.dzm;
+    r[8LL * np + ip] = t.dzp;
+  }
   // particles that deposit nothing sort after every home cell (still in spatial
   // order among themselves) and are never merged
   const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km + 1);
@@ -519,8 +539,7 @@ __global__ void cell_range_kernel(const PartParams<A> P, const unsigned int* key
   if (i == n - 1 || key[i + 1] != k) P.cell_rng[k].y = i + 1;
   const int s = slot_of[i];
   P.spid[i] = P.pid[s];
-#pragma unroll
-  for (int f = 0; f < 9; f++) P.srec[(long long)f * n + i] = P.rec[(long long)f * n + s];
+  for (int f = 0; f < P.nrec; f++) P.srec[(long long)f * n + i] = P.rec[(long long)f * n + s];
 }
 
 // home cell h (bit 0: +x, bit 1: +y, bit 2: +z) of lattice cell (i, j, k) in shifted
@@ -647,6 +666,55 @@ __global__ void deposit_busy_kernel(const PartParams<A> P, int nregions) {
     P.dep[P.N + cidx] = (A)acc1;
     P.dep[2 * P.N + cidx] = (A)acc2;
   }
+}
+
+// Tricubic deposit (LAGRANGE_TWOWAY_TRICUBIC, src/lagrange_feedback.c:117-146): a particle
+// with lower stencil corner im adds to the cells im-1 .. im+2 on each axis with the
+// weight wx[a] * wy[b] * wz[c], so a cell merges the 64 home cells around it, in
+// particle-index order (the heads kept in a small local array), halo cells dropped.
+template <typename A>
+__global__ void deposit_tricubic_kernel(const PartParams<A> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.NX) return;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
+  const int HX = P.NX + 1, HY = P.NY + 1, HZ = P.NZ + 1;
+  int pos[64], endp[64];
+  int m = 0;
+  for (int h = 0; h < 64; h++) {
+    // home (shifted by one) of the particles whose offset from this cell is a-1 on x etc.
+    const int a = h & 3, b = (h >> 2) & 3, c = h >> 4;
+    const int hx = i - a + 2, hy = j - b + 2, hz = k - c + 2;
+    pos[h] = endp[h] = 0;
+    if (hx < 0 || hx >= HX || hy < 0 || hy >= HY || hz < 0 || hz >= HZ) continue;
+    const int2 rg = P.cell_rng[((long long)hz * HY + hy) * HX + hx];
+    pos[h] = rg.x;
+    endp[h] = rg.y;
+    m += rg.y - rg.x;
+  }
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  const long long np = P.np;
+  const double* __restrict__ r = P.srec;
+  for (int left = m; left > 0; left--) {
+    int best = -1, bv = 0x7fffffff;
+    for (int h = 0; h < 64; h++)
+      if (pos[h] < endp[h]) {
+        const int v = P.spid[pos[h]];
+        if (v < bv) {
+          bv = v;
+          best = h;
+        }
+      }
+    const int slot = pos[best]++;
+    const int a = best & 3, b = (best >> 2) & 3, c = best >> 4;
+    const double w = r[(3 + a) * np + slot] * r[(7 + b) * np + slot] * r[(11 + c) * np + slot];
+    acc0 += r[slot] * w;
+    acc1 += r[np + slot] * w;
+    acc2 += r[2 * np + slot] * w;
+  }
+  P.dep[cidx] = (A)acc0;
+  P.dep[P.N + cidx] = (A)acc1;
+  P.dep[2 * P.N + cidx] = (A)acc2;
 }
 
 #endif  // __CUDACC__

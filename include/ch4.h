@@ -103,6 +103,7 @@ enum {
   CH4_F_SCALAR_LES = 1ull << 56,              /* scalar relaxation time from the LES one */
   CH4_F_FLUID_LES_WALE = 1ull << 57,          /* WALE eddy viscosity */
   CH4_F_FLUID_LES_LOCAL_STRAIN = 1ull << 58,  /* |S| from the populations' stress tensor */
+  CH4_F_LAGRANGE_TWOWAY_TRICUBIC = 1ull << 59, /* 64-cell cubic deposit, src/lagrange_feedback.c:117-146 */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63

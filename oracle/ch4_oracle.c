@@ -676,6 +676,14 @@ static void wrap_particles(ch4o_state *s) {
  * as the reference's border fold adds interior values into the halo and never
  * the reverse (src/lagrange_feedback.c:525-835).  Particles of zero or undefined
  * volume (tracers, beta = 0, probes) add nothing. */
+/* cubic kernel of the tricubic deposit (src/lagrange_feedback.c:839-848) */
+static double cubic_weight(double x) {
+  x = fabs(x);
+  if (x <= 1.0) return (1.5 * x - 2.5) * x * x + 1.0;
+  if (x < 2.0) return ((-0.5 * x + 2.5) * x - 4.0) * x + 2.0;
+  return 0.0;
+}
+
 static void deposit(const ch4o_state *s, double *D) {
   memset(D, 0, sizeof(double) * 3 * s->N);
   for (int ip = 0; ip < s->npart; ip++) {
@@ -692,6 +700,23 @@ static void deposit(const ch4o_state *s, double *D) {
     fp[0] = p->Dt_ux - gx + dr * (gx - p->ax);
     fp[1] = p->Dt_uy - gy + dr * (gy - p->ay);
     fp[2] = p->Dt_uz - gz + dr * (gz - p->az);
+    if (s->cfg.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) { /* src/lagrange_feedback.c:51-60, 117-146 */
+      double wx[4], wy[4], wz[4];
+      for (int n = -1; n <= 2; n++) {
+        wx[n + 1] = cubic_weight(t.dxm - (double)n);
+        wy[n + 1] = cubic_weight(t.dym - (double)n);
+        wz[n + 1] = cubic_weight(t.dzm - (double)n);
+      }
+      for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++)
+          for (int c = 0; c < 4; c++) {
+            int i = t.im + (a - 1), j = t.jm + (b - 1), k = t.km + (c - 1);
+            if (i < 0 || i >= s->NX || j < 0 || j >= s->NY || k < 0 || k >= s->NZ) continue;
+            double w = wx[a] * wy[b] * wz[c];
+            for (int q = 0; q < 3; q++) D[3 * cidx(s, i, j, k) + q] += fac * fp[q] * w;
+          }
+      continue;
+    }
     for (int a = 0; a < 3; a++)
       for (int c = 0; c < 8; c++) {
         int i = t.im + CORNER[c][0], j = t.jm + CORNER[c][1], k = t.km + CORNER[c][2];

@@ -56,6 +56,9 @@ FLAGSETS = {
     "les_ts": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_FLUID_BC_Y_M_SLIP", "LB_TEMPERATURE",
                "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LB_SCALAR", "LB_SCALAR_BUOYANCY", "LB_SCALAR_BC_Y",
                "LB_FLUID_LES", "LB_TEMPERATURE_LES", "LB_SCALAR_LES"],
+    "particles_tc": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                     "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                     "LAGRANGE_TWOWAY_TRICUBIC"],
     "particles_fa": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
                      "LAGRANGE_OUTPUT_FLUID_AVERAGES"],

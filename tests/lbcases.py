@@ -63,6 +63,9 @@ CASES = {
                                T_ref=0.5, beta_t=0.3, gravity_y=2e-3, gravity_x=1e-3)),
     "cpower": dict(flagset="cpower", NX=8, NY=7, NZ=6,
                    params=dict(tau_u=0.57, Amp_x=1e-9, Amp_y=8e-10, Amp_z=5e-10, seed=3)),
+    "particles_tc": dict(flagset="particles_tc", NX=10, NY=8, NZ=7, npart=300,
+                         params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=9,
+                                     time_dt_lagr_factor=2.0, particle_number=300)),
     "particles_1w": dict(flagset="particles_1w", NX=10, NY=8, NZ=7, npart=300,
                          params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=8,
                                      time_dt_lagr_factor=2.0, particle_number=300)),

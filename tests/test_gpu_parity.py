@@ -48,7 +48,7 @@ def rel_l2(a, b):
                                           ("scalar", 25), ("les", 25), ("particles", 12),
                                           ("particles_t", 12), ("particles_g", 12), ("particles_1w", 12),
                                           ("trt", 25), ("trt_les", 25), ("les_vd", 25), ("les_ls", 25),
-                                          ("les_ts", 25)])
+                                          ("les_ts", 25), ("particles_tc", 12)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):
     _, cfg, state = make_case(name, seed=11)
     ref = run_restatement(cfg, state, nsteps)
@@ -71,7 +71,8 @@ def test_fp64_bit_identical_to_oracle(name, nsteps):
 
 
 @pytest.mark.parametrize("name", ["kolmogorov", "rb", "hit", "walls2", "scalar", "les", "particles",
-                                  "particles_t", "particles_g", "trt", "trt_les", "les_vd", "les_ls", "les_ts"])
+                                  "particles_t", "particles_g", "trt", "trt_les", "les_vd", "les_ls", "les_ts",
+                                  "particles_tc"])
 def test_fp64_matches_compiled_reference(name):
     flagset, cfg, state = make_case(name, seed=5)
     if not O.ref_available(flagset):

@@ -25,7 +25,7 @@ def _assert_same(a, b, what):
                                           ("scalar", 20), ("les", 20), ("particles", 8),
                                           ("particles_t", 8), ("particles_g", 8), ("particles_1w", 8),
                                           ("trt", 20), ("trt_les", 20), ("les_vd", 20), ("les_ls", 20),
-                                          ("les_wale", 20), ("les_ts", 20), ("nozero", 15),
+                                          ("les_wale", 20), ("les_ts", 20), ("particles_tc", 8), ("nozero", 15),
                                           ("cpower", 15)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
