@@ -120,9 +120,9 @@ struct CellState {
 
 // Collision of direction q for all enabled sets, in place.  FMODE 0 / 1: unforced /
 // forced, fixed at compile time (the cell branches once, so the two forms are never both
-// issued under predication; FP32 store: 13 % fewer instructions with a force); FMODE 2:
-// decided per direction at run time (FP64 and FP16 stores: with the split the FP64
-// fluid+thermal kernel needs 164 registers instead of 128 and ran 5 % slower).
+// issued under predication; FP32 store: 13 % fewer instructions with a force, FP16 store:
+// +3 % measured); FMODE 2: decided per direction at run time (FP64: with the split its
+// fluid+thermal kernel needed 164 registers instead of 128 and ran 5 % slower).
 template <int q, bool EXACT, bool THERM, bool SCAL, int FMODE, typename A>
 __device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellState<A>& c, bool forcing, A* f, A* g,
                                             A* h) {
@@ -332,7 +332,7 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
     // the antisymmetric rate from the cell's own rate (LES) or the set's
     const A wm = LES ? trt_minus(c.invtau) : P.invtau_m[0];
     collide_trt<EXACT, THERM, SCAL>(P, c, forcing, wm, f, g, h);
-  } else if constexpr (sizeof(S) == 4) {
+  } else if constexpr (!EXACT) {
     if (forcing) {
       CH4_COLS(1)
     } else {
