@@ -13,13 +13,67 @@ The transfer is the caller's plumbing: `exchange` pairs the four point-to-point
 transfers of one step over a torch.distributed process group (NCCL between GPUs,
 gloo on CPU); `step_local` runs several slabs of one process, each unpacking straight
 from its neighbours' send buffers.
+
+With LB_FLUID_FORCING_NOZEROMODE / _CONSTANT_POWER every step also needs the force summed
+over the whole lattice: each slab's handle calls back (ch4_set_gather) with its block
+partial sums, and the callback gathers every slab's in z order -- an all-gather over the
+process group (`Slab.use_process_group`), or, for the slabs of one process stepped in
+threads, through host memory (`LocalGather`).
 """
 import ctypes as C
+import threading
 
 import numpy as np
 
 from . import Simulation, lib
 from . import abi
+
+
+GATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
+
+
+class _DeviceBytes:
+    """A device byte range as a __cuda_array_interface__ object (zero-copy torch view)."""
+
+    def __init__(self, ptr, nbytes):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _view(ptr, nbytes):
+    import torch
+    return torch.as_tensor(_DeviceBytes(ptr, nbytes), device="cuda")
+
+
+class LocalGather:
+    """The force-sum gather of n slabs of one process, each stepped in its own thread:
+    every slab copies its partials to host memory, waits for the others, and copies
+    the whole z-ordered set back to its device buffer on its stream."""
+
+    def __init__(self, n):
+        self.n = n
+        self.slots = [None] * n
+        self.barrier = threading.Barrier(n)
+
+    def callback(self, index):
+        import torch
+
+        def cb(local, all_, nbytes, stream, user):
+            try:
+                st = torch.cuda.ExternalStream(stream)
+                with torch.cuda.stream(st):
+                    self.slots[index] = _view(local, nbytes).cpu()
+                self.barrier.wait()
+                whole = torch.cat(self.slots)
+                with torch.cuda.stream(st):
+                    _view(all_, nbytes * self.n).copy_(whole)
+                    st.synchronize()
+                self.barrier.wait()  # nobody refills a slot before every slab has read them all
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a failed gather
+                self.barrier.abort()
+                return 1
+        return GATHER_FN(cb)
 
 
 def bounds(nz, nslabs):
@@ -82,6 +136,29 @@ class Slab:
         self.send_down, self.send_up, self.recv_up, self.recv_down = (
             torch.empty(n.value, dtype=torch.uint8, device=dev) for _ in range(4))
 
+    def set_gather(self, fn, nslabs):
+        """Register the force-sum gather (a GATHER_FN); kept alive with the slab."""
+        self._gather = fn
+        self.sim._check(lib().ch4_set_gather(self.sim.h, C.cast(fn, C.c_void_p), nslabs, None), "set_gather")
+
+    def use_process_group(self, rank, world, group=None):
+        """Gather the force sums with an all-gather over the process group (z order = rank order)."""
+        import torch
+        import torch.distributed as dist
+
+        def cb(local, all_, nbytes, stream, user):
+            try:
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                    loc, whole = _view(local, nbytes), _view(all_, nbytes * world)
+                    if world == 1:
+                        whole.copy_(loc)
+                    else:
+                        dist.all_gather_into_tensor(whole, loc, group=group)
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a failed gather
+                return 1
+        self.set_gather(GATHER_FN(cb), world)
+
     def set_pop(self, which, aos_whole):
         """Populations of the whole lattice, AoS [NZ][NY][NX][19]: this slab's planes."""
         self.sim.set_pop(which, np.ascontiguousarray(aos_whole[self.z0:self.z0 + self.nz]))
@@ -112,13 +189,54 @@ class Slab:
         self.sim.close()
 
 
+def _in_threads(slabs, fn):
+    """fn(slab) for every slab at once, one thread each (the force-sum gather of slabs of
+    one process meets in the middle of their steps)."""
+    errs = []
+
+    def run(s):
+        try:
+            fn(s)
+        except Exception as e:  # noqa: BLE001 - re-raised below
+            errs.append(e)
+    ts = [threading.Thread(target=run, args=(s,)) for s in slabs]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    if errs:
+        raise errs[0]
+
+
+def use_local_gather(slabs):
+    """Slabs of one process: gather the force sums through host memory (step_local and
+    initialize_local then run the slabs in threads)."""
+    g = LocalGather(len(slabs))
+    for i, s in enumerate(slabs):
+        s.set_gather(g.callback(i), len(slabs))
+        s.local_gather = True
+
+
+def initialize_local(slabs):
+    if any(getattr(s, "local_gather", False) for s in slabs):
+        _in_threads(slabs, lambda s: s.sim.initialize())
+    else:
+        for s in slabs:
+            s.sim.initialize()
+
+
 def step_local(slabs, n):
     """n steps of the slabs of one process (in z order): every slab unpacks straight
     from its neighbours' send buffers once all have packed."""
     m = len(slabs)
+    threaded = any(getattr(s, "local_gather", False) for s in slabs)
     for _ in range(n):
+        if threaded:
+            _in_threads(slabs, lambda s: s.sim.step(1))
+        else:
+            for s in slabs:
+                s.sim.step(1)
         for s in slabs:
-            s.sim.step(1)
             s.pack()
         for s in slabs:
             s.sim.synchronize()

@@ -326,6 +326,10 @@ struct ch4_handle {
   Lattice lat;
   // running rulers of ch4_dump_averages (ruler_*_running, src/output.c:765-768)
   std::vector<double> run[3];
+  // z-slab: the caller's gather of every slab's force sums
+  ch4_gather_fn gather = nullptr;
+  void* gather_user = nullptr;
+  int nslabs = 1;
 
   ch4_status fail(ch4_status s, const char* fmt, ...) {
     char buf[512];
@@ -578,6 +582,7 @@ struct Engine : EngineBase {
   // last step's (fm_i) and the one being built; reduction scratch
   A* fmbuf = nullptr;
   double* fmpart = nullptr;
+  double* fmall = nullptr;  // z-slab: every slab's block sums
   int fm_nblocks = 0, fm_i = 0;
   bool fmoments() const { return (c.flags & (CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER)) != 0; }
   const A* fm_last() const { return fmbuf ? fmbuf + 6 * fm_i : nullptr; }
@@ -628,6 +633,7 @@ struct Engine : EngineBase {
     cudaFree(pstatus);
     cudaFree(fmbuf);
     cudaFree(fmpart);
+    cudaFree(fmall);
   }
 
   void free_particles() {
@@ -1245,8 +1251,22 @@ struct Engine : EngineBase {
 
   ch4_status force_moments(const A* hit_cur, int with_prev, A* out) {
     const double amp[3] = {c.Amp_x, c.Amp_y, c.Amp_z};
-    const double norm = 1.0 / ((double)c.NX * (double)c.NY * (double)c.NZ);  // src/forcing.c:1139
-    return H->cuda(launch_force_moments(P, shape, hit_cur, with_prev, fmpart, fm_nblocks, norm, amp, out, H->stream),
+    const double norm = 1.0 / ((double)c.NX * (double)c.NY * (double)H->nz_all());  // src/forcing.c:1139
+    if (c.nz_global <= 0)
+      return H->cuda(launch_force_moments(P, shape, hit_cur, with_prev, fmpart, fm_nblocks, norm, amp, out, H->stream),
+                     "force corrections");
+    // z-slab: this slab's block sums, every slab's gathered in z order, the same corrections everywhere
+    if (!H->gather) return H->fail(CH4_ERR_STATE, "z-slab with global force corrections: no ch4_set_gather");
+    ch4_status st = H->cuda(
+        launch_force_moments(P, shape, hit_cur, with_prev, fmpart, fm_nblocks, norm, amp, out, H->stream, 1),
+        "force sums");
+    if (st) return st;
+    const size_t bytes = sizeof(double) * FM_SUMS * 2 * (size_t)fm_nblocks;
+    if (!fmall && cudaMalloc(&fmall, bytes * H->nslabs) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "gathered sums");
+    if (H->gather(fmpart, fmall, bytes, H->stream, H->gather_user) != 0)
+      return H->fail(CH4_ERR_CUDA, "the gather of the slabs' force sums failed");
+    return H->cuda(launch_force_moments(P, shape, hit_cur, with_prev, fmall, fm_nblocks * H->nslabs, norm, amp, out,
+                                        H->stream, 2),
                    "force corrections");
   }
 
@@ -1700,8 +1720,8 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
     if (c->nz_global > 65535) return why = "nz_global must be <= 65535", CH4_ERR_ARG;
     // z-slabs exchange populations only: no z-halo of u (LES), no global sums inside
     // the step (force corrections), no particle migration
-    if (c->flags & (CH4_F_FLUID_LES | CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_LAGRANGE))
-      return why = "z-slab handles run without LES, global force corrections and particles", CH4_ERR_UNSUPPORTED;
+    if (c->flags & (CH4_F_FLUID_LES | CH4_F_LAGRANGE))
+      return why = "z-slab handles run without LES and particles", CH4_ERR_UNSUPPORTED;
   }
   if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
     return why = "walls need NY >= 3", CH4_ERR_ARG;
@@ -2040,6 +2060,15 @@ ch4_status ch4_dump_averages(ch4_handle* h, const char* dir, double time_now, in
     const std::vector<int> fs = {DS, DS2, DEPSS, DDXS, DDYS, DDZS, DUXS, DUYS, DUZS, DNUSX, DNUSY, DNUSZ};
     if (!block("scalar_averages", fs, fs)) return h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
   }
+  return CH4_OK;
+}
+
+ch4_status ch4_set_gather(ch4_handle* h, ch4_gather_fn gather, int nslabs, void* user) {
+  if (!h || !gather || nslabs < 1) return CH4_ERR_ARG;
+  if (h->cfg.nz_global <= 0) return h->fail(CH4_ERR_ARG, "ch4_set_gather is for z-slab handles");
+  h->gather = gather;
+  h->gather_user = user;
+  h->nslabs = nslabs;
   return CH4_OK;
 }
 

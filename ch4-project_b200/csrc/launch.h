@@ -31,13 +31,14 @@ cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float*
                          double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
                          float* ut4 = nullptr);
 // global force corrections (NOZEROMODE / CONSTANT_POWER) of one step into fm[6];
-// partial holds nblocks * 9 * 2 doubles
+// partial holds nblocks * 9 * 2 doubles.  stage 0: sums and corrections; 1: the block
+// sums only; 2: the corrections from nblocks partials (e.g. gathered from every z-slab)
 cudaError_t launch_force_moments(const StepParams<double>& P, LaunchShape s, const double* hit_cur, int with_prev,
                                  double* partial, int nblocks, double norm, const double* amp, double* fm,
-                                 cudaStream_t st);
+                                 cudaStream_t st, int stage = 0);
 cudaError_t launch_force_moments(const StepParams<float>& P, LaunchShape s, const float* hit_cur, int with_prev,
                                  double* partial, int nblocks, double norm, const double* amp, float* fm,
-                                 cudaStream_t st);
+                                 cudaStream_t st, int stage = 0);
 // compact AoS chunk <-> SoA storage for one population set
 cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st);

@@ -23,9 +23,10 @@ cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float*
 }
 cudaError_t launch_force_moments(const StepParams<float>& P, LaunchShape s, const float* hit_cur, int with_prev,
                                  double* partial, int nblocks, double norm, const double* amp, float* fm,
-                                 cudaStream_t st) {
-  return s.storage == 2 ? force_moments_t<__half, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st)
-                        : force_moments_t<float, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st);
+                                 cudaStream_t st, int stage) {
+  return s.storage == 2
+             ? force_moments_t<__half, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st, stage)
+             : force_moments_t<float, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st, stage);
 }
 cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st) {

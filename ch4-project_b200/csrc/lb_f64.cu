@@ -65,8 +65,8 @@ cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const doubl
 }
 cudaError_t launch_force_moments(const StepParams<double>& P, LaunchShape s, const double* hit_cur, int with_prev,
                                  double* partial, int nblocks, double norm, const double* amp, double* fm,
-                                 cudaStream_t st) {
-  return force_moments_t<double, double>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st);
+                                 cudaStream_t st, int stage) {
+  return force_moments_t<double, double>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st, stage);
 }
 cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st) {

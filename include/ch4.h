@@ -284,6 +284,16 @@ ch4_status ch4_halo_bytes(ch4_handle *h, size_t *bytes);
 ch4_status ch4_halo_pack(ch4_handle *h, void *send_down, void *send_up);
 ch4_status ch4_halo_unpack(ch4_handle *h, const void *from_up, const void *from_down);
 
+/* Sums over the whole lattice from z-slabs: LB_FLUID_FORCING_NOZEROMODE and
+ * _CONSTANT_POWER need the force summed over every cell.  A slab handle forms its
+ * block partial sums (double-double, `bytes` of device memory) and calls `gather`, which
+ * must fill `all` with the partials of every slab in z order (nslabs * bytes, device)
+ * before work later on `stream` reads them (e.g. an all-gather on that stream), and
+ * return 0.  Every slab then forms the same corrections from the same numbers.
+ * Registered once per slab handle, before ch4_initialize; required for those flags. */
+typedef int (*ch4_gather_fn)(const void *local, void *all, size_t bytes, void *stream, void *user);
+ch4_status ch4_set_gather(ch4_handle *h, ch4_gather_fn gather, int nslabs, void *user);
+
 /* --- Lagrangian averages per particle type (dump_particle_averages) ------------ */
 
 /* Per type: the particle count, then the means of v, v^2, v^4, a, a^2, a^4 (per
