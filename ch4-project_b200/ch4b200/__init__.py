@@ -88,6 +88,7 @@ def lib():
         L.ch4_halo_pack.argtypes = [P, C.c_void_p, C.c_void_p]
         L.ch4_halo_unpack.argtypes = [P, C.c_void_p, C.c_void_p]
         L.ch4_set_gather.argtypes = [P, C.c_void_p, C.c_int, C.c_void_p]
+        L.ch4_set_exchange.argtypes = [P, C.c_void_p, C.c_void_p]
         L.ch4_dump_particle_averages.argtypes = [P, C.c_char_p, C.c_double]
         V = C.c_void_p
         L.ch4_averages_noalloc.argtypes = [V, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,

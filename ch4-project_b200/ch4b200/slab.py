@@ -19,6 +19,11 @@ over the whole lattice: each slab's handle calls back (ch4_set_gather) with its 
 partial sums, and the callback gathers every slab's in z order -- an all-gather over the
 process group (`Slab.use_process_group`), or, for the slabs of one process stepped in
 threads, through host memory (`LocalGather`).
+
+With LB_FLUID_LES the eddy viscosity differentiates u across the z faces: in the middle
+of every step each slab's handle calls back (ch4_set_exchange) with the u of its bottom
+and top planes, and the callback swaps them with the neighbours -- point to point over
+the process group, or between the threads of one process (`LocalExchange`).
 """
 import ctypes as C
 import threading
@@ -30,6 +35,8 @@ from . import abi
 
 
 GATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                          C.c_void_p)
 
 
 class _DeviceBytes:
@@ -74,6 +81,38 @@ class LocalGather:
                 self.barrier.abort()
                 return 1
         return GATHER_FN(cb)
+
+
+class LocalExchange:
+    """The u-face exchange of n slabs of one process (one device), each stepped in its
+    own thread: every slab publishes its send buffers once its stream has written them,
+    then copies its neighbours' into its own receive buffers."""
+
+    def __init__(self, n):
+        self.n = n
+        self.sends = [None] * n
+        self.barrier = threading.Barrier(n)
+
+    def callback(self, index):
+        import torch
+
+        def cb(send_down, send_up, from_up, from_down, nbytes, stream, user):
+            try:
+                st = torch.cuda.ExternalStream(stream)
+                st.synchronize()
+                self.sends[index] = (send_down, send_up)
+                self.barrier.wait()
+                above, below = self.sends[(index + 1) % self.n], self.sends[(index - 1) % self.n]
+                with torch.cuda.stream(st):
+                    _view(from_up, nbytes).copy_(_view(above[0], nbytes))
+                    _view(from_down, nbytes).copy_(_view(below[1], nbytes))
+                    st.synchronize()
+                self.barrier.wait()  # no slab rewrites its send buffers before all have read them
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a failed exchange
+                self.barrier.abort()
+                return 1
+        return EXCHANGE_FN(cb)
 
 
 def bounds(nz, nslabs):
@@ -141,10 +180,26 @@ class Slab:
         self._gather = fn
         self.sim._check(lib().ch4_set_gather(self.sim.h, C.cast(fn, C.c_void_p), nslabs, None), "set_gather")
 
+    def set_exchange(self, fn):
+        """Register the u-face exchange (an EXCHANGE_FN) for LES; kept alive with the slab."""
+        self._exchange = fn
+        self.sim._check(lib().ch4_set_exchange(self.sim.h, C.cast(fn, C.c_void_p), None), "set_exchange")
+
     def use_process_group(self, rank, world, group=None):
-        """Gather the force sums with an all-gather over the process group (z order = rank order)."""
+        """Gather the force sums with an all-gather over the process group (z order = rank
+        order) and swap the LES u faces point to point with the neighbouring ranks."""
         import torch
         import torch.distributed as dist
+
+        def xcb(send_down, send_up, from_up, from_down, nbytes, stream, user):
+            try:
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                    exchange(_view(send_down, nbytes), _view(send_up, nbytes), _view(from_up, nbytes),
+                             _view(from_down, nbytes), rank, world, group)
+                return 0
+            except Exception:  # noqa: BLE001 - reported to the library as a failed exchange
+                return 1
+        self.set_exchange(EXCHANGE_FN(xcb))
 
         def cb(local, all_, nbytes, stream, user):
             try:
@@ -214,6 +269,15 @@ def use_local_gather(slabs):
     g = LocalGather(len(slabs))
     for i, s in enumerate(slabs):
         s.set_gather(g.callback(i), len(slabs))
+        s.local_gather = True
+
+
+def use_local_exchange(slabs):
+    """Slabs of one process with LES: swap the u faces between their threads
+    (step_local then runs the slabs in threads)."""
+    x = LocalExchange(len(slabs))
+    for i, s in enumerate(slabs):
+        s.set_exchange(x.callback(i))
         s.local_gather = True
 
 

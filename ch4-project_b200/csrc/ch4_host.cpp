@@ -330,6 +330,9 @@ struct ch4_handle {
   ch4_gather_fn gather = nullptr;
   void* gather_user = nullptr;
   int nslabs = 1;
+  // z-slab with LES: the caller's exchange of the u planes at the faces
+  ch4_exchange_fn exchange = nullptr;
+  void* exchange_user = nullptr;
 
   ch4_status fail(ch4_status s, const char* fmt, ...) {
     char buf[512];
@@ -540,6 +543,7 @@ struct Engine : EngineBase {
   A *tprev = nullptr, *sprev = nullptr;
   A *kol = nullptr;
   A *ules = nullptr, *tau_les = nullptr;
+  A* uhalo = nullptr;  // z-slab LES: u faces sent down | up, received from up | down
   A* vd = nullptr;  // LB_FLUID_LES_VANDRIEST: pow(C_smag(y), 2) per row
   A *hit_ring = nullptr;  // (CHUNK+1) phase-table slots
   A *hit_last = nullptr;  // tables of the latest phases (those of F^n)
@@ -610,6 +614,7 @@ struct Engine : EngineBase {
     cudaFree(kol);
     cudaFree(ules);
     cudaFree(tau_les);
+    cudaFree(uhalo);
     cudaFree(vd);
     cudaFree(hit_ring);
     cudaFree(hit_last);
@@ -1082,6 +1087,7 @@ struct Engine : EngineBase {
     P.tprev = tprev;
     P.sprev = sprev;
     P.ules = ules;
+    P.ules_lo = P.ules_hi = nullptr;
     P.tau_les = tau_les;
     P.kol = kol;
     P.csmag2_y = vd;
@@ -1272,9 +1278,30 @@ struct Engine : EngineBase {
 
   ch4_status les_u() {
     // u^n with dt/2 F^{n-1}: prev tables are P.hit_prev
-    return H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                ules, H->stream),
-                   "les u");
+    ch4_status st = H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, nullptr, nullptr,
+                                         nullptr, ules, H->stream),
+                            "les u");
+    if (st || c.nz_global <= 0) return st;
+    // z-slab: u of the bottom plane down, of the top plane up, the neighbours' back
+    if (!H->exchange) return H->fail(CH4_ERR_STATE, "z-slab with LES: no ch4_set_exchange");
+    const size_t nxy = (size_t)c.NX * c.NY, part = 3 * nxy;
+    if (!uhalo && cudaMalloc(&uhalo, 4 * part * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u halo");
+    A *send_down = uhalo, *send_up = uhalo + part, *from_up = uhalo + 2 * part, *from_down = uhalo + 3 * part;
+    HaloCopy hc{};
+    for (int a = 0; a < 3; a++) {
+      hc.src[hc.n] = ules + (size_t)a * N;
+      hc.dst[hc.n] = send_down + (size_t)a * nxy;
+      hc.bytes[hc.n++] = nxy * sizeof(A);
+      hc.src[hc.n] = ules + (size_t)a * N + (size_t)(c.NZ - 1) * nxy;
+      hc.dst[hc.n] = send_up + (size_t)a * nxy;
+      hc.bytes[hc.n++] = nxy * sizeof(A);
+    }
+    if ((st = H->cuda(launch_halo_copy(hc, H->stream), "u faces"))) return st;
+    if (H->exchange(send_down, send_up, from_up, from_down, part * sizeof(A), H->stream, H->exchange_user) != 0)
+      return H->fail(CH4_ERR_CUDA, "the exchange of the slabs' u planes failed");
+    P.ules_lo = from_down;
+    P.ules_hi = from_up;
+    return CH4_OK;
   }
 
   ch4_status step(int n) override {
@@ -1720,8 +1747,7 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
     if (c->nz_global > 65535) return why = "nz_global must be <= 65535", CH4_ERR_ARG;
     // z-slabs exchange populations only: no z-halo of u (LES), no global sums inside
     // the step (force corrections), no particle migration
-    if (c->flags & (CH4_F_FLUID_LES | CH4_F_LAGRANGE))
-      return why = "z-slab handles run without LES and particles", CH4_ERR_UNSUPPORTED;
+    if (c->flags & CH4_F_LAGRANGE) return why = "z-slab handles run without particles", CH4_ERR_UNSUPPORTED;
   }
   if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
     return why = "walls need NY >= 3", CH4_ERR_ARG;
@@ -2069,6 +2095,14 @@ ch4_status ch4_set_gather(ch4_handle* h, ch4_gather_fn gather, int nslabs, void*
   h->gather = gather;
   h->gather_user = user;
   h->nslabs = nslabs;
+  return CH4_OK;
+}
+
+ch4_status ch4_set_exchange(ch4_handle* h, ch4_exchange_fn exchange, void* user) {
+  if (!h || !exchange) return CH4_ERR_ARG;
+  if (h->cfg.nz_global <= 0) return h->fail(CH4_ERR_ARG, "ch4_set_exchange is for z-slab handles");
+  h->exchange = exchange;
+  h->exchange_user = user;
   return CH4_OK;
 }
 

@@ -83,6 +83,8 @@ struct StepParams {
   A* sprev;
   // LES: u^n (3 SoA planes) and per-cell relaxation time output
   const A* ules;
+  const A* ules_lo;  // z-slab: u of the plane under the slab (3 planes of NX*NY), else null
+  const A* ules_hi;  // z-slab: u of the plane over the slab
   A* tau_les;
   // two-way coupling deposit of this and the previous step (3 SoA planes each)
   const A* dcur;

@@ -220,10 +220,16 @@ __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z
     auto at = [&](int a, int i, int j, int k) { return u[a * N + ((long long)k * NY + j) * NX + i]; };
     A g[3][3];
     const int xp = wrap(x + 1, NX), xm = wrap(x - 1, NX), zp = wrap(z + 1, NZ), zm = wrap(z - 1, NZ);
+    // z-slab: the planes beyond the slab's faces come from its neighbours
+    const long long nxy = (long long)NX * NY, inplane = (long long)y * NX + x;
+    const A* up_hi = (z == NZ - 1 && P.ules_hi) ? P.ules_hi : nullptr;
+    const A* up_lo = (z == 0 && P.ules_lo) ? P.ules_lo : nullptr;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       g[a][0] = (at(a, xp, y, z) - at(a, xm, y, z)) / A(2);
-      g[a][2] = (at(a, x, y, zp) - at(a, x, y, zm)) / A(2);
+      const A vp = up_hi ? up_hi[a * nxy + inplane] : at(a, x, y, zp);
+      const A vm = up_lo ? up_lo[a * nxy + inplane] : at(a, x, y, zm);
+      g[a][2] = (vp - vm) / A(2);
     }
     const bool walls = (F & K_FWALL) != 0;
     if (walls && y == 0) {

@@ -294,6 +294,15 @@ ch4_status ch4_halo_unpack(ch4_handle *h, const void *from_up, const void *from_
 typedef int (*ch4_gather_fn)(const void *local, void *all, size_t bytes, void *stream, void *user);
 ch4_status ch4_set_gather(ch4_handle *h, ch4_gather_fn gather, int nslabs, void *user);
 
+/* LES on z-slabs: the eddy viscosity takes d u / d z across the slab faces, so every
+ * step the slab sends the u of its bottom plane down and of its top plane up (3 x NX*NY
+ * values each, arithmetic precision) and needs its neighbours' in return.  `exchange`
+ * must deliver send_down to the slab below (its from_up) and send_up to the slab above
+ * (its from_down), ordered on `stream`, and return 0.  Required with LB_FLUID_LES. */
+typedef int (*ch4_exchange_fn)(const void *send_down, const void *send_up, void *from_up, void *from_down,
+                               size_t bytes, void *stream, void *user);
+ch4_status ch4_set_exchange(ch4_handle *h, ch4_exchange_fn exchange, void *user);
+
 /* --- Lagrangian averages per particle type (dump_particle_averages) ------------ */
 
 /* Per type: the particle count, then the means of v, v^2, v^4, a, a^2, a^4 (per

@@ -84,6 +84,44 @@ def test_slabs_with_global_force_corrections(name, nslabs):
             s.close()
 
 
+@pytest.mark.parametrize("name,nslabs", [("les", 2), ("les_vd", 3), ("les_ls", 2), ("les_wale", 2), ("les_ts", 2),
+                                          ("trt_les", 3)])
+def test_les_slabs_reproduce_the_single_lattice(name, nslabs):
+    """LES on slabs: the u planes beyond each face swapped in the middle of the step
+    (here between the threads of one process), so every cell's eddy viscosity and step
+    are the single lattice's, bit for bit."""
+    _, cfg, state = make_case(name, seed=45)
+    nsteps = 7
+    a = whole(cfg, state, nsteps)
+    slabs = [slab.Slab(cfg, z0, nz) for z0, nz in slab.bounds(cfg.NZ, nslabs)]
+    try:
+        slab.use_local_exchange(slabs)
+        for s in slabs:
+            for k, v in pop_items(state):
+                s.set_pop(k, v)
+        slab.initialize_local(slabs)
+        slab.step_local(slabs, nsteps)
+        for k, _ in pop_items(state):
+            b = np.concatenate([s.sim.get_pop(k) for s in slabs])
+            assert np.array_equal(b, a[k]), k
+    finally:
+        for s in slabs:
+            s.close()
+
+
+def test_les_slab_without_exchange_is_refused():
+    _, cfg, state = make_case("les", seed=46)
+    s = slab.Slab(cfg, 0, 3)
+    try:
+        for k, v in pop_items(state):
+            s.set_pop(k, v)
+        s.sim.initialize()
+        with pytest.raises(ch4b200.CH4Error):
+            s.sim.step(1)
+    finally:
+        s.close()
+
+
 def test_slab_without_gather_is_refused():
     _, cfg, state = make_case("nozero", seed=44)
     s = slab.Slab(cfg, 0, 3)
