@@ -51,7 +51,7 @@ def build(verbose=False):
             with open(o + ".ptxas.txt", "w") as f:  # registers, spills and shared memory per kernel
                 f.write(r.stdout + r.stderr)
         objs.append(o)
-    for src in ["ch4_host.cpp"]:
+    for src in ["ch4_host.cpp", "h5file.cpp"]:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if newer([s] + headers, o):

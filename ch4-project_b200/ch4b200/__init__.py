@@ -83,6 +83,9 @@ def lib():
         L.ch4_diagnostics.argtypes = [P, D, D, D, D]
         L.ch4_dump_averages.argtypes = [P, C.c_char_p, C.c_double, C.c_int]
         L.ch4_dump_fields_ascii.argtypes = [P, C.c_char_p, C.c_int]
+        L.ch4_output_h5.argtypes = [P, C.c_char_p, C.c_int, C.c_double, C.c_int]
+        L.ch4_write_pop_h5.argtypes = [P, C.c_char_p]
+        L.ch4_read_pop_h5.argtypes = [P, C.c_char_p, C.c_int, C.c_int, C.c_int]
         L.ch4_particle_averages.argtypes = [P, D]
         L.ch4_halo_bytes.argtypes = [P, C.POINTER(C.c_size_t)]
         L.ch4_halo_pack.argtypes = [P, C.c_void_p, C.c_void_p]
@@ -285,6 +288,23 @@ class Simulation:
     def dump_fields_ascii(self, directory, itime):
         """ch4_dump_fields_ascii: the OUTPUT_ASCII vel/temp/scal.<itime> files in `directory`."""
         self._check(lib().ch4_dump_fields_ascii(self.h, str(directory).encode(), int(itime)), "dump_fields_ascii")
+
+    def output_h5(self, directory, itime, time_now=0.0, grid=True, timestamp_real=False):
+        """ch4_output_h5: field_<n>.h5 (group /euler) and field_<n>.xmf in `directory`
+        (OUTPUT_H5_GRID adds the cell-centre coordinates; OUTPUT_H5_TIMESTAMP_REAL names the
+        files by (int)time_now instead of itime)."""
+        opts = (abi.H5_GRID if grid else 0) | (abi.H5_TIMESTAMP_REAL if timestamp_real else 0)
+        self._check(lib().ch4_output_h5(self.h, str(directory).encode(), int(itime), float(time_now), opts),
+                    "output_h5")
+
+    def write_pop_h5(self, path="pop.h5"):
+        """ch4_write_pop_h5: the populations (and HIT phases) as the reference's pop.h5."""
+        self._check(lib().ch4_write_pop_h5(self.h, str(path).encode()), "write_pop_h5")
+
+    def read_pop_h5(self, path="pop.h5", resume_u=True, resume_t=True, resume_s=True):
+        """ch4_read_pop_h5: load pop.h5 (before initialize), as the reference's resume does."""
+        self._check(lib().ch4_read_pop_h5(self.h, str(path).encode(), int(resume_u), int(resume_t), int(resume_s)),
+                    "read_pop_h5")
 
     @property
     def stream_handle(self):

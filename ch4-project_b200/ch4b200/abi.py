@@ -157,3 +157,8 @@ def flags_of(names):
 
 def set_flag_names(flags):
     return [n for n, b in FLAGS.items() if flags & b]
+
+
+# ch4_output_h5 options
+H5_GRID = 1
+H5_TIMESTAMP_REAL = 2

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/ch4.h"
+#include "h5file.hpp"
 #include "launch.h"
 
 using namespace ch4;
@@ -2189,6 +2190,238 @@ ch4_status ch4_dump_fields_ascii(ch4_handle* h, const char* dir, int itime) {
   if (ok && !t.empty()) ok = dump("temp", 4, [&](FILE* f, size_t idx) { std::fprintf(f, " %e", t[idx]); });
   if (ok && !s.empty()) ok = dump("scal", 4, [&](FILE* f, size_t idx) { std::fprintf(f, " %e", s[idx]); });
   return ok ? CH4_OK : h->fail(CH4_ERR_ARG, "cannot write in %s", dir ? dir : ".");
+}
+
+// HDF5 output (src/output_h5.c) -----------------------------------------------------
+
+namespace {
+
+// one double array written as a dataset: every `stride`-th value from `first`
+h5::Dataset h5_doubles(const char* name, const std::vector<uint64_t>& dims, const double* first, size_t stride) {
+  h5::Dataset d;
+  d.name = name;
+  d.type = h5::Type::f64();
+  d.dims = dims;
+  const size_t n = (size_t)(dims[0] * dims[1] * dims[2]);
+  d.write = [first, stride, n](FILE* f) {
+    if (stride == 1) return std::fwrite(first, sizeof(double), n, f) == n;
+    std::vector<double> buf(std::min<size_t>(n, 1 << 20));
+    for (size_t i0 = 0; i0 < n; i0 += buf.size()) {
+      const size_t m = std::min(buf.size(), n - i0);
+      for (size_t i = 0; i < m; i++) buf[i] = first[(i0 + i) * stride];
+      if (std::fwrite(buf.data(), sizeof(double), m, f) != m) return false;
+    }
+    return true;
+  };
+  return d;
+}
+
+// the XDMF companion of field_<n>.h5, as output_h5 prints it (src/output_h5.c:192-370)
+bool write_xmf(const std::string& path, const std::string& h5name, const ch4_config& c, bool grid, double time_now) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  const int NX = c.NX, NY = c.NY, NZ = c.NZ, size = (int)sizeof(double);
+  const char* h = h5name.c_str();
+  std::fprintf(f, "<?xml version=\"1.0\" ?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n<Xdmf Version=\"2.0\">\n<Domain>\n");
+  std::fprintf(f, "<Grid Name=\"FiniteVolumeLB\" GridType=\"Uniform\">\n");
+  if (grid) {
+    std::fprintf(f, "<Topology TopologyType=\"3DSMesh\" NumberOfElements=\"%d %d %d\"/>\n", NZ, NY, NX);
+    std::fprintf(f, "<Geometry GeometryType=\"X_Y_Z\">\n");
+    for (const char* a : {"X", "Y", "Z"}) {
+      std::fprintf(f, "<DataItem Name=\"%s\" Dimensions=\"%d %d %d\" NumberType=\"Float\" Precision=\"%d\" Format=\"HDF\">\n", a,
+                   NZ, NY, NX, size);
+      std::fprintf(f, "%s:/euler/position_%c\n</DataItem>\n", h, std::tolower(a[0]));
+    }
+    std::fprintf(f, "</Geometry>\n");
+  } else {
+    std::fprintf(f, "<Topology TopologyType=\"3DCoRectMesh\" NumberOfElements=\"%d %d %d\"/>\n", NZ, NY, NX);
+    std::fprintf(f, "<Geometry GeometryType=\"ORIGIN_DXDYDZ\">\n");
+    std::fprintf(f, "<DataItem Name=\"Z_Y_X\" Dimensions=\"3\" DataType=\"Float\" Format=\"XML\">\n0.5 0.5 0.5\n</DataItem>\n");
+    std::fprintf(f, "<DataItem Name=\"DZ_DY_DX\" Dimensions=\"3\" DataType=\"Float\" Format=\"XML\">\n1.0 1.0 1.0\n</DataItem>\n");
+    std::fprintf(f, "</Geometry>\n");
+  }
+  auto scalar = [&](const char* name) {
+    std::fprintf(f, "<Attribute Name=\"%s\" AttributeType=\"Scalar\" Center=\"Node\">\n", name);
+    std::fprintf(f, "<DataItem Dimensions=\"%d %d %d\" NumberType=\"Float\" Precision=\"%d\" Format=\"HDF\">\n", NZ, NY, NX, size);
+    std::fprintf(f, "%s:/euler/%s\n</DataItem>\n</Attribute>\n", h, name);
+  };
+  if (c.flags & CH4_F_LB_FLUID) {
+    for (const char* n : {"velocity_x", "velocity_y", "velocity_z", "density"}) scalar(n);
+    std::fprintf(f, "<Attribute Name=\"velocity\" AttributeType=\"Vector\" Center=\"Node\">\n");
+    std::fprintf(f, "<DataItem ItemType=\"Function\" Dimensions=\"%d %d %d 3\" \n   Function=\"JOIN($0 , $1, $2)\">\n", NZ, NY, NX);
+    for (const char* n : {"velocity_x", "velocity_y", "velocity_z"}) {
+      std::fprintf(f, "<DataItem Dimensions=\"%d %d %d 1\" NumberType=\"Float\" Precision=\"%d\" Format=\"HDF\">\n", NZ, NY, NX,
+                   size);
+      std::fprintf(f, "%s:/euler/%s\n</DataItem>\n", h, n);
+    }
+    std::fprintf(f, "</DataItem>\n</Attribute>\n");
+  }
+  if (c.flags & CH4_F_LB_TEMPERATURE) scalar("temperature");
+  if (c.flags & CH4_F_LB_SCALAR) scalar("scalar");
+  std::fprintf(f, "<Time Value=\" %e\" />\n</Grid>\n</Domain>\n</Xdmf>\n", time_now);
+  return std::fclose(f) == 0;
+}
+
+const char* const POP_SETS[3] = {"velocity", "temperature", "scalar"};
+
+std::vector<std::string> pop_members() {
+  std::vector<std::string> m;
+  for (int q = 0; q < 19; q++) m.push_back("p" + std::to_string(q));
+  return m;
+}
+
+}  // namespace
+
+ch4_status ch4_output_h5(ch4_handle* h, const char* dir, int itime, double time_now, int opts) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  if (c.nz_global > 0) return h->fail(CH4_ERR_UNSUPPORTED, "HDF5 output of a z-slab: gather the slabs' fields first");
+  const size_t n = (size_t)c.NX * c.NY * c.NZ;
+  std::vector<double> dens(n), u(3 * n), t, s, pos;
+  if (c.flags & CH4_F_LB_TEMPERATURE) t.resize(n);
+  if (c.flags & CH4_F_LB_SCALAR) s.resize(n);
+  ch4_status st = h->eng->fields(dens.data(), u.data(), t.empty() ? nullptr : t.data(), s.empty() ? nullptr : s.data(),
+                                 nullptr, 0);
+  if (st) return st;
+  const std::vector<uint64_t> dims{(uint64_t)c.NZ, (uint64_t)c.NY, (uint64_t)c.NX};
+  h5::Group g;
+  g.name = "euler";
+  if (opts & CH4_H5_GRID) {  // cell centres of the unit mesh, src/grid.c:136-500
+    pos.resize(3 * n);
+    for (int k = 0; k < c.NZ; k++)
+      for (int j = 0; j < c.NY; j++)
+        for (int i = 0; i < c.NX; i++) {
+          const size_t idx = ((size_t)k * c.NY + j) * c.NX + i;
+          pos[idx] = (double)i + 0.5;
+          pos[n + idx] = (double)j + 0.5;
+          pos[2 * n + idx] = (double)k + 0.5;
+        }
+    g.datasets.push_back(h5_doubles("position_x", dims, pos.data(), 1));
+    g.datasets.push_back(h5_doubles("position_y", dims, pos.data() + n, 1));
+    g.datasets.push_back(h5_doubles("position_z", dims, pos.data() + 2 * n, 1));
+  }
+  if (c.flags & CH4_F_LB_FLUID) {
+    g.datasets.push_back(h5_doubles("velocity_x", dims, u.data(), 3));
+    g.datasets.push_back(h5_doubles("velocity_y", dims, u.data() + 1, 3));
+    g.datasets.push_back(h5_doubles("velocity_z", dims, u.data() + 2, 3));
+    g.datasets.push_back(h5_doubles("density", dims, dens.data(), 1));
+  }
+  if (!t.empty()) g.datasets.push_back(h5_doubles("temperature", dims, t.data(), 1));
+  if (!s.empty()) g.datasets.push_back(h5_doubles("scalar", dims, s.data(), 1));
+  const int stamp = (opts & CH4_H5_TIMESTAMP_REAL) ? (int)time_now : itime;
+  const std::string stem = "field_" + std::to_string(stamp);
+  const std::string base = dir && *dir ? std::string(dir) + "/" : std::string();
+  std::string err;
+  if (!h5::write_file(base + stem + ".h5", {g}, err)) return h->fail(CH4_ERR_ARG, "%s", err.c_str());
+  if (!write_xmf(base + stem + ".xmf", stem + ".h5", c, (opts & CH4_H5_GRID) != 0, time_now))
+    return h->fail(CH4_ERR_ARG, "cannot write %s.xmf", stem.c_str());
+  return CH4_OK;
+}
+
+ch4_status ch4_write_pop_h5(ch4_handle* h, const char* path) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  if (c.nz_global > 0) return h->fail(CH4_ERR_UNSUPPORTED, "pop.h5 of a z-slab: write the whole lattice");
+  const size_t n = (size_t)c.NX * c.NY * c.NZ;
+  const std::vector<uint64_t> dims{(uint64_t)c.NZ, (uint64_t)c.NY, (uint64_t)c.NX};
+  const uint64_t set_flag[3] = {CH4_F_LB_FLUID, CH4_F_LB_TEMPERATURE, CH4_F_LB_SCALAR};
+  const char which[3] = {'p', 'g', 'h'};
+  std::vector<std::vector<double>> aos(3);
+  h5::Group g;
+  g.name = "population";
+  for (int k = 0; k < 3; k++) {
+    if (!(c.flags & set_flag[k])) continue;
+    aos[k].resize(19 * n);
+    ch4_status st = ch4_get_pop(h, which[k], aos[k].data(), 0);
+    if (st) return st;
+    h5::Dataset d;
+    d.name = POP_SETS[k];
+    d.type = h5::Type::compound(pop_members(), 8);  // struct pop {double p[19]}
+    d.dims = dims;
+    const double* src = aos[k].data();
+    d.write = [src, n](FILE* f) { return std::fwrite(src, sizeof(double), 19 * n, f) == 19 * n; };
+    g.datasets.push_back(d);
+  }
+  std::vector<h5::Group> groups{g};
+  if (c.flags & CH4_F_FORCING_HIT) {  // the phases, src/output_h5.c:466-525
+    h5::Group fg;
+    fg.name = "forcing";
+    h5::Attribute nk;
+    nk.name = "number of modes (nk)";
+    nk.type = h5::Type::i32();
+    const int32_t nmodes = NK;
+    nk.data.resize(4);
+    std::memcpy(nk.data.data(), &nmodes, 4);
+    h5::Attribute ph;
+    ph.name = "phi_u";
+    ph.type = h5::Type::compound({"x", "y", "z"}, 8);
+    ph.dims = {(uint64_t)NK};
+    ph.data.resize(sizeof(h->phi));
+    std::memcpy(ph.data.data(), h->phi, sizeof(h->phi));
+    fg.attributes = {nk, ph};
+    groups.push_back(fg);
+  }
+  std::string err;
+  if (!h5::write_file(path && *path ? path : "pop.h5", groups, err)) return h->fail(CH4_ERR_ARG, "%s", err.c_str());
+  return CH4_OK;
+}
+
+ch4_status ch4_read_pop_h5(ch4_handle* h, const char* path, int resume_u, int resume_t, int resume_s) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  if (c.nz_global > 0) return h->fail(CH4_ERR_UNSUPPORTED, "pop.h5 into a z-slab: read the whole lattice");
+  const size_t n = (size_t)c.NX * c.NY * c.NZ;
+  const char* file = path && *path ? path : "pop.h5";
+  h5::Reader r;
+  std::string err;
+  if (!r.open(file, err)) return h->fail(CH4_ERR_ARG, "%s", err.c_str());
+  const int want[3] = {resume_u && (c.flags & CH4_F_LB_FLUID), resume_t && (c.flags & CH4_F_LB_TEMPERATURE),
+                       resume_s && (c.flags & CH4_F_LB_SCALAR)};
+  const char which[3] = {'p', 'g', 'h'};
+  std::vector<double> aos;
+  for (int k = 0; k < 3; k++) {
+    if (!want[k]) continue;
+    h5::Object o;
+    if (!r.find(std::string("/population/") + POP_SETS[k], o, err))
+      return h->fail(CH4_ERR_ARG, "%s: /population/%s: %s", file, POP_SETS[k], err.c_str());
+    if (o.dims.size() != 3 || o.dims[0] != (uint64_t)c.NZ || o.dims[1] != (uint64_t)c.NY || o.dims[2] != (uint64_t)c.NX)
+      return h->fail(CH4_ERR_ARG, "%s: /population/%s is not NZ x NY x NX", file, POP_SETS[k]);
+    aos.resize(19 * n);
+    if (!r.read_members(o, pop_members(), aos.data(), 19, err)) return h->fail(CH4_ERR_ARG, "%s: %s", file, err.c_str());
+    ch4_status st = ch4_set_pop(h, which[k], aos.data(), 0);
+    if (st) return st;
+  }
+  // the phases, when the file has them (src/output_h5.c:640-700)
+  h5::Object fo;
+  if (resume_u && (c.flags & CH4_F_FORCING_HIT) && r.find("/forcing", fo, err)) {
+    for (const h5::Attribute& a : fo.attributes) {
+      if (a.name != "phi_u") continue;
+      if (a.dims.size() != 1 || a.dims[0] != (uint64_t)NK || a.type.kind != h5::Type::COMPOUND)
+        return h->fail(CH4_ERR_ARG, "%s: /forcing phi_u is not %d vectors", file, NK);
+      double phi[3 * NK];
+      for (int ii = 0; ii < NK; ii++)
+        for (int ax = 0; ax < 3; ax++) {
+          const char* nm[3] = {"x", "y", "z"};
+          bool found = false;
+          for (const h5::Member& m : a.type.members)
+            if (m.name == nm[ax]) {
+              const uint8_t* p = a.data.data() + (size_t)ii * a.type.size + m.offset;
+              if (m.fsize == 8) {
+                std::memcpy(&phi[3 * ii + ax], p, 8);
+              } else {
+                float x;
+                std::memcpy(&x, p, 4);
+                phi[3 * ii + ax] = x;
+              }
+              found = true;
+            }
+          if (!found) return h->fail(CH4_ERR_ARG, "%s: /forcing phi_u has no member %s", file, nm[ax]);
+        }
+      ch4_status st = ch4_set_hit_phases(h, phi);
+      if (st) return st;
+    }
+  }
+  return CH4_OK;
 }
 
 ch4_status ch4_step(ch4_handle* h, int nsteps) {

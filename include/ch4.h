@@ -334,6 +334,24 @@ ch4_status ch4_dump_particle_averages(ch4_handle *h, const char *dir, double tim
  * The reference writes them into RUN/ (OutDir). */
 ch4_status ch4_dump_fields_ascii(ch4_handle *h, const char *dir, int itime);
 
+/* HDF5 output with the reference's layout (src/output_h5.c), written by the library's own
+ * HDF5 container code (superblock version 0, symbol-table groups, contiguous datasets).
+ * ch4_output_h5: dir/field_<itime>.h5 (or field_<(int)time_now>.h5 with
+ * CH4_H5_TIMESTAMP_REAL) holding /euler/velocity_x, _y, _z and density (LB_FLUID),
+ * temperature, scalar, and with CH4_H5_GRID position_x, _y, _z (cell centres), each
+ * NZ x NY x NX doubles; plus the XDMF file field_<n>.xmf beside it (output_h5, :9-370).
+ * ch4_write_pop_h5: /population/velocity, temperature, scalar as NZ x NY x NX compounds
+ * {double p0 ... p18}, and with LB_FLUID_FORCING_HIT the group /forcing with the
+ * attributes "number of modes (nk)" and phi_u (nk vectors {x, y, z}) (write_pop_h5,
+ * :372-527).  ch4_read_pop_h5 loads the sets asked for (resume_u/_t/_s) into the handle
+ * like ch4_set_pop, and phi_u when present (read_pop_h5, :540-727): it reads files of
+ * this library and libhdf5's default format (contiguous datasets; float members of either
+ * size, found by name).  Call before ch4_initialize.  path NULL or "" means "pop.h5". */
+enum { CH4_H5_GRID = 1, CH4_H5_TIMESTAMP_REAL = 2 };
+ch4_status ch4_output_h5(ch4_handle *h, const char *dir, int itime, double time_now, int opts);
+ch4_status ch4_write_pop_h5(ch4_handle *h, const char *path);
+ch4_status ch4_read_pop_h5(ch4_handle *h, const char *path, int resume_u, int resume_t, int resume_s);
+
 /* Initial fields of initial_conditions (src/initial_conditions.c:3-500) for the
  * CH4_F_*_INITIAL_* flags, computed on the host: p, g, h as AoS [NZ][NY][NX][19]
  * (no halo; a pointer may be NULL when its set is off), and the HIT phases that

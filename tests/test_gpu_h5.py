@@ -1,0 +1,113 @@
+"""HDF5 output and restart through the C ABI (ch4_output_h5, ch4_write_pop_h5,
+ch4_read_pop_h5) with the reference's layout (src/output_h5.c): the files parse under
+the independent spec reader (tests/h5spec.py) and hold exactly the handle's fields and
+populations; a handle loaded from pop.h5 is the handle given the same populations with
+ch4_set_pop (the reference's resume path, src/initial_conditions.c:606), phases included."""
+import numpy as np
+import pytest
+
+import h5spec
+from lbcases import make_case, pop_items
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import ch4b200  # noqa: E402
+from ch4b200 import abi  # noqa: E402
+
+
+def started(cfg, state, nsteps):
+    sim = ch4b200.Simulation(cfg)
+    for k, v in pop_items(state):
+        sim.set_pop(k, v)
+    sim.initialize()
+    sim.step(nsteps)
+    return sim
+
+
+@pytest.mark.parametrize("name", ["rb", "scalar", "hit"])
+def test_field_file_holds_the_fields(name, tmp_path):
+    _, cfg, state = make_case(name, seed=61)
+    with started(cfg, state, 5) as sim:
+        sim.output_h5(tmp_path, 5, time_now=5.0, grid=True)
+        f = sim.fields()
+    got = h5spec.read(tmp_path / "field_5.h5")
+    shape = (cfg.NZ, cfg.NY, cfg.NX)
+    k, j, i = np.meshgrid(np.arange(cfg.NZ), np.arange(cfg.NY), np.arange(cfg.NX), indexing="ij")
+    assert np.array_equal(got["/euler/position_x"], i + 0.5)
+    assert np.array_equal(got["/euler/position_y"], j + 0.5)
+    assert np.array_equal(got["/euler/position_z"], k + 0.5)
+    for a, comp in enumerate("xyz"):
+        assert np.array_equal(got["/euler/velocity_" + comp], f["u"][..., a].reshape(shape)), comp
+    assert np.array_equal(got["/euler/density"], f["dens"].reshape(shape))
+    for flag, key, ds in (("LB_TEMPERATURE", "t", "temperature"), ("LB_SCALAR", "s", "scalar")):
+        on = bool(cfg.flags & abi.FLAGS[flag])
+        assert ("/euler/" + ds in got) == on, ds
+        if on:
+            assert np.array_equal(got["/euler/" + ds], f[key].reshape(shape)), ds
+    xmf = (tmp_path / "field_5.xmf").read_text()
+    assert xmf.startswith('<?xml version="1.0" ?>\n<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" []>\n')
+    assert '<Topology TopologyType="3DSMesh" NumberOfElements="%d %d %d"/>' % shape in xmf
+    for ds in [n for n in got if n.startswith("/euler/")]:
+        assert "field_5.h5:%s\n" % ds in xmf, ds
+    assert xmf.endswith('<Time Value=" 5.000000e+00" />\n</Grid>\n</Domain>\n</Xdmf>\n')
+
+
+def test_timestamp_and_no_grid(tmp_path):
+    _, cfg, state = make_case("rb", seed=62)
+    with started(cfg, state, 2) as sim:
+        sim.output_h5(tmp_path, 2, time_now=7.9, grid=False, timestamp_real=True)
+    got = h5spec.read(tmp_path / "field_7.h5")
+    assert "/euler/position_x" not in got and "/euler/velocity_x" in got
+    assert '<Topology TopologyType="3DCoRectMesh"' in (tmp_path / "field_7.xmf").read_text()
+
+
+@pytest.mark.parametrize("name", ["rb", "scalar", "hit"])
+def test_pop_file_restart(name, tmp_path):
+    _, cfg, state = make_case(name, seed=63)
+    path = tmp_path / "pop.h5"
+    with started(cfg, state, 6) as a:
+        a.write_pop_h5(path)
+        pops = {k: a.get_pop(k) for k, _ in pop_items(state)}
+        phases = a.get_hit_phases()
+    got = h5spec.read(path)
+    sets = {"p": "velocity", "g": "temperature", "h": "scalar"}
+    for k, arr in pops.items():
+        d = got["/population/" + sets[k]]
+        assert d.shape == (cfg.NZ, cfg.NY, cfg.NX)
+        back = np.stack([d["p%d" % q] for q in range(19)], axis=-1)
+        assert np.array_equal(back.reshape(arr.shape), arr), k
+    if name == "hit":
+        phi = got["/forcing@phi_u"]
+        assert got["/forcing@number of modes (nk)"].item() == 6
+        assert np.array_equal(np.stack([phi["x"], phi["y"], phi["z"]], 1).ravel(), phases.ravel())
+    else:
+        assert not any(n.startswith("/forcing") for n in got)
+    # resume from the file == the same populations (and phases) given directly
+    with ch4b200.Simulation(cfg) as b, ch4b200.Simulation(cfg) as c:
+        b.read_pop_h5(path)
+        for k, arr in pops.items():
+            c.set_pop(k, arr)
+        if name == "hit":
+            c.set_hit_phases(phases)
+            assert np.array_equal(b.get_hit_phases(), phases)
+        b.initialize()
+        c.initialize()
+        b.step(4)
+        c.step(4)
+        for k in pops:
+            assert np.array_equal(b.get_pop(k), c.get_pop(k)), k
+
+
+def test_read_pop_refuses_a_wrong_lattice(tmp_path):
+    _, cfg, state = make_case("rb", seed=64)
+    with started(cfg, state, 1) as a:
+        a.write_pop_h5(tmp_path / "pop.h5")
+    cfg.NX += 1
+    cfg.SX += 1
+    with ch4b200.Simulation(cfg) as b:
+        with pytest.raises(ch4b200.CH4Error):
+            b.read_pop_h5(tmp_path / "pop.h5")
