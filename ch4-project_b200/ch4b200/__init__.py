@@ -86,6 +86,9 @@ def lib():
         L.ch4_output_h5.argtypes = [P, C.c_char_p, C.c_int, C.c_double, C.c_int]
         L.ch4_write_pop_h5.argtypes = [P, C.c_char_p]
         L.ch4_read_pop_h5.argtypes = [P, C.c_char_p, C.c_int, C.c_int, C.c_int]
+        L.ch4_output_particles_h5.argtypes = [P, C.c_char_p, C.c_int, C.c_double, C.c_int]
+        L.ch4_write_particles_h5.argtypes = [P, C.c_char_p]
+        L.ch4_read_particles_h5.argtypes = [P, C.c_char_p]
         L.ch4_particle_averages.argtypes = [P, D]
         L.ch4_halo_bytes.argtypes = [P, C.POINTER(C.c_size_t)]
         L.ch4_halo_pack.argtypes = [P, C.c_void_p, C.c_void_p]
@@ -300,6 +303,20 @@ class Simulation:
     def write_pop_h5(self, path="pop.h5"):
         """ch4_write_pop_h5: the populations (and HIT phases) as the reference's pop.h5."""
         self._check(lib().ch4_write_pop_h5(self.h, str(path).encode()), "write_pop_h5")
+
+    def output_particles_h5(self, directory, itime, time_now=0.0, output_fluid=False, timestamp_real=False):
+        """ch4_output_particles_h5: particle_<n>.h5 (group /lagrange) and particle_<n>.xmf."""
+        opts = (abi.H5_LAGRANGE_OUTPUT_FLUID if output_fluid else 0) | (abi.H5_TIMESTAMP_REAL if timestamp_real else 0)
+        self._check(lib().ch4_output_particles_h5(self.h, str(directory).encode(), int(itime), float(time_now), opts),
+                    "output_particles_h5")
+
+    def write_particles_h5(self, path="part.h5"):
+        """ch4_write_particles_h5: the particles as the reference's part.h5."""
+        self._check(lib().ch4_write_particles_h5(self.h, str(path).encode()), "write_particles_h5")
+
+    def read_particles_h5(self, path="part.h5"):
+        """ch4_read_particles_h5: load part.h5 into the handle (before initialize)."""
+        self._check(lib().ch4_read_particles_h5(self.h, str(path).encode()), "read_particles_h5")
 
     def read_pop_h5(self, path="pop.h5", resume_u=True, resume_t=True, resume_s=True):
         """ch4_read_pop_h5: load pop.h5 (before initialize), as the reference's resume does."""

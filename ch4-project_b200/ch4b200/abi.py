@@ -162,3 +162,4 @@ def set_flag_names(flags):
 # ch4_output_h5 options
 H5_GRID = 1
 H5_TIMESTAMP_REAL = 2
+H5_LAGRANGE_OUTPUT_FLUID = 4

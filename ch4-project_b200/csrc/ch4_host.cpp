@@ -302,6 +302,7 @@ struct EngineBase {
   virtual ch4_status diag_sums(double* glob, double* rx, double* ry, double* rz) = 0;
   virtual ch4_status set_particles(const ch4_particle* parts, int n) = 0;
   virtual ch4_status get_particles(ch4_particle* parts, int n) = 0;
+  virtual int particle_count() const = 0;
   virtual size_t device_bytes() const = 0;
   // after a stream synchronisation: errors the kernels recorded on the device
   virtual ch4_status check() { return CH4_OK; }
@@ -939,6 +940,7 @@ struct Engine : EngineBase {
     return st;
   }
 
+  int particle_count() const override { return np; }
   ch4_status get_particles(ch4_particle* parts, int n) override {
     if (n > np || n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "asked for %d of %d particles", n, np);
     if (n == 0) return CH4_OK;
@@ -2422,6 +2424,235 @@ ch4_status ch4_read_pop_h5(ch4_handle* h, const char* path, int resume_u, int re
     }
   }
   return CH4_OK;
+}
+
+// particle HDF5 files (src/lagrange.c:1598-2600 output_particles, :4231-4540
+// write_point_particle_h5 / read_point_particle_h5) ------------------------------------
+
+namespace {
+
+// (dataset or member name, field of ch4_particle)
+using PField = std::pair<const char*, double ch4_particle::*>;
+
+// the per-particle datasets of output_particles, in its order, for the supported flags
+std::vector<PField> lagrange_fields(uint64_t fl, bool output_fluid) {
+  using P = ch4_particle;
+  std::vector<PField> v = {{"name", &P::name}, {"tau_drag", &P::tau_drag}, {"x", &P::x},   {"y", &P::y},
+                           {"z", &P::z},       {"vx", &P::vx},             {"vy", &P::vy}, {"vz", &P::vz},
+                           {"ax", &P::ax},     {"ay", &P::ay},             {"az", &P::az}};
+  const bool grad = fl & CH4_F_LAGRANGE_GRADIENT, am = fl & CH4_F_LAGRANGE_ADDEDMASS;
+  if (grad) {
+    v.insert(v.end(), {{"dx_ux", &P::dx_ux}, {"dy_ux", &P::dy_ux}, {"dz_ux", &P::dz_ux}, {"dx_uy", &P::dx_uy},
+                       {"dy_uy", &P::dy_uy}, {"dz_uy", &P::dz_uy}, {"dx_uz", &P::dx_uz}, {"dy_uz", &P::dy_uz},
+                       {"dz_uz", &P::dz_uz}});
+    if (am) v.push_back({"beta_coeff", &P::beta_coeff});
+  }
+  if (output_fluid) {
+    v.insert(v.end(), {{"ux", &P::ux}, {"uy", &P::uy}, {"uz", &P::uz}});
+    if (am) v.insert(v.end(), {{"Dt_ux", &P::Dt_ux}, {"Dt_uy", &P::Dt_uy}, {"Dt_uz", &P::Dt_uz}});
+  }
+  if (fl & CH4_F_LB_TEMPERATURE) {
+    v.insert(v.end(), {{"temperature", &P::t}, {"dt_t", &P::dt_t}});
+    if (grad) v.insert(v.end(), {{"dx_t", &P::dx_t}, {"dy_t", &P::dy_t}, {"dz_t", &P::dz_t}});
+  }
+  return v;
+}
+
+// the members of point_particle in part.h5, in write_point_particle_h5's order
+std::vector<PField> part_members(uint64_t fl) {
+  using P = ch4_particle;
+  std::vector<PField> v = {{"name", &P::name},     {"x", &P::x},           {"y", &P::y},
+                           {"z", &P::z},           {"vx", &P::vx},         {"vy", &P::vy},
+                           {"vz", &P::vz},         {"vx_old", &P::vx_old}, {"vy_old", &P::vy_old},
+                           {"vz_old", &P::vz_old}, {"ax", &P::ax},         {"ay", &P::ay},
+                           {"az", &P::az},         {"ax_old", &P::ax_old}, {"ay_old", &P::ay_old},
+                           {"az_old", &P::az_old}, {"tau_drag", &P::tau_drag}};
+  if (fl & CH4_F_LB_FLUID) {
+    v.insert(v.end(), {{"ux", &P::ux}, {"uy", &P::uy}, {"uz", &P::uz}, {"ux_old", &P::ux_old},
+                       {"uy_old", &P::uy_old}, {"uz_old", &P::uz_old}});
+    if (fl & CH4_F_LAGRANGE_GRADIENT) {
+      v.insert(v.end(), {{"dx_ux", &P::dx_ux}, {"dy_ux", &P::dy_ux}, {"dz_ux", &P::dz_ux}, {"dx_uy", &P::dx_uy},
+                         {"dy_uy", &P::dy_uy}, {"dz_uy", &P::dz_uy}, {"dx_uz", &P::dx_uz}, {"dy_uz", &P::dy_uz},
+                         {"dz_uz", &P::dz_uz}});
+      if (fl & CH4_F_LAGRANGE_ADDEDMASS) v.push_back({"beta_coeff", &P::beta_coeff});
+    }
+  }
+  if (fl & CH4_F_LB_TEMPERATURE) {
+    v.push_back({"t", &P::t});
+    if (fl & CH4_F_LAGRANGE_GRADIENT) v.insert(v.end(), {{"dx_t", &P::dx_t}, {"dy_t", &P::dy_t}, {"dz_t", &P::dz_t}});
+  }
+  return v;
+}
+
+bool particles_of(ch4_handle* h, std::vector<ch4_particle>& p, ch4_status& st) {
+  p.resize(h->eng->particle_count());
+  st = h->eng->get_particles(p.data(), (int)p.size());
+  return st == CH4_OK;
+}
+
+// the XDMF companion of particle_<n>.h5 (src/lagrange.c:2172-2590)
+bool write_particle_xmf(const std::string& path, const std::string& h5name, int np, uint64_t fl, bool output_fluid,
+                        double time_now) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return false;
+  const int size = (int)sizeof(double);
+  const char* h = h5name.c_str();
+  std::fprintf(f, "<?xml version=\"1.0\" ?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n<Xdmf Version=\"2.0\">\n<Domain>\n");
+  std::fprintf(f, "<Grid Name=\"Points\" GridType=\"Uniform\">\n");
+  std::fprintf(f, "<Topology TopologyType=\"Polyvertex\" NumberOfElements=\"%d\"/>\n", np);
+  std::fprintf(f, "<Geometry GeometryType=\"X_Y_Z\">\n");
+  for (const char* a : {"x", "y", "z"}) {
+    std::fprintf(f, "<DataItem Name=\"%s\" Dimensions=\"%d\" NumberType=\"Float\" Precision=\"%d\" Format=\"HDF\">\n", a, np,
+                 size);
+    std::fprintf(f, "%s:/lagrange/%s\n</DataItem>\n", h, a);
+  }
+  std::fprintf(f, "</Geometry>\n");
+  auto scalar = [&](const char* name) {
+    std::fprintf(f, "<Attribute Name=\"%s\" AttributeType=\"Scalar\" Center=\"Node\"> \n", name);
+    std::fprintf(f, "<DataItem Dimensions=\"%d\" NumberType=\"Float\" Precision=\"%d\" Format=\"HDF\">\n", np, size);
+    std::fprintf(f, "%s:/lagrange/%s\n</DataItem>\n</Attribute>\n", h, name);
+  };
+  auto joined = [&](const char* name, const char* type, std::initializer_list<const char*> parts) {
+    const int m = (int)parts.size();
+    std::fprintf(f, "<Attribute Name=\"%s\" AttributeType=\"%s\" Center=\"Node\"> \n", name, type);
+    if (m == 3)
+      std::fprintf(f, "<DataItem ItemType=\"Function\" Dimensions=\"%d 3\" \n   Function=\"JOIN($0 , $1, $2)\">\n", np);
+    else
+      std::fprintf(f, "<DataItem ItemType=\"Function\" Dimensions=\"%d 9\" \n   Function=\"JOIN($0,$1,$2,$3,$4,$5,$6,$7,$8)\">\n",
+                   np);
+    for (const char* p : parts) {
+      std::fprintf(f, "<DataItem Dimensions=\"%d 1\" NumberType=\"Float\" Precision=\"%d\" Format=\"HDF\">\n", np, size);
+      std::fprintf(f, "%s:/lagrange/%s\n</DataItem>\n", h, p);
+    }
+    std::fprintf(f, "</DataItem>\n</Attribute>\n");
+  };
+  scalar("name");
+  scalar("tau_drag");
+  joined("velocity", "Vector", {"vx", "vy", "vz"});
+  joined("acceleration", "Vector", {"ax", "ay", "az"});
+  if (fl & CH4_F_LAGRANGE_GRADIENT) {
+    joined("fluid velocity gradient", "Tensor",
+           {"dx_ux", "dy_ux", "dz_ux", "dx_uy", "dy_uy", "dz_uy", "dx_uz", "dy_uz", "dz_uz"});
+    if (fl & CH4_F_LAGRANGE_ADDEDMASS) scalar("beta_coeff");
+  }
+  if (output_fluid) {
+    joined("fluid_velocity", "Vector", {"ux", "uy", "uz"});
+    if (fl & CH4_F_LAGRANGE_ADDEDMASS) joined("fluid_acceleration", "Vector", {"Dt_ux", "Dt_uy", "Dt_uz"});
+  }
+  if (fl & CH4_F_LB_TEMPERATURE) {
+    scalar("temperature");
+    scalar("dt_t");
+    if (fl & CH4_F_LAGRANGE_GRADIENT) joined("temperature gradient", "Vector", {"dx_t", "dy_t", "dz_t"});
+  }
+  std::fprintf(f, "<Time Value=\" %e\" />\n</Grid>\n</Domain>\n</Xdmf>\n", time_now);
+  return std::fclose(f) == 0;
+}
+
+}  // namespace
+
+ch4_status ch4_output_particles_h5(ch4_handle* h, const char* dir, int itime, double time_now, int opts) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  if (!(c.flags & CH4_F_LAGRANGE)) return h->fail(CH4_ERR_STATE, "particle output without LAGRANGE");
+  std::vector<ch4_particle> p;
+  ch4_status st;
+  if (!particles_of(h, p, st)) return st;
+  const bool fluid = (opts & CH4_H5_LAGRANGE_OUTPUT_FLUID) != 0;
+  const uint64_t np = p.size();
+  h5::Group g;
+  g.name = "lagrange";
+  for (const PField& pf : lagrange_fields(c.flags, fluid)) {
+    h5::Dataset d;
+    d.name = pf.first;
+    d.type = h5::Type::f64();
+    d.dims = {np};
+    const ch4_particle* src = p.data();
+    auto field = pf.second;
+    d.write = [src, np, field](FILE* fp) {
+      std::vector<double> col(np);
+      for (uint64_t i = 0; i < np; i++) col[i] = src[i].*field;
+      return std::fwrite(col.data(), sizeof(double), np, fp) == np;
+    };
+    g.datasets.push_back(d);
+  }
+  const int stamp = (opts & CH4_H5_TIMESTAMP_REAL) ? (int)time_now : itime;
+  const std::string stem = "particle_" + std::to_string(stamp);
+  const std::string base = dir && *dir ? std::string(dir) + "/" : std::string();
+  std::string err;
+  if (!h5::write_file(base + stem + ".h5", {g}, err)) return h->fail(CH4_ERR_ARG, "%s", err.c_str());
+  if (!write_particle_xmf(base + stem + ".xmf", stem + ".h5", (int)np, c.flags, fluid, time_now))
+    return h->fail(CH4_ERR_ARG, "cannot write %s.xmf", stem.c_str());
+  return CH4_OK;
+}
+
+ch4_status ch4_write_particles_h5(ch4_handle* h, const char* path) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  if (!(c.flags & CH4_F_LAGRANGE)) return h->fail(CH4_ERR_STATE, "part.h5 without LAGRANGE");
+  std::vector<ch4_particle> p;
+  ch4_status st;
+  if (!particles_of(h, p, st)) return st;
+  const std::vector<PField> mem = part_members(c.flags);
+  std::vector<std::string> names;
+  for (const PField& m : mem) names.push_back(m.first);
+  h5::Group g;
+  g.name = "particles";
+  h5::Dataset d;
+  d.name = "point_particle";
+  d.type = h5::Type::compound(names, 8);
+  d.dims = {(uint64_t)p.size()};
+  const ch4_particle* src = p.data();
+  const size_t np = p.size();
+  d.write = [src, np, mem](FILE* fp) {
+    std::vector<double> rec(mem.size() * np);
+    for (size_t i = 0; i < np; i++)
+      for (size_t k = 0; k < mem.size(); k++) rec[i * mem.size() + k] = src[i].*(mem[k].second);
+    return std::fwrite(rec.data(), sizeof(double), rec.size(), fp) == rec.size();
+  };
+  g.datasets.push_back(d);
+  h5::Group pr;  // src/lagrange.c:4512-4530
+  pr.name = "properties";
+  h5::Attribute types;
+  types.name = "particle_types";
+  types.type = h5::Type::f64();
+  const double nt = c.particle_types > 0 ? c.particle_types : 1;
+  types.data.resize(8);
+  std::memcpy(types.data.data(), &nt, 8);
+  pr.attributes = {types};
+  std::string err;
+  if (!h5::write_file(path && *path ? path : "part.h5", {g, pr}, err)) return h->fail(CH4_ERR_ARG, "%s", err.c_str());
+  return CH4_OK;
+}
+
+ch4_status ch4_read_particles_h5(ch4_handle* h, const char* path) {
+  if (!h) return CH4_ERR_ARG;
+  const ch4_config& c = h->cfg;
+  if (!(c.flags & CH4_F_LAGRANGE)) return h->fail(CH4_ERR_STATE, "part.h5 without LAGRANGE");
+  const char* file = path && *path ? path : "part.h5";
+  h5::Reader r;
+  h5::Object o;
+  std::string err;
+  if (!r.open(file, err) || !r.find("/particles/point_particle", o, err))
+    return h->fail(CH4_ERR_ARG, "%s: %s", file, err.c_str());
+  if (o.dims.size() != 1 || o.type.kind != h5::Type::COMPOUND)
+    return h->fail(CH4_ERR_ARG, "%s: /particles/point_particle is not a 1-D compound", file);
+  // every member this build knows and the file has, by name
+  std::vector<PField> mem;
+  std::vector<std::string> names;
+  for (const PField& m : part_members(~0ull))
+    for (const h5::Member& fm : o.type.members)
+      if (fm.name == m.first) {
+        mem.push_back(m);
+        names.push_back(m.first);
+      }
+  const size_t np = (size_t)o.dims[0];
+  std::vector<double> rec(np * names.size());
+  if (!r.read_members(o, names, rec.data(), names.size(), err)) return h->fail(CH4_ERR_ARG, "%s: %s", file, err.c_str());
+  std::vector<ch4_particle> p(np);
+  std::memset(p.data(), 0, np * sizeof(ch4_particle));
+  for (size_t i = 0; i < np; i++)
+    for (size_t k = 0; k < mem.size(); k++) p[i].*(mem[k].second) = rec[i * mem.size() + k];
+  return ch4_set_particles(h, p.data(), (int)np);
 }
 
 ch4_status ch4_step(ch4_handle* h, int nsteps) {

@@ -347,10 +347,24 @@ ch4_status ch4_dump_fields_ascii(ch4_handle *h, const char *dir, int itime);
  * like ch4_set_pop, and phi_u when present (read_pop_h5, :540-727): it reads files of
  * this library and libhdf5's default format (contiguous datasets; float members of either
  * size, found by name).  Call before ch4_initialize.  path NULL or "" means "pop.h5". */
-enum { CH4_H5_GRID = 1, CH4_H5_TIMESTAMP_REAL = 2 };
+enum { CH4_H5_GRID = 1, CH4_H5_TIMESTAMP_REAL = 2, CH4_H5_LAGRANGE_OUTPUT_FLUID = 4 };
 ch4_status ch4_output_h5(ch4_handle *h, const char *dir, int itime, double time_now, int opts);
 ch4_status ch4_write_pop_h5(ch4_handle *h, const char *path);
 ch4_status ch4_read_pop_h5(ch4_handle *h, const char *path, int resume_u, int resume_t, int resume_s);
+
+/* Particle HDF5 files (src/lagrange.c).  ch4_output_particles_h5: dir/particle_<itime>.h5
+ * (or <(int)time_now> with CH4_H5_TIMESTAMP_REAL) with one dataset of particle_number
+ * doubles per field under /lagrange -- name, tau_drag, x..z, vx..vz, ax..az, the velocity
+ * gradient (LAGRANGE_GRADIENT) and beta_coeff (+ADDEDMASS), ux..uz and Dt_ux..Dt_uz with
+ * CH4_H5_LAGRANGE_OUTPUT_FLUID, temperature, dt_t and its gradient (LB_TEMPERATURE) -- and
+ * particle_<n>.xmf (output_particles, :1598-2590).  ch4_write_particles_h5: part.h5 with
+ * /particles/point_particle, a 1-D compound of the point_particle members of
+ * write_point_particle_h5 (:4231-4530), and /properties with the particle_types
+ * attribute.  ch4_read_particles_h5 loads such a file into the handle (ch4_set_particles;
+ * members found by name, absent ones 0).  path NULL or "" means "part.h5". */
+ch4_status ch4_output_particles_h5(ch4_handle *h, const char *dir, int itime, double time_now, int opts);
+ch4_status ch4_write_particles_h5(ch4_handle *h, const char *path);
+ch4_status ch4_read_particles_h5(ch4_handle *h, const char *path);
 
 /* Initial fields of initial_conditions (src/initial_conditions.c:3-500) for the
  * CH4_F_*_INITIAL_* flags, computed on the host: p, g, h as AoS [NZ][NY][NX][19]

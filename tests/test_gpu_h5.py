@@ -111,3 +111,95 @@ def test_read_pop_refuses_a_wrong_lattice(tmp_path):
     with ch4b200.Simulation(cfg) as b:
         with pytest.raises(ch4b200.CH4Error):
             b.read_pop_h5(tmp_path / "pop.h5")
+
+
+def _fields(flags, output_fluid):
+    """/lagrange dataset -> ch4_particle field, in output_particles' order."""
+    f = [(n, n) for n in ("name", "tau_drag", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")]
+    grad, am = flags & abi.FLAGS["LAGRANGE_GRADIENT"], flags & abi.FLAGS["LAGRANGE_ADDEDMASS"]
+    if grad:
+        f += [(n, n) for n in ("dx_ux", "dy_ux", "dz_ux", "dx_uy", "dy_uy", "dz_uy", "dx_uz", "dy_uz", "dz_uz")]
+        if am:
+            f.append(("beta_coeff", "beta_coeff"))
+    if output_fluid:
+        f += [("ux", "ux"), ("uy", "uy"), ("uz", "uz")]
+        if am:
+            f += [("Dt_ux", "Dt_ux"), ("Dt_uy", "Dt_uy"), ("Dt_uz", "Dt_uz")]
+    if flags & abi.FLAGS["LB_TEMPERATURE"]:
+        f += [("temperature", "t"), ("dt_t", "dt_t")]
+        if grad:
+            f += [("dx_t", "dx_t"), ("dy_t", "dy_t"), ("dz_t", "dz_t")]
+    return f
+
+
+def _particle_sim(name, seed, nsteps):
+    _, cfg, state = make_case(name, seed=seed)
+    sim = ch4b200.Simulation(cfg)
+    for k, v in pop_items(state):
+        sim.set_pop(k, v)
+    sim.set_particles(state["part"])
+    sim.initialize()
+    sim.step(nsteps)
+    return cfg, state, sim
+
+
+@pytest.mark.parametrize("name", ["particles", "particles_t"])
+def test_particle_file_holds_the_particles(name, tmp_path):
+    cfg, state, sim = _particle_sim(name, 65, 4)
+    with sim:
+        n = len(state["part"])
+        sim.output_particles_h5(tmp_path, 4, time_now=4.0, output_fluid=True)
+        parts = sim.get_particles(n)
+    got = h5spec.read(tmp_path / "particle_4.h5")
+    want = _fields(cfg.flags, True)
+    assert sorted(k for k in got) == sorted("/lagrange/" + d for d, _ in want)
+    for d, field in want:
+        assert np.array_equal(got["/lagrange/" + d], np.array([getattr(p, field) for p in parts])), d
+    xmf = (tmp_path / "particle_4.xmf").read_text()
+    assert '<Topology TopologyType="Polyvertex" NumberOfElements="%d"/>' % n in xmf
+    for d, _ in want:
+        assert "particle_4.h5:/lagrange/%s\n" % d in xmf, d
+
+
+@pytest.mark.parametrize("name", ["particles", "particles_t"])
+def test_part_file_restart(name, tmp_path):
+    cfg, state, a = _particle_sim(name, 66, 5)
+    n = len(state["part"])
+    with a:
+        a.write_pop_h5(tmp_path / "pop.h5")
+        a.write_particles_h5(tmp_path / "part.h5")
+        pops = {k: a.get_pop(k) for k, _ in pop_items(state)}
+        parts = a.get_particles(n)
+        phases = a.get_hit_phases()
+    got = h5spec.read(tmp_path / "part.h5")
+    rec = got["/particles/point_particle"]
+    members = rec.dtype.names
+    assert members[:17] == ("name", "x", "y", "z", "vx", "vy", "vz", "vx_old", "vy_old", "vz_old", "ax", "ay",
+                            "az", "ax_old", "ay_old", "az_old", "tau_drag")
+    assert ("t" in members) == bool(cfg.flags & abi.FLAGS["LB_TEMPERATURE"])
+    for m in members:
+        assert np.array_equal(rec[m], np.array([getattr(p, m) for p in parts])), m
+    assert got["/properties@particle_types"].item() == float(cfg.particle_types)
+    # the members part.h5 lacks start at 0, as in the reference's resume
+    trimmed = (ch4b200.Particle * n)()
+    for i, p in enumerate(parts):
+        for m in members:
+            setattr(trimmed[i], m, getattr(p, m))
+    with ch4b200.Simulation(cfg) as b, ch4b200.Simulation(cfg) as c:
+        b.read_pop_h5(tmp_path / "pop.h5")
+        b.read_particles_h5(tmp_path / "part.h5")
+        for k, arr in pops.items():
+            c.set_pop(k, arr)
+        c.set_particles(trimmed)
+        if cfg.flags & abi.FLAGS["LB_FLUID_FORCING_HIT"]:  # pop.h5 carries the phases
+            c.set_hit_phases(phases)
+        back = b.get_particles(n)
+        for m in (f for f, _ in ch4b200.Particle._fields_):
+            assert np.array_equal([getattr(p, m) for p in back], [getattr(p, m) for p in trimmed]), m
+        b.initialize()
+        c.initialize()
+        b.step(3)
+        c.step(3)
+        pb, pc = b.get_particles(n), c.get_particles(n)
+        for m in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.array_equal([getattr(p, m) for p in pb], [getattr(p, m) for p in pc]), m
