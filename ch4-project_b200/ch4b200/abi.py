@@ -46,6 +46,8 @@ FLAGS = {
     "LB_TEMPERATURE_FORCING": 1 << 25,
     "LAGRANGE_WRAP": 1 << 26,
     "LAGRANGE_GRADIENT_BRD2": 1 << 27,
+    "LAGRANGE_ORIENTATION": 1 << 60,
+    "LAGRANGE_ORIENTATION_JEFFREY": 1 << 61,
     # initial fields (ch4_initial_conditions)
     "LB_FLUID_INITIAL_KOLMOGOROV": 1 << 28,
     "LB_FLUID_INITIAL_POISEUILLE": 1 << 29,
@@ -121,6 +123,7 @@ PARTICLE_FIELDS = [
     "Dt_ux", "Dt_uy", "Dt_uz",
     "t", "t_old", "dt_t", "Dt_t",
     "dx_t", "dy_t", "dz_t",
+    "px", "py", "pz", "dt_px", "dt_py", "dt_pz", "aspect_ratio",
 ]
 
 

@@ -126,7 +126,8 @@ const uint64_t SUPPORTED =
     CH4_F_SCALAR_INITIAL_CONSTANT_BOT | CH4_F_SCALAR_INITIAL_CONSTANT_TOP | CH4_F_INITIAL_OTHER |
     CH4_F_FORCING_NOZEROMODE | CH4_F_FORCING_CONSTANT_POWER | CH4_F_OUTPUT_DIAGN_APPEND | CH4_F_LAGRANGE_GRAVITY |
     CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES | CH4_F_METHOD_TRT | CH4_F_FLUID_LES_VANDRIEST | CH4_F_TEMPERATURE_LES |
-    CH4_F_SCALAR_LES | CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN | CH4_F_LAGRANGE_TWOWAY_TRICUBIC;
+    CH4_F_SCALAR_LES | CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN | CH4_F_LAGRANGE_TWOWAY_TRICUBIC |
+    CH4_F_LAGRANGE_ORIENTATION | CH4_F_LAGRANGE_ORIENTATION_JEFFREY;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -698,6 +699,8 @@ struct Engine : EngineBase {
     Q.key = key;
     Q.order = order;
     Q.tricubic = (c.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) != 0;
+    Q.orient = (c.flags & CH4_F_LAGRANGE_ORIENTATION) != 0;
+    Q.jeffery = (c.flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) != 0;
     Q.nrec = Q.tricubic ? 15 : 9;
     Q.rec = rec;
     Q.srec = srec;
@@ -1647,6 +1650,8 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_TEMPERATURE_FORCING", CH4_F_TEMPERATURE_FORCING},
       {"LAGRANGE_WRAP", CH4_F_LAGRANGE_WRAP},
       {"LAGRANGE_GRADIENT_BRD2", CH4_F_LAGRANGE_GRADIENT_BRD2},
+      {"LAGRANGE_ORIENTATION", CH4_F_LAGRANGE_ORIENTATION},
+      {"LAGRANGE_ORIENTATION_JEFFREY", CH4_F_LAGRANGE_ORIENTATION_JEFFREY},
       {"LB_FLUID_INITIAL_KOLMOGOROV", CH4_F_FLUID_INITIAL_KOLMOGOROV},
       {"LB_FLUID_INITIAL_POISEUILLE", CH4_F_FLUID_INITIAL_POISEUILLE},
       {"LB_FLUID_INITIAL_PERTURBATION", CH4_F_FLUID_INITIAL_PERTURBATION},
@@ -1782,6 +1787,10 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
       return why = "LAGRANGE_TWOWAY is implemented with LAGRANGE_TWOWAY_MOMENTUM", CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) && !(c->flags & CH4_F_LAGRANGE_TWOWAY))
       return why = "LAGRANGE_TWOWAY_TRICUBIC needs LAGRANGE_TWOWAY", CH4_ERR_UNSUPPORTED;
+    if ((c->flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) &&
+        (c->flags & (CH4_F_LAGRANGE_ORIENTATION | CH4_F_LAGRANGE_GRADIENT)) !=
+            (CH4_F_LAGRANGE_ORIENTATION | CH4_F_LAGRANGE_GRADIENT))
+      return why = "LAGRANGE_ORIENTATION_JEFFREY needs LAGRANGE_ORIENTATION and LAGRANGE_GRADIENT", CH4_ERR_UNSUPPORTED;
     if (!(c->time_dt_lagr_factor >= 1.0)) return why = "time_dt_lagr_factor must be >= 1", CH4_ERR_ARG;
   }
   return CH4_OK;

@@ -46,6 +46,8 @@ struct PartParams {
   int gradient;   // LAGRANGE_GRADIENT
   int addedmass;  // LAGRANGE_ADDEDMASS
   int gravity;    // LAGRANGE_GRAVITY
+  int orient;     // LAGRANGE_ORIENTATION: renormalise p every sub-step
+  int jeffery;    // LAGRANGE_ORIENTATION_JEFFREY: Jeffery's equation for p
   double g[3];    // gravity_x, gravity_y, gravity_z
   double* pf;     // [PF_TOTAL][np] by state slot
   const int* pid; // particle index of each slot
@@ -252,7 +254,64 @@ __device__ __forceinline__ void interp_cells(const double* __restrict__ ut4, int
 // step reads is loaded once, up front (independent loads), and every result is
 // stored once at the end; the arithmetic is the reference's, expression for
 // expression.
-template <typename A>
+// orientation of one particle (src/lagrange.c:3470-3752): Jeffery's equation
+// dp/dt = W p + f S p - (p . f S p) p with f = (a^2 - 1) / (1 + a^2) for aspect ratio a,
+// S and W the symmetric and antisymmetric halves of A_ij = d_j u_i; Euler on the first
+// step, Adams-Bashforth 2 after; p renormalised.  Sums in the reference's order.
+static __device__ __noinline__ void orient_particle(double* pf, long long np, int ip, const double* gr, bool jeffery,
+                                             bool first, double dtl) {
+#define F(name) pf[CH4_PF(name) * np + ip]
+  double p[3] = {F(px), F(py), F(pz)}, fo[3] = {F(dt_px), F(dt_py), F(dt_pz)};
+  if (jeffery) {
+    const double a = F(aspect_ratio);
+    const double fa = (a * a - 1.0) / (1.0 + a * a);
+    double S[3][3], W[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        S[i][j] = 0.5 * (gr[3 * i + j] + gr[3 * j + i]);
+        W[i][j] = 0.5 * (gr[3 * i + j] - gr[3 * j + i]);
+      }
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) S[i][j] *= fa;
+    double tmp[3] = {0.0, 0.0, 0.0}, oso = 0.0, f[3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) tmp[i] += S[i][j] * p[j];
+#pragma unroll
+    for (int i = 0; i < 3; i++) oso += p[i] * tmp[i];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      f[i] = 0.0;
+#pragma unroll
+      for (int j = 0; j < 3; j++) f[i] += W[i][j] * p[j] + (S[i][j] * p[j]);
+      f[i] -= p[i] * oso;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      p[i] = first ? p[i] + dtl * f[i] : p[i] + 0.5 * dtl * (3. * f[i] - fo[i]);
+      fo[i] = f[i];
+    }
+  }
+  double norm = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; i++) norm += p[i] * p[i];
+#pragma unroll
+  for (int i = 0; i < 3; i++) p[i] /= sqrt(norm);
+  F(px) = p[0];
+  F(py) = p[1];
+  F(pz) = p[2];
+  F(dt_px) = fo[0];
+  F(dt_py) = fo[1];
+  F(dt_pz) = fo[2];
+#undef F
+}
+
+template <typename A, bool ORIENT = false>
 __global__ void particle_substep_kernel(const PartParams<A> P) {
   const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= P.np) return;
@@ -436,6 +495,7 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     F(ay_old) = ay;
     F(az_old) = az;
   }
+  if constexpr (ORIENT) orient_particle(pf, np, ip, gr, P.jeffery != 0, first, dtl);
   // ---- LAGRANGE_WRAP of sendrecv_particles
   F(x) = pwrapd(xn, P.SX);
   F(z) = pwrapd(zn, P.SZ);

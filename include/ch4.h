@@ -104,6 +104,8 @@ enum {
   CH4_F_FLUID_LES_WALE = 1ull << 57,          /* WALE eddy viscosity */
   CH4_F_FLUID_LES_LOCAL_STRAIN = 1ull << 58,  /* |S| from the populations' stress tensor */
   CH4_F_LAGRANGE_TWOWAY_TRICUBIC = 1ull << 59, /* 64-cell cubic deposit, src/lagrange_feedback.c:117-146 */
+  CH4_F_LAGRANGE_ORIENTATION = 1ull << 60,    /* orientation p renormalised every sub-step, src/lagrange.c:3470-3752 */
+  CH4_F_LAGRANGE_ORIENTATION_JEFFREY = 1ull << 61, /* Jeffery's equation for p (needs LAGRANGE_GRADIENT) */
   /* any other *_INITIAL_* flag of define.h: ch4_initial_conditions refuses it
    * (the caller can still set the populations itself) */
   CH4_F_INITIAL_OTHER = 1ull << 63
@@ -178,6 +180,10 @@ typedef struct {
   double Dt_ux, Dt_uy, Dt_uz;
   double t, t_old, dt_t, Dt_t;
   double dx_t, dy_t, dz_t;
+  /* LAGRANGE_ORIENTATION: unit orientation p and its last dp/dt; JEFFREY: aspect ratio */
+  double px, py, pz;
+  double dt_px, dt_py, dt_pz;
+  double aspect_ratio;
 } ch4_particle;
 
 /* Global averages of dump_averages (src/output.c:63-~760), FP64 sums over the

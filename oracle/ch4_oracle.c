@@ -521,6 +521,49 @@ static void interp_particle_t(const ch4o_state *s, const double *tf, ch4_particl
 
 /* move_particles for point particles, src/lagrange.c:2934-3470 (tracers
  * tau_drag == 0, Eulerian probes tau_drag < 0, Stokes drag + added mass) */
+/* orientation (src/lagrange.c:3470-3752): Jeffery's equation with the reference's
+ * loops and sum order, Euler on the first step and AB2 after, then p renormalised */
+static void orient_particle(ch4_particle *p, int jeffery, int first, double dtl) {
+  double P[3] = {p->px, p->py, p->pz}, Fold[3] = {p->dt_px, p->dt_py, p->dt_pz};
+  if (jeffery) {
+    const double A[3][3] = {{p->dx_ux, p->dy_ux, p->dz_ux}, {p->dx_uy, p->dy_uy, p->dz_uy},
+                            {p->dx_uz, p->dy_uz, p->dz_uz}};
+    const double alpha = p->aspect_ratio;
+    const double f_alpha = (alpha * alpha - 1.0) / (1.0 + alpha * alpha);
+    double S[3][3], W[3][3], TMP[3] = {0, 0, 0}, Fv[3], oso = 0.0;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) S[i][j] = 0.5 * (A[i][j] + A[j][i]);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) W[i][j] = 0.5 * (A[i][j] - A[j][i]);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) S[i][j] *= f_alpha;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) TMP[i] += S[i][j] * P[j];
+    for (int i = 0; i < 3; i++) oso += P[i] * TMP[i];
+    for (int i = 0; i < 3; i++) {
+      Fv[i] = 0.0;
+      for (int j = 0; j < 3; j++) Fv[i] += W[i][j] * P[j] + (S[i][j] * P[j]);
+      Fv[i] -= P[i] * oso;
+    }
+    for (int i = 0; i < 3; i++) {
+      if (first)
+        P[i] = P[i] + dtl * Fv[i];
+      else
+        P[i] = P[i] + 0.5 * dtl * (3. * Fv[i] - Fold[i]);
+      Fold[i] = Fv[i];
+    }
+  }
+  double norm = 0.0;
+  for (int i = 0; i < 3; i++) norm += P[i] * P[i];
+  for (int i = 0; i < 3; i++) P[i] /= sqrt(norm);
+  p->px = P[0];
+  p->py = P[1];
+  p->pz = P[2];
+  p->dt_px = Fold[0];
+  p->dt_py = Fold[1];
+  p->dt_pz = Fold[2];
+}
+
 static void move_particle(const ch4o_state *s, ch4_particle *p, int first, double dtl) {
   if (s->tf) { /* time derivatives of t along the path, src/lagrange.c:2997-3010 */
     if (first) {
@@ -1028,7 +1071,11 @@ static void one_step(ch4o_state *s) {
       for (int ip = 0; ip < s->npart; ip++) interp_particle(s, s->uf, &s->part[ip]);
       if (s->tf)
         for (int ip = 0; ip < s->npart; ip++) interp_particle_t(s, s->tf, &s->part[ip]);
-      for (int ip = 0; ip < s->npart; ip++) move_particle(s, &s->part[ip], first, dtl);
+      for (int ip = 0; ip < s->npart; ip++) {
+        move_particle(s, &s->part[ip], first, dtl);
+        if (s->cfg.flags & CH4_F_LAGRANGE_ORIENTATION)
+          orient_particle(&s->part[ip], (s->cfg.flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) != 0, first, dtl);
+      }
       wrap_particles(s);
     }
   }

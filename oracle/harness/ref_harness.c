@@ -108,6 +108,12 @@ static void write_part_layout(void) {
   F(dx_t); F(dy_t); F(dz_t);
 #endif
 #endif
+#ifdef LAGRANGE_ORIENTATION
+  F(px); F(py); F(pz); F(dt_px); F(dt_py); F(dt_pz);
+#ifdef LAGRANGE_ORIENTATION_JEFFREY
+  F(aspect_ratio);
+#endif
+#endif
 #undef F
   fclose(fp);
 }

@@ -44,6 +44,9 @@ FLAGSETS = {
             "LB_FLUID_BC_Y", "LB_FLUID_LES"],
     "particles": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                   "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    "particles_or": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                     "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                     "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY"],
     "particles_1w": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS"],
     "trt": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
@@ -143,9 +146,13 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
             "time_dump_diagn": 1e12, "time_dump_lagr": 1e12,
             "tau_drag_types": max(1, int(cfg.particle_types)), "tau_drag_min": 1.0, "tau_drag_max": 1.0,
             "beta_coeff_types": 1, "beta_coeff_min": 1.0, "beta_coeff_max": 1.0}
+    keys = list(PARAM_KEYS)
+    if int(cfg.flags) & abi.FLAGS["LAGRANGE_ORIENTATION_JEFFREY"]:  # src/parameters.c, read by the reference
+        keys += ["aspect_ratio_types", "aspect_ratio_min", "aspect_ratio_max"]
+        vals.update({"aspect_ratio_types": 1, "aspect_ratio_min": 1.0, "aspect_ratio_max": 1.0})
     vals.update(overrides or {})
     with open(path, "w") as f:
-        for k in PARAM_KEYS:
+        for k in keys:
             v = vals[k] if k in vals else getattr(cfg, k)
             f.write("%s %r\n" % (k, float(v) if not isinstance(v, int) else v))
 

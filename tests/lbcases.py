@@ -66,6 +66,9 @@ CASES = {
     "particles_tc": dict(flagset="particles_tc", NX=10, NY=8, NZ=7, npart=300,
                          params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=9,
                                      time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_or": dict(flagset="particles_or", NX=10, NY=8, NZ=7, npart=300,
+                         params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=4,
+                                     time_dt_lagr_factor=2.0, particle_number=300)),
     "particles_1w": dict(flagset="particles_1w", NX=10, NY=8, NZ=7, npart=300,
                          params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=8,
                                      time_dt_lagr_factor=2.0, particle_number=300)),
@@ -112,6 +115,12 @@ def make_case(name, seed=0, storage=0, **over):
         state["h"] = pops(rng, c["NX"], c["NY"], c["NZ"], 0.3, 1e-1)
     if "LAGRANGE" in flags:
         state["part"] = make_particles(rng, c["npart"], c["NX"], c["NY"], c["NZ"])
+        if "LAGRANGE_ORIENTATION" in flags:  # random unit orientations, rods and discs
+            ratios = [1.0, 5.0, 0.2, 20.0]
+            for i, p in enumerate(state["part"]):
+                v = rng.normal(size=3)
+                p.px, p.py, p.pz = v / np.linalg.norm(v)
+                p.aspect_ratio = ratios[i % len(ratios)]
     return c["flagset"], cfg, state
 
 

@@ -47,6 +47,7 @@ def rel_l2(a, b):
 @pytest.mark.parametrize("name,nsteps", [("kolmogorov", 25), ("rb", 25), ("hit", 20), ("walls2", 25),
                                           ("scalar", 25), ("les", 25), ("particles", 12),
                                           ("particles_t", 12), ("particles_g", 12), ("particles_1w", 12),
+                                          ("particles_or", 12),
                                           ("trt", 25), ("trt_les", 25), ("les_vd", 25), ("les_ls", 25),
                                           ("les_ts", 25), ("particles_tc", 12)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):

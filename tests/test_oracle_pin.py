@@ -24,6 +24,7 @@ def _assert_same(a, b, what):
 @pytest.mark.parametrize("name,nsteps", [("kolmogorov", 20), ("rb", 20), ("hit", 15), ("walls2", 20),
                                           ("scalar", 20), ("les", 20), ("particles", 8),
                                           ("particles_t", 8), ("particles_g", 8), ("particles_1w", 8),
+                                          ("particles_or", 8),
                                           ("trt", 20), ("trt_les", 20), ("les_vd", 20), ("les_ls", 20),
                                           ("les_wale", 20), ("les_ts", 20), ("particles_tc", 8), ("nozero", 15),
                                           ("cpower", 15)])
