@@ -4,6 +4,7 @@ Produces ch4-project_b200/ch4b200/libch4b200.so in-tree (it travels with the
 repository snapshot; nothing is installed).  The FP64 kernels are compiled with
 FMA contraction off (-fmad=false) so they round like the reference CPU build.
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -42,21 +43,28 @@ def build(verbose=False):
         ("lb_f32.cu", []),
         ("noalloc.cu", ["-fmad=false"]),
     ]
+    jobs = []  # (command, object, keep the ptxas report)
     for src, extra in units:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if newer([s] + headers, o):
-            r = run([NVCC] + ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v"] + extra
-                    + ["-c", s, "-o", o])
-            with open(o + ".ptxas.txt", "w") as f:  # registers, spills and shared memory per kernel
-                f.write(r.stdout + r.stderr)
+            jobs.append(([NVCC] + ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
+                         + extra + ["-c", s, "-o", o], o, True))
         objs.append(o)
     for src in ["ch4_host.cpp", "h5file.cpp"]:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if newer([s] + headers, o):
-            run(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", CUDA_INC, "-c", s, "-o", o])
+            jobs.append((["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", CUDA_INC, "-c", s, "-o", o],
+                         o, False))
         objs.append(o)
+    # the translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: (j, run(j[0])), jobs))
+    for (cmd, o, keep), r in results:
+        if keep:
+            with open(o + ".ptxas.txt", "w") as f:  # registers, spills and shared memory per kernel
+                f.write(r.stdout + r.stderr)
     if newer(objs, OUT):
         run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", OUT] + objs)
     return OUT

@@ -1008,7 +1008,11 @@ struct Engine : EngineBase {
         return H->fail(CH4_ERR_NOMEM, "home-cell ranges");
     }
     if (fmoments()) {
-      fm_nblocks = (int)std::min<long long>(4 * 148, (N + FM_BLOCK - 1) / FM_BLOCK);
+      // A z-slab's partials are gathered with every other slab's into one z-ordered array,
+      // so every slab must write the same number of blocks whatever its own depth (uneven
+      // slabs differ by a plane): slabs always use the full count, blocks past the slab's
+      // cells writing zero partials.
+      fm_nblocks = c.nz_global > 0 ? 4 * 148 : (int)std::min<long long>(4 * 148, (N + FM_BLOCK - 1) / FM_BLOCK);
       const A init[12] = {A(0), A(0), A(0), A(1), A(1), A(1), A(0), A(0), A(0), A(1), A(1), A(1)};
       if (cudaMalloc(&fmbuf, sizeof init) != cudaSuccess ||
           cudaMalloc(&fmpart, sizeof(double) * FM_SUMS * 2 * (size_t)fm_nblocks) != cudaSuccess)
@@ -2450,15 +2454,22 @@ std::vector<PField> lagrange_fields(uint64_t fl, bool output_fluid) {
                            {"z", &P::z},       {"vx", &P::vx},             {"vy", &P::vy}, {"vz", &P::vz},
                            {"ax", &P::ax},     {"ay", &P::ay},             {"az", &P::az}};
   const bool grad = fl & CH4_F_LAGRANGE_GRADIENT, am = fl & CH4_F_LAGRANGE_ADDEDMASS;
+  // the fluid-at-particle and orientation datasets sit inside the LAGRANGE_GRADIENT block
+  // of output_particles (src/lagrange.c:1783-2014)
   if (grad) {
     v.insert(v.end(), {{"dx_ux", &P::dx_ux}, {"dy_ux", &P::dy_ux}, {"dz_ux", &P::dz_ux}, {"dx_uy", &P::dx_uy},
                        {"dy_uy", &P::dy_uy}, {"dz_uy", &P::dz_uy}, {"dx_uz", &P::dx_uz}, {"dy_uz", &P::dy_uz},
                        {"dz_uz", &P::dz_uz}});
     if (am) v.push_back({"beta_coeff", &P::beta_coeff});
-  }
-  if (output_fluid) {
-    v.insert(v.end(), {{"ux", &P::ux}, {"uy", &P::uy}, {"uz", &P::uz}});
-    if (am) v.insert(v.end(), {{"Dt_ux", &P::Dt_ux}, {"Dt_uy", &P::Dt_uy}, {"Dt_uz", &P::Dt_uz}});
+    if (output_fluid) {
+      v.insert(v.end(), {{"ux", &P::ux}, {"uy", &P::uy}, {"uz", &P::uz}});
+      if (am) v.insert(v.end(), {{"Dt_ux", &P::Dt_ux}, {"Dt_uy", &P::Dt_uy}, {"Dt_uz", &P::Dt_uz}});
+    }
+    if (fl & CH4_F_LAGRANGE_ORIENTATION) {
+      v.insert(v.end(), {{"px", &P::px}, {"py", &P::py}, {"pz", &P::pz}, {"dt_px", &P::dt_px}, {"dt_py", &P::dt_py},
+                         {"dt_pz", &P::dt_pz}});
+      if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) v.push_back({"aspect_ratio", &P::aspect_ratio});
+    }
   }
   if (fl & CH4_F_LB_TEMPERATURE) {
     v.insert(v.end(), {{"temperature", &P::t}, {"dt_t", &P::dt_t}});
@@ -2484,6 +2495,12 @@ std::vector<PField> part_members(uint64_t fl) {
                          {"dy_uy", &P::dy_uy}, {"dz_uy", &P::dz_uy}, {"dx_uz", &P::dx_uz}, {"dy_uz", &P::dy_uz},
                          {"dz_uz", &P::dz_uz}});
       if (fl & CH4_F_LAGRANGE_ADDEDMASS) v.push_back({"beta_coeff", &P::beta_coeff});
+      // write_point_particle_h5, src/lagrange.c:4365-4394
+      if (fl & CH4_F_LAGRANGE_ORIENTATION) {
+        v.insert(v.end(), {{"px", &P::px}, {"py", &P::py}, {"pz", &P::pz}, {"dt_px", &P::dt_px},
+                           {"dt_py", &P::dt_py}, {"dt_pz", &P::dt_pz}});
+        if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) v.push_back({"aspect_ratio", &P::aspect_ratio});
+      }
     }
   }
   if (fl & CH4_F_LB_TEMPERATURE) {
@@ -2539,14 +2556,19 @@ bool write_particle_xmf(const std::string& path, const std::string& h5name, int 
   scalar("tau_drag");
   joined("velocity", "Vector", {"vx", "vy", "vz"});
   joined("acceleration", "Vector", {"ax", "ay", "az"});
-  if (fl & CH4_F_LAGRANGE_GRADIENT) {
+  if (fl & CH4_F_LAGRANGE_GRADIENT) {  // src/lagrange.c:2271-2456
     joined("fluid velocity gradient", "Tensor",
            {"dx_ux", "dy_ux", "dz_ux", "dx_uy", "dy_uy", "dz_uy", "dx_uz", "dy_uz", "dz_uz"});
     if (fl & CH4_F_LAGRANGE_ADDEDMASS) scalar("beta_coeff");
-  }
-  if (output_fluid) {
-    joined("fluid_velocity", "Vector", {"ux", "uy", "uz"});
-    if (fl & CH4_F_LAGRANGE_ADDEDMASS) joined("fluid_acceleration", "Vector", {"Dt_ux", "Dt_uy", "Dt_uz"});
+    if (output_fluid) {
+      joined("fluid_velocity", "Vector", {"ux", "uy", "uz"});
+      if (fl & CH4_F_LAGRANGE_ADDEDMASS) joined("fluid_acceleration", "Vector", {"Dt_ux", "Dt_uy", "Dt_uz"});
+    }
+    if (fl & CH4_F_LAGRANGE_ORIENTATION) {
+      joined("orientation", "Vector", {"px", "py", "pz"});
+      joined("angular velocity", "Vector", {"dt_px", "dt_py", "dt_pz"});
+      if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) scalar("aspect_ratio");
+    }
   }
   if (fl & CH4_F_LB_TEMPERATURE) {
     scalar("temperature");

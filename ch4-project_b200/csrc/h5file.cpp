@@ -11,7 +11,7 @@ namespace h5 {
 namespace {
 
 constexpr uint64_t UNDEF = ~0ull;
-constexpr int LEAF_K = 16;              // a symbol-table node holds up to 2K entries
+constexpr int LEAF_K = 32;              // a symbol-table node holds up to 2K entries
 constexpr int INTERNAL_K = 16;          // a group B-tree node has room for 2K children
 constexpr uint64_t HEAP_FREE_NULL = 1;  // "no free block" in a local heap's free-list head
 constexpr size_t ENTRY = 40;            // symbol-table entry with 8-byte offsets
@@ -240,11 +240,12 @@ Type Type::compound(const std::vector<std::string>& names, int fsize) {
 
 bool write_file(const std::string& path, const std::vector<Group>& groups, std::string& err) {
   for (const Group& g : groups) {
-    if (g.datasets.size() > 2 * LEAF_K) return err = "more than 32 datasets in an HDF5 group", false;
+    if (g.datasets.size() > 2 * LEAF_K)
+      return err = "more than " + std::to_string(2 * LEAF_K) + " datasets in an HDF5 group", false;
     for (const Attribute& a : g.attributes)
       if (a.data.size() != a.type.size * elements(a.dims)) return err = "attribute " + a.name + ": size mismatch", false;
   }
-  if (groups.size() > 2 * LEAF_K) return err = "more than 32 HDF5 groups", false;
+  if (groups.size() > 2 * LEAF_K) return err = "more than " + std::to_string(2 * LEAF_K) + " HDF5 groups", false;
   std::vector<std::string> gnames;
   for (const Group& g : groups) gnames.push_back(g.name);
   const Children root = children_of(gnames);
@@ -461,6 +462,9 @@ bool parse_type(const uint8_t* p, size_t n, Type& t, size_t& used, std::string& 
     Member m;
     m.name.assign((const char*)p + q, len);
     q += ver >= 3 ? len + 1 : ((len + 8) / 8) * 8;
+    // every field read below must lie inside the message
+    const size_t need = ver >= 3 ? (size_t)offbytes : (ver == 1 ? 4 + 28 : 4);
+    if (q + need > n) return err = "truncated compound member " + m.name, false;
     if (ver >= 3) {
       m.offset = (uint32_t)get(p + q, offbytes);
       q += offbytes;
@@ -477,6 +481,8 @@ bool parse_type(const uint8_t* p, size_t n, Type& t, size_t& used, std::string& 
     if (q > n || !parse_type(p + q, n - q, mt, mu, err)) return false;
     if (mt.kind != Type::FLOAT) return err = "compound member " + m.name + " is not a float", false;
     m.fsize = (int)mt.size;
+    if ((uint64_t)m.offset + (uint64_t)m.fsize > size)
+      return err = "compound member " + m.name + " lies outside its record", false;
     t.members.push_back(m);
     q += mu;
   }

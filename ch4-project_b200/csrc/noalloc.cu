@@ -29,6 +29,9 @@ namespace {
 static __device__ __align__(256) double g_avg_partial[CH4_NOALLOC_MAX_BLOCKS * ch4::NAVG * 2];
 
 // device address of g_avg_partial, looked up once per device with that device current
+// and kept for the process's lifetime (a cudaDeviceReset reloads the module and would
+// leave this address stale; the header tells callers not to reset a device they use
+// this entry point on)
 constexpr int MAX_DEVICES = 64;
 double* g_partial_addr[MAX_DEVICES] = {nullptr};
 std::mutex g_setup_mutex;

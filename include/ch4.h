@@ -473,7 +473,9 @@ ch4_status ch4_ensemble_set_shape(ch4_ensemble *e, int block, int rows_per_tile)
  * library until exit); lattices above CH4_NOALLOC_MAX_BLOCKS *
  * CH4_NOALLOC_CELLS_PER_BLOCK cells are refused with CH4_ERR_ARG.  The first call
  * on a device looks up that array's device address (make it before any stream
- * capture); all calls share the array, so calls that overlap on the GPU race.
+ * capture) and keeps it for the life of the process: a caller that resets a
+ * device (cudaDeviceReset) must not call this entry point on that device again in
+ * the same process.  All calls share the array, so calls that overlap on the GPU race.
  * Asynchronous on `stream` (a cudaStream_t, NULL = default stream). */
 #define CH4_NOALLOC_MAX_BLOCKS 2048
 #define CH4_NOALLOC_CELLS_PER_BLOCK 65536

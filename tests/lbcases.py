@@ -100,8 +100,11 @@ def make_particles(rng, n, NX, NY, NZ):
     return parts
 
 
-def make_case(name, seed=0, storage=0, **over):
+def make_case(name, seed=0, storage=0, dims=None, **over):
+    """(flagset, config, initial state) of a case; `dims` = (NX, NY, NZ) overrides its lattice."""
     c = dict(CASES[name])
+    if dims is not None:
+        c["NX"], c["NY"], c["NZ"] = dims
     params = dict(c["params"])
     params.update(over)
     flags = O.FLAGSETS[c["flagset"]]

@@ -117,14 +117,18 @@ def _fields(flags, output_fluid):
     """/lagrange dataset -> ch4_particle field, in output_particles' order."""
     f = [(n, n) for n in ("name", "tau_drag", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")]
     grad, am = flags & abi.FLAGS["LAGRANGE_GRADIENT"], flags & abi.FLAGS["LAGRANGE_ADDEDMASS"]
-    if grad:
+    if grad:  # the fluid and orientation datasets sit inside the gradient block (src/lagrange.c:1783-2014)
         f += [(n, n) for n in ("dx_ux", "dy_ux", "dz_ux", "dx_uy", "dy_uy", "dz_uy", "dx_uz", "dy_uz", "dz_uz")]
         if am:
             f.append(("beta_coeff", "beta_coeff"))
-    if output_fluid:
-        f += [("ux", "ux"), ("uy", "uy"), ("uz", "uz")]
-        if am:
-            f += [("Dt_ux", "Dt_ux"), ("Dt_uy", "Dt_uy"), ("Dt_uz", "Dt_uz")]
+        if output_fluid:
+            f += [("ux", "ux"), ("uy", "uy"), ("uz", "uz")]
+            if am:
+                f += [("Dt_ux", "Dt_ux"), ("Dt_uy", "Dt_uy"), ("Dt_uz", "Dt_uz")]
+        if flags & abi.FLAGS["LAGRANGE_ORIENTATION"]:
+            f += [(n, n) for n in ("px", "py", "pz", "dt_px", "dt_py", "dt_pz")]
+            if flags & abi.FLAGS["LAGRANGE_ORIENTATION_JEFFREY"]:
+                f.append(("aspect_ratio", "aspect_ratio"))
     if flags & abi.FLAGS["LB_TEMPERATURE"]:
         f += [("temperature", "t"), ("dt_t", "dt_t")]
         if grad:
@@ -143,7 +147,7 @@ def _particle_sim(name, seed, nsteps):
     return cfg, state, sim
 
 
-@pytest.mark.parametrize("name", ["particles", "particles_t"])
+@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or"])
 def test_particle_file_holds_the_particles(name, tmp_path):
     cfg, state, sim = _particle_sim(name, 65, 4)
     with sim:
@@ -161,7 +165,7 @@ def test_particle_file_holds_the_particles(name, tmp_path):
         assert "particle_4.h5:/lagrange/%s\n" % d in xmf, d
 
 
-@pytest.mark.parametrize("name", ["particles", "particles_t"])
+@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or"])
 def test_part_file_restart(name, tmp_path):
     cfg, state, a = _particle_sim(name, 66, 5)
     n = len(state["part"])
@@ -201,5 +205,8 @@ def test_part_file_restart(name, tmp_path):
         b.step(3)
         c.step(3)
         pb, pc = b.get_particles(n), c.get_particles(n)
-        for m in ("x", "y", "z", "vx", "vy", "vz"):
+        for m in ("x", "y", "z", "vx", "vy", "vz", "px", "py", "pz"):
             assert np.array_equal([getattr(p, m) for p in pb], [getattr(p, m) for p in pc]), m
+        if cfg.flags & abi.FLAGS["LAGRANGE_ORIENTATION"]:  # the orientation survives the restart
+            assert np.isfinite([p.px for p in pb]).all()
+            assert np.array_equal(rec["aspect_ratio"], [p.aspect_ratio for p in parts])

@@ -84,6 +84,32 @@ def test_slabs_with_global_force_corrections(name, nslabs):
             s.close()
 
 
+@pytest.mark.parametrize("name", ["nozero", "cpower"])
+def test_uneven_slabs_with_global_force_corrections(name):
+    """Slabs of different depth (NZ = 7 on 2 slabs: 4 and 3 planes, both more than one
+    reduction block of cells) gather the same number of block partials each, so the
+    z-ordered gather lines up and every slab forms the whole lattice's corrections."""
+    _, cfg, state = make_case(name, seed=47, dims=(24, 16, 7))
+    nsteps = 5
+    a = whole(cfg, state, nsteps)
+    bnds = slab.bounds(cfg.NZ, 2)
+    assert [n for _, n in bnds] == [4, 3]
+    slabs = [slab.Slab(cfg, z0, nz) for z0, nz in bnds]
+    try:
+        slab.use_local_gather(slabs)
+        for s in slabs:
+            for k, v in pop_items(state):
+                s.set_pop(k, v)
+        slab.initialize_local(slabs)
+        slab.step_local(slabs, nsteps)
+        for k, _ in pop_items(state):
+            b = np.concatenate([s.sim.get_pop(k) for s in slabs])
+            assert np.linalg.norm(b - a[k]) <= 1e-12 * np.linalg.norm(a[k]), k
+    finally:
+        for s in slabs:
+            s.close()
+
+
 @pytest.mark.parametrize("name,nslabs", [("les", 2), ("les_vd", 3), ("les_ls", 2), ("les_wale", 2), ("les_ts", 2),
                                           ("trt_les", 3)])
 def test_les_slabs_reproduce_the_single_lattice(name, nslabs):

@@ -2,7 +2,7 @@
 through it parses under an independent reader written from the file format specification
 (tests/h5spec.py, which asserts the structural rules a libhdf5 reader relies on), with
 every value where it was put, and the library's own reader reads it back by path and
-member name.  Groups hold up to 32 entries in one symbol-table node (12 here)."""
+member name.  Groups hold up to 64 entries in one symbol-table node (12 here)."""
 import os
 import shutil
 import subprocess
