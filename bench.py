@@ -10,9 +10,15 @@ dataset); FP32 arithmetic with FP32 population storage by default.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|f64]
   python bench.py --impl reference ...   (the reference solver's own CPU build)
 
-With N > 1 (torchrun, one process per GPU) every rank advances its own lattice
-(independent replicas: the single-lattice path has no exchange step here), timed as the
-max over ranks.  Prints ONE JSON line on rank 0.
+With N > 1 the lattice is NX x NY x (N*NZ), one z-slab of NX x NY x NZ per GPU (one
+process per GPU; launched under torchrun, or by this script itself when --gpus N > 1 is
+given without it), the slab faces exchanged over NCCL after every step (weak scaling),
+timed as the max over ranks.  Prints ONE JSON line on rank 0.
+
+At N = 1 the line also carries the reduced-precision error against the FP64 path on the
+same input (`error_vs_fp64`: u and T after the timed steps, Nusselt number and kinetic
+energy over the configuration's 20,000-step run) and the FP64 path's own throughput
+(`fp64`), and the end-to-end run's phases (`e2e.breakdown`).
 """
 import argparse
 import json
@@ -204,12 +210,15 @@ def cpu_sample_steps():
 
 
 def run_reference_arm(args):
+    """The reference's own CPU build on all host cores: W untimed warm-up steps in one
+    run, then exactly K timed steps of the whole lattice in another (the harness times
+    its step loop)."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
     if args.warmup > 0:
-        cpu_reference_run(1)
-    mlups, cores, sample = cpu_reference_run(cpu_sample_steps())
+        cpu_reference_run(args.warmup)
+    mlups, cores, sample = cpu_reference_run(args.steps)
     if mlups is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return 0
@@ -223,6 +232,82 @@ def run_reference_arm(args):
     }
     print(json.dumps(line))
     return 0
+
+
+def error_vs_fp64(W, K, window=20000, every=1000):
+    """FP32 and FP16-deviation storage against the FP64 path, all three from the same
+    initial state: relative L2 of u and T after the bench's W + K steps, and the Nusselt
+    number (nuy, src/output.c:332-349,577-579) and kinetic energy (ene) every `every`
+    steps up to `window` steps (the configuration's 20,000-step run).  Also the FP64
+    path's own throughput (K steps after W, CUDA events on its stream).  The FP64 path is
+    bit-identical to the reference's CPU build, so these are errors against the reference."""
+    import torch
+    import ch4b200
+    p0, g0 = initial_state(1234)
+    marks = list(range(every, window + 1, every))
+    runs = {}
+    fp64 = None
+    cells = NX * NY * NZ
+    for st in ("f64", "f32", "f16"):
+        with ch4b200.Simulation(make_cfg(st)) as sim:
+            sim.set_pop("p", p0)
+            sim.set_pop("g", g0)
+            sim.initialize()
+            sim.step(W)
+            sec = _event_time(sim.stream_handle, lambda: sim.step(K))
+            f = sim.fields()
+            done = W + K
+            nu, ke = [], []
+            for m in marks:
+                if m > done:
+                    sim.step(m - done)
+                    done = m
+                a = sim.averages()
+                nu.append(a["nuy"])
+                ke.append(a["ene"])
+            runs[st] = {"u": f["u"], "t": f["t"], "nu": np.array(nu), "ke": np.array(ke)}
+            del f
+            if st == "f64":
+                peak, kind = measured_peak()
+                ms = sec / K * 1e3
+                fp64 = {"value": cells / (ms * 1e-3) / 1e6, "unit": "MLUPS", "ms_per_step": ms, "steps": K,
+                        "warmup": W, "bytes_per_cell": BYTES_PER_CELL["f64"],
+                        "roofline_frac": BYTES_PER_CELL["f64"] * cells / (ms * 1e-3) / 1e9 / peak,
+                        "peak_kind": kind}
+    ref = runs["f64"]
+    rel = lambda a, b: float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+    out = {"against": "FP64 path (bit-identical to the reference CPU build)", "lattice": [NX, NY, NZ],
+           "fields_after_steps": W + K, "window_steps": [every, window], "every": every,
+           "nu_fp64": [float(ref["nu"][0]), float(ref["nu"][-1])],
+           "ke_fp64": [float(ref["ke"][0]), float(ref["ke"][-1])]}
+    for st in ("f32", "f16"):
+        r = runs[st]
+        enu = np.abs(r["nu"] - ref["nu"]) / np.abs(ref["nu"])
+        eke = np.abs(r["ke"] - ref["ke"]) / np.abs(ref["ke"])
+        out[st] = {"u_rel_l2": rel(r["u"], ref["u"]), "t_rel_l2": rel(r["t"], ref["t"]),
+                   "nu_rel_err_max": float(enu.max()), "nu_rel_err_final": float(enu[-1]),
+                   "nu_window_mean_rel_err": float(abs(r["nu"].mean() - ref["nu"].mean()) / abs(ref["nu"].mean())),
+                   "ke_rel_err_max": float(eke.max()), "ke_rel_err_final": float(eke[-1])}
+    return out, fp64
+
+
+def spawn_ranks(args):
+    """--gpus N > 1 without a launcher: run this script as N local ranks (one per GPU)
+    under torch.distributed.run; rank 0 prints the line."""
+    import signal
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    pr = subprocess.Popen(cmd, start_new_session=True)
+    try:
+        return pr.wait(timeout=1800)
+    except subprocess.TimeoutExpired:
+        os.killpg(pr.pid, signal.SIGTERM)
+        pr.wait(timeout=60)
+        return 1
 
 
 # ---------------------------------------------------------------------------
@@ -547,7 +632,12 @@ def main():
     ap.add_argument("--step-scale", type=float, default=1.0)
     ap.add_argument("--hit-size", type=int, default=256)
     ap.add_argument("--particles", type=int, default=1000000)
+    ap.add_argument("--no-error", action="store_true", help="skip the FP32/FP16 error study against FP64")
+    ap.add_argument("--error-window", type=int, default=20000)
+    ap.add_argument("--error-every", type=int, default=1000)
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "ours":
+        return spawn_ranks(args)
     if args.workload == "ensemble":
         return bench_ensemble(args)
     if args.workload == "serve":
@@ -627,26 +717,46 @@ def main():
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
+        ph = {}
         t0 = time.perf_counter()
         s2, run2 = new_sim()
         with s2:
+            t1 = time.perf_counter()
             s2.set_pop("p", p0)
             s2.set_pop("g", g0)
+            t2 = time.perf_counter()
             s2.initialize()
+            t3 = time.perf_counter()
             run2(K)
+            s2.synchronize()
+            t4 = time.perf_counter()
             f2 = s2.fields()
-        t1 = time.perf_counter()
-        sec = t1 - t0
+            t5 = time.perf_counter()
+        t6 = time.perf_counter()
+        sec = t6 - t0
         if world > 1:
             t = torch.tensor([sec], device="cuda")
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             sec = float(t.item())
-        h2d = 2 * p0.nbytes
+        # bytes over the bus: the library rounds the caller's FP64 populations to the
+        # arithmetic type on the host before the copy (FP32 forms: 4 bytes per value)
+        wire = 8 if args.storage == "f64" else 4
+        h2d = 2 * p0.size * wire
         d2h = 5 * cells * 8  # dens, u(3), t of ch4_get_fields (no scalar set: s is zero-filled on the host)
+        ph = {"create_s": t1 - t0, "upload_s": t2 - t1, "upload_gbps": h2d / (t2 - t1) / 1e9,
+              "initialize_s": t3 - t2, "steps_s": t4 - t3, "download_s": t5 - t4,
+              "download_gbps": d2h / (t5 - t4) / 1e9, "close_s": t6 - t5,
+              "caller_bytes_uploaded": 2 * p0.nbytes}
         e2e = {"value": world * cells * K / sec / 1e6, "unit": "MLUPS",
                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
-               "includes": "create + AoS FP64 upload of p,g + initialize + K steps + hydro-field download"}
+               "includes": "create + AoS FP64 upload of p,g (rounded to the storage's arithmetic type on the host) "
+                           "+ initialize + K steps + hydro-field download",
+               "breakdown": ph}
         del f2
+
+    err = fp64 = None
+    if world == 1 and not args.no_error:
+        err, fp64 = error_vs_fp64(W, K, args.error_window, args.error_every)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -672,6 +782,8 @@ def main():
             "gpu_launches": K * (3 if slab_mode else 1),  # lb_step (+ halo pack and unpack per step)
             "clocks": clk.summary(),
             "finite": finite,
+            "error_vs_fp64": err,
+            "fp64": fp64,
         }
         print(json.dumps(line))
     if world > 1:

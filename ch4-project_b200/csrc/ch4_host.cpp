@@ -534,6 +534,15 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.shift[2] = (float)(0.5 * (c.S_bot + c.S_top));
 }
 
+// one AoS row between the caller's FP64 array and a staging chunk of the arithmetic type
+inline void copy_row(double* dst, const double* src, size_t n) { std::memcpy(dst, src, n * sizeof(double)); }
+inline void copy_row(float* dst, const double* src, size_t n) {
+  for (size_t i = 0; i < n; i++) dst[i] = (float)src[i];  // round to nearest, as the device's conversion
+}
+inline void copy_row(double* dst, const float* src, size_t n) {
+  for (size_t i = 0; i < n; i++) dst[i] = (double)src[i];
+}
+
 template <typename A>
 struct Engine : EngineBase {
   ch4_handle* H;
@@ -543,6 +552,10 @@ struct Engine : EngineBase {
   size_t sbytes;
   void* f[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
   int cur = 0;  // which of the two buffers holds f^n
+  // sets still owed the rest state of a new handle (p = w, g = h = 0): filled on first
+  // use, so a caller that uploads its own populations never pays for the fill
+  bool rest_pending[3] = {false, false, false};
+  bool filling = false;
   A *tprev = nullptr, *sprev = nullptr;
   A *kol = nullptr;
   A *ules = nullptr, *tau_les = nullptr;
@@ -550,11 +563,13 @@ struct Engine : EngineBase {
   A* vd = nullptr;  // LB_FLUID_LES_VANDRIEST: pow(C_smag(y), 2) per row
   A *hit_ring = nullptr;  // (CHUNK+1) phase-table slots
   A *hit_last = nullptr;  // tables of the latest phases (those of F^n)
-  double* staging_d = nullptr;  // device AoS chunk
-  double* staging_h = nullptr;  // pinned host chunk
+  // AoS chunks in the arithmetic type A (the host rounds the caller's FP64 values to A
+  // while it copies them in, so FP32 handles move half the bytes over the bus)
+  A* staging_d = nullptr;  // device AoS chunk
+  A* staging_h = nullptr;  // pinned host chunk
   // second pair: the host fills one pinned chunk while the other is copied and converted
-  double* staging_d2 = nullptr;
-  double* staging_h2 = nullptr;
+  A* staging_d2 = nullptr;
+  A* staging_h2 = nullptr;
   size_t staging_bytes = 0, hit_h_bytes = 0;
   cudaEvent_t up_ev[2] = {nullptr, nullptr};
   A* hit_h = nullptr;           // pinned host phase tables
@@ -717,6 +732,7 @@ struct Engine : EngineBase {
 
   // dump_averages (src/output.c:63-~720): hydro fields in FP64, deterministic sums, normalisation
   ch4_status averages(ch4_averages* out) override {
+    if (ch4_status rs = ready()) return rs;
     bind_pops(cur);
     const size_t n1 = (size_t)N;
     const int nblocks = (int)std::min<long long>(4 * 148, (N + AVG_BLOCK - 1) / AVG_BLOCK);
@@ -756,6 +772,7 @@ struct Engine : EngineBase {
   }
 
   ch4_status diag_sums(double* glob, double* rx, double* ry, double* rz) override {
+    if (ch4_status rs = ready()) return rs;
     bind_pops(cur);
     const size_t n1 = (size_t)N;
     const int nblocks = (int)std::min<long long>(4 * 148, (N + DIAG_BLOCK - 1) / DIAG_BLOCK);
@@ -894,6 +911,7 @@ struct Engine : EngineBase {
   // or the fixed-value rule of a temperature/scalar wall), not a stream from across the
   // face, so that row stays out of the exchange (a slip wall streams it: exchanged).
   ch4_status halo(bool pack, void* a, void* b) override {
+    if (ch4_status rs = ready()) return rs;
     const size_t row = (size_t)c.NX * sbytes, plane = row * c.NY, top = (size_t)(c.NZ - 1) * plane;
     const uint32_t F = P.feat;
     const bool local_top[3] = {(F & K_FWALL) && !(F & K_FSLIP_P), (F & K_TWALL) != 0, (F & K_SWALL) != 0};
@@ -1047,31 +1065,22 @@ struct Engine : EngineBase {
     if (!(hit_h = static_cast<A*>(PinnedPool::get(hit_h_bytes)))) return H->fail(CH4_ERR_NOMEM, "pinned hit tables");
     if (cudaEventCreateWithFlags(&hit_ev, cudaEventDisableTiming) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "event");
     // staging for AoS exchange: a few z-planes at a time (<= 64 MiB)
-    const size_t plane = (size_t)c.NX * c.NY * NPOP * sizeof(double);
+    const size_t plane = (size_t)c.NX * c.NY * NPOP * sizeof(A);
     chunk_planes = std::max<size_t>(1, std::min<size_t>((size_t)c.NZ, (64u << 20) / plane));
     if (cudaMalloc(&staging_d, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "staging");
     staging_bytes = chunk_planes * plane;
-    if (!(staging_h = static_cast<double*>(PinnedPool::get(staging_bytes))))
+    if (!(staging_h = static_cast<A*>(PinnedPool::get(staging_bytes))))
       return H->fail(CH4_ERR_NOMEM, "pinned staging");
     if (chunk_planes < (size_t)c.NZ) {  // more than one chunk: double-buffer the upload
       if (cudaMalloc(&staging_d2, chunk_planes * plane) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "staging");
-      if (!(staging_h2 = static_cast<double*>(PinnedPool::get(staging_bytes))))
+      if (!(staging_h2 = static_cast<A*>(PinnedPool::get(staging_bytes))))
         return H->fail(CH4_ERR_NOMEM, "pinned staging");
     }
     for (cudaEvent_t& e : up_ev)
       if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "event");
     fill_params();
-    // rest state p = w (src/initial_conditions.c:45), g = h = 0: one z-slab chunk of it is
-    // built in the pinned staging buffer, copied once, and converted into every chunk
-    const size_t rest_n = (size_t)c.NX * c.NY * NPOP * chunk_planes;
-    for (size_t i = 0; i < rest_n; i++) staging_h[i] = H->lat.w[i % NPOP];
-    ch4_status st = fill_repeated(0);
-    if (st) return st;
-    if (nsets_on[1] || nsets_on[2]) {
-      std::fill(staging_h, staging_h + rest_n, 0.0);
-      if (nsets_on[1] && (st = fill_repeated(1))) return st;
-      if (nsets_on[2] && (st = fill_repeated(2))) return st;
-    }
+    for (int s = 0; s < 3; s++) rest_pending[s] = nsets_on[s] != 0;
+    ch4_status st;
     // Kolmogorov tables (src/forcing.c:390-400), host libm
     {
       std::vector<A> t(nk);
@@ -1115,7 +1124,7 @@ struct Engine : EngineBase {
 
   // every z-slab chunk of a set <- the AoS chunk held in staging_h
   ch4_status fill_repeated(int set) {
-    const size_t bytes = (size_t)c.NX * c.NY * NPOP * chunk_planes * sizeof(double);
+    const size_t bytes = (size_t)c.NX * c.NY * NPOP * chunk_planes * sizeof(A);
     bind_pops(cur);
     ch4_status st = H->cuda(cudaMemcpyAsync(staging_d, staging_h, bytes, cudaMemcpyHostToDevice, H->stream), "fill");
     for (int z0 = 0; z0 < c.NZ && !st; z0 += (int)chunk_planes) {
@@ -1125,6 +1134,24 @@ struct Engine : EngineBase {
     return st ? st : H->cuda(cudaStreamSynchronize(H->stream), "fill sync");
   }
 
+  // the rest state p = w (src/initial_conditions.c:45), g = h = 0 in every set the caller
+  // has not uploaded: one z-slab chunk of it is built in the pinned staging buffer, copied
+  // once, and converted into every chunk on the device
+  ch4_status ready() {
+    if (filling) return CH4_OK;
+    filling = true;
+    const size_t rest_n = (size_t)c.NX * c.NY * NPOP * chunk_planes;
+    ch4_status st = CH4_OK;
+    for (int s = 0; s < 3 && !st; s++) {
+      if (!rest_pending[s]) continue;
+      for (size_t i = 0; i < rest_n; i++) staging_h[i] = (A)(s == 0 ? H->lat.w[i % NPOP] : 0.0);
+      st = fill_repeated(s);
+      rest_pending[s] = false;
+    }
+    filling = false;
+    return st;
+  }
+
   // Reference-layout AoS (with `brd` halo) -> device SoA, in z-slab chunks through
   // pinned staging.  With two staging pairs the host copies chunk k+1 (rows split over
   // host threads) while chunk k is transferred and converted.
@@ -1132,23 +1159,22 @@ struct Engine : EngineBase {
     const size_t row = (size_t)c.NX * NPOP;
     const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
     bind_pops(cur);
-    double* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
-    double* db[2] = {staging_d, staging_d2 ? staging_d2 : staging_d};
+    A* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
+    A* db[2] = {staging_d, staging_d2 ? staging_d2 : staging_d};
     int b = 0;
     ch4_status st;
     for (int z0 = 0; z0 < c.NZ; z0 += (int)chunk_planes) {
       int nz = std::min<int>((int)chunk_planes, c.NZ - z0);
       // the copy out of hb[b] two chunks ago must be finished before it is refilled
       if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "upload wait"))) return st;
-      double* dst = hb[b];
+      A* dst = hb[b];
       host_parallel((size_t)nz * c.NY, 64, [&](size_t r0, size_t r1) {
         for (size_t r = r0; r < r1; r++) {
           const size_t zl = r / c.NY, y = r % c.NY;
-          std::memcpy(dst + r * row, aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
-                      row * sizeof(double));
+          copy_row(dst + r * row, aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, row);
         }
       });
-      if ((st = H->cuda(cudaMemcpyAsync(db[b], dst, (size_t)nz * c.NY * row * sizeof(double), cudaMemcpyHostToDevice,
+      if ((st = H->cuda(cudaMemcpyAsync(db[b], dst, (size_t)nz * c.NY * row * sizeof(A), cudaMemcpyHostToDevice,
                                         H->stream),
                         "upload")))
         return st;
@@ -1163,17 +1189,19 @@ struct Engine : EngineBase {
   ch4_status set_pop(int set, const double* aos, int brd) override {
     if (!nsets_on[set]) return H->fail(CH4_ERR_ARG, "population set %d is not enabled", set);
     H->initialized = false;
+    rest_pending[set] = false;
     return upload_chunks(set, aos, brd);
   }
 
   ch4_status get_pop(int set, double* aos, int brd) override {
+    if (ch4_status rs = ready()) return rs;
     if (!nsets_on[set]) return H->fail(CH4_ERR_ARG, "population set %d is not enabled", set);
     const size_t row = (size_t)c.NX * NPOP;
     const size_t PX = c.NX + 2 * brd, PY = c.NY + 2 * brd;
     bind_pops(cur);
     // chunk k+1 is converted and transferred while the host threads unpack chunk k
-    double* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
-    double* db[2] = {staging_d, staging_d2 ? staging_d2 : staging_d};
+    A* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
+    A* db[2] = {staging_d, staging_d2 ? staging_d2 : staging_d};
     const int nchunks = (int)((c.NZ + chunk_planes - 1) / chunk_planes);
     const int depth = staging_h2 ? 2 : 1;
     ch4_status st;
@@ -1182,7 +1210,7 @@ struct Engine : EngineBase {
       ch4_status s2;
       if ((s2 = H->cuda(launch_soa_to_aos(P, shape, set, f[set][cur], db[b], z0, nz, H->stream), "soa_to_aos")))
         return s2;
-      if ((s2 = H->cuda(cudaMemcpyAsync(hb[b], db[b], (size_t)nz * c.NY * row * sizeof(double),
+      if ((s2 = H->cuda(cudaMemcpyAsync(hb[b], db[b], (size_t)nz * c.NY * row * sizeof(A),
                                         cudaMemcpyDeviceToHost, H->stream),
                         "download")))
         return s2;
@@ -1193,12 +1221,11 @@ struct Engine : EngineBase {
     for (int k = 0; k < nchunks; k++) {
       const int z0 = k * (int)chunk_planes, nz = std::min<int>((int)chunk_planes, c.NZ - z0), b = k & 1;
       if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "download sync"))) return st;
-      const double* srcb = hb[b];
+      const A* srcb = hb[b];
       host_parallel((size_t)nz * c.NY, 64, [&](size_t r0, size_t r1) {
         for (size_t r = r0; r < r1; r++) {
           const size_t zl = r / c.NY, y = r % c.NY;
-          std::memcpy(aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, srcb + r * row,
-                      row * sizeof(double));
+          copy_row(aos + (((z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, srcb + r * row, row);
         }
       });
       if (k + depth < nchunks && (st = issue(k + depth))) return st;
@@ -1243,6 +1270,7 @@ struct Engine : EngineBase {
   }
 
   ch4_status initialize() override {
+    if (ch4_status rs = ready()) return rs;
     bind_pops(cur);
     ch4_status st;
     if (nsets_on[1] || nsets_on[2])
@@ -1315,6 +1343,7 @@ struct Engine : EngineBase {
   }
 
   ch4_status step(int n) override {
+    if (ch4_status rs = ready()) return rs;
     ch4_status st;
     const bool hit = (c.flags & CH4_F_FORCING_HIT) != 0;
     const size_t slot = (size_t)NK * L();
@@ -1398,8 +1427,8 @@ struct Engine : EngineBase {
   // device array -> caller's host array through the two pinned staging buffers: chunk
   // k+1 is in flight while host threads copy chunk k out
   ch4_status download_bounce(const double* dsrc, double* hdst, size_t count) {
-    const size_t cap = chunk_planes * (size_t)c.NX * c.NY * NPOP;
-    double* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
+    const size_t cap = staging_bytes / sizeof(double);
+    double* hb[2] = {reinterpret_cast<double*>(staging_h), reinterpret_cast<double*>(staging_h2 ? staging_h2 : staging_h)};
     const size_t nchunks = (count + cap - 1) / cap;
     const size_t depth = staging_h2 ? 2 : 1;
     ch4_status st;
@@ -1425,6 +1454,7 @@ struct Engine : EngineBase {
   }
 
   ch4_status fields(double* dens, double* u, double* t, double* s, double* force, int brd) override {
+    if (ch4_status rs = ready()) return rs;
     bind_pops(cur);
     ch4_status st;
     double* d = nullptr;
@@ -2762,17 +2792,18 @@ size_t slot_bytes(const ch4_config& c, int storage) {
 // AoS FP64 (halo width brd) <-> SoA device storage of one set, through a temporary staging buffer
 ch4_status move_pop(const StepParams<float>& P, LaunchShape shape, int set, void* soa, double* host, int brd, bool up,
                     cudaStream_t st, std::string& err) {
+  // FP32 staging: the caller's FP64 values are rounded to the arithmetic type on the host
   const int NX = P.NX, NY = P.NY, NZ = P.NZ;
   const size_t row = (size_t)NX * NPOP, plane = row * NY;
-  const int nzc = (int)std::max<size_t>(1, std::min<size_t>((size_t)NZ, (32u << 20) / (plane * sizeof(double))));
-  double* dstage = nullptr;
-  std::vector<double> hstage(plane * nzc);
+  const int nzc = (int)std::max<size_t>(1, std::min<size_t>((size_t)NZ, (32u << 20) / (plane * sizeof(float))));
+  float* dstage = nullptr;
+  std::vector<float> hstage(plane * nzc);
   auto fail = [&](const char* what, cudaError_t e) {
     err = std::string(what) + ": " + cudaGetErrorString(e);
     if (dstage) cudaFree(dstage);
     return CH4_ERR_CUDA;
   };
-  cudaError_t e = cudaMalloc(&dstage, plane * nzc * sizeof(double));
+  cudaError_t e = cudaMalloc(&dstage, plane * nzc * sizeof(float));
   if (e) return fail("staging", e);
   const size_t PX = NX + 2 * brd, PY = NY + 2 * brd;
   for (int z0 = 0; z0 < NZ; z0 += nzc) {
@@ -2780,21 +2811,21 @@ ch4_status move_pop(const StepParams<float>& P, LaunchShape shape, int set, void
     if (up) {
       for (int zl = 0; zl < nz; zl++)
         for (int y = 0; y < NY; y++)
-          std::memcpy(hstage.data() + ((size_t)zl * NY + y) * row,
-                      host + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, row * sizeof(double));
-      if ((e = cudaMemcpyAsync(dstage, hstage.data(), plane * nz * sizeof(double), cudaMemcpyHostToDevice, st)))
+          copy_row(hstage.data() + ((size_t)zl * NY + y) * row,
+                   host + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP, row);
+      if ((e = cudaMemcpyAsync(dstage, hstage.data(), plane * nz * sizeof(float), cudaMemcpyHostToDevice, st)))
         return fail("upload", e);
       if ((e = launch_aos_to_soa(P, shape, set, dstage, soa, z0, nz, st))) return fail("aos_to_soa", e);
       if ((e = cudaStreamSynchronize(st))) return fail("upload sync", e);
     } else {
       if ((e = launch_soa_to_aos(P, shape, set, soa, dstage, z0, nz, st))) return fail("soa_to_aos", e);
-      if ((e = cudaMemcpyAsync(hstage.data(), dstage, plane * nz * sizeof(double), cudaMemcpyDeviceToHost, st)))
+      if ((e = cudaMemcpyAsync(hstage.data(), dstage, plane * nz * sizeof(float), cudaMemcpyDeviceToHost, st)))
         return fail("download", e);
       if ((e = cudaStreamSynchronize(st))) return fail("download sync", e);
       for (int zl = 0; zl < nz; zl++)
         for (int y = 0; y < NY; y++)
-          std::memcpy(host + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
-                      hstage.data() + ((size_t)zl * NY + y) * row, row * sizeof(double));
+          copy_row(host + (((size_t)(z0 + zl + brd) * PY + (y + brd)) * PX + brd) * NPOP,
+                   hstage.data() + ((size_t)zl * NY + y) * row, row);
     }
   }
   cudaFree(dstage);

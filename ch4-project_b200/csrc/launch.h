@@ -39,14 +39,14 @@ cudaError_t launch_force_moments(const StepParams<double>& P, LaunchShape s, con
 cudaError_t launch_force_moments(const StepParams<float>& P, LaunchShape s, const float* hit_cur, int with_prev,
                                  double* partial, int nblocks, double norm, const double* amp, float* fm,
                                  cudaStream_t st, int stage = 0);
-// compact AoS chunk <-> SoA storage for one population set
+// compact AoS chunk (in the arithmetic type) <-> SoA storage for one population set
 cudaError_t launch_aos_to_soa(const StepParams<double>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
                               int nz, cudaStream_t st);
-cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
+cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const float* aos, void* soa, int z0,
                               int nz, cudaStream_t st);
 cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
                               int nz, cudaStream_t st);
-cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
+cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, float* aos, int z0,
                               int nz, cudaStream_t st);
 // copies of up to 30 device regions (z-slab face exchange), in 4-byte words when every
 // region's size and addresses allow it, else in 2-byte words

@@ -28,12 +28,12 @@ cudaError_t launch_force_moments(const StepParams<float>& P, LaunchShape s, cons
              ? force_moments_t<__half, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st, stage)
              : force_moments_t<float, float>(P, s, hit_cur, with_prev, partial, nblocks, norm, amp, fm, st, stage);
 }
-cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const double* aos, void* soa, int z0,
+cudaError_t launch_aos_to_soa(const StepParams<float>& P, LaunchShape s, int set, const float* aos, void* soa, int z0,
                               int nz, cudaStream_t st) {
   return s.storage == 2 ? a2s_t<__half, float>(P, set, aos, soa, z0, nz, st)
                         : a2s_t<float, float>(P, set, aos, soa, z0, nz, st);
 }
-cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, double* aos, int z0,
+cudaError_t launch_soa_to_aos(const StepParams<float>& P, LaunchShape s, int set, const void* soa, float* aos, int z0,
                               int nz, cudaStream_t st) {
   return s.storage == 2 ? s2a_t<__half, float>(P, set, soa, aos, z0, nz, st)
                         : s2a_t<float, float>(P, set, soa, aos, z0, nz, st);

@@ -373,28 +373,31 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
   }
 }
 
-// Compact AoS FP64 chunk (reference `pop` records of z-planes [z0, z0+nz), no
-// halo) <-> SoA storage.  The host moves the halo-padded caller arrays row by row.
+// Compact AoS chunk (reference `pop` records of z-planes [z0, z0+nz), no halo) in the
+// arithmetic type <-> SoA storage.  The host moves the halo-padded FP64 caller arrays
+// row by row, rounding to the arithmetic type on the way for the FP32 forms (the same
+// round-to-nearest conversion the storage codec would apply to an FP64 value, so the
+// stored populations are those of an FP64 chunk, with half the bytes on the bus).
 template <typename S, typename A>
-__global__ void aos_to_soa_kernel(const double* aos, S* soa, int NX, int NY, int z0, int nz, long long N, StepParams<A> P,
+__global__ void aos_to_soa_kernel(const A* aos, S* soa, int NX, int NY, int z0, int nz, long long N, StepParams<A> P,
                                   int set) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long cells = (long long)NX * NY * nz;
   if (t >= cells * Q) return;
   const int q = (int)(t % Q);
   const long long c = t / Q;
-  Codec<S, A>::store(soa, (long long)q * N + (long long)z0 * NX * NY + c, (A)aos[t], P.w[q], P.shift[set]);
+  Codec<S, A>::store(soa, (long long)q * N + (long long)z0 * NX * NY + c, aos[t], P.w[q], P.shift[set]);
 }
 
 template <typename S, typename A>
-__global__ void soa_to_aos_kernel(const S* soa, double* aos, int NX, int NY, int z0, int nz, long long N,
-                                  StepParams<A> P, int set) {
+__global__ void soa_to_aos_kernel(const S* soa, A* aos, int NX, int NY, int z0, int nz, long long N, StepParams<A> P,
+                                  int set) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long cells = (long long)NX * NY * nz;
   if (t >= cells * Q) return;
   const int q = (int)(t % Q);
   const long long c = t / Q;
-  aos[t] = (double)Codec<S, A>::load(soa, (long long)q * N + (long long)z0 * NX * NY + c, P.w[q], P.shift[set]);
+  aos[t] = Codec<S, A>::load(soa, (long long)q * N + (long long)z0 * NX * NY + c, P.w[q], P.shift[set]);
 }
 
 #include "force_moments.cuh"
