@@ -18,6 +18,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <sched.h>
 #include <thread>
 #include <vector>
 
@@ -31,12 +32,25 @@ namespace {
 
 constexpr int NPOP = Q;
 
-// body(i0, i1) over [0, n), split across up to 8 host threads (one thread when n is
-// below 2 * grain).  Host<->pinned copies run at a few GB/s per thread; the first
-// touch of a freshly allocated caller array faults its pages in the same threads.
+// host threads for the staging copies: the cores this process may run on (its CPU
+// affinity set), at most 16
+inline size_t host_threads() {
+  static const size_t n = [] {
+    cpu_set_t set;
+    size_t c = 0;
+    if (sched_getaffinity(0, sizeof set, &set) == 0) c = (size_t)CPU_COUNT(&set);
+    if (c == 0) c = std::thread::hardware_concurrency();
+    return std::max<size_t>(1, std::min<size_t>(16, c));
+  }();
+  return n;
+}
+
+// body(i0, i1) over [0, n), split across the host threads (one thread when n is below
+// 2 * grain).  Host<->pinned copies run at a few GB/s per thread; the first touch of a
+// freshly allocated caller array faults its pages in the same threads.
 template <class F>
 void host_parallel(size_t n, size_t grain, F&& body) {
-  const size_t hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const size_t hw = host_threads();
   const size_t nt = std::min(hw, std::max<size_t>(1, n / std::max<size_t>(1, grain)));
   std::vector<std::thread> pool;
   for (size_t t = 1; t < nt; t++) pool.emplace_back([&body, n, nt, t] { body(n * t / nt, n * (t + 1) / nt); });
@@ -1424,35 +1438,6 @@ struct Engine : EngineBase {
     return CH4_OK;
   }
 
-  // device array -> caller's host array through the two pinned staging buffers: chunk
-  // k+1 is in flight while host threads copy chunk k out
-  ch4_status download_bounce(const double* dsrc, double* hdst, size_t count) {
-    const size_t cap = staging_bytes / sizeof(double);
-    double* hb[2] = {reinterpret_cast<double*>(staging_h), reinterpret_cast<double*>(staging_h2 ? staging_h2 : staging_h)};
-    const size_t nchunks = (count + cap - 1) / cap;
-    const size_t depth = staging_h2 ? 2 : 1;
-    ch4_status st;
-    auto issue = [&](size_t k) {
-      const size_t b = depth == 2 ? (k & 1) : 0, len = std::min(cap, count - k * cap);
-      ch4_status s2 = H->cuda(
-          cudaMemcpyAsync(hb[b], dsrc + k * cap, len * sizeof(double), cudaMemcpyDeviceToHost, H->stream), "download");
-      return s2 ? s2 : H->cuda(cudaEventRecord(up_ev[b], H->stream), "download event");
-    };
-    for (size_t k = 0; k < std::min(depth, nchunks); k++)
-      if ((st = issue(k))) return st;
-    for (size_t k = 0; k < nchunks; k++) {
-      const size_t b = depth == 2 ? (k & 1) : 0, len = std::min(cap, count - k * cap);
-      if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "download sync"))) return st;
-      const double* srcb = hb[b];
-      double* out = hdst + k * cap;
-      host_parallel(len, 1 << 16, [&](size_t i0, size_t i1) {
-        std::memcpy(out + i0, srcb + i0, (i1 - i0) * sizeof(double));
-      });
-      if (k + depth < nchunks && (st = issue(k + depth))) return st;
-    }
-    return CH4_OK;
-  }
-
   ch4_status fields(double* dens, double* u, double* t, double* s, double* force, int brd) override {
     if (ch4_status rs = ready()) return rs;
     bind_pops(cur);
@@ -1460,31 +1445,63 @@ struct Engine : EngineBase {
     double* d = nullptr;
     const size_t n1 = (size_t)N;
     if (brd == 0) {
-      // only the requested fields, straight into the caller's arrays; vectors are
-      // interleaved on the device
-      if ((st = H->cuda(cudaMalloc(&d, 12 * n1 * sizeof(double)), "fields scratch"))) return st;
-      double *dd = d, *du = d + n1, *dt = d + 4 * n1, *ds = d + 5 * n1, *dfo = d + 6 * n1, *vec = d + 9 * n1;
+      // only the requested fields, straight into the caller's arrays: z-slab chunks are
+      // formed on the device in the arithmetic type (vectors interleaved), copied through
+      // the two pinned staging buffers (chunk k+1 in flight while host threads widen
+      // chunk k to FP64 into the caller's arrays)
+      const int want = (dens ? 1 : 0) | (u ? 2 : 0) | (t && nsets_on[1] ? 4 : 0) | (s && nsets_on[2] ? 8 : 0) |
+                       (force ? 16 : 0);
+      if (t && !nsets_on[1]) std::fill(t, t + n1, 0.0);
+      if (s && !nsets_on[2]) std::fill(s, s + n1, 0.0);
+      if (!want) return CH4_OK;
+      const int nvals = ((want & 1) ? 1 : 0) + ((want & 2) ? 3 : 0) + ((want & 4) ? 1 : 0) + ((want & 8) ? 1 : 0) +
+                        ((want & 16) ? 3 : 0);
+      const size_t plane = (size_t)c.NX * c.NY;
+      const int cz = (int)std::max<size_t>(1, std::min<size_t>((size_t)c.NZ, staging_bytes / (nvals * sizeof(A) * plane)));
+      const int nchunks = (c.NZ + cz - 1) / cz;
+      const int depth = staging_h2 ? 2 : 1;
+      A* hb[2] = {staging_h, staging_h2 ? staging_h2 : staging_h};
+      A* db[2] = {staging_d, staging_d2 ? staging_d2 : staging_d};
       const A* hit = (c.flags & CH4_F_FORCING_HIT) ? hit_last : nullptr;
-      st = H->cuda(launch_hydro(P, shape, hit, twoway() ? dbuf[dcur_i] : nullptr, fm_last(), dens ? dd : nullptr,
-                                u ? du : nullptr, t && nsets_on[1] ? dt : nullptr, s && nsets_on[2] ? ds : nullptr,
-                                force ? dfo : nullptr, nullptr, H->stream),
-                   "hydro");
-      if (!st && dens) st = download_bounce(dd, dens, n1);
-      if (!st && u && !(st = H->cuda(launch_interleave3(du, vec, (long long)n1, H->stream), "interleave")))
-        st = download_bounce(vec, u, 3 * n1);
-      if (!st && t) {
-        if (nsets_on[1]) st = download_bounce(dt, t, n1);
-        else std::fill(t, t + n1, 0.0);
+      const A* dep = twoway() ? dbuf[dcur_i] : nullptr;
+      auto issue = [&](int k) -> ch4_status {
+        const int z0 = k * cz, nz = std::min(cz, c.NZ - z0), b = depth == 2 ? (k & 1) : 0;
+        ch4_status s2;
+        if ((s2 = H->cuda(launch_fields_chunk(P, shape, hit, dep, fm_last(), z0, nz, want, db[b], H->stream), "fields")))
+          return s2;
+        if ((s2 = H->cuda(cudaMemcpyAsync(hb[b], db[b], (size_t)nvals * nz * plane * sizeof(A), cudaMemcpyDeviceToHost,
+                                          H->stream),
+                          "fields download")))
+          return s2;
+        return H->cuda(cudaEventRecord(up_ev[b], H->stream), "fields event");
+      };
+      for (int k = 0; k < std::min(depth, nchunks); k++)
+        if ((st = issue(k))) return st;
+      for (int k = 0; k < nchunks; k++) {
+        const int z0 = k * cz, nz = std::min(cz, c.NZ - z0), b = depth == 2 ? (k & 1) : 0;
+        if ((st = H->cuda(cudaEventSynchronize(up_ev[b]), "fields sync"))) return st;
+        const size_t n = (size_t)nz * plane, off = (size_t)z0 * plane;
+        const A* src = hb[b];
+        // [dst, count] in the order of the chunk's blocks
+        std::pair<double*, size_t> blocks[5];
+        int nb = 0;
+        if (want & 1) blocks[nb++] = {dens + off, n};
+        if (want & 2) blocks[nb++] = {u + 3 * off, 3 * n};
+        if (want & 4) blocks[nb++] = {t + off, n};
+        if (want & 8) blocks[nb++] = {s + off, n};
+        if (want & 16) blocks[nb++] = {force + 3 * off, 3 * n};
+        const size_t total = (size_t)nvals * n;
+        host_parallel(total, 1 << 16, [&](size_t i0, size_t i1) {
+          size_t base = 0;
+          for (int q = 0; q < nb; q++) {
+            const size_t a = std::max(i0, base), e = std::min(i1, base + blocks[q].second);
+            if (a < e) copy_row(blocks[q].first + (a - base), src + a, e - a);
+            base += blocks[q].second;
+          }
+        });
+        if (k + depth < nchunks && (st = issue(k + depth))) return st;
       }
-      if (!st && s) {
-        if (nsets_on[2]) st = download_bounce(ds, s, n1);
-        else std::fill(s, s + n1, 0.0);
-      }
-      if (!st && force && !(st = H->cuda(launch_interleave3(dfo, vec, (long long)n1, H->stream), "interleave")))
-        st = download_bounce(vec, force, 3 * n1);
-      cudaStreamSynchronize(H->stream);
-      cudaFree(d);
-      return st;
+      return CH4_OK;
     }
     // scratch planes: dens | u (3) | t | s | force (3)
     if ((st = H->cuda(cudaMalloc(&d, 9 * n1 * sizeof(double)), "fields scratch"))) return st;

@@ -30,6 +30,12 @@ cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float*
                          const float* fm, double* dens,
                          double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
                          float* ut4 = nullptr);
+// the hydro fields of z-planes [z0, z0 + nz) in the arithmetic type into a chunk buffer
+// (want: bit 0 dens, 1 u, 2 t, 3 s, 4 force; layout in fields_chunk_kernel)
+cudaError_t launch_fields_chunk(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep,
+                                const double* fm, int z0, int nz, int want, double* out, cudaStream_t st);
+cudaError_t launch_fields_chunk(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep,
+                                const float* fm, int z0, int nz, int want, float* out, cudaStream_t st);
 // global force corrections (NOZEROMODE / CONSTANT_POWER) of one step into fm[6];
 // partial holds nblocks * 9 * 2 doubles.  stage 0: sums and corrections; 1: the block
 // sums only; 2: the corrections from nblocks partials (e.g. gathered from every z-slab)
@@ -58,8 +64,6 @@ struct HaloCopy {
 };
 cudaError_t launch_halo_copy(const HaloCopy& H, cudaStream_t st);
 
-// vec[3 i + a] = planes[a n + i], a = 0..2 (planar vector field -> interleaved)
-cudaError_t launch_interleave3(const double* planes, double* vec, long long n, cudaStream_t st);
 
 // Lagrangian particles: state slot i <- slot order2[i] into P.pf_alt / P.pid_alt (with
 // sort != 0 the home-cell keys are computed and radix-sorted into key2 / order2 first)

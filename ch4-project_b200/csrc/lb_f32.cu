@@ -21,6 +21,11 @@ cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float*
   return s.storage == 2 ? hydro_t<__half, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, st)
                         : hydro_t<float, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, st);
 }
+cudaError_t launch_fields_chunk(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep,
+                                const float* fm, int z0, int nz, int want, float* out, cudaStream_t st) {
+  return s.storage == 2 ? fields_chunk_t<__half, float>(P, s, hit, dep, fm, z0, nz, want, out, st)
+                        : fields_chunk_t<float, float>(P, s, hit, dep, fm, z0, nz, want, out, st);
+}
 cudaError_t launch_force_moments(const StepParams<float>& P, LaunchShape s, const float* hit_cur, int with_prev,
                                  double* partial, int nblocks, double norm, const double* amp, float* fm,
                                  cudaStream_t st, int stage) {

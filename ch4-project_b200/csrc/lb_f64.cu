@@ -9,16 +9,6 @@
 #include "part_avg.cuh"
 
 namespace ch4 {
-namespace {
-__global__ void interleave3_kernel(const double* __restrict__ planes, double* __restrict__ vec, long long n) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double a = planes[i], b = planes[n + i], c = planes[2 * n + i];
-  vec[3 * i] = a;
-  vec[3 * i + 1] = b;
-  vec[3 * i + 2] = c;
-}
-}  // namespace
 
 template <typename W>
 __global__ void halo_copy_kernel(const HaloCopy H) {
@@ -45,17 +35,15 @@ cudaError_t launch_halo_copy(const HaloCopy& H, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_interleave3(const double* planes, double* vec, long long n, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
-  interleave3_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(planes, vec, n);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_step(const StepParams<double>& P, LaunchShape s, cudaStream_t st) {
   return step_t<double, double>(P, s, st);
 }
 cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStream_t st) {
   return init_prev_t<double, double>(P, s, st);
+}
+cudaError_t launch_fields_chunk(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep,
+                                const double* fm, int z0, int nz, int want, double* out, cudaStream_t st) {
+  return fields_chunk_t<double, double>(P, s, hit, dep, fm, z0, nz, want, out, st);
 }
 cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep, const double* fm,
                          double* dens,

@@ -317,6 +317,26 @@ __device__ __forceinline__ void store_ut4<double>(double* ut4, long long idx, do
   reinterpret_cast<double2*>(ut4)[2 * idx + 1] = make_double2(c, d);
 }
 
+// hydro_fields of one cell (src/lb.c:420-539): rho = m(f), u = mv(f)/rho + dt/2 F with
+// F built from the kept t^{n-1} and the given tables / deposit / corrections
+template <typename S, typename A, bool THERM, bool SCAL>
+__device__ __forceinline__ void hydro_cell(const StepParams<A>& P, int x, int y, int z, long long idx, const A* hit,
+                                           const A* dep, const A* fm, A& rho, A& ux, A& uy, A& uz, A& Fx, A& Fy,
+                                           A& Fz) {
+  A f[Q];
+  load_set<S, A, 0>(P, idx, f);
+  rho = mom0(f);
+  Fx = Fy = Fz = A(0);
+  if (P.feat & K_FORCING) {
+    const A tp = THERM ? P.tprev[idx] : A(0);
+    const A sp = SCAL ? P.sprev[idx] : A(0);
+    cell_force(P, x, y, z, idx, tp, sp, hit, dep, fm, Fx, Fy, Fz);
+  }
+  ux = momx(f) / rho + P.hdt * Fx;
+  uy = momy(f) / rho + P.hdt * Fy;
+  uz = momz(f) / rho + P.hdt * Fz;
+}
+
 template <typename S, typename A, bool THERM, bool SCAL>
 __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, const A* fm, double* dens, double* u,
                              double* t, double* s, double* force, A* u_arith, A* ut4) {
@@ -325,18 +345,8 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
   if (x >= P.NX) return;
   const int y = blockIdx.y, z = blockIdx.z;
   const long long idx = ((long long)z * P.NY + y) * P.NX + x;
-  A f[Q];
-  load_set<S, A, 0>(P, idx, f);
-  const A rho = mom0(f);
-  A Fx = A(0), Fy = A(0), Fz = A(0);
-  if (P.feat & K_FORCING) {
-    const A tp = THERM ? P.tprev[idx] : A(0);
-    const A sp = SCAL ? P.sprev[idx] : A(0);
-    cell_force(P, x, y, z, idx, tp, sp, hit, dep, fm, Fx, Fy, Fz);
-  }
-  const A ux = momx(f) / rho + P.hdt * Fx;
-  const A uy = momy(f) / rho + P.hdt * Fy;
-  const A uz = momz(f) / rho + P.hdt * Fz;
+  A rho, ux, uy, uz, Fx, Fy, Fz;
+  hydro_cell<S, A, THERM, SCAL>(P, x, y, z, idx, hit, dep, fm, rho, ux, uy, uz, Fx, Fy, Fz);
   if (dens) dens[idx] = (double)rho;
   if (u) {
     u[idx] = (double)ux;
@@ -370,6 +380,59 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
       load_set<S, A, 2>(P, idx, h);
       s[idx] = (double)mom0(h);
     }
+  }
+}
+
+// The hydrodynamic fields of z-planes [z0, z0 + gridDim.z) in the arithmetic type, for
+// the host to widen into the caller's FP64 arrays: out holds, chunk-local and only for
+// the fields in `want` (bit 0 dens, 1 u, 2 t, 3 s, 4 force), dens | u (x, y, z per
+// cell) | t | s | force (x, y, z per cell), each block n = NX * NY * nz cells (vectors 3n).
+// The values are hydro_kernel's, before its widening to FP64.
+template <typename S, typename A, bool THERM, bool SCAL>
+__global__ void fields_chunk_kernel(const StepParams<A> P, const A* hit, const A* dep, const A* fm, int z0, int want,
+                                    A* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= P.NX) return;
+  const int y = blockIdx.y, zl = blockIdx.z, z = z0 + zl;
+  const long long idx = ((long long)z * P.NY + y) * P.NX + x;
+  const long long n = (long long)P.NX * P.NY * gridDim.z, i = ((long long)zl * P.NY + y) * P.NX + x;
+  A rho, ux, uy, uz, Fx, Fy, Fz;
+  hydro_cell<S, A, THERM, SCAL>(P, x, y, z, idx, hit, dep, fm, rho, ux, uy, uz, Fx, Fy, Fz);
+  A* o = out;
+  if (want & 1) {
+    o[i] = rho;
+    o += n;
+  }
+  if (want & 2) {
+    o[3 * i] = ux;
+    o[3 * i + 1] = uy;
+    o[3 * i + 2] = uz;
+    o += 3 * n;
+  }
+  if (want & 4) {
+    A tt = A(0);
+    if constexpr (THERM) {
+      A g[Q];
+      load_set<S, A, 1>(P, idx, g);
+      tt = mom0(g);
+    }
+    o[i] = tt;
+    o += n;
+  }
+  if (want & 8) {
+    A sv = A(0);
+    if constexpr (SCAL) {
+      A h[Q];
+      load_set<S, A, 2>(P, idx, h);
+      sv = mom0(h);
+    }
+    o[i] = sv;
+    o += n;
+  }
+  if (want & 16) {
+    o[3 * i] = Fx;
+    o[3 * i + 1] = Fy;
+    o[3 * i + 2] = Fz;
   }
 }
 
