@@ -84,6 +84,24 @@ FLAGS = {
 }
 INITIAL_OTHER = 1 << 63  # another *_INITIAL_* flag of define.h
 
+# second flag word (ch4_config.flags2), same values as include/ch4.h
+FLAGS2 = {
+    "LB_FLUID_BC_X": 1 << 0,
+    "LB_FLUID_BC_X_P_SLIP": 1 << 1,
+    "LB_FLUID_BC_X_M_SLIP": 1 << 2,
+    "LB_FLUID_BC_Z": 1 << 3,
+    "LB_FLUID_BC_Z_P_SLIP": 1 << 4,
+    "LB_FLUID_BC_Z_M_SLIP": 1 << 5,
+    "LB_TEMPERATURE_BC_X": 1 << 6,
+    "LB_TEMPERATURE_BC_X_P_NOFLUX": 1 << 7,
+    "LB_TEMPERATURE_BC_X_M_NOFLUX": 1 << 8,
+    "LB_TEMPERATURE_BC_Z": 1 << 9,
+    "LB_TEMPERATURE_BC_Z_P_NOFLUX": 1 << 10,
+    "LB_TEMPERATURE_BC_Z_M_NOFLUX": 1 << 11,
+    "LB_SCALAR_BC_X": 1 << 12,
+    "LB_SCALAR_BC_Z": 1 << 13,
+}
+
 
 class Config(C.Structure):
     _fields_ = [
@@ -111,6 +129,7 @@ class Config(C.Structure):
         ("noise_u", C.c_double), ("noise_t", C.c_double),
         ("particle_types", C.c_int),
         ("nz_global", C.c_int), ("z_offset", C.c_int),
+        ("flags2", C.c_uint64),
     ]
 
 
@@ -152,14 +171,36 @@ class Averages(C.Structure):
 
 
 def flags_of(names):
+    """The first flag word (ch4_config.flags) of a list of define.h names."""
     v = 0
     for n in names:
-        v |= FLAGS[n]
+        if n not in FLAGS2:
+            v |= FLAGS[n]
     return v
 
 
-def set_flag_names(flags):
-    return [n for n, b in FLAGS.items() if flags & b]
+def flags2_of(names):
+    """The second flag word (ch4_config.flags2) of a list of define.h names."""
+    v = 0
+    for n in names:
+        if n not in FLAGS:
+            v |= FLAGS2[n]
+    return v
+
+
+def set_flags(cfg, names):
+    """Both flag words of a config from a list of define.h names."""
+    cfg.flags = flags_of(names)
+    cfg.flags2 = flags2_of(names)
+    return cfg
+
+
+def has_flag(cfg, name):
+    return bool(cfg.flags & FLAGS[name]) if name in FLAGS else bool(cfg.flags2 & FLAGS2[name])
+
+
+def set_flag_names(flags, flags2=0):
+    return [n for n, b in FLAGS.items() if flags & b] + [n for n, b in FLAGS2.items() if flags2 & b]
 
 
 # ch4_output_h5 options

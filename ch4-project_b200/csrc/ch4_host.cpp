@@ -142,6 +142,11 @@ const uint64_t SUPPORTED =
     CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES | CH4_F_METHOD_TRT | CH4_F_FLUID_LES_VANDRIEST | CH4_F_TEMPERATURE_LES |
     CH4_F_SCALAR_LES | CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN | CH4_F_LAGRANGE_TWOWAY_TRICUBIC |
     CH4_F_LAGRANGE_ORIENTATION | CH4_F_LAGRANGE_ORIENTATION_JEFFREY;
+const uint64_t SUPPORTED2 =
+    CH4_F2_FLUID_BC_X | CH4_F2_FLUID_BC_X_P_SLIP | CH4_F2_FLUID_BC_X_M_SLIP | CH4_F2_FLUID_BC_Z |
+    CH4_F2_FLUID_BC_Z_P_SLIP | CH4_F2_FLUID_BC_Z_M_SLIP | CH4_F2_TEMPERATURE_BC_X | CH4_F2_TEMPERATURE_BC_X_P_NOFLUX |
+    CH4_F2_TEMPERATURE_BC_X_M_NOFLUX | CH4_F2_TEMPERATURE_BC_Z | CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX |
+    CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX | CH4_F2_SCALAR_BC_X | CH4_F2_SCALAR_BC_Z;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -481,6 +486,23 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   if (fl & CH4_F_FLUID_LES_WALE) F |= K_WALE;
   if (fl & CH4_F_FLUID_LES_LOCAL_STRAIN) F |= K_LSTRAIN;
   P.feat = F;
+  uint32_t WB = 0;
+  const uint64_t f2 = c.flags2;
+  if (f2 & CH4_F2_FLUID_BC_X) WB |= W_FX;
+  if (f2 & CH4_F2_FLUID_BC_Z) WB |= W_FZ;
+  if (f2 & CH4_F2_FLUID_BC_X_P_SLIP) WB |= W_FSLIP_XP;
+  if (f2 & CH4_F2_FLUID_BC_X_M_SLIP) WB |= W_FSLIP_XM;
+  if (f2 & CH4_F2_FLUID_BC_Z_P_SLIP) WB |= W_FSLIP_ZP;
+  if (f2 & CH4_F2_FLUID_BC_Z_M_SLIP) WB |= W_FSLIP_ZM;
+  if (f2 & CH4_F2_TEMPERATURE_BC_X) WB |= W_TX;
+  if (f2 & CH4_F2_TEMPERATURE_BC_Z) WB |= W_TZ;
+  if (f2 & CH4_F2_TEMPERATURE_BC_X_P_NOFLUX) WB |= W_TNOFLUX_XP;
+  if (f2 & CH4_F2_TEMPERATURE_BC_X_M_NOFLUX) WB |= W_TNOFLUX_XM;
+  if (f2 & CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX) WB |= W_TNOFLUX_ZP;
+  if (f2 & CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX) WB |= W_TNOFLUX_ZM;
+  if (f2 & CH4_F2_SCALAR_BC_X) WB |= W_SX;
+  if (f2 & CH4_F2_SCALAR_BC_Z) WB |= W_SZ;
+  P.walls = WB;
   P.fm_prev = P.fm_cur = nullptr;
   for (int q = 0; q < NPOP; q++) P.w[q] = (A)lat.w[q];
   const double invtau = 1.0 / c.tau_u;
@@ -546,6 +568,18 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.shift[0] = 1.0f;
   P.shift[1] = (float)T0;
   P.shift[2] = (float)(0.5 * (c.S_bot + c.S_top));
+}
+
+// walls per axis (bit 0 x, 1 y, 2 z) of the fluid, and of the temperature or scalar fields
+// (the one-sided gradients of gradient_vector / gradient_scalar, src/gradients.c:161-230, 529-620)
+inline int fluid_walls(const ch4_config& c) {
+  return ((c.flags2 & CH4_F2_FLUID_BC_X) ? 1 : 0) | ((c.flags & CH4_F_FLUID_BC_Y) ? 2 : 0) |
+         ((c.flags2 & CH4_F2_FLUID_BC_Z) ? 4 : 0);
+}
+inline int value_walls(const ch4_config& c) {
+  return ((c.flags2 & (CH4_F2_TEMPERATURE_BC_X | CH4_F2_SCALAR_BC_X)) ? 1 : 0) |
+         ((c.flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) ? 2 : 0) |
+         ((c.flags2 & (CH4_F2_TEMPERATURE_BC_Z | CH4_F2_SCALAR_BC_Z)) ? 4 : 0);
 }
 
 // one AoS row between the caller's FP64 array and a staging chunk of the arithmetic type
@@ -769,8 +803,8 @@ struct Engine : EngineBase {
     Q.u = du;
     Q.t = nsets_on[1] ? dt : nullptr;
     Q.s = nsets_on[2] ? ds : nullptr;
-    Q.fwall = (c.flags & CH4_F_FLUID_BC_Y) != 0;
-    Q.twall = (c.flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+    Q.fwall = fluid_walls(c);
+    Q.twall = value_walls(c);
     Q.nu = c.nu;
     Q.kappa = c.kappa;
     Q.partial = part;
@@ -811,8 +845,8 @@ struct Engine : EngineBase {
     Q.u = du;
     Q.t = nsets_on[1] ? dt : nullptr;
     Q.s = nsets_on[2] ? ds : nullptr;
-    Q.fwall = (c.flags & CH4_F_FLUID_BC_Y) != 0;
-    Q.twall = (c.flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+    Q.fwall = fluid_walls(c);
+    Q.twall = value_walls(c);
     Q.nu = c.nu;
     Q.kappa = c.kappa;
     Q.chi = c.chi;
@@ -1736,6 +1770,22 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_FLUID_LES_LOCAL_STRAIN", CH4_F_FLUID_LES_LOCAL_STRAIN},
       {"LAGRANGE_TWOWAY_TRICUBIC", CH4_F_LAGRANGE_TWOWAY_TRICUBIC},
   };
+  static const M map2[] = {
+      {"LB_FLUID_BC_X", CH4_F2_FLUID_BC_X},
+      {"LB_FLUID_BC_X_P_SLIP", CH4_F2_FLUID_BC_X_P_SLIP},
+      {"LB_FLUID_BC_X_M_SLIP", CH4_F2_FLUID_BC_X_M_SLIP},
+      {"LB_FLUID_BC_Z", CH4_F2_FLUID_BC_Z},
+      {"LB_FLUID_BC_Z_P_SLIP", CH4_F2_FLUID_BC_Z_P_SLIP},
+      {"LB_FLUID_BC_Z_M_SLIP", CH4_F2_FLUID_BC_Z_M_SLIP},
+      {"LB_TEMPERATURE_BC_X", CH4_F2_TEMPERATURE_BC_X},
+      {"LB_TEMPERATURE_BC_X_P_NOFLUX", CH4_F2_TEMPERATURE_BC_X_P_NOFLUX},
+      {"LB_TEMPERATURE_BC_X_M_NOFLUX", CH4_F2_TEMPERATURE_BC_X_M_NOFLUX},
+      {"LB_TEMPERATURE_BC_Z", CH4_F2_TEMPERATURE_BC_Z},
+      {"LB_TEMPERATURE_BC_Z_P_NOFLUX", CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX},
+      {"LB_TEMPERATURE_BC_Z_M_NOFLUX", CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX},
+      {"LB_SCALAR_BC_X", CH4_F2_SCALAR_BC_X},
+      {"LB_SCALAR_BC_Z", CH4_F2_SCALAR_BC_Z},
+  };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
   static const char* neutral[] = {"LB", "GRID_REGULAR", "GRID_POP_D3Q19", "METHOD_STREAMING", "METHOD_EDGES_AND_CORNERS",
@@ -1744,7 +1794,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
                                   "OUTPUT_H5", "OUTPUT_H5_GRID", "OUTPUT_H5_TIMESTAMP_REAL", "OUTPUT_AT_START",
                                   "OUTPUT_ASCII", "VERBOSE", "LB_TEMPERATURE_BUOYANCY_T0_REF",
                                   "LB_TEMPERATURE_BUOYANCY_T0_TOP", "LB_TEMPERATURE_BUOYANCY_T0_BOT", "LB_FLUID_LES_OUTPUT"};
-  uint64_t flags = 0;
+  uint64_t flags = 0, flags2 = 0;
   int t0 = CH4_T0_MEAN;
   bool d3q19 = false, streaming = false;
   size_t pos = 0;
@@ -1765,6 +1815,11 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
     for (const M& m : map)
       if (name == m.name) {
         flags |= m.bit;
+        known = true;
+      }
+    for (const M& m : map2)
+      if (name == m.name) {
+        flags2 |= m.bit;
         known = true;
       }
     for (const char* nn : neutral)
@@ -1788,6 +1843,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
     return CH4_ERR_UNSUPPORTED;
   }
   cfg->flags = flags | CH4_F_LB_FLUID;
+  cfg->flags2 = flags2;
   cfg->t0_kind = t0;
   return CH4_OK;
 }
@@ -1797,6 +1853,7 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
   if ((long long)c->NX * c->NY * c->NZ >= (1ll << 31)) return why = "lattice too large (cells >= 2^31)", CH4_ERR_ARG;
   if (c->NY > 65535 || c->NZ > 65535) return why = "NY and NZ must be <= 65535 (launch grid)", CH4_ERR_ARG;
   if (c->flags & ~SUPPORTED) return why = "flag outside the implemented hot path", CH4_ERR_UNSUPPORTED;
+  if (c->flags2 & ~SUPPORTED2) return why = "flag outside the implemented hot path", CH4_ERR_UNSUPPORTED;
   if (c->storage < 0 || c->storage > 2) return why = "unknown storage", CH4_ERR_ARG;
   const int nz_all = c->nz_global > 0 ? c->nz_global : c->NZ;
   if (c->time_dt != 1.0 || c->SX != c->NX || c->SY != c->NY || c->SZ != nz_all)
@@ -1810,6 +1867,28 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
   }
   if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
     return why = "walls need NY >= 3", CH4_ERR_ARG;
+  {
+    const uint64_t f2 = c->flags2;
+    const bool wx = f2 & (CH4_F2_FLUID_BC_X | CH4_F2_TEMPERATURE_BC_X | CH4_F2_SCALAR_BC_X);
+    const bool wz = f2 & (CH4_F2_FLUID_BC_Z | CH4_F2_TEMPERATURE_BC_Z | CH4_F2_SCALAR_BC_Z);
+    if (wx && c->NX < 3) return why = "walls need NX >= 3", CH4_ERR_ARG;
+    if (wz && c->NZ < 3) return why = "walls need NZ >= 3", CH4_ERR_ARG;
+    // the slab exchange carries whole rows of the face planes; walls on x and z would need
+    // per-cell masks (and z walls lie on one slab only)
+    if ((wx || wz) && c->nz_global > 0) return why = "z-slab handles have walls on y only", CH4_ERR_UNSUPPORTED;
+    // a slip wall next to a wall on another axis takes, at the edge, halo values the
+    // other axis's loop wrote (src/boundary_conditions.c:578-952): not reproduced
+    const int fw = ((f2 & CH4_F2_FLUID_BC_X) ? 1 : 0) + ((c->flags & CH4_F_FLUID_BC_Y) ? 1 : 0) +
+                   ((f2 & CH4_F2_FLUID_BC_Z) ? 1 : 0);
+    const bool slip = (f2 & (CH4_F2_FLUID_BC_X_P_SLIP | CH4_F2_FLUID_BC_X_M_SLIP | CH4_F2_FLUID_BC_Z_P_SLIP |
+                             CH4_F2_FLUID_BC_Z_M_SLIP)) ||
+                      (c->flags & (CH4_F_FLUID_BC_Y_P_SLIP | CH4_F_FLUID_BC_Y_M_SLIP));
+    if (slip && fw > 1) return why = "slip walls need every other axis periodic", CH4_ERR_UNSUPPORTED;
+    if ((f2 & (CH4_F2_FLUID_BC_X_P_SLIP | CH4_F2_FLUID_BC_X_M_SLIP)) && !(f2 & CH4_F2_FLUID_BC_X))
+      return why = "LB_FLUID_BC_X_*_SLIP needs LB_FLUID_BC_X", CH4_ERR_ARG;
+    if ((f2 & (CH4_F2_FLUID_BC_Z_P_SLIP | CH4_F2_FLUID_BC_Z_M_SLIP)) && !(f2 & CH4_F2_FLUID_BC_Z))
+      return why = "LB_FLUID_BC_Z_*_SLIP needs LB_FLUID_BC_Z", CH4_ERR_ARG;
+  }
   if (!(c->tau_u > 0.5)) return why = "tau_u must exceed 0.5", CH4_ERR_ARG;
   {
     const uint64_t les_variants = CH4_F_FLUID_LES_VANDRIEST | CH4_F_TEMPERATURE_LES | CH4_F_SCALAR_LES |
@@ -1830,7 +1909,7 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
              CH4_ERR_UNSUPPORTED;
   }
   if (c->flags & CH4_F_LAGRANGE) {
-    if (c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_LB_SCALAR))
+    if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_LB_SCALAR)) || c->flags2)
       return why = "particles are implemented for the periodic box (fluid, optionally temperature)",
              CH4_ERR_UNSUPPORTED;
     if (!(c->flags & CH4_F_LAGRANGE_WRAP)) return why = "particles need LAGRANGE_WRAP", CH4_ERR_UNSUPPORTED;
@@ -3282,8 +3361,8 @@ ch4_status ch4_ensemble_averages(ch4_ensemble* E, int slot, ch4_averages* out) {
   Q.u = du;
   Q.t = s->nsets_on[1] ? dt : nullptr;
   Q.s = s->nsets_on[2] ? ds : nullptr;
-  Q.fwall = (c.flags & CH4_F_FLUID_BC_Y) != 0;
-  Q.twall = (c.flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+  Q.fwall = fluid_walls(c);
+  Q.twall = value_walls(c);
   Q.nu = c.nu;
   Q.kappa = c.kappa;
   Q.partial = part;

@@ -20,7 +20,7 @@ struct AvgParams {
   const double* u;     // 3 planes
   const double* t;     // may be null
   const double* s;     // may be null
-  int fwall, twall;    // one-sided y gradients for u / for t and s
+  int fwall, twall;    // walls per axis (bit 0 x, 1 y, 2 z): one-sided gradients of u / of t and s
   double nu, kappa, chi;
   double* partial;     // [gridDim.x][NAVG][2]
 };
@@ -46,14 +46,19 @@ __device__ __forceinline__ DD dd_add(DD a, DD b) {
   return dd_add(r, b.lo);
 }
 
-__device__ __forceinline__ double gfield(const AvgParams& P, const double* f, int i, int j, int k, int b, bool walls) {
-  const int NX = P.NX, NY = P.NY, NZ = P.NZ;
-  auto at = [&](int ii, int jj, int kk) { return f[((long long)kk * NY + jj) * NX + ii]; };
-  if (b == 0) return (at(i + 1 == NX ? 0 : i + 1, j, k) - at(i == 0 ? NX - 1 : i - 1, j, k)) / 2.0;
-  if (b == 2) return (at(i, j, k + 1 == NZ ? 0 : k + 1) - at(i, j, k == 0 ? NZ - 1 : k - 1)) / 2.0;
-  if (walls && j == 0) return -1.5 * at(i, 0, k) + 2.0 * at(i, 1, k) + -0.5 * at(i, 2, k);
-  if (walls && j == NY - 1) return 1.5 * at(i, NY - 1, k) + -2.0 * at(i, NY - 2, k) + 0.5 * at(i, NY - 3, k);
-  return (at(i, j + 1 == NY ? 0 : j + 1, k) - at(i, j == 0 ? NY - 1 : j - 1, k)) / 2.0;
+// d f / d x_b at an interior cell: centred with periodic wrap, one-sided of second order
+// at the walls of the axes in the mask `walls` (src/gradients.c:161-230, 529-620)
+__device__ __forceinline__ double gfield(const AvgParams& P, const double* f, int i, int j, int k, int b, int walls) {
+  const int NX = P.NX, NY = P.NY;
+  const int n = b == 0 ? P.NX : b == 1 ? P.NY : P.NZ;
+  const int c = b == 0 ? i : b == 1 ? j : k;
+  auto at = [&](int o) {
+    const int ii = b == 0 ? o : i, jj = b == 1 ? o : j, kk = b == 2 ? o : k;
+    return f[((long long)kk * NY + jj) * NX + ii];
+  };
+  if (((walls >> b) & 1) && c == 0) return -1.5 * at(0) + 2.0 * at(1) + -0.5 * at(2);
+  if (((walls >> b) & 1) && c == n - 1) return 1.5 * at(n - 1) + -2.0 * at(n - 2) + 0.5 * at(n - 3);
+  return (at(c + 1 == n ? 0 : c + 1) - at(c == 0 ? n - 1 : c - 1)) / 2.0;
 }
 
 // per-cell contributions in ch4_averages order (unit cell volume)
@@ -71,7 +76,7 @@ __device__ __forceinline__ void cell_terms(const AvgParams& P, long long c, doub
   v[7] = 0.5 * (ux * ux + uy * uy + uz * uz);
   double g[3][3];
   for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++) g[a][b] = gfield(P, P.u + a * N, i, j, k, b, P.fwall != 0);
+    for (int b = 0; b < 3; b++) g[a][b] = gfield(P, P.u + a * N, i, j, k, b, P.fwall);
   const double xx = g[0][0], xy = g[0][1], xz = g[0][2], yx = g[1][0], yy = g[1][1], yz = g[1][2], zx = g[2][0],
                zy = g[2][1], zz = g[2][2];
   v[8] = ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) + (yx + xy) * (yx + xy) +
@@ -81,8 +86,8 @@ __device__ __forceinline__ void cell_terms(const AvgParams& P, long long c, doub
   for (int q = 9; q < NAVG; q++) v[q] = 0.0;
   if (P.t) {
     const double t = P.t[c];
-    const double gx = gfield(P, P.t, i, j, k, 0, P.twall != 0), gy = gfield(P, P.t, i, j, k, 1, P.twall != 0),
-                 gz = gfield(P, P.t, i, j, k, 2, P.twall != 0);
+    const double gx = gfield(P, P.t, i, j, k, 0, P.twall), gy = gfield(P, P.t, i, j, k, 1, P.twall),
+                 gz = gfield(P, P.t, i, j, k, 2, P.twall);
     v[9] = t;
     v[10] = t * t;
     v[11] = P.kappa * (gx * gx + gy * gy + gz * gz);
@@ -170,7 +175,7 @@ __device__ __forceinline__ void cell_terms_full(const AvgParams& P, long long c,
   v[11] = 0.5 * (ux * ux + uy * uy + uz * uz);
   double g[3][3];
   for (int a = 0; a < 3; a++)
-    for (int b = 0; b < 3; b++) g[a][b] = gfield(P, P.u + a * N, i, j, k, b, P.fwall != 0);
+    for (int b = 0; b < 3; b++) g[a][b] = gfield(P, P.u + a * N, i, j, k, b, P.fwall);
   const double xx = g[0][0], xy = g[0][1], xz = g[0][2], yx = g[1][0], yy = g[1][1], yz = g[1][2], zx = g[2][0],
                zy = g[2][1], zz = g[2][2];
   v[12] = ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) + (yx + xy) * (yx + xy) +
@@ -180,8 +185,8 @@ __device__ __forceinline__ void cell_terms_full(const AvgParams& P, long long c,
   for (int q = 13; q < NDIAG; q++) v[q] = 0.0;
   if (P.t) {
     const double t = P.t[c];
-    const double gx = gfield(P, P.t, i, j, k, 0, P.twall != 0), gy = gfield(P, P.t, i, j, k, 1, P.twall != 0),
-                 gz = gfield(P, P.t, i, j, k, 2, P.twall != 0);
+    const double gx = gfield(P, P.t, i, j, k, 0, P.twall), gy = gfield(P, P.t, i, j, k, 1, P.twall),
+                 gz = gfield(P, P.t, i, j, k, 2, P.twall);
     v[13] = t;
     v[14] = t * t;
     v[15] = P.kappa * (gx * gx + gy * gy + gz * gz);
@@ -198,8 +203,8 @@ __device__ __forceinline__ void cell_terms_full(const AvgParams& P, long long c,
   }
   if (P.s) {
     const double sv = P.s[c];
-    const double gx = gfield(P, P.s, i, j, k, 0, P.twall != 0), gy = gfield(P, P.s, i, j, k, 1, P.twall != 0),
-                 gz = gfield(P, P.s, i, j, k, 2, P.twall != 0);
+    const double gx = gfield(P, P.s, i, j, k, 0, P.twall), gy = gfield(P, P.s, i, j, k, 1, P.twall),
+                 gz = gfield(P, P.s, i, j, k, 2, P.twall);
     v[26] = sv;
     v[27] = sv * sv;
     v[28] = P.chi * (gx * gx + gy * gy + gz * gz);

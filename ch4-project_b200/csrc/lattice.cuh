@@ -24,6 +24,15 @@ __host__ __device__ constexpr int cy(int q) {
 __host__ __device__ constexpr int cz(int q) {
   return q == 5 || q == 11 || q == 12 || q == 15 || q == 17 ? 1 : (q == 6 || q == 13 || q == 14 || q == 16 || q == 18 ? -1 : 0);
 }
+// mirror image of direction q across axis a (0 x, 1 y, 2 z): inv_x, inv_y, inv_z of src/lb.c
+__host__ __device__ constexpr int qmirror(int q, int a) {
+  return a == 1 ? (q == 3 ? 4 : q == 4 ? 3 : q == 7 ? 8 : q == 8 ? 7 : q == 9 ? 10 : q == 10 ? 9 :
+                   q == 15 ? 17 : q == 17 ? 15 : q == 16 ? 18 : q == 18 ? 16 : q)
+       : a == 0 ? (q == 1 ? 2 : q == 2 ? 1 : q == 7 ? 9 : q == 9 ? 7 : q == 8 ? 10 : q == 10 ? 8 :
+                   q == 11 ? 12 : q == 12 ? 11 : q == 13 ? 14 : q == 14 ? 13 : q)
+                : (q == 5 ? 6 : q == 6 ? 5 : q == 11 ? 13 : q == 13 ? 11 : q == 12 ? 14 : q == 14 ? 12 :
+                   q == 15 ? 16 : q == 16 ? 15 : q == 17 ? 18 : q == 18 ? 17 : q);
+}
 // opposite direction inv[q] and the y-mirror inv_y[q]
 __host__ __device__ constexpr int qinv(int q) {
   return q == 0 ? 0 : (q <= 6 ? (q % 2 ? q + 1 : q - 1) : (q <= 10 ? 17 - q : (q <= 14 ? 25 - q : 33 - q)));
@@ -64,6 +73,24 @@ enum : uint32_t {
   K_LSTRAIN = 1u << 26     // LB_FLUID_LES_LOCAL_STRAIN: |S| from the populations' stress tensor
 };
 
+// walls on x and z (those on y are K_FWALL / K_TWALL / K_SWALL of `feat`)
+enum : uint32_t {
+  W_FX = 1u << 0,        // fluid walls at x = 0 and x = NX-1
+  W_FZ = 1u << 1,        // fluid walls at z = 0 and z = NZ-1
+  W_FSLIP_XP = 1u << 2,  // specular upper x wall
+  W_FSLIP_XM = 1u << 3,
+  W_FSLIP_ZP = 1u << 4,
+  W_FSLIP_ZM = 1u << 5,
+  W_TX = 1u << 6,        // temperature walls on x (T_top on both sides)
+  W_TZ = 1u << 7,        // temperature walls on z (T_top / T_bot)
+  W_TNOFLUX_XP = 1u << 8,
+  W_TNOFLUX_XM = 1u << 9,
+  W_TNOFLUX_ZP = 1u << 10,
+  W_TNOFLUX_ZM = 1u << 11,
+  W_SX = 1u << 12,       // scalar walls on x (S_top / S_bot)
+  W_SZ = 1u << 13        // scalar walls on z
+};
+
 template <typename A>
 struct StepParams {
   int NX, NY, NZ;
@@ -71,6 +98,7 @@ struct StepParams {
   int zoff;     // global z of plane 0 (z-slab of a larger lattice), else 0
   int Lhit;     // NX + NY + global NZ: length of one HIT table row
   uint32_t feat;
+  uint32_t walls;  // W_* bits
   // populations (storage type erased; cast in the kernel)
   const void* fin[3];
   void* fout[3];

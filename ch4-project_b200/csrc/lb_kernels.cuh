@@ -224,12 +224,25 @@ __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z
     const long long nxy = (long long)NX * NY, inplane = (long long)y * NX + x;
     const A* up_hi = (z == NZ - 1 && P.ules_hi) ? P.ules_hi : nullptr;
     const A* up_lo = (z == 0 && P.ules_lo) ? P.ules_lo : nullptr;
+    // one-sided second-order differences at the walls of an axis (src/gradients.c:161-230)
+    const bool wx = (P.walls & W_FX) != 0, wz = (P.walls & W_FZ) != 0;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-      g[a][0] = (at(a, xp, y, z) - at(a, xm, y, z)) / A(2);
-      const A vp = up_hi ? up_hi[a * nxy + inplane] : at(a, x, y, zp);
-      const A vm = up_lo ? up_lo[a * nxy + inplane] : at(a, x, y, zm);
-      g[a][2] = (vp - vm) / A(2);
+      if (wx && x == 0)
+        g[a][0] = A(-1.5) * at(a, 0, y, z) + A(2) * at(a, 1, y, z) + A(-0.5) * at(a, 2, y, z);
+      else if (wx && x == NX - 1)
+        g[a][0] = A(1.5) * at(a, NX - 1, y, z) + A(-2) * at(a, NX - 2, y, z) + A(0.5) * at(a, NX - 3, y, z);
+      else
+        g[a][0] = (at(a, xp, y, z) - at(a, xm, y, z)) / A(2);
+      if (wz && z == 0) {
+        g[a][2] = A(-1.5) * at(a, x, y, 0) + A(2) * at(a, x, y, 1) + A(-0.5) * at(a, x, y, 2);
+      } else if (wz && z == NZ - 1) {
+        g[a][2] = A(1.5) * at(a, x, y, NZ - 1) + A(-2) * at(a, x, y, NZ - 2) + A(0.5) * at(a, x, y, NZ - 3);
+      } else {
+        const A vp = up_hi ? up_hi[a * nxy + inplane] : at(a, x, y, zp);
+        const A vm = up_lo ? up_lo[a * nxy + inplane] : at(a, x, y, zm);
+        g[a][2] = (vp - vm) / A(2);
+      }
     }
     const bool walls = (F & K_FWALL) != 0;
     if (walls && y == 0) {

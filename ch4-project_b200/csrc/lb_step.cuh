@@ -67,29 +67,89 @@ __device__ __forceinline__ int nbr_delta(const Nbr& n) {
   return d;
 }
 
-// push one set; wallmode: 0 periodic in y, 1 fluid walls, 2 value walls (T or S).
-// top/bot: this cell is the last/first interior row of a walled set (uniform per block).
-// WALLS = false is the form for rows that touch no wall: every value streams to x + c_q.
+// The walls one set meets at this cell: per axis (0 x, 1 y, 2 z) whether a direction with
+// c_a = +1 (hp) or -1 (hm) leaves through a wall of this set, and per side the fluid's slip
+// flag or the value walls' fac.  Built only for cells on a wall row, column or plane.
+struct Walls {
+  uint32_t hit;   // bit a: a wall of this set at the upper end of axis a at this cell, bit 3 + a: lower
+  uint32_t slip;  // the same bits for the fluid's specular walls
+};
+
+// fac = 2((T_wall - T_ref) - t) of a value wall of set 1 (temperature) or 2 (scalar) on
+// axis a, upper (plus) or lower side, src/boundary_conditions.c:966-1236, 1249-1520: y walls
+// T_top / T_bot with the fixed-flux and no-flux variants, x walls T_top on both sides (as
+// the reference has it), z walls T_top / T_bot; scalar walls S_top / S_bot on every axis
+template <int set, typename A>
+__device__ __forceinline__ A wall_fac(const StepParams<A>& P, int a, bool plus, A tt, A ss) {
+  const uint32_t F = P.feat, WL = P.walls;
+  if constexpr (set == 2) return A(2) * (((plus ? P.S_top : P.S_bot) - P.S_ref) - ss);
+  if (a == 1) {
+    A T_wall = plus ? P.T_top : P.T_bot;
+    if (plus && (F & K_TFLUX_P)) T_wall = A(0.5) * P.grad_T_top + tt + P.T_ref;
+    if (!plus && (F & K_TFLUX_M)) T_wall = A(-0.5) * P.grad_T_bot + tt + P.T_ref;
+    if (F & (plus ? K_TNOFLUX_P : K_TNOFLUX_M)) return A(0);
+    return A(2) * ((T_wall - P.T_ref) - tt);
+  }
+  if (a == 0) {
+    if (WL & (plus ? W_TNOFLUX_XP : W_TNOFLUX_XM)) return A(0);
+    return A(2) * ((P.T_top - P.T_ref) - tt);
+  }
+  if (WL & (plus ? W_TNOFLUX_ZP : W_TNOFLUX_ZM)) return A(0);
+  return A(2) * (((plus ? P.T_top : P.T_bot) - P.T_ref) - tt);
+}
+
+// push one set; wallmode: 0 no walls, 1 fluid walls, 2 value walls (temperature or scalar).
+// WALLS = false is the form for cells that touch no wall: every value streams to x + c_q.
 template <typename S, typename A, int set, int q, bool WALLS>
 __device__ __forceinline__ void push_one(const StepParams<A>& P, int idx, const Nbr& nb, const A* post, int wallmode,
-                                         bool top, bool bot, bool slip_top, bool slip_bot, A fac_top, A fac_bot) {
+                                         const Walls& W, A tt, A ss) {
   const float sh = P.shift[set];
   if constexpr (WALLS) {
-    const bool hits_wall = (cy(q) > 0 && top) || (cy(q) < 0 && bot);
-    if (cy(q) != 0 && wallmode != 0 && hits_wall) {
+    // the wall bit of each axis this direction leaves through (compile-time masks: q is fixed)
+    constexpr uint32_t mx = cx(q) > 0 ? 1u : cx(q) < 0 ? 8u : 0u;
+    constexpr uint32_t my = cy(q) > 0 ? 2u : cy(q) < 0 ? 16u : 0u;
+    constexpr uint32_t mz = cz(q) > 0 ? 4u : cz(q) < 0 ? 32u : 0u;
+    const bool hx = (W.hit & mx) != 0, hy = (W.hit & my) != 0, hz = (W.hit & mz) != 0;
+    if (wallmode != 0 && (hx || hy || hz)) {
       if (wallmode == 1) {
-        const bool slip = cy(q) > 0 ? slip_top : slip_bot;
-        if (slip) {  // specular reflection, src/boundary_conditions.c:753,786
-          constexpr int r = qinv_y(q);
-          Codec<S, A>::store(plane_out<S, A, set>(P, r), idx + nbr_delta<q, false>(nb), post[q], P.w[r], sh);
-        } else {  // halfway bounce-back, src/boundary_conditions.c:775,798
-          constexpr int r = qinv(q);
-          Codec<S, A>::store(plane_out<S, A, set>(P, r), idx, post[q], P.w[r], sh);
+        // a slip wall stands alone on its axis (the other axes are periodic), so a direction
+        // that meets it meets no other wall
+        if (int(hx) + int(hy) + int(hz) == 1) {
+          const bool sx = (W.slip & mx) != 0, sy = (W.slip & my) != 0, sz = (W.slip & mz) != 0;
+          // specular reflection: the hit axis keeps the cell's coordinate, the others stream
+          // (src/boundary_conditions.c:606-610 (x), 751-753 (y), 895-899 (z))
+          if (hx && sx) {
+            constexpr int r = qmirror(q, 0);
+            const int d = (cy(q) < 0 ? nb.ym : cy(q) > 0 ? nb.yp : 0) + (cz(q) < 0 ? nb.zm : cz(q) > 0 ? nb.zp : 0);
+            Codec<S, A>::store(plane_out<S, A, set>(P, r), idx + d, post[q], P.w[r], sh);
+            return;
+          }
+          if (hy && sy) {
+            constexpr int r = qmirror(q, 1);
+            Codec<S, A>::store(plane_out<S, A, set>(P, r), idx + nbr_delta<q, false>(nb), post[q], P.w[r], sh);
+            return;
+          }
+          if (hz && sz) {
+            constexpr int r = qmirror(q, 2);
+            const int d = (cx(q) < 0 ? nb.xm : cx(q) > 0 ? nb.xp : 0) + (cy(q) < 0 ? nb.ym : cy(q) > 0 ? nb.yp : 0);
+            Codec<S, A>::store(plane_out<S, A, set>(P, r), idx + d, post[q], P.w[r], sh);
+            return;
+          }
         }
-      } else {  // fixed value / flux wall: rhs(x).p[inv q] + w[inv q]*fac, src/boundary_conditions.c:1019-1027
+        // halfway bounce-back, src/boundary_conditions.c:623,775,917
         constexpr int r = qinv(q);
-        const A fac = cy(q) > 0 ? fac_top : fac_bot;
-        Codec<S, A>::store(plane_out<S, A, set>(P, r), idx, post[r] + P.w[r] * fac, P.w[r], sh);
+        Codec<S, A>::store(plane_out<S, A, set>(P, r), idx, post[q], P.w[r], sh);
+      } else {
+        // fixed value / flux walls: the reference's loops run y, then x, then z, each writing
+        // the slot the cell pulls as inv[q]; the last wall the direction crosses decides
+        // (src/boundary_conditions.c:1019-1027, 1118-1151, 1186-1224).  Temperature walls on
+        // x store rhs(x).p[q] + w[inv q] fac, every other value wall rhs(x).p[inv q] + ...
+        constexpr int r = qinv(q);
+        const int a = hz ? 2 : hx ? 0 : 1;
+        const bool plus = a == 2 ? cz(q) > 0 : a == 0 ? cx(q) > 0 : cy(q) > 0;
+        const A fac = wall_fac<set>(P, a, plus, tt, ss);
+        const A base = (set == 1 && a == 0) ? post[q] : post[r];
+        Codec<S, A>::store(plane_out<S, A, set>(P, r), idx, base + P.w[r] * fac, P.w[r], sh);
       }
       return;
     }
@@ -99,12 +159,22 @@ __device__ __forceinline__ void push_one(const StepParams<A>& P, int idx, const 
 
 template <typename S, typename A, int set, bool WALLS>
 __device__ __forceinline__ void push_set(const StepParams<A>& P, int idx, const Nbr& nb, const A* post, int wallmode,
-                                         bool top, bool bot, bool slip_top, bool slip_bot, A fac_top, A fac_bot) {
-#define CH4_PUSH(Q_) push_one<S, A, set, Q_, WALLS>(P, idx, nb, post, wallmode, top, bot, slip_top, slip_bot, fac_top, fac_bot);
+                                         const Walls& W, A tt, A ss) {
+#define CH4_PUSH(Q_) push_one<S, A, set, Q_, WALLS>(P, idx, nb, post, wallmode, W, tt, ss);
   CH4_PUSH(0) CH4_PUSH(1) CH4_PUSH(2) CH4_PUSH(3) CH4_PUSH(4) CH4_PUSH(5) CH4_PUSH(6) CH4_PUSH(7) CH4_PUSH(8)
   CH4_PUSH(9) CH4_PUSH(10) CH4_PUSH(11) CH4_PUSH(12) CH4_PUSH(13) CH4_PUSH(14) CH4_PUSH(15) CH4_PUSH(16)
   CH4_PUSH(17) CH4_PUSH(18)
 #undef CH4_PUSH
+}
+
+// The push of a cell on a wall row, column or plane, out of line: wall cells are a thin
+// shell of the lattice, and keeping their case in its own function keeps the registers of
+// the bulk path (every other cell) at what the bulk needs.  `post` is the caller's copy of
+// the post-collision values; P is a kernel or shared-memory parameter block.
+template <typename S, typename A, int set>
+__device__ __noinline__ void push_walled(const StepParams<A>& P, int idx, Nbr nb, const A* post, int wallmode,
+                                         Walls W, A tt, A ss) {
+  push_set<S, A, set, true>(P, idx, nb, post, wallmode, W, tt, ss);
 }
 
 // Per-cell quantities shared by the collision of every direction.
@@ -345,41 +415,48 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
 #undef CH4_COL
 
   const Nbr nb = neighbours(x, y, z, P.NX, P.NY, P.NZ);
+  const uint32_t WL = P.walls;
   const bool toprow = y == P.NY - 1, botrow = y == 0;
+  const bool xedge = (WL & (W_FX | W_TX | W_SX)) && (x == 0 || x == P.NX - 1);
+  const bool zedge = (WL & (W_FZ | W_TZ | W_SZ)) && (z == 0 || z == P.NZ - 1);
+  Walls W{0u, 0u};
 #ifndef CH4_NO_WALL_SPLIT
-  if (!(toprow || botrow)) {  // uniform per block: rows that touch no wall stream every value
-    push_set<S, A, 0, false>(P, idx, nb, f, 0, false, false, false, false, A(0), A(0));
-    if constexpr (THERM) push_set<S, A, 1, false>(P, idx, nb, g, 0, false, false, false, false, A(0), A(0));
-    if constexpr (SCAL) push_set<S, A, 2, false>(P, idx, nb, h, 0, false, false, false, false, A(0), A(0));
+  if (!(toprow || botrow || xedge || zedge)) {  // cells that touch no wall stream every value
+    push_set<S, A, 0, false>(P, idx, nb, f, 0, W, c.tt, c.ss);
+    if constexpr (THERM) push_set<S, A, 1, false>(P, idx, nb, g, 0, W, c.tt, c.ss);
+    if constexpr (SCAL) push_set<S, A, 2, false>(P, idx, nb, h, 0, W, c.tt, c.ss);
     return;
   }
 #endif
-  push_set<S, A, 0, true>(P, idx, nb, f, (F & K_FWALL) ? 1 : 0, toprow, botrow, (F & K_FSLIP_P) != 0,
-                          (F & K_FSLIP_M) != 0, A(0), A(0));
+  // the wall bits of this cell for walls on the axes (x, y, z) of a set
+  const uint32_t at = (x == P.NX - 1 ? 1u : 0u) | (toprow ? 2u : 0u) | (z == P.NZ - 1 ? 4u : 0u) |
+                      (x == 0 ? 8u : 0u) | (botrow ? 16u : 0u) | (z == 0 ? 32u : 0u);
+  auto on = [&](bool wx, bool wy, bool wz) { return at & ((wx ? 9u : 0u) | (wy ? 18u : 0u) | (wz ? 36u : 0u)); };
+  A tmp[Q];
+  {
+    W.hit = on((WL & W_FX) != 0, (F & K_FWALL) != 0, (WL & W_FZ) != 0);
+    W.slip = W.hit & (((WL & W_FSLIP_XP) ? 1u : 0u) | ((F & K_FSLIP_P) ? 2u : 0u) | ((WL & W_FSLIP_ZP) ? 4u : 0u) |
+                      ((WL & W_FSLIP_XM) ? 8u : 0u) | ((F & K_FSLIP_M) ? 16u : 0u) | ((WL & W_FSLIP_ZM) ? 32u : 0u));
+#pragma unroll
+    for (int q = 0; q < Q; q++) tmp[q] = f[q];
+    push_walled<S, A, 0>(P, idx, nb, tmp, W.hit ? 1 : 0, W, c.tt, c.ss);
+  }
   if constexpr (THERM) {
-    A fac_top = A(0), fac_bot = A(0);
-    if (F & K_TWALL) {  // src/boundary_conditions.c:966-1081
-      A T_wall = P.T_top;
-      if (F & K_TFLUX_P) T_wall = A(0.5) * P.grad_T_top + c.tt + P.T_ref;
-      fac_top = (F & K_TNOFLUX_P) ? A(0) : A(2) * ((T_wall - P.T_ref) - c.tt);
-      T_wall = P.T_bot;
-      if (F & K_TFLUX_M) T_wall = A(-0.5) * P.grad_T_bot + c.tt + P.T_ref;
-      fac_bot = (F & K_TNOFLUX_M) ? A(0) : A(2) * ((T_wall - P.T_ref) - c.tt);
-    }
-    push_set<S, A, 1, true>(P, idx, nb, g, (F & K_TWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
+    W.hit = on((WL & W_TX) != 0, (F & K_TWALL) != 0, (WL & W_TZ) != 0);
+#pragma unroll
+    for (int q = 0; q < Q; q++) tmp[q] = g[q];
+    push_walled<S, A, 1>(P, idx, nb, tmp, W.hit ? 2 : 0, W, c.tt, c.ss);
   }
   if constexpr (SCAL) {
-    A fac_top = A(0), fac_bot = A(0);
-    if (F & K_SWALL) {  // src/boundary_conditions.c:1249-1380
-      fac_top = A(2) * ((P.S_top - P.S_ref) - c.ss);
-      fac_bot = A(2) * ((P.S_bot - P.S_ref) - c.ss);
-    }
-    push_set<S, A, 2, true>(P, idx, nb, h, (F & K_SWALL) ? 2 : 0, toprow, botrow, false, false, fac_top, fac_bot);
+    W.hit = on((WL & W_SX) != 0, (F & K_SWALL) != 0, (WL & W_SZ) != 0);
+#pragma unroll
+    for (int q = 0; q < Q; q++) tmp[q] = h[q];
+    push_walled<S, A, 2>(P, idx, nb, tmp, W.hit ? 2 : 0, W, c.tt, c.ss);
   }
 }
 
 template <typename S, typename A, bool THERM, bool SCAL, int V = 0>
-__global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
+__global__ void __launch_bounds__(128) lb_step_kernel(const __grid_constant__ StepParams<A> P) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
   lb_cell<S, A, THERM, SCAL, V>(P, x, blockIdx.y, blockIdx.z);
@@ -390,7 +467,7 @@ __global__ void __launch_bounds__(128) lb_step_kernel(const StepParams<A> P) {
 // compiler may take a few more and lose a block per SM (-13 % measured).  (A minimum-blocks
 // hint on the other forms raises their registers instead; they keep the plain bound.)
 template <typename S, typename A, bool THERM, bool SCAL>
-__global__ void __launch_bounds__(128, 4) lb_step_kernel_cap128(const StepParams<A> P) {
+__global__ void __launch_bounds__(128, 4) lb_step_kernel_cap128(const __grid_constant__ StepParams<A> P) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
   lb_cell<S, A, THERM, SCAL, 0>(P, x, blockIdx.y, blockIdx.z);

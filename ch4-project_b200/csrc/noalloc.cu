@@ -80,8 +80,8 @@ extern "C" ch4_status ch4_averages_noalloc(const double* dens, const double* u, 
   P.u = u;
   P.t = t;
   P.s = s;
-  P.fwall = fluid_walls != 0;
-  P.twall = scalar_walls != 0;
+  P.fwall = fluid_walls ? 2 : 0;  // walls at y = 0 and y = NY - 1 (bit 1 of the wall mask)
+  P.twall = scalar_walls ? 2 : 0;
   P.nu = nu;
   P.kappa = kappa;
   P.partial = partial;

@@ -111,6 +111,30 @@ enum {
   CH4_F_INITIAL_OTHER = 1ull << 63
 };
 
+/* Second word of compile-time flags (ch4_config.flags2): walls on x and z, and the
+ * Lagrangian options added after the first word filled up. */
+enum {
+  /* fluid walls on x and z: no-slip bounce-back, or specular (slip) on one side,
+   * src/boundary_conditions.c:578-720 (x), 879-952 (z) */
+  CH4_F2_FLUID_BC_X = 1ull << 0,
+  CH4_F2_FLUID_BC_X_P_SLIP = 1ull << 1,
+  CH4_F2_FLUID_BC_X_M_SLIP = 1ull << 2,
+  CH4_F2_FLUID_BC_Z = 1ull << 3,
+  CH4_F2_FLUID_BC_Z_P_SLIP = 1ull << 4,
+  CH4_F2_FLUID_BC_Z_M_SLIP = 1ull << 5,
+  /* temperature walls on x and z: fixed value (x: T_top on both sides, as the
+   * reference has it; z: T_top / T_bot) or no flux, src/boundary_conditions.c:1083-1236 */
+  CH4_F2_TEMPERATURE_BC_X = 1ull << 6,
+  CH4_F2_TEMPERATURE_BC_X_P_NOFLUX = 1ull << 7,
+  CH4_F2_TEMPERATURE_BC_X_M_NOFLUX = 1ull << 8,
+  CH4_F2_TEMPERATURE_BC_Z = 1ull << 9,
+  CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX = 1ull << 10,
+  CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX = 1ull << 11,
+  /* scalar walls on x and z: fixed value S_top / S_bot, src/boundary_conditions.c:1380-1520 */
+  CH4_F2_SCALAR_BC_X = 1ull << 12,
+  CH4_F2_SCALAR_BC_Z = 1ull << 13
+};
+
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
 typedef enum {
   CH4_T0_MEAN = 0, /* default: 0.5*(T_bot+T_top) */
@@ -163,6 +187,8 @@ typedef struct {
    * and the caller exchanges the populations crossing the slab faces after every step
    * (ch4_halo_pack / ch4_halo_unpack).  nz_global = 0: the handle is the whole lattice. */
   int nz_global, z_offset;
+  /* CH4_F2_* bits (the second word of define.h flags) */
+  uint64_t flags2;
 } ch4_config;
 
 /* One Lagrangian particle (the fields of point_particle, src/typedef.h:391-481,

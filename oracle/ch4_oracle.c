@@ -35,6 +35,17 @@ static const int CY[NPOP] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 0, 0, 1, 
 static const int CZ[NPOP] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, -1, 1, -1};
 static const int INV[NPOP] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
 static const int INV_Y[NPOP] = {0, 1, 2, 4, 3, 5, 6, 8, 7, 10, 9, 11, 12, 13, 14, 17, 18, 15, 16};
+/* mirror images across x and z (src/lb.c:200-230 inv_x, inv_z) */
+static int mirror(int q, int axis) {
+  for (int r = 0; r < NPOP; r++) {
+    int cx = CX[q], cy = CY[q], cz = CZ[q];
+    if (axis == 0) cx = -cx;
+    if (axis == 1) cy = -cy;
+    if (axis == 2) cz = -cz;
+    if (CX[r] == cx && CY[r] == cy && CZ[r] == cz) return r;
+  }
+  return q;
+}
 
 struct ch4o_state {
   ch4_config cfg;
@@ -200,6 +211,46 @@ static inline size_t cidx(const ch4o_state *s, int i, int j, int k) {
   return ((size_t)k * (size_t)s->NY + (size_t)j) * (size_t)s->NX + (size_t)i;
 }
 
+/* walls per axis (bit 0 x, 1 y, 2 z) of the fluid, and of the temperature or scalar
+ * fields (gradient_scalar, src/gradients.c:529-620) */
+static int fluid_walls(const ch4_config *c) {
+  return ((c->flags2 & CH4_F2_FLUID_BC_X) ? 1 : 0) | ((c->flags & CH4_F_FLUID_BC_Y) ? 2 : 0) |
+         ((c->flags2 & CH4_F2_FLUID_BC_Z) ? 4 : 0);
+}
+static int scalar_walls(const ch4_config *c) {
+  return ((c->flags2 & (CH4_F2_TEMPERATURE_BC_X | CH4_F2_SCALAR_BC_X)) ? 1 : 0) |
+         ((c->flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) ? 2 : 0) |
+         ((c->flags2 & (CH4_F2_TEMPERATURE_BC_Z | CH4_F2_SCALAR_BC_Z)) ? 4 : 0);
+}
+
+/* gradient_vector / gradient_scalar of one field component at an interior cell
+ * (src/gradients.c:78-240, 505-620): centred with periodic halos, one-sided 2nd
+ * order at the walls of the axes in the mask `walls` (bit 0 x, 1 y, 2 z) */
+static double grad_field(const ch4o_state *s, const double *f, int ncomp, int a, int b, int i, int j, int k,
+                         int walls) {
+  const int n[3] = {s->NX, s->NY, s->NZ};
+  int at[3] = {i, j, k};
+  const int m = n[b], c = at[b];
+#define FV(o)                                              \
+  (at[b] = (o), f[cidx(s, at[0], at[1], at[2]) * ncomp + a])
+  const double h1 = 1.0, h2 = 1.0;
+  double r;
+  if (((walls >> b) & 1) && c == 0) {
+    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
+    const double v0 = FV(0), v1 = FV(1), v2 = FV(2);
+    r = a0 * v0 + a1 * v1 + a2 * v2;
+  } else if (((walls >> b) & 1) && c == m - 1) {
+    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
+    const double v0 = FV(m - 1), v1 = FV(m - 2), v2 = FV(m - 3);
+    r = a0 * v0 + a1 * v1 + a2 * v2;
+  } else {
+    const double vp = FV((c + 1) % m), vm = FV((c + m - 1) % m);
+    r = (vp - vm) / 2.0;
+  }
+#undef FV
+  return r;
+}
+
 /* m(), mvx(), mvy(), mvz() macros, src/typedef.h:286-291 (fixed summation order) */
 static inline double mom0(const double *a) {
   return (a[0] + a[1] + a[2] + a[3] + a[4] + a[5] + a[6] + a[7] + a[8] + a[9] + a[10] + a[11] + a[12] + a[13] + a[14] +
@@ -240,7 +291,7 @@ static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k,
                       double ux, double uy, double uz, double u2, double tau_prev) {
   const int NX = s->NX, NY = s->NY, NZ = s->NZ;
   const uint64_t fl = s->cfg.flags;
-  const int walls = (fl & CH4_F_FLUID_BC_Y) != 0;
+  const int walls = fluid_walls(&s->cfg);
   if (fl & CH4_F_FLUID_LES_LOCAL_STRAIN) {
     double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Sxz = 0, Syz = 0;
     for (int pp = 0; pp < NPOP; pp++) {
@@ -265,30 +316,12 @@ static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k,
     double nu_les = s_norm * pow(C_smag * 1.0, 2.0);
     return 3.0 * (nu_les + s->cfg.nu) + 0.5;
   }
-  double g[3][3]; /* g[a][b] = d u_a / d x_b  (tens.ab with a=component) */
-  int ip = (i + 1) % NX, im = (i + NX - 1) % NX;
-  int kp = (k + 1) % NZ, km = (k + NZ - 1) % NZ;
-  for (int a = 0; a < 3; a++) {
-    g[a][0] = (u[3 * cidx(s, ip, j, k) + a] - u[3 * cidx(s, im, j, k) + a]) / 2.0;
-    g[a][2] = (u[3 * cidx(s, i, j, kp) + a] - u[3 * cidx(s, i, j, km) + a]) / 2.0;
-  }
-  if (walls && j == 0) {
-    /* h1 = h2 = 1: a0 = -(2+1)/(1*2), a1 = 2/1, a2 = -1/(1*2) */
-    double h1 = 1.0, h2 = 1.0;
-    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
-    for (int a = 0; a < 3; a++)
-      g[a][1] = a0 * u[3 * cidx(s, i, j, k) + a] + a1 * u[3 * cidx(s, i, j + 1, k) + a] +
-                a2 * u[3 * cidx(s, i, j + 2, k) + a];
-  } else if (walls && j == NY - 1) {
-    double h1 = 1.0, h2 = 1.0;
-    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
-    for (int a = 0; a < 3; a++)
-      g[a][1] = a0 * u[3 * cidx(s, i, j, k) + a] + a1 * u[3 * cidx(s, i, j - 1, k) + a] +
-                a2 * u[3 * cidx(s, i, j - 2, k) + a];
-  } else {
-    int jp = (j + 1) % NY, jm = (j + NY - 1) % NY;
-    for (int a = 0; a < 3; a++) g[a][1] = (u[3 * cidx(s, i, jp, k) + a] - u[3 * cidx(s, i, jm, k) + a]) / 2.0;
-  }
+  double g[3][3]; /* g[a][b] = d u_a / d x_b  (tens.ab with a=component); one-sided at walls */
+  (void)NX;
+  (void)NY;
+  (void)NZ;
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) g[a][b] = grad_field(s, u, 3, a, b, i, j, k, walls);
   /* tens.xx = g[0][0], tens.xy = g[0][1] (d ux/dy), tens.yx = g[1][0] ... */
   double xx = g[0][0], xy = g[0][1], xz = g[0][2];
   double yx = g[1][0], yy = g[1][1], yz = g[1][2];
@@ -1002,51 +1035,88 @@ static void one_step(ch4o_state *s) {
         for (int set = 0; set < 3; set++) {
           if (!s->nsets_on[set]) continue;
           double *out = s->fn[set];
-          int wall = 0, slip_p = 0, slip_m = 0;
-          double fac_top = 0.0, fac_bot = 0.0;
+          /* walls of this set per axis and, per axis and side (0: m, 1: p), the fluid's
+           * slip flag or the value walls' fac */
+          int wall[3] = {0, 0, 0}, slip[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+          double fac[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
           if (set == 0) {
-            wall = (c->flags & CH4_F_FLUID_BC_Y) != 0;
-            slip_p = (c->flags & CH4_F_FLUID_BC_Y_P_SLIP) != 0;
-            slip_m = (c->flags & CH4_F_FLUID_BC_Y_M_SLIP) != 0;
+            wall[0] = (c->flags2 & CH4_F2_FLUID_BC_X) != 0;
+            wall[1] = (c->flags & CH4_F_FLUID_BC_Y) != 0;
+            wall[2] = (c->flags2 & CH4_F2_FLUID_BC_Z) != 0;
+            slip[0][1] = (c->flags2 & CH4_F2_FLUID_BC_X_P_SLIP) != 0;
+            slip[0][0] = (c->flags2 & CH4_F2_FLUID_BC_X_M_SLIP) != 0;
+            slip[1][1] = (c->flags & CH4_F_FLUID_BC_Y_P_SLIP) != 0;
+            slip[1][0] = (c->flags & CH4_F_FLUID_BC_Y_M_SLIP) != 0;
+            slip[2][1] = (c->flags2 & CH4_F2_FLUID_BC_Z_P_SLIP) != 0;
+            slip[2][0] = (c->flags2 & CH4_F2_FLUID_BC_Z_M_SLIP) != 0;
           } else if (set == 1) {
-            wall = (c->flags & CH4_F_TEMPERATURE_BC_Y) != 0;
-            if (wall) { /* src/boundary_conditions.c:966-1081 */
+            wall[1] = (c->flags & CH4_F_TEMPERATURE_BC_Y) != 0;
+            if (wall[1]) { /* src/boundary_conditions.c:966-1081 */
               double T_wall = c->T_top;
               if (c->flags & CH4_F_TEMPERATURE_BC_Y_P_FLUX) T_wall = 0.5 * c->grad_T_top + tt + c->T_ref;
-              fac_top = 2.0 * ((T_wall - c->T_ref) - tt);
-              if (c->flags & CH4_F_TEMPERATURE_BC_Y_P_NOFLUX) fac_top = 0.0;
+              fac[1][1] = 2.0 * ((T_wall - c->T_ref) - tt);
+              if (c->flags & CH4_F_TEMPERATURE_BC_Y_P_NOFLUX) fac[1][1] = 0.0;
               T_wall = c->T_bot;
               if (c->flags & CH4_F_TEMPERATURE_BC_Y_M_FLUX) T_wall = -0.5 * c->grad_T_bot + tt + c->T_ref;
-              fac_bot = 2.0 * ((T_wall - c->T_ref) - tt);
-              if (c->flags & CH4_F_TEMPERATURE_BC_Y_M_NOFLUX) fac_bot = 0.0;
+              fac[1][0] = 2.0 * ((T_wall - c->T_ref) - tt);
+              if (c->flags & CH4_F_TEMPERATURE_BC_Y_M_NOFLUX) fac[1][0] = 0.0;
+            }
+            wall[0] = (c->flags2 & CH4_F2_TEMPERATURE_BC_X) != 0;
+            if (wall[0]) { /* src/boundary_conditions.c:1083-1158: T_top on both sides */
+              fac[0][1] = (c->flags2 & CH4_F2_TEMPERATURE_BC_X_P_NOFLUX) ? 0.0 : 2.0 * ((c->T_top - c->T_ref) - tt);
+              fac[0][0] = (c->flags2 & CH4_F2_TEMPERATURE_BC_X_M_NOFLUX) ? 0.0 : 2.0 * ((c->T_top - c->T_ref) - tt);
+            }
+            wall[2] = (c->flags2 & CH4_F2_TEMPERATURE_BC_Z) != 0;
+            if (wall[2]) { /* src/boundary_conditions.c:1160-1236 */
+              fac[2][1] = (c->flags2 & CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX) ? 0.0 : 2.0 * ((c->T_top - c->T_ref) - tt);
+              fac[2][0] = (c->flags2 & CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX) ? 0.0 : 2.0 * ((c->T_bot - c->T_ref) - tt);
             }
           } else {
-            wall = (c->flags & CH4_F_SCALAR_BC_Y) != 0;
-            if (wall) { /* src/boundary_conditions.c:1249-1380 */
-              fac_top = 2.0 * ((c->S_top - c->S_ref) - ss);
-              fac_bot = 2.0 * ((c->S_bot - c->S_ref) - ss);
-            }
+            wall[1] = (c->flags & CH4_F_SCALAR_BC_Y) != 0;
+            wall[0] = (c->flags2 & CH4_F2_SCALAR_BC_X) != 0;
+            wall[2] = (c->flags2 & CH4_F2_SCALAR_BC_Z) != 0;
+            for (int a = 0; a < 3; a++)
+              if (wall[a]) { /* src/boundary_conditions.c:1249-1520 */
+                fac[a][1] = 2.0 * ((c->S_top - c->S_ref) - ss);
+                fac[a][0] = 2.0 * ((c->S_bot - c->S_ref) - ss);
+              }
           }
+          const int n3[3] = {NX, NY, NZ}, at3[3] = {i, j, k};
           for (int q = 0; q < NPOP; q++) {
-            int ty = j + CY[q];
-            int tx = (i + CX[q] + NX) % NX, tz = (k + CZ[q] + NZ) % NZ;
-            if (wall && (ty < 0 || ty >= NY)) {
-              if (set == 0) {
-                int slip = ty >= NY ? slip_p : slip_m;
-                if (slip) /* specular: src/boundary_conditions.c:753,786 */
-                  out[(size_t)INV_Y[q] * N + cidx(s, tx, j, tz)] = post[0][q];
-                else /* no-slip bounce-back: src/boundary_conditions.c:775,798 */
-                  out[(size_t)INV[q] * N + idx] = post[0][q];
-              } else {
-                /* fixed-value walls: the slot pulled as inv[q] holds
-                 * rhs(x).p[inv q] + w[inv q]*fac (src/boundary_conditions.c:1019-1027,1065-1073) */
-                int r = INV[q];
-                double fac = ty >= NY ? fac_top : fac_bot;
-                out[(size_t)r * N + idx] = post[set][r] + s->w[r] * fac;
+            const int cq[3] = {CX[q], CY[q], CZ[q]};
+            int hit[3], side[3], any = 0;
+            for (int a = 0; a < 3; a++) {
+              const int t = at3[a] + cq[a];
+              hit[a] = wall[a] && (t < 0 || t >= n3[a]);
+              side[a] = t >= n3[a];
+              any |= hit[a];
+            }
+            const int tx = (i + CX[q] + NX) % NX, ty = (j + CY[q] + NY) % NY, tz = (k + CZ[q] + NZ) % NZ;
+            if (!any) {
+              out[(size_t)q * N + cidx(s, tx, ty, tz)] = post[set][q];
+            } else if (set == 0) {
+              /* slip walls stand alone on their axis (other axes periodic), so at most
+               * one axis is hit when one is a slip wall */
+              const int a = hit[0] ? 0 : hit[1] ? 1 : 2;
+              if (!hit[(a + 1) % 3] && !hit[(a + 2) % 3] && slip[a][side[a]]) {
+                /* specular: the hit axis keeps the cell's coordinate, the others stream,
+                 * src/boundary_conditions.c:606-610 (x), 751-753 (y), 895-899 (z) */
+                int d[3] = {tx, ty, tz};
+                d[a] = at3[a];
+                out[(size_t)mirror(q, a) * N + cidx(s, d[0], d[1], d[2])] = post[0][q];
+              } else { /* no-slip halfway bounce-back, src/boundary_conditions.c:623,775,917 */
+                out[(size_t)INV[q] * N + idx] = post[0][q];
               }
             } else {
-              ty = (ty + NY) % NY;
-              out[(size_t)q * N + cidx(s, tx, ty, tz)] = post[set][q];
+              /* value walls: the reference's loops run y, then x, then z, each writing the
+               * slot the cell pulls as inv[q]; the last one the direction crosses wins.
+               * y and z walls store rhs(x).p[inv q] + w[inv q] fac, x walls of the
+               * temperature rhs(x).p[q] + w[inv q] fac (src/boundary_conditions.c:1019-1027,
+               * 1118-1151, 1186-1224) */
+              const int a = hit[2] ? 2 : hit[0] ? 0 : 1;
+              const int r = INV[q];
+              const double base = (set == 1 && a == 0) ? post[set][q] : post[set][r];
+              out[(size_t)r * N + idx] = base + s->w[r] * fac[a][side[a]];
             }
           }
         }
@@ -1342,27 +1412,7 @@ int ch4o_get_particles(ch4o_state *s, ch4_particle *parts, int n) {
   return CH4_OK;
 }
 
-/* gradient_vector / gradient_scalar of one field component at an interior cell
- * (src/gradients.c:78-240, 505-620): centred with periodic halos, one-sided 2nd
- * order at y walls when `walls` */
-static double grad_field(const ch4o_state *s, const double *f, int ncomp, int a, int b, int i, int j, int k,
-                         int walls) {
-  const int NX = s->NX, NY = s->NY, NZ = s->NZ;
-#define FV(ii, jj, kk) f[cidx(s, (ii), (jj), (kk)) * ncomp + a]
-  if (b == 0) return (FV((i + 1) % NX, j, k) - FV((i + NX - 1) % NX, j, k)) / 2.0;
-  if (b == 2) return (FV(i, j, (k + 1) % NZ) - FV(i, j, (k + NZ - 1) % NZ)) / 2.0;
-  const double h1 = 1.0, h2 = 1.0;
-  if (walls && j == 0) {
-    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
-    return a0 * FV(i, 0, k) + a1 * FV(i, 1, k) + a2 * FV(i, 2, k);
-  }
-  if (walls && j == NY - 1) {
-    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
-    return a0 * FV(i, NY - 1, k) + a1 * FV(i, NY - 2, k) + a2 * FV(i, NY - 3, k);
-  }
-  return (FV(i, (j + 1) % NY, k) - FV(i, (j + NY - 1) % NY, k)) / 2.0;
-#undef FV
-}
+
 
 /* dump_averages global sums, src/output.c:63-~720, in the reference's loop order
  * (x outermost, z innermost) with unit cell volume, normalised as src/output.c:498-707 */
@@ -1372,8 +1422,8 @@ int ch4o_averages_get(ch4o_state *s, ch4_averages *out) {
   double *dens = (double *)malloc(sizeof(double) * N), *u = (double *)malloc(sizeof(double) * 3 * N);
   double *t = (double *)calloc(N, sizeof(double)), *sc = (double *)calloc(N, sizeof(double));
   hydro(s, s->hit_cur, s->dcur, s->fm_cur, dens, u, t, sc);
-  const int fw = (c->flags & CH4_F_FLUID_BC_Y) != 0;
-  const int tw = (c->flags & (CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) != 0;
+  const int fw = fluid_walls(c);
+  const int tw = scalar_walls(c);
   ch4_averages o;
   memset(&o, 0, sizeof(o));
   const double vol = 1.0;

@@ -92,6 +92,21 @@ FLAGSETS = {
                  "LB_TEMPERATURE_INITIAL_CONSTANT_MEAN", "LB_TEMPERATURE_INITIAL_ADD_NOISE",
                  "LB_SCALAR_INITIAL_CONSTANT", "LB_SCALAR_INITIAL_CONSTANT_TOP"],
 }
+FLAGSETS.update({
+    "duct": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
+             "LB_FLUID_BC_Y", "LB_FLUID_BC_Z"],
+    "duct_les": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
+                 "LB_FLUID_BC_Y", "LB_FLUID_BC_Z", "LB_FLUID_LES"],
+    "box": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_X", "LB_FLUID_BC_Y", "LB_FLUID_BC_Z", "LB_TEMPERATURE",
+            "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_X", "LB_TEMPERATURE_BC_Y", "LB_TEMPERATURE_BC_Z",
+            "LB_TEMPERATURE_BC_Z_P_NOFLUX", "LB_SCALAR", "LB_SCALAR_BUOYANCY", "LB_SCALAR_BC_X", "LB_SCALAR_BC_Y",
+            "LB_SCALAR_BC_Z"],
+    "slipx": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_X", "LB_FLUID_BC_X_P_SLIP", "LB_TEMPERATURE",
+              "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_X", "LB_TEMPERATURE_BC_X_M_NOFLUX"],
+    "slipz": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Z", "LB_FLUID_BC_Z_P_SLIP", "LB_FLUID_BC_Z_M_SLIP",
+              "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Z", "LB_TEMPERATURE_BC_Z_M_NOFLUX",
+              "LB_SCALAR", "LB_SCALAR_BC_Z"],
+})
 # non-flag configuration implied by a flag set (define.h variants of one setting)
 FLAGSET_EXTRA = {"walls2": {"t0_kind": abi.T0_REF}}
 
@@ -108,7 +123,10 @@ def make_config(NX, NY, NZ, flags, storage=abi.STORE_F64, **kw):
     """Fill an abi.Config the way assign_parameters does (src/parameters.c:41-811)."""
     c = abi.Config()
     c.NX, c.NY, c.NZ = NX, NY, NZ
-    c.flags = abi.flags_of(flags) if isinstance(flags, (list, tuple)) else int(flags)
+    if isinstance(flags, (list, tuple)):
+        abi.set_flags(c, flags)
+    else:
+        c.flags = int(flags)
     c.storage = storage
     c.SX, c.SY, c.SZ = float(NX), float(NY), float(NZ)
     c.time_dt = 1.0

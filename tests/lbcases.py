@@ -79,6 +79,21 @@ CASES = {
                         params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=5,
                                     T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
                                     time_dt_lagr_factor=2.0, particle_number=250)),
+    # walls on x and z
+    "duct": dict(flagset="duct", NX=7, NY=8, NZ=6,
+                 params=dict(tau_u=0.6, Amp_x=4e-3, Amp_y=1e-3, Amp_z=2e-3)),
+    "duct_les": dict(flagset="duct_les", NX=8, NY=9, NZ=7,
+                     params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "box": dict(flagset="box", NX=7, NY=8, NZ=6,
+                params=dict(tau_u=0.58, tau_t=0.62, tau_s=0.66, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
+                            S_bot=0.2, S_top=0.7, S_ref=0.1, beta_s=0.2, gravity_y=2e-3, gravity_x=5e-4,
+                            gravity_z=-3e-4)),
+    "slipx": dict(flagset="slipx", NX=8, NY=6, NZ=5,
+                  params=dict(tau_u=0.57, tau_t=0.61, T_bot=0.3, T_top=1.0, T_ref=0.5, beta_t=0.3,
+                              gravity_x=2e-3, gravity_y=7e-4)),
+    "slipz": dict(flagset="slipz", NX=6, NY=5, NZ=8,
+                  params=dict(tau_u=0.59, tau_t=0.63, tau_s=0.6, T_bot=1.0, T_top=0.1, T_ref=0.5, beta_t=0.25,
+                              S_bot=0.4, S_top=0.9, S_ref=0.2, gravity_z=2e-3, gravity_x=6e-4)),
 }
 
 

@@ -91,3 +91,38 @@ def test_device_bytes_admission():
     assert n >= 2 * 2 * 19 * cells * 4
     c.storage = abi.STORE_F16
     assert ch4b200.device_bytes(c) < n
+
+
+def test_walls_on_x_and_z_are_read_from_define_h(tmp_path):
+    """LB_FLUID_BC_X / _Z and the temperature and scalar walls on x and z land in the
+    second flag word; a slip wall next to a wall on another axis is refused at create."""
+    import ch4b200
+    from ch4b200 import abi
+    d = tmp_path / "define.h"
+    d.write_text("#define GRID_POP_D3Q19\n#define METHOD_STREAMING\n#define LB_FLUID\n#define LB_FLUID_BC\n"
+                 "#define LB_FLUID_BC_X\n#define LB_FLUID_BC_Z\n#define LB_FLUID_BC_Z_P_SLIP\n"
+                 "#define LB_TEMPERATURE\n#define LB_TEMPERATURE_BC_X\n#define LB_TEMPERATURE_BC_X_M_NOFLUX\n")
+    c = ch4b200.default_config()
+    ch4b200.read_define(c, str(d))
+    assert c.flags2 == abi.flags2_of(["LB_FLUID_BC_X", "LB_FLUID_BC_Z", "LB_FLUID_BC_Z_P_SLIP",
+                                      "LB_TEMPERATURE_BC_X", "LB_TEMPERATURE_BC_X_M_NOFLUX"])
+    assert abi.has_flag(c, "LB_FLUID_BC_X") and not abi.has_flag(c, "LB_FLUID_BC_Y")
+
+
+@pytest.mark.parametrize("names", [
+    ["LB_FLUID", "LB_FLUID_BC_X", "LB_FLUID_BC_Z", "LB_FLUID_BC_Z_P_SLIP"],
+    ["LB_FLUID", "LB_FLUID_BC_Y", "LB_FLUID_BC_Y_M_SLIP", "LB_FLUID_BC_X"],
+    ["LB_FLUID", "LB_FLUID_BC_X_P_SLIP"],
+])
+def test_slip_wall_beside_another_wall_is_refused(names):
+    """Checked before any device call: a slip wall needs every other axis periodic, and
+    a slip flag needs its axis's walls."""
+    import ctypes as C
+    c = ch4b200.default_config()
+    c.NX, c.NY, c.NZ = 6, 5, 4
+    c.SX, c.SY, c.SZ = 6.0, 5.0, 4.0
+    c.tau_u = 0.6
+    abi.set_flags(c, names)
+    h = C.c_void_p()
+    rc = ch4b200.lib().ch4_create(C.byref(c), C.byref(h))
+    assert rc in (abi.ERR_UNSUPPORTED, abi.ERR_ARG) and not h.value

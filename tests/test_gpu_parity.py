@@ -49,7 +49,8 @@ def rel_l2(a, b):
                                           ("particles_t", 12), ("particles_g", 12), ("particles_1w", 12),
                                           ("particles_or", 12),
                                           ("trt", 25), ("trt_les", 25), ("les_vd", 25), ("les_ls", 25),
-                                          ("les_ts", 25), ("particles_tc", 12)])
+                                          ("les_ts", 25), ("particles_tc", 12), ("duct", 25), ("duct_les", 25),
+                                          ("box", 25), ("slipx", 25), ("slipz", 25)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):
     _, cfg, state = make_case(name, seed=11)
     ref = run_restatement(cfg, state, nsteps)
@@ -73,7 +74,7 @@ def test_fp64_bit_identical_to_oracle(name, nsteps):
 
 @pytest.mark.parametrize("name", ["kolmogorov", "rb", "hit", "walls2", "scalar", "les", "particles",
                                   "particles_t", "particles_g", "trt", "trt_les", "les_vd", "les_ls", "les_ts",
-                                  "particles_tc"])
+                                  "particles_tc", "duct", "duct_les", "box", "slipx", "slipz"])
 def test_fp64_matches_compiled_reference(name):
     flagset, cfg, state = make_case(name, seed=5)
     if not O.ref_available(flagset):
@@ -93,7 +94,7 @@ def test_fp64_matches_compiled_reference(name):
 # of rho within 1e-5, of T within 1e-6 (40 steps).
 # FP16 deviations (11-bit mantissa): u within 0.2, rho within 1e-3, T within 2e-2.
 @pytest.mark.parametrize("storage,tol_u,tol_rho,tol_t", [(1, 1e-3, 1e-5, 1e-6), (2, 0.2, 1e-3, 2e-2)])
-@pytest.mark.parametrize("name", ["kolmogorov", "rb", "scalar", "hit", "trt"])
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "scalar", "hit", "trt", "box"])
 def test_reduced_precision_error_bounds(name, storage, tol_u, tol_rho, tol_t):
     _, cfg64, state = make_case(name, seed=2)
     _, cfg, _ = make_case(name, seed=2, storage=storage)
@@ -134,7 +135,7 @@ def test_particles_fp32_fluid_close_to_fp64():
     assert rel_l2(pos(gpu), pos(ref)) < 1e-6
 
 
-@pytest.mark.parametrize("name", ["kolmogorov", "rb", "walls2", "scalar", "particles"])
+@pytest.mark.parametrize("name", ["kolmogorov", "rb", "walls2", "scalar", "particles", "box", "duct"])
 def test_fp64_averages_match_oracle(name):
     """Global sums of dump_averages: the device's double-double reduction against the
     oracle's sequential FP64 sum -- within 1e-12 relative (1e-18 absolute for means

@@ -27,7 +27,8 @@ def _assert_same(a, b, what):
                                           ("particles_or", 8),
                                           ("trt", 20), ("trt_les", 20), ("les_vd", 20), ("les_ls", 20),
                                           ("les_wale", 20), ("les_ts", 20), ("particles_tc", 8), ("nozero", 15),
-                                          ("cpower", 15)])
+                                          ("cpower", 15), ("duct", 20), ("duct_les", 20), ("box", 20),
+                                          ("slipx", 20), ("slipz", 20)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
@@ -62,6 +63,7 @@ def test_flagset_headers_match_product_flags(flagset):
     cfg = ch4b200.default_config()
     ch4b200.read_define(cfg, os.path.join(os.path.dirname(O.__file__), "configs", flagset + ".h"))
     assert cfg.flags == abi.flags_of(O.FLAGSETS[flagset])
+    assert cfg.flags2 == abi.flags2_of(O.FLAGSETS[flagset])
     assert cfg.t0_kind == O.FLAGSET_EXTRA.get(flagset, {}).get("t0_kind", abi.T0_MEAN)
 
 
