@@ -100,6 +100,8 @@ FLAGS2 = {
     "LB_TEMPERATURE_BC_Z_M_NOFLUX": 1 << 11,
     "LB_SCALAR_BC_X": 1 << 12,
     "LB_SCALAR_BC_Z": 1 << 13,
+    "LAGRANGE_TEMPERATURE": 1 << 14,
+    "LAGRANGE_TWOWAY_TEMPERATURE": 1 << 15,
 }
 
 
@@ -143,6 +145,7 @@ PARTICLE_FIELDS = [
     "t", "t_old", "dt_t", "Dt_t",
     "dx_t", "dy_t", "dz_t",
     "px", "py", "pz", "dt_px", "dt_py", "dt_pz", "aspect_ratio",
+    "t_p", "cp_p",
 ]
 
 

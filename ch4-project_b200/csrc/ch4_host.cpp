@@ -146,7 +146,14 @@ const uint64_t SUPPORTED2 =
     CH4_F2_FLUID_BC_X | CH4_F2_FLUID_BC_X_P_SLIP | CH4_F2_FLUID_BC_X_M_SLIP | CH4_F2_FLUID_BC_Z |
     CH4_F2_FLUID_BC_Z_P_SLIP | CH4_F2_FLUID_BC_Z_M_SLIP | CH4_F2_TEMPERATURE_BC_X | CH4_F2_TEMPERATURE_BC_X_P_NOFLUX |
     CH4_F2_TEMPERATURE_BC_X_M_NOFLUX | CH4_F2_TEMPERATURE_BC_Z | CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX |
-    CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX | CH4_F2_SCALAR_BC_X | CH4_F2_SCALAR_BC_Z;
+    CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX | CH4_F2_SCALAR_BC_X | CH4_F2_SCALAR_BC_Z | CH4_F2_LAGRANGE_TEMPERATURE |
+    CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE;
+// the walls of the second flag word
+const uint64_t WALLS2 = CH4_F2_FLUID_BC_X | CH4_F2_FLUID_BC_X_P_SLIP | CH4_F2_FLUID_BC_X_M_SLIP | CH4_F2_FLUID_BC_Z |
+                        CH4_F2_FLUID_BC_Z_P_SLIP | CH4_F2_FLUID_BC_Z_M_SLIP | CH4_F2_TEMPERATURE_BC_X |
+                        CH4_F2_TEMPERATURE_BC_X_P_NOFLUX | CH4_F2_TEMPERATURE_BC_X_M_NOFLUX | CH4_F2_TEMPERATURE_BC_Z |
+                        CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX | CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX | CH4_F2_SCALAR_BC_X |
+                        CH4_F2_SCALAR_BC_Z;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -734,7 +741,12 @@ struct Engine : EngineBase {
   }
 
   size_t nhome() const { return (size_t)(c.NX + 1) * (c.NY + 1) * (c.NZ + 1); }
-  int nrec() const { return (c.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) ? 15 : 9; }
+  bool twoway_temp() const { return (c.flags2 & CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE) != 0; }
+  // deposit record fields: fac*fp (3) + the stencil weights (6 trilinear, 12 tricubic), then
+  // with the thermal coupling fac*sp
+  int nrec() const { return ((c.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) ? 15 : 9) + (twoway_temp() ? 1 : 0); }
+  // planes of a deposit buffer: the force, and the temperature source with the thermal coupling
+  int dplanes() const { return twoway_temp() ? 4 : 3; }
 
   PartParams<A> part_params() {
     PartParams<A> Q{};
@@ -775,6 +787,10 @@ struct Engine : EngineBase {
     Q.dense = dense;
     Q.dep = dbuf[dcur_i];
     Q.status = pstatus;
+    Q.lagr_temp = (c.flags2 & CH4_F2_LAGRANGE_TEMPERATURE) != 0;
+    Q.twoway_temp = twoway_temp();
+    Q.kappa = c.kappa;
+    Q.nu = c.nu;
     return Q;
   }
 
@@ -914,6 +930,14 @@ struct Engine : EngineBase {
       h[(size_t)PF_DR * n + i] = (3.0 - beta) / (2.0 * beta);
       double squared_radius = 3.0 * c.nu * beta * tau;
       h[(size_t)PF_VOL * n + i] = (4. / 3.) * 3.14159265359 * std::pow(squared_radius, 3. / 2.);
+      if (c.flags2 & CH4_F2_LAGRANGE_TEMPERATURE) {
+        // 1/tau_heat = 2 kappa / (tau_drag nu cp_p (3 - beta)) times dt_lagr, and exp(-fac1),
+        // src/lagrange.c:4009-4017 (host libm, as the reference)
+        double fac1 = (c.kappa * 2.0) / (tau * c.nu * parts[i].cp_p * (3 - beta));
+        fac1 *= c.time_dt / c.time_dt_lagr_factor;
+        h[(size_t)PF_TFAC * n + i] = fac1;
+        h[(size_t)PF_TEXP * n + i] = std::exp(-fac1);
+      }
     }
     if ((st = H->cuda(cudaMemcpy(pf, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice), "particles up")))
       return st;
@@ -1063,8 +1087,9 @@ struct Engine : EngineBase {
     }
     if (twoway()) {
       for (int b = 0; b < 2; b++) {
-        if (cudaMalloc(&dbuf[b], 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "deposit");
-        if (cudaMemset(dbuf[b], 0, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "deposit memset");
+        if (cudaMalloc(&dbuf[b], dplanes() * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "deposit");
+        if (cudaMemset(dbuf[b], 0, dplanes() * N * sizeof(A)) != cudaSuccess)
+          return H->fail(CH4_ERR_CUDA, "deposit memset");
       }
       const size_t nreg = (size_t)((c.NX + GATHER_BLOCK - 1) / GATHER_BLOCK) * c.NY * c.NZ;
       if (cudaMalloc(&crng, sizeof(int2) * nhome()) != cudaSuccess ||
@@ -1159,6 +1184,7 @@ struct Engine : EngineBase {
     P.kol = kol;
     P.csmag2_y = vd;
     P.dcur = P.dprev = nullptr;
+    P.tsrc = nullptr;
     P.fm_prev = P.fm_cur = fmbuf;  // both slots hold {0, 1} until the first correction
   }
 
@@ -1425,6 +1451,10 @@ struct Engine : EngineBase {
           dcur_i ^= 1;
           P.dcur = dbuf[dcur_i];
           P.dprev = dbuf[dcur_i ^ 1];
+          if (twoway_temp()) {  // this step's temperature source, the 4th plane of the deposit
+            P.tsrc = dbuf[dcur_i] + 3 * N;
+            P.feat |= K_TSRC;
+          }
           P.feat |= K_TWOWAY;
           if (c.resume || n_step > 1) {
             PartParams<A> Q = part_params();
@@ -1432,7 +1462,8 @@ struct Engine : EngineBase {
             if ((st = H->cuda(launch_deposit(Q, key2, order2, cubtmp, bytes, H->stream), "deposit"))) return st;
             // the deposit's sort already holds the slots in home-cell order
             if (np > 0 && ++since_reorder >= REORDER_EVERY && (st = reorder_particles(0))) return st;
-          } else if ((st = H->cuda(cudaMemsetAsync(dbuf[dcur_i], 0, 3 * N * sizeof(A), H->stream), "deposit zero"))) {
+          } else if ((st = H->cuda(cudaMemsetAsync(dbuf[dcur_i], 0, dplanes() * N * sizeof(A), H->stream),
+                                   "deposit zero"))) {
             return st;
           }
         }
@@ -1629,7 +1660,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
     double* dst;
     bool needed;
   };
-  double NX, NY, NZ, particle_number = 0, resume = 0, tau_drag_types = 1, beta_coeff_types = 1;
+  double NX, NY, NZ, particle_number = 0, resume = 0, tau_drag_types = 1, beta_coeff_types = 1, cp_coeff_types = 1;
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
@@ -1652,6 +1683,8 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
       {"tau_drag_types", &tau_drag_types, (fl & CH4_F_LAGRANGE) != 0},
       {"beta_coeff_types", &beta_coeff_types,
        (fl & CH4_F_LAGRANGE) && (fl & CH4_F_LAGRANGE_GRADIENT) && (fl & CH4_F_LAGRANGE_ADDEDMASS)},
+      // LAGRANGE_TEMPERATURE multiplies the types by the specific-heat classes, src/parameters.c:606-618
+      {"cp_coeff_types", &cp_coeff_types, (fl & CH4_F_LAGRANGE) && (cfg->flags2 & CH4_F2_LAGRANGE_TEMPERATURE)},
       {"noise_u", &cfg->noise_u, (fl & CH4_F_FLUID_INITIAL_ADD_NOISE) != 0},  // src/parameters.c:216-220
       {"noise_t", &cfg->noise_t, T && (fl & CH4_F_TEMPERATURE_INITIAL_ADD_NOISE)},  // src/parameters.c:347-351
   };
@@ -1670,7 +1703,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   cfg->NZ = (int)NZ;
   cfg->particle_number = (int)particle_number;
   cfg->resume = (int)resume;
-  cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types;
+  cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types * (int)cp_coeff_types;
   // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
   cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
   cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;
@@ -1785,6 +1818,8 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_TEMPERATURE_BC_Z_M_NOFLUX", CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX},
       {"LB_SCALAR_BC_X", CH4_F2_SCALAR_BC_X},
       {"LB_SCALAR_BC_Z", CH4_F2_SCALAR_BC_Z},
+      {"LAGRANGE_TEMPERATURE", CH4_F2_LAGRANGE_TEMPERATURE},
+      {"LAGRANGE_TWOWAY_TEMPERATURE", CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -1909,8 +1944,17 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
              CH4_ERR_UNSUPPORTED;
   }
   if (c->flags & CH4_F_LAGRANGE) {
-    if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_LB_SCALAR)) || c->flags2)
+    if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_LB_SCALAR)) || (c->flags2 & WALLS2))
       return why = "particles are implemented for the periodic box (fluid, optionally temperature)",
+             CH4_ERR_UNSUPPORTED;
+    if ((c->flags2 & CH4_F2_LAGRANGE_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
+      return why = "LAGRANGE_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
+    // the heat exchange reads the particle temperature (src/typedef.h:467-470) and enters the
+    // temperature populations through LB_TEMPERATURE_FORCING's source (src/forcing.c:1452-1476)
+    if ((c->flags2 & CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE) &&
+        (!(c->flags2 & CH4_F2_LAGRANGE_TEMPERATURE) || !(c->flags & CH4_F_LAGRANGE_TWOWAY) ||
+         !(c->flags & CH4_F_TEMPERATURE_FORCING)))
+      return why = "LAGRANGE_TWOWAY_TEMPERATURE needs LAGRANGE_TEMPERATURE, LAGRANGE_TWOWAY and LB_TEMPERATURE_FORCING",
              CH4_ERR_UNSUPPORTED;
     if (!(c->flags & CH4_F_LAGRANGE_WRAP)) return why = "particles need LAGRANGE_WRAP", CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_LAGRANGE_TWOWAY) && !(c->flags & CH4_F_LAGRANGE_TWOWAY_MOMENTUM))
@@ -2574,7 +2618,7 @@ namespace {
 using PField = std::pair<const char*, double ch4_particle::*>;
 
 // the per-particle datasets of output_particles, in its order, for the supported flags
-std::vector<PField> lagrange_fields(uint64_t fl, bool output_fluid) {
+std::vector<PField> lagrange_fields(uint64_t fl, uint64_t fl2, bool output_fluid) {
   using P = ch4_particle;
   std::vector<PField> v = {{"name", &P::name}, {"tau_drag", &P::tau_drag}, {"x", &P::x},   {"y", &P::y},
                            {"z", &P::z},       {"vx", &P::vx},             {"vy", &P::vy}, {"vz", &P::vz},
@@ -2600,12 +2644,14 @@ std::vector<PField> lagrange_fields(uint64_t fl, bool output_fluid) {
   if (fl & CH4_F_LB_TEMPERATURE) {
     v.insert(v.end(), {{"temperature", &P::t}, {"dt_t", &P::dt_t}});
     if (grad) v.insert(v.end(), {{"dx_t", &P::dx_t}, {"dy_t", &P::dy_t}, {"dz_t", &P::dz_t}});
+    if (fl2 & CH4_F2_LAGRANGE_TEMPERATURE)  // src/lagrange.c:2090-2103
+      v.insert(v.end(), {{"temperature_particle", &P::t_p}, {"cp_particle", &P::cp_p}});
   }
   return v;
 }
 
 // the members of point_particle in part.h5, in write_point_particle_h5's order
-std::vector<PField> part_members(uint64_t fl) {
+std::vector<PField> part_members(uint64_t fl, uint64_t fl2) {
   using P = ch4_particle;
   std::vector<PField> v = {{"name", &P::name},     {"x", &P::x},           {"y", &P::y},
                            {"z", &P::z},           {"vx", &P::vx},         {"vy", &P::vy},
@@ -2632,6 +2678,8 @@ std::vector<PField> part_members(uint64_t fl) {
   if (fl & CH4_F_LB_TEMPERATURE) {
     v.push_back({"t", &P::t});
     if (fl & CH4_F_LAGRANGE_GRADIENT) v.insert(v.end(), {{"dx_t", &P::dx_t}, {"dy_t", &P::dy_t}, {"dz_t", &P::dz_t}});
+    if (fl2 & CH4_F2_LAGRANGE_TEMPERATURE)  // src/lagrange.c:4442-4447
+      v.insert(v.end(), {{"temperature_particle", &P::t_p}, {"cp_particle", &P::cp_p}});
   }
   return v;
 }
@@ -2643,8 +2691,8 @@ bool particles_of(ch4_handle* h, std::vector<ch4_particle>& p, ch4_status& st) {
 }
 
 // the XDMF companion of particle_<n>.h5 (src/lagrange.c:2172-2590)
-bool write_particle_xmf(const std::string& path, const std::string& h5name, int np, uint64_t fl, bool output_fluid,
-                        double time_now) {
+bool write_particle_xmf(const std::string& path, const std::string& h5name, int np, uint64_t fl, uint64_t fl2,
+                        bool output_fluid, double time_now) {
   FILE* f = std::fopen(path.c_str(), "w");
   if (!f) return false;
   const int size = (int)sizeof(double);
@@ -2700,6 +2748,10 @@ bool write_particle_xmf(const std::string& path, const std::string& h5name, int 
     scalar("temperature");
     scalar("dt_t");
     if (fl & CH4_F_LAGRANGE_GRADIENT) joined("temperature gradient", "Vector", {"dx_t", "dy_t", "dz_t"});
+    if (fl2 & CH4_F2_LAGRANGE_TEMPERATURE) {  // src/lagrange.c:2515-2529
+      scalar("temperature_particle");
+      scalar("cp_particle");
+    }
   }
   std::fprintf(f, "<Time Value=\" %e\" />\n</Grid>\n</Domain>\n</Xdmf>\n", time_now);
   return std::fclose(f) == 0;
@@ -2718,7 +2770,7 @@ ch4_status ch4_output_particles_h5(ch4_handle* h, const char* dir, int itime, do
   const uint64_t np = p.size();
   h5::Group g;
   g.name = "lagrange";
-  for (const PField& pf : lagrange_fields(c.flags, fluid)) {
+  for (const PField& pf : lagrange_fields(c.flags, c.flags2, fluid)) {
     h5::Dataset d;
     d.name = pf.first;
     d.type = h5::Type::f64();
@@ -2737,7 +2789,7 @@ ch4_status ch4_output_particles_h5(ch4_handle* h, const char* dir, int itime, do
   const std::string base = dir && *dir ? std::string(dir) + "/" : std::string();
   std::string err;
   if (!h5::write_file(base + stem + ".h5", {g}, err)) return h->fail(CH4_ERR_ARG, "%s", err.c_str());
-  if (!write_particle_xmf(base + stem + ".xmf", stem + ".h5", (int)np, c.flags, fluid, time_now))
+  if (!write_particle_xmf(base + stem + ".xmf", stem + ".h5", (int)np, c.flags, c.flags2, fluid, time_now))
     return h->fail(CH4_ERR_ARG, "cannot write %s.xmf", stem.c_str());
   return CH4_OK;
 }
@@ -2749,7 +2801,7 @@ ch4_status ch4_write_particles_h5(ch4_handle* h, const char* path) {
   std::vector<ch4_particle> p;
   ch4_status st;
   if (!particles_of(h, p, st)) return st;
-  const std::vector<PField> mem = part_members(c.flags);
+  const std::vector<PField> mem = part_members(c.flags, c.flags2);
   std::vector<std::string> names;
   for (const PField& m : mem) names.push_back(m.first);
   h5::Group g;
@@ -2796,7 +2848,7 @@ ch4_status ch4_read_particles_h5(ch4_handle* h, const char* path) {
   // every member this build knows and the file has, by name
   std::vector<PField> mem;
   std::vector<std::string> names;
-  for (const PField& m : part_members(~0ull))
+  for (const PField& m : part_members(~0ull, ~0ull))
     for (const h5::Member& fm : o.type.members)
       if (fm.name == m.first) {
         mem.push_back(m);

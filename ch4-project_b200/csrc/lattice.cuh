@@ -62,7 +62,7 @@ enum : uint32_t {
   K_LES = 1u << 15,
   K_TWOWAY = 1u << 16,
   K_BETA2 = 1u << 17,
-  K_TSRC = 1u << 18,
+  K_TSRC = 1u << 18,     // temperature source of the particles' heat exchange (tsrc), added after the collision
   K_NOZERO = 1u << 19,  // LB_FLUID_FORCING_NOZEROMODE: subtract the mean force
   K_CPOWER = 1u << 20,  // LB_FLUID_FORCING_CONSTANT_POWER: scale to a fixed mean power
   K_TRT = 1u << 21,     // METHOD_TRT: two-relaxation-time collision
@@ -117,6 +117,8 @@ struct StepParams {
   // two-way coupling deposit of this and the previous step (3 SoA planes each)
   const A* dcur;
   const A* dprev;
+  // LAGRANGE_TWOWAY_TEMPERATURE: this step's temperature source (one plane)
+  const A* tsrc;
   // global force corrections {f0x, f0y, f0z, coeffx, coeffy, coeffz} of the previous
   // and current step (NOZEROMODE / CONSTANT_POWER), device arrays of 6
   const A* fm_prev;

@@ -181,6 +181,7 @@ __device__ __noinline__ void push_walled(const StepParams<A>& P, int idx, Nbr nb
 template <typename A>
 struct CellState {
   A rho, ux, uy, uz, u2, tt, ss;
+  A ts;  // temperature source of the particles (K_TSRC), else 0
   A Fx, Fy, Fz;
   A invtau, it, is;
   A base, uF;  // FP32 form: 1 - u2/(2 cs^2), u.F
@@ -217,6 +218,7 @@ __device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellSt
       const A geq = c.tt * P.w[q] * poly;
       A s = g[q];
       s += -c.it * (g[q] - geq);
+      if (P.feat & K_TSRC) s += P.w[q] * c.ts;  // add_forcing's w t_source, src/forcing.c:1475
       g[q] = s;
     }
     if constexpr (SCAL) {
@@ -242,7 +244,10 @@ __device__ __forceinline__ void collide_one(const StepParams<A>& P, const CellSt
       const A feq = (c.rho * P.w[q]) * poly;
       f[q] = f[q] + c.invtau * (feq - f[q]);
     }
-    if constexpr (THERM) g[q] += c.it * ((c.tt * P.w[q]) * poly - g[q]);
+    if constexpr (THERM) {
+      g[q] += c.it * ((c.tt * P.w[q]) * poly - g[q]);
+      if (P.feat & K_TSRC) g[q] += P.w[q] * c.ts;
+    }
     if constexpr (SCAL) h[q] += c.is * ((c.ss * P.w[q]) * poly - h[q]);
   }
 }
@@ -307,6 +312,9 @@ __device__ __forceinline__ void collide_trt(const StepParams<A>& P, const CellSt
 #pragma unroll
     for (int q = 0; q < Q; q++) eq[q] = EXACT ? c.tt * P.w[q] * poly[q] : (c.tt * P.w[q]) * poly[q];
     trt_set(g, eq, c.it, (P.feat & K_TLES) ? trt_minus(c.it) : P.invtau_m[1]);
+    if (P.feat & K_TSRC)
+#pragma unroll
+      for (int q = 0; q < Q; q++) g[q] += P.w[q] * c.ts;
   }
   if constexpr (SCAL) {
 #pragma unroll
@@ -338,6 +346,7 @@ __device__ __forceinline__ void lb_cell(const StepParams<A>& P, int x, int y, in
   const A mx = momx(f), my = momy(f), mz = momz(f);
   c.tt = THERM ? mom0(g) : A(0);
   c.ss = SCAL ? mom0(h) : A(0);
+  c.ts = (THERM && (F & K_TSRC)) ? P.tsrc[idx] : A(0);
 
   // u^n = mv/rho + dt/2 F^{n-1} (src/lb.c:464-466); F^n for Guo (src/forcing.c:1423-1435)
   A px = A(0), py = A(0), pz = A(0);

@@ -33,7 +33,11 @@ namespace ch4 {
 constexpr int PF_FIELDS = (int)(sizeof(ch4_particle) / sizeof(double));
 constexpr int PF_VOL = PF_FIELDS;      // (4/3) pi r^3 with r^2 = 3 nu beta tau_drag
 constexpr int PF_DR = PF_FIELDS + 1;   // rho_p / rho_f = (3 - beta) / (2 beta)
-constexpr int PF_TOTAL = PF_FIELDS + 2;
+// LAGRANGE_TEMPERATURE: fac1 = dt_lagr / tau_heat and exp(-fac1) of src/lagrange.c:4009-4017,
+// per-particle constants computed on the host with the host libm
+constexpr int PF_TFAC = PF_FIELDS + 2;
+constexpr int PF_TEXP = PF_FIELDS + 3;
+constexpr int PF_TOTAL = PF_FIELDS + 4;
 constexpr int GATHER_BLOCK = 128;  // threads (cells along x) per block of the first deposit pass
 
 template <typename A>
@@ -75,6 +79,9 @@ struct PartParams {
   int* dense;            // the listed cells, compacted in region order
   A* dep;                // 3 SoA planes, output
   int* status;           // set to 1 when a particle position is outside [0, S] or not finite
+  int lagr_temp;         // LAGRANGE_TEMPERATURE: the particle temperature relaxes towards the fluid's
+  int twoway_temp;       // LAGRANGE_TWOWAY_TEMPERATURE: record field nrec-1 holds fac * sp, dep a 4th plane
+  double kappa, nu;
 };
 
 #ifdef __CUDACC__
@@ -496,6 +503,10 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
     F(az_old) = az;
   }
   if constexpr (ORIENT) orient_particle(pf, np, ip, gr, P.jeffery != 0, first, dtl);
+  if (P.lagr_temp) {  // T_p <- (T_p + fac1 T) exp(-fac1), src/lagrange.c:4007-4018
+    const double fac1 = pf[(long long)PF_TFAC * np + ip], e = pf[(long long)PF_TEXP * np + ip];
+    F(t_p) = (F(t_p) + fac1 * v[3]) * e;
+  }
   // ---- LAGRANGE_WRAP of sendrecv_particles
   F(x) = pwrapd(xn, P.SX);
   F(z) = pwrapd(zn, P.SZ);
@@ -532,6 +543,10 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
   r[1LL * np + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;
   r[2LL * np + ip] = live ? fac * (F(Dt_uz) - gz + dr * (gz - F(az))) : 0.0;
+  if (P.twoway_temp) {  // src/lagrange_feedback.c:181-190: sp = Dt_t + (T_p - T) kappa / (nu beta tau_drag)
+    const double fac2 = P.kappa / (P.nu * F(beta_coeff) * F(tau_drag));
+    r[(long long)(P.nrec - 1) * np + ip] = live ? fac * (F(Dt_t) + (F(t_p) - F(t)) * fac2) : 0.0;
+  }
   if (P.tricubic) {  // cubic weights of the offsets -1 .. 2, src/lagrange_feedback.c:51-60
 #pragma unroll
     for (int n = -1; n <= 2; n++) {
@@ -611,23 +626,30 @@ __device__ __forceinline__ long long home_of(int i, int j, int k, int h, int HX,
 // contribution of the particle at sorted position `slot` to a cell that is corner
 // (di, dj, dk) of its stencil: the ip corner when di == 0 (weight dxm), the im corner
 // when di == 1 (dxp); accumulated as the reference does, acc += (fac*fp) * vol
-__device__ __forceinline__ void deposit_add(const double* __restrict__ r, long long np, int slot, int best,
-                                            double& acc0, double& acc1, double& acc2) {
+// (the momentum's three record fields 0..2 with MOM, the temperature source's field trec
+// with TEMP)
+template <bool MOM, bool TEMP>
+__device__ __forceinline__ void deposit_add(const double* __restrict__ r, long long np, int slot, int best, int trec,
+                                            double* acc) {
   const int di = best & 1, dj = (best >> 1) & 1, dk = (best >> 2) & 1;
   const double wx = r[(3 + di) * np + slot];
   const double wy = r[(5 + dj) * np + slot];
   const double wz = r[(7 + dk) * np + slot];
   const double vol = wx * wy * wz;
-  acc0 += r[slot] * vol;
-  acc1 += r[np + slot] * vol;
-  acc2 += r[2 * np + slot] * vol;
+  if constexpr (MOM) {
+    acc[0] += r[slot] * vol;
+    acc[1] += r[np + slot] * vol;
+    acc[2] += r[2 * np + slot] * vol;
+  }
+  if constexpr (TEMP) acc[3] += r[trec * np + slot] * vol;
 }
 
 // Merge of the 8 home lists of one cell in particle-index order (the reference's
 // summation order).  The list heads stay in registers: every index into pos/endp/head
 // is a constant after unrolling, one dependent load per merged particle.
+template <bool MOM, bool TEMP>
 __device__ __forceinline__ void deposit_merge(const int* __restrict__ spid, const double* __restrict__ r, long long np,
-                                              int* pos, const int* endp, double& acc0, double& acc1, double& acc2) {
+                                              int* pos, const int* endp, int trec, double* acc) {
   constexpr int NONE = 0x7fffffff;
   int head[8];
 #pragma unroll
@@ -648,8 +670,45 @@ __device__ __forceinline__ void deposit_merge(const int* __restrict__ spid, cons
         slot = pos[h]++;
         head[h] = pos[h] < endp[h] ? spid[pos[h]] : NONE;
       }
-    deposit_add(r, np, slot, best, acc0, acc1, acc2);
+    deposit_add<MOM, TEMP>(r, np, slot, best, trec, acc);
   }
+}
+
+// The temperature source that the reference's scalar border fold (add_sendrecv_borders_scalar,
+// src/lagrange_feedback.c:261-523) adds onto a face cell: the deposit on the halo cell
+// (vi, vj, vk) one beyond the opposite face, summed over its home lists in particle order
+// (homes outside the lattice hold nobody).
+template <typename A>
+__device__ __forceinline__ double halo_image_t(const PartParams<A>& P, int vi, int vj, int vk) {
+  const int HX = P.NX + 1, HY = P.NY + 1, HZ = P.NZ + 1;
+  int pos[8], endp[8];
+#pragma unroll
+  for (int h = 0; h < 8; h++) {
+    const int hx = vi + (h & 1), hy = vj + ((h >> 1) & 1), hz = vk + ((h >> 2) & 1);
+    pos[h] = endp[h] = 0;
+    if (hx >= 0 && hx < HX && hy >= 0 && hy < HY && hz >= 0 && hz < HZ) {
+      const int2 rg = P.cell_rng[((long long)hz * HY + hy) * HX + hx];
+      pos[h] = rg.x;
+      endp[h] = rg.y;
+    }
+  }
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  deposit_merge<false, true>(P.spid, P.srec, P.np, pos, endp, P.nrec - 1, acc);
+  return acc[3];
+}
+
+// The face folds of the temperature source, in the reference's order: per axis x, y, z,
+// the image beyond the upper face onto the first layer, then the image beyond the lower
+// face onto the last layer (edge and corner images are lost, as in the reference).
+template <typename A>
+__device__ __forceinline__ double fold_faces_t(const PartParams<A>& P, int i, int j, int k, double acc) {
+  if (i == 0) acc += halo_image_t(P, P.NX, j, k);
+  if (i == P.NX - 1) acc += halo_image_t(P, -1, j, k);
+  if (j == 0) acc += halo_image_t(P, i, P.NY, k);
+  if (j == P.NY - 1) acc += halo_image_t(P, i, -1, k);
+  if (k == 0) acc += halo_image_t(P, i, j, P.NZ);
+  if (k == P.NZ - 1) acc += halo_image_t(P, i, j, -1);
+  return acc;
 }
 
 // Deposit on every lattice cell, first pass: cells whose 8 home cells hold no
@@ -682,14 +741,21 @@ __global__ void __launch_bounds__(GATHER_BLOCK) deposit_gather_kernel(const Part
       }
       m += cnt;
     }
-    if (m >= 2) {
+    // with the temperature source a face cell also takes the images of the halo cells
+    // beyond the opposite face: the merge pass does those
+    const bool face = P.twoway_temp && (i == 0 || i == P.NX - 1 || j == 0 || j == P.NY - 1 || k == 0 || k == P.NZ - 1);
+    if (m >= 2 || face) {
       P.busy[(long long)bid * GATHER_BLOCK + atomicAdd(&s_n, 1)] = (int)cidx;  // the merge writes this cell
     } else {
-      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-      if (m == 1) deposit_add(P.srec, P.np, slot, best, acc0, acc1, acc2);
-      P.dep[cidx] = (A)acc0;
-      P.dep[P.N + cidx] = (A)acc1;
-      P.dep[2 * P.N + cidx] = (A)acc2;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      if (m == 1) {
+        if (P.twoway_temp) deposit_add<true, true>(P.srec, P.np, slot, best, P.nrec - 1, acc);
+        else deposit_add<true, false>(P.srec, P.np, slot, best, 0, acc);
+      }
+      P.dep[cidx] = (A)acc[0];
+      P.dep[P.N + cidx] = (A)acc[1];
+      P.dep[2 * P.N + cidx] = (A)acc[2];
+      if (P.twoway_temp) P.dep[3 * P.N + cidx] = (A)acc[3];
     }
   }
   __syncthreads();
@@ -720,11 +786,16 @@ __global__ void deposit_busy_kernel(const PartParams<A> P, int nregions) {
       pos[h] = rg.x;
       endp[h] = rg.y;
     }
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
-    deposit_merge(P.spid, P.srec, P.np, pos, endp, acc0, acc1, acc2);
-    P.dep[cidx] = (A)acc0;
-    P.dep[P.N + cidx] = (A)acc1;
-    P.dep[2 * P.N + cidx] = (A)acc2;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (P.twoway_temp) {
+      deposit_merge<true, true>(P.spid, P.srec, P.np, pos, endp, P.nrec - 1, acc);
+      P.dep[3 * P.N + cidx] = (A)fold_faces_t(P, i, j, k, acc[3]);
+    } else {
+      deposit_merge<true, false>(P.spid, P.srec, P.np, pos, endp, 0, acc);
+    }
+    P.dep[cidx] = (A)acc[0];
+    P.dep[P.N + cidx] = (A)acc[1];
+    P.dep[2 * P.N + cidx] = (A)acc[2];
   }
 }
 
@@ -732,14 +803,10 @@ __global__ void deposit_busy_kernel(const PartParams<A> P, int nregions) {
 // with lower stencil corner im adds to the cells im-1 .. im+2 on each axis with the
 // weight wx[a] * wy[b] * wz[c], so a cell merges the 64 home cells around it, in
 // particle-index order (the heads kept in a small local array), halo cells dropped.
+// the 64 home ranges around cell (i, j, k) (possibly a halo cell); returns the particles listed
 template <typename A>
-__global__ void deposit_tricubic_kernel(const PartParams<A> P) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.NX) return;
-  const int j = blockIdx.y, k = blockIdx.z;
-  const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
+__device__ __forceinline__ int tricubic_homes(const PartParams<A>& P, int i, int j, int k, int* pos, int* endp) {
   const int HX = P.NX + 1, HY = P.NY + 1, HZ = P.NZ + 1;
-  int pos[64], endp[64];
   int m = 0;
   for (int h = 0; h < 64; h++) {
     // home (shifted by one) of the particles whose offset from this cell is a-1 on x etc.
@@ -752,9 +819,16 @@ __global__ void deposit_tricubic_kernel(const PartParams<A> P) {
     endp[h] = rg.y;
     m += rg.y - rg.x;
   }
-  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  return m;
+}
+
+// merge of m listed particles in particle-index order; MOM: the momentum fields, and with
+// P.twoway_temp the temperature source into acc[3]
+template <bool MOM, typename A>
+__device__ __forceinline__ void tricubic_merge(const PartParams<A>& P, int* pos, const int* endp, int m, double* acc) {
   const long long np = P.np;
   const double* __restrict__ r = P.srec;
+  const int trec = P.nrec - 1;
   for (int left = m; left > 0; left--) {
     int best = -1, bv = 0x7fffffff;
     for (int h = 0; h < 64; h++)
@@ -768,13 +842,60 @@ __global__ void deposit_tricubic_kernel(const PartParams<A> P) {
     const int slot = pos[best]++;
     const int a = best & 3, b = (best >> 2) & 3, c = best >> 4;
     const double w = r[(3 + a) * np + slot] * r[(7 + b) * np + slot] * r[(11 + c) * np + slot];
-    acc0 += r[slot] * w;
-    acc1 += r[np + slot] * w;
-    acc2 += r[2 * np + slot] * w;
+    if constexpr (MOM) {
+      acc[0] += r[slot] * w;
+      acc[1] += r[np + slot] * w;
+      acc[2] += r[2 * np + slot] * w;
+    }
+    if (P.twoway_temp) acc[3] += r[trec * np + slot] * w;
   }
-  P.dep[cidx] = (A)acc0;
-  P.dep[P.N + cidx] = (A)acc1;
-  P.dep[2 * P.N + cidx] = (A)acc2;
+}
+
+// the temperature deposit on halo cell (i, j, k), in particle order
+template <typename A>
+__device__ __noinline__ double tricubic_image_t(const PartParams<A>& P, int i, int j, int k) {
+  int pos[64], endp[64];
+  const int m = tricubic_homes(P, i, j, k, pos, endp);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  tricubic_merge<false>(P, pos, endp, m, acc);
+  return acc[3];
+}
+
+template <typename A>
+__global__ void deposit_tricubic_kernel(const PartParams<A> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.NX) return;
+  const int j = blockIdx.y, k = blockIdx.z;
+  const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
+  int pos[64], endp[64];
+  const int m = tricubic_homes(P, i, j, k, pos, endp);
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  tricubic_merge<true>(P, pos, endp, m, acc);
+  P.dep[cidx] = (A)acc[0];
+  P.dep[P.N + cidx] = (A)acc[1];
+  P.dep[2 * P.N + cidx] = (A)acc[2];
+  if (P.twoway_temp) {
+    // the scalar border fold with a border two cells wide (src/typedef.h:325-326): per
+    // axis, the images of the two halo layers beyond the upper face onto the first two
+    // layers, then those beyond the lower face onto the last two
+    double t = acc[3];
+    const int n3[3] = {P.NX, P.NY, P.NZ};
+    const int c3[3] = {i, j, k};
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+      if (c3[ax] < 2) {
+        int v[3] = {i, j, k};
+        v[ax] += n3[ax];
+        t += tricubic_image_t(P, v[0], v[1], v[2]);
+      }
+      if (c3[ax] >= n3[ax] - 2) {
+        int v[3] = {i, j, k};
+        v[ax] -= n3[ax];
+        t += tricubic_image_t(P, v[0], v[1], v[2]);
+      }
+    }
+    P.dep[3 * P.N + cidx] = (A)t;
+  }
 }
 
 #endif  // __CUDACC__

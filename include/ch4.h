@@ -132,7 +132,13 @@ enum {
   CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX = 1ull << 11,
   /* scalar walls on x and z: fixed value S_top / S_bot, src/boundary_conditions.c:1380-1520 */
   CH4_F2_SCALAR_BC_X = 1ull << 12,
-  CH4_F2_SCALAR_BC_Z = 1ull << 13
+  CH4_F2_SCALAR_BC_Z = 1ull << 13,
+  /* particle temperature with thermal inertia, dT_p/dt = (T - T_p)/tau_heat,
+   * src/lagrange.c:4007-4018 */
+  CH4_F2_LAGRANGE_TEMPERATURE = 1ull << 14,
+  /* two-way thermal coupling: the particles' heat exchange deposited as a temperature
+   * source (with LB_TEMPERATURE_FORCING), src/lagrange_feedback.c:181-230 */
+  CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE = 1ull << 15
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
@@ -210,6 +216,9 @@ typedef struct {
   double px, py, pz;
   double dt_px, dt_py, dt_pz;
   double aspect_ratio;
+  /* LAGRANGE_TEMPERATURE: the particle's own temperature and specific heat (relative to
+   * the fluid's), src/typedef.h:467-470 */
+  double t_p, cp_p;
 } ch4_particle;
 
 /* Global averages of dump_averages (src/output.c:63-~760), FP64 sums over the

@@ -74,6 +74,8 @@ struct ch4o_state {
   double *pvol, *pdr; /* per-particle volume (4/3 pi r^3) and rho_p/rho_f */
   /* two-way deposit of this and the previous step, velocity field for the particles */
   double *dcur, *dprev, *uf, *tf;
+  /* LAGRANGE_TWOWAY_TEMPERATURE: temperature source deposited this step (t_source_twoway) */
+  double *tsrc;
   /* build_forcing's global corrections of the previous and current step:
    * mean force f0 (NOZEROMODE) and per-component power coefficients (CONSTANT_POWER) */
   double fm_prev[6], fm_cur[6];
@@ -703,6 +705,13 @@ static void move_particle(const ch4o_state *s, ch4_particle *p, int first, doubl
     p->ay_old = p->ay;
     p->az_old = p->az;
   }
+  if (s->cfg.flags2 & CH4_F2_LAGRANGE_TEMPERATURE) {
+    /* particle temperature, src/lagrange.c:4007-4018: 1/tau_heat =
+     * 2 kappa / (tau_drag nu cp_p (3 - beta)), T_p <- (T_p + fac1 T) exp(-fac1) */
+    double fac1 = (s->cfg.kappa * 2.0) / (p->tau_drag * s->cfg.nu * p->cp_p * (3 - p->beta_coeff));
+    fac1 *= dtl;
+    p->t_p = (p->t_p + fac1 * p->t) * exp(-fac1);
+  }
 }
 
 /* sendrecv_particles on one rank (src/lagrange.c:4028-4221): LAGRANGE_WRAP puts
@@ -760,8 +769,52 @@ static double cubic_weight(double x) {
   return 0.0;
 }
 
-static void deposit(const ch4o_state *s, double *D) {
+/* halo width BRD of the reference build for the flag set (src/typedef.h:313-331) */
+static int brd_of(const ch4_config *c) {
+  return (c->flags & (CH4_F_LAGRANGE_GRADIENT_BRD2 | CH4_F_FLUID_LES | CH4_F_LAGRANGE_TWOWAY_TRICUBIC)) ? 2 : 1;
+}
+
+/* add_sendrecv_borders_scalar of one rank (src/lagrange_feedback.c:261-523) on a
+ * halo-padded field H: per axis x, y, z, the upper halo layers are added onto the first
+ * interior layers and then the lower halo layers onto the last ones (faces only: the
+ * edge and corner steps add interior values into halo cells, so deposits there are
+ * lost); the interior is copied to TS. */
+static void fold_scalar(const ch4o_state *s, double *H, int B, double *TS) {
+  const int L[3] = {s->NX, s->NY, s->NZ};
+  const int PX = s->NX + 2 * B, PY = s->NY + 2 * B;
+#define HI(i, j, k) H[((size_t)(k) * PY + (j)) * PX + (i)]
+  for (int a = 0; a < 3; a++) {
+    const int o1 = (a + 1) % 3, o2 = (a + 2) % 3;
+    int c[3];
+    for (c[o2] = B; c[o2] < L[o2] + B; c[o2]++)
+      for (c[o1] = B; c[o1] < L[o1] + B; c[o1]++) {
+        for (int i = 0; i < B; i++) { /* upper halo i + L + B onto interior i + B */
+          int d[3] = {c[0], c[1], c[2]}, sc[3] = {c[0], c[1], c[2]};
+          d[a] = i + B;
+          sc[a] = i + L[a] + B;
+          HI(d[0], d[1], d[2]) += HI(sc[0], sc[1], sc[2]);
+        }
+        for (int i = 0; i < B; i++) { /* lower halo i onto interior i + L */
+          int d[3] = {c[0], c[1], c[2]}, sc[3] = {c[0], c[1], c[2]};
+          d[a] = i + L[a];
+          sc[a] = i;
+          HI(d[0], d[1], d[2]) += HI(sc[0], sc[1], sc[2]);
+        }
+      }
+  }
+  for (int k = 0; k < s->NZ; k++)
+    for (int j = 0; j < s->NY; j++)
+      for (int i = 0; i < s->NX; i++) TS[cidx(s, i, j, k)] = HI(i + B, j + B, k + B);
+#undef HI
+}
+
+static void deposit(const ch4o_state *s, double *D, double *TS) {
   memset(D, 0, sizeof(double) * 3 * s->N);
+  /* the temperature deposit lands on the halo-padded field of the reference, folded at the end */
+  const int B = brd_of(&s->cfg);
+  const int PX = s->NX + 2 * B, PY = s->NY + 2 * B, PZ = s->NZ + 2 * B;
+  double *H = TS ? (double *)calloc((size_t)PX * PY * PZ, sizeof(double)) : NULL;
+#define HAT(i, j, k) H[((size_t)((k) + B) * PY + ((j) + B)) * PX + ((i) + B)]
   for (int ip = 0; ip < s->npart; ip++) {
     const ch4_particle *p = &s->part[ip];
     const double fac = s->pvol[ip], dr = s->pdr[ip];
@@ -776,6 +829,13 @@ static void deposit(const ch4o_state *s, double *D) {
     fp[0] = p->Dt_ux - gx + dr * (gx - p->ax);
     fp[1] = p->Dt_uy - gy + dr * (gy - p->ay);
     fp[2] = p->Dt_uz - gz + dr * (gz - p->az);
+    /* LAGRANGE_TWOWAY_TEMPERATURE, src/lagrange_feedback.c:181-230: the particle's heat
+     * exchange sp = Dt_t + (T_p - T) kappa / (nu beta tau_drag), times its volume */
+    double sp = 0.0;
+    if (TS) {
+      const double fac2 = s->cfg.kappa / (s->cfg.nu * p->beta_coeff * p->tau_drag);
+      sp = p->Dt_t + (p->t_p - p->t) * fac2;
+    }
     if (s->cfg.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) { /* src/lagrange_feedback.c:51-60, 117-146 */
       double wx[4], wy[4], wz[4];
       for (int n = -1; n <= 2; n++) {
@@ -787,8 +847,9 @@ static void deposit(const ch4o_state *s, double *D) {
         for (int b = 0; b < 4; b++)
           for (int c = 0; c < 4; c++) {
             int i = t.im + (a - 1), j = t.jm + (b - 1), k = t.km + (c - 1);
-            if (i < 0 || i >= s->NX || j < 0 || j >= s->NY || k < 0 || k >= s->NZ) continue;
             double w = wx[a] * wy[b] * wz[c];
+            if (TS) HAT(i, j, k) += fac * sp * w;
+            if (i < 0 || i >= s->NX || j < 0 || j >= s->NY || k < 0 || k >= s->NZ) continue;
             for (int q = 0; q < 3; q++) D[3 * cidx(s, i, j, k) + q] += fac * fp[q] * w;
           }
       continue;
@@ -799,6 +860,16 @@ static void deposit(const ch4o_state *s, double *D) {
         if (i < 0 || i >= s->NX || j < 0 || j >= s->NY || k < 0 || k >= s->NZ) continue;
         D[3 * cidx(s, i, j, k) + a] += fac * fp[a] * t.vol[c];
       }
+    if (TS)
+      for (int c = 0; c < 8; c++) {
+        int i = t.im + CORNER[c][0], j = t.jm + CORNER[c][1], k = t.km + CORNER[c][2];
+        HAT(i, j, k) += fac * sp * t.vol[c];
+      }
+  }
+#undef HAT
+  if (TS) {
+    fold_scalar(s, H, B, TS);
+    free(H);
   }
 }
 
@@ -915,10 +986,12 @@ static void one_step(ch4o_state *s) {
     double *tmp = s->dprev;
     s->dprev = s->dcur;
     s->dcur = tmp;
-    if (c->resume || s->itime > 1)
-      deposit(s, s->dcur);
-    else
+    if (c->resume || s->itime > 1) {
+      deposit(s, s->dcur, s->tsrc);
+    } else {
       memset(s->dcur, 0, sizeof(double) * 3 * N);
+      if (s->tsrc) memset(s->tsrc, 0, sizeof(double) * N);
+    }
   }
 
   /* global corrections of this step's build_forcing, with u^n of the previous one */
@@ -1028,6 +1101,9 @@ static void one_step(ch4o_state *s) {
               r += trt_coll(b, feqs[set], q, invtau_cell[set], trt_minus(invtau_cell[set]));
             else
               r += -invtau_cell[set] * (b[q] - feq);
+            /* add_forcing's temperature source w t_source (src/forcing.c:1475): with
+             * LAGRANGE_TWOWAY_TEMPERATURE the particles' deposit, else zero */
+            if (set == 1 && s->tsrc) r += s->w[q] * s->tsrc[idx];
             post[set][q] = r;
           }
         }
@@ -1187,6 +1263,7 @@ int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
   s->force = (double *)calloc(3 * s->N, sizeof(double));
   if (cfg->flags & CH4_F_LAGRANGE_TWOWAY) {
     s->dcur = (double *)calloc(3 * s->N, sizeof(double));
+    if (cfg->flags2 & CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE) s->tsrc = (double *)calloc(s->N, sizeof(double));
     s->dprev = (double *)calloc(3 * s->N, sizeof(double));
   }
   if (cfg->flags & CH4_F_LAGRANGE) s->uf = (double *)calloc(3 * s->N, sizeof(double));
@@ -1252,6 +1329,7 @@ int ch4o_destroy(ch4o_state *s) {
   free(s->pvol);
   free(s->pdr);
   free(s->dcur);
+  free(s->tsrc);
   free(s->dprev);
   free(s->uf);
   free(s->tf);

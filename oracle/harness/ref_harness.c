@@ -107,6 +107,9 @@ static void write_part_layout(void) {
 #ifdef LAGRANGE_GRADIENT
   F(dx_t); F(dy_t); F(dz_t);
 #endif
+#ifdef LAGRANGE_TEMPERATURE
+  F(t_p); F(cp_p);
+#endif
 #endif
 #ifdef LAGRANGE_ORIENTATION
   F(px); F(py); F(pz); F(dt_px); F(dt_py); F(dt_pz);

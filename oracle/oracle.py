@@ -106,6 +106,14 @@ FLAGSETS.update({
     "slipz": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Z", "LB_FLUID_BC_Z_P_SLIP", "LB_FLUID_BC_Z_M_SLIP",
               "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Z", "LB_TEMPERATURE_BC_Z_M_NOFLUX",
               "LB_SCALAR", "LB_SCALAR_BC_Z"],
+    "particles_tt": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE",
+                     "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_FORCING", "LAGRANGE", "LAGRANGE_WRAP",
+                     "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TEMPERATURE", "LAGRANGE_TWOWAY",
+                     "LAGRANGE_TWOWAY_MOMENTUM", "LAGRANGE_TWOWAY_TEMPERATURE"],
+    "particles_ttc": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE",
+                      "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_FORCING", "LAGRANGE", "LAGRANGE_WRAP",
+                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TEMPERATURE", "LAGRANGE_TWOWAY",
+                      "LAGRANGE_TWOWAY_MOMENTUM", "LAGRANGE_TWOWAY_TEMPERATURE", "LAGRANGE_TWOWAY_TRICUBIC"],
 })
 # non-flag configuration implied by a flag set (define.h variants of one setting)
 FLAGSET_EXTRA = {"walls2": {"t0_kind": abi.T0_REF}}
@@ -168,6 +176,12 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
     if int(cfg.flags) & abi.FLAGS["LAGRANGE_ORIENTATION_JEFFREY"]:  # src/parameters.c, read by the reference
         keys += ["aspect_ratio_types", "aspect_ratio_min", "aspect_ratio_max"]
         vals.update({"aspect_ratio_types": 1, "aspect_ratio_min": 1.0, "aspect_ratio_max": 1.0})
+    if int(cfg.flags) & abi.FLAGS["LB_TEMPERATURE_FORCING"]:  # src/parameters.c: the source amplitude
+        keys += ["Amp_t"]
+        vals.update({"Amp_t": 0.0})
+    if int(cfg.flags2) & abi.FLAGS2["LAGRANGE_TEMPERATURE"]:  # src/parameters.c:606-618
+        keys += ["cp_coeff_types", "cp_coeff_min", "cp_coeff_max"]
+        vals.update({"cp_coeff_types": 1, "cp_coeff_min": 1.0, "cp_coeff_max": 1.0})
     vals.update(overrides or {})
     with open(path, "w") as f:
         for k in keys:

@@ -28,6 +28,8 @@ for name in sys.argv[1:] or sorted(CASES):
     out = {"seed": SEED, "nsteps": NSTEPS}
     if "part" in ref:
         temperature = ("t", "dt_t", "Dt_t", "dx_t") if "t" in ref["part"] else ()
+        if "t_p" in ref["part"]:
+            temperature += ("t_p",)
         for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux") + temperature:
             out["out_part_" + f] = ref["part"][f]
     for k, v in pop_items(state):

@@ -79,6 +79,15 @@ CASES = {
                         params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=5,
                                     T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
                                     time_dt_lagr_factor=2.0, particle_number=250)),
+    # particles with their own temperature, coupled back through momentum and heat
+    "particles_tt": dict(flagset="particles_tt", NX=9, NY=8, NZ=7, npart=250,
+                         params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=12,
+                                     T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
+                                     time_dt_lagr_factor=2.0, particle_number=250)),
+    "particles_ttc": dict(flagset="particles_ttc", NX=9, NY=8, NZ=7, npart=250,
+                          params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=13,
+                                      T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
+                                      time_dt_lagr_factor=2.0, particle_number=250)),
     # walls on x and z
     "duct": dict(flagset="duct", NX=7, NY=8, NZ=6,
                  params=dict(tau_u=0.6, Amp_x=4e-3, Amp_y=1e-3, Amp_z=2e-3)),
@@ -133,6 +142,15 @@ def make_case(name, seed=0, storage=0, dims=None, **over):
         state["h"] = pops(rng, c["NX"], c["NY"], c["NZ"], 0.3, 1e-1)
     if "LAGRANGE" in flags:
         state["part"] = make_particles(rng, c["npart"], c["NX"], c["NY"], c["NZ"])
+        if "LAGRANGE_TEMPERATURE" in flags:
+            # inertial particles only (the thermal relaxation and exchange rates divide by
+            # tau_drag and beta), specific heats 0.5 .. 2, temperatures about the fluid's
+            cps = [0.5, 1.0, 2.0]
+            for i, p in enumerate(state["part"]):
+                p.tau_drag = [0.5, 2.0, 5.0][i % 3]
+                p.beta_coeff = [1.0, 2.0, 0.5][(i // 3) % 3]  # 3 - beta divides the heat rate
+                p.cp_p = cps[(i // 9) % 3]
+                p.t_p = 0.3 + 0.4 * rng.random()
         if "LAGRANGE_ORIENTATION" in flags:  # random unit orientations, rods and discs
             ratios = [1.0, 5.0, 0.2, 20.0]
             for i, p in enumerate(state["part"]):

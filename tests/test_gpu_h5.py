@@ -113,7 +113,7 @@ def test_read_pop_refuses_a_wrong_lattice(tmp_path):
             b.read_pop_h5(tmp_path / "pop.h5")
 
 
-def _fields(flags, output_fluid):
+def _fields(flags, output_fluid, flags2=0):
     """/lagrange dataset -> ch4_particle field, in output_particles' order."""
     f = [(n, n) for n in ("name", "tau_drag", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")]
     grad, am = flags & abi.FLAGS["LAGRANGE_GRADIENT"], flags & abi.FLAGS["LAGRANGE_ADDEDMASS"]
@@ -133,6 +133,8 @@ def _fields(flags, output_fluid):
         f += [("temperature", "t"), ("dt_t", "dt_t")]
         if grad:
             f += [("dx_t", "dx_t"), ("dy_t", "dy_t"), ("dz_t", "dz_t")]
+        if flags2 & abi.FLAGS2["LAGRANGE_TEMPERATURE"]:
+            f += [("temperature_particle", "t_p"), ("cp_particle", "cp_p")]
     return f
 
 
@@ -147,7 +149,7 @@ def _particle_sim(name, seed, nsteps):
     return cfg, state, sim
 
 
-@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or"])
+@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or", "particles_tt"])
 def test_particle_file_holds_the_particles(name, tmp_path):
     cfg, state, sim = _particle_sim(name, 65, 4)
     with sim:
@@ -155,7 +157,7 @@ def test_particle_file_holds_the_particles(name, tmp_path):
         sim.output_particles_h5(tmp_path, 4, time_now=4.0, output_fluid=True)
         parts = sim.get_particles(n)
     got = h5spec.read(tmp_path / "particle_4.h5")
-    want = _fields(cfg.flags, True)
+    want = _fields(cfg.flags, True, cfg.flags2)
     assert sorted(k for k in got) == sorted("/lagrange/" + d for d, _ in want)
     for d, field in want:
         assert np.array_equal(got["/lagrange/" + d], np.array([getattr(p, field) for p in parts])), d
@@ -165,7 +167,7 @@ def test_particle_file_holds_the_particles(name, tmp_path):
         assert "particle_4.h5:/lagrange/%s\n" % d in xmf, d
 
 
-@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or"])
+@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or", "particles_tt"])
 def test_part_file_restart(name, tmp_path):
     cfg, state, a = _particle_sim(name, 66, 5)
     n = len(state["part"])
@@ -181,14 +183,15 @@ def test_part_file_restart(name, tmp_path):
     assert members[:17] == ("name", "x", "y", "z", "vx", "vy", "vz", "vx_old", "vy_old", "vz_old", "ax", "ay",
                             "az", "ax_old", "ay_old", "az_old", "tau_drag")
     assert ("t" in members) == bool(cfg.flags & abi.FLAGS["LB_TEMPERATURE"])
+    field = {"temperature_particle": "t_p", "cp_particle": "cp_p"}  # member name -> ch4_particle field
     for m in members:
-        assert np.array_equal(rec[m], np.array([getattr(p, m) for p in parts])), m
+        assert np.array_equal(rec[m], np.array([getattr(p, field.get(m, m)) for p in parts])), m
     assert got["/properties@particle_types"].item() == float(cfg.particle_types)
     # the members part.h5 lacks start at 0, as in the reference's resume
     trimmed = (ch4b200.Particle * n)()
     for i, p in enumerate(parts):
         for m in members:
-            setattr(trimmed[i], m, getattr(p, m))
+            setattr(trimmed[i], field.get(m, m), getattr(p, field.get(m, m)))
     with ch4b200.Simulation(cfg) as b, ch4b200.Simulation(cfg) as c:
         b.read_pop_h5(tmp_path / "pop.h5")
         b.read_particles_h5(tmp_path / "part.h5")

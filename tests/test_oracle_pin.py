@@ -28,7 +28,7 @@ def _assert_same(a, b, what):
                                           ("trt", 20), ("trt_les", 20), ("les_vd", 20), ("les_ls", 20),
                                           ("les_wale", 20), ("les_ts", 20), ("particles_tc", 8), ("nozero", 15),
                                           ("cpower", 15), ("duct", 20), ("duct_les", 20), ("box", 20),
-                                          ("slipx", 20), ("slipz", 20)])
+                                          ("slipx", 20), ("slipz", 20), ("particles_tt", 8), ("particles_ttc", 8)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
@@ -81,7 +81,7 @@ def test_restatement_matches_golden_fixture(name):
     mine = run_restatement(cfg, state, int(g["nsteps"]))
     for k, _ in pop_items(state):
         _assert_same(mine[k], g["out_" + k], k)
-    for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux", "t", "dt_t", "Dt_t", "dx_t"):
+    for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux", "t", "dt_t", "Dt_t", "dx_t", "t_p"):
         if "out_part_" + f in g.files:
             _assert_same(mine["part"][f], g["out_part_" + f], "particle " + f)
     for k in ("u", "t", "s", "phi"):
