@@ -776,7 +776,7 @@ struct Engine : EngineBase {
     Q.tricubic = (c.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) != 0;
     Q.orient = (c.flags & CH4_F_LAGRANGE_ORIENTATION) != 0;
     Q.jeffery = (c.flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) != 0;
-    Q.nrec = Q.tricubic ? 15 : 9;
+    Q.nrec = nrec();
     Q.rec = rec;
     Q.srec = srec;
     Q.spid = spid;
