@@ -102,6 +102,18 @@ FLAGS2 = {
     "LB_SCALAR_BC_Z": 1 << 13,
     "LAGRANGE_TEMPERATURE": 1 << 14,
     "LAGRANGE_TWOWAY_TEMPERATURE": 1 << 15,
+    "LB_FLUID_BC": 1 << 16,
+    "LB_TEMPERATURE_BC": 1 << 17,
+    "LB_SCALAR_BC": 1 << 18,
+    "LAGRANGE_BC_INELASTIC": 1 << 19,
+    "LAGRANGE_BC_INELASTIC_REINJECT": 1 << 20,
+    "LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM": 1 << 21,
+    "LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO": 1 << 22,
+    "LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF": 1 << 23,
+    "LAGRANGE_SMALLTAUD": 1 << 24,
+    "LAGRANGE_SMALLTAUD_BETA": 1 << 25,
+    "LAGRANGE_SMALLTAUD_FLOATER": 1 << 26,
+    "LAGRANGE_TWOWAY_SMALLTAUD": 1 << 27,
 }
 
 

@@ -147,13 +147,11 @@ const uint64_t SUPPORTED2 =
     CH4_F2_FLUID_BC_Z_P_SLIP | CH4_F2_FLUID_BC_Z_M_SLIP | CH4_F2_TEMPERATURE_BC_X | CH4_F2_TEMPERATURE_BC_X_P_NOFLUX |
     CH4_F2_TEMPERATURE_BC_X_M_NOFLUX | CH4_F2_TEMPERATURE_BC_Z | CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX |
     CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX | CH4_F2_SCALAR_BC_X | CH4_F2_SCALAR_BC_Z | CH4_F2_LAGRANGE_TEMPERATURE |
-    CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE;
-// the walls of the second flag word
-const uint64_t WALLS2 = CH4_F2_FLUID_BC_X | CH4_F2_FLUID_BC_X_P_SLIP | CH4_F2_FLUID_BC_X_M_SLIP | CH4_F2_FLUID_BC_Z |
-                        CH4_F2_FLUID_BC_Z_P_SLIP | CH4_F2_FLUID_BC_Z_M_SLIP | CH4_F2_TEMPERATURE_BC_X |
-                        CH4_F2_TEMPERATURE_BC_X_P_NOFLUX | CH4_F2_TEMPERATURE_BC_X_M_NOFLUX | CH4_F2_TEMPERATURE_BC_Z |
-                        CH4_F2_TEMPERATURE_BC_Z_P_NOFLUX | CH4_F2_TEMPERATURE_BC_Z_M_NOFLUX | CH4_F2_SCALAR_BC_X |
-                        CH4_F2_SCALAR_BC_Z;
+    CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE | CH4_F2_FLUID_BC | CH4_F2_TEMPERATURE_BC | CH4_F2_SCALAR_BC |
+    CH4_F2_LAGRANGE_BC_INELASTIC | CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT |
+    CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM | CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO |
+    CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF | CH4_F2_LAGRANGE_SMALLTAUD |
+    CH4_F2_LAGRANGE_SMALLTAUD_BETA | CH4_F2_LAGRANGE_SMALLTAUD_FLOATER | CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -791,6 +789,31 @@ struct Engine : EngineBase {
     Q.twoway_temp = twoway_temp();
     Q.kappa = c.kappa;
     Q.nu = c.nu;
+    // halos of the particles' fields and the gradient mode (src/boundary_conditions.c:2786-2940,
+    // src/gradients.c:119-500, 526-827)
+    const uint64_t f2 = c.flags2;
+    Q.fw = fluid_walls(c);
+    Q.sw = value_walls(c);
+    Q.slip_lo = ((f2 & CH4_F2_FLUID_BC_X_M_SLIP) ? 1 : 0) | ((c.flags & CH4_F_FLUID_BC_Y_M_SLIP) ? 2 : 0) |
+                ((f2 & CH4_F2_FLUID_BC_Z_M_SLIP) ? 4 : 0);
+    Q.slip_hi = ((f2 & CH4_F2_FLUID_BC_X_P_SLIP) ? 1 : 0) | ((c.flags & CH4_F_FLUID_BC_Y_P_SLIP) ? 2 : 0) |
+                ((f2 & CH4_F2_FLUID_BC_Z_P_SLIP) ? 4 : 0);
+    Q.bc_u = ((f2 & CH4_F2_FLUID_BC) || Q.fw) ? 1 : 0;
+    Q.bc_t = ((f2 & (CH4_F2_TEMPERATURE_BC | CH4_F2_SCALAR_BC)) || Q.sw) ? 1 : 0;
+    Q.t_ywall = (nsets_on[1] && (c.flags & CH4_F_TEMPERATURE_BC_Y)) ? 1 : 0;
+    Q.T_bot = c.T_bot;
+    Q.T_top = c.T_top;
+    Q.T_ref = c.T_ref;
+    // particles at the walls and the small-tau_drag models (src/lagrange.c:3425-3466, 3754-3998)
+    Q.inelastic = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC) != 0;
+    Q.reinject = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) != 0;
+    Q.rj_vzero = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO) != 0;
+    Q.rj_half = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF) != 0;
+    const bool stau = (f2 & CH4_F2_LAGRANGE_SMALLTAUD) != 0;
+    Q.stau_beta = stau && (f2 & CH4_F2_LAGRANGE_SMALLTAUD_BETA);
+    Q.stau_floater = stau && (f2 & CH4_F2_LAGRANGE_SMALLTAUD_FLOATER);
+    Q.twoway_stau = (f2 & CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD) != 0;
+    Q.beta_t = c.beta_t;
     return Q;
   }
 
@@ -1664,8 +1687,12 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
+  // gravity_x/y/z (src/parameters.c:234-241, with LB_FLUID_FORCING_GRAVITY): read where
+  // buoyancy, the particles' gravity, their Stokes re-injection or a small-tau_drag model uses it
   const bool grav = (forcing && (fl & (CH4_F_TEMPERATURE_BUOYANCY | CH4_F_SCALAR_BUOYANCY))) ||
-                    (fl & CH4_F_LAGRANGE_GRAVITY);
+                    (fl & CH4_F_LAGRANGE_GRAVITY) ||
+                    ((fl & CH4_F_LAGRANGE) &&
+                     (cfg->flags2 & (CH4_F2_LAGRANGE_SMALLTAUD | CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT)));
   std::vector<K> keys = {
       {"resume", &resume, true}, {"NX", &NX, true}, {"NY", &NY, true}, {"NZ", &NZ, true}, {"SX", &cfg->SX, true}, {"SY", &cfg->SY, true},
       {"SZ", &cfg->SZ, true}, {"time_dt", &cfg->time_dt, true}, {"tau_u", &cfg->tau_u, true},
@@ -1820,12 +1847,23 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LB_SCALAR_BC_Z", CH4_F2_SCALAR_BC_Z},
       {"LAGRANGE_TEMPERATURE", CH4_F2_LAGRANGE_TEMPERATURE},
       {"LAGRANGE_TWOWAY_TEMPERATURE", CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE},
+      {"LB_FLUID_BC", CH4_F2_FLUID_BC},
+      {"LB_TEMPERATURE_BC", CH4_F2_TEMPERATURE_BC},
+      {"LB_SCALAR_BC", CH4_F2_SCALAR_BC},
+      {"LAGRANGE_BC_INELASTIC", CH4_F2_LAGRANGE_BC_INELASTIC},
+      {"LAGRANGE_BC_INELASTIC_REINJECT", CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT},
+      {"LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM", CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM},
+      {"LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO", CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO},
+      {"LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF", CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF},
+      {"LAGRANGE_SMALLTAUD", CH4_F2_LAGRANGE_SMALLTAUD},
+      {"LAGRANGE_SMALLTAUD_BETA", CH4_F2_LAGRANGE_SMALLTAUD_BETA},
+      {"LAGRANGE_SMALLTAUD_FLOATER", CH4_F2_LAGRANGE_SMALLTAUD_FLOATER},
+      {"LAGRANGE_TWOWAY_SMALLTAUD", CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
   static const char* neutral[] = {"LB", "GRID_REGULAR", "GRID_POP_D3Q19", "METHOD_STREAMING", "METHOD_EDGES_AND_CORNERS",
-                                  "METHOD_FORCING_GUO", "LB_FLUID_FORCING_GRAVITY", "LB_FLUID_BC", "LB_TEMPERATURE_BC",
-                                  "LB_SCALAR_BC", "SYSTEM_RANDOM48", "SYSTEM_TIMING", "TIMING", "NEW_SENDRECV",
+                                  "METHOD_FORCING_GUO", "LB_FLUID_FORCING_GRAVITY", "SYSTEM_RANDOM48", "SYSTEM_TIMING", "TIMING", "NEW_SENDRECV",
                                   "OUTPUT_H5", "OUTPUT_H5_GRID", "OUTPUT_H5_TIMESTAMP_REAL", "OUTPUT_AT_START",
                                   "OUTPUT_ASCII", "VERBOSE", "LB_TEMPERATURE_BUOYANCY_T0_REF",
                                   "LB_TEMPERATURE_BUOYANCY_T0_TOP", "LB_TEMPERATURE_BUOYANCY_T0_BOT", "LB_FLUID_LES_OUTPUT"};
@@ -1944,9 +1982,21 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
              CH4_ERR_UNSUPPORTED;
   }
   if (c->flags & CH4_F_LAGRANGE) {
-    if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_LB_SCALAR)) || (c->flags2 & WALLS2))
-      return why = "particles are implemented for the periodic box (fluid, optionally temperature)",
-             CH4_ERR_UNSUPPORTED;
+    if (c->flags & CH4_F_LB_SCALAR)
+      return why = "particles are implemented with the fluid and optionally the temperature", CH4_ERR_UNSUPPORTED;
+    const uint64_t f2 = c->flags2;
+    // random re-injection draws from the reference's single drand48 stream
+    if ((f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) && !(f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM))
+      return why = "LAGRANGE_BC_INELASTIC_REINJECT is implemented with _NORANDOM", CH4_ERR_UNSUPPORTED;
+    // the small-tau_drag velocity reads Du/Dt, which only the added-mass term computes
+    // (elsewhere the reference reads an unset local, src/lagrange.c:2941, 3433)
+    if ((f2 & CH4_F2_LAGRANGE_SMALLTAUD) && (f2 & CH4_F2_LAGRANGE_SMALLTAUD_BETA) &&
+        (c->flags & (CH4_F_LAGRANGE_ADDEDMASS | CH4_F_LAGRANGE_GRADIENT)) !=
+            (CH4_F_LAGRANGE_ADDEDMASS | CH4_F_LAGRANGE_GRADIENT))
+      return why = "LAGRANGE_SMALLTAUD_BETA needs LAGRANGE_ADDEDMASS and LAGRANGE_GRADIENT", CH4_ERR_UNSUPPORTED;
+    if ((f2 & CH4_F2_LAGRANGE_SMALLTAUD) && (f2 & CH4_F2_LAGRANGE_SMALLTAUD_FLOATER) &&
+        !(c->flags & CH4_F_LB_TEMPERATURE))
+      return why = "LAGRANGE_SMALLTAUD_FLOATER needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
     if ((c->flags2 & CH4_F2_LAGRANGE_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
       return why = "LAGRANGE_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
     // the heat exchange reads the particle temperature (src/typedef.h:467-470) and enters the

@@ -22,6 +22,7 @@
 // each home-cell list stays in particle-index order whatever the slot order, and
 // every per-cell sum keeps the reference's order.
 #pragma once
+#include <cfloat>
 #include <cstddef>
 
 #include "../../include/ch4.h"
@@ -82,6 +83,18 @@ struct PartParams {
   int lagr_temp;         // LAGRANGE_TEMPERATURE: the particle temperature relaxes towards the fluid's
   int twoway_temp;       // LAGRANGE_TWOWAY_TEMPERATURE: record field nrec-1 holds fac * sp, dep a 4th plane
   double kappa, nu;
+  // halos of the fields the particles see (boundary_conditions_hydro) and the gradient
+  // mode (masks: bit a = axis a)
+  int fw;                 // fluid walls
+  int slip_lo, slip_hi;   // slip fluid walls at the lower / upper end
+  int sw;                 // temperature or scalar walls (wall rows of the t gradient)
+  int bc_u, bc_t;         // wall-mode gradients: LB_FLUID_BC / LB_TEMPERATURE_BC or LB_SCALAR_BC
+  int t_ywall;            // t extrapolated beyond the y temperature walls
+  double T_bot, T_top, T_ref;
+  // particles at the fluid walls and the small-tau_drag models
+  int inelastic, reinject, rj_vzero, rj_half;
+  int stau_beta, stau_floater, twoway_stau;
+  double beta_t;
 };
 
 #ifdef __CUDACC__
@@ -140,120 +153,388 @@ __device__ __forceinline__ void corner(int c, int& di, int& dj, int& dk) {
   dk = (c == 3 || c == 5 || c == 6 || c == 7);
 }
 
-// Wrapped offsets of the 4x4x4 neighbourhood (lower stencil corner - 1 ... + 2 on
-// each axis) that the trilinear value and gradient of a particle read.
-struct PNbr {
-  long long zo[4];
-  int yo[4], xo[4];
-};
-
-// periodic index for i in [-2, n + 1] (the neighbourhood of a stencil): one wrap
-// suffices for n >= 2; a lattice one cell wide maps everything to 0
+// periodic index for i in [-2, n + 1] (the reach of a stencil and its gradients): one
+// wrap suffices for n >= 2; a lattice one cell wide maps everything to 0
 __device__ __forceinline__ int pmod(int i, int n) {
   if (n == 1) return 0;
   return i < 0 ? i + n : (i >= n ? i - n : i);
 }
 
-// Trilinear value (and with GRAD the gradient) of one lattice field at a particle from
-// its neighbourhood block b[z][y][x] (lower stencil corner at block index 1 on each
-// axis), `lo`/`hi` flagging a stencil whose lower corner is the halo layer -1 / whose
-// upper corner is the halo layer n on each axis.  Per corner the gradient is centred,
-// (u(c+1) - u(c-1)) / 2, or one-sided of second order on those halo layers
-// (LAGRANGE_INTERPOLATION_FIX, src/gradients.c:358-420 for vectors, 731-800 for
-// scalars); the eight corners are summed in the reference's order with the weights of
-// make_stencil (src/lagrange.c:1266-1439).  Only the 8 corners and, with GRAD, their 24
-// face neighbours are read.
-template <bool GRAD, typename A>
-__device__ __forceinline__ void interp_block(const A (&b)[4][4][4], const double* vol, const bool* lo, const bool* hi,
-                                             double& val, double* grad) {
-  double acc = 0.0;
+// the four values (u_x, u_y, u_z, t) of cell c of ut4: FP32 as one 16-byte load, FP64 as two
+__device__ __forceinline__ void load_cell(const float* __restrict__ ut4, long long c, double* v) {
+  const float4 q = __ldg(reinterpret_cast<const float4*>(ut4) + c);
+  v[0] = q.x;
+  v[1] = q.y;
+  v[2] = q.z;
+  v[3] = q.w;
+}
+__device__ __forceinline__ void load_cell(const double* __restrict__ ut4, long long c, double* v) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(ut4) + 2 * c);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(ut4) + 2 * c + 1);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = b.x;
+  v[3] = b.y;
+}
+
+// The fields the particles see at stencil cell (i, j, k), every coordinate in [-2, n + 1]
+// (boundary_conditions_hydro, src/boundary_conditions.c:2786-2940).  Every halo cell is
+// the periodic image, except on the first layer beyond a wall: beyond a fluid wall u is
+// the u of the cell next to the wall mirrored (all components, or only the normal one
+// on a slip wall), the axes taken x, y, z, so that an edge cell carries both mirrors;
+// beyond a temperature wall on y, t is (2 (T_wall - T_ref) / t0 - 1) t0 of the row next
+// to the wall.  With HALO false the lattice is periodic on every axis.
+template <bool HALO, int NF, typename A>
+__device__ __forceinline__ void cell_fields(const PartParams<A>& P, int i, int j, int k, double* v) {
+  int ui = pmod(i, P.NX), uj = pmod(j, P.NY), uk = pmod(k, P.NZ);
+  if constexpr (!HALO) {
+    double w[4];
+    load_cell(P.ut4, ((long long)uk * P.NY + uj) * P.NX + ui, w);
 #pragma unroll
-  for (int c = 0; c < 8; c++) {
-    int di, dj, dk;
-    corner(c, di, dj, dk);
-    const double term = (double)b[1 + dk][1 + dj][1 + di] * vol[c];
-    acc = c == 0 ? term : acc + term;
-  }
-  val = acc;
-  if constexpr (GRAD) {
+    for (int a = 0; a < NF; a++) v[a] = w[a];
+  } else {
+    const int tj = uj;  // t: periodic on x and z, and on y without temperature walls
+    const bool tw = P.t_ywall && (j == -1 || j == P.NY);
+    int flip = 0;       // bit a: u_a changes sign
+    if (P.fw & 1) {
+      if (i == -1) ui = 0, flip ^= (P.slip_lo & 1) ? 1 : 7;
+      else if (i == P.NX) ui = P.NX - 1, flip ^= (P.slip_hi & 1) ? 1 : 7;
+    }
+    if (P.fw & 2) {
+      if (j == -1) uj = 0, flip ^= (P.slip_lo & 2) ? 2 : 7;
+      else if (j == P.NY) uj = P.NY - 1, flip ^= (P.slip_hi & 2) ? 2 : 7;
+    }
+    if (P.fw & 4) {
+      if (k == -1) uk = 0, flip ^= (P.slip_lo & 4) ? 4 : 7;
+      else if (k == P.NZ) uk = P.NZ - 1, flip ^= (P.slip_hi & 4) ? 4 : 7;
+    }
+    double w[4];
+    const long long cu = ((long long)uk * P.NY + uj) * P.NX + ui;
+    load_cell(P.ut4, cu, w);
 #pragma unroll
-    for (int ax = 0; ax < 3; ax++) {
-      double g = 0.0;
-#pragma unroll
-      for (int c = 0; c < 8; c++) {
-        int di, dj, dk;
-        corner(c, di, dj, dk);
-        const int x = 1 + di, y = 1 + dj, z = 1 + dk;
-        const int d = ax == 0 ? di : ax == 1 ? dj : dk;  // 0: lower corner, 1: upper corner
-        // value at offset s along ax from the corner (indices clamped so that every
-        // unrolled form is in range; the branches below use only in-range offsets)
-        auto at = [&](int s) -> double {
-          const int xx = ax == 0 ? min(max(x + s, 0), 3) : x;
-          const int yy = ax == 1 ? min(max(y + s, 0), 3) : y;
-          const int zz = ax == 2 ? min(max(z + s, 0), 3) : z;
-          return (double)b[zz][yy][xx];
-        };
-        double gc;
-        if (d == 0 && lo[ax])
-          gc = -1.5 * at(0) + 2.0 * at(1) + -0.5 * at(2);
-        else if (d == 1 && hi[ax])
-          gc = 1.5 * at(0) + -2.0 * at(-1) + 0.5 * at(-2);
-        else
-          gc = (at(1) - at(-1)) / 2.0;
-        const double term = gc * vol[c];
-        g = c == 0 ? term : g + term;
+    for (int a = 0; a < 3; a++) v[a] = (flip >> a) & 1 ? -w[a] : w[a];
+    if constexpr (NF == 4) {
+      const int ty = tw ? (j == -1 ? 0 : P.NY - 1) : tj;
+      const long long ct = ((long long)pmod(k, P.NZ) * P.NY + ty) * P.NX + pmod(i, P.NX);
+      double t0 = w[3];
+      if (ct != cu) t0 = (double)P.ut4[4 * ct + 3];
+      if (tw) {
+        const double T_wall = j == -1 ? P.T_bot : P.T_top;
+        const double fac = 2.0 * (T_wall - P.T_ref) / t0 - 1.0;
+        t0 = fac * t0;
       }
-      grad[ax] = g;
+      v[3] = t0;
     }
   }
 }
 
-// block entries an interpolation reads: the 8 corners, and with GRAD their face neighbours
-template <bool GRAD>
-__device__ __forceinline__ constexpr bool block_used(int x, int y, int z) {
-  const int inner = (x == 1 || x == 2) + (y == 1 || y == 2) + (z == 1 || z == 2);
-  return inner == 3 || (GRAD && inner == 2);
+// d/dx_b (b = 0, 1, 2) of the fields [F0, F1) at stencil cell c: gradient_vector /
+// gradient_scalar with LAGRANGE (src/gradients.c:78-500, 505-835), second order, in the
+// reference's statement order:
+//  - centred, (f(c + e_b) - f(c - e_b)) / 2, on the interior rows;
+//  - in wall mode (`bc`: the umbrella LB_FLUID_BC for u, LB_TEMPERATURE_BC /
+//    LB_SCALAR_BC for t) on the first and last row of an axis in `walls`: one-sided,
+//    -1.5 f(c) + 2 f(c + e) - 0.5 f(c + 2e) (and mirrored);
+//  - on a halo layer (LAGRANGE_INTERPOLATION_FIX): in wall mode the one-sided difference
+//    of the interior cell next to it, that cell then standing in for the halo one in the
+//    later axes' differences as well; otherwise the one-sided difference of the halo
+//    cell itself;
+//  - zero along an axis one cell wide.
+template <bool HALO, int NF, int F0, int F1, typename A>
+__device__ __forceinline__ void cell_grad(const PartParams<A>& P, const int* c, bool bc, int walls, double (*g)[3]) {
+  const int n[3] = {P.NX, P.NY, P.NZ};
+  const bool wm = HALO && bc;  // wall mode
+  int s[3] = {c[0], c[1], c[2]};
+  // every sample position is chosen first (selects, no branches), then all of them are read
+  int q[3][3][3];  // [axis][sample][coordinate]
+  int kind[3];     // 0 centred, +1 forward, -1 backward one-sided
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    const bool lo = c[b] == -1, hi = c[b] == n[b];
+    const bool wall = wm && ((walls >> b) & 1);
+    kind[b] = (lo || (wall && c[b] == 0)) ? 1 : (hi || (wall && c[b] == n[b] - 1)) ? -1 : 0;
+    if (wm && lo) s[b] = 0;
+    if (wm && hi) s[b] = n[b] - 1;
+    const bool shifted = wm && (lo || hi);
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+      const int base = shifted ? s[e] : c[e];
+      q[b][0][e] = q[b][1][e] = q[b][2][e] = base;
+    }
+    const int pb = shifted ? s[b] : c[b];
+    q[b][0][b] = kind[b] == 0 ? c[b] - 1 : pb;
+    q[b][1][b] = kind[b] == 0 ? c[b] + 1 : pb + kind[b];
+    q[b][2][b] = pb + 2 * kind[b];
+  }
+  double v[3][3][NF];
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    cell_fields<HALO, NF>(P, q[b][0][0], q[b][0][1], q[b][0][2], v[b][0]);
+    cell_fields<HALO, NF>(P, q[b][1][0], q[b][1][1], q[b][1][2], v[b][1]);
+    if (kind[b] != 0) {
+      cell_fields<HALO, NF>(P, q[b][2][0], q[b][2][1], q[b][2][2], v[b][2]);
+    } else {
+#pragma unroll
+      for (int a = 0; a < NF; a++) v[b][2][a] = 0.0;
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 3; b++)
+#pragma unroll
+    for (int a = F0; a < F1; a++) {
+      const double v0 = v[b][0][a], v1 = v[b][1][a], v2 = v[b][2][a];
+      double r = kind[b] > 0 ? -1.5 * v0 + 2.0 * v1 + -0.5 * v2 : 1.5 * v0 + -2.0 * v1 + 0.5 * v2;
+      if (kind[b] == 0) r = (v1 - v0) / 2.0;
+      g[a][b] = n[b] == 1 ? 0.0 : r;
+    }
 }
 
-// Value (and gradient) of the fields of ut4 at a particle: FP32 cells are read as one
-// 16-byte vector (u_x, u_y, u_z, t); FP64 cells field by field.
-template <bool GRAD>
-__device__ __forceinline__ void interp_cells(const float* __restrict__ ut4, int nf, const PNbr& o, const double* vol,
-                                             const bool* lo, const bool* hi, double* val, double* grad) {
-  float b[4][4][4][4];  // [field][z][y][x]
+// Trilinear value (and with GRAD the gradient) of (u_x, u_y, u_z[, t]) at a particle,
+// streamed corner by corner: the 8 stencil cells in the reference's order with the
+// weights of make_stencil (src/lagrange.c:1266-1439, 1442-1593), each corner's values
+// and gradients read from the cache and folded into the sums at once.
+template <bool HALO, int NF, bool GRAD, typename A>
+__device__ __forceinline__ void interp_fields(const PartParams<A>& P, const Stencil& t, double* val, double (*gra)[3]) {
+  const bool same = !HALO || (P.bc_u == P.bc_t && P.fw == P.sw);
+  // two corners in flight where the registers allow it (the periodic three-field form)
+  constexpr int UNR = (!HALO && NF == 3) ? 2 : 1;
+#pragma unroll UNR
+  for (int cc = 0; cc < 8; cc++) {
+    int di, dj, dk;
+    corner(cc, di, dj, dk);
+    const int c[3] = {t.im + di, t.jm + dj, t.km + dk};
+    const double w = ((di ? t.dxm : t.dxp) * (dj ? t.dym : t.dyp)) * (dk ? t.dzm : t.dzp);
+    double v[NF];
+    cell_fields<HALO, NF>(P, c[0], c[1], c[2], v);
 #pragma unroll
-  for (int z = 0; z < 4; z++)
+    for (int a = 0; a < NF; a++) {
+      const double term = v[a] * w;
+      val[a] = cc == 0 ? term : val[a] + term;
+    }
+    if constexpr (GRAD) {
+      double g[NF][3];
+      if (same) {
+        cell_grad<HALO, NF, 0, NF>(P, c, P.bc_u != 0, P.fw, g);
+      } else {
+        cell_grad<HALO, NF, 0, 3>(P, c, P.bc_u != 0, P.fw, g);
+        if constexpr (NF == 4) cell_grad<HALO, NF, 3, 4>(P, c, P.bc_t != 0, P.sw, g);
+      }
 #pragma unroll
-    for (int y = 0; y < 4; y++)
+      for (int a = 0; a < NF; a++)
 #pragma unroll
-      for (int x = 0; x < 4; x++)
-        if (block_used<GRAD>(x, y, z)) {
-          const float4 v = reinterpret_cast<const float4*>(ut4)[o.zo[z] + o.yo[y] + o.xo[x]];
-          b[0][z][y][x] = v.x;
-          b[1][z][y][x] = v.y;
-          b[2][z][y][x] = v.z;
-          b[3][z][y][x] = v.w;
+        for (int b = 0; b < 3; b++) {
+          const double term = g[a][b] * w;
+          gra[a][b] = cc == 0 ? term : gra[a][b] + term;
         }
-#pragma unroll
-  for (int a = 0; a < 4; a++)
-    if (a < nf) interp_block<GRAD>(b[a], vol, lo, hi, val[a], grad + 3 * a);
+    }
+  }
 }
 
-template <bool GRAD>
-__device__ __forceinline__ void interp_cells(const double* __restrict__ ut4, int nf, const PNbr& o, const double* vol,
-                                             const bool* lo, const bool* hi, double* val, double* grad) {
+// The periodic form (no wall, no wall mode): every value a particle reads lies in the
+// 4x4x4 block from its stencil's lower corner - 1 to + 2, and each derivative is a
+// difference along one line of four cells of that block.  The lines are read in three
+// passes (along x, y, z; four lines of four independent loads each) and every corner's
+// value and derivatives are folded into the sums in the reference's corner order as soon
+// as the corners before it are in (a line hands out its two corners out of that order).
+// Per line (cells L0..L3, corners at L1 and L2): centred (L2 - L0) / 2 and (L3 - L1) / 2,
+// or, when a corner is the halo layer -1 / n, the one-sided -1.5 L1 + 2 L2 - 0.5 L3 /
+// 1.5 L2 - 2 L1 + 0.5 L0 (LAGRANGE_INTERPOLATION_FIX, src/gradients.c:370-489, 728-826).
+// Arithmetic in the storage precision: FP64 reproduces the reference bit for bit; the
+// FP32 path interpolates in FP32, as its lattice arithmetic.
+struct PBlock {
+  long long zo[4];
+  int yo[4], xo[4];
+};
+
+// corner index of the reference's order for corner (di, dj, dk)
+__host__ __device__ constexpr int corner_id(int di, int dj, int dk) {
+  return dk == 0 ? (dj == 0 ? di : (di == 0 ? 2 : 4)) : (dj == 0 ? (di == 0 ? 3 : 6) : (di == 0 ? 5 : 7));
+}
+// after line l of the pass along `axis`, every corner below this id is in
+__host__ __device__ constexpr int corners_done(int axis, int l) {
+  return axis == 0 ? (l == 0 ? 2 : l == 1 ? 3 : l == 2 ? 5 : 8)
+         : axis == 1 ? (l == 0 ? 1 : l == 1 ? 3 : l == 2 ? 6 : 8)
+                     : (l == 0 ? 1 : l == 1 ? 2 : l == 2 ? 4 : 8);
+}
+
+template <int NF, typename C>
+__device__ __forceinline__ void load_line(const C* __restrict__ ut4, const PBlock& o, int axis, int a, int b,
+                                          C (*L)[NF]) {
 #pragma unroll
-  for (int a = 0; a < 4; a++) {
-    if (a >= nf) break;
-    double b[4][4][4];
+  for (int q = 0; q < 4; q++) {
+    const long long c = axis == 0 ? o.zo[b] + o.yo[a] + o.xo[q]
+                        : axis == 1 ? o.zo[b] + o.yo[q] + o.xo[a]
+                                    : o.zo[q] + o.yo[b] + o.xo[a];
+    double w[4];
+    load_cell(ut4, c, w);
 #pragma unroll
-    for (int z = 0; z < 4; z++)
+    for (int f = 0; f < NF; f++) L[q][f] = (C)w[f];
+  }
+}
+
+// hint that a cache line is about to be read (no register, no fault on a valid address)
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.L2 [%0];" ::"l"(p)); }
+
+template <int NF, bool GRAD, typename C>
+__device__ __forceinline__ void interp_lines(const PartParams<C>& P, const Stencil& t, double* val, double (*gra)[3]) {
+  PBlock o;
 #pragma unroll
-      for (int y = 0; y < 4; y++)
+  for (int q = 0; q < 4; q++) {
+    o.xo[q] = pmod(t.im - 1 + q, P.NX);
+    o.yo[q] = pmod(t.jm - 1 + q, P.NY) * P.NX;
+    o.zo[q] = (long long)pmod(t.km - 1 + q, P.NZ) * P.NX * P.NY;
+  }
+  if constexpr (GRAD) {  // the cells only the y and z passes read: on their way while x runs
 #pragma unroll
-        for (int x = 0; x < 4; x++)
-          if (block_used<GRAD>(x, y, z)) b[z][y][x] = ut4[4 * (o.zo[z] + o.yo[y] + o.xo[x]) + a];
-    interp_block<GRAD>(b, vol, lo, hi, val[a], grad + 3 * a);
+    for (int a = 1; a < 3; a++)
+#pragma unroll
+      for (int b = 1; b < 3; b++)
+#pragma unroll
+        for (int q = 0; q < 4; q += 3) {
+          prefetch_l2(P.ut4 + 4 * (o.zo[b] + o.yo[q] + o.xo[a]));
+          prefetch_l2(P.ut4 + 4 * (o.zo[q] + o.yo[b] + o.xo[a]));
+        }
+  }
+  const bool lo[3] = {t.im == -1, t.jm == -1, t.km == -1};
+  const bool hi[3] = {t.im + 1 == P.NX, t.jm + 1 == P.NY, t.km + 1 == P.NZ};
+  const bool one[3] = {P.NX == 1, P.NY == 1, P.NZ == 1};
+  C w[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    int di, dj, dk;
+    corner(c, di, dj, dk);
+    w[c] = (C)(((di ? t.dxm : t.dxp) * (dj ? t.dym : t.dyp)) * (dk ? t.dzm : t.dzp));
+  }
+  C acc[NF], g[3][NF];
+#pragma unroll
+  for (int axis = 0; axis < (GRAD ? 3 : 1); axis++) {
+    C cv[8][NF], cg[8][NF];  // per corner (compile-time indices only: registers)
+#pragma unroll
+    for (int line = 0; line < 4; line++) {
+      const int a = 1 + (line & 1), b = 1 + (line >> 1);  // block coordinates on the other two axes
+      C L[4][NF];
+      load_line<NF>(P.ut4, o, axis, a, b, L);
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        const int di = axis == 0 ? k : a - 1;
+        const int dj = axis == 1 ? k : (axis == 0 ? a - 1 : b - 1);
+        const int dk = axis == 2 ? k : b - 1;
+        const int id = corner_id(di, dj, dk);
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+          cv[id][f] = L[1 + k][f];
+          C d;
+          if (k == 0)
+            d = lo[axis] ? (C)-1.5 * L[1][f] + (C)2.0 * L[2][f] + (C)-0.5 * L[3][f] : (L[2][f] - L[0][f]) / (C)2.0;
+          else
+            d = hi[axis] ? (C)1.5 * L[2][f] + (C)-2.0 * L[1][f] + (C)0.5 * L[0][f] : (L[3][f] - L[1][f]) / (C)2.0;
+          cg[id][f] = one[axis] ? (C)0 : d;
+        }
+      }
+#pragma unroll
+      for (int id = (line == 0 ? 0 : corners_done(axis, line - 1)); id < corners_done(axis, line); id++)
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+          if (axis == 0) {
+            const C term = cv[id][f] * w[id];
+            acc[f] = id == 0 ? term : acc[f] + term;
+          }
+          const C gt = cg[id][f] * w[id];
+          g[axis][f] = id == 0 ? gt : g[axis][f] + gt;
+        }
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < NF; f++) {
+    val[f] = (double)acc[f];
+    if constexpr (GRAD) {
+#pragma unroll
+      for (int b = 0; b < 3; b++) gra[f][b] = (double)g[b][f];
+    }
+  }
+}
+
+// The walls of move_particles (src/lagrange.c:3754-3998), zero radius, y then x then z,
+// each test on the position the previous ones left.  Elastic (fac1 = -1, fac2 = 1): the
+// position is mirrored at the wall and an outward normal velocity reversed;
+// LAGRANGE_BC_INELASTIC (fac1 = fac2 = 0): the position is put on the wall (x, z: the
+// upper one at S (1 - FLT_EPSILON)) and the tangential and an outward normal velocity
+// zeroed; LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM: a particle that crossed a y wall
+// re-enters through the other one (y + SY, y - (SY - FLT_EPSILON)) with zero or the
+// Stokes settling velocity, halved (VELOCITY_STOKES_HALF) at the bottom wall only, and
+// the temperature of the wall it re-enters through.
+template <typename A>
+__device__ __forceinline__ void particle_walls(const PartParams<A>& P, double tau, double beta, double& x, double& y,
+                                               double& z, double& vx, double& vy, double& vz, double& tp) {
+  const double fac1 = P.inelastic ? 0.0 : -1.0, fac2 = P.inelastic ? 0.0 : 1.0;
+  const double radius = 0.0, eps = (double)FLT_EPSILON;
+  if (P.fw & 2) {
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      if (!(side == 0 ? y < radius : y >= P.SY - radius)) continue;
+      if (!P.reinject) {
+        if (side == 0) {
+          y = fac1 * (y - radius) + radius;
+          vx *= fac2;
+          if (vy < 0.0) vy *= fac1;
+          vz *= fac2;
+        } else {
+          y = fac1 * (y - (P.SY - radius)) + (P.SY - radius);
+          vx *= fac2;
+          if (vy > 0.0) vy *= fac1;
+          vz *= fac2;
+        }
+      }
+      if (P.inelastic && P.reinject) {
+        if (side == 0)
+          y += P.SY;
+        else
+          y -= (P.SY - eps);
+        if (P.rj_vzero) {
+          vx = 0.0;
+          vy = 0.0;
+          vz = 0.0;
+        } else {
+          vx = -P.g[0] * (1.0 - beta) * tau;
+          vy = -P.g[1] * (1.0 - beta) * tau;
+          vz = -P.g[2] * (1.0 - beta) * tau;
+        }
+        if (side == 0 && P.rj_half) {
+          vx /= 2.0;
+          vy /= 2.0;
+          vz /= 2.0;
+        }
+        if (P.lagr_temp) tp = side == 0 ? P.T_top : P.T_bot;
+      }
+    }
+  }
+  if (P.fw & 1) {
+    if (x < radius) {
+      x *= fac1;
+      if (vx < 0.0) vx *= fac1;
+      vy *= fac2;
+      vz *= fac2;
+    }
+    if (x >= P.SX - radius) {
+      x = P.SX - fac2 * (x - P.SX) - (1.0 - fac2) * P.SX * eps;
+      if (vx > 0.0) vx *= fac1;
+      vy *= fac2;
+      vz *= fac2;
+    }
+  }
+  if (P.fw & 4) {
+    if (z < radius) {
+      z *= fac1;
+      vx *= fac2;
+      vy *= fac2;
+      if (vz < 0.0) vz *= fac1;
+    }
+    if (z >= P.SZ - radius) {
+      z = P.SZ - fac2 * (z - P.SZ) - (1.0 - fac2) * P.SZ * eps;
+      vx *= fac2;
+      vy *= fac2;
+      if (vz > 0.0) vz *= fac1;
+    }
   }
 }
 
@@ -318,98 +599,111 @@ static __device__ __noinline__ void orient_particle(double* pf, long long np, in
 #undef F
 }
 
-template <typename A, bool ORIENT = false>
-__global__ void particle_substep_kernel(const PartParams<A> P) {
+// FP32: four blocks of 128 per SM (<= 128 registers); FP64 keeps twice the registers
+template <typename A, bool ORIENT, bool HALO, int NF>
+__global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_kernel(const PartParams<A> P) {
   const int ip = blockIdx.x * blockDim.x + threadIdx.x;
   if (ip >= P.np) return;
   double* pf = P.pf;
   const long long np = P.np;
 #define F(name) pf[CH4_PF(name) * np + ip]
   const double x0 = F(x), y0 = F(y), z0 = F(z);
-  const double vx0 = F(vx), vy0 = F(vy), vz0 = F(vz);
-  const double vxo0 = F(vx_old), vyo0 = F(vy_old), vzo0 = F(vz_old);
-  const double uxo0 = F(ux_old), uyo0 = F(uy_old), uzo0 = F(uz_old);
-  const double axo0 = F(ax_old), ayo0 = F(ay_old), azo0 = F(az_old);
-  const double tau = F(tau_drag), beta = F(beta_coeff);
-  const double told0 = P.has_t ? F(t_old) : 0.0;
+  if constexpr (!HALO) {  // the state the push reads after the interpolation: on its way meanwhile
+    prefetch_l2(&F(vx));
+    prefetch_l2(&F(vy));
+    prefetch_l2(&F(vz));
+    prefetch_l2(&F(tau_drag));
+    prefetch_l2(&F(beta_coeff));
+    prefetch_l2(&F(vx_old));
+    prefetch_l2(&F(vy_old));
+    prefetch_l2(&F(vz_old));
+    prefetch_l2(&F(ux_old));
+    prefetch_l2(&F(uy_old));
+    prefetch_l2(&F(uz_old));
+    prefetch_l2(&F(ax_old));
+    prefetch_l2(&F(ay_old));
+    prefetch_l2(&F(az_old));
+  }
   // ---- interpolate_vector_at_particles, interpolate_scalar_at_particles(t, 't')
   //      (src/lagrange.c:1211-1439, 1442-1593)
-  Stencil t;
-  double px, py, pz;
-  wrapped_position(P, x0, y0, z0, px, py, pz);
-  make_stencil(px, py, pz, t);
-  PNbr o;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    o.xo[q] = pmod(t.im - 1 + q, P.NX);
-    o.yo[q] = pmod(t.jm - 1 + q, P.NY) * P.NX;
-    o.zo[q] = (long long)pmod(t.km - 1 + q, P.NZ) * P.NX * P.NY;
-  }
-  const bool lo[3] = {t.im == -1, t.jm == -1, t.km == -1};
-  const bool hi[3] = {t.im + 1 == P.NX, t.jm + 1 == P.NY, t.km + 1 == P.NZ};
-  double v[4], gr[12];  // u_x, u_y, u_z, t and their gradient rows
-  const int nf = P.has_t ? 4 : 3;
-  if (P.gradient) {
-    interp_cells<true>(P.ut4, nf, o, t.vol, lo, hi, v, gr);
-  } else {
-    interp_cells<false>(P.ut4, nf, o, t.vol, lo, hi, v, gr);
-    // without LAGRANGE_GRADIENT the added-mass term reads the stored gradients
-    gr[0] = F(dx_ux);
-    gr[1] = F(dy_ux);
-    gr[2] = F(dz_ux);
-    gr[3] = F(dx_uy);
-    gr[4] = F(dy_uy);
-    gr[5] = F(dz_uy);
-    gr[6] = F(dx_uz);
-    gr[7] = F(dy_uz);
-    gr[8] = F(dz_uz);
+  double v[NF], gr[NF][3];
+  {
+    Stencil t;
+    double px, py, pz;
+    wrapped_position(P, x0, y0, z0, px, py, pz);
+    make_stencil(px, py, pz, t);
+    if constexpr (HALO) {
+      if (P.gradient)
+        interp_fields<HALO, NF, true>(P, t, v, gr);
+      else
+        interp_fields<HALO, NF, false>(P, t, v, gr);
+    } else {
+      if (P.gradient)
+        interp_lines<NF, true>(P, t, v, gr);
+      else
+        interp_lines<NF, false>(P, t, v, gr);
+    }
   }
   const double ux = v[0], uy = v[1], uz = v[2];
   F(ux) = ux;
   F(uy) = uy;
   F(uz) = uz;
   if (P.gradient) {
-    F(dx_ux) = gr[0];
-    F(dy_ux) = gr[1];
-    F(dz_ux) = gr[2];
-    F(dx_uy) = gr[3];
-    F(dy_uy) = gr[4];
-    F(dz_uy) = gr[5];
-    F(dx_uz) = gr[6];
-    F(dy_uz) = gr[7];
-    F(dz_uz) = gr[8];
+    F(dx_ux) = gr[0][0];
+    F(dy_ux) = gr[0][1];
+    F(dz_ux) = gr[0][2];
+    F(dx_uy) = gr[1][0];
+    F(dy_uy) = gr[1][1];
+    F(dz_uy) = gr[1][2];
+    F(dx_uz) = gr[2][0];
+    F(dy_uz) = gr[2][1];
+    F(dz_uz) = gr[2][2];
+  } else {  // without LAGRANGE_GRADIENT the added-mass term reads the stored gradients
+    gr[0][0] = F(dx_ux);
+    gr[0][1] = F(dy_ux);
+    gr[0][2] = F(dz_ux);
+    gr[1][0] = F(dx_uy);
+    gr[1][1] = F(dy_uy);
+    gr[1][2] = F(dz_uy);
+    gr[2][0] = F(dx_uz);
+    gr[2][1] = F(dy_uz);
+    gr[2][2] = F(dz_uz);
   }
-  // ---- move_particles (src/lagrange.c:3040-3440)
+  // ---- move_particles (src/lagrange.c:2934-3470)
+  const double vx0 = F(vx), vy0 = F(vy), vz0 = F(vz);
+  const double tau = F(tau_drag), beta = F(beta_coeff);
   const double dtl = P.dtl;
   const bool first = P.first != 0;
-  if (P.has_t) {
+  if constexpr (NF == 4) {
     const double tv = v[3];
-    const double* gt = gr + 9;
     if (P.gradient) {
-      F(dx_t) = gt[0];
-      F(dy_t) = gt[1];
-      F(dz_t) = gt[2];
+      F(dx_t) = gr[3][0];
+      F(dy_t) = gr[3][1];
+      F(dz_t) = gr[3][2];
     }
-    F(t) = tv;
     // time derivatives of t along the path, src/lagrange.c:2997-3010
     if (first) {
       F(t_old) = tv;
     } else {
-      const double dt_t = (tv - told0) / dtl;
+      const double dt_t = (tv - F(t_old)) / dtl;
       F(dt_t) = dt_t;
       F(t_old) = tv;
-      if (P.gradient) F(Dt_t) = dt_t + (ux - vx0) * gt[0] + (uy - vy0) * gt[1] + (uz - vz0) * gt[2];
+      if (P.gradient) F(Dt_t) = dt_t + (ux - vx0) * gr[3][0] + (uy - vy0) * gr[3][1] + (uz - vz0) * gr[3][2];
     }
+    F(t) = tv;
   }
   double xn = x0, yn = y0, zn = z0;
+  double vx = vx0, vy = vy0, vz = vz0;
   if (tau < 0.0) {  // Eulerian probe
-    F(vx) = ux;
-    F(vy) = uy;
-    F(vz) = uz;
+    vx = ux;
+    vy = uy;
+    vz = uz;
   }
   if (tau == 0.0) {  // tracer
-    const double vx = ux, vy = uy, vz = uz;
-    double vxo = vxo0, vyo = vyo0, vzo = vzo0;
+    vx = ux;
+    vy = uy;
+    vz = uz;
+    double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
     if (first) {
       vxo = vx;
       vyo = vy;
@@ -427,9 +721,6 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
       yn = y0 + dtl * 0.5 * (3.0 * vy - vyo);
       zn = z0 + dtl * 0.5 * (3.0 * vz - vzo);
     }
-    F(vx) = vx;
-    F(vy) = vy;
-    F(vz) = vz;
     F(vx_old) = vx;
     F(vy_old) = vy;
     F(vz_old) = vz;
@@ -439,28 +730,35 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
   }
   if (tau > 0.0) {  // Stokes drag (+ added mass)
     const double invtau = 1.0 / tau;
-    double vx = vx0, vy = vy0, vz = vz0;
     double ax = (ux - vx) * invtau, ay = (uy - vy) * invtau, az = (uz - vz) * invtau;
     if (P.gravity) {  // -g, src/lagrange.c:3312-3323
       ax -= P.g[0];
       ay -= P.g[1];
       az -= P.g[2];
     }
-    double uxo = uxo0, uyo = uyo0, uzo = uzo0;
+    // Du/Dt of the added-mass term (the stored one where the term is off, as the
+    // small-tau_drag models read it)
+    double Dx = 0.0, Dy = 0.0, Dz = 0.0;
+    if (P.stau_beta || P.stau_floater) {
+      Dx = F(Dt_ux);
+      Dy = F(Dt_uy);
+      Dz = F(Dt_uz);
+    }
     if (P.addedmass && beta != 0.0) {
       if (P.gravity) {  // -(-beta) g, src/lagrange.c:3330-3339
         ax -= (-beta) * P.g[0];
         ay -= (-beta) * P.g[1];
         az -= (-beta) * P.g[2];
       }
+      double uxo = F(ux_old), uyo = F(uy_old), uzo = F(uz_old);
       if (first) {
         uxo = ux;
         uyo = uy;
         uzo = uz;
       }
-      const double Dx = (ux - uxo) / dtl + (ux - vx) * gr[0] + (uy - vy) * gr[1] + (uz - vz) * gr[2];
-      const double Dy = (uy - uyo) / dtl + (ux - vx) * gr[3] + (uy - vy) * gr[4] + (uz - vz) * gr[5];
-      const double Dz = (uz - uzo) / dtl + (ux - vx) * gr[6] + (uy - vy) * gr[7] + (uz - vz) * gr[8];
+      Dx = (ux - uxo) / dtl + (ux - vx) * gr[0][0] + (uy - vy) * gr[0][1] + (uz - vz) * gr[0][2];
+      Dy = (uy - uyo) / dtl + (ux - vx) * gr[1][0] + (uy - vy) * gr[1][1] + (uz - vz) * gr[1][2];
+      Dz = (uz - uzo) / dtl + (ux - vx) * gr[2][0] + (uy - vy) * gr[2][1] + (uz - vz) * gr[2][2];
       ax += Dx * beta;
       ay += Dy * beta;
       az += Dz * beta;
@@ -468,14 +766,15 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
       F(Dt_uy) = Dy;
       F(Dt_uz) = Dz;
     }
+    const double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
     if (first) {
       xn = x0 + dtl * vx;
       yn = y0 + dtl * vy;
       zn = z0 + dtl * vz;
     } else {
-      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo0);
-      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo0);
-      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo0);
+      xn = x0 + dtl * 0.5 * (3.0 * vx - vxo);
+      yn = y0 + dtl * 0.5 * (3.0 * vy - vyo);
+      zn = z0 + dtl * 0.5 * (3.0 * vz - vzo);
     }
     F(vx_old) = vx;
     F(vy_old) = vy;
@@ -488,24 +787,49 @@ __global__ void particle_substep_kernel(const PartParams<A> P) {
       vy += dtl * ay;
       vz += dtl * az;
     } else {
-      vx += dtl * 0.5 * (3.0 * ax - axo0);
-      vy += dtl * 0.5 * (3.0 * ay - ayo0);
-      vz += dtl * 0.5 * (3.0 * az - azo0);
+      vx += dtl * 0.5 * (3.0 * ax - F(ax_old));
+      vy += dtl * 0.5 * (3.0 * ay - F(ay_old));
+      vz += dtl * 0.5 * (3.0 * az - F(az_old));
     }
-    F(vx) = vx;
-    F(vy) = vy;
-    F(vz) = vz;
     F(ax) = ax;
     F(ay) = ay;
     F(az) = az;
     F(ax_old) = ax;
     F(ay_old) = ay;
     F(az_old) = az;
+    if (P.stau_beta && tau < 10.0) {
+      // small-tau_drag velocity, src/lagrange.c:3425-3445: u - g (1 - beta) tau - Du/Dt (1 - beta) tau
+      vx = ux;
+      vy = uy;
+      vz = uz;
+      vx -= P.g[0] * (1.0 - beta) * tau;
+      vy -= P.g[1] * (1.0 - beta) * tau;
+      vz -= P.g[2] * (1.0 - beta) * tau;
+      vx -= Dx * (1.0 - beta) * tau;
+      vy -= Dy * (1.0 - beta) * tau;
+      vz -= Dz * (1.0 - beta) * tau;
+    }
+    if (P.stau_floater) {
+      // thermal floater, src/lagrange.c:3446-3464: u + tau (1 - beta + 2/3 beta_t (t - 0.4)) (-g - Du/Dt)
+      vx = ux;
+      vy = uy;
+      vz = uz;
+      const double tt = NF == 4 ? v[NF - 1] : 0.0;
+      const double fac1 = tau * (1.0 - beta + 2. / 3. * P.beta_t * (tt - 0.4));
+      vx += fac1 * (-P.g[0] - Dx);
+      vy += fac1 * (-P.g[1] - Dy);
+      vz += fac1 * (-P.g[2] - Dz);
+    }
   }
-  if constexpr (ORIENT) orient_particle(pf, np, ip, gr, P.jeffery != 0, first, dtl);
+  if constexpr (ORIENT) orient_particle(pf, np, ip, &gr[0][0], P.jeffery != 0, first, dtl);
+  double tp = P.lagr_temp ? F(t_p) : 0.0;
+  if constexpr (HALO) particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp);
+  F(vx) = vx;
+  F(vy) = vy;
+  F(vz) = vz;
   if (P.lagr_temp) {  // T_p <- (T_p + fac1 T) exp(-fac1), src/lagrange.c:4007-4018
     const double fac1 = pf[(long long)PF_TFAC * np + ip], e = pf[(long long)PF_TEXP * np + ip];
-    F(t_p) = (F(t_p) + fac1 * v[3]) * e;
+    F(t_p) = (tp + fac1 * v[NF - 1]) * e;
   }
   // ---- LAGRANGE_WRAP of sendrecv_particles
   F(x) = pwrapd(xn, P.SX);
@@ -540,9 +864,15 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   // gravity_vector of src/lagrange_feedback.c:95-103 (y points down)
   const double gx = P.gravity ? P.g[0] : 0.0, gy = P.gravity ? -P.g[1] : 0.0, gz = P.gravity ? P.g[2] : 0.0;
   double* r = P.rec;
-  r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
-  r[1LL * np + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;
-  r[2LL * np + ip] = live ? fac * (F(Dt_uz) - gz + dr * (gz - F(az))) : 0.0;
+  if (P.twoway_stau) {  // (Du/Dt - g)(1 - rho_p/rho_f), src/lagrange_feedback.c:106-110
+    r[0LL * np + ip] = live ? fac * ((F(Dt_ux) - gx) * (1 - dr)) : 0.0;
+    r[1LL * np + ip] = live ? fac * ((F(Dt_uy) - gy) * (1 - dr)) : 0.0;
+    r[2LL * np + ip] = live ? fac * ((F(Dt_uz) - gz) * (1 - dr)) : 0.0;
+  } else {
+    r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
+    r[1LL * np + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;
+    r[2LL * np + ip] = live ? fac * (F(Dt_uz) - gz + dr * (gz - F(az))) : 0.0;
+  }
   if (P.twoway_temp) {  // src/lagrange_feedback.c:181-190: sp = Dt_t + (T_p - T) kappa / (nu beta tau_drag)
     const double fac2 = P.kappa / (P.nu * F(beta_coeff) * F(tau_drag));
     r[(long long)(P.nrec - 1) * np + ip] = live ? fac * (F(Dt_t) + (F(t_p) - F(t)) * fac2) : 0.0;

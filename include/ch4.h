@@ -138,7 +138,29 @@ enum {
   CH4_F2_LAGRANGE_TEMPERATURE = 1ull << 14,
   /* two-way thermal coupling: the particles' heat exchange deposited as a temperature
    * source (with LB_TEMPERATURE_FORCING), src/lagrange_feedback.c:181-230 */
-  CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE = 1ull << 15
+  CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE = 1ull << 15,
+  /* the wall umbrellas LB_FLUID_BC / LB_TEMPERATURE_BC / LB_SCALAR_BC (implied by any wall
+   * of their kind): with them the particles' gradients on the halo layers are the
+   * one-sided ones of the next interior cell, src/gradients.c:245-369, 626-726 */
+  CH4_F2_FLUID_BC = 1ull << 16,
+  CH4_F2_TEMPERATURE_BC = 1ull << 17,
+  CH4_F2_SCALAR_BC = 1ull << 18,
+  /* particles at the fluid walls, src/lagrange.c:3754-3998: elastic by default;
+   * fully inelastic; re-injection through the opposite y wall (NORANDOM: same x and z)
+   * with zero or (half) the Stokes settling velocity */
+  CH4_F2_LAGRANGE_BC_INELASTIC = 1ull << 19,
+  CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT = 1ull << 20,
+  CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM = 1ull << 21,
+  CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO = 1ull << 22,
+  CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF = 1ull << 23,
+  /* small-tau_drag velocity of inertial particles, src/lagrange.c:3425-3466: BETA for
+   * 0 < tau_drag < 10, FLOATER (thermal buoyancy) for every tau_drag > 0 */
+  CH4_F2_LAGRANGE_SMALLTAUD = 1ull << 24,
+  CH4_F2_LAGRANGE_SMALLTAUD_BETA = 1ull << 25,
+  CH4_F2_LAGRANGE_SMALLTAUD_FLOATER = 1ull << 26,
+  /* two-way force of the small-tau_drag model, (Du/Dt - g)(1 - rho_p/rho_f),
+   * src/lagrange_feedback.c:106-110 */
+  CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD = 1ull << 27
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */

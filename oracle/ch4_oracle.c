@@ -21,6 +21,7 @@
  */
 #include "ch4_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -406,53 +407,129 @@ static inline int pwrap(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n :
 
 /* u component a at interior coordinates (i,j,k) in [-1, N]: the halo is the
  * periodic copy made by boundary_conditions_hydro (src/boundary_conditions.c:2786) */
-static inline double uat(const ch4o_state *s, const double *u, int a, int i, int j, int k) {
-  return u[3 * cidx(s, pwrap(i, s->NX), pwrap(j, s->NY), pwrap(k, s->NZ)) + a];
+/* ---- the particle fields' halo and gradients ---------------------------------------
+ * boundary_conditions_hydro (src/boundary_conditions.c:2786-2997): every halo cell first
+ * holds the periodic copy (sendrecv), then on the walled axes (with LB_FLUID_BC) the first
+ * layer is overwritten, x then y then z: u mirrored (-u; on a slip wall only the normal
+ * component flips), and t extrapolated to the wall value on the y temperature walls (with
+ * LB_TEMPERATURE_BC).  The flags below follow the reference's macros: the walls of an axis
+ * only act inside their umbrella (LB_FLUID_BC / LB_TEMPERATURE_BC), which a wall flag implies. */
+static int fluid_bc(const ch4_config *c) { return (c->flags2 & CH4_F2_FLUID_BC) || fluid_walls(c); }
+static int value_bc(const ch4_config *c) {
+  return (c->flags2 & (CH4_F2_TEMPERATURE_BC | CH4_F2_SCALAR_BC)) || scalar_walls(c);
 }
 
-/* d u_a / d x_b at a cell of the particle stencil (gradient_vector with LAGRANGE,
- * src/gradients.c:78-95): centred inside, and on the first halo layer the one-sided
- * 2nd-order stencil of LAGRANGE_INTERPOLATION_FIX (src/gradients.c:358-420) */
-static double grad_at(const ch4o_state *s, const double *u, int a, int b, int i, int j, int k) {
-  const int n = b == 0 ? s->NX : b == 1 ? s->NY : s->NZ;
-  const int c = b == 0 ? i : b == 1 ? j : k;
-  const int di = b == 0, dj = b == 1, dk = b == 2;
+/* u_a at a stencil cell (-2 .. N+1 on each axis) */
+static double uat(const ch4o_state *s, const double *u, int a, int i, int j, int k) {
+  const int n[3] = {s->NX, s->NY, s->NZ};
+  const int fw = fluid_walls(&s->cfg);
+  const int sp[3] = {(s->cfg.flags2 & CH4_F2_FLUID_BC_X_P_SLIP) != 0, (s->cfg.flags & CH4_F_FLUID_BC_Y_P_SLIP) != 0,
+                     (s->cfg.flags2 & CH4_F2_FLUID_BC_Z_P_SLIP) != 0};
+  const int sm[3] = {(s->cfg.flags2 & CH4_F2_FLUID_BC_X_M_SLIP) != 0, (s->cfg.flags & CH4_F_FLUID_BC_Y_M_SLIP) != 0,
+                     (s->cfg.flags2 & CH4_F2_FLUID_BC_Z_M_SLIP) != 0};
+  int c[3] = {i, j, k};
+  double f = 1.0;
+  for (int b = 0; b < 3; b++) {
+    if (((fw >> b) & 1) && c[b] == -1) {
+      c[b] = 0;
+      f = (sm[b] && a != b) ? f : -f;
+    } else if (((fw >> b) & 1) && c[b] == n[b]) {
+      c[b] = n[b] - 1;
+      f = (sp[b] && a != b) ? f : -f;
+    } else {
+      c[b] = c[b] < 0 ? c[b] + n[b] : (c[b] >= n[b] ? c[b] - n[b] : c[b]);
+    }
+  }
+  const double v = u[3 * cidx(s, c[0], c[1], c[2]) + a];
+  return f == 1.0 ? v : -v;
+}
+
+/* t at a stencil cell: periodic copies; with temperature walls on y the first layer
+ * beyond each wall is (2 (T_wall - T_ref) / t - 1) t of the row next to it */
+static double tat(const ch4o_state *s, const double *t, int i, int j, int k) {
+  const int NX = s->NX, NY = s->NY, NZ = s->NZ;
+  const int x = i < 0 ? i + NX : (i >= NX ? i - NX : i), z = k < 0 ? k + NZ : (k >= NZ ? k - NZ : k);
+  if ((s->cfg.flags & CH4_F_TEMPERATURE_BC_Y) && (j == -1 || j == NY)) {
+    const double T_wall = j == -1 ? s->cfg.T_bot : s->cfg.T_top;
+    const double t0 = t[cidx(s, x, j == -1 ? 0 : NY - 1, z)];
+    const double fac = 2.0 * (T_wall - s->cfg.T_ref) / t0 - 1.0;
+    return fac * t0;
+  }
+  const int y = j < 0 ? j + NY : (j >= NY ? j - NY : j);
+  return t[cidx(s, x, y, z)];
+}
+
+/* one field of the gradient engine: u_a (a = 0..2) or t (a = 3) */
+static double fat(const ch4o_state *s, const double *f, int a, int i, int j, int k) {
+  return a < 3 ? uat(s, f, a, i, j, k) : tat(s, f, i, j, k);
+}
+
+/* gradient_vector / gradient_scalar with LAGRANGE at a stencil cell (src/gradients.c:78-500,
+ * 505-835), all three axes of field a, in the reference's statement order:
+ *  1. centred differences (on the halo layers they are overwritten by 3, whatever the
+ *     halo width);
+ *  2. with the umbrella (LB_FLUID_BC for u, LB_TEMPERATURE_BC / LB_SCALAR_BC for t), the
+ *     one-sided second-order difference on the first and last rows of a walled axis;
+ *  3. LAGRANGE_INTERPOLATION_FIX on the halo layers: with the umbrella the one-sided
+ *     difference of the interior cell next to the layer, the index moved there (and kept for
+ *     the later axes), else the one-sided difference of the halo cell itself;
+ *  4. zero along an axis one cell wide. */
+static void grad_cell(const ch4o_state *s, const double *f, int a, int i, int j, int k, double g[3]) {
+  const int n[3] = {s->NX, s->NY, s->NZ};
+  const int bc = a < 3 ? fluid_bc(&s->cfg) : value_bc(&s->cfg);
+  const int walls = a < 3 ? fluid_walls(&s->cfg) : scalar_walls(&s->cfg);
   const double h1 = 1.0, h2 = 1.0;
-  if (c == -1) {
-    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
-    return a0 * uat(s, u, a, i, j, k) + a1 * uat(s, u, a, i + di, j + dj, k + dk) +
-           a2 * uat(s, u, a, i + 2 * di, j + 2 * dj, k + 2 * dk);
+  const double l0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), l1 = (h1 + h2) / (h1 * h2), l2 = -(h1) / (h2 * (h1 + h2));
+  const double u0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), u1 = -(h1 + h2) / (h1 * h2), u2 = (h1) / (h2 * (h1 + h2));
+  int c[3] = {i, j, k};
+#define AT(b, o) (d[0] = c[0], d[1] = c[1], d[2] = c[2], d[b] += (o), fat(s, f, a, d[0], d[1], d[2]))
+  int d[3];
+  for (int b = 0; b < 3; b++) {
+    g[b] = 0.0;
+    if (c[b] >= 0 && c[b] <= n[b] - 1) { /* the halo layers (-1, n) are overwritten below */
+      const double vp = AT(b, 1), vm = AT(b, -1);
+      g[b] = (vp - vm) / 2.0;
+    }
   }
-  if (c == n) {
-    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
-    return a0 * uat(s, u, a, i, j, k) + a1 * uat(s, u, a, i - di, j - dj, k - dk) +
-           a2 * uat(s, u, a, i - 2 * di, j - 2 * dj, k - 2 * dk);
+  if (bc) {
+    for (int b = 0; b < 3; b++) {
+      if (!((walls >> b) & 1)) continue;
+      if (c[b] == 0) {
+        const double v0 = AT(b, 0), v1 = AT(b, 1), v2 = AT(b, 2);
+        g[b] = l0 * v0 + l1 * v1 + l2 * v2;
+      }
+      if (c[b] == n[b] - 1) {
+        const double v0 = AT(b, 0), v1 = AT(b, -1), v2 = AT(b, -2);
+        g[b] = u0 * v0 + u1 * v1 + u2 * v2;
+      }
+    }
+    for (int b = 0; b < 3; b++) {
+      if (c[b] == -1) {
+        c[b] = 0;
+        const double v0 = AT(b, 0), v1 = AT(b, 1), v2 = AT(b, 2);
+        g[b] = l0 * v0 + l1 * v1 + l2 * v2;
+      }
+      if (c[b] == n[b]) {
+        c[b] = n[b] - 1;
+        const double v0 = AT(b, 0), v1 = AT(b, -1), v2 = AT(b, -2);
+        g[b] = u0 * v0 + u1 * v1 + u2 * v2;
+      }
+    }
+  } else {
+    for (int b = 0; b < 3; b++) {
+      if (c[b] == -1) {
+        const double v0 = AT(b, 0), v1 = AT(b, 1), v2 = AT(b, 2);
+        g[b] = l0 * v0 + l1 * v1 + l2 * v2;
+      }
+      if (c[b] == n[b]) {
+        const double v0 = AT(b, 0), v1 = AT(b, -1), v2 = AT(b, -2);
+        g[b] = u0 * v0 + u1 * v1 + u2 * v2;
+      }
+    }
   }
-  return (uat(s, u, a, i + di, j + dj, k + dk) - uat(s, u, a, i - di, j - dj, k - dk)) / 2.0;
-}
-
-/* scalar field at interior coordinates in [-1, N] (periodic halo) */
-static inline double tat(const ch4o_state *s, const double *t, int i, int j, int k) {
-  return t[cidx(s, pwrap(i, s->NX), pwrap(j, s->NY), pwrap(k, s->NZ))];
-}
-
-/* d t / d x_b at a cell of the particle stencil: gradient_scalar with LAGRANGE
- * (src/gradients.c:505-520) and LAGRANGE_INTERPOLATION_FIX, SECOND_ORDER_GRAD on the
- * first halo layer of a box without temperature walls (src/gradients.c:731-800) */
-static double tgrad_at(const ch4o_state *s, const double *t, int b, int i, int j, int k) {
-  const int n = b == 0 ? s->NX : b == 1 ? s->NY : s->NZ;
-  const int c = b == 0 ? i : b == 1 ? j : k;
-  const int di = b == 0, dj = b == 1, dk = b == 2;
-  const double h1 = 1.0, h2 = 1.0;
-  if (c == -1) {
-    double a0 = -(2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = (h1 + h2) / (h1 * h2), a2 = -(h1) / (h2 * (h1 + h2));
-    return a0 * tat(s, t, i, j, k) + a1 * tat(s, t, i + di, j + dj, k + dk) + a2 * tat(s, t, i + 2 * di, j + 2 * dj, k + 2 * dk);
-  }
-  if (c == n) {
-    double a0 = (2.0 * h1 + h2) / (h1 * (h1 + h2)), a1 = -(h1 + h2) / (h1 * h2), a2 = (h1) / (h2 * (h1 + h2));
-    return a0 * tat(s, t, i, j, k) + a1 * tat(s, t, i - di, j - dj, k - dk) + a2 * tat(s, t, i - 2 * di, j - 2 * dj, k - 2 * dk);
-  }
-  return (tat(s, t, i + di, j + dj, k + dk) - tat(s, t, i - di, j - dj, k - dk)) / 2.0;
+#undef AT
+  for (int b = 0; b < 3; b++)
+    if (n[b] == 1) g[b] = 0.0;
 }
 
 /* cell of the stencil and the six distances (src/lagrange.c:1231-1287) */
@@ -505,13 +582,14 @@ static void interp_particle(const ch4o_state *s, const double *u, ch4_particle *
   p->uy = v[1];
   p->uz = v[2];
   if (s->cfg.flags & CH4_F_LAGRANGE_GRADIENT) {
-    double gr[3][3];
+    double gr[3][3], gc[8][3][3];
+    for (int c = 0; c < 8; c++)
+      for (int a = 0; a < 3; a++) grad_cell(s, u, a, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2], gc[c][a]);
     for (int a = 0; a < 3; a++)
       for (int b = 0; b < 3; b++) {
         double acc = 0.0;
         for (int c = 0; c < 8; c++) {
-          double term =
-              grad_at(s, u, a, b, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2]) * t.vol[c];
+          double term = gc[c][a][b] * t.vol[c];
           acc = c == 0 ? term : acc + term;
         }
         gr[a][b] = acc;
@@ -539,11 +617,12 @@ static void interp_particle_t(const ch4o_state *s, const double *tf, ch4_particl
   }
   p->t = acc;
   if (s->cfg.flags & CH4_F_LAGRANGE_GRADIENT) {
-    double g[3];
+    double g[3], gc[8][3];
+    for (int c = 0; c < 8; c++) grad_cell(s, tf, 3, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2], gc[c]);
     for (int b = 0; b < 3; b++) {
       double a = 0.0;
       for (int c = 0; c < 8; c++) {
-        double term = tgrad_at(s, tf, b, t.im + CORNER[c][0], t.jm + CORNER[c][1], t.km + CORNER[c][2]) * t.vol[c];
+        double term = gc[c][b] * t.vol[c];
         a = c == 0 ? term : a + term;
       }
       g[b] = a;
@@ -597,6 +676,95 @@ static void orient_particle(ch4_particle *p, int jeffery, int first, double dtl)
   p->dt_px = Fold[0];
   p->dt_py = Fold[1];
   p->dt_pz = Fold[2];
+}
+
+/* the walls of move_particles (src/lagrange.c:3754-3998), zero radius, y then x then z,
+ * each wall tested on the position the previous tests left.  Elastic (fac1 = -1,
+ * fac2 = 1): the position is mirrored at the wall and an outward normal velocity
+ * reversed.  LAGRANGE_BC_INELASTIC (fac1 = fac2 = 0): the position is put on the wall
+ * (x and z: SX (1 - FLT_EPSILON) at the upper one), the tangential velocity and an
+ * outward normal one zeroed.  LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM: a particle that
+ * crossed a y wall re-enters through the other one (y + SY, y - (SY - FLT_EPSILON)), with
+ * zero or the Stokes settling velocity -g (1 - beta) tau_drag (halved with
+ * VELOCITY_STOKES_HALF, at the bottom wall only, as the reference has it) and, with
+ * LAGRANGE_TEMPERATURE, the temperature of the wall it
+ * re-enters through. */
+static void particle_walls(const ch4o_state *s, ch4_particle *p) {
+  const ch4_config *c = &s->cfg;
+  const uint64_t f2 = c->flags2;
+  if (!fluid_bc(c)) return;
+  const int inel = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC) != 0, reinj = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) != 0;
+  const double fac1 = inel ? 0.0 : -1.0, fac2 = inel ? 0.0 : 1.0;
+  const double radius = 0.0;
+  const double flt_eps = (double)FLT_EPSILON;
+  if (c->flags & CH4_F_FLUID_BC_Y) {
+    for (int side = 0; side < 2; side++) {
+      const int crossed = side == 0 ? p->y < radius : p->y >= c->SY - radius;
+      if (!crossed) continue;
+      if (!reinj) {
+        if (side == 0) {
+          p->y = fac1 * (p->y - radius) + radius;
+          p->vx *= fac2;
+          if (p->vy < 0.0) p->vy *= fac1;
+          p->vz *= fac2;
+        } else {
+          p->y = fac1 * (p->y - (c->SY - radius)) + (c->SY - radius);
+          p->vx *= fac2;
+          if (p->vy > 0.0) p->vy *= fac1;
+          p->vz *= fac2;
+        }
+      }
+      if (inel && reinj) {
+        if (side == 0)
+          p->y += c->SY;
+        else
+          p->y -= (c->SY - flt_eps);
+        if (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO) {
+          p->vx = 0.0;
+          p->vy = 0.0;
+          p->vz = 0.0;
+        } else {
+          p->vx = -c->gravity_x * (1.0 - p->beta_coeff) * p->tau_drag;
+          p->vy = -c->gravity_y * (1.0 - p->beta_coeff) * p->tau_drag;
+          p->vz = -c->gravity_z * (1.0 - p->beta_coeff) * p->tau_drag;
+        }
+        if (side == 0 && (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF)) {
+          p->vx /= 2.0;
+          p->vy /= 2.0;
+          p->vz /= 2.0;
+        }
+        if (f2 & CH4_F2_LAGRANGE_TEMPERATURE) p->t_p = side == 0 ? c->T_top : c->T_bot;
+      }
+    }
+  }
+  if (f2 & CH4_F2_FLUID_BC_X) {
+    if (p->x < radius) {
+      p->x *= fac1;
+      if (p->vx < 0.0) p->vx *= fac1;
+      p->vy *= fac2;
+      p->vz *= fac2;
+    }
+    if (p->x >= c->SX - radius) {
+      p->x = c->SX - fac2 * (p->x - c->SX) - (1.0 - fac2) * c->SX * flt_eps;
+      if (p->vx > 0.0) p->vx *= fac1;
+      p->vy *= fac2;
+      p->vz *= fac2;
+    }
+  }
+  if (f2 & CH4_F2_FLUID_BC_Z) {
+    if (p->z < radius) {
+      p->z *= fac1;
+      p->vx *= fac2;
+      p->vy *= fac2;
+      if (p->vz < 0.0) p->vz *= fac1;
+    }
+    if (p->z >= c->SZ - radius) {
+      p->z = c->SZ - fac2 * (p->z - c->SZ) - (1.0 - fac2) * c->SZ * flt_eps;
+      p->vx *= fac2;
+      p->vy *= fac2;
+      if (p->vz > 0.0) p->vz *= fac1;
+    }
+  }
 }
 
 static void move_particle(const ch4o_state *s, ch4_particle *p, int first, double dtl) {
@@ -704,7 +872,34 @@ static void move_particle(const ch4o_state *s, ch4_particle *p, int first, doubl
     p->ax_old = p->ax;
     p->ay_old = p->ay;
     p->az_old = p->az;
+    const int stau = (s->cfg.flags2 & CH4_F2_LAGRANGE_SMALLTAUD) != 0;
+    if (stau && (s->cfg.flags2 & CH4_F2_LAGRANGE_SMALLTAUD_BETA) && p->tau_drag < 10.0 && p->tau_drag > 0.0) {
+      /* small-tau_drag velocity, src/lagrange.c:3425-3445: u - g (1 - beta) tau - Du/Dt (1 - beta) tau.
+       * Du/Dt is the one the added-mass term just computed (the reference's local Dt_u); for
+       * beta = 0 the reference reads that local as the previous particle left it, here the
+       * particle's own stored Du/Dt is read. */
+      p->vx = p->ux;
+      p->vy = p->uy;
+      p->vz = p->uz;
+      p->vx -= s->cfg.gravity_x * (1.0 - p->beta_coeff) * p->tau_drag;
+      p->vy -= s->cfg.gravity_y * (1.0 - p->beta_coeff) * p->tau_drag;
+      p->vz -= s->cfg.gravity_z * (1.0 - p->beta_coeff) * p->tau_drag;
+      p->vx -= p->Dt_ux * (1.0 - p->beta_coeff) * p->tau_drag;
+      p->vy -= p->Dt_uy * (1.0 - p->beta_coeff) * p->tau_drag;
+      p->vz -= p->Dt_uz * (1.0 - p->beta_coeff) * p->tau_drag;
+    }
+    if (stau && (s->cfg.flags2 & CH4_F2_LAGRANGE_SMALLTAUD_FLOATER)) {
+      /* thermal floater, src/lagrange.c:3446-3464: v = u + tau (1 - beta + 2/3 beta_t (t - 0.4)) (-g - Du/Dt) */
+      p->vx = p->ux;
+      p->vy = p->uy;
+      p->vz = p->uz;
+      const double fac1 = p->tau_drag * (1.0 - p->beta_coeff + 2. / 3. * s->cfg.beta_t * (p->t - 0.4));
+      p->vx += fac1 * (-s->cfg.gravity_x - p->Dt_ux);
+      p->vy += fac1 * (-s->cfg.gravity_y - p->Dt_uy);
+      p->vz += fac1 * (-s->cfg.gravity_z - p->Dt_uz);
+    }
   }
+  particle_walls(s, p);
   if (s->cfg.flags2 & CH4_F2_LAGRANGE_TEMPERATURE) {
     /* particle temperature, src/lagrange.c:4007-4018: 1/tau_heat =
      * 2 kappa / (tau_drag nu cp_p (3 - beta)), T_p <- (T_p + fac1 T) exp(-fac1) */
@@ -826,9 +1021,15 @@ static void deposit(const ch4o_state *s, double *D, double *TS) {
     const double gx = grav ? s->cfg.gravity_x : 0.0, gy = grav ? -s->cfg.gravity_y : 0.0,
                  gz = grav ? s->cfg.gravity_z : 0.0;
     double fp[3];
-    fp[0] = p->Dt_ux - gx + dr * (gx - p->ax);
-    fp[1] = p->Dt_uy - gy + dr * (gy - p->ay);
-    fp[2] = p->Dt_uz - gz + dr * (gz - p->az);
+    if (s->cfg.flags2 & CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD) { /* src/lagrange_feedback.c:106-110 */
+      fp[0] = (p->Dt_ux - gx) * (1 - dr);
+      fp[1] = (p->Dt_uy - gy) * (1 - dr);
+      fp[2] = (p->Dt_uz - gz) * (1 - dr);
+    } else {
+      fp[0] = p->Dt_ux - gx + dr * (gx - p->ax);
+      fp[1] = p->Dt_uy - gy + dr * (gy - p->ay);
+      fp[2] = p->Dt_uz - gz + dr * (gz - p->az);
+    }
     /* LAGRANGE_TWOWAY_TEMPERATURE, src/lagrange_feedback.c:181-230: the particle's heat
      * exchange sp = Dt_t + (T_p - T) kappa / (nu beta tau_drag), times its volume */
     double sp = 0.0;

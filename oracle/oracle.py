@@ -114,7 +114,34 @@ FLAGSETS.update({
                       "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_FORCING", "LAGRANGE", "LAGRANGE_WRAP",
                       "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TEMPERATURE", "LAGRANGE_TWOWAY",
                       "LAGRANGE_TWOWAY_MOMENTUM", "LAGRANGE_TWOWAY_TEMPERATURE", "LAGRANGE_TWOWAY_TRICUBIC"],
+    # particles in wall-bounded flows
+    "particles_rb": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+                     "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
+                     "LAGRANGE_GRAVITY", "LAGRANGE_TEMPERATURE", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    "particles_duct": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_BC_Y",
+                       "LB_FLUID_BC_Z", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
+                       "LAGRANGE_BC_INELASTIC", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                       "LAGRANGE_TWOWAY_TRICUBIC"],
+    "particles_slip": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV", "LB_FLUID_BC_X",
+                       "LB_FLUID_BC_X_P_SLIP", "LB_TEMPERATURE", "LB_TEMPERATURE_BC_X", "LAGRANGE", "LAGRANGE_WRAP",
+                       "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    "particles_reinj": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+                        "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT",
+                        "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY", "LAGRANGE_TEMPERATURE", "LAGRANGE_BC_INELASTIC",
+                        "LAGRANGE_BC_INELASTIC_REINJECT", "LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM",
+                        "LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF", "LAGRANGE_SMALLTAUD",
+                        "LAGRANGE_SMALLTAUD_BETA", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                        "LAGRANGE_TWOWAY_SMALLTAUD"],
+    "particles_bc": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_FLUID_BC", "LB_TEMPERATURE",
+                     "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT",
+                     "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY", "LAGRANGE_SMALLTAUD", "LAGRANGE_SMALLTAUD_FLOATER",
+                     "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
 })
+# a wall of a kind implies its umbrella flag, as in every define.h of the reference
+for _names in FLAGSETS.values():
+    for _kind in ("LB_FLUID_BC", "LB_TEMPERATURE_BC", "LB_SCALAR_BC"):
+        if _kind not in _names and any(n.startswith(_kind + "_") for n in _names):
+            _names.append(_kind)
 # non-flag configuration implied by a flag set (define.h variants of one setting)
 FLAGSET_EXTRA = {"walls2": {"t0_kind": abi.T0_REF}}
 

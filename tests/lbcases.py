@@ -88,6 +88,26 @@ CASES = {
                           params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=13,
                                       T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
                                       time_dt_lagr_factor=2.0, particle_number=250)),
+    # particles in wall-bounded flows
+    "particles_rb": dict(flagset="particles_rb", NX=9, NY=8, NZ=7, npart=250,
+                         params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
+                                     gravity_y=1e-3, gravity_x=2e-4, seed=14, time_dt_lagr_factor=2.0,
+                                     particle_number=250)),
+    "particles_duct": dict(flagset="particles_duct", NX=10, NY=8, NZ=7, npart=300,
+                           params=dict(tau_u=0.6, Amp_x=4e-3, Amp_y=1e-3, Amp_z=2e-3, seed=15,
+                                       time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_slip": dict(flagset="particles_slip", NX=8, NY=7, NZ=6, npart=250,
+                           params=dict(tau_u=0.57, tau_t=0.61, T_bot=0.3, T_top=1.0, T_ref=0.5, Amp_x=2e-3,
+                                       Amp_y=1e-3, Amp_z=5e-4, seed=16, time_dt_lagr_factor=2.0,
+                                       particle_number=250)),
+    "particles_reinj": dict(flagset="particles_reinj", NX=9, NY=8, NZ=7, npart=250,
+                            params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
+                                        gravity_y=1e-3, gravity_x=2e-4, gravity_z=-1e-4, seed=17,
+                                        time_dt_lagr_factor=2.0, particle_number=250)),
+    "particles_bc": dict(flagset="particles_bc", NX=9, NY=8, NZ=7, npart=250,
+                         params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=18,
+                                     T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3, gravity_x=3e-4,
+                                     time_dt_lagr_factor=2.0, particle_number=250)),
     # walls on x and z
     "duct": dict(flagset="duct", NX=7, NY=8, NZ=6,
                  params=dict(tau_u=0.6, Amp_x=4e-3, Amp_y=1e-3, Amp_z=2e-3)),
@@ -151,6 +171,20 @@ def make_case(name, seed=0, storage=0, dims=None, **over):
                 p.beta_coeff = [1.0, 2.0, 0.5][(i // 3) % 3]  # 3 - beta divides the heat rate
                 p.cp_p = cps[(i // 9) % 3]
                 p.t_p = 0.3 + 0.4 * rng.random()
+        walls = [a for a, w in enumerate(("LB_FLUID_BC_X", "LB_FLUID_BC_Y", "LB_FLUID_BC_Z")) if w in flags]
+        if walls:
+            # every fifth particle starts a hair inside a wall, moving out through it
+            # (inertial particles keep that velocity into their first sub-step)
+            size = (c["NX"], c["NY"], c["NZ"])
+            for i, p in enumerate(state["part"]):
+                if i % 5 != 2:
+                    continue
+                a = walls[(i // 5) % len(walls)]
+                upper = (i // 10) % 2 == 1
+                pos = size[a] - 1e-3 * (1 + i % 7) if upper else 1e-3 * (1 + i % 7)
+                vel = 0.02 * (1 + i % 3) * (1 if upper else -1)
+                setattr(p, "xyz"[a], pos)
+                setattr(p, "v" + "xyz"[a], vel)
         if "LAGRANGE_ORIENTATION" in flags:  # random unit orientations, rods and discs
             ratios = [1.0, 5.0, 0.2, 20.0]
             for i, p in enumerate(state["part"]):

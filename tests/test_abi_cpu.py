@@ -94,8 +94,8 @@ def test_device_bytes_admission():
 
 
 def test_walls_on_x_and_z_are_read_from_define_h(tmp_path):
-    """LB_FLUID_BC_X / _Z and the temperature and scalar walls on x and z land in the
-    second flag word; a slip wall next to a wall on another axis is refused at create."""
+    """LB_FLUID_BC_X / _Z, the temperature and scalar walls on x and z and the wall
+    umbrellas land in the second flag word."""
     import ch4b200
     from ch4b200 import abi
     d = tmp_path / "define.h"
@@ -104,7 +104,7 @@ def test_walls_on_x_and_z_are_read_from_define_h(tmp_path):
                  "#define LB_TEMPERATURE\n#define LB_TEMPERATURE_BC_X\n#define LB_TEMPERATURE_BC_X_M_NOFLUX\n")
     c = ch4b200.default_config()
     ch4b200.read_define(c, str(d))
-    assert c.flags2 == abi.flags2_of(["LB_FLUID_BC_X", "LB_FLUID_BC_Z", "LB_FLUID_BC_Z_P_SLIP",
+    assert c.flags2 == abi.flags2_of(["LB_FLUID_BC", "LB_FLUID_BC_X", "LB_FLUID_BC_Z", "LB_FLUID_BC_Z_P_SLIP",
                                       "LB_TEMPERATURE_BC_X", "LB_TEMPERATURE_BC_X_M_NOFLUX"])
     assert abi.has_flag(c, "LB_FLUID_BC_X") and not abi.has_flag(c, "LB_FLUID_BC_Y")
 
@@ -126,3 +126,23 @@ def test_slip_wall_beside_another_wall_is_refused(names):
     h = C.c_void_p()
     rc = ch4b200.lib().ch4_create(C.byref(c), C.byref(h))
     assert rc in (abi.ERR_UNSUPPORTED, abi.ERR_ARG) and not h.value
+
+
+def test_particle_wall_and_small_tau_flags_are_read_from_define_h(tmp_path):
+    """The particles' wall rules and small-tau_drag models are flags of the second word;
+    random re-injection (the reference's drand48 stream) is refused at create."""
+    import ctypes as C
+    d = tmp_path / "define.h"
+    d.write_text("#define GRID_POP_D3Q19\n#define METHOD_STREAMING\n#define LB_FLUID\n#define LB_FLUID_BC\n"
+                 "#define LB_FLUID_BC_Y\n#define LAGRANGE\n#define LAGRANGE_WRAP\n#define LAGRANGE_BC_INELASTIC\n"
+                 "#define LAGRANGE_BC_INELASTIC_REINJECT\n#define LAGRANGE_SMALLTAUD\n"
+                 "#define LAGRANGE_SMALLTAUD_BETA\n#define LAGRANGE_TWOWAY_SMALLTAUD\n")
+    c = ch4b200.default_config()
+    ch4b200.read_define(c, str(d))
+    assert abi.has_flag(c, "LAGRANGE_BC_INELASTIC_REINJECT") and abi.has_flag(c, "LAGRANGE_SMALLTAUD_BETA")
+    assert abi.has_flag(c, "LB_FLUID_BC") and abi.has_flag(c, "LAGRANGE_TWOWAY_SMALLTAUD")
+    c.NX, c.NY, c.NZ = 6, 5, 4
+    c.SX, c.SY, c.SZ = 6.0, 5.0, 4.0
+    c.tau_u, c.time_dt, c.time_dt_lagr_factor = 0.6, 1.0, 1.0
+    h = C.c_void_p()
+    assert ch4b200.lib().ch4_create(C.byref(c), C.byref(h)) == abi.ERR_UNSUPPORTED and not h.value

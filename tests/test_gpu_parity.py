@@ -51,7 +51,8 @@ def rel_l2(a, b):
                                           ("trt", 25), ("trt_les", 25), ("les_vd", 25), ("les_ls", 25),
                                           ("les_ts", 25), ("particles_tc", 12), ("duct", 25), ("duct_les", 25),
                                           ("box", 25), ("slipx", 25), ("slipz", 25), ("particles_tt", 12),
-                                          ("particles_ttc", 12)])
+                                          ("particles_ttc", 12), ("particles_rb", 12), ("particles_duct", 12),
+                                          ("particles_slip", 12), ("particles_reinj", 12), ("particles_bc", 12)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):
     _, cfg, state = make_case(name, seed=11)
     ref = run_restatement(cfg, state, nsteps)
@@ -76,7 +77,8 @@ def test_fp64_bit_identical_to_oracle(name, nsteps):
 @pytest.mark.parametrize("name", ["kolmogorov", "rb", "hit", "walls2", "scalar", "les", "particles",
                                   "particles_t", "particles_g", "trt", "trt_les", "les_vd", "les_ls", "les_ts",
                                   "particles_tc", "duct", "duct_les", "box", "slipx", "slipz", "particles_tt",
-                                  "particles_ttc"])
+                                  "particles_ttc", "particles_rb", "particles_duct", "particles_slip",
+                                  "particles_reinj", "particles_bc"])
 def test_fp64_matches_compiled_reference(name):
     flagset, cfg, state = make_case(name, seed=5)
     if not O.ref_available(flagset):

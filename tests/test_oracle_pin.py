@@ -28,7 +28,9 @@ def _assert_same(a, b, what):
                                           ("trt", 20), ("trt_les", 20), ("les_vd", 20), ("les_ls", 20),
                                           ("les_wale", 20), ("les_ts", 20), ("particles_tc", 8), ("nozero", 15),
                                           ("cpower", 15), ("duct", 20), ("duct_les", 20), ("box", 20),
-                                          ("slipx", 20), ("slipz", 20), ("particles_tt", 8), ("particles_ttc", 8)])
+                                          ("slipx", 20), ("slipz", 20), ("particles_tt", 8), ("particles_ttc", 8),
+                                          ("particles_rb", 8), ("particles_duct", 8), ("particles_slip", 8),
+                                          ("particles_reinj", 8), ("particles_bc", 8)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
