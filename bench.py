@@ -18,7 +18,9 @@ timed as the max over ranks.  Prints ONE JSON line on rank 0.
 At N = 1 the line also carries the reduced-precision error against the FP64 path on the
 same input (`error_vs_fp64`: u and T after the timed steps, Nusselt number and kinetic
 energy over the configuration's 20,000-step run) and the FP64 path's own throughput
-(`fp64`), and the end-to-end run's phases (`e2e.breakdown`).
+(`fp64`), the end-to-end run's phases (`e2e.breakdown`), and the forced-HIT
+configuration (256^3, FP32, 10^6 two-way coupled particles) as its own record
+(`hit_particles`: MLUPS, particle updates/s, ms per step; `--no-hit` skips it).
 """
 import argparse
 import json
@@ -550,26 +552,24 @@ def bench_serve(args):
 TAU_ETA = 10.0  # Kolmogorov time in steps that sets tau_p = St * tau_eta
 
 
-def bench_hit_particles(args):
-    """Forced HIT 256^3 (FP32), 1e6 particles: tracers and Stokes particles with added
-    mass, beta in {0, 1, 3} x St in {0.1, 1, 5} with tau_p = St * 10 steps, except that
-    the bubbles (beta = 3) stop at St = 2: at St = 5 their radius sqrt(3 nu beta tau_p)
-    is 1.22 cells and the explicit two-way deposit diverges within ~20 steps (the FP64
-    oracle shows the same).  Trilinear interpolation with gradients, two-way momentum
-    deposit.  MLUPS and particle updates per second."""
+def hit_particles_run(n, npart, steps, warmup, storage="f32"):
+    """Forced HIT n^3 with npart two-way coupled particles: tracers and Stokes particles with
+    added mass, beta in {0, 1, 3} x St in {0.1, 1, 5} with tau_p = St * 10 steps, except that
+    the bubbles (beta = 3) stop at St = 2: at St = 5 their radius sqrt(3 nu beta tau_p) is
+    1.22 cells and the explicit two-way deposit diverges within ~20 steps (the FP64 oracle
+    shows the same).  Trilinear interpolation with gradients, two-way momentum deposit.
+    Device-resident timing of `steps` steps (CUDA events on the handle's stream)."""
     import torch
     import ch4b200
     from ch4b200 import abi
     torch.cuda.set_device(0)
-    n = args.hit_size
-    npart = args.particles
     c = ch4b200.default_config()
     c.NX = c.NY = c.NZ = n
     c.SX = c.SY = c.SZ = float(n)
     c.flags = abi.flags_of(["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                             "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY",
                             "LAGRANGE_TWOWAY_MOMENTUM"])
-    c.storage = {"f64": abi.STORE_F64, "f16": abi.STORE_F16}.get(args.storage, abi.STORE_F32)
+    c.storage = {"f64": abi.STORE_F64, "f16": abi.STORE_F16}.get(storage, abi.STORE_F32)
     c.tau_u = 0.51
     c.nu = (c.tau_u - 0.5) / 3.0
     c.Amp_x = c.Amp_y = c.Amp_z = 5e-6
@@ -592,19 +592,33 @@ def bench_hit_particles(args):
     with ch4b200.Simulation(c) as sim:
         sim.set_particles(parts)
         sim.initialize()
-        sim.step(max(3, args.warmup))
+        sim.step(max(3, warmup))
         sim.synchronize()
-        sec = _event_time(sim.stream_handle, lambda: sim.step(args.steps))
+        sec = _event_time(sim.stream_handle, lambda: sim.step(steps))
         f = sim.fields()
     cells = n ** 3
-    print(json.dumps({
-        "metric": "MLUPS and particle updates/s", "value": cells * args.steps / sec / 1e6, "unit": "MLUPS",
-        "particles_per_s": npart * args.steps / sec, "n_gpus": 1, "steps": args.steps,
-        "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True, "dtype": args.storage,
-        "data": "synthetic", "config": {"workload": "hit_%d3_particles_%d_twoway" % (n, npart), "tau_eta_steps": TAU_ETA,
-                                        "classes": "tracers + beta{0,1,3} x St{0.1,1,5}, bubbles St<=2"},
+    ms_step = sec / steps * 1e3
+    peak, peak_kind = measured_peak()
+    # lb_step's own bytes per cell: populations read + written, the two-way force read
+    # (the hydro pass for the interpolation and the particle kernels come on top)
+    bpc = 2 * 19 * {"f64": 8, "f16": 2}.get(storage, 4) + 12 + 24
+    achieved = bpc * cells / (ms_step * 1e-3) / 1e9
+    return {
+        "metric": "MLUPS and particle updates/s", "value": cells * steps / sec / 1e6, "unit": "MLUPS",
+        "particles_per_s": npart * steps / sec, "n_gpus": 1, "steps": steps, "warmup": max(3, warmup),
+        "ms_per_step": ms_step, "higher_is_better": True, "dtype": storage, "data": "synthetic",
+        "config": {"workload": "hit_%d3_particles_%d_twoway" % (n, npart), "tau_eta_steps": TAU_ETA,
+                   "classes": "tracers + beta{0,1,3} x St{0.1,1,5}, bubbles St<=2"},
+        "roofline": {"bound": "hbm", "bytes_per_cell": bpc, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "basis": "whole step time against the lattice step's own bytes per cell"},
         "finite": bool(np.isfinite(f["u"]).all()),
-    }))
+    }
+
+
+def bench_hit_particles(args):
+    """The HIT + particles configuration on its own line (MLUPS and particle updates/s)."""
+    print(json.dumps(hit_particles_run(args.hit_size, args.particles, args.steps, args.warmup, args.storage)))
     return 0
 
 
@@ -635,6 +649,7 @@ def main():
     ap.add_argument("--no-error", action="store_true", help="skip the FP32/FP16 error study against FP64")
     ap.add_argument("--error-window", type=int, default=20000)
     ap.add_argument("--error-every", type=int, default=1000)
+    ap.add_argument("--no-hit", action="store_true", help="skip the HIT + particles sub-record")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "ours":
         return spawn_ranks(args)
@@ -758,6 +773,11 @@ def main():
     if world == 1 and not args.no_error:
         err, fp64 = error_vs_fp64(W, K, args.error_window, args.error_every)
 
+    # the third configuration (forced HIT 256^3 + 10^6 two-way particles) beside the headline
+    hit = None
+    if world == 1 and not args.no_hit:
+        hit = hit_particles_run(args.hit_size, args.particles, max(K, 20), W)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         mlups, cores, sample = cpu_reference_run(cpu_sample_steps())
@@ -784,6 +804,7 @@ def main():
             "finite": finite,
             "error_vs_fp64": err,
             "fp64": fp64,
+            "hit_particles": hit,
         }
         print(json.dumps(line))
     if world > 1:
