@@ -690,6 +690,11 @@ def main():
     def new_sim():
         if slab_mode:
             s = slabmod.Slab(gcfg, rank * NZ, NZ)
+            # the faces move inside ch4_step, overlapped with the slab's interior planes
+            if world > 1:
+                s.use_process_group(rank, world)
+            else:
+                slabmod.use_local_faces([s])
             return s.sim, (lambda n: s.step(n, rank, world))
         s = ch4b200.Simulation(cfg)
         return s, s.step
@@ -799,7 +804,8 @@ def main():
                          "bytes_per_cell": BYTES_PER_CELL[args.storage], "kernel": "lb_step_kernel"},
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": K * (3 if slab_mode else 1),  # lb_step (+ halo pack and unpack per step)
+            # lb_step (slabs: face planes + interior, halo pack and unpack per step)
+            "gpu_launches": K * (4 if slab_mode else 1),
             "clocks": clk.summary(),
             "finite": finite,
             "error_vs_fp64": err,

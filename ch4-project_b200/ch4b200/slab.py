@@ -10,9 +10,12 @@ y walls and forcing are plane-local, so the decomposition reproduces the single
 lattice bit for bit (HIT tables run over the whole lattice's z).
 
 The transfer is the caller's plumbing: `exchange` pairs the four point-to-point
-transfers of one step over a torch.distributed process group (NCCL between GPUs,
-gloo on CPU); `step_local` runs several slabs of one process, each unpacking straight
-from its neighbours' send buffers.
+transfers of one step over a torch.distributed process group (NCCL between GPUs, or
+through host copies over gloo); `step_local` runs several slabs of one process, each
+unpacking straight from its neighbours' send buffers.  Registered as the handle's face
+exchange (ch4_set_face_exchange: `Slab.use_process_group`, `use_local_faces`), the
+transfer runs inside ch4_step on a second stream while the slab's interior planes are
+stepped.
 
 With LB_FLUID_FORCING_NOZEROMODE / _CONSTANT_POWER every step also needs the force summed
 over the whole lattice: each slab's handle calls back (ch4_set_gather) with its block
@@ -155,10 +158,37 @@ def exchange(send_down, send_up, recv_up, recv_down, rank, world, group=None):
         recv_down.copy_(send_up)
         return
     below, above = neighbours(rank, world)
-    ops = [dist.P2POp(dist.isend, send_down, below, group), dist.P2POp(dist.irecv, recv_up, above, group),
-           dist.P2POp(dist.isend, send_up, above, group), dist.P2POp(dist.irecv, recv_down, below, group)]
+    staged = send_down.is_cuda and dist.get_backend(group) == "gloo"
+    if staged:  # gloo moves host memory: device faces through host copies (blocking)
+        import torch
+        torch.cuda.current_stream().synchronize()
+        bufs = [send_down.cpu(), torch.empty(recv_up.shape, dtype=recv_up.dtype), send_up.cpu(),
+                torch.empty(recv_down.shape, dtype=recv_down.dtype)]
+    else:
+        bufs = [send_down, recv_up, send_up, recv_down]
+    ops = [dist.P2POp(dist.isend, bufs[0], below, group), dist.P2POp(dist.irecv, bufs[1], above, group),
+           dist.P2POp(dist.isend, bufs[2], above, group), dist.P2POp(dist.irecv, bufs[3], below, group)]
     for w in dist.batch_isend_irecv(ops):
         w.wait()
+    if staged:
+        recv_up.copy_(bufs[1])
+        recv_down.copy_(bufs[3])
+
+
+def all_gather(whole, local, world, group=None):
+    """whole <- the `local` of every rank in rank order (NCCL on the current stream, or
+    through host memory over gloo)."""
+    import torch
+    import torch.distributed as dist
+    if world == 1:
+        whole.copy_(local)
+    elif local.is_cuda and dist.get_backend(group) == "gloo":
+        torch.cuda.current_stream().synchronize()
+        parts = [torch.empty(local.shape, dtype=local.dtype) for _ in range(world)]
+        dist.all_gather(parts, local.cpu(), group=group)
+        whole.copy_(torch.cat(parts))
+    else:
+        dist.all_gather_into_tensor(whole, local, group=group)
 
 
 class Slab:
@@ -185,11 +215,20 @@ class Slab:
         self._exchange = fn
         self.sim._check(lib().ch4_set_exchange(self.sim.h, C.cast(fn, C.c_void_p), None), "set_exchange")
 
-    def use_process_group(self, rank, world, group=None):
-        """Gather the force sums with an all-gather over the process group (z order = rank
-        order) and swap the LES u faces point to point with the neighbouring ranks."""
+    def set_face_exchange(self, fn):
+        """Register the population-face transfer (an EXCHANGE_FN) that ch4_step runs itself,
+        overlapped with the interior planes; kept alive with the slab."""
+        self._faces = fn
+        self.sim._check(lib().ch4_set_face_exchange(self.sim.h, C.cast(fn, C.c_void_p) if fn else None, None),
+                        "set_face_exchange")
+        self.self_exchanging = fn is not None
+
+    def use_process_group(self, rank, world, group=None, overlap=True):
+        """Over the process group: the force sums all-gathered (z order = rank order), the
+        LES u faces and the population faces swapped point to point with the neighbouring
+        ranks -- NCCL on the handle's streams, or host-staged over gloo.  With `overlap` the
+        population faces move inside ch4_step while the interior planes are stepped."""
         import torch
-        import torch.distributed as dist
 
         def xcb(send_down, send_up, from_up, from_down, nbytes, stream, user):
             try:
@@ -200,15 +239,13 @@ class Slab:
             except Exception:  # noqa: BLE001 - reported to the library as a failed exchange
                 return 1
         self.set_exchange(EXCHANGE_FN(xcb))
+        if overlap:
+            self.set_face_exchange(EXCHANGE_FN(xcb))
 
         def cb(local, all_, nbytes, stream, user):
             try:
                 with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
-                    loc, whole = _view(local, nbytes), _view(all_, nbytes * world)
-                    if world == 1:
-                        whole.copy_(loc)
-                    else:
-                        dist.all_gather_into_tensor(whole, loc, group=group)
+                    all_gather(_view(all_, nbytes * world), _view(local, nbytes), world, group)
                 return 0
             except Exception:  # noqa: BLE001 - reported to the library as a failed gather
                 return 1
@@ -229,9 +266,13 @@ class Slab:
                         "halo_unpack")
 
     def step(self, n, rank, world, group=None):
-        """n steps of a slab of a multi-rank lattice: step, pack, exchange on the
-        handle's stream, unpack."""
+        """n steps of a slab of a multi-rank lattice: with the face exchange registered,
+        ch4_step moves the faces itself; else step, pack, exchange on the handle's stream,
+        unpack."""
         import torch
+        if getattr(self, "self_exchanging", False):
+            self.sim.step(n)
+            return
         stream = torch.cuda.ExternalStream(self.sim.stream_handle)
         for _ in range(n):
             self.sim.step(1)
@@ -281,6 +322,16 @@ def use_local_exchange(slabs):
         s.local_gather = True
 
 
+def use_local_faces(slabs):
+    """Slabs of one process: the population faces move inside every ch4_step, overlapped
+    with the slab's interior planes, swapped between the slabs' threads (step_local then
+    runs the slabs in threads)."""
+    x = LocalExchange(len(slabs))
+    for i, s in enumerate(slabs):
+        s.set_face_exchange(x.callback(i))
+        s.local_gather = True
+
+
 def initialize_local(slabs):
     if any(getattr(s, "local_gather", False) for s in slabs):
         _in_threads(slabs, lambda s: s.sim.initialize())
@@ -293,6 +344,9 @@ def step_local(slabs, n):
     """n steps of the slabs of one process (in z order): every slab unpacks straight
     from its neighbours' send buffers once all have packed."""
     m = len(slabs)
+    if all(getattr(s, "self_exchanging", False) for s in slabs):
+        _in_threads(slabs, lambda s: s.sim.step(n))
+        return
     threaded = any(getattr(s, "local_gather", False) for s in slabs)
     for _ in range(n):
         if threaded:

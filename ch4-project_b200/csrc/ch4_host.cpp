@@ -360,6 +360,9 @@ struct ch4_handle {
   // z-slab with LES: the caller's exchange of the u planes at the faces
   ch4_exchange_fn exchange = nullptr;
   void* exchange_user = nullptr;
+  // z-slab: the caller's transfer of the population faces, run inside ch4_step
+  ch4_exchange_fn face_exchange = nullptr;
+  void* face_user = nullptr;
 
   ch4_status fail(ch4_status s, const char* fmt, ...) {
     char buf[512];
@@ -460,6 +463,9 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.NZ = c.NZ;
   P.N = N;
   P.zoff = c.nz_global > 0 ? c.z_offset : 0;
+  P.zfirst = 0;
+  P.zstride = 1;
+  P.zcount = c.NZ;
   P.Lhit = c.NX + c.NY + (c.nz_global > 0 ? c.nz_global : c.NZ);
   uint32_t F = 0;
   const uint64_t fl = c.flags;
@@ -613,6 +619,11 @@ struct Engine : EngineBase {
   A *kol = nullptr;
   A *ules = nullptr, *tau_les = nullptr;
   A* uhalo = nullptr;  // z-slab LES: u faces sent down | up, received from up | down
+  // z-slab with the face exchange inside the step: the four face buffers (sent down | up,
+  // received from up | down), the stream the transfer runs on and its two events
+  char* faces = nullptr;
+  cudaStream_t comm = nullptr;
+  cudaEvent_t ev_packed = nullptr, ev_moved = nullptr;
   A* vd = nullptr;  // LB_FLUID_LES_VANDRIEST: pow(C_smag(y), 2) per row
   A *hit_ring = nullptr;  // (CHUNK+1) phase-table slots
   A *hit_last = nullptr;  // tables of the latest phases (those of F^n)
@@ -686,6 +697,10 @@ struct Engine : EngineBase {
     cudaFree(ules);
     cudaFree(tau_les);
     cudaFree(uhalo);
+    cudaFree(faces);
+    if (ev_packed) cudaEventDestroy(ev_packed);
+    if (ev_moved) cudaEventDestroy(ev_moved);
+    if (comm) cudaStreamDestroy(comm);
     cudaFree(vd);
     cudaFree(hit_ring);
     cudaFree(hit_last);
@@ -1411,6 +1426,49 @@ struct Engine : EngineBase {
                    "force corrections");
   }
 
+  // One step of a slab that moves its faces itself: the two face planes first, their
+  // leaving populations packed and handed to the caller's transfer on the second stream,
+  // the interior planes stepped meanwhile, the received values unpacked at the end.  The
+  // interior's cells write no slot that the pack reads or the unpack writes (those are
+  // the face planes' slots in the directions that cross the z faces), so the result is
+  // the plain step's.
+  ch4_status step_overlapped() {
+    ch4_status st;
+    const size_t hb = halo_bytes();
+    if (!faces) {
+      if (cudaMalloc(&faces, 4 * hb) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "face buffers");
+      if ((st = H->cuda(cudaStreamCreateWithFlags(&comm, cudaStreamNonBlocking), "face stream"))) return st;
+      if ((st = H->cuda(cudaEventCreateWithFlags(&ev_packed, cudaEventDisableTiming), "face event"))) return st;
+      if ((st = H->cuda(cudaEventCreateWithFlags(&ev_moved, cudaEventDisableTiming), "face event"))) return st;
+    }
+    char *send_down = faces, *send_up = faces + hb, *from_up = faces + 2 * hb, *from_down = faces + 3 * hb;
+    StepParams<A> Q = P;
+    Q.zfirst = 0;
+    Q.zstride = c.NZ > 1 ? c.NZ - 1 : 1;
+    Q.zcount = c.NZ > 1 ? 2 : 1;
+    if ((st = H->cuda(launch_step(Q, shape, H->stream), "lb_step faces"))) return st;
+    // pack reads the state this step writes: the output buffer
+    const int keep = cur;
+    cur ^= 1;
+    st = halo(true, send_down, send_up);
+    cur = keep;
+    if (st) return st;
+    if ((st = H->cuda(cudaEventRecord(ev_packed, H->stream), "faces packed"))) return st;
+    if ((st = H->cuda(cudaStreamWaitEvent(comm, ev_packed, 0), "face stream wait"))) return st;
+    if (H->face_exchange(send_down, send_up, from_up, from_down, hb, comm, H->face_user) != 0)
+      return H->fail(CH4_ERR_CUDA, "the exchange of the slabs' faces failed");
+    if ((st = H->cuda(cudaEventRecord(ev_moved, comm), "faces moved"))) return st;
+    Q.zfirst = 1;
+    Q.zstride = 1;
+    Q.zcount = c.NZ - 2;
+    if ((st = H->cuda(launch_step(Q, shape, H->stream), "lb_step interior"))) return st;
+    if ((st = H->cuda(cudaStreamWaitEvent(H->stream, ev_moved, 0), "faces wait"))) return st;
+    cur ^= 1;
+    st = halo(false, from_up, from_down);
+    cur = keep;
+    return st;
+  }
+
   ch4_status les_u() {
     // u^n with dt/2 F^{n-1}: prev tables are P.hit_prev
     ch4_status st = H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, nullptr, nullptr,
@@ -1500,7 +1558,11 @@ struct Engine : EngineBase {
         }
         if (c.flags & CH4_F_FLUID_LES)
           if ((st = les_u())) return st;
-        if ((st = H->cuda(launch_step(P, shape, H->stream), "lb_step"))) return st;
+        if (H->face_exchange) {
+          if ((st = step_overlapped())) return st;
+        } else if ((st = H->cuda(launch_step(P, shape, H->stream), "lb_step"))) {
+          return st;
+        }
         if (fmoments()) fm_i ^= 1;
         cur ^= 1;
         H->itime++;
@@ -2339,6 +2401,14 @@ ch4_status ch4_set_exchange(ch4_handle* h, ch4_exchange_fn exchange, void* user)
   if (h->cfg.nz_global <= 0) return h->fail(CH4_ERR_ARG, "ch4_set_exchange is for z-slab handles");
   h->exchange = exchange;
   h->exchange_user = user;
+  return CH4_OK;
+}
+
+ch4_status ch4_set_face_exchange(ch4_handle* h, ch4_exchange_fn exchange, void* user) {
+  if (!h) return CH4_ERR_ARG;
+  if (h->cfg.nz_global <= 0) return h->fail(CH4_ERR_ARG, "ch4_set_face_exchange is for z-slab handles");
+  h->face_exchange = exchange;
+  h->face_user = user;
   return CH4_OK;
 }
 

@@ -96,6 +96,10 @@ struct StepParams {
   int NX, NY, NZ;
   long long N;  // cells
   int zoff;     // global z of plane 0 (z-slab of a larger lattice), else 0
+  // planes of one launch of the step kernel: zfirst + k * zstride, k < zcount (the whole
+  // lattice: 0, 1, NZ; a slab that overlaps its face exchange steps its two face planes
+  // and then its interior)
+  int zfirst, zstride, zcount;
   int Lhit;     // NX + NY + global NZ: length of one HIT table row
   uint32_t feat;
   uint32_t walls;  // W_* bits

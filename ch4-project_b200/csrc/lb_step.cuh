@@ -468,7 +468,7 @@ template <typename S, typename A, bool THERM, bool SCAL, int V = 0>
 __global__ void __launch_bounds__(128) lb_step_kernel(const __grid_constant__ StepParams<A> P) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
-  lb_cell<S, A, THERM, SCAL, V>(P, x, blockIdx.y, blockIdx.z);
+  lb_cell<S, A, THERM, SCAL, V>(P, x, blockIdx.y, P.zfirst + (int)blockIdx.z * P.zstride);
 }
 
 // The FP64 BGK step with two population sets, held to 128 registers (four 128-thread
@@ -479,5 +479,5 @@ template <typename S, typename A, bool THERM, bool SCAL>
 __global__ void __launch_bounds__(128, 4) lb_step_kernel_cap128(const __grid_constant__ StepParams<A> P) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
-  lb_cell<S, A, THERM, SCAL, 0>(P, x, blockIdx.y, blockIdx.z);
+  lb_cell<S, A, THERM, SCAL, 0>(P, x, blockIdx.y, P.zfirst + (int)blockIdx.z * P.zstride);
 }

@@ -366,6 +366,16 @@ typedef int (*ch4_exchange_fn)(const void *send_down, const void *send_up, void 
                                size_t bytes, void *stream, void *user);
 ch4_status ch4_set_exchange(ch4_handle *h, ch4_exchange_fn exchange, void *user);
 
+/* The population faces moved inside ch4_step, overlapped with the interior: with
+ * `exchange` registered, every step of a slab handle streams its two face planes first,
+ * packs what leaves through them (as ch4_halo_pack), calls `exchange` with the four face
+ * buffers (halo_bytes each: send_down, send_up, from_up, from_down) and the handle's
+ * second stream, on which the transfer must be ordered, steps the interior planes while
+ * it runs, and unpacks what arrived (as ch4_halo_unpack) before the step ends.  The
+ * caller then calls ch4_step alone, no ch4_halo_pack / ch4_halo_unpack.  NULL switches it
+ * off.  Replaces, with sendrecv_borders_pop (src/lb.c:733-1058), the MPI face exchange. */
+ch4_status ch4_set_face_exchange(ch4_handle *h, ch4_exchange_fn exchange, void *user);
+
 /* --- Lagrangian averages per particle type (dump_particle_averages) ------------ */
 
 /* Per type: the particle count, then the means of v, v^2, v^4, a, a^2, a^4 (per
