@@ -691,10 +691,8 @@ def main():
         if slab_mode:
             s = slabmod.Slab(gcfg, rank * NZ, NZ)
             # the faces move inside ch4_step, overlapped with the slab's interior planes
-            if world > 1:
-                s.use_process_group(rank, world)
-            else:
-                slabmod.use_local_faces([s])
+            # (one rank: the slab's own faces, a device copy on the handle's second stream)
+            s.use_process_group(rank, world)
             return s.sim, (lambda n: s.step(n, rank, world))
         s = ch4b200.Simulation(cfg)
         return s, s.step
