@@ -15,6 +15,7 @@ module, and only as the checker / the timed CPU reference.
 import ctypes as C
 import json
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -303,16 +304,21 @@ def particle_averages(part, types):
     return out
 
 
-def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None, parts=None, params=None):
+def run_reference(flagset, cfg, nsteps, pops, phi=None, seed=None, workdir=None, parts=None, params=None,
+                  patched=False):
     """Run the compiled reference on injected populations.
 
     pops: dict which -> AoS array [NZ][NY][NX][NPOP] (interior cells).
+    patched: the build with the library's integration patch (ch4ref_b200: the time loop on
+    the GPU through include/ch4.h); its define.h is the flag set's header.
     Returns dict of output arrays (AoS / per-cell) and the timing record.
     """
-    exe = ref_binary(flagset)
+    exe = ref_binary(flagset) + ("_b200" if patched else "")
     if not os.path.exists(exe):
         raise FileNotFoundError(exe)
     tmp = workdir or tempfile.mkdtemp(prefix="ch4ref_")
+    if patched:
+        shutil.copyfile(os.path.join(HERE, "configs", flagset + ".h"), os.path.join(tmp, "define.h"))
     write_param_in(os.path.join(tmp, "param.in"), cfg, nsteps, params)
     for which, arr in pops.items():
         np.ascontiguousarray(arr, dtype=np.float64).tofile(os.path.join(tmp, "in_%s.bin" % which))
