@@ -114,6 +114,7 @@ FLAGS2 = {
     "LAGRANGE_SMALLTAUD_BETA": 1 << 25,
     "LAGRANGE_SMALLTAUD_FLOATER": 1 << 26,
     "LAGRANGE_TWOWAY_SMALLTAUD": 1 << 27,
+    "LB_FLUID_LES_SMAGORINSKY_LILLY": 1 << 28,
 }
 
 

@@ -151,7 +151,8 @@ const uint64_t SUPPORTED2 =
     CH4_F2_LAGRANGE_BC_INELASTIC | CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT |
     CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM | CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO |
     CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF | CH4_F2_LAGRANGE_SMALLTAUD |
-    CH4_F2_LAGRANGE_SMALLTAUD_BETA | CH4_F2_LAGRANGE_SMALLTAUD_FLOATER | CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD;
+    CH4_F2_LAGRANGE_SMALLTAUD_BETA | CH4_F2_LAGRANGE_SMALLTAUD_FLOATER | CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD |
+    CH4_F2_FLUID_LES_SMAGORINSKY_LILLY;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -496,6 +497,7 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   if (fl & CH4_F_SCALAR_LES) F |= K_SLES;
   if (fl & CH4_F_FLUID_LES_WALE) F |= K_WALE;
   if (fl & CH4_F_FLUID_LES_LOCAL_STRAIN) F |= K_LSTRAIN;
+  if (c.flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) F |= K_LILLY;
   P.feat = F;
   uint32_t WB = 0;
   const uint64_t f2 = c.flags2;
@@ -537,6 +539,7 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.hdt = (A)(0.5 * c.time_dt);
   P.nu = (A)c.nu;
   P.csmag2 = (A)std::pow(c.C_smag * 1.0, 2.0);
+  P.lilly_bg = (A)(c.beta_t * c.gravity_y);
   P.kappa = (A)c.kappa;
   P.chi = (A)c.chi;
   P.tau_u = (A)c.tau_u;
@@ -618,6 +621,7 @@ struct Engine : EngineBase {
   A *tprev = nullptr, *sprev = nullptr;
   A *kol = nullptr;
   A *ules = nullptr, *tau_les = nullptr;
+  double* lest = nullptr;  // Smagorinsky-Lilly: t^n
   A* uhalo = nullptr;  // z-slab LES: u faces sent down | up, received from up | down
   // z-slab with the face exchange inside the step: the four face buffers (sent down | up,
   // received from up | down), the stream the transfer runs on and its two events
@@ -695,6 +699,7 @@ struct Engine : EngineBase {
     cudaFree(sprev);
     cudaFree(kol);
     cudaFree(ules);
+    cudaFree(lest);
     cudaFree(tau_les);
     cudaFree(uhalo);
     cudaFree(faces);
@@ -1152,6 +1157,8 @@ struct Engine : EngineBase {
     if (c.flags & CH4_F_FLUID_LES) {
       if (cudaMalloc(&ules, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
       if (cudaMalloc(&tau_les, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tau_les");
+      if ((c.flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) && cudaMalloc(&lest, N * sizeof(double)) != cudaSuccess)
+        return H->fail(CH4_ERR_NOMEM, "Lilly t");
       if (c.flags & CH4_F_FLUID_LES_VANDRIEST) {
         // C_smag(y) of src/les.c:136-142: the test is on the row index with the LES halo
         // (BRD = 2, src/typedef.h:317), the distance on the cell centre y = j + 0.5
@@ -1217,6 +1224,7 @@ struct Engine : EngineBase {
     P.tprev = tprev;
     P.sprev = sprev;
     P.ules = ules;
+    P.les_t = lest;
     P.ules_lo = P.ules_hi = nullptr;
     P.tau_les = tau_les;
     P.kol = kol;
@@ -1471,7 +1479,8 @@ struct Engine : EngineBase {
 
   ch4_status les_u() {
     // u^n with dt/2 F^{n-1}: prev tables are P.hit_prev
-    ch4_status st = H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, nullptr, nullptr,
+    // (with Smagorinsky-Lilly also t^n = m(g^n), the reference's t at the collision)
+    ch4_status st = H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, lest, nullptr,
                                          nullptr, ules, H->stream),
                             "les u");
     if (st || c.nz_global <= 0) return st;
@@ -1921,6 +1930,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_SMALLTAUD_BETA", CH4_F2_LAGRANGE_SMALLTAUD_BETA},
       {"LAGRANGE_SMALLTAUD_FLOATER", CH4_F2_LAGRANGE_SMALLTAUD_FLOATER},
       {"LAGRANGE_TWOWAY_SMALLTAUD", CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD},
+      {"LB_FLUID_LES_SMAGORINSKY_LILLY", CH4_F2_FLUID_LES_SMAGORINSKY_LILLY},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2030,6 +2040,12 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
                                   CH4_F_FLUID_LES_WALE | CH4_F_FLUID_LES_LOCAL_STRAIN;
     if ((c->flags & les_variants) && !(c->flags & CH4_F_FLUID_LES))
       return why = "LES variants need LB_FLUID_LES", CH4_ERR_UNSUPPORTED;
+    // Smagorinsky-Lilly reads t = m(g); with LB_TEMPERATURE_FORCING the reference's t carries
+    // half the source as well (src/lb.c:490-496): not built
+    if ((c->flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) &&
+        (!(c->flags & CH4_F_FLUID_LES) || !(c->flags & CH4_F_LB_TEMPERATURE) || (c->flags & CH4_F_TEMPERATURE_FORCING)))
+      return why = "LB_FLUID_LES_SMAGORINSKY_LILLY needs LB_FLUID_LES and LB_TEMPERATURE, without LB_TEMPERATURE_FORCING",
+             CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_TEMPERATURE_LES) && !(c->flags & CH4_F_LB_TEMPERATURE))
       return why = "LB_TEMPERATURE_LES needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_SCALAR_LES) && !(c->flags & CH4_F_LB_SCALAR))

@@ -70,7 +70,8 @@ enum : uint32_t {
   K_TLES = 1u << 23,       // LB_TEMPERATURE_LES: thermal relaxation time from the LES one
   K_SLES = 1u << 24,       // LB_SCALAR_LES: scalar relaxation time from the LES one
   K_WALE = 1u << 25,       // LB_FLUID_LES_WALE: WALE eddy viscosity
-  K_LSTRAIN = 1u << 26     // LB_FLUID_LES_LOCAL_STRAIN: |S| from the populations' stress tensor
+  K_LSTRAIN = 1u << 26,    // LB_FLUID_LES_LOCAL_STRAIN: |S| from the populations' stress tensor
+  K_LILLY = 1u << 27       // LB_FLUID_LES_SMAGORINSKY_LILLY: |S| damped by the stratification
 };
 
 // walls on x and z (those on y are K_FWALL / K_TWALL / K_SWALL of `feat`)
@@ -118,6 +119,9 @@ struct StepParams {
   const A* ules_lo;  // z-slab: u of the plane under the slab (3 planes of NX*NY), else null
   const A* ules_hi;  // z-slab: u of the plane over the slab
   A* tau_les;
+  // LB_FLUID_LES_SMAGORINSKY_LILLY: t^n = m(g^n) (one FP64 plane) and beta_t * gravity_y
+  const double* les_t;
+  A lilly_bg;
   // two-way coupling deposit of this and the previous step (3 SoA planes each)
   const A* dcur;
   const A* dprev;

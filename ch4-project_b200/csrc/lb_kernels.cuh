@@ -264,6 +264,26 @@ __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z
                             (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
                             (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
   }
+  if (F & K_LILLY) {
+    // Smagorinsky-Lilly (src/les.c:156-176): Ri = beta_t g_y (dT/dy)^+ / |S|^2, |S| times
+    // sqrt(1 - Ri) for Ri < 1, else 0.  dT/dy of gradient_scalar: one-sided at the y
+    // walls of the temperature or scalar, centred (periodic) elsewhere.  The reference
+    // squares |S| with the host pow (within an ulp of the product here)
+    const double* t = P.les_t;
+    auto tv = [&](int j) { return A(t[((long long)z * NY + j) * NX + x]); };
+    A gy;
+    const bool wy = (F & (K_TWALL | K_SWALL)) != 0;
+    if (wy && y == 0)
+      gy = A(-1.5) * tv(0) + A(2) * tv(1) + A(-0.5) * tv(2);
+    else if (wy && y == NY - 1)
+      gy = A(1.5) * tv(NY - 1) + A(-2) * tv(NY - 2) + A(0.5) * tv(NY - 3);
+    else
+      gy = (tv(wrap(y + 1, NY)) - tv(wrap(y - 1, NY))) / A(2);
+    const A N2 = gy < A(0) ? A(0) : P.lilly_bg * gy;
+    const A Ri = N2 / (s_norm * s_norm);
+    const A Cb = Ri < A(1) ? sqrt(A(1) - Ri / A(1)) : A(0);
+    s_norm = s_norm * Cb;
+  }
   A nu_les = s_norm * ((F & K_VANDRIEST) ? P.csmag2_y[y] : P.csmag2);
   if (F & K_WALE) {  // Nicoud & Ducros 1999, src/les.c:182-248 (C_wale = 0.5)
     const A Sxx = xx, Syy = yy, Szz = zz;

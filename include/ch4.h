@@ -160,7 +160,10 @@ enum {
   CH4_F2_LAGRANGE_SMALLTAUD_FLOATER = 1ull << 26,
   /* two-way force of the small-tau_drag model, (Du/Dt - g)(1 - rho_p/rho_f),
    * src/lagrange_feedback.c:106-110 */
-  CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD = 1ull << 27
+  CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD = 1ull << 27,
+  /* Smagorinsky-Lilly: |S| damped by the buoyancy of a stable stratification,
+   * sqrt(1 - Ri) with Ri = beta_t g_y (dT/dy)^+ / |S|^2, src/les.c:156-176 */
+  CH4_F2_FLUID_LES_SMAGORINSKY_LILLY = 1ull << 28
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */

@@ -290,11 +290,34 @@ static double vandriest(const ch4o_state *s, int j) {
   return c->C_smag * (1.0 - exp((-(c->Amp_x * ((c->SY - yc))) / c->nu) / 26.0));
 }
 
-static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k, const double *f, double rho,
-                      double ux, double uy, double uz, double u2, double tau_prev) {
+/* LB_FLUID_LES_SMAGORINSKY_LILLY (src/les.c:156-176): |S| times
+ * Cb = sqrt(1 - Ri/Pr) (0 for Ri >= 1), Ri = N^2 / pow(|S|, 2), N^2 = beta_t g_y dT/dy for a
+ * stable stratification (dT/dy >= 0), else 0; dT/dy of gradient_scalar(t^n) */
+static double lilly(const ch4o_state *s, const double *t, int i, int j, int k, double s_norm) {
+  const double gy = grad_field(s, t, 1, 0, 1, i, j, k, scalar_walls(&s->cfg));
+  double N2;
+  if (gy < 0) {
+    N2 = 0;
+  } else {
+    N2 = s->cfg.beta_t * s->cfg.gravity_y * gy;
+  }
+  const double Ri = N2 / pow(s_norm, 2.0);
+  const double prandtl = 1.0;
+  double Cb;
+  if (Ri < 1) {
+    Cb = sqrt(1 - (Ri / prandtl));
+  } else {
+    Cb = 0;
+  }
+  return s_norm * Cb;
+}
+
+static double les_tau(const ch4o_state *s, const double *u, const double *t, int i, int j, int k, const double *f,
+                      double rho, double ux, double uy, double uz, double u2, double tau_prev) {
   const int NX = s->NX, NY = s->NY, NZ = s->NZ;
   const uint64_t fl = s->cfg.flags;
   const int walls = fluid_walls(&s->cfg);
+  const int lil = (s->cfg.flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) != 0;
   if (fl & CH4_F_FLUID_LES_LOCAL_STRAIN) {
     double Sxx = 0, Syy = 0, Szz = 0, Sxy = 0, Sxz = 0, Syz = 0;
     for (int pp = 0; pp < NPOP; pp++) {
@@ -316,6 +339,7 @@ static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k,
                                             Szx * Szx + Szy * Szy + Szz * Szz));
     double C_smag = s->cfg.C_smag;
     if (fl & CH4_F_FLUID_LES_VANDRIEST) C_smag = vandriest(s, j);
+    if (lil) s_norm = lilly(s, t, i, j, k, s_norm);
     double nu_les = s_norm * pow(C_smag * 1.0, 2.0);
     return 3.0 * (nu_les + s->cfg.nu) + 0.5;
   }
@@ -335,6 +359,7 @@ static double les_tau(const ch4o_state *s, const double *u, int i, int j, int k,
   double vol = 1.0; /* (dx*dy*dz)^(1/3) on the unit lattice */
   double C_smag = s->cfg.C_smag;
   if (fl & CH4_F_FLUID_LES_VANDRIEST) C_smag = vandriest(s, j);
+  if (lil) s_norm = lilly(s, t, i, j, k, s_norm);
   double nu_les = s_norm * pow(C_smag * vol, 2.0);
   if (fl & CH4_F_FLUID_LES_WALE) { /* src/les.c:182-248 */
     double SSxx = xx, SSyy = yy, SSzz = zz;
@@ -1208,10 +1233,13 @@ static void one_step(ch4o_state *s) {
   }
 
   /* u^n field (needed by LES gradients, src/fluid.c:1056-1075) */
-  double *uarr = NULL;
+  double *uarr = NULL, *tarr = NULL;
   if (c->flags & CH4_F_FLUID_LES) {
     uarr = (double *)malloc(sizeof(double) * 3 * N);
-    hydro(s, s->hit_prev, s->dprev, s->fm_prev, NULL, uarr, NULL, NULL);
+    /* t^n = m(g^n) for the Smagorinsky-Lilly correction (its halo the periodic copy,
+     * src/fluid.c:1058-1061) */
+    if (c->flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) tarr = (double *)malloc(sizeof(double) * N);
+    hydro(s, s->hit_prev, s->dprev, s->fm_prev, NULL, uarr, tarr, NULL);
   }
 
   const double invtau_u = 1.0 / c->tau_u;
@@ -1254,7 +1282,7 @@ static void one_step(ch4o_state *s) {
         double invtau = invtau_u;
         double invtau_cell[3] = {invtau_set[0], invtau_set[1], invtau_set[2]};
         if (c->flags & CH4_F_FLUID_LES) {
-          double tl = les_tau(s, uarr, i, j, k, a, rho, ux, uy, uz, u2, s->tau_les[idx]);
+          double tl = les_tau(s, uarr, tarr, i, j, k, a, rho, ux, uy, uz, u2, s->tau_les[idx]);
           s->tau_les[idx] = tl;
           invtau = 1.0 / tl;
           /* tau_t_les / tau_s_les (src/les.c:273-326), turbulent Prandtl and Schmidt 1 */
@@ -1407,6 +1435,7 @@ static void one_step(ch4o_state *s) {
     s->fn[set] = tmp;
   }
   free(uarr);
+  free(tarr);
 
   /* Lagrangian sub-steps, src/main.c:164-185: u^{n+1} with dt/2 F^n, then
    * interpolate + move + wrap time_dt_lagr_factor times */

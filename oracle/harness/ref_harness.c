@@ -259,7 +259,9 @@ int main(int argc, char **argv) {
   }
 #endif
 
-  /* src/main.c:24-48 */
+  /* src/main.c:24-48 (with the integration patch ch4_initialize does this on the GPU,
+     from the state and phases as initial_conditions and initialization_forcing left them) */
+#ifndef CH4_B200
 #ifdef LB_FLUID
   hydro_fields('p');
 #endif
@@ -281,6 +283,7 @@ int main(int argc, char **argv) {
   hydro_fields('h');
 #endif
 #endif
+#endif /* CH4_B200 */
 
 #ifdef LAGRANGE
   {

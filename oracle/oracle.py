@@ -137,6 +137,9 @@ FLAGSETS.update({
                      "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT",
                      "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY", "LAGRANGE_SMALLTAUD", "LAGRANGE_SMALLTAUD_FLOATER",
                      "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    # Smagorinsky-Lilly in a stably stratified channel
+    "les_lilly": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
+                  "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SMAGORINSKY_LILLY"],
 })
 # a wall of a kind implies its umbrella flag, as in every define.h of the reference
 for _names in FLAGSETS.values():

@@ -108,6 +108,10 @@ CASES = {
                          params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=18,
                                      T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3, gravity_x=3e-4,
                                      time_dt_lagr_factor=2.0, particle_number=250)),
+    # Smagorinsky-Lilly: T rising with y (stable), so the buoyancy damps |S| where Ri < 1
+    "les_lilly": dict(flagset="les_lilly", NX=8, NY=9, NZ=6,
+                      params=dict(tau_u=0.52, tau_t=0.55, Amp_x=0.02, T_bot=0.0, T_top=1.0, T_ref=0.5, beta_t=0.3,
+                                  gravity_y=1e-3, gravity_x=0.0)),
     # walls on x and z
     "duct": dict(flagset="duct", NX=7, NY=8, NZ=6,
                  params=dict(tau_u=0.6, Amp_x=4e-3, Amp_y=1e-3, Amp_z=2e-3)),
@@ -155,7 +159,7 @@ def make_case(name, seed=0, storage=0, dims=None, **over):
     params.update(O.FLAGSET_EXTRA.get(c["flagset"], {}))
     cfg = O.make_config(c["NX"], c["NY"], c["NZ"], flags, storage=storage, **params)
     rng = np.random.default_rng(seed)
-    state = {"p": pops(rng, c["NX"], c["NY"], c["NZ"], 1.0, 3e-2 if name == "les" else 1e-2)}
+    state = {"p": pops(rng, c["NX"], c["NY"], c["NZ"], 1.0, 3e-2 if name in ("les", "les_lilly") else 1e-2)}
     if "LB_TEMPERATURE" in flags:
         state["g"] = rb_temperature_pops(rng, c["NX"], c["NY"], c["NZ"], cfg.T_bot, cfg.T_top, 1e-2)
     if "LB_SCALAR" in flags:

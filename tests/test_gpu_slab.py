@@ -111,6 +111,7 @@ def test_uneven_slabs_with_global_force_corrections(name):
 
 
 @pytest.mark.parametrize("name,nslabs", [("les", 2), ("les_vd", 3), ("les_ls", 2), ("les_wale", 2), ("les_ts", 2),
+                                          ("les_lilly", 2),
                                           ("trt_les", 3)])
 def test_les_slabs_reproduce_the_single_lattice(name, nslabs):
     """LES on slabs: the u planes beyond each face swapped in the middle of the step

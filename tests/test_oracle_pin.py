@@ -30,7 +30,7 @@ def _assert_same(a, b, what):
                                           ("cpower", 15), ("duct", 20), ("duct_les", 20), ("box", 20),
                                           ("slipx", 20), ("slipz", 20), ("particles_tt", 8), ("particles_ttc", 8),
                                           ("particles_rb", 8), ("particles_duct", 8), ("particles_slip", 8),
-                                          ("particles_reinj", 8), ("particles_bc", 8)])
+                                          ("particles_reinj", 8), ("particles_bc", 8), ("les_lilly", 20)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
