@@ -341,8 +341,9 @@ __device__ __forceinline__ void interp_fields(const PartParams<A>& P, const Sten
 // 1.5 L2 - 2 L1 + 0.5 L0 (LAGRANGE_INTERPOLATION_FIX, src/gradients.c:370-489, 728-826).
 // Arithmetic in the storage precision: FP64 reproduces the reference bit for bit; the
 // FP32 path interpolates in FP32, as its lattice arithmetic.
-struct PBlock {  // cell offsets (lattices hold fewer than 2^31 cells)
-  int zo[4], yo[4], xo[4];
+struct PBlock {
+  long long zo[4];
+  int yo[4], xo[4];
 };
 
 // corner index of the reference's order for corner (di, dj, dk)
@@ -361,7 +362,7 @@ __device__ __forceinline__ void load_line(const C* __restrict__ ut4, const PBloc
                                           C (*L)[NF]) {
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    const int c = axis == 0 ? o.zo[b] + o.yo[a] + o.xo[q]
+    const long long c = axis == 0 ? o.zo[b] + o.yo[a] + o.xo[q]
                         : axis == 1 ? o.zo[b] + o.yo[q] + o.xo[a]
                                     : o.zo[q] + o.yo[b] + o.xo[a];
     double w[4];
@@ -381,7 +382,7 @@ __device__ __forceinline__ void interp_lines(const PartParams<C>& P, const Stenc
   for (int q = 0; q < 4; q++) {
     o.xo[q] = pmod(t.im - 1 + q, P.NX);
     o.yo[q] = pmod(t.jm - 1 + q, P.NY) * P.NX;
-    o.zo[q] = pmod(t.km - 1 + q, P.NZ) * P.NX * P.NY;
+    o.zo[q] = (long long)pmod(t.km - 1 + q, P.NZ) * P.NX * P.NY;
   }
   if constexpr (GRAD) {  // the cells only the y and z passes read: on their way while x runs
 #pragma unroll
