@@ -3181,11 +3181,14 @@ ch4_status ens_rebuild(ch4_ensemble* E) {
   for (int i = 0; i < (int)E->slots.size(); i++) {
     const Slot& s = E->slots[i];
     if (!s.used || !s.initialized) continue;
-    for (int y0 = 0; y0 < s.cfg.NY; y0 += E->rows) tiles.push_back({i, y0, std::min(E->rows, s.cfg.NY - y0), 0});
+    // tiles of `rows` lines (y + NY z) each, so a 3-D lattice spreads over as many CTAs as a
+    // quasi-2-D one of the same size
+    const int lines = s.cfg.NY * s.cfg.NZ;
+    for (int l0 = 0; l0 < lines; l0 += E->rows) tiles.push_back({i, l0, std::min(E->rows, lines - l0), 0});
   }
   std::stable_sort(tiles.begin(), tiles.end(), [&](const EnsTile& a, const EnsTile& b) {
     const Slot &sa = E->slots[a.slot], &sb = E->slots[b.slot];
-    return (long long)sa.cfg.NX * a.ny * sa.cfg.NZ > (long long)sb.cfg.NX * b.ny * sb.cfg.NZ;
+    return (long long)sa.cfg.NX * a.ny > (long long)sb.cfg.NX * b.ny;
   });
   ch4_status st;
   if ((int)tiles.size() > E->tiles_cap) {

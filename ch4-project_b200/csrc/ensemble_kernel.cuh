@@ -24,23 +24,27 @@ __global__ void __launch_bounds__(256) ensemble_step_kernel(const StepParams<A>*
     int* dst = reinterpret_cast<int*>(&sp);
     for (int w = threadIdx.x; w < WORDS; w += blockDim.x) dst[w] = src[w];
     __syncthreads();
-    const int NX = sp.NX, rows = tl.ny, NZ = sp.NZ;
-    const int ncell = NX * rows * NZ;
-    // cell i = x + NX * (r + rows * z), advanced by blockDim.x without dividing per cell
-    const int dx = (int)blockDim.x % NX, drow = (int)blockDim.x / NX;
-    int x = (int)threadIdx.x % NX, row = (int)threadIdx.x / NX;  // row = r + rows * z
-    int r = row % rows, z = row / rows;
+    // a tile is tl.ny consecutive lines (a line: the NX cells of one (y, z)) from line tl.y0
+    // in z-major order, line = y + NY z: rows of one plane for a quasi-2-D lattice, and a
+    // 3-D lattice splits into NY NZ / rows tiles as well
+    const int NX = sp.NX, NY = sp.NY;
+    const int ncell = NX * tl.ny;
+    // cell i = x + NX * r, advanced by blockDim.x without dividing per cell
+    const int dx = (int)blockDim.x % NX, dline = (int)blockDim.x / NX;
+    int x = (int)threadIdx.x % NX;
+    const int line0 = tl.y0 + (int)threadIdx.x / NX;
+    int y = line0 % NY, z = line0 / NY;
     for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
-      lb_cell<S, A, THERM, SCAL>(sp, x, tl.y0 + r, z);
+      lb_cell<S, A, THERM, SCAL>(sp, x, y, z);
       x += dx;
-      r += drow;
+      y += dline;
       if (x >= NX) {
         x -= NX;
-        r += 1;
+        y += 1;
       }
-      if (r >= rows) {
-        z += r / rows;
-        r %= rows;
+      while (y >= NY) {
+        y -= NY;
+        z += 1;
       }
     }
     __syncthreads();  // sp and tile_id are reused by the next tile
