@@ -620,8 +620,7 @@ struct Engine : EngineBase {
   bool filling = false;
   A *tprev = nullptr, *sprev = nullptr;
   A *kol = nullptr;
-  A *ules = nullptr, *tau_les = nullptr;
-  double* lest = nullptr;  // Smagorinsky-Lilly: t^n
+  A *ules = nullptr, *tau_les = nullptr;  // LES: u^n as (u_x, u_y, u_z, t^n) per cell
   A* uhalo = nullptr;  // z-slab LES: u faces sent down | up, received from up | down
   // z-slab with the face exchange inside the step: the four face buffers (sent down | up,
   // received from up | down), the stream the transfer runs on and its two events
@@ -699,7 +698,6 @@ struct Engine : EngineBase {
     cudaFree(sprev);
     cudaFree(kol);
     cudaFree(ules);
-    cudaFree(lest);
     cudaFree(tau_les);
     cudaFree(uhalo);
     cudaFree(faces);
@@ -1155,10 +1153,8 @@ struct Engine : EngineBase {
         return H->fail(CH4_ERR_CUDA, "force corrections");
     }
     if (c.flags & CH4_F_FLUID_LES) {
-      if (cudaMalloc(&ules, 3 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
+      if (cudaMalloc(&ules, 4 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
       if (cudaMalloc(&tau_les, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tau_les");
-      if ((c.flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) && cudaMalloc(&lest, N * sizeof(double)) != cudaSuccess)
-        return H->fail(CH4_ERR_NOMEM, "Lilly t");
       if (c.flags & CH4_F_FLUID_LES_VANDRIEST) {
         // C_smag(y) of src/les.c:136-142: the test is on the row index with the LES halo
         // (BRD = 2, src/typedef.h:317), the distance on the cell centre y = j + 0.5
@@ -1224,7 +1220,6 @@ struct Engine : EngineBase {
     P.tprev = tprev;
     P.sprev = sprev;
     P.ules = ules;
-    P.les_t = lest;
     P.ules_lo = P.ules_hi = nullptr;
     P.tau_les = tau_les;
     P.kol = kol;
@@ -1479,25 +1474,26 @@ struct Engine : EngineBase {
 
   ch4_status les_u() {
     // u^n with dt/2 F^{n-1}: prev tables are P.hit_prev
-    // (with Smagorinsky-Lilly also t^n = m(g^n), the reference's t at the collision)
-    ch4_status st = H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, lest, nullptr,
-                                         nullptr, ules, H->stream),
+    // one (u_x, u_y, u_z, t) vector per cell; t^n = m(g^n), the reference's t at the
+    // collision, only for Smagorinsky-Lilly
+    const int lil = (c.flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) != 0;
+    ch4_status st = H->cuda(launch_hydro(P, shape, P.hit_prev, P.dprev, P.fm_prev, nullptr, nullptr, nullptr, nullptr,
+                                         nullptr, nullptr, H->stream, ules, lil),
                             "les u");
     if (st || c.nz_global <= 0) return st;
     // z-slab: u of the bottom plane down, of the top plane up, the neighbours' back
     if (!H->exchange) return H->fail(CH4_ERR_STATE, "z-slab with LES: no ch4_set_exchange");
-    const size_t nxy = (size_t)c.NX * c.NY, part = 3 * nxy;
+    // (the face planes of the vector array are contiguous: one copy each)
+    const size_t nxy = (size_t)c.NX * c.NY, part = 4 * nxy;
     if (!uhalo && cudaMalloc(&uhalo, 4 * part * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u halo");
     A *send_down = uhalo, *send_up = uhalo + part, *from_up = uhalo + 2 * part, *from_down = uhalo + 3 * part;
     HaloCopy hc{};
-    for (int a = 0; a < 3; a++) {
-      hc.src[hc.n] = ules + (size_t)a * N;
-      hc.dst[hc.n] = send_down + (size_t)a * nxy;
-      hc.bytes[hc.n++] = nxy * sizeof(A);
-      hc.src[hc.n] = ules + (size_t)a * N + (size_t)(c.NZ - 1) * nxy;
-      hc.dst[hc.n] = send_up + (size_t)a * nxy;
-      hc.bytes[hc.n++] = nxy * sizeof(A);
-    }
+    hc.src[hc.n] = ules;
+    hc.dst[hc.n] = send_down;
+    hc.bytes[hc.n++] = part * sizeof(A);
+    hc.src[hc.n] = ules + (size_t)(c.NZ - 1) * part;
+    hc.dst[hc.n] = send_up;
+    hc.bytes[hc.n++] = part * sizeof(A);
     if ((st = H->cuda(launch_halo_copy(hc, H->stream), "u faces"))) return st;
     if (H->exchange(send_down, send_up, from_up, from_down, part * sizeof(A), H->stream, H->exchange_user) != 0)
       return H->fail(CH4_ERR_CUDA, "the exchange of the slabs' u planes failed");

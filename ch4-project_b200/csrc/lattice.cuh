@@ -114,13 +114,12 @@ struct StepParams {
   // previous-step temperature / scalar (t^{n-1}), read and overwritten in place
   A* tprev;
   A* sprev;
-  // LES: u^n (3 SoA planes) and per-cell relaxation time output
+  // LES: u^n as (u_x, u_y, u_z, t^n) per cell and per-cell relaxation time output
   const A* ules;
-  const A* ules_lo;  // z-slab: u of the plane under the slab (3 planes of NX*NY), else null
+  const A* ules_lo;  // z-slab: the vectors of the plane under the slab (NX*NY), else null
   const A* ules_hi;  // z-slab: u of the plane over the slab
   A* tau_les;
-  // LB_FLUID_LES_SMAGORINSKY_LILLY: t^n = m(g^n) (one FP64 plane) and beta_t * gravity_y
-  const double* les_t;
+  // LB_FLUID_LES_SMAGORINSKY_LILLY: beta_t * gravity_y (t^n is the fourth component of ules)
   A lilly_bg;
   // two-way coupling deposit of this and the previous step (3 SoA planes each)
   const A* dcur;

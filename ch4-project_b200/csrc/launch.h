@@ -21,15 +21,16 @@ cudaError_t launch_step(const StepParams<float>& P, LaunchShape s, cudaStream_t 
 cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStream_t st);
 cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStream_t st);
 // hydro fields / force (FP64 outputs), optional arithmetic-precision u planes (u_arith)
-// and (u_x, u_y, u_z, t) per cell for the particles (ut4)
+// and (u_x, u_y, u_z, t) per cell for the particles and LES (ut4; t only with ut4_t and a
+// temperature set, else 0)
 cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep,
                          const double* fm, double* dens,
                          double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st,
-                         double* ut4 = nullptr);
+                         double* ut4 = nullptr, int ut4_t = 1);
 cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep,
                          const float* fm, double* dens,
                          double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
-                         float* ut4 = nullptr);
+                         float* ut4 = nullptr, int ut4_t = 1);
 // the hydro fields of z-planes [z0, z0 + nz) in the arithmetic type into a chunk buffer
 // (want: bit 0 dens, 1 u, 2 t, 3 s, 4 force; layout in fields_chunk_kernel)
 cudaError_t launch_fields_chunk(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep,

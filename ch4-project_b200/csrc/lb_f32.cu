@@ -17,9 +17,9 @@ cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStre
 cudaError_t launch_hydro(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep, const float* fm,
                          double* dens,
                          double* u, double* t, double* sc, double* force, float* u_arith, cudaStream_t st,
-                         float* ut4) {
-  return s.storage == 2 ? hydro_t<__half, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, st)
-                        : hydro_t<float, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, st);
+                         float* ut4, int ut4_t) {
+  return s.storage == 2 ? hydro_t<__half, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, ut4_t, st)
+                        : hydro_t<float, float>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, ut4_t, st);
 }
 cudaError_t launch_fields_chunk(const StepParams<float>& P, LaunchShape s, const float* hit, const float* dep,
                                 const float* fm, int z0, int nz, int want, float* out, cudaStream_t st) {

@@ -48,8 +48,8 @@ cudaError_t launch_fields_chunk(const StepParams<double>& P, LaunchShape s, cons
 cudaError_t launch_hydro(const StepParams<double>& P, LaunchShape s, const double* hit, const double* dep, const double* fm,
                          double* dens,
                          double* u, double* t, double* sc, double* force, double* u_arith, cudaStream_t st,
-                         double* ut4) {
-  return hydro_t<double, double>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, st);
+                         double* ut4, int ut4_t) {
+  return hydro_t<double, double>(P, s, hit, dep, fm, dens, u, t, sc, force, u_arith, ut4, ut4_t, st);
 }
 cudaError_t launch_force_moments(const StepParams<double>& P, LaunchShape s, const double* hit_cur, int with_prev,
                                  double* partial, int nblocks, double norm, const double* amp, double* fm,

@@ -183,6 +183,17 @@ __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >=
 // 2nd order at the y walls) or, with LB_FLUID_LES_LOCAL_STRAIN, from the populations'
 // stress tensor; C_smag per row with LB_FLUID_LES_VANDRIEST; WALE with LB_FLUID_LES_WALE.
 // f, rho, ux..u2: the cell's populations and the collision's rho, u^n, |u|^2.
+// the four values of cell c of a (u_x, u_y, u_z, t) array
+__device__ __forceinline__ void ld4(const float* p, long long c, float* v) {
+  const float4 q = __ldg(reinterpret_cast<const float4*>(p) + c);
+  v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, long long c, double* v) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p) + 2 * c);
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 2 * c + 1);
+  v[0] = a.x, v[1] = a.y, v[2] = b.x, v[3] = b.y;
+}
+
 template <bool EXACT, typename A>
 __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z, long long idx, const A* f, A rho,
                                      A ux, A uy, A uz, A u2) {
@@ -216,46 +227,59 @@ __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z
     s_norm = fabs(fac) * sqrt(A(2) * (QQxx * QQxx + QQxy * QQxy + QQxz * QQxz + QQyx * QQyx + QQyy * QQyy +
                                       QQyz * QQyz + QQzx * QQzx + QQzy * QQzy + QQzz * QQzz));
   } else {
+    // u^n as (u_x, u_y, u_z, t) per cell: one vector load per neighbour
     const A* u = P.ules;
-    auto at = [&](int a, int i, int j, int k) { return u[a * N + ((long long)k * NY + j) * NX + i]; };
-    A g[3][3];
+    auto cell = [&](int i, int j, int k) { return ((long long)k * NY + j) * NX + i; };
+    A g[3][3], v0[4], v1[4], v2[4];
     const int xp = wrap(x + 1, NX), xm = wrap(x - 1, NX), zp = wrap(z + 1, NZ), zm = wrap(z - 1, NZ);
     // z-slab: the planes beyond the slab's faces come from its neighbours
-    const long long nxy = (long long)NX * NY, inplane = (long long)y * NX + x;
+    const long long inplane = (long long)y * NX + x;
     const A* up_hi = (z == NZ - 1 && P.ules_hi) ? P.ules_hi : nullptr;
     const A* up_lo = (z == 0 && P.ules_lo) ? P.ules_lo : nullptr;
     // one-sided second-order differences at the walls of an axis (src/gradients.c:161-230)
     const bool wx = (P.walls & W_FX) != 0, wz = (P.walls & W_FZ) != 0;
+    auto side = [&](int b, bool fwd) {  // g[a][b] from the three samples v0, v1, v2
 #pragma unroll
-    for (int a = 0; a < 3; a++) {
-      if (wx && x == 0)
-        g[a][0] = A(-1.5) * at(a, 0, y, z) + A(2) * at(a, 1, y, z) + A(-0.5) * at(a, 2, y, z);
-      else if (wx && x == NX - 1)
-        g[a][0] = A(1.5) * at(a, NX - 1, y, z) + A(-2) * at(a, NX - 2, y, z) + A(0.5) * at(a, NX - 3, y, z);
-      else
-        g[a][0] = (at(a, xp, y, z) - at(a, xm, y, z)) / A(2);
-      if (wz && z == 0) {
-        g[a][2] = A(-1.5) * at(a, x, y, 0) + A(2) * at(a, x, y, 1) + A(-0.5) * at(a, x, y, 2);
-      } else if (wz && z == NZ - 1) {
-        g[a][2] = A(1.5) * at(a, x, y, NZ - 1) + A(-2) * at(a, x, y, NZ - 2) + A(0.5) * at(a, x, y, NZ - 3);
-      } else {
-        const A vp = up_hi ? up_hi[a * nxy + inplane] : at(a, x, y, zp);
-        const A vm = up_lo ? up_lo[a * nxy + inplane] : at(a, x, y, zm);
-        g[a][2] = (vp - vm) / A(2);
-      }
+      for (int a = 0; a < 3; a++)
+        g[a][b] = fwd ? A(-1.5) * v0[a] + A(2) * v1[a] + A(-0.5) * v2[a] : A(1.5) * v0[a] + A(-2) * v1[a] + A(0.5) * v2[a];
+    };
+    auto centred = [&](int b) {  // g[a][b] = (v0 - v1) / 2, v0 the + neighbour
+#pragma unroll
+      for (int a = 0; a < 3; a++) g[a][b] = (v0[a] - v1[a]) / A(2);
+    };
+    if (wx && x == 0) {
+      ld4(u, cell(0, y, z), v0), ld4(u, cell(1, y, z), v1), ld4(u, cell(2, y, z), v2);
+      side(0, true);
+    } else if (wx && x == NX - 1) {
+      ld4(u, cell(NX - 1, y, z), v0), ld4(u, cell(NX - 2, y, z), v1), ld4(u, cell(NX - 3, y, z), v2);
+      side(0, false);
+    } else {
+      ld4(u, cell(xp, y, z), v0), ld4(u, cell(xm, y, z), v1);
+      centred(0);
+    }
+    if (wz && z == 0) {
+      ld4(u, cell(x, y, 0), v0), ld4(u, cell(x, y, 1), v1), ld4(u, cell(x, y, 2), v2);
+      side(2, true);
+    } else if (wz && z == NZ - 1) {
+      ld4(u, cell(x, y, NZ - 1), v0), ld4(u, cell(x, y, NZ - 2), v1), ld4(u, cell(x, y, NZ - 3), v2);
+      side(2, false);
+    } else {
+      if (up_hi) ld4(up_hi, inplane, v0);
+      else ld4(u, cell(x, y, zp), v0);
+      if (up_lo) ld4(up_lo, inplane, v1);
+      else ld4(u, cell(x, y, zm), v1);
+      centred(2);
     }
     const bool walls = (F & K_FWALL) != 0;
     if (walls && y == 0) {
-#pragma unroll
-      for (int a = 0; a < 3; a++) g[a][1] = A(-1.5) * at(a, x, 0, z) + A(2) * at(a, x, 1, z) + A(-0.5) * at(a, x, 2, z);
+      ld4(u, cell(x, 0, z), v0), ld4(u, cell(x, 1, z), v1), ld4(u, cell(x, 2, z), v2);
+      side(1, true);
     } else if (walls && y == NY - 1) {
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-        g[a][1] = A(1.5) * at(a, x, NY - 1, z) + A(-2) * at(a, x, NY - 2, z) + A(0.5) * at(a, x, NY - 3, z);
+      ld4(u, cell(x, NY - 1, z), v0), ld4(u, cell(x, NY - 2, z), v1), ld4(u, cell(x, NY - 3, z), v2);
+      side(1, false);
     } else {
-      const int yp = wrap(y + 1, NY), ym = wrap(y - 1, NY);
-#pragma unroll
-      for (int a = 0; a < 3; a++) g[a][1] = (at(a, x, yp, z) - at(a, x, ym, z)) / A(2);
+      ld4(u, cell(x, wrap(y + 1, NY), z), v0), ld4(u, cell(x, wrap(y - 1, NY), z), v1);
+      centred(1);
     }
     xx = g[0][0], xy = g[0][1], xz = g[0][2];
     yx = g[1][0], yy = g[1][1], yz = g[1][2];
@@ -269,8 +293,8 @@ __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z
     // sqrt(1 - Ri) for Ri < 1, else 0.  dT/dy of gradient_scalar: one-sided at the y
     // walls of the temperature or scalar, centred (periodic) elsewhere.  The reference
     // squares |S| with the host pow (within an ulp of the product here)
-    const double* t = P.les_t;
-    auto tv = [&](int j) { return A(t[((long long)z * NY + j) * NX + x]); };
+    const A* t = P.ules + 3;  // the fourth component of u^n's vectors is t^n
+    auto tv = [&](int j) { return t[4 * (((long long)z * NY + j) * NX + x)]; };
     A gy;
     const bool wy = (F & (K_TWALL | K_SWALL)) != 0;
     if (wy && y == 0)
@@ -372,7 +396,7 @@ __device__ __forceinline__ void hydro_cell(const StepParams<A>& P, int x, int y,
 
 template <typename S, typename A, bool THERM, bool SCAL>
 __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, const A* fm, double* dens, double* u,
-                             double* t, double* s, double* force, A* u_arith, A* ut4) {
+                             double* t, double* s, double* force, A* u_arith, A* ut4, int ut4_t) {
   // grid (x blocks, NY, NZ): no index division
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= P.NX) return;
@@ -398,7 +422,7 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
   }
   A tt4 = A(0);
   if constexpr (THERM) {
-    if (t || ut4) {
+    if (t || (ut4 && ut4_t)) {
       A g[Q];
       load_set<S, A, 1>(P, idx, g);
       const A tt = mom0(g);
