@@ -20,7 +20,10 @@ same input (`error_vs_fp64`: u and T after the timed steps, Nusselt number and k
 energy over the configuration's 20,000-step run) and the FP64 path's own throughput
 (`fp64`), the end-to-end run's phases (`e2e.breakdown`), and the forced-HIT
 configuration (256^3, FP32, 10^6 two-way coupled particles) as its own record
-(`hit_particles`: MLUPS, particle updates/s, ms per step; `--no-hit` skips it).
+(`hit_particles`: MLUPS, particle updates/s, ms per step; `--no-hit` skips it), the batched
+ensemble (`ensemble`: solves/hour against the FP64 path one case at a time) and the served
+request stream (`serve`: p50/p99 latency and aggregate MLUPS against the FP64 path serving the
+same requests one at a time, step counts scaled by --serve-step-scale).
 """
 import argparse
 import json
@@ -397,6 +400,36 @@ def bench_ensemble(args):
                           "ensemble_mlups": cells / t_step / 1e6, "tile_block": block, "tile_rows": rows,
                           "throughput_only": True}))
         return 0
+    if getattr(args, "record_only", False):
+        # throughput against the FP64 path's per-case step time (a + b cells, fitted on the
+        # sample); the accuracy study is the standalone line's
+        ens.close()
+        xs, ts = [], []
+        for i in sample:
+            nx, ny, ra = cases[i]
+            p0, g0 = state_of(i, nx, ny)
+            with ch4b200.Simulation(cfg_of(nx, ny, ra, abi.STORE_F64)) as sim:
+                sim.set_pop("p", p0)
+                sim.set_pop("g", g0)
+                sim.initialize()
+                sim.step(20)
+                sim.synchronize()
+                ts.append(_event_time(sim.stream_handle, lambda: sim.step(100)) / 100)
+            xs.append(nx * ny)
+        a, b = np.polyfit(np.array(xs, float), np.array(ts), 1)[::-1]
+        t64 = sum(max(a + b * nx * ny, min(ts)) for nx, ny, _ in cases)
+        solves_h64 = 3600.0 * len(cases) / (S * t64)
+        peak, kind = measured_peak()
+        bpc = BYTES_PER_CELL.get(args.storage, BYTES_PER_CELL["f32"])
+        return {"metric": "ensemble solves/hour", "value": solves_h, "unit": "solves/h",
+                "config": {"workload": "ensemble_%d_quasi2d_rayleigh_benard" % len(cases), "cells_total": cells,
+                           "steps_per_solve": S, "storage": args.storage, "tile_block": block, "tile_rows": rows},
+                "ensemble_ms_per_step": t_step * 1e3, "ensemble_mlups": cells / t_step / 1e6,
+                "roofline_frac": bpc * cells / t_step / 1e9 / peak, "peak_kind": kind,
+                "fp64_one_at_a_time": {"solves_per_hour": solves_h64, "fit_seconds_per_step": [a, b],
+                                       "sample_cases": len(sample)},
+                "speedup_vs_fp64_one_at_a_time": solves_h / solves_h64,
+                "accuracy": "bench.py --workload ensemble (Nusselt and kinetic energy against FP64)"}
     # the rest of the solve: T fields of the sampled cases at the short horizon, then Nu over [S/2, S]
     done = 100 + K
     nu_ens = {i: [] for i in sample}
@@ -508,7 +541,7 @@ def bench_ensemble(args):
     return 0
 
 
-def bench_serve(args):
+def bench_serve(args, record_only=False):
     """Poisson request stream (20/s) of Kolmogorov and Rayleigh-Benard cubes, half with
     LES (C_s 0.17) and 1e4-1e5 tracers; step counts log-uniform in [500, 20000] times
     --step-scale.  p50/p99 latency and aggregate MLUPS against the FP64 path serving the
@@ -523,7 +556,10 @@ def bench_serve(args):
         serve.request_state(r)
         serve.request_particles(r)
     runs = {}
-    for name, cap in (("all_in_flight", None), ("cells_in_flight_%d" % args.cells_in_flight, args.cells_in_flight)):
+    policies = (("all_in_flight", None), ("cells_in_flight_%d" % args.cells_in_flight, args.cells_in_flight))
+    if record_only:  # the default bench line's record: the capped policy alone
+        policies = policies[1:]
+    for name, cap in policies:
         srv = serve.Server(abi.STORE_F32, block=100, cells_in_flight=cap)
         t0 = time.perf_counter()
         done = srv.run(copy.deepcopy(reqs))
@@ -535,7 +571,7 @@ def bench_serve(args):
     base = serve.serve_fp64_one_at_a_time(copy.deepcopy(reqs))
     lat64 = np.array([r.latency for r in base])
     span64 = max(r.finished for r in base) - min(r.arrival for r in base)
-    print(json.dumps({
+    rec = {
         "metric": "served p50/p99 latency and aggregate MLUPS", "value": runs[best]["mlups"], "unit": "MLUPS",
         "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic", "policy": best,
         "config": {"workload": "served_stream", "requests": len(reqs), "rate_per_s": 20.0,
@@ -545,7 +581,11 @@ def bench_serve(args):
         "policies": runs,
         "fp64_one_at_a_time": {"p50_s": float(np.percentile(lat64, 50)), "p99_s": float(np.percentile(lat64, 99)),
                                "mlups": work / span64 / 1e6},
-    }))
+        "throughput_vs_fp64_one_at_a_time": runs[best]["mlups"] / (work / span64 / 1e6),
+    }
+    if record_only:
+        return rec
+    print(json.dumps(rec))
     return 0
 
 
@@ -650,6 +690,10 @@ def main():
     ap.add_argument("--error-window", type=int, default=20000)
     ap.add_argument("--error-every", type=int, default=1000)
     ap.add_argument("--no-hit", action="store_true", help="skip the HIT + particles sub-record")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble sub-record")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream sub-record")
+    ap.add_argument("--serve-step-scale", type=float, default=1.0,
+                    help="step counts of the served-stream sub-record, times the configuration's")
     args = ap.parse_args()
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "ours":
         return spawn_ranks(args)
@@ -780,6 +824,19 @@ def main():
     hit = None
     if world == 1 and not args.no_hit:
         hit = hit_particles_run(args.hit_size, args.particles, max(K, 20), W)
+    # the batched ensemble (fourth configuration) and the served stream (fifth, step counts
+    # scaled by --serve-step-scale) against the FP64 path one case at a time
+    ens_rec = srv_rec = None
+    if world == 1 and not args.no_ensemble:
+        import copy as _copy
+        ea = _copy.copy(args)
+        ea.record_only, ea.storage, ea.steps = True, "f32", 100
+        ens_rec = bench_ensemble(ea)
+    if world == 1 and not args.no_serve:
+        import copy as _copy
+        sa = _copy.copy(args)
+        sa.step_scale = args.serve_step_scale
+        srv_rec = bench_serve(sa, record_only=True)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -809,6 +866,8 @@ def main():
             "error_vs_fp64": err,
             "fp64": fp64,
             "hit_particles": hit,
+            "ensemble": ens_rec,
+            "serve": srv_rec,
         }
         print(json.dumps(line))
     if world > 1:
