@@ -9,12 +9,13 @@ together in blocks of steps:
   for all of them, ch4_ensemble_*), one ensemble per population-set layout;
 * LES and particle requests run on their own handle and CUDA stream
   (ch4_create/ch4_step), overlapping with the ensembles on the device;
-* between blocks, finished requests are retired (their memory freed) and waiting
-  requests are admitted in arrival order while the device-memory budget allows and,
+* while a block runs, waiting requests are admitted (built and uploaded) in arrival order
+  while the device-memory budget allows and,
   with `cells_in_flight`, while the admitted lattices stay under that many cells (a
   request is always admitted when nothing runs): small requests then batch together
   while large ones do not share the device with a long queue, which shortens the
-  median latency without leaving the device idle.
+  median latency without leaving the device idle; after a block finished requests are
+  retired (their memory freed).
 
 A request's result is the same alone and in the mix: ensemble slots advance
 bit-for-bit as they would alone, and dedicated handles are independent.
@@ -220,20 +221,30 @@ class Server:
         req.admitted = now
         return True
 
-    def advance(self):
-        """One block: every active simulation advances by the same number of steps."""
+    def launch(self):
+        """Enqueue one block: every active simulation advances by the same number of steps
+        (asynchronously, each on its stream).  Returns the block and the entries in it."""
         n = min(self.block, min(a[5] for a in self.active))
         for ens in self.ensembles.values():
             ens.step(n)
         for a in self.active:
             if a[1] == "sim":
                 a[2].step(n)
+        return n, list(self.active)
+
+    def finish(self, n, launched):
+        """Wait for a launched block and count its steps."""
         for ens in self.ensembles.values():
             ens.synchronize()
-        for a in self.active:
+        for a in launched:
             if a[1] == "sim":
                 a[2].synchronize()
             a[5] -= n
+
+    def advance(self):
+        """One block, launched and waited for."""
+        n, launched = self.launch()
+        self.finish(n, launched)
         return n
 
     def retire(self, now):
@@ -253,6 +264,10 @@ class Server:
         self.active = keep
 
     def run(self, requests, clock=time.perf_counter):
+        """Serve `requests` (arrival times in seconds from the start).  The next block is on
+        the device while the host admits the requests that arrived meanwhile: a new
+        simulation (its handle, state upload and initialisation) is built while the others
+        step, and joins from the next block on."""
         pending = sorted(requests, key=lambda r: r.arrival)
         waiting = []
         t0 = clock()
@@ -260,16 +275,19 @@ class Server:
             now = clock() - t0
             while pending and pending[0].arrival <= now:
                 waiting.append(pending.pop(0))
-            while waiting and self.try_admit(waiting[0], now):
+            block = self.launch() if self.active else None
+            while waiting and self.try_admit(waiting[0], clock() - t0):
                 waiting.pop(0)
-            if not self.active:
+            if block is None:
+                if self.active:
+                    continue
                 if pending:
                     time.sleep(max(0.0, pending[0].arrival - (clock() - t0)))
                     continue
                 if waiting:
                     raise RuntimeError("request %d does not fit the device-memory budget" % waiting[0].rid)
                 break
-            self.advance()
+            self.finish(*block)
             self.retire(clock() - t0)
         for ens in self.ensembles.values():
             ens.close()
