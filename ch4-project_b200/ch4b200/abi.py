@@ -115,6 +115,13 @@ FLAGS2 = {
     "LAGRANGE_SMALLTAUD_FLOATER": 1 << 26,
     "LAGRANGE_TWOWAY_SMALLTAUD": 1 << 27,
     "LB_FLUID_LES_SMAGORINSKY_LILLY": 1 << 28,
+    "LAGRANGE_ORIENTATION_SECONDORIENTATION": 1 << 29,
+    "LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS": 1 << 30,
+    "LAGRANGE_ORIENTATION_ACTIVE": 1 << 31,
+    "LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC": 1 << 32,
+    "LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE": 1 << 33,
+    "LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION": 1 << 34,
+    "LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION": 1 << 35,
 }
 
 
@@ -159,6 +166,7 @@ PARTICLE_FIELDS = [
     "dx_t", "dy_t", "dz_t",
     "px", "py", "pz", "dt_px", "dt_py", "dt_pz", "aspect_ratio",
     "t_p", "cp_p",
+    "nx", "ny", "nz", "dt_nx", "dt_ny", "dt_nz", "gyrotaxis_velocity", "swim_velocity",
 ]
 
 

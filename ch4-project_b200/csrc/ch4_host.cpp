@@ -152,7 +152,10 @@ const uint64_t SUPPORTED2 =
     CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM | CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO |
     CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_STOKES_HALF | CH4_F2_LAGRANGE_SMALLTAUD |
     CH4_F2_LAGRANGE_SMALLTAUD_BETA | CH4_F2_LAGRANGE_SMALLTAUD_FLOATER | CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD |
-    CH4_F2_FLUID_LES_SMAGORINSKY_LILLY;
+    CH4_F2_FLUID_LES_SMAGORINSKY_LILLY | CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION |
+    CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE |
+    CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE |
+    CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -792,6 +795,15 @@ struct Engine : EngineBase {
     Q.tricubic = (c.flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) != 0;
     Q.orient = (c.flags & CH4_F_LAGRANGE_ORIENTATION) != 0;
     Q.jeffery = (c.flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) != 0;
+    Q.second = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION) != 0;
+    Q.gyro = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) != 0;
+    Q.swim = 0;
+    if (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)  // the reference's #if / #elif order
+      Q.swim = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC)            ? 2
+               : (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE)        ? 3
+               : (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION)  ? 4
+               : (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION) ? 5
+                                                                                    : 1;
     Q.nrec = nrec();
     Q.rec = rec;
     Q.srec = srec;
@@ -1751,9 +1763,11 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
     bool needed;
   };
   double NX, NY, NZ, particle_number = 0, resume = 0, tau_drag_types = 1, beta_coeff_types = 1, cp_coeff_types = 1;
+  double aspect_ratio_types = 1, gyrotaxis_velocity_types = 1, swim_velocity_types = 1;
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
+  const bool orient = (fl & CH4_F_LAGRANGE_GRADIENT) && (fl & CH4_F_LAGRANGE_ORIENTATION);
   // gravity_x/y/z (src/parameters.c:234-241, with LB_FLUID_FORCING_GRAVITY): read where
   // buoyancy, the particles' gravity, their Stokes re-injection or a small-tau_drag model uses it
   const bool grav = (forcing && (fl & (CH4_F_TEMPERATURE_BUOYANCY | CH4_F_SCALAR_BUOYANCY))) ||
@@ -1779,6 +1793,14 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
        (fl & CH4_F_LAGRANGE) && (fl & CH4_F_LAGRANGE_GRADIENT) && (fl & CH4_F_LAGRANGE_ADDEDMASS)},
       // LAGRANGE_TEMPERATURE multiplies the types by the specific-heat classes, src/parameters.c:606-618
       {"cp_coeff_types", &cp_coeff_types, (fl & CH4_F_LAGRANGE) && (cfg->flags2 & CH4_F2_LAGRANGE_TEMPERATURE)},
+      // ... and the orientation classes, src/parameters.c:620-696 (under LAGRANGE_GRADIENT and
+      // LAGRANGE_ORIENTATION)
+      {"aspect_ratio_types", &aspect_ratio_types, (fl & CH4_F_LAGRANGE) && orient && (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY)},
+      {"gyrotaxis_velocity_types", &gyrotaxis_velocity_types,
+       (fl & CH4_F_LAGRANGE) && orient && (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) &&
+           (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS)},
+      {"swim_velocity_types", &swim_velocity_types,
+       (fl & CH4_F_LAGRANGE) && orient && (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)},
       {"noise_u", &cfg->noise_u, (fl & CH4_F_FLUID_INITIAL_ADD_NOISE) != 0},  // src/parameters.c:216-220
       {"noise_t", &cfg->noise_t, T && (fl & CH4_F_TEMPERATURE_INITIAL_ADD_NOISE)},  // src/parameters.c:347-351
   };
@@ -1797,7 +1819,8 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   cfg->NZ = (int)NZ;
   cfg->particle_number = (int)particle_number;
   cfg->resume = (int)resume;
-  cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types * (int)cp_coeff_types;
+  cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types * (int)cp_coeff_types * (int)aspect_ratio_types *
+                        (int)gyrotaxis_velocity_types * (int)swim_velocity_types;
   // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
   cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
   cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;
@@ -1927,6 +1950,13 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_SMALLTAUD_FLOATER", CH4_F2_LAGRANGE_SMALLTAUD_FLOATER},
       {"LAGRANGE_TWOWAY_SMALLTAUD", CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD},
       {"LB_FLUID_LES_SMAGORINSKY_LILLY", CH4_F2_FLUID_LES_SMAGORINSKY_LILLY},
+      {"LAGRANGE_ORIENTATION_SECONDORIENTATION", CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION},
+      {"LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS", CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS},
+      {"LAGRANGE_ORIENTATION_ACTIVE", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE},
+      {"LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC},
+      {"LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE},
+      {"LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION},
+      {"LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2089,6 +2119,29 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
         (c->flags & (CH4_F_LAGRANGE_ORIENTATION | CH4_F_LAGRANGE_GRADIENT)) !=
             (CH4_F_LAGRANGE_ORIENTATION | CH4_F_LAGRANGE_GRADIENT))
       return why = "LAGRANGE_ORIENTATION_JEFFREY needs LAGRANGE_ORIENTATION and LAGRANGE_GRADIENT", CH4_ERR_UNSUPPORTED;
+    {
+      // the orientation variants, as src/lagrange.c nests them
+      const uint64_t f2 = c->flags2;
+      const uint64_t modes = CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE |
+                             CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION |
+                             CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION;
+      if ((f2 & (CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)) &&
+          !(c->flags & CH4_F_LAGRANGE_ORIENTATION))
+        return why = "LAGRANGE_ORIENTATION_SECONDORIENTATION and _ACTIVE need LAGRANGE_ORIENTATION", CH4_ERR_UNSUPPORTED;
+      if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) && !(c->flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY))
+        return why = "LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS needs LAGRANGE_ORIENTATION_JEFFREY", CH4_ERR_UNSUPPORTED;
+      if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) && !(c->flags & CH4_F_LAGRANGE_GRADIENT))
+        return why = "LAGRANGE_ORIENTATION_ACTIVE needs LAGRANGE_GRADIENT (swim_velocity is read under it)",
+               CH4_ERR_UNSUPPORTED;
+      if ((f2 & modes) && !(f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE))
+        return why = "the LAGRANGE_ORIENTATION_ACTIVE_* modes need LAGRANGE_ORIENTATION_ACTIVE", CH4_ERR_UNSUPPORTED;
+      if ((f2 & (CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION |
+                 CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION)) &&
+          !(f2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION))
+        return why = "swimming along n needs LAGRANGE_ORIENTATION_SECONDORIENTATION", CH4_ERR_UNSUPPORTED;
+      if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
+        return why = "LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
+    }
     if (!(c->time_dt_lagr_factor >= 1.0)) return why = "time_dt_lagr_factor must be >= 1", CH4_ERR_ARG;
   }
   return CH4_OK;
@@ -2749,6 +2802,21 @@ namespace {
 // (dataset or member name, field of ch4_particle)
 using PField = std::pair<const char*, double ch4_particle::*>;
 
+// after p and dp/dt: n and dn/dt (SECONDORIENTATION), aspect_ratio (JEFFREY),
+// gyrotaxis_velocity (GYROTAXIS), swim_velocity (ACTIVE) -- the order of output_particles
+// (src/lagrange.c:1925-1992) and of write_point_particle_h5 (src/lagrange.c:4378-4407)
+void orientation_extras(std::vector<PField>& v, uint64_t fl, uint64_t fl2) {
+  using P = ch4_particle;
+  if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION)
+    v.insert(v.end(), {{"nx", &P::nx}, {"ny", &P::ny}, {"nz", &P::nz}, {"dt_nx", &P::dt_nx}, {"dt_ny", &P::dt_ny},
+                       {"dt_nz", &P::dt_nz}});
+  if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) {
+    v.push_back({"aspect_ratio", &P::aspect_ratio});
+    if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) v.push_back({"gyrotaxis_velocity", &P::gyrotaxis_velocity});
+  }
+  if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) v.push_back({"swim_velocity", &P::swim_velocity});
+}
+
 // the per-particle datasets of output_particles, in its order, for the supported flags
 std::vector<PField> lagrange_fields(uint64_t fl, uint64_t fl2, bool output_fluid) {
   using P = ch4_particle;
@@ -2770,7 +2838,7 @@ std::vector<PField> lagrange_fields(uint64_t fl, uint64_t fl2, bool output_fluid
     if (fl & CH4_F_LAGRANGE_ORIENTATION) {
       v.insert(v.end(), {{"px", &P::px}, {"py", &P::py}, {"pz", &P::pz}, {"dt_px", &P::dt_px}, {"dt_py", &P::dt_py},
                          {"dt_pz", &P::dt_pz}});
-      if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) v.push_back({"aspect_ratio", &P::aspect_ratio});
+      orientation_extras(v, fl, fl2);
     }
   }
   if (fl & CH4_F_LB_TEMPERATURE) {
@@ -2803,7 +2871,7 @@ std::vector<PField> part_members(uint64_t fl, uint64_t fl2) {
       if (fl & CH4_F_LAGRANGE_ORIENTATION) {
         v.insert(v.end(), {{"px", &P::px}, {"py", &P::py}, {"pz", &P::pz}, {"dt_px", &P::dt_px},
                            {"dt_py", &P::dt_py}, {"dt_pz", &P::dt_pz}});
-        if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) v.push_back({"aspect_ratio", &P::aspect_ratio});
+        orientation_extras(v, fl, fl2);
       }
     }
   }
@@ -2873,7 +2941,15 @@ bool write_particle_xmf(const std::string& path, const std::string& h5name, int 
     if (fl & CH4_F_LAGRANGE_ORIENTATION) {
       joined("orientation", "Vector", {"px", "py", "pz"});
       joined("angular velocity", "Vector", {"dt_px", "dt_py", "dt_pz"});
-      if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) scalar("aspect_ratio");
+      if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION) {
+        joined("second orientation", "Vector", {"nx", "ny", "nz"});
+        joined("second angular velocity", "Vector", {"dt_nx", "dt_ny", "dt_nz"});
+      }
+      if (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) {
+        scalar("aspect_ratio");
+        if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) scalar("gyrotaxis_velocity");
+      }
+      if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) scalar("swim_velocity");
     }
   }
   if (fl & CH4_F_LB_TEMPERATURE) {

@@ -95,6 +95,9 @@ struct PartParams {
   int inelastic, reinject, rj_vzero, rj_half;
   int stau_beta, stau_floater, twoway_stau;
   double beta_t;
+  // orientation variants: the second orientation, gyrotaxis, the swimming mode of active
+  // tracers (0 none, 1 along p, 2 ballistic, 3 while dT/dt > 0, 4 along n, 5 rods p, discs n)
+  int second, gyro, swim;
 };
 
 #ifdef __CUDACC__
@@ -538,19 +541,29 @@ __device__ __forceinline__ void particle_walls(const PartParams<A>& P, double ta
   }
 }
 
-// One Lagrangian sub-step for one particle: interpolate, move, wrap.  The state the
-// step reads is loaded once, up front (independent loads), and every result is
-// stored once at the end; the arithmetic is the reference's, expression for
-// expression.
 // orientation of one particle (src/lagrange.c:3470-3752): Jeffery's equation
 // dp/dt = W p + f S p - (p . f S p) p with f = (a^2 - 1) / (1 + a^2) for aspect ratio a,
 // S and W the symmetric and antisymmetric halves of A_ij = d_j u_i; Euler on the first
-// step, Adams-Bashforth 2 after; p renormalised.  Sums in the reference's order.
-static __device__ __noinline__ void orient_particle(double* pf, long long np, int ip, const double* gr, bool jeffery,
-                                             bool first, double dtl) {
+// step, Adams-Bashforth 2 after; p renormalised.  With SECONDORIENTATION a second vector n
+// follows dn/dt = W n - p (p . f S n) and is renormalised too; with GYROTAXIS the stretched
+// S takes -1/(2 v0) (-g + a) p_0 in its first column (the reference adds the rest of that
+// outer product to the velocity-gradient matrix, which it does not read again; without
+// particle gravity the vector is (0, 0, 1)).  Sums in the reference's order.
+struct OrientOpts {
+  bool jeffery, second, gyro, gravity;
+  double g[3];
+};
+
+static __device__ __noinline__ void orient_particle(double* pf, long long np, int ip, const double* gr,
+                                                    const OrientOpts o, bool first, double dtl) {
 #define F(name) pf[CH4_PF(name) * np + ip]
   double p[3] = {F(px), F(py), F(pz)}, fo[3] = {F(dt_px), F(dt_py), F(dt_pz)};
-  if (jeffery) {
+  double n[3] = {0.0, 0.0, 0.0}, fno[3] = {0.0, 0.0, 0.0};
+  if (o.second) {
+    n[0] = F(nx), n[1] = F(ny), n[2] = F(nz);
+    fno[0] = F(dt_nx), fno[1] = F(dt_ny), fno[2] = F(dt_nz);
+  }
+  if (o.jeffery) {
     const double a = F(aspect_ratio);
     const double fa = (a * a - 1.0) / (1.0 + a * a);
     double S[3][3], W[3][3];
@@ -565,6 +578,22 @@ static __device__ __noinline__ void orient_particle(double* pf, long long np, in
     for (int i = 0; i < 3; i++)
 #pragma unroll
       for (int j = 0; j < 3; j++) S[i][j] *= fa;
+    if (o.gyro && F(gyrotaxis_velocity) != 0) {
+      const double gyro = -0.5 / F(gyrotaxis_velocity);
+      double va[3];
+      if (o.gravity) {
+        va[0] = gyro * (-o.g[0] + F(ax));
+        va[1] = gyro * (-o.g[1] + F(ay));
+        va[2] = gyro * (-o.g[2] + F(az));
+      } else {
+        va[0] = gyro * 0.0;
+        va[1] = gyro * 0.0;
+        va[2] = gyro * 1.0;
+      }
+      S[0][0] += va[0] * p[0];
+      S[1][0] += va[1] * p[0];
+      S[2][0] += va[2] * p[0];
+    }
     double tmp[3] = {0.0, 0.0, 0.0}, oso = 0.0, f[3];
 #pragma unroll
     for (int i = 0; i < 3; i++)
@@ -579,10 +608,34 @@ static __device__ __noinline__ void orient_particle(double* pf, long long np, in
       for (int j = 0; j < 3; j++) f[i] += W[i][j] * p[j] + (S[i][j] * p[j]);
       f[i] -= p[i] * oso;
     }
+    double fn[3] = {0.0, 0.0, 0.0};
+    if (o.second) {
+      double tn[3] = {0.0, 0.0, 0.0}, osn = 0.0;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) tn[i] += S[i][j] * n[j];
+#pragma unroll
+      for (int i = 0; i < 3; i++) osn += p[i] * tn[i];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        fn[i] = 0.0;
+#pragma unroll
+        for (int j = 0; j < 3; j++) fn[i] += W[i][j] * n[j];
+        fn[i] -= p[i] * osn;
+      }
+    }
 #pragma unroll
     for (int i = 0; i < 3; i++) {
       p[i] = first ? p[i] + dtl * f[i] : p[i] + 0.5 * dtl * (3. * f[i] - fo[i]);
       fo[i] = f[i];
+    }
+    if (o.second) {
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        n[i] = first ? n[i] + dtl * fn[i] : n[i] + 0.5 * dtl * (3. * fn[i] - fno[i]);
+        fno[i] = fn[i];
+      }
     }
   }
   double norm = 0.0;
@@ -596,9 +649,56 @@ static __device__ __noinline__ void orient_particle(double* pf, long long np, in
   F(dt_px) = fo[0];
   F(dt_py) = fo[1];
   F(dt_pz) = fo[2];
+  if (o.second) {
+    double nn = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) nn += n[i] * n[i];
+#pragma unroll
+    for (int i = 0; i < 3; i++) n[i] /= sqrt(nn);
+    F(nx) = n[0];
+    F(ny) = n[1];
+    F(nz) = n[2];
+    F(dt_nx) = fno[0];
+    F(dt_ny) = fno[1];
+    F(dt_nz) = fno[2];
+  }
 #undef F
 }
 
+// The swimming velocity of an active tracer (LAGRANGE_ORIENTATION_ACTIVE, src/lagrange.c:
+// 3045-3190), after v = u: mode 1 v += s p, 2 v = s p (ballistic), 3 v += s p while dT/dt > 0,
+// 4 v += s n, 5 v += s p for rods (a >= 1) and s n for discs.
+static __device__ __noinline__ void swim_velocity(const double* pf, long long np, int ip, int mode, double& vx,
+                                                  double& vy, double& vz) {
+#define F(name) pf[CH4_PF(name) * np + ip]
+  const double s = F(swim_velocity);
+  const bool along_n = mode == 4 || (mode == 5 && !(F(aspect_ratio) >= 1.0));
+  const double dx = along_n ? F(nx) : F(px), dy = along_n ? F(ny) : F(py), dz = along_n ? F(nz) : F(pz);
+  if (mode == 2) {
+    vx = (s) * (dx);
+    vy = (s) * (dy);
+    vz = (s) * (dz);
+  } else if (mode == 3) {
+    double reactivity;
+    if (F(dt_t) > 0.0)
+      reactivity = 1.0;
+    else
+      reactivity = 0.0;
+    vx += reactivity * (s) * (dx);
+    vy += reactivity * (s) * (dy);
+    vz += reactivity * (s) * (dz);
+  } else {
+    vx += (s) * (dx);
+    vy += (s) * (dy);
+    vz += (s) * (dz);
+  }
+#undef F
+}
+
+// One Lagrangian sub-step for one particle: interpolate, move, wrap.  The state the
+// step reads is loaded once, up front (independent loads), and every result is
+// stored once at the end; the arithmetic is the reference's, expression for
+// expression.
 // FP32: four blocks of 128 per SM (<= 128 registers); FP64 keeps twice the registers
 template <typename A, bool ORIENT, bool HALO, int NF>
 __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_kernel(const PartParams<A> P) {
@@ -703,6 +803,8 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
     vx = ux;
     vy = uy;
     vz = uz;
+    if constexpr (ORIENT)  // active tracers need LAGRANGE_ORIENTATION
+      if (P.swim) swim_velocity(pf, np, ip, P.swim, vx, vy, vz);
     double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
     if (first) {
       vxo = vx;
@@ -821,7 +923,10 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
       vz += fac1 * (-P.g[2] - Dz);
     }
   }
-  if constexpr (ORIENT) orient_particle(pf, np, ip, &gr[0][0], P.jeffery != 0, first, dtl);
+  if constexpr (ORIENT) {
+    const OrientOpts o{P.jeffery != 0, P.second != 0, P.gyro != 0, P.gravity != 0, {P.g[0], P.g[1], P.g[2]}};
+    orient_particle(pf, np, ip, &gr[0][0], o, first, dtl);
+  }
   double tp = P.lagr_temp ? F(t_p) : 0.0;
   if constexpr (HALO) particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp);
   F(vx) = vx;

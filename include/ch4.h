@@ -163,7 +163,20 @@ enum {
   CH4_F2_LAGRANGE_TWOWAY_SMALLTAUD = 1ull << 27,
   /* Smagorinsky-Lilly: |S| damped by the buoyancy of a stable stratification,
    * sqrt(1 - Ri) with Ri = beta_t g_y (dT/dy)^+ / |S|^2, src/les.c:156-176 */
-  CH4_F2_FLUID_LES_SMAGORINSKY_LILLY = 1ull << 28
+  CH4_F2_FLUID_LES_SMAGORINSKY_LILLY = 1ull << 28,
+  /* orientation variants, src/lagrange.c:3470-3752 (with LAGRANGE_ORIENTATION): a second
+   * orientation n turned by the same Jeffery tensors; gravitational gyrotaxis in Jeffery's
+   * stretching term */
+  CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION = 1ull << 29,
+  CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS = 1ull << 30,
+  /* swimming tracers, src/lagrange.c:3045-3190: fluid velocity + swim_velocity along p
+   * (default), along p without the fluid (BALLISTIC), along p while dT/dt > 0 (TEMPERATURE),
+   * along n (SECONDORIENTATION), along p for rods and n for discs (SELECTIVEORIENTATION) */
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE = 1ull << 31,
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC = 1ull << 32,
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE = 1ull << 33,
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION = 1ull << 34,
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION = 1ull << 35
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
@@ -244,6 +257,11 @@ typedef struct {
   /* LAGRANGE_TEMPERATURE: the particle's own temperature and specific heat (relative to
    * the fluid's), src/typedef.h:467-470 */
   double t_p, cp_p;
+  /* LAGRANGE_ORIENTATION_SECONDORIENTATION: a second unit vector n and its last dn/dt;
+   * LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS: the gyrotactic velocity; LAGRANGE_ORIENTATION_ACTIVE:
+   * the swimming velocity (src/typedef.h:419-437) */
+  double nx, ny, nz, dt_nx, dt_ny, dt_nz;
+  double gyrotaxis_velocity, swim_velocity;
 } ch4_particle;
 
 /* Global averages of dump_averages (src/output.c:63-~760), FP64 sums over the

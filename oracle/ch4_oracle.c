@@ -662,8 +662,11 @@ static void interp_particle_t(const ch4o_state *s, const double *tf, ch4_particl
  * tau_drag == 0, Eulerian probes tau_drag < 0, Stokes drag + added mass) */
 /* orientation (src/lagrange.c:3470-3752): Jeffery's equation with the reference's
  * loops and sum order, Euler on the first step and AB2 after, then p renormalised */
-static void orient_particle(ch4_particle *p, int jeffery, int first, double dtl) {
+static void orient_particle(const ch4o_state *s, ch4_particle *p, int jeffery, int first, double dtl) {
+  const uint64_t f2 = s->cfg.flags2;
+  const int second = (f2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION) != 0;
   double P[3] = {p->px, p->py, p->pz}, Fold[3] = {p->dt_px, p->dt_py, p->dt_pz};
+  double N[3] = {p->nx, p->ny, p->nz}, FNold[3] = {p->dt_nx, p->dt_ny, p->dt_nz};
   if (jeffery) {
     const double A[3][3] = {{p->dx_ux, p->dy_ux, p->dz_ux}, {p->dx_uy, p->dy_uy, p->dz_uy},
                             {p->dx_uz, p->dy_uz, p->dz_uz}};
@@ -676,6 +679,25 @@ static void orient_particle(ch4_particle *p, int jeffery, int first, double dtl)
       for (int j = 0; j < 3; j++) W[i][j] = 0.5 * (A[i][j] - A[j][i]);
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) S[i][j] *= f_alpha;
+    if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) && p->gyrotaxis_velocity != 0) {
+      /* gravitational gyrotaxis, src/lagrange.c:3531-3565: -1/(2 v0) (-g + a) p_j added to
+       * the stretched S -- as the reference writes it, to its first column only (the other
+       * entries go to the velocity-gradient matrix, which is not read again) */
+      const double gyro = -0.5 / p->gyrotaxis_velocity;
+      double a[3];
+      if (s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) {
+        a[0] = gyro * (-s->cfg.gravity_x + p->ax);
+        a[1] = gyro * (-s->cfg.gravity_y + p->ay);
+        a[2] = gyro * (-s->cfg.gravity_z + p->az);
+      } else {
+        a[0] = gyro * 0.0;
+        a[1] = gyro * 0.0;
+        a[2] = gyro * 1.0;
+      }
+      S[0][0] += a[0] * P[0];
+      S[1][0] += a[1] * P[0];
+      S[2][0] += a[2] * P[0];
+    }
     for (int i = 0; i < 3; i++)
       for (int j = 0; j < 3; j++) TMP[i] += S[i][j] * P[j];
     for (int i = 0; i < 3; i++) oso += P[i] * TMP[i];
@@ -684,6 +706,18 @@ static void orient_particle(ch4_particle *p, int jeffery, int first, double dtl)
       for (int j = 0; j < 3; j++) Fv[i] += W[i][j] * P[j] + (S[i][j] * P[j]);
       Fv[i] -= P[i] * oso;
     }
+    double FN[3];
+    if (second) { /* the second orientation, src/lagrange.c:3604-3627: W n - p (p . S n) */
+      double TN[3] = {0, 0, 0}, osn = 0.0;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) TN[i] += S[i][j] * N[j];
+      for (int i = 0; i < 3; i++) osn += P[i] * TN[i];
+      for (int i = 0; i < 3; i++) {
+        FN[i] = 0.0;
+        for (int j = 0; j < 3; j++) FN[i] += W[i][j] * N[j];
+        FN[i] -= P[i] * osn;
+      }
+    }
     for (int i = 0; i < 3; i++) {
       if (first)
         P[i] = P[i] + dtl * Fv[i];
@@ -691,6 +725,14 @@ static void orient_particle(ch4_particle *p, int jeffery, int first, double dtl)
         P[i] = P[i] + 0.5 * dtl * (3. * Fv[i] - Fold[i]);
       Fold[i] = Fv[i];
     }
+    if (second)
+      for (int i = 0; i < 3; i++) {
+        if (first)
+          N[i] = N[i] + dtl * FN[i];
+        else
+          N[i] = N[i] + 0.5 * dtl * (3. * FN[i] - FNold[i]);
+        FNold[i] = FN[i];
+      }
   }
   double norm = 0.0;
   for (int i = 0; i < 3; i++) norm += P[i] * P[i];
@@ -701,6 +743,46 @@ static void orient_particle(ch4_particle *p, int jeffery, int first, double dtl)
   p->dt_px = Fold[0];
   p->dt_py = Fold[1];
   p->dt_pz = Fold[2];
+  if (second) {
+    double nn = 0.0;
+    for (int i = 0; i < 3; i++) nn += N[i] * N[i];
+    for (int i = 0; i < 3; i++) N[i] /= sqrt(nn);
+    p->nx = N[0];
+    p->ny = N[1];
+    p->nz = N[2];
+    p->dt_nx = FNold[0];
+    p->dt_ny = FNold[1];
+    p->dt_nz = FNold[2];
+  }
+}
+
+/* the swimming velocity of an active tracer, src/lagrange.c:3045-3190 (after v = u) */
+static void swim(const ch4o_state *s, ch4_particle *p) {
+  const uint64_t f2 = s->cfg.flags2;
+  if (!(f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)) return;
+  if (f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC) {
+    p->vx = (p->swim_velocity) * (p->px);
+    p->vy = (p->swim_velocity) * (p->py);
+    p->vz = (p->swim_velocity) * (p->pz);
+  } else if (f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE) {
+    double reactivity;
+    if (p->dt_t > 0.0)
+      reactivity = 1.0;
+    else
+      reactivity = 0.0;
+    p->vx += reactivity * (p->swim_velocity) * (p->px);
+    p->vy += reactivity * (p->swim_velocity) * (p->py);
+    p->vz += reactivity * (p->swim_velocity) * (p->pz);
+  } else if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION) ||
+             ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION) && !(p->aspect_ratio >= 1.0))) {
+    p->vx += (p->swim_velocity) * (p->nx);
+    p->vy += (p->swim_velocity) * (p->ny);
+    p->vz += (p->swim_velocity) * (p->nz);
+  } else {
+    p->vx += (p->swim_velocity) * (p->px);
+    p->vy += (p->swim_velocity) * (p->py);
+    p->vz += (p->swim_velocity) * (p->pz);
+  }
 }
 
 /* the walls of move_particles (src/lagrange.c:3754-3998), zero radius, y then x then z,
@@ -812,6 +894,7 @@ static void move_particle(const ch4o_state *s, ch4_particle *p, int first, doubl
     p->vx = p->ux;
     p->vy = p->uy;
     p->vz = p->uz;
+    swim(s, p);
     if (first) {
       p->vx_old = p->vx;
       p->vy_old = p->vy;
@@ -1450,7 +1533,7 @@ static void one_step(ch4o_state *s) {
       for (int ip = 0; ip < s->npart; ip++) {
         move_particle(s, &s->part[ip], first, dtl);
         if (s->cfg.flags & CH4_F_LAGRANGE_ORIENTATION)
-          orient_particle(&s->part[ip], (s->cfg.flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) != 0, first, dtl);
+          orient_particle(s, &s->part[ip], (s->cfg.flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) != 0, first, dtl);
       }
       wrap_particles(s);
     }

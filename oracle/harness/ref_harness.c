@@ -121,8 +121,17 @@ static void write_part_layout(void) {
 #endif
 #ifdef LAGRANGE_ORIENTATION
   F(px); F(py); F(pz); F(dt_px); F(dt_py); F(dt_pz);
+#ifdef LAGRANGE_ORIENTATION_SECONDORIENTATION
+  F(nx); F(ny); F(nz); F(dt_nx); F(dt_ny); F(dt_nz);
+#endif
 #ifdef LAGRANGE_ORIENTATION_JEFFREY
   F(aspect_ratio);
+#ifdef LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS
+  F(gyrotaxis_velocity);
+#endif
+#endif
+#ifdef LAGRANGE_ORIENTATION_ACTIVE
+  F(swim_velocity);
 #endif
 #endif
 #undef F

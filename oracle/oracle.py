@@ -137,6 +137,29 @@ FLAGSETS.update({
                      "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT",
                      "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY", "LAGRANGE_SMALLTAUD", "LAGRANGE_SMALLTAUD_FLOATER",
                      "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    # orientation variants and swimming tracers
+    "particles_or2": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY", "LAGRANGE_TWOWAY",
+                      "LAGRANGE_TWOWAY_MOMENTUM", "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY",
+                      "LAGRANGE_ORIENTATION_SECONDORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS",
+                      "LAGRANGE_ORIENTATION_ACTIVE"],
+    "particles_swimt": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE",
+                        "LB_TEMPERATURE_BUOYANCY", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT",
+                        "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY",
+                        "LAGRANGE_ORIENTATION_ACTIVE", "LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE"],
+    "particles_swimb": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION",
+                        "LAGRANGE_ORIENTATION_SECONDORIENTATION", "LAGRANGE_ORIENTATION_ACTIVE",
+                        "LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC"],
+    "particles_swims": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION",
+                        "LAGRANGE_ORIENTATION_JEFFREY", "LAGRANGE_ORIENTATION_SECONDORIENTATION",
+                        "LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS", "LAGRANGE_ORIENTATION_ACTIVE",
+                        "LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION"],
+    "particles_swimn": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION",
+                        "LAGRANGE_ORIENTATION_JEFFREY", "LAGRANGE_ORIENTATION_SECONDORIENTATION",
+                        "LAGRANGE_ORIENTATION_ACTIVE", "LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION"],
     # Smagorinsky-Lilly in a stably stratified channel
     "les_lilly": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
                   "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SMAGORINSKY_LILLY"],
@@ -207,6 +230,11 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
     if int(cfg.flags) & abi.FLAGS["LAGRANGE_ORIENTATION_JEFFREY"]:  # src/parameters.c, read by the reference
         keys += ["aspect_ratio_types", "aspect_ratio_min", "aspect_ratio_max"]
         vals.update({"aspect_ratio_types": 1, "aspect_ratio_min": 1.0, "aspect_ratio_max": 1.0})
+    for flag, key in (("LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS", "gyrotaxis_velocity"),  # src/parameters.c:638-649
+                      ("LAGRANGE_ORIENTATION_ACTIVE", "swim_velocity")):  # src/parameters.c:684-696
+        if int(cfg.flags2) & abi.FLAGS2[flag]:
+            keys += [key + "_types", key + "_min", key + "_max"]
+            vals.update({key + "_types": 1, key + "_min": 1.0, key + "_max": 1.0})
     if int(cfg.flags) & abi.FLAGS["LB_TEMPERATURE_FORCING"]:  # src/parameters.c: the source amplitude
         keys += ["Amp_t"]
         vals.update({"Amp_t": 0.0})

@@ -30,7 +30,8 @@ for name in sys.argv[1:] or sorted(CASES):
         temperature = ("t", "dt_t", "Dt_t", "dx_t") if "t" in ref["part"] else ()
         if "t_p" in ref["part"]:
             temperature += ("t_p",)
-        for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux") + temperature:
+        orientation = tuple(f for f in ("px", "py", "pz", "dt_px", "nx", "ny", "nz", "dt_nx") if f in ref["part"])
+        for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux") + temperature + orientation:
             out["out_part_" + f] = ref["part"][f]
     for k, v in pop_items(state):
         out["in_sha256_" + k] = hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest()

@@ -108,6 +108,23 @@ CASES = {
                          params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=18,
                                      T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3, gravity_x=3e-4,
                                      time_dt_lagr_factor=2.0, particle_number=250)),
+    # orientation variants and swimming tracers
+    "particles_or2": dict(flagset="particles_or2", NX=10, NY=8, NZ=7, npart=300,
+                          params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=21, gravity_x=2e-5,
+                                      gravity_y=1e-4, gravity_z=-3e-5, time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_swimt": dict(flagset="particles_swimt", NX=9, NY=8, NZ=7, npart=250,
+                            params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=22,
+                                        T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
+                                        time_dt_lagr_factor=2.0, particle_number=250)),
+    "particles_swimb": dict(flagset="particles_swimb", NX=10, NY=8, NZ=7, npart=300,
+                            params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=23,
+                                        time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_swims": dict(flagset="particles_swims", NX=10, NY=8, NZ=7, npart=300,
+                            params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=24,
+                                        time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_swimn": dict(flagset="particles_swimn", NX=10, NY=8, NZ=7, npart=300,
+                            params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=25,
+                                        time_dt_lagr_factor=2.0, particle_number=300)),
     # Smagorinsky-Lilly: T rising with y (stable), so the buoyancy damps |S| where Ri < 1
     "les_lilly": dict(flagset="les_lilly", NX=8, NY=9, NZ=6,
                       params=dict(tau_u=0.52, tau_t=0.55, Amp_x=0.02, T_bot=0.0, T_top=1.0, T_ref=0.5, beta_t=0.3,
@@ -195,6 +212,16 @@ def make_case(name, seed=0, storage=0, dims=None, **over):
                 v = rng.normal(size=3)
                 p.px, p.py, p.pz = v / np.linalg.norm(v)
                 p.aspect_ratio = ratios[i % len(ratios)]
+        if "LAGRANGE_ORIENTATION_SECONDORIENTATION" in flags:  # a second random unit vector
+            for p in state["part"]:
+                v = rng.normal(size=3)
+                p.nx, p.ny, p.nz = v / np.linalg.norm(v)
+        if "LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS" in flags:  # 0 switches the term off
+            for i, p in enumerate(state["part"]):
+                p.gyrotaxis_velocity = [0.0, 0.5, 2.0, -1.0, 10.0][i % 5]
+        if "LAGRANGE_ORIENTATION_ACTIVE" in flags:
+            for i, p in enumerate(state["part"]):
+                p.swim_velocity = [0.01, 0.0, 0.03, 0.002][(i // 4) % 4]
     return c["flagset"], cfg, state
 
 

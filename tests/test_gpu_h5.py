@@ -127,8 +127,14 @@ def _fields(flags, output_fluid, flags2=0):
                 f += [("Dt_ux", "Dt_ux"), ("Dt_uy", "Dt_uy"), ("Dt_uz", "Dt_uz")]
         if flags & abi.FLAGS["LAGRANGE_ORIENTATION"]:
             f += [(n, n) for n in ("px", "py", "pz", "dt_px", "dt_py", "dt_pz")]
+            if flags2 & abi.FLAGS2["LAGRANGE_ORIENTATION_SECONDORIENTATION"]:  # src/lagrange.c:1925-1962
+                f += [(n, n) for n in ("nx", "ny", "nz", "dt_nx", "dt_ny", "dt_nz")]
             if flags & abi.FLAGS["LAGRANGE_ORIENTATION_JEFFREY"]:
                 f.append(("aspect_ratio", "aspect_ratio"))
+                if flags2 & abi.FLAGS2["LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS"]:
+                    f.append(("gyrotaxis_velocity", "gyrotaxis_velocity"))
+            if flags2 & abi.FLAGS2["LAGRANGE_ORIENTATION_ACTIVE"]:
+                f.append(("swim_velocity", "swim_velocity"))
     if flags & abi.FLAGS["LB_TEMPERATURE"]:
         f += [("temperature", "t"), ("dt_t", "dt_t")]
         if grad:
@@ -149,7 +155,8 @@ def _particle_sim(name, seed, nsteps):
     return cfg, state, sim
 
 
-@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or", "particles_tt"])
+@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or", "particles_tt", "particles_swims",
+                                  "particles_swimt"])
 def test_particle_file_holds_the_particles(name, tmp_path):
     cfg, state, sim = _particle_sim(name, 65, 4)
     with sim:
@@ -167,7 +174,7 @@ def test_particle_file_holds_the_particles(name, tmp_path):
         assert "particle_4.h5:/lagrange/%s\n" % d in xmf, d
 
 
-@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or", "particles_tt"])
+@pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or", "particles_tt", "particles_swims"])
 def test_part_file_restart(name, tmp_path):
     cfg, state, a = _particle_sim(name, 66, 5)
     n = len(state["part"])

@@ -30,7 +30,9 @@ def _assert_same(a, b, what):
                                           ("cpower", 15), ("duct", 20), ("duct_les", 20), ("box", 20),
                                           ("slipx", 20), ("slipz", 20), ("particles_tt", 8), ("particles_ttc", 8),
                                           ("particles_rb", 8), ("particles_duct", 8), ("particles_slip", 8),
-                                          ("particles_reinj", 8), ("particles_bc", 8), ("les_lilly", 20)])
+                                          ("particles_reinj", 8), ("particles_bc", 8), ("les_lilly", 20),
+                                          ("particles_or2", 8), ("particles_swimt", 8), ("particles_swimb", 8),
+                                          ("particles_swims", 8), ("particles_swimn", 8)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
@@ -83,7 +85,8 @@ def test_restatement_matches_golden_fixture(name):
     mine = run_restatement(cfg, state, int(g["nsteps"]))
     for k, _ in pop_items(state):
         _assert_same(mine[k], g["out_" + k], k)
-    for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux", "t", "dt_t", "Dt_t", "dx_t", "t_p"):
+    for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux", "t", "dt_t", "Dt_t", "dx_t", "t_p", "px", "py", "pz",
+              "dt_px", "nx", "ny", "nz", "dt_nx"):
         if "out_part_" + f in g.files:
             _assert_same(mine["part"][f], g["out_part_" + f], "particle " + f)
     for k in ("u", "t", "s", "phi"):
