@@ -27,6 +27,14 @@ With LB_FLUID_LES the eddy viscosity differentiates u across the z faces: in the
 of every step each slab's handle calls back (ch4_set_exchange) with the u of its bottom
 and top planes, and the callback swaps them with the neighbours -- point to point over
 the process group, or between the threads of one process (`LocalExchange`).
+
+Lagrangian particles (periodic lattices, one-way coupling) use the same callback: after
+the hydrodynamic pass every slab swaps the two planes of u next to each face (the
+interpolation stencil reaches two planes beyond the slab), and after every sub-step the
+particles that left the slab move to the neighbour below or above
+(sendrecv_particles, src/lagrange.c:4028-4221).  Every slab takes the whole particle
+array (`Slab.set_particles`) and keeps the particles in its planes; `gather_particles`
+puts the slabs' particles back into one array in the caller's order.
 """
 import ctypes as C
 import threading
@@ -251,6 +259,16 @@ class Slab:
                 return 1
         self.set_gather(GATHER_FN(cb), world)
 
+    def set_particles(self, parts):
+        """Every particle of the lattice (a ch4b200.Particle array): the slab keeps those in
+        its planes."""
+        self.sim.set_particles(parts)
+        self.nparts = len(parts)
+
+    def get_particles_into(self, parts):
+        """Write this slab's particles into their entries of `parts` (all particles)."""
+        self.sim._check(lib().ch4_get_particles(self.sim.h, parts, len(parts)), "get_particles")
+
     def set_pop(self, which, aos_whole):
         """Populations of the whole lattice, AoS [NZ][NY][NX][19]: this slab's planes."""
         self.sim.set_pop(which, np.ascontiguousarray(aos_whole[self.z0:self.z0 + self.nz]))
@@ -283,6 +301,15 @@ class Slab:
 
     def close(self):
         self.sim.close()
+
+
+def gather_particles(slabs, n):
+    """The particles of the slabs of one process as one array of n, in the caller's order."""
+    from . import Particle
+    out = (Particle * n)()
+    for s in slabs:
+        s.get_particles_into(out)
+    return out
 
 
 def _in_threads(slabs, fn):

@@ -655,6 +655,18 @@ struct Engine : EngineBase {
   double* pf_alt = nullptr;
   int* pid_alt = nullptr;
   int since_reorder = 0;
+  // z-slab particles: set_particles / get_particles take every particle of the lattice
+  // (np_all); the slab holds np of them.  The particles' u has two halo planes on either
+  // side; particles that leave the slab move through four buffers (send down, send up,
+  // from up, from down) of MIG_HEAD + mig_cap * MIG_REC values each
+  int np_all = 0;
+  bool pslab() const { return c.nz_global > 0 && lagr(); }
+  double* mig = nullptr;
+  int mig_cap = 0;
+  int* keep = nullptr;
+  int* mig_cnt = nullptr;
+  size_t uplane() const { return (size_t)c.NX * c.NY * 4; }  // values of one plane of upart
+  A* ut_in() const { return upart + (pslab() ? 2 * uplane() : 0); }
   // re-sort of the state slots by home cell every REORDER_EVERY steps (a particle
   // moves well under a cell in that time, so the order stays close to sorted)
   static constexpr int REORDER_EVERY = 4;
@@ -734,6 +746,12 @@ struct Engine : EngineBase {
   }
 
   void free_particles() {
+    cudaFree(mig);
+    cudaFree(keep);
+    cudaFree(mig_cnt);
+    mig = nullptr;
+    keep = mig_cnt = nullptr;
+    mig_cap = 0;
     cudaFree(pf);
     cudaFree(pf_alt);
     cudaFree(pid);
@@ -757,6 +775,7 @@ struct Engine : EngineBase {
     cubtmp = nullptr;
     cubbytes = 0;
     np = 0;
+    np_all = 0;
   }
 
   size_t nhome() const { return (size_t)(c.NX + 1) * (c.NY + 1) * (c.NZ + 1); }
@@ -774,6 +793,10 @@ struct Engine : EngineBase {
     Q.NZ = c.NZ;
     Q.N = N;
     Q.np = np;
+    Q.slab = pslab();
+    Q.zoff = pslab() ? c.z_offset : 0;
+    Q.NZg = pslab() ? c.nz_global : c.NZ;
+    Q.nsort = pslab() ? np_all : np;
     Q.SX = c.SX;
     Q.SY = c.SY;
     Q.SZ = c.SZ;
@@ -788,7 +811,7 @@ struct Engine : EngineBase {
     Q.pid = pid;
     Q.pf_alt = pf_alt;
     Q.pid_alt = pid_alt;
-    Q.ut4 = upart;
+    Q.ut4 = ut_in();
     Q.has_t = nsets_on[1];
     Q.key = key;
     Q.order = order;
@@ -942,7 +965,8 @@ struct Engine : EngineBase {
     if (n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "bad particle array");
     ch4_status st;
     if ((st = H->cuda(cudaStreamSynchronize(H->stream), "sync"))) return st;
-    if (n != np) {
+    const bool sl = pslab();
+    if (n != (sl ? np_all : np) || (sl && !mig)) {
       free_particles();
       if (n > 0) {
         if (cudaMalloc(&pf, sizeof(double) * PF_TOTAL * (size_t)n) != cudaSuccess ||
@@ -959,6 +983,17 @@ struct Engine : EngineBase {
                                    cudaMalloc(&srec, sizeof(double) * nrec() * (size_t)n) == cudaSuccess &&
                                    cudaMalloc(&spid, sizeof(int) * (size_t)n) == cudaSuccess));
           if (!ok) return H->fail(CH4_ERR_NOMEM, "sort buffers");
+          if (sl) {
+            // crossings of one face in one sub-step: at most the particles within a cell
+            // of it (|v| dt < 1), about n / NZ, with a wide margin
+            mig_cap = (int)std::min<long long>(n, 4LL * ((n + c.nz_global - 1) / c.nz_global) + 64);
+            const size_t one = MIG_HEAD + (size_t)mig_cap * MIG_REC;
+            if (cudaMalloc(&mig, 4 * one * sizeof(double)) != cudaSuccess ||
+                cudaMalloc(&keep, sizeof(int) * (size_t)n) != cudaSuccess ||
+                cudaMalloc(&mig_cnt, 3 * sizeof(int)) != cudaSuccess)
+              return H->fail(CH4_ERR_NOMEM, "particle exchange buffers");
+            np_all = n;
+          }
           np = n;
           PartParams<A> Q = part_params();
           size_t bytes = 0;
@@ -974,30 +1009,88 @@ struct Engine : EngineBase {
     for (int i = 0; i < n; i++)
       if (!std::isfinite(parts[i].x) || !std::isfinite(parts[i].y) || !std::isfinite(parts[i].z))
         return H->fail(CH4_ERR_ARG, "particle %d has a non-finite position", i);
+    // the caller's indices of the particles held here: all, or a z-slab's own
+    std::vector<int> ids;
+    {
+      const PartParams<A> Q = part_params();
+      for (int i = 0; i < n; i++)
+        if (!sl || slab_owns(Q, pwrapd(parts[i].z, c.SZ))) ids.push_back(i);
+    }
+    n = (int)ids.size();
+    np = n;
     // AoS -> SoA with the two per-particle deposit constants (src/lagrange_feedback.c:84-90, host libm)
     std::vector<double> h((size_t)PF_TOTAL * n);
-    const double* raw = reinterpret_cast<const double*>(parts);
     for (int i = 0; i < n; i++) {
-      for (int f = 0; f < PF_FIELDS; f++) h[(size_t)f * n + i] = raw[(size_t)i * PF_FIELDS + f];
-      double beta = parts[i].beta_coeff, tau = parts[i].tau_drag;
+      const ch4_particle& pi = parts[ids[i]];
+      const double* raw = reinterpret_cast<const double*>(&pi);
+      for (int f = 0; f < PF_FIELDS; f++) h[(size_t)f * n + i] = raw[f];
+      double beta = pi.beta_coeff, tau = pi.tau_drag;
       h[(size_t)PF_DR * n + i] = (3.0 - beta) / (2.0 * beta);
       double squared_radius = 3.0 * c.nu * beta * tau;
       h[(size_t)PF_VOL * n + i] = (4. / 3.) * 3.14159265359 * std::pow(squared_radius, 3. / 2.);
       if (c.flags2 & CH4_F2_LAGRANGE_TEMPERATURE) {
         // 1/tau_heat = 2 kappa / (tau_drag nu cp_p (3 - beta)) times dt_lagr, and exp(-fac1),
         // src/lagrange.c:4009-4017 (host libm, as the reference)
-        double fac1 = (c.kappa * 2.0) / (tau * c.nu * parts[i].cp_p * (3 - beta));
+        double fac1 = (c.kappa * 2.0) / (tau * c.nu * pi.cp_p * (3 - beta));
         fac1 *= c.time_dt / c.time_dt_lagr_factor;
         h[(size_t)PF_TFAC * n + i] = fac1;
         h[(size_t)PF_TEXP * n + i] = std::exp(-fac1);
       }
     }
-    if ((st = H->cuda(cudaMemcpy(pf, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice), "particles up")))
+    if (n > 0 &&
+        (st = H->cuda(cudaMemcpy(pf, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice), "particles up")))
       return st;
-    std::vector<int> ids(n);
-    for (int i = 0; i < n; i++) ids[i] = i;
     since_reorder = REORDER_EVERY;  // sort at the first opportunity
+    if (n == 0) return CH4_OK;
     return H->cuda(cudaMemcpy(pid, ids.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "particle ids up");
+  }
+
+  // z-slab: u^{n+1} of the two planes next to each face to the neighbours, theirs into the
+  // two halo planes on either side (the interpolation stencil of a particle reaches two
+  // planes beyond the slab)
+  ch4_status u_halo() {
+    if (!H->exchange) return H->fail(CH4_ERR_STATE, "z-slab with particles: no ch4_set_exchange");
+    // u^{n+1} of the face planes needs the populations the neighbours stream in: the faces
+    // must have moved inside the step
+    if (!H->face_exchange)
+      return H->fail(CH4_ERR_STATE, "z-slab with particles: the faces must move inside ch4_step (ch4_set_face_exchange)");
+    const size_t pl = uplane();
+    A* in = ut_in();
+    if (H->exchange(in, in + (size_t)(c.NZ - 2) * pl, in + (size_t)c.NZ * pl, upart, 2 * pl * sizeof(A), H->stream,
+                    H->exchange_user) != 0)
+      return H->fail(CH4_ERR_CUDA, "the exchange of the slabs' particle u planes failed");
+    return CH4_OK;
+  }
+
+  // z-slab: the particles that left the slab go to the neighbours, theirs come in
+  // (sendrecv_particles, src/lagrange.c:4028-4221)
+  ch4_status migrate() {
+    if (!H->exchange) return H->fail(CH4_ERR_STATE, "z-slab with particles: no ch4_set_exchange");
+    const size_t one = MIG_HEAD + (size_t)mig_cap * MIG_REC;
+    double *sd = mig, *su = mig + one, *fu = mig + 2 * one, *fd = mig + 3 * one;
+    PartParams<A> Q = part_params();
+    ch4_status st;
+    if ((st = H->cuda(launch_particle_leave(Q, sd, su, mig_cap, keep, mig_cnt, H->stream), "particles leave")))
+      return st;
+    if (H->exchange(sd, su, fu, fd, one * sizeof(double), H->stream, H->exchange_user) != 0)
+      return H->fail(CH4_ERR_CUDA, "the exchange of the slabs' particles failed");
+    int nk = 0;
+    double nd = 0, nu = 0;
+    if ((st = H->cuda(cudaMemcpyAsync(&nk, mig_cnt, sizeof(int), cudaMemcpyDeviceToHost, H->stream), "counts")) ||
+        (st = H->cuda(cudaMemcpyAsync(&nd, fd, sizeof(double), cudaMemcpyDeviceToHost, H->stream), "counts")) ||
+        (st = H->cuda(cudaMemcpyAsync(&nu, fu, sizeof(double), cudaMemcpyDeviceToHost, H->stream), "counts")) ||
+        (st = H->cuda(cudaStreamSynchronize(H->stream), "counts")))
+      return st;
+    const long long n_new = (long long)nk + (long long)nd + (long long)nu;
+    if (nd < 0 || nu < 0 || nd > mig_cap || nu > mig_cap || n_new > np_all)
+      return H->fail(CH4_ERR_STATE, "particle exchange: %d kept + %g + %g arriving exceeds the %d particles", nk, nd,
+                     nu, np_all);
+    if ((st = H->cuda(launch_particle_arrive(Q, keep, nk, fd, (int)nd, fu, (int)nu, H->stream), "particles arrive")))
+      return st;
+    std::swap(pf, pf_alt);
+    std::swap(pid, pid_alt);
+    np = (int)n_new;
+    return CH4_OK;
   }
 
   // slot order <- order2 (sorted by home cell); with sort, compute and sort the keys here
@@ -1017,6 +1110,10 @@ struct Engine : EngineBase {
     int flag = 0;
     ch4_status st;
     if ((st = H->cuda(cudaMemcpy(&flag, pstatus, sizeof(int), cudaMemcpyDeviceToHost), "particle status"))) return st;
+    if (flag & 2)
+      return H->fail(CH4_ERR_STATE,
+                     "more particles left a z-slab through one face in one sub-step than its exchange "
+                     "buffer holds; particles were lost");
     if (flag)
       return H->fail(CH4_ERR_NUMERIC,
                      "a particle position left the box or became non-finite (the coupled particle-fluid "
@@ -1070,6 +1167,7 @@ struct Engine : EngineBase {
   }
 
   ch4_status particle_averages(int types, double* out) override {
+    if (pslab()) return H->fail(CH4_ERR_UNSUPPORTED, "particle averages of a z-slab: average the gathered particles");
     if (np <= 0) return H->fail(CH4_ERR_ARG, "no particles");
     if (types < 1) return H->fail(CH4_ERR_ARG, "particle_types must be >= 1");
     const int nblk = (int)std::min<long long>(4 * 148, ((long long)np + 127) / 128);
@@ -1088,8 +1186,13 @@ struct Engine : EngineBase {
 
   int particle_count() const override { return np; }
   ch4_status get_particles(ch4_particle* parts, int n) override {
-    if (n > np || n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "asked for %d of %d particles", n, np);
-    if (n == 0) return CH4_OK;
+    // a z-slab fills the entries of the particles it holds in an array of all of them
+    const int lim = pslab() ? np_all : np;
+    if (n < 0 || (n > 0 && !parts)) return H->fail(CH4_ERR_ARG, "bad particle array");
+    if (pslab() && n != np_all)
+      return H->fail(CH4_ERR_ARG, "a z-slab fills an array of all %d particles (asked for %d)", np_all, n);
+    if (!pslab() && n > np) return H->fail(CH4_ERR_ARG, "asked for %d of %d particles", n, np);
+    if (n == 0 || np == 0) return CH4_OK;
     std::vector<double> h((size_t)PF_TOTAL * np);
     std::vector<int> ids(np);
     ch4_status st;
@@ -1101,7 +1204,7 @@ struct Engine : EngineBase {
     double* raw = reinterpret_cast<double*>(parts);
     for (int s = 0; s < np; s++) {
       const int i = ids[s];  // the caller's index of state slot s
-      if (i < 0 || i >= np) return H->fail(CH4_ERR_CUDA, "particle index table corrupted");
+      if (i < 0 || i >= lim) return H->fail(CH4_ERR_CUDA, "particle index table corrupted");
       if (i < n)
         for (int f = 0; f < PF_FIELDS; f++) raw[(size_t)i * PF_FIELDS + f] = h[(size_t)f * np + s];
     }
@@ -1133,7 +1236,8 @@ struct Engine : EngineBase {
     }
     if (nsets_on[1] && cudaMalloc(&tprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tprev");
     if (nsets_on[2] && cudaMalloc(&sprev, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "sprev");
-    if (lagr() && cudaMalloc(&upart, 4 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "u for particles");
+    if (lagr() && cudaMalloc(&upart, (pslab() ? (size_t)(c.NZ + 4) * uplane() : 4 * (size_t)N) * sizeof(A)) != cudaSuccess)
+      return H->fail(CH4_ERR_NOMEM, "u for particles");
     if (lagr()) {
       if (cudaMalloc(&pstatus, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "particle status");
       if (cudaMemset(pstatus, 0, sizeof(int)) != cudaSuccess) return H->fail(CH4_ERR_CUDA, "particle status");
@@ -1587,13 +1691,16 @@ struct Engine : EngineBase {
           // u^{n+1} with dt/2 F^n, then the Lagrangian sub-steps (src/main.c:164-185)
           bind_pops(cur);
           if ((st = H->cuda(launch_hydro(P, shape, P.hit_cur, twoway() ? P.dcur : nullptr, fm_last(), nullptr, nullptr, nullptr,
-                                         nullptr, nullptr, nullptr, H->stream, upart),
+                                         nullptr, nullptr, nullptr, H->stream, ut_in()),
                             "particle u")))
             return st;
-          PartParams<A> Q = part_params();
-          Q.first = (n_step == 1 && c.resume == 0);
-          for (int sub = 0; sub < (int)c.time_dt_lagr_factor; sub++)
+          if (pslab() && (st = u_halo())) return st;
+          for (int sub = 0; sub < (int)c.time_dt_lagr_factor; sub++) {
+            PartParams<A> Q = part_params();
+            Q.first = (n_step == 1 && c.resume == 0);
             if ((st = H->cuda(launch_particle_substep(Q, H->stream), "particle substep"))) return st;
+            if (pslab() && (st = migrate())) return st;  // move_particles ends with sendrecv_particles
+          }
         }
       }
       if (hit && (st = H->cuda(cudaMemcpyAsync(hit_last, hit_ring + (size_t)m * slot, slot * sizeof(A),
@@ -2032,9 +2139,17 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
   if (c->nz_global > 0) {
     if (c->z_offset < 0 || c->z_offset + c->NZ > c->nz_global) return why = "z-slab outside the lattice", CH4_ERR_ARG;
     if (c->nz_global > 65535) return why = "nz_global must be <= 65535", CH4_ERR_ARG;
-    // z-slabs exchange populations only: no z-halo of u (LES), no global sums inside
-    // the step (force corrections), no particle migration
-    if (c->flags & CH4_F_LAGRANGE) return why = "z-slab handles run without particles", CH4_ERR_UNSUPPORTED;
+    // particles on z-slabs: a periodic lattice (no wall of any set and no wall-mode
+    // gradient: the particles read only u halos exchanged between slabs), one-way coupling,
+    // slabs at least two planes deep (the two halo planes of u come from one neighbour)
+    if (c->flags & CH4_F_LAGRANGE) {
+      if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) ||
+          (c->flags2 & (CH4_F2_FLUID_BC | CH4_F2_TEMPERATURE_BC | CH4_F2_SCALAR_BC)))
+        return why = "particles on z-slabs need a periodic lattice", CH4_ERR_UNSUPPORTED;
+      if (c->flags & CH4_F_LAGRANGE_TWOWAY)
+        return why = "particles on z-slabs run with one-way coupling", CH4_ERR_UNSUPPORTED;
+      if (c->NZ < 2) return why = "particles on z-slabs need slabs of at least two planes", CH4_ERR_UNSUPPORTED;
+    }
   }
   if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) && c->NY < 3)
     return why = "walls need NY >= 3", CH4_ERR_ARG;

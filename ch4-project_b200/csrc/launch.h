@@ -75,6 +75,18 @@ cudaError_t launch_particle_reorder(const PartParams<float>& P, unsigned int* ke
 // Lagrangian particles: one sub-step (interpolate + move + wrap)
 cudaError_t launch_particle_substep(const PartParams<double>& P, cudaStream_t st);
 cudaError_t launch_particle_substep(const PartParams<float>& P, cudaStream_t st);
+// z-slab particle exchange (sendrecv_particles): leavers into the two send buffers (2-value
+// header + records of 1 + PF_TOTAL values, at most cap each way), kept slots into keep,
+// counts[3] = kept, down, up; then the new slots (kept, from below, from above) into
+// P.pf_alt / P.pid_alt
+cudaError_t launch_particle_leave(const PartParams<double>& P, double* send_down, double* send_up, int cap, int* keep,
+                                  int* counts, cudaStream_t st);
+cudaError_t launch_particle_leave(const PartParams<float>& P, double* send_down, double* send_up, int cap, int* keep,
+                                  int* counts, cudaStream_t st);
+cudaError_t launch_particle_arrive(const PartParams<double>& P, const int* keep, int nkeep, const double* from_down,
+                                   int nd, const double* from_up, int nu, cudaStream_t st);
+cudaError_t launch_particle_arrive(const PartParams<float>& P, const int* keep, int nkeep, const double* from_down,
+                                   int nd, const double* from_up, int nu, cudaStream_t st);
 // two-way deposit into P.dep; `tmp`/`tmp_bytes` is CUB scratch (query with tmp == nullptr),
 // key2/order2 are the sort's output buffers
 cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,

@@ -48,6 +48,14 @@ cudaError_t launch_particle_reorder(const PartParams<float>& P, unsigned int* ke
                                     size_t& tmp_bytes, int sort, cudaStream_t st) {
   return reorder_t<float>(P, key2, order2, tmp, tmp_bytes, sort, st);
 }
+cudaError_t launch_particle_leave(const PartParams<float>& P, double* send_down, double* send_up, int cap, int* keep,
+                                  int* counts, cudaStream_t st) {
+  return leave_t<float>(P, send_down, send_up, cap, keep, counts, st);
+}
+cudaError_t launch_particle_arrive(const PartParams<float>& P, const int* keep, int nkeep, const double* from_down,
+                                   int nd, const double* from_up, int nu, cudaStream_t st) {
+  return arrive_t<float>(P, keep, nkeep, from_down, nd, from_up, nu, st);
+}
 cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
                            cudaStream_t st) {
   return deposit_t<float>(P, key2, order2, tmp, tmp_bytes, st);

@@ -95,6 +95,14 @@ cudaError_t launch_particle_reorder(const PartParams<double>& P, unsigned int* k
                                     size_t& tmp_bytes, int sort, cudaStream_t st) {
   return reorder_t<double>(P, key2, order2, tmp, tmp_bytes, sort, st);
 }
+cudaError_t launch_particle_leave(const PartParams<double>& P, double* send_down, double* send_up, int cap, int* keep,
+                                  int* counts, cudaStream_t st) {
+  return leave_t<double>(P, send_down, send_up, cap, keep, counts, st);
+}
+cudaError_t launch_particle_arrive(const PartParams<double>& P, const int* keep, int nkeep, const double* from_down,
+                                   int nd, const double* from_up, int nu, cudaStream_t st) {
+  return arrive_t<double>(P, keep, nkeep, from_down, nd, from_up, nu, st);
+}
 cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
                            cudaStream_t st) {
   return deposit_t<double>(P, key2, order2, tmp, tmp_bytes, st);

@@ -23,6 +23,7 @@
 // every per-cell sum keeps the reference's order.
 #pragma once
 #include <cfloat>
+#include <cmath>
 #include <cstddef>
 
 #include "../../include/ch4.h"
@@ -46,6 +47,11 @@ struct PartParams {
   int NX, NY, NZ;
   long long N;
   int np;
+  // z-slab of a larger periodic lattice (slab != 0): particles hold global positions, the
+  // slab owns those with z in [zoff, zoff + NZ) (src/lagrange.c:4083-4090), and ut4 points
+  // at local plane 0 of an array with two halo planes on either side (the neighbours' u)
+  int slab, zoff, NZg;  // NZg: the whole lattice's NZ (= NZ without slabs)
+  int nsort;            // entries of the sort by particle index (np; all particles with slabs)
   double SX, SY, SZ, dtl;
   int first;      // itime == 1 && resume == 0 (src/lagrange.c:3190)
   int gradient;   // LAGRANGE_GRADIENT
@@ -100,9 +106,21 @@ struct PartParams {
   int second, gyro, swim;
 };
 
-#ifdef __CUDACC__
+// periodic wrap of a coordinate into [0, S) (the reference's wrap, src/lagrange.c)
+__host__ __device__ __forceinline__ double pwrapd(double x, double S) { return (x) - floor((x) / S) * S; }
 
-__device__ __forceinline__ double pwrapd(double x, double S) { return (x) - floor((x) / S) * S; }
+// z-slab particle exchange buffers: a 2-value header (the count), then per particle its
+// index and its state
+constexpr int MIG_HEAD = 2, MIG_REC = PF_TOTAL + 1;
+
+// whether a z-slab owns a wrapped z (the last slab also takes z == SZ, which the wrap can
+// round to)
+template <typename A>
+__host__ __device__ __forceinline__ bool slab_owns(const PartParams<A>& P, double pz) {
+  return pz >= (double)P.zoff && (pz < (double)(P.zoff + P.NZ) || (P.zoff + P.NZ == P.NZg && pz <= P.SZ));
+}
+
+#ifdef __CUDACC__
 
 struct Stencil {
   int im, jm, km;
@@ -120,10 +138,14 @@ __device__ __forceinline__ bool wrapped_position(const PartParams<A>& P, double 
   px = pwrapd(x, P.SX);
   py = pwrapd(y, P.SY);
   pz = pwrapd(z, P.SZ);
-  const bool ok = px >= 0.0 && px <= P.SX && py >= 0.0 && py <= P.SY && pz >= 0.0 && pz <= P.SZ;
+  // a z-slab reads u only within its two halo planes: a particle it does not own (one that
+  // crossed more than the neighbouring slab in one sub-step) is reported, not interpolated
+  const bool ok = px >= 0.0 && px <= P.SX && py >= 0.0 && py <= P.SY && pz >= 0.0 && pz <= P.SZ &&
+                  (!P.slab || slab_owns(P, pz));
   if (!ok) {
     atomicOr(P.status, 1);
-    px = py = pz = 0.0;
+    px = py = 0.0;
+    pz = P.slab ? (double)P.zoff + 0.5 : 0.0;
   }
   return ok;
 }
@@ -385,7 +407,8 @@ __device__ __forceinline__ void interp_lines(const PartParams<C>& P, const Stenc
   for (int q = 0; q < 4; q++) {
     o.xo[q] = pmod(t.im - 1 + q, P.NX);
     o.yo[q] = pmod(t.jm - 1 + q, P.NY) * P.NX;
-    o.zo[q] = (long long)pmod(t.km - 1 + q, P.NZ) * P.NX * P.NY;
+    o.zo[q] = P.slab ? (long long)(t.km - P.zoff - 1 + q) * P.NX * P.NY  // halo planes -2 .. NZ+1
+                     : (long long)pmod(t.km - 1 + q, P.NZ) * P.NX * P.NY;
   }
   if constexpr (GRAD) {  // the cells only the y and z passes read: on their way while x runs
 #pragma unroll
@@ -399,8 +422,8 @@ __device__ __forceinline__ void interp_lines(const PartParams<C>& P, const Stenc
         }
   }
   const bool lo[3] = {t.im == -1, t.jm == -1, t.km == -1};
-  const bool hi[3] = {t.im + 1 == P.NX, t.jm + 1 == P.NY, t.km + 1 == P.NZ};
-  const bool one[3] = {P.NX == 1, P.NY == 1, P.NZ == 1};
+  const bool hi[3] = {t.im + 1 == P.NX, t.jm + 1 == P.NY, t.km + 1 == P.NZg};  // the lattice's last layer
+  const bool one[3] = {P.NX == 1, P.NY == 1, P.NZg == 1};
   C w[8];
 #pragma unroll
   for (int c = 0; c < 8; c++) {
@@ -999,7 +1022,7 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   }
   // particles that deposit nothing sort after every home cell (still in spatial
   // order among themselves) and are never merged
-  const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km + 1);
+  const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km - P.zoff + 1);
   const unsigned int nh = (unsigned)(P.NX + 1) * (unsigned)(P.NY + 1) * (unsigned)(P.NZ + 1);
   P.key[o] = (live ? 0u : nh) + (hz * (unsigned)(P.NY + 1) + hy) * (unsigned)(P.NX + 1) + hx;
   P.order[o] = ip;
@@ -1017,7 +1040,7 @@ __global__ void particle_key_kernel(const PartParams<A> P) {
   wrapped_position(P, pf[CH4_PF(x) * np + ip], pf[CH4_PF(y) * np + ip], pf[CH4_PF(z) * np + ip], px, py, pz);
   Stencil t;
   make_stencil(px, py, pz, t);
-  const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km + 1);
+  const unsigned int hx = (unsigned)(t.im + 1), hy = (unsigned)(t.jm + 1), hz = (unsigned)(t.km - P.zoff + 1);
   const int o = P.pid[ip];
   P.key[o] = (hz * (unsigned)(P.NY + 1) + hy) * (unsigned)(P.NX + 1) + hx;
   P.order[o] = ip;
@@ -1033,6 +1056,67 @@ __global__ void particle_permute_kernel(const PartParams<A> P, const int* __rest
   P.pid_alt[i] = P.pid[s];
 #pragma unroll 5
   for (int f = 0; f < PF_TOTAL; f++) P.pf_alt[f * np + i] = P.pf[f * np + s];
+}
+
+// z-slab particle exchange (sendrecv_particles, src/lagrange.c:4028-4221).  A particle
+// whose wrapped z left the slab goes to the neighbour below or above (the nearer way round
+// the periodic z): its index and state (1 + PF_TOTAL values) are appended to that
+// direction's buffer, after a 2-value header (the count); the others are listed to keep.
+// counts: [0] kept, [1] down, [2] up.  More than `cap` leavers one way: status bit 2.
+
+template <typename A>
+__global__ void particle_leave_kernel(const PartParams<A> P, double* send_down, double* send_up, int cap, int* keep,
+                                      int* counts) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= P.np) return;
+  const long long np = P.np;
+  const double pz = pwrapd(P.pf[CH4_PF(z) * np + ip], P.SZ);
+  if (slab_owns(P, pz)) {
+    keep[atomicAdd(counts, 1)] = ip;
+    return;
+  }
+  double d = pz - ((double)P.zoff + 0.5 * (double)P.NZ);
+  if (d > 0.5 * P.SZ) d -= P.SZ;
+  if (d < -0.5 * P.SZ) d += P.SZ;
+  const int dir = d < 0.0 ? 1 : 2;
+  const int k = atomicAdd(counts + dir, 1);
+  if (k >= cap) {
+    atomicOr(P.status, 2);
+    return;
+  }
+  double* b = (dir == 1 ? send_down : send_up) + MIG_HEAD + (long long)k * MIG_REC;
+  b[0] = (double)P.pid[ip];
+  for (int f = 0; f < PF_TOTAL; f++) b[1 + f] = P.pf[f * np + ip];
+}
+
+// the counts into the buffers' headers
+static __global__ void particle_leave_heads_kernel(double* send_down, double* send_up, int cap, const int* counts) {
+  if (threadIdx.x == 0) {
+    send_down[0] = (double)min(counts[1], cap);
+    send_up[0] = (double)min(counts[2], cap);
+  }
+}
+
+// slot i of (pf_alt, pid_alt), np_new = nkeep + nd + nu slots: the kept slots, then the
+// arrivals from below and from above (P.np: the slots before the exchange)
+template <typename A>
+__global__ void particle_arrive_kernel(const PartParams<A> P, const int* __restrict__ keep, int nkeep,
+                                       const double* from_down, int nd, const double* from_up, int nu) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n_new = (long long)nkeep + nd + nu;
+  if (i >= n_new) return;
+  const long long np = P.np;
+  if (i < nkeep) {
+    const int s = keep[i];
+    P.pid_alt[i] = P.pid[s];
+    for (int f = 0; f < PF_TOTAL; f++) P.pf_alt[f * n_new + i] = P.pf[f * np + s];
+    return;
+  }
+  const int j = i - nkeep;
+  const double* b = (j < nd ? from_down + MIG_HEAD + (long long)j * MIG_REC
+                            : from_up + MIG_HEAD + (long long)(j - nd) * MIG_REC);
+  P.pid_alt[i] = (int)b[0];
+  for (int f = 0; f < PF_TOTAL; f++) P.pf_alt[f * n_new + i] = b[1 + f];
 }
 
 // [start, end) of every home cell in the sorted key array, and the records and

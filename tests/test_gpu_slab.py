@@ -207,3 +207,68 @@ def test_overlapped_faces_reproduce_the_single_lattice(name, storage, nslabs, ex
     finally:
         for s in slabs:
             s.close()
+
+
+def _owner(z, bounds):
+    for i, (z0, nz) in enumerate(bounds):
+        if z0 <= z < z0 + nz:
+            return i
+    return len(bounds) - 1
+
+
+@pytest.mark.parametrize("name,nslabs,swim", [("particles_1w", 2, None), ("particles_swimb", 3, 0.35),
+                                               ("particles_swims", 2, 0.2), ("particles_swimt", 3, 0.25)])
+def test_particles_on_slabs_reproduce_the_single_lattice(name, nslabs, swim):
+    """One-way particles on z-slabs: the population faces move inside the step, then each
+    slab interpolates from its u planes plus two halo planes from either neighbour and hands
+    the particles that leave it to the neighbour after every sub-step (here between the
+    threads of one process).  Swimmers at a few
+    tenths of a cell per step cross the faces and the periodic z boundary many times; every
+    particle field and population equals the single lattice's, bit for bit."""
+    _, cfg, state = make_case(name, seed=47)
+    parts = state["part"]
+    if swim is not None:
+        for p in parts:
+            p.swim_velocity = swim
+    nsteps = 10
+    n = len(parts)
+    with ch4b200.Simulation(cfg) as sim:
+        for k, v in pop_items(state):
+            sim.set_pop(k, v)
+        sim.set_particles(parts)
+        sim.initialize()
+        sim.step(nsteps)
+        want = sim.get_particles(n)
+        pops = {k: sim.get_pop(k) for k, _ in pop_items(state)}
+    b = slab.bounds(cfg.NZ, nslabs)
+    slabs = [slab.Slab(cfg, z0, nz) for z0, nz in b]
+    try:
+        slab.use_local_faces(slabs)  # u^{n+1} of the face planes needs the faces moved inside the step
+        slab.use_local_exchange(slabs)
+        for s in slabs:
+            for k, v in pop_items(state):
+                s.set_pop(k, v)
+            s.set_particles(parts)
+        slab.initialize_local(slabs)
+        slab.step_local(slabs, nsteps)
+        got = slab.gather_particles(slabs, n)
+        for k, _ in pop_items(state):
+            assert np.array_equal(np.concatenate([s.sim.get_pop(k) for s in slabs]), pops[k]), k
+    finally:
+        for s in slabs:
+            s.close()
+    fields = [f for f, _ in ch4b200.Particle._fields_]
+    for f in fields:
+        a = np.array([getattr(p, f) for p in want])
+        g = np.array([getattr(p, f) for p in got])
+        assert np.array_equal(a, g), "particle field %s: max |d| %g" % (f, np.abs(a - g).max())
+    moved = sum(_owner(parts[i].z % cfg.SZ, b) != _owner(want[i].z % cfg.SZ, b) for i in range(n))
+    if swim is not None:
+        assert moved > n // 10, "only %d of %d particles changed slab" % (moved, n)
+
+
+def test_particles_on_slabs_refuse_walls_and_two_way_coupling():
+    for name in ("particles", "particles_rb"):
+        _, cfg, _ = make_case(name, seed=48)
+        with pytest.raises(ch4b200.CH4Error):
+            slab.Slab(cfg, 0, cfg.NZ // 2)
