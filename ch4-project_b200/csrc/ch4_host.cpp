@@ -797,6 +797,7 @@ struct Engine : EngineBase {
     Q.zoff = pslab() ? c.z_offset : 0;
     Q.NZg = pslab() ? c.nz_global : c.NZ;
     Q.nsort = pslab() ? np_all : np;
+    Q.rstride = pslab() ? np_all : np;
     Q.SX = c.SX;
     Q.SY = c.SY;
     Q.SZ = c.SZ;
@@ -1661,9 +1662,26 @@ struct Engine : EngineBase {
           if (c.resume || n_step > 1) {
             PartParams<A> Q = part_params();
             size_t bytes = cubbytes;
-            if ((st = H->cuda(launch_deposit(Q, key2, order2, cubtmp, bytes, H->stream), "deposit"))) return st;
-            // the deposit's sort already holds the slots in home-cell order
-            if (np > 0 && ++since_reorder >= REORDER_EVERY && (st = reorder_particles(0))) return st;
+            if (pslab()) {
+              // the records of the particles next to a face go to the neighbour, theirs come in
+              if (!H->exchange) return H->fail(CH4_ERR_STATE, "z-slab with particles: no ch4_set_exchange");
+              const size_t one = MIG_HEAD + (size_t)mig_cap * MIG_REC;
+              double *sd = mig, *su = mig + one, *fu = mig + 2 * one, *fd = mig + 3 * one;
+              if ((st = H->cuda(launch_deposit(Q, key2, order2, cubtmp, bytes, H->stream, 1), "deposit records")) ||
+                  (st = H->cuda(launch_ghosts_out(Q, sd, su, mig_cap, mig_cnt, H->stream), "deposit ghosts")))
+                return st;
+              if (H->exchange(sd, su, fu, fd, one * sizeof(double), H->stream, H->exchange_user) != 0)
+                return H->fail(CH4_ERR_CUDA, "the exchange of the slabs' deposit records failed");
+              if ((st = H->cuda(launch_ghosts_in(Q, fd, fu, mig_cap, H->stream), "deposit ghosts")) ||
+                  (st = H->cuda(launch_deposit(Q, key2, order2, cubtmp, bytes, H->stream, 2), "deposit")))
+                return st;
+              // (the sort holds ghosts too: the slots are re-sorted on their own)
+              if (np > 0 && ++since_reorder >= REORDER_EVERY && (st = reorder_particles(1))) return st;
+            } else {
+              if ((st = H->cuda(launch_deposit(Q, key2, order2, cubtmp, bytes, H->stream), "deposit"))) return st;
+              // the deposit's sort already holds the slots in home-cell order
+              if (np > 0 && ++since_reorder >= REORDER_EVERY && (st = reorder_particles(0))) return st;
+            }
           } else if ((st = H->cuda(cudaMemsetAsync(dbuf[dcur_i], 0, dplanes() * N * sizeof(A), H->stream),
                                    "deposit zero"))) {
             return st;
@@ -2140,14 +2158,15 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
     if (c->z_offset < 0 || c->z_offset + c->NZ > c->nz_global) return why = "z-slab outside the lattice", CH4_ERR_ARG;
     if (c->nz_global > 65535) return why = "nz_global must be <= 65535", CH4_ERR_ARG;
     // particles on z-slabs: a periodic lattice (no wall of any set and no wall-mode
-    // gradient: the particles read only u halos exchanged between slabs), one-way coupling,
-    // slabs at least two planes deep (the two halo planes of u come from one neighbour)
+    // gradient: the particles read only u halos exchanged between slabs), slabs at least two
+    // planes deep (the two halo planes of u come from one neighbour)
     if (c->flags & CH4_F_LAGRANGE) {
       if ((c->flags & (CH4_F_FLUID_BC_Y | CH4_F_TEMPERATURE_BC_Y | CH4_F_SCALAR_BC_Y)) ||
           (c->flags2 & (CH4_F2_FLUID_BC | CH4_F2_TEMPERATURE_BC | CH4_F2_SCALAR_BC)))
         return why = "particles on z-slabs need a periodic lattice", CH4_ERR_UNSUPPORTED;
-      if (c->flags & CH4_F_LAGRANGE_TWOWAY)
-        return why = "particles on z-slabs run with one-way coupling", CH4_ERR_UNSUPPORTED;
+      // (the tricubic and the thermal deposits fold values across the box faces differently)
+      if ((c->flags & CH4_F_LAGRANGE_TWOWAY_TRICUBIC) || (c->flags2 & CH4_F2_LAGRANGE_TWOWAY_TEMPERATURE))
+        return why = "particles on z-slabs deposit with the trilinear momentum kernel only", CH4_ERR_UNSUPPORTED;
       if (c->NZ < 2) return why = "particles on z-slabs need slabs of at least two planes", CH4_ERR_UNSUPPORTED;
     }
   }

@@ -89,10 +89,21 @@ cudaError_t launch_particle_arrive(const PartParams<float>& P, const int* keep, 
                                    int nd, const double* from_up, int nu, cudaStream_t st);
 // two-way deposit into P.dep; `tmp`/`tmp_bytes` is CUB scratch (query with tmp == nullptr),
 // key2/order2 are the sort's output buffers
+// (stage 0: all; 1: the keys and records of the slab's own particles; 2: the sort and gather)
 cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
-                           cudaStream_t st);
+                           cudaStream_t st, int stage = 0);
 cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
-                           cudaStream_t st);
+                           cudaStream_t st, int stage = 0);
+// z-slab two-way deposit: the ghost records for the neighbours out (between stages 1 and 2),
+// the neighbours' in
+cudaError_t launch_ghosts_out(const PartParams<double>& P, double* send_down, double* send_up, int cap, int* counts,
+                              cudaStream_t st);
+cudaError_t launch_ghosts_out(const PartParams<float>& P, double* send_down, double* send_up, int cap, int* counts,
+                              cudaStream_t st);
+cudaError_t launch_ghosts_in(const PartParams<double>& P, const double* from_down, const double* from_up, int cap,
+                             cudaStream_t st);
+cudaError_t launch_ghosts_in(const PartParams<float>& P, const double* from_down, const double* from_up, int cap,
+                             cudaStream_t st);
 
 // Lagrangian averages per particle type (dump_particle_averages): partial holds
 // types * 3 * nblk * 11 * 2 doubles, out_dev receives [types][CH4_PART_AVG_FIELDS]

@@ -57,8 +57,16 @@ cudaError_t launch_particle_arrive(const PartParams<float>& P, const int* keep, 
   return arrive_t<float>(P, keep, nkeep, from_down, nd, from_up, nu, st);
 }
 cudaError_t launch_deposit(const PartParams<float>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
-                           cudaStream_t st) {
-  return deposit_t<float>(P, key2, order2, tmp, tmp_bytes, st);
+                           cudaStream_t st, int stage) {
+  return deposit_t<float>(P, key2, order2, tmp, tmp_bytes, st, stage);
+}
+cudaError_t launch_ghosts_out(const PartParams<float>& P, double* send_down, double* send_up, int cap, int* counts,
+                              cudaStream_t st) {
+  return ghosts_out_t<float>(P, send_down, send_up, cap, counts, st);
+}
+cudaError_t launch_ghosts_in(const PartParams<float>& P, const double* from_down, const double* from_up, int cap,
+                             cudaStream_t st) {
+  return ghosts_in_t<float>(P, from_down, from_up, cap, st);
 }
 template <typename S, bool T, bool H>
 static cudaError_t ens_t(const StepParams<float>* params, const EnsTile* tiles, int ntiles, int* counter, int grid,

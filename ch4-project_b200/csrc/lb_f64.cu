@@ -104,7 +104,15 @@ cudaError_t launch_particle_arrive(const PartParams<double>& P, const int* keep,
   return arrive_t<double>(P, keep, nkeep, from_down, nd, from_up, nu, st);
 }
 cudaError_t launch_deposit(const PartParams<double>& P, unsigned int* key2, int* order2, void* tmp, size_t& tmp_bytes,
-                           cudaStream_t st) {
-  return deposit_t<double>(P, key2, order2, tmp, tmp_bytes, st);
+                           cudaStream_t st, int stage) {
+  return deposit_t<double>(P, key2, order2, tmp, tmp_bytes, st, stage);
+}
+cudaError_t launch_ghosts_out(const PartParams<double>& P, double* send_down, double* send_up, int cap, int* counts,
+                              cudaStream_t st) {
+  return ghosts_out_t<double>(P, send_down, send_up, cap, counts, st);
+}
+cudaError_t launch_ghosts_in(const PartParams<double>& P, const double* from_down, const double* from_up, int cap,
+                             cudaStream_t st) {
+  return ghosts_in_t<double>(P, from_down, from_up, cap, st);
 }
 }  // namespace ch4

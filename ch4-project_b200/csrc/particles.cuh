@@ -52,6 +52,8 @@ struct PartParams {
   // at local plane 0 of an array with two halo planes on either side (the neighbours' u)
   int slab, zoff, NZg;  // NZg: the whole lattice's NZ (= NZ without slabs)
   int nsort;            // entries of the sort by particle index (np; all particles with slabs)
+  int rstride;          // stride of the deposit records (np; all particles with slabs: the
+                        // slab's own particles, then the neighbours' ghosts)
   double SX, SY, SZ, dtl;
   int first;      // itime == 1 && resume == 0 (src/lagrange.c:3190)
   int gradient;   // LAGRANGE_GRADIENT
@@ -61,7 +63,7 @@ struct PartParams {
   int jeffery;    // LAGRANGE_ORIENTATION_JEFFREY: Jeffery's equation for p
   double g[3];    // gravity_x, gravity_y, gravity_z
   double* pf;     // [PF_TOTAL][np] by state slot
-  const int* pid; // particle index of each slot
+  int* pid;       // particle index of each slot (z-slab ghosts: also of the ghost record slots)
   double* pf_alt; // reorder target of pf / pid
   int* pid_alt;
   const A* ut4;   // u^{n+1} and t^{n+1} = m(g^{n+1}) per cell, (ux, uy, uz, t) (t = 0 without LB_TEMPERATURE)
@@ -992,33 +994,34 @@ __global__ void deposit_prepare_kernel(const PartParams<A> P) {
   // gravity_vector of src/lagrange_feedback.c:95-103 (y points down)
   const double gx = P.gravity ? P.g[0] : 0.0, gy = P.gravity ? -P.g[1] : 0.0, gz = P.gravity ? P.g[2] : 0.0;
   double* r = P.rec;
+  const long long rs = P.rstride;
   if (P.twoway_stau) {  // (Du/Dt - g)(1 - rho_p/rho_f), src/lagrange_feedback.c:106-110
-    r[0LL * np + ip] = live ? fac * ((F(Dt_ux) - gx) * (1 - dr)) : 0.0;
-    r[1LL * np + ip] = live ? fac * ((F(Dt_uy) - gy) * (1 - dr)) : 0.0;
-    r[2LL * np + ip] = live ? fac * ((F(Dt_uz) - gz) * (1 - dr)) : 0.0;
+    r[0LL * rs + ip] = live ? fac * ((F(Dt_ux) - gx) * (1 - dr)) : 0.0;
+    r[1LL * rs + ip] = live ? fac * ((F(Dt_uy) - gy) * (1 - dr)) : 0.0;
+    r[2LL * rs + ip] = live ? fac * ((F(Dt_uz) - gz) * (1 - dr)) : 0.0;
   } else {
-    r[0LL * np + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
-    r[1LL * np + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;
-    r[2LL * np + ip] = live ? fac * (F(Dt_uz) - gz + dr * (gz - F(az))) : 0.0;
+    r[0LL * rs + ip] = live ? fac * (F(Dt_ux) - gx + dr * (gx - F(ax))) : 0.0;
+    r[1LL * rs + ip] = live ? fac * (F(Dt_uy) - gy + dr * (gy - F(ay))) : 0.0;
+    r[2LL * rs + ip] = live ? fac * (F(Dt_uz) - gz + dr * (gz - F(az))) : 0.0;
   }
   if (P.twoway_temp) {  // src/lagrange_feedback.c:181-190: sp = Dt_t + (T_p - T) kappa / (nu beta tau_drag)
     const double fac2 = P.kappa / (P.nu * F(beta_coeff) * F(tau_drag));
-    r[(long long)(P.nrec - 1) * np + ip] = live ? fac * (F(Dt_t) + (F(t_p) - F(t)) * fac2) : 0.0;
+    r[(long long)(P.nrec - 1) * rs + ip] = live ? fac * (F(Dt_t) + (F(t_p) - F(t)) * fac2) : 0.0;
   }
   if (P.tricubic) {  // cubic weights of the offsets -1 .. 2, src/lagrange_feedback.c:51-60
 #pragma unroll
     for (int n = -1; n <= 2; n++) {
-      r[(4LL + n) * np + ip] = cubic_weight(t.dxm - (double)n);
-      r[(8LL + n) * np + ip] = cubic_weight(t.dym - (double)n);
-      r[(12LL + n) * np + ip] = cubic_weight(t.dzm - (double)n);
+      r[(4LL + n) * rs + ip] = cubic_weight(t.dxm - (double)n);
+      r[(8LL + n) * rs + ip] = cubic_weight(t.dym - (double)n);
+      r[(12LL + n) * rs + ip] = cubic_weight(t.dzm - (double)n);
     }
   } else {
-    r[3LL * np + ip] = t.dxm;
-    r[4LL * np + ip] = t.dxp;
-    r[5LL * np + ip] = t.dym;
-    r[6LL * np + ip] = t.dyp;
-    r[7LL * np + ip] = t.dzm;
-    r[8LL * np + ip] = t.dzp;
+    r[3LL * rs + ip] = t.dxm;
+    r[4LL * rs + ip] = t.dxp;
+    r[5LL * rs + ip] = t.dym;
+    r[6LL * rs + ip] = t.dyp;
+    r[7LL * rs + ip] = t.dzm;
+    r[8LL * rs + ip] = t.dzp;
   }
   // particles that deposit nothing sort after every home cell (still in spatial
   // order among themselves) and are never merged
@@ -1119,13 +1122,70 @@ __global__ void particle_arrive_kernel(const PartParams<A> P, const int* __restr
   for (int f = 0; f < PF_TOTAL; f++) P.pf_alt[f * n_new + i] = b[1 + f];
 }
 
+// z-slab two-way deposit: ghost records.  A depositing particle whose home layer is the
+// slab's lowest (local home plane -1) or highest (NZ - 1) also deposits into the
+// neighbour's planes: its index, its home cell within the plane and its record go to that
+// neighbour (not across the lattice's periodic z boundary, where the single lattice drops
+// the contribution).  Received, a ghost is listed under the receiving slab's home layer 0
+// (from below) or NZ (from above) with its own index, so every cell merges the same
+// particles in the same index order as the single lattice.  Buffers as the particle
+// exchange's: 2-value header, then 2 + nrec values per ghost.
+template <typename A>
+__global__ void ghost_leave_kernel(const PartParams<A> P, double* send_down, double* send_up, int cap, int* counts) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= P.np) return;
+  const unsigned int hxy = (unsigned)(P.NX + 1) * (unsigned)(P.NY + 1);
+  const int o = P.pid[ip];
+  const unsigned int k = P.key[o];
+  if (k >= hxy * (unsigned)(P.NZ + 1)) return;  // deposits nothing
+  const unsigned int hz = k / hxy;
+  int dir = 0;
+  if (hz == 0 && P.zoff > 0) dir = 1;
+  if (hz == (unsigned)P.NZ && P.zoff + P.NZ < P.NZg) dir = 2;
+  if (dir == 0) return;
+  const int g = atomicAdd(counts + dir, 1);
+  if (g >= cap) {
+    atomicOr(P.status, 2);
+    return;
+  }
+  double* b = (dir == 1 ? send_down : send_up) + MIG_HEAD + (long long)g * (2 + P.nrec);
+  b[0] = (double)o;
+  b[1] = (double)(k - hz * hxy);
+  for (int f = 0; f < P.nrec; f++) b[2 + f] = P.rec[(long long)f * P.rstride + ip];
+}
+
+// the ghosts from below (home layer 0) and from above (home layer NZ): records into slots
+// np + g, keys and slots under their particle indices; threads [0, cap) read the buffer
+// from below, [cap, 2 cap) the one from above
+template <typename A>
+__global__ void ghost_arrive_kernel(const PartParams<A> P, const double* from_down, const double* from_up, int cap) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 2 * cap) return;
+  const int nd = min((int)from_down[0], cap), nu = min((int)from_up[0], cap);
+  const bool up = t >= cap;
+  const int g = up ? t - cap : t;
+  if (g >= (up ? nu : nd)) return;
+  const double* b = (up ? from_up : from_down) + MIG_HEAD + (long long)g * (2 + P.nrec);
+  const long long slot = (long long)P.np + (up ? nd : 0) + g;
+  const int o = (int)b[0];
+  if (slot >= P.rstride || o < 0 || o >= P.nsort) {
+    atomicOr(P.status, 2);
+    return;
+  }
+  const unsigned int hxy = (unsigned)(P.NX + 1) * (unsigned)(P.NY + 1);
+  P.key[o] = (up ? (unsigned)P.NZ : 0u) * hxy + (unsigned)b[1];
+  P.order[o] = (int)slot;
+  P.pid[slot] = o;
+  for (int f = 0; f < P.nrec; f++) P.rec[(long long)f * P.rstride + slot] = b[2 + f];
+}
+
 // [start, end) of every home cell in the sorted key array, and the records and
 // particle indices copied into sorted order (the gather then reads each home list
 // as one contiguous run)
 template <typename A>
 __global__ void cell_range_kernel(const PartParams<A> P, const unsigned int* key, const int* slot_of, unsigned int nh) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = P.np;
+  const int n = P.nsort;
   if (i >= n) return;
   const unsigned int k = key[i];
   if (k >= nh) return;
@@ -1133,7 +1193,7 @@ __global__ void cell_range_kernel(const PartParams<A> P, const unsigned int* key
   if (i == n - 1 || key[i + 1] != k) P.cell_rng[k].y = i + 1;
   const int s = slot_of[i];
   P.spid[i] = P.pid[s];
-  for (int f = 0; f < P.nrec; f++) P.srec[(long long)f * n + i] = P.rec[(long long)f * n + s];
+  for (int f = 0; f < P.nrec; f++) P.srec[(long long)f * n + i] = P.rec[(long long)f * P.rstride + s];
 }
 
 // home cell h (bit 0: +x, bit 1: +y, bit 2: +z) of lattice cell (i, j, k) in shifted
@@ -1212,7 +1272,7 @@ __device__ __forceinline__ double halo_image_t(const PartParams<A>& P, int vi, i
     }
   }
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  deposit_merge<false, true>(P.spid, P.srec, P.np, pos, endp, P.nrec - 1, acc);
+  deposit_merge<false, true>(P.spid, P.srec, P.nsort, pos, endp, P.nrec - 1, acc);
   return acc[3];
 }
 
@@ -1268,8 +1328,8 @@ __global__ void __launch_bounds__(GATHER_BLOCK) deposit_gather_kernel(const Part
     } else {
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
       if (m == 1) {
-        if (P.twoway_temp) deposit_add<true, true>(P.srec, P.np, slot, best, P.nrec - 1, acc);
-        else deposit_add<true, false>(P.srec, P.np, slot, best, 0, acc);
+        if (P.twoway_temp) deposit_add<true, true>(P.srec, P.nsort, slot, best, P.nrec - 1, acc);
+        else deposit_add<true, false>(P.srec, P.nsort, slot, best, 0, acc);
       }
       P.dep[cidx] = (A)acc[0];
       P.dep[P.N + cidx] = (A)acc[1];
@@ -1307,10 +1367,10 @@ __global__ void deposit_busy_kernel(const PartParams<A> P, int nregions) {
     }
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     if (P.twoway_temp) {
-      deposit_merge<true, true>(P.spid, P.srec, P.np, pos, endp, P.nrec - 1, acc);
+      deposit_merge<true, true>(P.spid, P.srec, P.nsort, pos, endp, P.nrec - 1, acc);
       P.dep[3 * P.N + cidx] = (A)fold_faces_t(P, i, j, k, acc[3]);
     } else {
-      deposit_merge<true, false>(P.spid, P.srec, P.np, pos, endp, 0, acc);
+      deposit_merge<true, false>(P.spid, P.srec, P.nsort, pos, endp, 0, acc);
     }
     P.dep[cidx] = (A)acc[0];
     P.dep[P.N + cidx] = (A)acc[1];
@@ -1345,7 +1405,7 @@ __device__ __forceinline__ int tricubic_homes(const PartParams<A>& P, int i, int
 // P.twoway_temp the temperature source into acc[3]
 template <bool MOM, typename A>
 __device__ __forceinline__ void tricubic_merge(const PartParams<A>& P, int* pos, const int* endp, int m, double* acc) {
-  const long long np = P.np;
+  const long long np = P.nsort;
   const double* __restrict__ r = P.srec;
   const int trec = P.nrec - 1;
   for (int left = m; left > 0; left--) {

@@ -217,12 +217,16 @@ def _owner(z, bounds):
 
 
 @pytest.mark.parametrize("name,nslabs,swim", [("particles_1w", 2, None), ("particles_swimb", 3, 0.35),
-                                               ("particles_swims", 2, 0.2), ("particles_swimt", 3, 0.25)])
+                                               ("particles_swims", 2, 0.2), ("particles_swimt", 3, 0.25),
+                                               ("particles", 2, None), ("particles_or", 3, None),
+                                               ("particles_g", 3, None), ("particles_t", 2, None)])
 def test_particles_on_slabs_reproduce_the_single_lattice(name, nslabs, swim):
     """One-way particles on z-slabs: the population faces move inside the step, then each
     slab interpolates from its u planes plus two halo planes from either neighbour and hands
     the particles that leave it to the neighbour after every sub-step (here between the
-    threads of one process).  Swimmers at a few
+    threads of one process).  With two-way coupling the deposit records of the particles
+    next to a face are also handed over, so every cell merges the same particles in the same
+    index order as the single lattice.  Swimmers at a few
     tenths of a cell per step cross the faces and the periodic z boundary many times; every
     particle field and population equals the single lattice's, bit for bit."""
     _, cfg, state = make_case(name, seed=47)
@@ -267,8 +271,8 @@ def test_particles_on_slabs_reproduce_the_single_lattice(name, nslabs, swim):
         assert moved > n // 10, "only %d of %d particles changed slab" % (moved, n)
 
 
-def test_particles_on_slabs_refuse_walls_and_two_way_coupling():
-    for name in ("particles", "particles_rb"):
+def test_particles_on_slabs_refuse_walls_and_the_folded_deposits():
+    for name in ("particles_tc", "particles_ttc", "particles_rb"):
         _, cfg, _ = make_case(name, seed=48)
         with pytest.raises(ch4b200.CH4Error):
             slab.Slab(cfg, 0, cfg.NZ // 2)
