@@ -1,7 +1,8 @@
 """z-slabs on two ranks (two processes, one torch.distributed process group over gloo),
 stepped through Slab.use_process_group: the population faces move inside ch4_step
 (host-staged gloo transfers on the slab's second stream), the NOZEROMODE force sums are
-all-gathered and the LES u faces swapped between the ranks.  Both ranks run on the one
+all-gathered, the LES u faces swapped between the ranks, and Lagrangian particles cross
+between the ranks with their u halo planes and deposit records.  Both ranks run on the one
 GPU of the box; every transfer goes through host memory, so no kernel of one rank waits
 on the other's.  The two slabs together reproduce the single lattice: bit for bit, or to
 1e-12 with the gathered force sums."""
@@ -42,24 +43,39 @@ def _rank(rank, world, port, name, q):
             s.use_process_group(rank, world)
             for k, v in pop_items(state):
                 s.set_pop(k, v)
+            if "part" in state:
+                s.set_particles(state["part"])
             s.sim.initialize()
             s.step(NSTEPS, rank, world)
-            q.put((rank, {k: s.sim.get_pop(k) for k, _ in pop_items(state)}))
+            out = {k: s.sim.get_pop(k) for k, _ in pop_items(state)}
+            if "part" in state:
+                n = len(state["part"])
+                arr = (ch4b200.Particle * n)()
+                for p in arr:
+                    p.x = float("nan")  # entries this rank does not hold stay NaN
+                s.get_particles_into(arr)
+                out["part"] = np.ctypeslib.as_array(arr).view(np.float64).reshape(n, -1).copy()
+            q.put((rank, out))
         finally:
             s.close()
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("name", ["rb", "les", "nozero"])
+@pytest.mark.parametrize("name", ["rb", "les", "nozero", "particles"])
 def test_two_ranks_reproduce_the_single_lattice(name):
     _, cfg, state = make_case(name, seed=49)
     with ch4b200.Simulation(cfg) as sim:
         for k, v in pop_items(state):
             sim.set_pop(k, v)
+        if "part" in state:
+            sim.set_particles(state["part"])
         sim.initialize()
         sim.step(NSTEPS)
         want = {k: sim.get_pop(k) for k, _ in pop_items(state)}
+        if "part" in state:
+            n = len(state["part"])
+            want["part"] = np.ctypeslib.as_array(sim.get_particles(n)).view(np.float64).reshape(n, -1).copy()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = 31000 + random.randint(0, 2000)
@@ -70,6 +86,12 @@ def test_two_ranks_reproduce_the_single_lattice(name):
     for p in procs:
         p.join(120)
         assert p.exitcode == 0
+    if "part" in want:
+        ix = [f for f, _ in ch4b200.Particle._fields_].index("x")
+        held = [~np.isnan(got[r]["part"][:, ix]) for r in (0, 1)]
+        assert np.all(held[0] ^ held[1]), "every particle on exactly one rank"
+        merged = np.where(held[0][:, None], got[0]["part"], got[1]["part"])
+        assert np.array_equal(merged, want.pop("part"))
     for k, a in want.items():
         b = np.concatenate([got[0][k], got[1][k]])
         if name == "nozero":
