@@ -122,6 +122,8 @@ FLAGS2 = {
     "LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE": 1 << 33,
     "LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION": 1 << 34,
     "LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION": 1 << 35,
+    "LAGRANGE_ORIENTATION_DIFFUSION": 1 << 36,
+    "LAGRANGE_ORIENTATION_RANDOM": 1 << 37,
 }
 
 
@@ -167,6 +169,7 @@ PARTICLE_FIELDS = [
     "px", "py", "pz", "dt_px", "dt_py", "dt_pz", "aspect_ratio",
     "t_p", "cp_p",
     "nx", "ny", "nz", "dt_nx", "dt_ny", "dt_nz", "gyrotaxis_velocity", "swim_velocity",
+    "rotational_diffusion",
 ]
 
 

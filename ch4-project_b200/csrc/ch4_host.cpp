@@ -155,7 +155,8 @@ const uint64_t SUPPORTED2 =
     CH4_F2_FLUID_LES_SMAGORINSKY_LILLY | CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION |
     CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE |
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE |
-    CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION;
+    CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION |
+    CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -661,6 +662,13 @@ struct Engine : EngineBase {
   // from up, from down) of MIG_HEAD + mig_cap * MIG_REC values each
   int np_all = 0;
   bool pslab() const { return c.nz_global > 0 && lagr(); }
+  // orientation noise: the draws of one sub-step for every particle (pinned, then on the device)
+  int noise() const {
+    return ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION) ? 1 : 0) |
+           ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_RANDOM) ? 2 : 0);
+  }
+  double* rnd_h = nullptr;
+  double* rnd_d = nullptr;
   double* mig = nullptr;
   int mig_cap = 0;
   int* keep = nullptr;
@@ -746,6 +754,9 @@ struct Engine : EngineBase {
   }
 
   void free_particles() {
+    cudaFreeHost(rnd_h);
+    cudaFree(rnd_d);
+    rnd_h = rnd_d = nullptr;
     cudaFree(mig);
     cudaFree(keep);
     cudaFree(mig_cnt);
@@ -798,6 +809,8 @@ struct Engine : EngineBase {
     Q.NZg = pslab() ? c.nz_global : c.NZ;
     Q.nsort = pslab() ? np_all : np;
     Q.rstride = pslab() ? np_all : np;
+    Q.noise = noise();
+    Q.rnd = rnd_d;
     Q.SX = c.SX;
     Q.SY = c.SY;
     Q.SZ = c.SZ;
@@ -984,6 +997,9 @@ struct Engine : EngineBase {
                                    cudaMalloc(&srec, sizeof(double) * nrec() * (size_t)n) == cudaSuccess &&
                                    cudaMalloc(&spid, sizeof(int) * (size_t)n) == cudaSuccess));
           if (!ok) return H->fail(CH4_ERR_NOMEM, "sort buffers");
+          if (noise() && (cudaMallocHost(&rnd_h, 6 * sizeof(double) * (size_t)n) != cudaSuccess ||
+                          cudaMalloc(&rnd_d, 6 * sizeof(double) * (size_t)n) != cudaSuccess))
+            return H->fail(CH4_ERR_NOMEM, "orientation noise buffers");
           if (sl) {
             // crossings of one face in one sub-step: at most the particles within a cell
             // of it (|v| dt < 1), about n / NZ, with a wide margin
@@ -1092,6 +1108,33 @@ struct Engine : EngineBase {
     std::swap(pid, pid_alt);
     np = (int)n_new;
     return CH4_OK;
+  }
+
+  // the orientation noise of one sub-step: for every particle in the caller's order (the
+  // reference's array order), three random_gauss draws (DIFFUSION), then the two draws of
+  // random_vector (RANDOM, src/random.c:139-150, host libm as the reference), from the
+  // handle's drand48 stream, which the HIT phase walk of this step has already advanced
+  ch4_status draw_noise() {
+    ch4_status st;
+    if ((st = H->cuda(cudaStreamSynchronize(H->stream), "noise buffer"))) return st;  // the last draws are used
+    const int nz = noise();
+    for (int i = 0; i < np; i++) {
+      double* r = rnd_h + 6 * (size_t)i;
+      if (nz & 1) {
+        r[0] = H->random_gauss(0.0, 1.0);
+        r[1] = H->random_gauss(0.0, 1.0);
+        r[2] = H->random_gauss(0.0, 1.0);
+      }
+      if (nz & 2) {
+        const double theta = std::acos(2.0 * H->myrand() - 1.0);
+        const double phi = 2 * 3.14159265359 * H->myrand();
+        r[3] = std::sin(theta) * std::sin(phi);
+        r[4] = std::sin(theta) * std::cos(phi);
+        r[5] = std::cos(theta);
+      }
+    }
+    return H->cuda(cudaMemcpyAsync(rnd_d, rnd_h, 6 * sizeof(double) * (size_t)np, cudaMemcpyHostToDevice, H->stream),
+                   "noise up");
   }
 
   // slot order <- order2 (sorted by home cell); with sort, compute and sort the keys here
@@ -1626,7 +1669,8 @@ struct Engine : EngineBase {
     const size_t slot = (size_t)NK * L();
     int done = 0;
     while (done < n) {
-      const int m = std::min(CHUNK, n - done);
+      // (orientation noise draws from the stream between two phase walks: one step at a time)
+      const int m = noise() ? 1 : std::min(CHUNK, n - done);
       if (hit) {
         // tables for phi_n (slot 0 = latest) and the m next phase sets
         if ((st = H->cuda(cudaEventSynchronize(hit_ev), "hit event"))) return st;
@@ -1714,6 +1758,7 @@ struct Engine : EngineBase {
             return st;
           if (pslab() && (st = u_halo())) return st;
           for (int sub = 0; sub < (int)c.time_dt_lagr_factor; sub++) {
+            if (noise() && np > 0 && (st = draw_noise())) return st;
             PartParams<A> Q = part_params();
             Q.first = (n_step == 1 && c.resume == 0);
             if ((st = H->cuda(launch_particle_substep(Q, H->stream), "particle substep"))) return st;
@@ -1888,7 +1933,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
     bool needed;
   };
   double NX, NY, NZ, particle_number = 0, resume = 0, tau_drag_types = 1, beta_coeff_types = 1, cp_coeff_types = 1;
-  double aspect_ratio_types = 1, gyrotaxis_velocity_types = 1, swim_velocity_types = 1;
+  double aspect_ratio_types = 1, gyrotaxis_velocity_types = 1, swim_velocity_types = 1, rotational_diffusion_types = 1;
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
@@ -1924,6 +1969,8 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
       {"gyrotaxis_velocity_types", &gyrotaxis_velocity_types,
        (fl & CH4_F_LAGRANGE) && orient && (fl & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) &&
            (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS)},
+      {"rotational_diffusion_types", &rotational_diffusion_types,
+       (fl & CH4_F_LAGRANGE) && orient && (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION)},
       {"swim_velocity_types", &swim_velocity_types,
        (fl & CH4_F_LAGRANGE) && orient && (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)},
       {"noise_u", &cfg->noise_u, (fl & CH4_F_FLUID_INITIAL_ADD_NOISE) != 0},  // src/parameters.c:216-220
@@ -1945,7 +1992,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   cfg->particle_number = (int)particle_number;
   cfg->resume = (int)resume;
   cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types * (int)cp_coeff_types * (int)aspect_ratio_types *
-                        (int)gyrotaxis_velocity_types * (int)swim_velocity_types;
+                        (int)gyrotaxis_velocity_types * (int)rotational_diffusion_types * (int)swim_velocity_types;
   // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
   cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
   cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;
@@ -2082,6 +2129,8 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE},
       {"LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION},
       {"LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION},
+      {"LAGRANGE_ORIENTATION_DIFFUSION", CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION},
+      {"LAGRANGE_ORIENTATION_RANDOM", CH4_F2_LAGRANGE_ORIENTATION_RANDOM},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2275,6 +2324,16 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
         return why = "swimming along n needs LAGRANGE_ORIENTATION_SECONDORIENTATION", CH4_ERR_UNSUPPORTED;
       if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
         return why = "LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
+      const uint64_t noise = CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM;
+      if ((f2 & noise) && !(c->flags & CH4_F_LAGRANGE_ORIENTATION))
+        return why = "LAGRANGE_ORIENTATION_DIFFUSION and _RANDOM need LAGRANGE_ORIENTATION", CH4_ERR_UNSUPPORTED;
+      if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION) && !(c->flags & CH4_F_LAGRANGE_GRADIENT))
+        return why = "LAGRANGE_ORIENTATION_DIFFUSION needs LAGRANGE_GRADIENT (rotational_diffusion is read under it)",
+               CH4_ERR_UNSUPPORTED;
+      // the draws come from one drand48 stream in the order of the whole particle array
+      if ((f2 & noise) && c->nz_global > 0)
+        return why = "orientation noise runs on whole lattices (one random stream over all particles)",
+               CH4_ERR_UNSUPPORTED;
     }
     if (!(c->time_dt_lagr_factor >= 1.0)) return why = "time_dt_lagr_factor must be >= 1", CH4_ERR_ARG;
   }
@@ -2937,9 +2996,10 @@ namespace {
 using PField = std::pair<const char*, double ch4_particle::*>;
 
 // after p and dp/dt: n and dn/dt (SECONDORIENTATION), aspect_ratio (JEFFREY),
-// gyrotaxis_velocity (GYROTAXIS), swim_velocity (ACTIVE) -- the order of output_particles
+// gyrotaxis_velocity (GYROTAXIS), rotational_diffusion (DIFFUSION: a member of part.h5 only,
+// with `compound`), swim_velocity (ACTIVE) -- the order of output_particles
 // (src/lagrange.c:1925-1992) and of write_point_particle_h5 (src/lagrange.c:4378-4407)
-void orientation_extras(std::vector<PField>& v, uint64_t fl, uint64_t fl2) {
+void orientation_extras(std::vector<PField>& v, uint64_t fl, uint64_t fl2, bool compound = false) {
   using P = ch4_particle;
   if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION)
     v.insert(v.end(), {{"nx", &P::nx}, {"ny", &P::ny}, {"nz", &P::nz}, {"dt_nx", &P::dt_nx}, {"dt_ny", &P::dt_ny},
@@ -2948,6 +3008,8 @@ void orientation_extras(std::vector<PField>& v, uint64_t fl, uint64_t fl2) {
     v.push_back({"aspect_ratio", &P::aspect_ratio});
     if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) v.push_back({"gyrotaxis_velocity", &P::gyrotaxis_velocity});
   }
+  if (compound && (fl2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION))
+    v.push_back({"rotational_diffusion", &P::rotational_diffusion});
   if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) v.push_back({"swim_velocity", &P::swim_velocity});
 }
 
@@ -3005,7 +3067,7 @@ std::vector<PField> part_members(uint64_t fl, uint64_t fl2) {
       if (fl & CH4_F_LAGRANGE_ORIENTATION) {
         v.insert(v.end(), {{"px", &P::px}, {"py", &P::py}, {"pz", &P::pz}, {"dt_px", &P::dt_px},
                            {"dt_py", &P::dt_py}, {"dt_pz", &P::dt_pz}});
-        orientation_extras(v, fl, fl2);
+        orientation_extras(v, fl, fl2, true);
       }
     }
   }

@@ -106,6 +106,11 @@ struct PartParams {
   // orientation variants: the second orientation, gyrotaxis, the swimming mode of active
   // tracers (0 none, 1 along p, 2 ballistic, 3 while dT/dt > 0, 4 along n, 5 rods p, discs n)
   int second, gyro, swim;
+  // orientation noise (bit 0 rotational diffusion, bit 1 a random p every sub-step): per
+  // particle index, the three gaussian draws xi and the random unit vector, drawn by the
+  // host from the handle's drand48 stream in particle order for this sub-step
+  int noise;
+  const double* rnd;  // [6][index]: xi[3], then the random p[3] (6 values per particle)
 };
 
 // periodic wrap of a coordinate into [0, S) (the reference's wrap, src/lagrange.c)
@@ -576,11 +581,12 @@ __device__ __forceinline__ void particle_walls(const PartParams<A>& P, double ta
 // particle gravity the vector is (0, 0, 1)).  Sums in the reference's order.
 struct OrientOpts {
   bool jeffery, second, gyro, gravity;
+  int noise;
   double g[3];
 };
 
 static __device__ __noinline__ void orient_particle(double* pf, long long np, int ip, const double* gr,
-                                                    const OrientOpts o, bool first, double dtl) {
+                                                    const OrientOpts o, bool first, double dtl, const double* rnd) {
 #define F(name) pf[CH4_PF(name) * np + ip]
   double p[3] = {F(px), F(py), F(pz)}, fo[3] = {F(dt_px), F(dt_py), F(dt_pz)};
   double n[3] = {0.0, 0.0, 0.0}, fno[3] = {0.0, 0.0, 0.0};
@@ -662,6 +668,24 @@ static __device__ __noinline__ void orient_particle(double* pf, long long np, in
         fno[i] = fn[i];
       }
     }
+  }
+  if (o.noise & 1) {  // rotational diffusion, src/lagrange.c:3680-3696: p += sqrt(2 D_r dt) (I - p p) xi
+    double tmp[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) tmp[i] += ((i == j ? 1.0 : 0.0) - p[i] * p[j]) * rnd[j];
+    const double two_d_r = 2.0 * F(rotational_diffusion);
+#pragma unroll
+    for (int i = 0; i < 3; i++) p[i] += sqrt(two_d_r * dtl) * tmp[i];
+  }
+  if (o.noise & 2) {  // a random unit p, src/lagrange.c:3698-3713 (the host drew it)
+    p[0] = rnd[3];
+    p[1] = rnd[4];
+    p[2] = rnd[5];
+    fo[0] = (p[0] - F(px)) / dtl;
+    fo[1] = (p[1] - F(py)) / dtl;
+    fo[2] = (p[2] - F(pz)) / dtl;
   }
   double norm = 0.0;
 #pragma unroll
@@ -949,8 +973,8 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
     }
   }
   if constexpr (ORIENT) {
-    const OrientOpts o{P.jeffery != 0, P.second != 0, P.gyro != 0, P.gravity != 0, {P.g[0], P.g[1], P.g[2]}};
-    orient_particle(pf, np, ip, &gr[0][0], o, first, dtl);
+    const OrientOpts o{P.jeffery != 0, P.second != 0, P.gyro != 0, P.gravity != 0, P.noise, {P.g[0], P.g[1], P.g[2]}};
+    orient_particle(pf, np, ip, &gr[0][0], o, first, dtl, P.noise ? P.rnd + 6LL * P.pid[ip] : nullptr);
   }
   double tp = P.lagr_temp ? F(t_p) : 0.0;
   if constexpr (HALO) particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp);

@@ -176,7 +176,13 @@ enum {
   CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC = 1ull << 32,
   CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE = 1ull << 33,
   CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION = 1ull << 34,
-  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION = 1ull << 35
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION = 1ull << 35,
+  /* orientation noise, src/lagrange.c:3680-3713, drawn from the handle's drand48 stream in
+   * particle order every sub-step (after the step's HIT phase walk): rotational diffusion
+   * p += sqrt(2 D_r dt) (I - p p) xi with xi three random_gauss draws, or a new random unit
+   * p every sub-step (RANDOM, dp/dt the difference quotient) */
+  CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION = 1ull << 36,
+  CH4_F2_LAGRANGE_ORIENTATION_RANDOM = 1ull << 37
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
@@ -262,6 +268,8 @@ typedef struct {
    * the swimming velocity (src/typedef.h:419-437) */
   double nx, ny, nz, dt_nx, dt_ny, dt_nz;
   double gyrotaxis_velocity, swim_velocity;
+  /* LAGRANGE_ORIENTATION_DIFFUSION: the rotational diffusivity D_r */
+  double rotational_diffusion;
 } ch4_particle;
 
 /* Global averages of dump_averages (src/output.c:63-~760), FP64 sums over the

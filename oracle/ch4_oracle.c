@@ -662,7 +662,7 @@ static void interp_particle_t(const ch4o_state *s, const double *tf, ch4_particl
  * tau_drag == 0, Eulerian probes tau_drag < 0, Stokes drag + added mass) */
 /* orientation (src/lagrange.c:3470-3752): Jeffery's equation with the reference's
  * loops and sum order, Euler on the first step and AB2 after, then p renormalised */
-static void orient_particle(const ch4o_state *s, ch4_particle *p, int jeffery, int first, double dtl) {
+static void orient_particle(ch4o_state *s, ch4_particle *p, int jeffery, int first, double dtl) {
   const uint64_t f2 = s->cfg.flags2;
   const int second = (f2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION) != 0;
   double P[3] = {p->px, p->py, p->pz}, Fold[3] = {p->dt_px, p->dt_py, p->dt_pz};
@@ -733,6 +733,28 @@ static void orient_particle(const ch4o_state *s, ch4_particle *p, int jeffery, i
           N[i] = N[i] + 0.5 * dtl * (3. * FN[i] - FNold[i]);
         FNold[i] = FN[i];
       }
+  }
+  if (f2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION) {
+    /* rotational diffusion, src/lagrange.c:3680-3696: p += sqrt(2 D_r dt) (I - p p) xi */
+    double xi[3], tmp[3] = {0, 0, 0};
+    xi[0] = random_gauss(s, 0.0, 1.0);
+    xi[1] = random_gauss(s, 0.0, 1.0);
+    xi[2] = random_gauss(s, 0.0, 1.0);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) tmp[i] += ((i == j ? 1.0 : 0.0) - P[i] * P[j]) * xi[j];
+    const double two_d_r = 2.0 * p->rotational_diffusion;
+    for (int i = 0; i < 3; i++) P[i] += sqrt(two_d_r * dtl) * tmp[i];
+  }
+  if (f2 & CH4_F2_LAGRANGE_ORIENTATION_RANDOM) {
+    /* a random unit p, src/lagrange.c:3698-3713 with random_vector (src/random.c:139-150) */
+    const double theta = acos(2.0 * myrand(s) - 1.0);
+    const double phi = 2 * 3.14159265359 * myrand(s);
+    P[0] = sin(theta) * sin(phi);
+    P[1] = sin(theta) * cos(phi);
+    P[2] = cos(theta);
+    Fold[0] = (P[0] - p->px) / dtl;
+    Fold[1] = (P[1] - p->py) / dtl;
+    Fold[2] = (P[2] - p->pz) / dtl;
   }
   double norm = 0.0;
   for (int i = 0; i < 3; i++) norm += P[i] * P[i];

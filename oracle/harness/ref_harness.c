@@ -130,6 +130,9 @@ static void write_part_layout(void) {
   F(gyrotaxis_velocity);
 #endif
 #endif
+#ifdef LAGRANGE_ORIENTATION_DIFFUSION
+  F(rotational_diffusion);
+#endif
 #ifdef LAGRANGE_ORIENTATION_ACTIVE
   F(swim_velocity);
 #endif

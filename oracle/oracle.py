@@ -160,6 +160,14 @@ FLAGSETS.update({
                         "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION",
                         "LAGRANGE_ORIENTATION_JEFFREY", "LAGRANGE_ORIENTATION_SECONDORIENTATION",
                         "LAGRANGE_ORIENTATION_ACTIVE", "LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION"],
+    # orientation noise from the drand48 stream (rotational diffusion; a random p every sub-step)
+    "particles_rdiff": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                        "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY", "LAGRANGE_ORIENTATION_DIFFUSION",
+                        "LAGRANGE_ORIENTATION_ACTIVE"],
+    "particles_rand": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV", "LAGRANGE", "LAGRANGE_WRAP",
+                       "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION",
+                       "LAGRANGE_ORIENTATION_RANDOM", "LAGRANGE_ORIENTATION_ACTIVE"],
     # Smagorinsky-Lilly in a stably stratified channel
     "les_lilly": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
                   "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SMAGORINSKY_LILLY"],
@@ -231,6 +239,7 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
         keys += ["aspect_ratio_types", "aspect_ratio_min", "aspect_ratio_max"]
         vals.update({"aspect_ratio_types": 1, "aspect_ratio_min": 1.0, "aspect_ratio_max": 1.0})
     for flag, key in (("LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS", "gyrotaxis_velocity"),  # src/parameters.c:638-649
+                      ("LAGRANGE_ORIENTATION_DIFFUSION", "rotational_diffusion"),  # src/parameters.c:668-681
                       ("LAGRANGE_ORIENTATION_ACTIVE", "swim_velocity")):  # src/parameters.c:684-696
         if int(cfg.flags2) & abi.FLAGS2[flag]:
             keys += [key + "_types", key + "_min", key + "_max"]

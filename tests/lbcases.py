@@ -125,6 +125,12 @@ CASES = {
     "particles_swimn": dict(flagset="particles_swimn", NX=10, NY=8, NZ=7, npart=300,
                             params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=25,
                                         time_dt_lagr_factor=2.0, particle_number=300)),
+    # orientation noise drawn from the drand48 stream, with HIT phase walks in between
+    "particles_rdiff": dict(flagset="particles_rdiff", NX=10, NY=8, NZ=7, npart=300,
+                            params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=26,
+                                        time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_rand": dict(flagset="particles_rand", NX=9, NY=10, NZ=6, npart=200,
+                           params=dict(tau_u=0.6, Amp_x=3e-3, seed=27, time_dt_lagr_factor=3.0, particle_number=200)),
     # Smagorinsky-Lilly: T rising with y (stable), so the buoyancy damps |S| where Ri < 1
     "les_lilly": dict(flagset="les_lilly", NX=8, NY=9, NZ=6,
                       params=dict(tau_u=0.52, tau_t=0.55, Amp_x=0.02, T_bot=0.0, T_top=1.0, T_ref=0.5, beta_t=0.3,
@@ -222,6 +228,9 @@ def make_case(name, seed=0, storage=0, dims=None, **over):
         if "LAGRANGE_ORIENTATION_ACTIVE" in flags:
             for i, p in enumerate(state["part"]):
                 p.swim_velocity = [0.01, 0.0, 0.03, 0.002][(i // 4) % 4]
+        if "LAGRANGE_ORIENTATION_DIFFUSION" in flags:  # 0 for some: their p is still normalised
+            for i, p in enumerate(state["part"]):
+                p.rotational_diffusion = [0.0, 0.01, 0.1, 0.002][(i // 2) % 4]
     return c["flagset"], cfg, state
 
 

@@ -54,7 +54,8 @@ def rel_l2(a, b):
                                           ("particles_ttc", 12), ("particles_rb", 12), ("particles_duct", 12),
                                           ("particles_slip", 12), ("particles_reinj", 12), ("particles_bc", 12),
                                           ("particles_or2", 12), ("particles_swimt", 12), ("particles_swimb", 12),
-                                          ("particles_swims", 12), ("particles_swimn", 12)])
+                                          ("particles_swims", 12), ("particles_swimn", 12), ("particles_rdiff", 12),
+                                          ("particles_rand", 12)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):
     _, cfg, state = make_case(name, seed=11)
     ref = run_restatement(cfg, state, nsteps)
@@ -81,7 +82,8 @@ def test_fp64_bit_identical_to_oracle(name, nsteps):
                                   "particles_tc", "duct", "duct_les", "box", "slipx", "slipz", "particles_tt",
                                   "particles_ttc", "particles_rb", "particles_duct", "particles_slip",
                                   "particles_reinj", "particles_bc", "particles_or2", "particles_swimt",
-                                  "particles_swimb", "particles_swims", "particles_swimn"])
+                                  "particles_swimb", "particles_swims", "particles_swimn", "particles_rdiff",
+                                  "particles_rand"])
 def test_fp64_matches_compiled_reference(name):
     flagset, cfg, state = make_case(name, seed=5)
     if not O.ref_available(flagset):
