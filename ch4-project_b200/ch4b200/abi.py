@@ -124,6 +124,8 @@ FLAGS2 = {
     "LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION": 1 << 35,
     "LAGRANGE_ORIENTATION_DIFFUSION": 1 << 36,
     "LAGRANGE_ORIENTATION_RANDOM": 1 << 37,
+    "LB_FLUID_LES_SISM": 1 << 38,
+    "LB_FLUID_LES_SISM_KALMAN": 1 << 39,
 }
 
 

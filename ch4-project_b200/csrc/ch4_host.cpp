@@ -156,7 +156,8 @@ const uint64_t SUPPORTED2 =
     CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE |
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE |
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION |
-    CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM;
+    CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM | CH4_F2_FLUID_LES_SISM |
+    CH4_F2_FLUID_LES_SISM_KALMAN;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -502,6 +503,8 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   if (fl & CH4_F_FLUID_LES_WALE) F |= K_WALE;
   if (fl & CH4_F_FLUID_LES_LOCAL_STRAIN) F |= K_LSTRAIN;
   if (c.flags2 & CH4_F2_FLUID_LES_SMAGORINSKY_LILLY) F |= K_LILLY;
+  if (c.flags2 & CH4_F2_FLUID_LES_SISM) F |= K_SISM;
+  if (c.flags2 & CH4_F2_FLUID_LES_SISM_KALMAN) F |= K_KALMAN;
   P.feat = F;
   uint32_t WB = 0;
   const uint64_t f2 = c.flags2;
@@ -544,6 +547,18 @@ void build_params(StepParams<A>& P, const ch4_config& c, const Lattice& lat, con
   P.nu = (A)c.nu;
   P.csmag2 = (A)std::pow(c.C_smag * 1.0, 2.0);
   P.lilly_bg = (A)(c.beta_t * c.gravity_y);
+  {  // LB_FLUID_LES_SISM constants, src/les.c:50-74 (c_exp as finally set: dt / 100)
+    const double f_v = 0.0033626, L = (double)c.SY / 2.0;
+    const double c_exp = c.time_dt / 100;
+    const double var_mean = 3.628 * (f_v / L) * c.time_dt * f_v;
+    P.sism_1mc = (A)(1.0 - c_exp);
+    P.sism_c = (A)c_exp;
+    P.sism_var2 = (A)(var_mean * var_mean);
+    P.sism_fv = (A)f_v;
+    P.sism_floor = (A)(0.1 * f_v * f_v);
+    P.um_old = nullptr;
+    P.um_new = P.kal_p = P.kal_v = nullptr;
+  }
   P.kappa = (A)c.kappa;
   P.chi = (A)c.chi;
   P.tau_u = (A)c.tau_u;
@@ -625,6 +640,10 @@ struct Engine : EngineBase {
   A *tprev = nullptr, *sprev = nullptr;
   A *kol = nullptr;
   A *ules = nullptr, *tau_les = nullptr;  // LES: u^n as (u_x, u_y, u_z, t^n) per cell
+  // LB_FLUID_LES_SISM: the running mean of u (two 4-vector arrays: this step's and the last
+  // one's) and the Kalman P and variance (3 planes each)
+  A *um_a = nullptr, *um_b = nullptr, *kal_p = nullptr, *kal_v = nullptr;
+  bool sism() const { return (c.flags2 & CH4_F2_FLUID_LES_SISM) != 0; }
   A* uhalo = nullptr;  // z-slab LES: u faces sent down | up, received from up | down
   // z-slab with the face exchange inside the step: the four face buffers (sent down | up,
   // received from up | down), the stream the transfer runs on and its two events
@@ -721,6 +740,10 @@ struct Engine : EngineBase {
     cudaFree(sprev);
     cudaFree(kol);
     cudaFree(ules);
+    cudaFree(um_a);
+    cudaFree(um_b);
+    cudaFree(kal_p);
+    cudaFree(kal_v);
     cudaFree(tau_les);
     cudaFree(uhalo);
     cudaFree(faces);
@@ -1314,6 +1337,11 @@ struct Engine : EngineBase {
     }
     if (c.flags & CH4_F_FLUID_LES) {
       if (cudaMalloc(&ules, 4 * N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "ules");
+      if (sism() && (cudaMalloc(&um_a, 4 * N * sizeof(A)) != cudaSuccess ||
+                     cudaMalloc(&um_b, 4 * N * sizeof(A)) != cudaSuccess ||
+                     cudaMalloc(&kal_p, 3 * N * sizeof(A)) != cudaSuccess ||
+                     cudaMalloc(&kal_v, 3 * N * sizeof(A)) != cudaSuccess))
+        return H->fail(CH4_ERR_NOMEM, "LES running mean");
       if (cudaMalloc(&tau_les, N * sizeof(A)) != cudaSuccess) return H->fail(CH4_ERR_NOMEM, "tau_les");
       if (c.flags & CH4_F_FLUID_LES_VANDRIEST) {
         // C_smag(y) of src/les.c:136-142: the test is on the row index with the LES halo
@@ -1741,6 +1769,14 @@ struct Engine : EngineBase {
         }
         if (c.flags & CH4_F_FLUID_LES)
           if ((st = les_u())) return st;
+        if (sism()) {  // this step's running mean of u, from the last one and u^n
+          P.um_old = um_a;
+          P.um_new = um_b;
+          P.kal_p = kal_p;
+          P.kal_v = kal_v;
+          if ((st = H->cuda(launch_sism(P, H->stream), "les mean"))) return st;
+          std::swap(um_a, um_b);  // the step reads um_new = this step's (um_a from now on)
+        }
         if (H->face_exchange) {
           if ((st = step_overlapped())) return st;
         } else if ((st = H->cuda(launch_step(P, shape, H->stream), "lb_step"))) {
@@ -2131,6 +2167,8 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION},
       {"LAGRANGE_ORIENTATION_DIFFUSION", CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION},
       {"LAGRANGE_ORIENTATION_RANDOM", CH4_F2_LAGRANGE_ORIENTATION_RANDOM},
+      {"LB_FLUID_LES_SISM", CH4_F2_FLUID_LES_SISM},
+      {"LB_FLUID_LES_SISM_KALMAN", CH4_F2_FLUID_LES_SISM_KALMAN},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2255,6 +2293,17 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
         (!(c->flags & CH4_F_FLUID_LES) || !(c->flags & CH4_F_LB_TEMPERATURE) || (c->flags & CH4_F_TEMPERATURE_FORCING)))
       return why = "LB_FLUID_LES_SMAGORINSKY_LILLY needs LB_FLUID_LES and LB_TEMPERATURE, without LB_TEMPERATURE_FORCING",
              CH4_ERR_UNSUPPORTED;
+    // shear-improved Smagorinsky: the reference's temperature / scalar LES times call the
+    // fluid's again (src/les.c:282-326), updating the running mean twice per step; the mean
+    // of a z-slab would need the neighbours' updated means in the reference's loop order
+    if ((c->flags2 & CH4_F2_FLUID_LES_SISM) && !(c->flags & CH4_F_FLUID_LES))
+      return why = "LB_FLUID_LES_SISM needs LB_FLUID_LES", CH4_ERR_UNSUPPORTED;
+    if ((c->flags2 & CH4_F2_FLUID_LES_SISM_KALMAN) && !(c->flags2 & CH4_F2_FLUID_LES_SISM))
+      return why = "LB_FLUID_LES_SISM_KALMAN needs LB_FLUID_LES_SISM", CH4_ERR_UNSUPPORTED;
+    if ((c->flags2 & CH4_F2_FLUID_LES_SISM) && (c->flags & (CH4_F_TEMPERATURE_LES | CH4_F_SCALAR_LES)))
+      return why = "LB_FLUID_LES_SISM runs without LB_TEMPERATURE_LES / LB_SCALAR_LES", CH4_ERR_UNSUPPORTED;
+    if ((c->flags2 & CH4_F2_FLUID_LES_SISM) && c->nz_global > 0)
+      return why = "LB_FLUID_LES_SISM runs on whole lattices", CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_TEMPERATURE_LES) && !(c->flags & CH4_F_LB_TEMPERATURE))
       return why = "LB_TEMPERATURE_LES needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
     if ((c->flags & CH4_F_SCALAR_LES) && !(c->flags & CH4_F_LB_SCALAR))

@@ -71,7 +71,9 @@ enum : uint32_t {
   K_SLES = 1u << 24,       // LB_SCALAR_LES: scalar relaxation time from the LES one
   K_WALE = 1u << 25,       // LB_FLUID_LES_WALE: WALE eddy viscosity
   K_LSTRAIN = 1u << 26,    // LB_FLUID_LES_LOCAL_STRAIN: |S| from the populations' stress tensor
-  K_LILLY = 1u << 27       // LB_FLUID_LES_SMAGORINSKY_LILLY: |S| damped by the stratification
+  K_LILLY = 1u << 27,      // LB_FLUID_LES_SMAGORINSKY_LILLY: |S| damped by the stratification
+  K_SISM = 1u << 28,       // LB_FLUID_LES_SISM: |S| less |S| of the running mean of u
+  K_KALMAN = 1u << 29      // LB_FLUID_LES_SISM_KALMAN: that mean from a Kalman filter
 };
 
 // walls on x and z (those on y are K_FWALL / K_TWALL / K_SWALL of `feat`)
@@ -119,6 +121,15 @@ struct StepParams {
   const A* ules_lo;  // z-slab: the vectors of the plane under the slab (NX*NY), else null
   const A* ules_hi;  // z-slab: u of the plane over the slab
   A* tau_les;
+  // LB_FLUID_LES_SISM: the running mean of u as (x, y, z, 0) vectors per cell before this
+  // step's update (um_old) and after it (um_new, written by sism_filter_kernel, which also
+  // keeps the Kalman P and variance, 3 planes each); the rate (1 - c, c), the Kalman
+  // var_mean^2, f_v and the variance floor 0.1 f_v^2
+  const A* um_old;
+  A* um_new;
+  A* kal_p;
+  A* kal_v;
+  A sism_1mc, sism_c, sism_var2, sism_fv, sism_floor;
   // LB_FLUID_LES_SMAGORINSKY_LILLY: beta_t * gravity_y (t^n is the fourth component of ules)
   A lilly_bg;
   // two-way coupling deposit of this and the previous step (3 SoA planes each)

@@ -17,6 +17,10 @@ struct LaunchShape {
 // fused collide-force-stream step
 cudaError_t launch_step(const StepParams<double>& P, LaunchShape s, cudaStream_t st);
 cudaError_t launch_step(const StepParams<float>& P, LaunchShape s, cudaStream_t st);
+// LB_FLUID_LES_SISM: this step's running mean of u (P.um_new, and the Kalman state) from
+// the previous one and u^n (P.ules)
+cudaError_t launch_sism(const StepParams<double>& P, cudaStream_t st);
+cudaError_t launch_sism(const StepParams<float>& P, cudaStream_t st);
 // t^{n-1} := m(g), s^{n-1} := m(h)
 cudaError_t launch_init_prev(const StepParams<double>& P, LaunchShape s, cudaStream_t st);
 cudaError_t launch_init_prev(const StepParams<float>& P, LaunchShape s, cudaStream_t st);

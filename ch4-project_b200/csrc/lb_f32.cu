@@ -48,6 +48,7 @@ cudaError_t launch_particle_reorder(const PartParams<float>& P, unsigned int* ke
                                     size_t& tmp_bytes, int sort, cudaStream_t st) {
   return reorder_t<float>(P, key2, order2, tmp, tmp_bytes, sort, st);
 }
+cudaError_t launch_sism(const StepParams<float>& P, cudaStream_t st) { return sism_t<float>(P, st); }
 cudaError_t launch_particle_leave(const PartParams<float>& P, double* send_down, double* send_up, int cap, int* keep,
                                   int* counts, cudaStream_t st) {
   return leave_t<float>(P, send_down, send_up, cap, keep, counts, st);

@@ -288,6 +288,54 @@ __device__ __forceinline__ A les_tau(const StepParams<A>& P, int x, int y, int z
                             (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
                             (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
   }
+  if (F & K_SISM) {
+    // shear-improved Smagorinsky (src/les.c:46-130): |S| less |S| of the running mean of u
+    // when larger.  The reference updates the mean cell by cell inside its collision loop
+    // (z, y, x order) and differentiates it at once: a neighbour before this cell in that
+    // order holds its updated mean, one after it the previous step's; the mean has no halo
+    // copies, so beyond the lattice it is zero; walls one-sided as for u
+    auto cell = [&](int i, int j, int k) { return ((long long)k * NY + j) * NX + i; };
+    auto um = [&](int i, int j, int k, A* v) {
+      if (i < 0 || i >= NX || j < 0 || j >= NY || k < 0 || k >= NZ) {
+        v[0] = v[1] = v[2] = A(0);
+        return;
+      }
+      const long long c = cell(i, j, k);
+      ld4(c <= idx ? P.um_new : P.um_old, c, v);
+    };
+    A g[3][3], v0[4], v1[4], v2[4];
+    auto side = [&](int b, bool fwd) {
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+        g[a][b] = fwd ? A(-1.5) * v0[a] + A(2) * v1[a] + A(-0.5) * v2[a] : A(1.5) * v0[a] + A(-2) * v1[a] + A(0.5) * v2[a];
+    };
+    auto centred = [&](int b) {
+#pragma unroll
+      for (int a = 0; a < 3; a++) g[a][b] = (v0[a] - v1[a]) / A(2);
+    };
+    const bool wall[3] = {(P.walls & W_FX) != 0, (F & K_FWALL) != 0, (P.walls & W_FZ) != 0};
+    const int at[3] = {x, y, z}, n[3] = {NX, NY, NZ};
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      auto pt = [&](int o, A* v) { um(b == 0 ? o : x, b == 1 ? o : y, b == 2 ? o : z, v); };
+      if (wall[b] && at[b] == 0) {
+        pt(0, v0), pt(1, v1), pt(2, v2);
+        side(b, true);
+      } else if (wall[b] && at[b] == n[b] - 1) {
+        pt(n[b] - 1, v0), pt(n[b] - 2, v1), pt(n[b] - 3, v2);
+        side(b, false);
+      } else {
+        pt(at[b] + 1, v0), pt(at[b] - 1, v1);
+        centred(b);
+      }
+    }
+    const A mxx = g[0][0], mxy = g[0][1], mxz = g[0][2], myx = g[1][0], myy = g[1][1], myz = g[1][2];
+    const A mzx = g[2][0], mzy = g[2][1], mzz = g[2][2];
+    const A s_mean = sqrt(A(0.5) * ((mxx + mxx) * (mxx + mxx) + (mxy + myx) * (mxy + myx) + (mxz + mzx) * (mxz + mzx) +
+                                    (myx + mxy) * (myx + mxy) + (myy + myy) * (myy + myy) + (myz + mzy) * (myz + mzy) +
+                                    (mzx + mxz) * (mzx + mxz) + (mzy + myz) * (mzy + myz) + (mzz + mzz) * (mzz + mzz)));
+    if (s_norm > s_mean) s_norm = s_norm - s_mean;
+  }
   if (F & K_LILLY) {
     // Smagorinsky-Lilly (src/les.c:156-176): Ri = beta_t g_y (dT/dy)^+ / |S|^2, |S| times
     // sqrt(1 - Ri) for Ri < 1, else 0.  dT/dy of gradient_scalar: one-sided at the y
@@ -438,6 +486,41 @@ __global__ void hydro_kernel(const StepParams<A> P, const A* hit, const A* dep, 
       s[idx] = (double)mom0(h);
     }
   }
+}
+
+// LB_FLUID_LES_SISM: this step's running mean of u per cell, from the previous one (or u^n
+// on the first step of the run) and u^n (src/les.c:55-114): an exponential filter, or with
+// K_KALMAN a Kalman filter whose P and variance are kept per cell.  Per cell only; the step
+// kernel then reads the old or the new mean of each neighbour as the reference's in-place
+// update order has it.
+template <typename A>
+__global__ void sism_filter_kernel(const StepParams<A> P) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (idx >= P.N) return;
+  A u[4], m[4];
+  ld4(P.ules, idx, u);
+  if (P.les_first) {
+    m[0] = u[0], m[1] = u[1], m[2] = u[2];
+  } else {
+    ld4(P.um_old, idx, m);
+  }
+  if (!(P.feat & K_KALMAN)) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) m[a] = P.sism_1mc * m[a] + P.sism_c * u[a];
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const long long o = a * P.N + idx;
+      const A p0 = P.les_first ? P.sism_var2 : P.kal_p[o], v0 = P.les_first ? P.sism_var2 : P.kal_v[o];
+      const A pre = m[a], Ppre = p0 + P.sism_var2;
+      const A K = Ppre * (A(1) / (Ppre + v0));
+      m[a] = pre + K * (u[a] - pre);
+      P.kal_p[o] = Ppre - (K * Ppre);
+      const A vk = P.sism_fv * fabs(m[a] - u[a]);
+      P.kal_v[o] = vk > P.sism_floor ? vk : P.sism_floor;
+    }
+  }
+  store_ut4<A>(P.um_new, idx, m[0], m[1], m[2], A(0));
 }
 
 // The hydrodynamic fields of z-planes [z0, z0 + gridDim.z) in the arithmetic type, for

@@ -182,7 +182,13 @@ enum {
    * p += sqrt(2 D_r dt) (I - p p) xi with xi three random_gauss draws, or a new random unit
    * p every sub-step (RANDOM, dp/dt the difference quotient) */
   CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION = 1ull << 36,
-  CH4_F2_LAGRANGE_ORIENTATION_RANDOM = 1ull << 37
+  CH4_F2_LAGRANGE_ORIENTATION_RANDOM = 1ull << 37,
+  /* shear-improved Smagorinsky, src/les.c:46-130: |S| less |S| of a running mean of u (an
+   * exponential filter with rate dt/100, or a Kalman filter with KALMAN), the mean updated
+   * cell by cell in the reference's loop order (its gradient sees the cells before a cell
+   * already updated, and zero beyond the lattice) */
+  CH4_F2_FLUID_LES_SISM = 1ull << 38,
+  CH4_F2_FLUID_LES_SISM_KALMAN = 1ull << 39
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */

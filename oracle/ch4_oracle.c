@@ -69,6 +69,7 @@ struct ch4o_state {
   double *hit_prev, *hit_cur; /* [NK][NX+NY+NZ] */
   /* LES relaxation time field (src/les.c:266 tau_u_les_total) */
   double *tau_les;
+  double *u_mean, *kal_p, *kal_v; /* LB_FLUID_LES_SISM: running mean of u (3 per cell), Kalman P and var */
   /* particles */
   int npart;
   ch4_particle *part;
@@ -290,6 +291,67 @@ static double vandriest(const ch4o_state *s, int j) {
   return c->C_smag * (1.0 - exp((-(c->Amp_x * ((c->SY - yc))) / c->nu) / 26.0));
 }
 
+/* LB_FLUID_LES_SISM (src/les.c:46-130): the running mean of u at cell (i, j, k) is updated
+ * here, as the reference does inside tau_u_les, cell by cell in its loop order (k, j, i), so
+ * the gradient of the mean at a cell sees the cells before it already updated; the mean has
+ * no halo copies (zero beyond the lattice).  |S| less |S| of the mean, when larger. */
+static double sism(ch4o_state *s, const double *u, int i, int j, int k, double s_norm) {
+  const ch4_config *c = &s->cfg;
+  const double f_v = 0.0033626, L = c->SY / 2.0;
+  double c_exp = 3.628 * (f_v / L) * c->time_dt;
+  c_exp = c->time_dt / 100;
+  const size_t idx = cidx(s, i, j, k);
+  double *um = s->u_mean + 3 * idx;
+  const double *uu = u + 3 * idx;
+  if (s->itime == 1)
+    for (int a = 0; a < 3; a++) um[a] = uu[a];
+  if (!(c->flags2 & CH4_F2_FLUID_LES_SISM_KALMAN)) {
+    for (int a = 0; a < 3; a++) um[a] = (1.0 - c_exp) * um[a] + c_exp * uu[a];
+  } else {
+    const double var_mean = 3.628 * (f_v / L) * c->time_dt * f_v;
+    double *P = s->kal_p + 3 * idx, *V = s->kal_v + 3 * idx;
+    if (s->itime == 1)
+      for (int a = 0; a < 3; a++) P[a] = V[a] = var_mean * var_mean;
+    for (int a = 0; a < 3; a++) {
+      const double pre = um[a], Ppre = P[a] + var_mean * var_mean;
+      const double K = Ppre * (1.0 / (Ppre + V[a]));
+      um[a] = pre + K * (uu[a] - pre);
+      P[a] = Ppre - (K * Ppre);
+      const double vk = f_v * fabs(um[a] - uu[a]);
+      V[a] = vk > 0.1 * f_v * f_v ? vk : 0.1 * f_v * f_v;
+    }
+  }
+  /* gradient_vector(u_mean): centred, one-sided 2nd order at the fluid walls, zero beyond
+   * the lattice elsewhere */
+  const int walls = fluid_walls(c);
+  const int n[3] = {s->NX, s->NY, s->NZ};
+  double g[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) {
+      int at[3] = {i, j, k};
+      const int m = n[b], cc = at[b];
+#define UM(o) (at[b] = (o), (at[b] < 0 || at[b] >= m) ? 0.0 : s->u_mean[cidx(s, at[0], at[1], at[2]) * 3 + a])
+      if (((walls >> b) & 1) && cc == 0) {
+        const double v0 = UM(0), v1 = UM(1), v2 = UM(2);
+        g[a][b] = -1.5 * v0 + 2.0 * v1 + -0.5 * v2;
+      } else if (((walls >> b) & 1) && cc == m - 1) {
+        const double v0 = UM(m - 1), v1 = UM(m - 2), v2 = UM(m - 3);
+        g[a][b] = 1.5 * v0 + -2.0 * v1 + 0.5 * v2;
+      } else {
+        const double vp = UM(cc + 1), vm = UM(cc - 1);
+        g[a][b] = (vp - vm) / 2.0;
+      }
+#undef UM
+    }
+  const double xx = g[0][0], xy = g[0][1], xz = g[0][2], yx = g[1][0], yy = g[1][1], yz = g[1][2];
+  const double zx = g[2][0], zy = g[2][1], zz = g[2][2];
+  const double s_mean = sqrt(0.5 * ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) +
+                                    (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
+                                    (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
+  if (s_norm > s_mean) s_norm = s_norm - s_mean;
+  return s_norm;
+}
+
 /* LB_FLUID_LES_SMAGORINSKY_LILLY (src/les.c:156-176): |S| times
  * Cb = sqrt(1 - Ri/Pr) (0 for Ri >= 1), Ri = N^2 / pow(|S|, 2), N^2 = beta_t g_y dT/dy for a
  * stable stratification (dT/dy >= 0), else 0; dT/dy of gradient_scalar(t^n) */
@@ -312,7 +374,7 @@ static double lilly(const ch4o_state *s, const double *t, int i, int j, int k, d
   return s_norm * Cb;
 }
 
-static double les_tau(const ch4o_state *s, const double *u, const double *t, int i, int j, int k, const double *f,
+static double les_tau(ch4o_state *s, const double *u, const double *t, int i, int j, int k, const double *f,
                       double rho, double ux, double uy, double uz, double u2, double tau_prev) {
   const int NX = s->NX, NY = s->NY, NZ = s->NZ;
   const uint64_t fl = s->cfg.flags;
@@ -337,6 +399,7 @@ static double les_tau(const ch4o_state *s, const double *u, const double *t, int
     double fac = -1.0 / (2 * s->cs2 * rho * tprev * s->cfg.time_dt);
     double s_norm = fabs(fac) * sqrt(2.0 * (Sxx * Sxx + Sxy * Sxy + Sxz * Sxz + Syx * Syx + Syy * Syy + Syz * Syz +
                                             Szx * Szx + Szy * Szy + Szz * Szz));
+    if (s->cfg.flags2 & CH4_F2_FLUID_LES_SISM) s_norm = sism(s, u, i, j, k, s_norm);
     double C_smag = s->cfg.C_smag;
     if (fl & CH4_F_FLUID_LES_VANDRIEST) C_smag = vandriest(s, j);
     if (lil) s_norm = lilly(s, t, i, j, k, s_norm);
@@ -356,6 +419,7 @@ static double les_tau(const ch4o_state *s, const double *u, const double *t, int
   double s_norm = sqrt(0.5 * ((xx + xx) * (xx + xx) + (xy + yx) * (xy + yx) + (xz + zx) * (xz + zx) +
                               (yx + xy) * (yx + xy) + (yy + yy) * (yy + yy) + (yz + zy) * (yz + zy) +
                               (zx + xz) * (zx + xz) + (zy + yz) * (zy + yz) + (zz + zz) * (zz + zz)));
+  if (s->cfg.flags2 & CH4_F2_FLUID_LES_SISM) s_norm = sism(s, u, i, j, k, s_norm);
   double vol = 1.0; /* (dx*dy*dz)^(1/3) on the unit lattice */
   double C_smag = s->cfg.C_smag;
   if (fl & CH4_F_FLUID_LES_VANDRIEST) C_smag = vandriest(s, j);
@@ -1605,6 +1669,11 @@ int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
   if ((cfg->flags & CH4_F_LAGRANGE) && (cfg->flags & CH4_F_LB_TEMPERATURE))
     s->tf = (double *)calloc(s->N, sizeof(double));
   s->tau_les = (double *)calloc(s->N, sizeof(double));
+  if (cfg->flags2 & CH4_F2_FLUID_LES_SISM) {
+    s->u_mean = (double *)calloc(3 * s->N, sizeof(double));
+    s->kal_p = (double *)calloc(3 * s->N, sizeof(double));
+    s->kal_v = (double *)calloc(3 * s->N, sizeof(double));
+  }
   /* constant force tables */
   const double LX = cfg->SX, LY = cfg->SY, nu = cfg->nu;
   s->kol_x = (double *)calloc((size_t)s->NY, sizeof(double));
@@ -1655,6 +1724,9 @@ int ch4o_destroy(ch4o_state *s) {
   free(s->sprev);
   free(s->force);
   free(s->tau_les);
+  free(s->u_mean);
+  free(s->kal_p);
+  free(s->kal_v);
   free(s->kol_x);
   free(s->kol_y);
   free(s->kol_z);

@@ -168,6 +168,10 @@ FLAGSETS.update({
     "particles_rand": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV", "LAGRANGE", "LAGRANGE_WRAP",
                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION",
                        "LAGRANGE_ORIENTATION_RANDOM", "LAGRANGE_ORIENTATION_ACTIVE"],
+    # shear-improved Smagorinsky: exponential running mean (periodic), Kalman mean (channel)
+    "les_sism": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV", "LB_FLUID_LES", "LB_FLUID_LES_SISM"],
+    "les_kalman": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
+                   "LB_FLUID_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SISM", "LB_FLUID_LES_SISM_KALMAN"],
     # Smagorinsky-Lilly in a stably stratified channel
     "les_lilly": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
                   "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SMAGORINSKY_LILLY"],

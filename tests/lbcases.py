@@ -41,6 +41,10 @@ CASES = {
                                S_bot=0.2, S_top=0.7, S_ref=0.1, beta_s=0.3, gravity_y=2e-3, gravity_x=1e-3)),
     "les": dict(flagset="les", NX=8, NY=9, NZ=6,
                 params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "les_sism": dict(flagset="les_sism", NX=8, NY=9, NZ=6,
+                     params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
+    "les_kalman": dict(flagset="les_kalman", NX=8, NY=9, NZ=6,
+                       params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
     "les_vd": dict(flagset="les_vd", NX=8, NY=12, NZ=6,
                    params=dict(tau_u=0.52, Amp_x=0.02, Amp_y=0.01, Amp_z=0.005)),
     "les_ls": dict(flagset="les_ls", NX=8, NY=9, NZ=6,
