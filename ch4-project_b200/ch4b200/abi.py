@@ -126,6 +126,9 @@ FLAGS2 = {
     "LAGRANGE_ORIENTATION_RANDOM": 1 << 37,
     "LB_FLUID_LES_SISM": 1 << 38,
     "LB_FLUID_LES_SISM_KALMAN": 1 << 39,
+    "LAGRANGE_ORIENTATION_ACTIVE_JUMP": 1 << 40,
+    "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE": 1 << 41,
+    "LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS": 1 << 42,
 }
 
 
@@ -172,6 +175,7 @@ PARTICLE_FIELDS = [
     "t_p", "cp_p",
     "nx", "ny", "nz", "dt_nx", "dt_ny", "dt_nz", "gyrotaxis_velocity", "swim_velocity",
     "rotational_diffusion",
+    "shear_rate", "critical_shear_rate", "time_from_jump", "jump_time", "px_jump", "py_jump", "pz_jump",
 ]
 
 

@@ -157,7 +157,8 @@ const uint64_t SUPPORTED2 =
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE |
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION |
     CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM | CH4_F2_FLUID_LES_SISM |
-    CH4_F2_FLUID_LES_SISM_KALMAN;
+    CH4_F2_FLUID_LES_SISM_KALMAN | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP |
+    CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -833,6 +834,9 @@ struct Engine : EngineBase {
     Q.nsort = pslab() ? np_all : np;
     Q.rstride = pslab() ? np_all : np;
     Q.noise = noise();
+    Q.jump_flags = ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) ? 1 : 0) |
+                   ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS) ? 2 : 0);
+    Q.log001 = std::log(0.01);
     Q.rnd = rnd_d;
     Q.SX = c.SX;
     Q.SY = c.SY;
@@ -859,7 +863,8 @@ struct Engine : EngineBase {
     Q.gyro = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) != 0;
     Q.swim = 0;
     if (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)  // the reference's #if / #elif order
-      Q.swim = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC)            ? 2
+      Q.swim = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP)                 ? 6
+               : (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC)          ? 2
                : (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE)        ? 3
                : (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION)  ? 4
                : (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION) ? 5
@@ -1970,6 +1975,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   };
   double NX, NY, NZ, particle_number = 0, resume = 0, tau_drag_types = 1, beta_coeff_types = 1, cp_coeff_types = 1;
   double aspect_ratio_types = 1, gyrotaxis_velocity_types = 1, swim_velocity_types = 1, rotational_diffusion_types = 1;
+  double critical_shear_rate_types = 1, jump_time_types = 1;
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
@@ -2009,6 +2015,12 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
        (fl & CH4_F_LAGRANGE) && orient && (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION)},
       {"swim_velocity_types", &swim_velocity_types,
        (fl & CH4_F_LAGRANGE) && orient && (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)},
+      {"critical_shear_rate_types", &critical_shear_rate_types,
+       (fl & CH4_F_LAGRANGE) && orient && (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) &&
+           (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP)},
+      {"jump_time_types", &jump_time_types,
+       (fl & CH4_F_LAGRANGE) && orient && (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) &&
+           (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP)},
       {"noise_u", &cfg->noise_u, (fl & CH4_F_FLUID_INITIAL_ADD_NOISE) != 0},  // src/parameters.c:216-220
       {"noise_t", &cfg->noise_t, T && (fl & CH4_F_TEMPERATURE_INITIAL_ADD_NOISE)},  // src/parameters.c:347-351
   };
@@ -2028,7 +2040,8 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   cfg->particle_number = (int)particle_number;
   cfg->resume = (int)resume;
   cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types * (int)cp_coeff_types * (int)aspect_ratio_types *
-                        (int)gyrotaxis_velocity_types * (int)rotational_diffusion_types * (int)swim_velocity_types;
+                        (int)gyrotaxis_velocity_types * (int)rotational_diffusion_types * (int)swim_velocity_types *
+                        (int)critical_shear_rate_types * (int)jump_time_types;
   // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
   cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
   cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;
@@ -2169,6 +2182,9 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_ORIENTATION_RANDOM", CH4_F2_LAGRANGE_ORIENTATION_RANDOM},
       {"LB_FLUID_LES_SISM", CH4_F2_FLUID_LES_SISM},
       {"LB_FLUID_LES_SISM_KALMAN", CH4_F2_FLUID_LES_SISM_KALMAN},
+      {"LAGRANGE_ORIENTATION_ACTIVE_JUMP", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP},
+      {"LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE},
+      {"LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2354,7 +2370,8 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
     {
       // the orientation variants, as src/lagrange.c nests them
       const uint64_t f2 = c->flags2;
-      const uint64_t modes = CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE |
+      const uint64_t modes = CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP |
+                             CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE |
                              CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION |
                              CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION;
       if ((f2 & (CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)) &&
@@ -2373,6 +2390,12 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
         return why = "swimming along n needs LAGRANGE_ORIENTATION_SECONDORIENTATION", CH4_ERR_UNSUPPORTED;
       if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
         return why = "LAGRANGE_ORIENTATION_ACTIVE_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
+      if ((f2 & (CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS)) &&
+          !(f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP))
+        return why = "the LAGRANGE_ORIENTATION_ACTIVE_JUMP_* variants need LAGRANGE_ORIENTATION_ACTIVE_JUMP",
+               CH4_ERR_UNSUPPORTED;
+      if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
+        return why = "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
       const uint64_t noise = CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM;
       if ((f2 & noise) && !(c->flags & CH4_F_LAGRANGE_ORIENTATION))
         return why = "LAGRANGE_ORIENTATION_DIFFUSION and _RANDOM need LAGRANGE_ORIENTATION", CH4_ERR_UNSUPPORTED;
@@ -3059,7 +3082,16 @@ void orientation_extras(std::vector<PField>& v, uint64_t fl, uint64_t fl2, bool 
   }
   if (compound && (fl2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION))
     v.push_back({"rotational_diffusion", &P::rotational_diffusion});
-  if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) v.push_back({"swim_velocity", &P::swim_velocity});
+  if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) {
+    v.push_back({"swim_velocity", &P::swim_velocity});
+    // src/lagrange.c:1993-2011 (datasets) and 4411-4425 (part.h5, with the jump's direction;
+    // time_from_jump is not written)
+    if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP) {
+      v.insert(v.end(), {{"critical_shear_rate", &P::critical_shear_rate}, {"shear_rate", &P::shear_rate},
+                         {"jump_time", &P::jump_time}});
+      if (compound) v.insert(v.end(), {{"px_jump", &P::px_jump}, {"py_jump", &P::py_jump}, {"pz_jump", &P::pz_jump}});
+    }
+  }
 }
 
 // the per-particle datasets of output_particles, in its order, for the supported flags
@@ -3194,7 +3226,14 @@ bool write_particle_xmf(const std::string& path, const std::string& h5name, int 
         scalar("aspect_ratio");
         if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_JEFFREY_GYROTAXIS) scalar("gyrotaxis_velocity");
       }
-      if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) scalar("swim_velocity");
+      if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE) {
+        scalar("swim_velocity");
+        if (fl2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP) {
+          scalar("critical_shear_rate");
+          scalar("shear_rate");
+          scalar("jump_time");
+        }
+      }
     }
   }
   if (fl & CH4_F_LB_TEMPERATURE) {

@@ -106,6 +106,10 @@ struct PartParams {
   // orientation variants: the second orientation, gyrotaxis, the swimming mode of active
   // tracers (0 none, 1 along p, 2 ballistic, 3 while dT/dt > 0, 4 along n, 5 rods p, discs n)
   int second, gyro, swim;
+  // swim mode 6, run and tumble: bit 0 the temperature in the shear rate's place, bit 1
+  // high-pass (jump below the critical value); log(0.01) of the host libm
+  int jump_flags;
+  double log001;
   // orientation noise (bit 0 rotational diffusion, bit 1 a random p every sub-step): per
   // particle index, the three gaussian draws xi and the random unit vector, drawn by the
   // host from the handle's drand48 stream in particle order for this sub-step
@@ -716,10 +720,44 @@ static __device__ __noinline__ void orient_particle(double* pf, long long np, in
 
 // The swimming velocity of an active tracer (LAGRANGE_ORIENTATION_ACTIVE, src/lagrange.c:
 // 3045-3190), after v = u: mode 1 v += s p, 2 v = s p (ballistic), 3 v += s p while dT/dt > 0,
-// 4 v += s n, 5 v += s p for rods (a >= 1) and s n for discs.
-static __device__ __noinline__ void swim_velocity(const double* pf, long long np, int ip, int mode, double& vx,
-                                                  double& vy, double& vz) {
+// 4 v += s n, 5 v += s p for rods (a >= 1) and s n for discs, 6 run and tumble (jumps along
+// the orientation at the last jump, decaying with exp(-time_from_jump / jump_time)).
+static __device__ __noinline__ void swim_velocity(double* pf, long long np, int ip, int mode, int jflags,
+                                                  double log001, double dtl, double& vx, double& vy, double& vz) {
 #define F(name) pf[CH4_PF(name) * np + ip]
+  if (mode == 6) {  // src/lagrange.c:3048-3130, the shear rate as the reference writes it
+    double shear_rate;
+    if (jflags & 1) {
+      shear_rate = F(t);
+    } else {
+      shear_rate = sqrt(2.) * sqrt((F(dx_ux)) * (F(dx_ux)) + (F(dy_uy)) * (F(dz_uy)) + (F(dz_uz)) * (F(dz_uz)) +
+                                   0.5 * ((F(dy_ux)) + (F(dx_uy))) * ((F(dy_ux)) + (F(dx_uy))) +
+                                   0.5 * ((F(dz_ux)) + (F(dx_uz))) * ((F(dz_ux)) + (F(dx_uz))) +
+                                   0.5 * ((F(dy_uz)) + (F(dz_uy))) * ((F(dy_uz)) + (F(dz_uy))));
+      F(shear_rate) = shear_rate;
+    }
+    const double jump_time_duration = -(F(jump_time)) * log001;
+    double amp;
+    if (F(time_from_jump) > jump_time_duration) {
+      amp = 0.0;
+      const bool go = (jflags & 2) ? shear_rate < F(critical_shear_rate) : shear_rate > F(critical_shear_rate);
+      if (go) {
+        F(time_from_jump) = 0.0;
+        amp = F(swim_velocity);
+        F(px_jump) = F(px);
+        F(py_jump) = F(py);
+        F(pz_jump) = F(pz);
+      }
+    } else {
+      amp = F(swim_velocity) * exp(-(F(time_from_jump)) / (F(jump_time)));
+      if (F(jump_time) == 0.0) amp = 0.0;
+    }
+    vx += amp * (F(px_jump));
+    vy += amp * (F(py_jump));
+    vz += amp * (F(pz_jump));
+    F(time_from_jump) += dtl;
+    return;
+  }
   const double s = F(swim_velocity);
   const bool along_n = mode == 4 || (mode == 5 && !(F(aspect_ratio) >= 1.0));
   const double dx = along_n ? F(nx) : F(px), dy = along_n ? F(ny) : F(py), dz = along_n ? F(nz) : F(pz);
@@ -853,7 +891,7 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
     vy = uy;
     vz = uz;
     if constexpr (ORIENT)  // active tracers need LAGRANGE_ORIENTATION
-      if (P.swim) swim_velocity(pf, np, ip, P.swim, vx, vy, vz);
+      if (P.swim) swim_velocity(pf, np, ip, P.swim, P.jump_flags, P.log001, dtl, vx, vy, vz);
     double vxo = F(vx_old), vyo = F(vy_old), vzo = F(vz_old);
     if (first) {
       vxo = vx;

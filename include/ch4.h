@@ -188,7 +188,15 @@ enum {
    * cell by cell in the reference's loop order (its gradient sees the cells before a cell
    * already updated, and zero beyond the lattice) */
   CH4_F2_FLUID_LES_SISM = 1ull << 38,
-  CH4_F2_FLUID_LES_SISM_KALMAN = 1ull << 39
+  CH4_F2_FLUID_LES_SISM_KALMAN = 1ull << 39,
+  /* run-and-tumble swimmers, src/lagrange.c:3048-3130: a tracer jumps along its present p
+   * when the shear rate sqrt(2 S:S) (the reference's expression, with dy_uy * dz_uy) exceeds
+   * its critical value (HIGHPASS: falls below it; TEMPERATURE: the fluid temperature takes
+   * the shear rate's place) and its last jump has decayed, then swims with
+   * swim_velocity * exp(-time_from_jump / jump_time) */
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP = 1ull << 40,
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE = 1ull << 41,
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS = 1ull << 42
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
@@ -276,6 +284,10 @@ typedef struct {
   double gyrotaxis_velocity, swim_velocity;
   /* LAGRANGE_ORIENTATION_DIFFUSION: the rotational diffusivity D_r */
   double rotational_diffusion;
+  /* LAGRANGE_ORIENTATION_ACTIVE_JUMP (src/typedef.h:438-440): the last shear rate, the
+   * critical one, the time since the last jump, the jump's decay time and its direction */
+  double shear_rate, critical_shear_rate, time_from_jump, jump_time;
+  double px_jump, py_jump, pz_jump;
 } ch4_particle;
 
 /* Global averages of dump_averages (src/output.c:63-~760), FP64 sums over the

@@ -843,9 +843,44 @@ static void orient_particle(ch4o_state *s, ch4_particle *p, int jeffery, int fir
 }
 
 /* the swimming velocity of an active tracer, src/lagrange.c:3045-3190 (after v = u) */
-static void swim(const ch4o_state *s, ch4_particle *p) {
+static void swim(const ch4o_state *s, ch4_particle *p, double dtl) {
   const uint64_t f2 = s->cfg.flags2;
   if (!(f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE)) return;
+  if (f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP) {
+    /* run and tumble, src/lagrange.c:3048-3130 (the shear rate as the reference writes it) */
+    double shear_rate;
+    if (f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) {
+      shear_rate = p->t;
+    } else {
+      p->shear_rate = shear_rate =
+          sqrt(2.) * sqrt((p->dx_ux) * (p->dx_ux) + (p->dy_uy) * (p->dz_uy) + (p->dz_uz) * (p->dz_uz) +
+                          0.5 * ((p->dy_ux) + (p->dx_uy)) * ((p->dy_ux) + (p->dx_uy)) +
+                          0.5 * ((p->dz_ux) + (p->dx_uz)) * ((p->dz_ux) + (p->dx_uz)) +
+                          0.5 * ((p->dy_uz) + (p->dz_uy)) * ((p->dy_uz) + (p->dz_uy)));
+    }
+    const double jump_time_duration = -(p->jump_time) * log(0.01);
+    double amp;
+    if (p->time_from_jump > jump_time_duration) {
+      amp = 0.0;
+      const int go = (f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS) ? shear_rate < p->critical_shear_rate
+                                                                            : shear_rate > p->critical_shear_rate;
+      if (go) {
+        p->time_from_jump = 0.0;
+        amp = p->swim_velocity;
+        p->px_jump = p->px;
+        p->py_jump = p->py;
+        p->pz_jump = p->pz;
+      }
+    } else {
+      amp = p->swim_velocity * exp(-(p->time_from_jump) / (p->jump_time));
+      if (p->jump_time == 0.0) amp = 0.0;
+    }
+    p->vx += amp * (p->px_jump);
+    p->vy += amp * (p->py_jump);
+    p->vz += amp * (p->pz_jump);
+    p->time_from_jump += dtl;
+    return;
+  }
   if (f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_BALLISTIC) {
     p->vx = (p->swim_velocity) * (p->px);
     p->vy = (p->swim_velocity) * (p->py);
@@ -980,7 +1015,7 @@ static void move_particle(const ch4o_state *s, ch4_particle *p, int first, doubl
     p->vx = p->ux;
     p->vy = p->uy;
     p->vz = p->uz;
-    swim(s, p);
+    swim(s, p, dtl);
     if (first) {
       p->vx_old = p->vx;
       p->vy_old = p->vy;

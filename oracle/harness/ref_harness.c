@@ -135,6 +135,9 @@ static void write_part_layout(void) {
 #endif
 #ifdef LAGRANGE_ORIENTATION_ACTIVE
   F(swim_velocity);
+#ifdef LAGRANGE_ORIENTATION_ACTIVE_JUMP
+  F(shear_rate); F(critical_shear_rate); F(time_from_jump); F(jump_time); F(px_jump); F(py_jump); F(pz_jump);
+#endif
 #endif
 #endif
 #undef F

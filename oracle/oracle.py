@@ -172,6 +172,16 @@ FLAGSETS.update({
     "les_sism": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV", "LB_FLUID_LES", "LB_FLUID_LES_SISM"],
     "les_kalman": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
                    "LB_FLUID_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SISM", "LB_FLUID_LES_SISM_KALMAN"],
+    # run-and-tumble swimmers: jumps triggered by the shear rate, or (high-pass) by a low temperature
+    "particles_jump": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
+                       "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
+                       "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY", "LAGRANGE_ORIENTATION_ACTIVE",
+                       "LAGRANGE_ORIENTATION_ACTIVE_JUMP"],
+    "particles_jumpt": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LB_TEMPERATURE",
+                        "LB_TEMPERATURE_BUOYANCY", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT",
+                        "LAGRANGE_ADDEDMASS", "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_ACTIVE",
+                        "LAGRANGE_ORIENTATION_ACTIVE_JUMP", "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE",
+                        "LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS"],
     # Smagorinsky-Lilly in a stably stratified channel
     "les_lilly": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_BC_Y", "LB_TEMPERATURE",
                   "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SMAGORINSKY_LILLY"],
@@ -246,6 +256,10 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
                       ("LAGRANGE_ORIENTATION_DIFFUSION", "rotational_diffusion"),  # src/parameters.c:668-681
                       ("LAGRANGE_ORIENTATION_ACTIVE", "swim_velocity")):  # src/parameters.c:684-696
         if int(cfg.flags2) & abi.FLAGS2[flag]:
+            keys += [key + "_types", key + "_min", key + "_max"]
+            vals.update({key + "_types": 1, key + "_min": 1.0, key + "_max": 1.0})
+    if int(cfg.flags2) & abi.FLAGS2["LAGRANGE_ORIENTATION_ACTIVE_JUMP"]:  # src/parameters.c:698-722
+        for key in ("critical_shear_rate", "jump_time"):
             keys += [key + "_types", key + "_min", key + "_max"]
             vals.update({key + "_types": 1, key + "_min": 1.0, key + "_max": 1.0})
     if int(cfg.flags) & abi.FLAGS["LB_TEMPERATURE_FORCING"]:  # src/parameters.c: the source amplitude

@@ -135,6 +135,14 @@ CASES = {
                                         time_dt_lagr_factor=2.0, particle_number=300)),
     "particles_rand": dict(flagset="particles_rand", NX=9, NY=10, NZ=6, npart=200,
                            params=dict(tau_u=0.6, Amp_x=3e-3, seed=27, time_dt_lagr_factor=3.0, particle_number=200)),
+    # run-and-tumble swimmers
+    "particles_jump": dict(flagset="particles_jump", NX=10, NY=8, NZ=7, npart=300,
+                           params=dict(tau_u=0.55, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=28,
+                                       time_dt_lagr_factor=2.0, particle_number=300)),
+    "particles_jumpt": dict(flagset="particles_jumpt", NX=9, NY=8, NZ=7, npart=250,
+                            params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=29,
+                                        T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3,
+                                        time_dt_lagr_factor=2.0, particle_number=250)),
     # Smagorinsky-Lilly: T rising with y (stable), so the buoyancy damps |S| where Ri < 1
     "les_lilly": dict(flagset="les_lilly", NX=8, NY=9, NZ=6,
                       params=dict(tau_u=0.52, tau_t=0.55, Amp_x=0.02, T_bot=0.0, T_top=1.0, T_ref=0.5, beta_t=0.3,
@@ -232,6 +240,15 @@ def make_case(name, seed=0, storage=0, dims=None, **over):
         if "LAGRANGE_ORIENTATION_ACTIVE" in flags:
             for i, p in enumerate(state["part"]):
                 p.swim_velocity = [0.01, 0.0, 0.03, 0.002][(i // 4) % 4]
+        if "LAGRANGE_ORIENTATION_ACTIVE_JUMP" in flags:  # thresholds either side of the flow's values
+            crit = ([0.3, 0.5, 0.7, 1e10] if "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE" in flags
+                    else [1e-5, 1e-4, 1e-3, 1e10])
+            for i, p in enumerate(state["part"]):
+                p.critical_shear_rate = crit[i % 4]
+                p.jump_time = [0.0, 0.5, 2.0, 5.0][(i // 4) % 4]
+                p.time_from_jump = [0.0, 0.3, 3.0, 30.0][(i // 16) % 4]
+                v = rng.normal(size=3)
+                p.px_jump, p.py_jump, p.pz_jump = v / np.linalg.norm(v)
         if "LAGRANGE_ORIENTATION_DIFFUSION" in flags:  # 0 for some: their p is still normalised
             for i, p in enumerate(state["part"]):
                 p.rotational_diffusion = [0.0, 0.01, 0.1, 0.002][(i // 2) % 4]

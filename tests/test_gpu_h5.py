@@ -135,6 +135,8 @@ def _fields(flags, output_fluid, flags2=0):
                     f.append(("gyrotaxis_velocity", "gyrotaxis_velocity"))
             if flags2 & abi.FLAGS2["LAGRANGE_ORIENTATION_ACTIVE"]:
                 f.append(("swim_velocity", "swim_velocity"))
+                if flags2 & abi.FLAGS2["LAGRANGE_ORIENTATION_ACTIVE_JUMP"]:  # src/lagrange.c:1993-2011
+                    f += [(n, n) for n in ("critical_shear_rate", "shear_rate", "jump_time")]
     if flags & abi.FLAGS["LB_TEMPERATURE"]:
         f += [("temperature", "t"), ("dt_t", "dt_t")]
         if grad:
@@ -156,7 +158,7 @@ def _particle_sim(name, seed, nsteps):
 
 
 @pytest.mark.parametrize("name", ["particles", "particles_t", "particles_or", "particles_tt", "particles_swims",
-                                  "particles_swimt"])
+                                  "particles_swimt", "particles_jump"])
 def test_particle_file_holds_the_particles(name, tmp_path):
     cfg, state, sim = _particle_sim(name, 65, 4)
     with sim:
