@@ -41,6 +41,7 @@ constexpr int PF_TFAC = PF_FIELDS + 2;
 constexpr int PF_TEXP = PF_FIELDS + 3;
 constexpr int PF_TOTAL = PF_FIELDS + 4;
 constexpr int GATHER_BLOCK = 128;  // threads (cells along x) per block of the first deposit pass
+constexpr int GATHER_KB = 8;       // planes per block of that pass (each thread walks a column)
 
 template <typename A>
 struct PartParams {
@@ -1361,46 +1362,60 @@ __device__ __forceinline__ double fold_faces_t(const PartParams<A>& P, int i, in
 // cells' appends serialised the whole pass).
 template <typename A>
 __global__ void __launch_bounds__(GATHER_BLOCK) deposit_gather_kernel(const PartParams<A> P) {
-  // grid (x blocks, NY, NZ): no index division
+  // grid (x blocks, NY, groups of GATHER_KB planes): a thread walks its column up z and
+  // keeps the home ranges of plane k + 1 for the next cell (4 range loads per cell, not 8)
   __shared__ int s_n;
-  if (threadIdx.x == 0) s_n = 0;
-  __syncthreads();
   const int i = blockIdx.x * GATHER_BLOCK + threadIdx.x;
-  const int j = blockIdx.y, k = blockIdx.z;
-  const int bid = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  if (i < P.NX) {
-    const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
-    const int HX = P.NX + 1, HY = P.NY + 1;
-    int m = 0, best = 0, slot = 0;
+  const int j = blockIdx.y;
+  const int k0 = blockIdx.z * GATHER_KB, k1 = min(k0 + GATHER_KB, P.NZ);
+  const int HX = P.NX + 1, HY = P.NY + 1;
+  int2 lo[4], hi[4];
+  if (i < P.NX)
 #pragma unroll
-    for (int h = 0; h < 8; h++) {
-      const int2 rg = P.cell_rng[home_of(i, j, k, h, HX, HY)];
-      const int cnt = rg.y - rg.x;
-      if (cnt > 0) {
-        best = h;
-        slot = rg.x;
+    for (int h = 0; h < 4; h++) lo[h] = P.cell_rng[((long long)k0 * HY + j + (h >> 1)) * HX + i + (h & 1)];
+  for (int k = k0; k < k1; k++) {
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const int bid = (k * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;  // one region per block row and plane
+    if (i < P.NX) {
+      const long long cidx = ((long long)k * P.NY + j) * P.NX + i;
+#pragma unroll
+      for (int h = 0; h < 4; h++) hi[h] = P.cell_rng[((long long)(k + 1) * HY + j + (h >> 1)) * HX + i + (h & 1)];
+      // homes h = bit 0 +x, bit 1 +y, bit 2 +z (home_of's order)
+      int m = 0, best = 0, slot = 0;
+#pragma unroll
+      for (int h = 0; h < 8; h++) {
+        const int2 rg = h < 4 ? lo[h] : hi[h - 4];
+        const int cnt = rg.y - rg.x;
+        if (cnt > 0) {
+          best = h;
+          slot = rg.x;
+        }
+        m += cnt;
       }
-      m += cnt;
-    }
-    // with the temperature source a face cell also takes the images of the halo cells
-    // beyond the opposite face: the merge pass does those
-    const bool face = P.twoway_temp && (i == 0 || i == P.NX - 1 || j == 0 || j == P.NY - 1 || k == 0 || k == P.NZ - 1);
-    if (m >= 2 || face) {
-      P.busy[(long long)bid * GATHER_BLOCK + atomicAdd(&s_n, 1)] = (int)cidx;  // the merge writes this cell
-    } else {
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      if (m == 1) {
-        if (P.twoway_temp) deposit_add<true, true>(P.srec, P.nsort, slot, best, P.nrec - 1, acc);
-        else deposit_add<true, false>(P.srec, P.nsort, slot, best, 0, acc);
+      // with the temperature source a face cell also takes the images of the halo cells
+      // beyond the opposite face: the merge pass does those
+      const bool face =
+          P.twoway_temp && (i == 0 || i == P.NX - 1 || j == 0 || j == P.NY - 1 || k == 0 || k == P.NZ - 1);
+      if (m >= 2 || face) {
+        P.busy[(long long)bid * GATHER_BLOCK + atomicAdd(&s_n, 1)] = (int)cidx;  // the merge writes this cell
+      } else {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        if (m == 1) {
+          if (P.twoway_temp) deposit_add<true, true>(P.srec, P.nsort, slot, best, P.nrec - 1, acc);
+          else deposit_add<true, false>(P.srec, P.nsort, slot, best, 0, acc);
+        }
+        P.dep[cidx] = (A)acc[0];
+        P.dep[P.N + cidx] = (A)acc[1];
+        P.dep[2 * P.N + cidx] = (A)acc[2];
+        if (P.twoway_temp) P.dep[3 * P.N + cidx] = (A)acc[3];
       }
-      P.dep[cidx] = (A)acc[0];
-      P.dep[P.N + cidx] = (A)acc[1];
-      P.dep[2 * P.N + cidx] = (A)acc[2];
-      if (P.twoway_temp) P.dep[3 * P.N + cidx] = (A)acc[3];
+#pragma unroll
+      for (int h = 0; h < 4; h++) lo[h] = hi[h];
     }
+    __syncthreads();
+    if (threadIdx.x == 0) P.bcount[bid] = s_n;
   }
-  __syncthreads();
-  if (threadIdx.x == 0) P.bcount[bid] = s_n;
 }
 
 // The listed cells of every region, compacted to P.dense[boff[r] ...].
