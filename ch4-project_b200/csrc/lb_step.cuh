@@ -471,6 +471,17 @@ __global__ void __launch_bounds__(128) lb_step_kernel(const __grid_constant__ St
   lb_cell<S, A, THERM, SCAL, V>(P, x, blockIdx.y, P.zfirst + (int)blockIdx.z * P.zstride);
 }
 
+// FP32 arithmetic, fluid + temperature, Smagorinsky LES: held to 64 registers (eight
+// 128-thread blocks per SM) it runs 8-11 % faster than at the 88 it takes unbounded, a few
+// spilled values included (measured on Rayleigh-Benard LES at 96^3 and 192^3; the
+// single-set LES kernel already fits 64, the 80-register bound measured slower)
+template <typename S, typename A, bool THERM, bool SCAL, int V>
+__global__ void __launch_bounds__(128, 8) lb_step_kernel_les64(const __grid_constant__ StepParams<A> P) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= P.NX) return;
+  lb_cell<S, A, THERM, SCAL, V>(P, x, blockIdx.y, P.zfirst + (int)blockIdx.z * P.zstride);
+}
+
 // The FP64 BGK step with two population sets, held to 128 registers (four 128-thread
 // blocks per SM): the allocation at which it runs at the HBM roofline; left to itself the
 // compiler may take a few more and lose a block per SM (-13 % measured).  (A minimum-blocks
