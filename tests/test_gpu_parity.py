@@ -118,6 +118,23 @@ def test_reduced_precision_error_bounds(name, storage, tol_u, tol_rho, tol_t):
         assert et < tol_t, "t rel L2 %g" % et
 
 
+@pytest.mark.parametrize("name", ["les_sism", "les_kalman", "les_lilly", "particles_jump", "particles_rdiff",
+                                  "particles_swims", "particles_rb", "duct"])
+def test_fp32_newer_flag_sets_close_to_fp64(name):
+    """The FP32 path of the flag sets added with the later features: the lattice in FP32
+    arithmetic and storage (particles keep FP64 state) stays within 1e-2 relative L2 of u
+    after 20 steps of the FP64 oracle (eddy-viscosity switches such as SISM's |S| > |S_mean|
+    may flip on a rounding difference, hence the looser bound than the plain flows')."""
+    _, cfg64, state = make_case(name, seed=31)
+    _, cfg, _ = make_case(name, seed=31, storage=1)
+    ref = run_restatement(cfg64, state, 20)
+    gpu = run_gpu(cfg, state, 20)
+    assert rel_l2(gpu["u"], ref["u"]) < 1e-2
+    if "part" in state:
+        for f in ("x", "y", "z"):
+            assert np.abs(gpu["part"][f] - ref["part"][f]).max() < 1e-4, f
+
+
 def test_larger_lattice_bit_identical():
     # 32x24x16 thermal convection, 120 steps: FP64 GPU == oracle
     _, cfg, state = make_case("rb", seed=9)
