@@ -63,6 +63,10 @@ MULTIBLOCK = {
     "hit_multiblock": ("hit", (300, 6, 5), 60, 22),
     "les_multiblock": ("les", (160, 9, 5), 60, 23),
     "particles_multiblock": ("particles", (140, 8, 6), 30, 24),
+    # walls on x and z (the x walls on both ends of a multi-block row); shear-improved LES,
+    # whose running mean is read across block boundaries in the reference's loop order
+    "duct_multiblock": ("duct", (150, 8, 6), 60, 25),
+    "sism_multiblock": ("les_kalman", (170, 9, 5), 60, 26),
 }
 
 
