@@ -192,7 +192,10 @@ DIAG_FIELDS = ["x", "y", "z", "ux", "uy", "uz", "ux2", "uy2", "uz2", "rho", "rho
 PART_AVG_FIELDS = ["count", "vx", "vy", "vz", "vx2", "vy2", "vz2", "vx4", "vy4", "vz4",
                    "ax", "ay", "az", "ax2", "ay2", "az2", "ax4", "ay4", "az4",
                    "t", "t2", "t4", "dt_t", "dt_t2",
-                   "ux", "uy", "uz", "ux2", "uy2", "uz2", "ux4", "uy4", "uz4"]
+                   "ux", "uy", "uz", "ux2", "uy2", "uz2", "ux4", "uy4", "uz4",
+                   "dt_px", "dt_py", "dt_pz", "dt_px2", "dt_py2", "dt_pz2", "dt_px4", "dt_py4", "dt_pz4",
+                   "dt_nx", "dt_ny", "dt_nz", "dt_nx2", "dt_ny2", "dt_nz2", "dt_nx4", "dt_ny4", "dt_nz4",
+                   "t_p"]
 
 AVERAGE_FIELDS = ["rho", "ux", "uy", "uz", "ux2", "uy2", "uz2", "ene", "eps",
                   "t", "t2", "epst", "dxt", "dyt", "dzt", "uxt", "uyt", "uzt", "nux", "nuy", "nuz",

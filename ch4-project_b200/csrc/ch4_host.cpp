@@ -25,6 +25,7 @@
 #include "../../include/ch4.h"
 #include "h5file.hpp"
 #include "launch.h"
+#include "part_avg.cuh"
 
 using namespace ch4;
 
@@ -1244,7 +1245,7 @@ struct Engine : EngineBase {
     if (types < 1) return H->fail(CH4_ERR_ARG, "particle_types must be >= 1");
     const int nblk = (int)std::min<long long>(4 * 148, ((long long)np + 127) / 128);
     double* d = nullptr;
-    const size_t part_n = (size_t)types * 3 * nblk * 11 * 2, out_n = (size_t)types * CH4_PART_AVG_FIELDS;
+    const size_t part_n = (size_t)types * PAVG_GROUPS * nblk * PAVG_GROUP * 2, out_n = (size_t)types * CH4_PART_AVG_FIELDS;
     ch4_status st = H->cuda(cudaMalloc(&d, (part_n + out_n) * sizeof(double)), "particle averages scratch");
     if (st) return st;
     st = H->cuda(launch_particle_averages(pf, np, types, d, nblk, d + part_n, H->stream), "particle averages");
@@ -2779,7 +2780,17 @@ ch4_status ch4_dump_particle_averages(ch4_handle* h, const char* dir, double tim
     std::fprintf(f, "%e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e %e ", time_now, (double)type, o.vx, o.vy,
                  o.vz, o.vx2, o.vy2, o.vz2, o.vx4, o.vy4, o.vz4, o.ax, o.ay, o.az, o.ax2, o.ay2, o.az2, o.ax4, o.ay4,
                  o.az4);
-    if (c.flags & CH4_F_LB_TEMPERATURE) std::fprintf(f, "%e %e %e %e %e ", o.t, o.t2, o.t4, o.dt_t, o.dt_t2);
+    if ((c.flags & CH4_F_LAGRANGE_GRADIENT) && (c.flags & CH4_F_LAGRANGE_ORIENTATION)) {
+      std::fprintf(f, "%e %e %e %e %e %e %e %e %e ", o.dt_px, o.dt_py, o.dt_pz, o.dt_px2, o.dt_py2, o.dt_pz2, o.dt_px4,
+                   o.dt_py4, o.dt_pz4);
+      if (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_SECONDORIENTATION)
+        std::fprintf(f, "%e %e %e %e %e %e %e %e %e ", o.dt_nx, o.dt_ny, o.dt_nz, o.dt_nx2, o.dt_ny2, o.dt_nz2, o.dt_nx4,
+                     o.dt_ny4, o.dt_nz4);
+    }
+    if (c.flags & CH4_F_LB_TEMPERATURE) {
+      std::fprintf(f, "%e %e %e %e %e ", o.t, o.t2, o.t4, o.dt_t, o.dt_t2);
+      if (c.flags2 & CH4_F2_LAGRANGE_TEMPERATURE) std::fprintf(f, "%e ", o.t_p);
+    }
     if (c.flags & CH4_F_LAGRANGE_OUTPUT_FLUID_AVERAGES)
       std::fprintf(f, "%e %e %e %e %e %e %e %e %e ", o.ux, o.uy, o.uz, o.ux2, o.uy2, o.uz2, o.ux4, o.uy4, o.uz4);
     std::fprintf(f, "\n");

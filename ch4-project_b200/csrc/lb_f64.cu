@@ -66,7 +66,7 @@ cudaError_t launch_soa_to_aos(const StepParams<double>& P, LaunchShape, int set,
 }
 cudaError_t launch_particle_averages(const double* pf, int np, int types, double* partial, int nblk, double* out_dev,
                                      cudaStream_t st) {
-  part_avg_partial_kernel<<<dim3(nblk, types, 3), PAVG_BLOCK, 0, st>>>(pf, np, types, partial);
+  part_avg_partial_kernel<<<dim3(nblk, types, PAVG_GROUPS), PAVG_BLOCK, 0, st>>>(pf, np, types, partial);
   cudaError_t e = cudaGetLastError();
   if (e) return e;
   part_avg_final_kernel<<<types, 64, 0, st>>>(partial, nblk, out_dev);

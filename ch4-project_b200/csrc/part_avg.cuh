@@ -1,9 +1,10 @@
 // Lagrangian averages per particle type: the sums of dump_particle_averages
 // (src/lagrange.c:2598-2931).  A particle's type is (int)name % particle_types
 // (src/lagrange.c:2698).  Per type: the count and the sums of v, v^2, v^4, a, a^2,
-// a^4 (each component), with a temperature set of t, t^2, t^4, dt_t, dt_t^2, and of
-// u, u^2, u^4 (the fluid velocity at the particle, LAGRANGE_OUTPUT_FLUID_AVERAGES);
-// each sum is then multiplied by 1/count, as the reference normalises.
+// a^4 (each component), with a temperature set of t, t^2, t^4, dt_t, dt_t^2, of
+// u, u^2, u^4 (the fluid velocity at the particle, LAGRANGE_OUTPUT_FLUID_AVERAGES), of
+// dp/dt and dn/dt with squares and fourth powers (orientation) and of t_p (particle
+// temperature); each sum is then multiplied by 1/count, as the reference normalises.
 //
 // The sums run in double-double over a fixed assignment of state slots to threads
 // and a fixed tree (no atomics); the reference adds in particle order in plain FP64,
@@ -15,8 +16,9 @@
 
 namespace ch4 {
 
-constexpr int PAVG_FIELDS = CH4_PART_AVG_FIELDS;  // count + 32 sums (ch4_part_avg order)
-constexpr int PAVG_GROUP = 11;                     // fields per block (three groups)
+constexpr int PAVG_FIELDS = CH4_PART_AVG_FIELDS;  // count + 51 sums (ch4_part_avg order)
+constexpr int PAVG_GROUP = 11;                     // fields per block
+constexpr int PAVG_GROUPS = (PAVG_FIELDS + PAVG_GROUP - 1) / PAVG_GROUP;
 constexpr int PAVG_BLOCK = 128;
 
 #ifdef __CUDACC__
@@ -42,17 +44,23 @@ __device__ __forceinline__ double pavg_term(const double* pf, long long np, long
     const double d = at(CH4_PF(dt_t));
     return f == 22 ? d : d * d;
   }
-  // fluid velocity at the particle: u, u^2, u^4 (fields 24-32)
-  const int p = (f - 24) / 3, c = (f - 24) % 3;
-  const double x = at(CH4_PF(ux) + c);
-  return p == 0 ? x : p == 1 ? x * x : pow4(x);
+  // fluid velocity at the particle: u, u^2, u^4 (fields 24-32), then dp/dt and dn/dt with
+  // their squares and fourth powers (fields 33-50), then t_p (51); past the last field, 0
+  if (f <= 50) {
+    const int base = f <= 32 ? CH4_PF(ux) : f <= 41 ? CH4_PF(dt_px) : CH4_PF(dt_nx);
+    const int q = f <= 32 ? f - 24 : f <= 41 ? f - 33 : f - 42;
+    const int p = q / 3, c = q % 3;
+    const double x = at(base + c);
+    return p == 0 ? x : p == 1 ? x * x : pow4(x);
+  }
+  return f == 51 ? at(CH4_PF(t_p)) : 0.0;
 }
 
 // grid (nblk, types, 3): block b sums field group blockIdx.z of type blockIdx.y over
 // the slots b*PAVG_BLOCK + tid (stride nblk*PAVG_BLOCK); partial[((t*3+g)*nblk+b)*PAVG_GROUP+f] = {hi, lo}
 __global__ void __launch_bounds__(PAVG_BLOCK) part_avg_partial_kernel(const double* __restrict__ pf, int np, int types,
                                                                        double* __restrict__ partial) {
-  const int type = blockIdx.y, g = blockIdx.z, nblk = gridDim.x;
+  const int type = blockIdx.y, g = blockIdx.z, nblk = gridDim.x;  // gridDim.z == PAVG_GROUPS
   DD acc[PAVG_GROUP];
 #pragma unroll
   for (int f = 0; f < PAVG_GROUP; f++) acc[f] = DD{0.0, 0.0};
@@ -83,7 +91,7 @@ __global__ void __launch_bounds__(PAVG_BLOCK) part_avg_partial_kernel(const doub
     __syncthreads();
   }
   if (threadIdx.x < PAVG_GROUP) {
-    double* o = partial + (((long long)type * 3 + g) * nblk + blockIdx.x) * PAVG_GROUP * 2;
+    double* o = partial + (((long long)type * PAVG_GROUPS + g) * nblk + blockIdx.x) * PAVG_GROUP * 2;
     o[threadIdx.x * 2] = sh[0][threadIdx.x][0];
     o[threadIdx.x * 2 + 1] = sh[0][threadIdx.x][1];
   }
@@ -97,7 +105,7 @@ __global__ void part_avg_final_kernel(const double* __restrict__ partial, int nb
     const int g = f / PAVG_GROUP, k = f % PAVG_GROUP;
     DD acc{0.0, 0.0};
     for (int b = 0; b < nblk; b++) {
-      const double* p = partial + (((long long)type * 3 + g) * nblk + b) * PAVG_GROUP * 2 + k * 2;
+      const double* p = partial + (((long long)type * PAVG_GROUPS + g) * nblk + b) * PAVG_GROUP * 2 + k * 2;
       acc = dd_add(acc, DD{p[0], p[1]});
     }
     sum[f] = acc.hi;

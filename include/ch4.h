@@ -426,15 +426,20 @@ ch4_status ch4_set_face_exchange(ch4_handle *h, ch4_exchange_fn exchange, void *
 /* --- Lagrangian averages per particle type (dump_particle_averages) ------------ */
 
 /* Per type: the particle count, then the means of v, v^2, v^4, a, a^2, a^4 (per
- * component), of t, t^2, t^4, dt_t, dt_t^2 (meaningful with LB_TEMPERATURE) and of the
- * fluid velocity at the particle u, u^2, u^4 (src/lagrange.c:2598-2931). */
-#define CH4_PART_AVG_FIELDS 33
+ * component), of t, t^2, t^4, dt_t, dt_t^2 (meaningful with LB_TEMPERATURE), of the
+ * fluid velocity at the particle u, u^2, u^4, of dp/dt and dn/dt with their squares and
+ * fourth powers (LAGRANGE_ORIENTATION, _SECONDORIENTATION) and of the particle
+ * temperature t_p (LAGRANGE_TEMPERATURE) (src/lagrange.c:2598-2931). */
+#define CH4_PART_AVG_FIELDS 52
 typedef struct {
   double count;
   double vx, vy, vz, vx2, vy2, vz2, vx4, vy4, vz4;
   double ax, ay, az, ax2, ay2, az2, ax4, ay4, az4;
   double t, t2, t4, dt_t, dt_t2;
   double ux, uy, uz, ux2, uy2, uz2, ux4, uy4, uz4;
+  double dt_px, dt_py, dt_pz, dt_px2, dt_py2, dt_pz2, dt_px4, dt_py4, dt_pz4;
+  double dt_nx, dt_ny, dt_nz, dt_nx2, dt_ny2, dt_nz2, dt_nx4, dt_ny4, dt_nz4;
+  double t_p;
 } ch4_part_avg;
 
 /* The averages of every particle type (out[cfg.particle_types]) at the current state.
@@ -443,9 +448,10 @@ typedef struct {
 ch4_status ch4_particle_averages(ch4_handle *h, ch4_part_avg *out);
 
 /* One dump of dump_particle_averages into dir/particle_averages.dat (appended): per
- * type a line of time_now, type, the v and a means, the temperature means with
- * LB_TEMPERATURE and the fluid-velocity means with LAGRANGE_OUTPUT_FLUID_AVERAGES, in the
- * reference's "%e " format. */
+ * type a line of time_now, type, the v and a means, the dp/dt (and dn/dt) means with
+ * LAGRANGE_GRADIENT + LAGRANGE_ORIENTATION (+ _SECONDORIENTATION), the temperature means
+ * with LB_TEMPERATURE (and t_p with LAGRANGE_TEMPERATURE) and the fluid-velocity means with
+ * LAGRANGE_OUTPUT_FLUID_AVERAGES, in the reference's order and "%e " format. */
 ch4_status ch4_dump_particle_averages(ch4_handle *h, const char *dir, double time_now);
 
 /* The OUTPUT_ASCII field dumps of dump_averages (src/output.c:1107-1200): dir/vel.<itime>

@@ -345,16 +345,19 @@ def particle_averages(part, types):
         s[22] += dt
         s[23] += dt * dt
         k = 24
-        vals = [float(part["u" + c][ip]) if "u" + c in part else 0.0 for c in "xyz"]
-        for x in vals:
-            s[k] += x
-            k += 1
-        for x in vals:
-            s[k] += x * x
-            k += 1
-        for x in vals:
-            s[k] += math.pow(x, 4.0)
-            k += 1
+        # u (fields 24-32), then dp/dt (33-41) and dn/dt (42-50) with the orientation
+        for base in ("u", "dt_p", "dt_n"):
+            vals = [float(part[base + c][ip]) if base + c in part else 0.0 for c in "xyz"]
+            for x in vals:
+                s[k] += x
+                k += 1
+            for x in vals:
+                s[k] += x * x
+                k += 1
+            for x in vals:
+                s[k] += math.pow(x, 4.0)
+                k += 1
+        s[51] += float(part["t_p"][ip]) if "t_p" in part else 0.0  # LAGRANGE_TEMPERATURE
     out = []
     for ty in range(types):
         norm = 1.0 / sums[ty][0] if sums[ty][0] else float("inf")

@@ -21,7 +21,8 @@ if not torch.cuda.is_available():
 import ch4b200  # noqa: E402
 from ch4b200 import abi  # noqa: E402
 
-CASES = [("particles", "particles_fa", 3), ("particles_t", "particles_t", 4), ("particles_g", "particles_g", 2)]
+CASES = [("particles", "particles_fa", 3), ("particles_t", "particles_t", 4), ("particles_or2", "particles_or2", 2),
+         ("particles_tt", "particles_tt", 2), ("particles_g", "particles_g", 2)]
 
 
 def run(case, types, nsteps, seed):
@@ -49,7 +50,7 @@ def test_means_match_restatement_of_same_state(case, flagset, types):
             assert abs(g - e) <= 1e-12 * abs(e) + 1e-300, (f, ty, g, e)
 
 
-@pytest.mark.parametrize("case,flagset,types", CASES[:2])
+@pytest.mark.parametrize("case,flagset,types", CASES[:4])
 def test_dump_file_matches_reference(case, flagset, types, tmp_path):
     if not O.ref_available(flagset):
         pytest.skip("reference build missing")

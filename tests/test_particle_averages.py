@@ -13,22 +13,34 @@ import oracle as O
 from lbcases import make_case, pop_items
 
 
-def expected_rows(avg, time_now, therm, fluid):
+def expected_rows(avg, time_now, therm, fluid, orient=0, tp=False):
+    """The reference's columns (src/lagrange.c:2880-2922): v and a blocks, dp/dt (orient
+    >= 1) and dn/dt (orient 2) blocks, the temperature block (+ t_p), the fluid block."""
     rows = []
     for ty, a in enumerate(avg):
         r = [time_now, float(ty)] + a[1:19]
+        if orient >= 1:
+            r += a[33:42]
+        if orient >= 2:
+            r += a[42:51]
         if therm:
             r += a[19:24]
+            if tp:
+                r.append(a[51])
         if fluid:
             r += a[24:33]
         rows.append(r)
     return np.array(rows)
 
 
-@pytest.mark.parametrize("case,flagset,types,therm,fluid", [("particles", "particles_fa", 3, False, True),
-                                                            ("particles_t", "particles_t", 4, True, False),
-                                                            ("particles", "particles", 1, False, False)])
-def test_restatement_matches_reference_file(case, flagset, types, therm, fluid):
+@pytest.mark.parametrize("case,flagset,types,therm,fluid,orient,tp",
+                         [("particles", "particles_fa", 3, False, True, 0, False),
+                          ("particles_t", "particles_t", 4, True, False, 0, False),
+                          ("particles", "particles", 1, False, False, 0, False),
+                          ("particles_or2", "particles_or2", 2, False, False, 2, False),
+                          ("particles_or", "particles_or", 3, False, False, 1, False),
+                          ("particles_tt", "particles_tt", 2, True, False, 0, True)])
+def test_restatement_matches_reference_file(case, flagset, types, therm, fluid, orient, tp):
     if not O.ref_available(flagset):
         pytest.skip("reference build oracle/_ref/%s missing" % flagset)
     _, cfg, state = make_case(case, seed=21)
@@ -36,7 +48,7 @@ def test_restatement_matches_reference_file(case, flagset, types, therm, fluid):
     nsteps = 7
     ref = O.run_reference(flagset, cfg, nsteps, dict(pop_items(state)), parts=state["part"])
     got = np.loadtxt(ref["dat"]["particle_averages.dat"].splitlines(), ndmin=2)
-    exp = expected_rows(O.particle_averages(ref["part"], types), float(nsteps), therm, fluid)
+    exp = expected_rows(O.particle_averages(ref["part"], types), float(nsteps), therm, fluid, orient, tp)
     assert got.shape == exp.shape
     assert np.all(np.abs(got - exp) <= 5e-6 * np.abs(exp) + 1e-300)
 
