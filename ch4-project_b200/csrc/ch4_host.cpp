@@ -690,6 +690,15 @@ struct Engine : EngineBase {
   }
   double* rnd_h = nullptr;
   double* rnd_d = nullptr;
+  // random re-entry through the y walls (REINJECT without NORANDOM): re-entry counts and the
+  // drawn x, z by particle index
+  bool rj_random() const {
+    return (c.flags2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) && !(c.flags2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM);
+  }
+  int* rj_count = nullptr;
+  double* rj_xz = nullptr;
+  std::vector<int> rj_count_h;
+  std::vector<double> rj_xz_h;
   double* mig = nullptr;
   int mig_cap = 0;
   int* keep = nullptr;
@@ -779,6 +788,10 @@ struct Engine : EngineBase {
   }
 
   void free_particles() {
+    cudaFree(rj_count);
+    cudaFree(rj_xz);
+    rj_count = nullptr;
+    rj_xz = nullptr;
     cudaFreeHost(rnd_h);
     cudaFree(rnd_d);
     rnd_h = rnd_d = nullptr;
@@ -835,6 +848,8 @@ struct Engine : EngineBase {
     Q.nsort = pslab() ? np_all : np;
     Q.rstride = pslab() ? np_all : np;
     Q.noise = noise();
+    Q.rj_random = rj_random();
+    Q.rj_count = rj_count;
     Q.jump_flags = ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) ? 1 : 0) |
                    ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS) ? 2 : 0);
     Q.log001 = std::log(0.01);
@@ -1026,6 +1041,9 @@ struct Engine : EngineBase {
                                    cudaMalloc(&srec, sizeof(double) * nrec() * (size_t)n) == cudaSuccess &&
                                    cudaMalloc(&spid, sizeof(int) * (size_t)n) == cudaSuccess));
           if (!ok) return H->fail(CH4_ERR_NOMEM, "sort buffers");
+          if (rj_random() && (cudaMalloc(&rj_count, sizeof(int) * (size_t)n) != cudaSuccess ||
+                              cudaMalloc(&rj_xz, 2 * sizeof(double) * (size_t)n) != cudaSuccess))
+            return H->fail(CH4_ERR_NOMEM, "re-entry buffers");
           if (noise() && (cudaMallocHost(&rnd_h, 6 * sizeof(double) * (size_t)n) != cudaSuccess ||
                           cudaMalloc(&rnd_d, 6 * sizeof(double) * (size_t)n) != cudaSuccess))
             return H->fail(CH4_ERR_NOMEM, "orientation noise buffers");
@@ -1164,6 +1182,35 @@ struct Engine : EngineBase {
     }
     return H->cuda(cudaMemcpyAsync(rnd_d, rnd_h, 6 * sizeof(double) * (size_t)np, cudaMemcpyHostToDevice, H->stream),
                    "noise up");
+  }
+
+  // random re-entry (src/lagrange.c:3811-3817, 3891-3898): for every particle that re-entered
+  // in the last sub-step, in the caller's order, x = SX u and z = SZ u from the handle's
+  // stream (a second re-entry in the same sub-step draws again; the last pair stands)
+  ch4_status reinject_random() {
+    ch4_status st;
+    rj_count_h.resize((size_t)np);
+    if ((st = H->cuda(cudaMemcpyAsync(rj_count_h.data(), rj_count, sizeof(int) * (size_t)np, cudaMemcpyDeviceToHost,
+                                      H->stream),
+                      "re-entries")) ||
+        (st = H->cuda(cudaStreamSynchronize(H->stream), "re-entries")))
+      return st;
+    rj_xz_h.assign(2 * (size_t)np, 0.0);
+    bool any = false;
+    for (int i = 0; i < np; i++)
+      for (int k = 0; k < rj_count_h[(size_t)i]; k++) {
+        rj_xz_h[2 * (size_t)i] = c.SX * H->myrand();
+        rj_xz_h[2 * (size_t)i + 1] = c.SZ * H->myrand();
+        any = true;
+      }
+    if (!any) return CH4_OK;
+    if ((st = H->cuda(cudaMemcpyAsync(rj_xz, rj_xz_h.data(), 2 * sizeof(double) * (size_t)np, cudaMemcpyHostToDevice,
+                                      H->stream),
+                      "re-entry positions")))
+      return st;
+    PartParams<A> Q = part_params();
+    if ((st = H->cuda(launch_particle_reinject(Q, rj_xz, H->stream), "re-entry"))) return st;
+    return H->cuda(cudaStreamSynchronize(H->stream), "re-entry");  // rj_xz_h is reused
   }
 
   // slot order <- order2 (sorted by home cell); with sort, compute and sort the keys here
@@ -1704,7 +1751,7 @@ struct Engine : EngineBase {
     int done = 0;
     while (done < n) {
       // (orientation noise draws from the stream between two phase walks: one step at a time)
-      const int m = noise() ? 1 : std::min(CHUNK, n - done);
+      const int m = (noise() || rj_random()) ? 1 : std::min(CHUNK, n - done);
       if (hit) {
         // tables for phi_n (slot 0 = latest) and the m next phase sets
         if ((st = H->cuda(cudaEventSynchronize(hit_ev), "hit event"))) return st;
@@ -1804,6 +1851,7 @@ struct Engine : EngineBase {
             PartParams<A> Q = part_params();
             Q.first = (n_step == 1 && c.resume == 0);
             if ((st = H->cuda(launch_particle_substep(Q, H->stream), "particle substep"))) return st;
+            if (rj_random() && np > 0 && (st = reinject_random())) return st;
             if (pslab() && (st = migrate())) return st;  // move_particles ends with sendrecv_particles
           }
         }
@@ -2339,8 +2387,11 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
       return why = "particles are implemented with the fluid and optionally the temperature", CH4_ERR_UNSUPPORTED;
     const uint64_t f2 = c->flags2;
     // random re-injection draws from the reference's single drand48 stream
-    if ((f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) && !(f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM))
-      return why = "LAGRANGE_BC_INELASTIC_REINJECT is implemented with _NORANDOM", CH4_ERR_UNSUPPORTED;
+    // random re-entry and orientation noise would interleave their draws particle by particle
+    // within a sub-step, after the re-entries are known: not built
+    if ((f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) && !(f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM) &&
+        (f2 & (CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM)))
+      return why = "random re-injection runs without orientation noise", CH4_ERR_UNSUPPORTED;
     // the small-tau_drag velocity reads Du/Dt, which only the added-mass term computes
     // (elsewhere the reference reads an unset local, src/lagrange.c:2941, 3433)
     if ((f2 & CH4_F2_LAGRANGE_SMALLTAUD) && (f2 & CH4_F2_LAGRANGE_SMALLTAUD_BETA) &&

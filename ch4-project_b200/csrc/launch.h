@@ -91,6 +91,10 @@ cudaError_t launch_particle_arrive(const PartParams<double>& P, const int* keep,
                                    int nd, const double* from_up, int nu, cudaStream_t st);
 cudaError_t launch_particle_arrive(const PartParams<float>& P, const int* keep, int nkeep, const double* from_down,
                                    int nd, const double* from_up, int nu, cudaStream_t st);
+// random re-entry through the y walls: the drawn x and z ([2][index]) into the particles
+// that re-entered in the last sub-step
+cudaError_t launch_particle_reinject(const PartParams<double>& P, const double* xz, cudaStream_t st);
+cudaError_t launch_particle_reinject(const PartParams<float>& P, const double* xz, cudaStream_t st);
 // two-way deposit into P.dep; `tmp`/`tmp_bytes` is CUB scratch (query with tmp == nullptr),
 // key2/order2 are the sort's output buffers
 // (stage 0: all; 1: the keys and records of the slab's own particles; 2: the sort and gather)

@@ -49,6 +49,9 @@ cudaError_t launch_particle_reorder(const PartParams<float>& P, unsigned int* ke
   return reorder_t<float>(P, key2, order2, tmp, tmp_bytes, sort, st);
 }
 cudaError_t launch_sism(const StepParams<float>& P, cudaStream_t st) { return sism_t<float>(P, st); }
+cudaError_t launch_particle_reinject(const PartParams<float>& P, const double* xz, cudaStream_t st) {
+  return reinject_t<float>(P, xz, st);
+}
 cudaError_t launch_particle_leave(const PartParams<float>& P, double* send_down, double* send_up, int cap, int* keep,
                                   int* counts, cudaStream_t st) {
   return leave_t<float>(P, send_down, send_up, cap, keep, counts, st);

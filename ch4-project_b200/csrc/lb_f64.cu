@@ -96,6 +96,9 @@ cudaError_t launch_particle_reorder(const PartParams<double>& P, unsigned int* k
   return reorder_t<double>(P, key2, order2, tmp, tmp_bytes, sort, st);
 }
 cudaError_t launch_sism(const StepParams<double>& P, cudaStream_t st) { return sism_t<double>(P, st); }
+cudaError_t launch_particle_reinject(const PartParams<double>& P, const double* xz, cudaStream_t st) {
+  return reinject_t<double>(P, xz, st);
+}
 cudaError_t launch_particle_leave(const PartParams<double>& P, double* send_down, double* send_up, int cap, int* keep,
                                   int* counts, cudaStream_t st) {
   return leave_t<double>(P, send_down, send_up, cap, keep, counts, st);

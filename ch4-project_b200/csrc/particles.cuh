@@ -111,6 +111,12 @@ struct PartParams {
   // high-pass (jump below the critical value); log(0.01) of the host libm
   int jump_flags;
   double log001;
+  // LAGRANGE_BC_INELASTIC_REINJECT without _NORANDOM: the sub-step records, by particle
+  // index, how many times each particle re-entered (0, 1, or 2 when the first re-entry lands
+  // on the opposite wall), and particle_reinject_kernel then puts in the random x and z the
+  // host drew from the handle's stream in particle order
+  int rj_random;
+  int* rj_count;
   // orientation noise (bit 0 rotational diffusion, bit 1 a random p every sub-step): per
   // particle index, the three gaussian draws xi and the random unit vector, drawn by the
   // host from the handle's drand48 stream in particle order for this sub-step
@@ -502,10 +508,11 @@ __device__ __forceinline__ void interp_lines(const PartParams<C>& P, const Stenc
 // Stokes settling velocity, halved (VELOCITY_STOKES_HALF) at the bottom wall only, and
 // the temperature of the wall it re-enters through.
 template <typename A>
-__device__ __forceinline__ void particle_walls(const PartParams<A>& P, double tau, double beta, double& x, double& y,
-                                               double& z, double& vx, double& vy, double& vz, double& tp) {
+__device__ __forceinline__ int particle_walls(const PartParams<A>& P, double tau, double beta, double& x, double& y,
+                                              double& z, double& vx, double& vy, double& vz, double& tp) {
   const double fac1 = P.inelastic ? 0.0 : -1.0, fac2 = P.inelastic ? 0.0 : 1.0;
   const double radius = 0.0, eps = (double)FLT_EPSILON;
+  int random_reentries = 0;
   if (P.fw & 2) {
 #pragma unroll
     for (int side = 0; side < 2; side++) {
@@ -543,9 +550,13 @@ __device__ __forceinline__ void particle_walls(const PartParams<A>& P, double ta
           vz /= 2.0;
         }
         if (P.lagr_temp) tp = side == 0 ? P.T_top : P.T_bot;
+        if (P.rj_random) random_reentries++;
       }
     }
   }
+  // a randomly re-entered particle's x and z are SX u, SZ u with u in [0, 1): inside the
+  // box, so the x and z walls leave it alone (its x and z are put in after the sub-step)
+  if (random_reentries > 0) return random_reentries;
   if (P.fw & 1) {
     if (x < radius) {
       x *= fac1;
@@ -574,6 +585,7 @@ __device__ __forceinline__ void particle_walls(const PartParams<A>& P, double ta
       if (vz > 0.0) vz *= fac1;
     }
   }
+  return 0;
 }
 
 // orientation of one particle (src/lagrange.c:3470-3752): Jeffery's equation
@@ -1016,7 +1028,10 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
     orient_particle(pf, np, ip, &gr[0][0], o, first, dtl, P.noise ? P.rnd + 6LL * P.pid[ip] : nullptr);
   }
   double tp = P.lagr_temp ? F(t_p) : 0.0;
-  if constexpr (HALO) particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp);
+  if constexpr (HALO) {
+    const int reentries = particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp);
+    if (P.rj_random) P.rj_count[P.pid[ip]] = reentries;
+  }
   F(vx) = vx;
   F(vy) = vy;
   F(vz) = vz;
@@ -1153,6 +1168,19 @@ __global__ void particle_leave_kernel(const PartParams<A> P, double* send_down, 
   double* b = (dir == 1 ? send_down : send_up) + MIG_HEAD + (long long)k * MIG_REC;
   b[0] = (double)P.pid[ip];
   for (int f = 0; f < PF_TOTAL; f++) b[1 + f] = P.pf[f * np + ip];
+}
+
+// random re-entry: the x and z the host drew (by particle index) for every particle that
+// re-entered in this sub-step
+template <typename A>
+__global__ void particle_reinject_kernel(const PartParams<A> P, const double* __restrict__ xz) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= P.np) return;
+  const int o = P.pid[ip];
+  if (P.rj_count[o] == 0) return;
+  const long long np = P.np;
+  P.pf[CH4_PF(x) * np + ip] = xz[2LL * o];
+  P.pf[CH4_PF(z) * np + ip] = xz[2LL * o + 1];
 }
 
 // the counts into the buffers' headers

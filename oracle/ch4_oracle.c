@@ -917,7 +917,7 @@ static void swim(const ch4o_state *s, ch4_particle *p, double dtl) {
  * VELOCITY_STOKES_HALF, at the bottom wall only, as the reference has it) and, with
  * LAGRANGE_TEMPERATURE, the temperature of the wall it
  * re-enters through. */
-static void particle_walls(const ch4o_state *s, ch4_particle *p) {
+static void particle_walls(ch4o_state *s, ch4_particle *p) {
   const ch4_config *c = &s->cfg;
   const uint64_t f2 = c->flags2;
   if (!fluid_bc(c)) return;
@@ -943,10 +943,15 @@ static void particle_walls(const ch4o_state *s, ch4_particle *p) {
         }
       }
       if (inel && reinj) {
+        /* without NORANDOM the particle re-enters at a random x and z (src/lagrange.c:
+         * 3811-3817, 3891-3898): two draws from the stream, x first */
+        const int rnd = !(f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_NORANDOM);
+        if (rnd) p->x = c->SX * myrand(s);
         if (side == 0)
           p->y += c->SY;
         else
           p->y -= (c->SY - flt_eps);
+        if (rnd) p->z = c->SZ * myrand(s);
         if (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT_VELOCITY_ZERO) {
           p->vx = 0.0;
           p->vy = 0.0;
@@ -995,7 +1000,7 @@ static void particle_walls(const ch4o_state *s, ch4_particle *p) {
   }
 }
 
-static void move_particle(const ch4o_state *s, ch4_particle *p, int first, double dtl) {
+static void move_particle(ch4o_state *s, ch4_particle *p, int first, double dtl) {
   if (s->tf) { /* time derivatives of t along the path, src/lagrange.c:2997-3010 */
     if (first) {
       p->t_old = p->t;

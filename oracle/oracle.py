@@ -172,6 +172,12 @@ FLAGSETS.update({
     "les_sism": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_KOLMOGOROV", "LB_FLUID_LES", "LB_FLUID_LES_SISM"],
     "les_kalman": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_POISEUILLE", "LB_FLUID_FORCING_KOLMOGOROV",
                    "LB_FLUID_BC_Y", "LB_FLUID_LES", "LB_FLUID_LES_SISM", "LB_FLUID_LES_SISM_KALMAN"],
+    # random re-injection through the y walls (two draws per re-injected particle), x walls too
+    "particles_rjr": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_FLUID_BC_X", "LB_TEMPERATURE",
+                      "LB_TEMPERATURE_BUOYANCY", "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP",
+                      "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY", "LAGRANGE_TEMPERATURE",
+                      "LAGRANGE_BC_INELASTIC", "LAGRANGE_BC_INELASTIC_REINJECT", "LAGRANGE_TWOWAY",
+                      "LAGRANGE_TWOWAY_MOMENTUM"],
     # run-and-tumble swimmers: jumps triggered by the shear rate, or (high-pass) by a low temperature
     "particles_jump": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
