@@ -129,6 +129,7 @@ FLAGS2 = {
     "LAGRANGE_ORIENTATION_ACTIVE_JUMP": 1 << 40,
     "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE": 1 << 41,
     "LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS": 1 << 42,
+    "LAGRANGE_ORIENTATION_BC": 1 << 43,
 }
 
 

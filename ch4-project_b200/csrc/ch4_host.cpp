@@ -159,7 +159,8 @@ const uint64_t SUPPORTED2 =
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SECONDORIENTATION | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_SELECTIVEORIENTATION |
     CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM | CH4_F2_FLUID_LES_SISM |
     CH4_F2_FLUID_LES_SISM_KALMAN | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP |
-    CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS;
+    CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS |
+    CH4_F2_LAGRANGE_ORIENTATION_BC;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -849,6 +850,7 @@ struct Engine : EngineBase {
     Q.rstride = pslab() ? np_all : np;
     Q.noise = noise();
     Q.rj_random = rj_random();
+    Q.orient_bc = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_BC) != 0;
     Q.rj_count = rj_count;
     Q.jump_flags = ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) ? 1 : 0) |
                    ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS) ? 2 : 0);
@@ -2234,6 +2236,7 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_ORIENTATION_ACTIVE_JUMP", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP},
       {"LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE},
       {"LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS},
+      {"LAGRANGE_ORIENTATION_BC", CH4_F2_LAGRANGE_ORIENTATION_BC},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2449,6 +2452,8 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
       if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
         return why = "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
       const uint64_t noise = CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM;
+      if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_BC) && !(c->flags & CH4_F_LAGRANGE_ORIENTATION))
+        return why = "LAGRANGE_ORIENTATION_BC needs LAGRANGE_ORIENTATION", CH4_ERR_UNSUPPORTED;
       if ((f2 & noise) && !(c->flags & CH4_F_LAGRANGE_ORIENTATION))
         return why = "LAGRANGE_ORIENTATION_DIFFUSION and _RANDOM need LAGRANGE_ORIENTATION", CH4_ERR_UNSUPPORTED;
       if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION) && !(c->flags & CH4_F_LAGRANGE_GRADIENT))

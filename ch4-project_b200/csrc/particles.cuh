@@ -117,6 +117,7 @@ struct PartParams {
   // host drew from the handle's stream in particle order
   int rj_random;
   int* rj_count;
+  int orient_bc;  // LAGRANGE_ORIENTATION_BC: p_y turned back into the cell at the y walls
   // orientation noise (bit 0 rotational diffusion, bit 1 a random p every sub-step): per
   // particle index, the three gaussian draws xi and the random unit vector, drawn by the
   // host from the handle's drand48 stream in particle order for this sub-step
@@ -509,7 +510,8 @@ __device__ __forceinline__ void interp_lines(const PartParams<C>& P, const Stenc
 // the temperature of the wall it re-enters through.
 template <typename A>
 __device__ __forceinline__ int particle_walls(const PartParams<A>& P, double tau, double beta, double& x, double& y,
-                                              double& z, double& vx, double& vy, double& vz, double& tp) {
+                                              double& z, double& vx, double& vy, double& vz, double& tp,
+                                              int& crossings) {
   const double fac1 = P.inelastic ? 0.0 : -1.0, fac2 = P.inelastic ? 0.0 : 1.0;
   const double radius = 0.0, eps = (double)FLT_EPSILON;
   int random_reentries = 0;
@@ -517,6 +519,7 @@ __device__ __forceinline__ int particle_walls(const PartParams<A>& P, double tau
 #pragma unroll
     for (int side = 0; side < 2; side++) {
       if (!(side == 0 ? y < radius : y >= P.SY - radius)) continue;
+      crossings |= 1 << side;
       if (!P.reinject) {
         if (side == 0) {
           y = fac1 * (y - radius) + radius;
@@ -1029,8 +1032,15 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
   }
   double tp = P.lagr_temp ? F(t_p) : 0.0;
   if constexpr (HALO) {
-    const int reentries = particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp);
+    int crossings = 0;
+    const int reentries = particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp, crossings);
     if (P.rj_random) P.rj_count[P.pid[ip]] = reentries;
+    if constexpr (ORIENT) {
+      if (P.orient_bc) {  // after the orientation update, src/lagrange.c:3866-3870, 3942-3946
+        if ((crossings & 1) && F(py) < 0.0) F(py) *= -1.0;
+        if ((crossings & 2) && F(py) > 0.0) F(py) *= -1.0;
+      }
+    }
   }
   F(vx) = vx;
   F(vy) = vy;

@@ -196,7 +196,10 @@ enum {
    * swim_velocity * exp(-time_from_jump / jump_time) */
   CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP = 1ull << 40,
   CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE = 1ull << 41,
-  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS = 1ull << 42
+  CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS = 1ull << 42,
+  /* orientation at the y walls, src/lagrange.c:3866-3870, 3942-3946: a particle crossing the
+   * bottom wall turns p_y upwards, one crossing the top wall downwards */
+  CH4_F2_LAGRANGE_ORIENTATION_BC = 1ull << 43
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */

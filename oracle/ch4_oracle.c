@@ -917,10 +917,11 @@ static void swim(const ch4o_state *s, ch4_particle *p, double dtl) {
  * VELOCITY_STOKES_HALF, at the bottom wall only, as the reference has it) and, with
  * LAGRANGE_TEMPERATURE, the temperature of the wall it
  * re-enters through. */
-static void particle_walls(ch4o_state *s, ch4_particle *p) {
+static int particle_walls(ch4o_state *s, ch4_particle *p) {
   const ch4_config *c = &s->cfg;
   const uint64_t f2 = c->flags2;
-  if (!fluid_bc(c)) return;
+  int crossings = 0; /* bit 0 the bottom y wall, bit 1 the top one */
+  if (!fluid_bc(c)) return 0;
   const int inel = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC) != 0, reinj = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) != 0;
   const double fac1 = inel ? 0.0 : -1.0, fac2 = inel ? 0.0 : 1.0;
   const double radius = 0.0;
@@ -929,6 +930,7 @@ static void particle_walls(ch4o_state *s, ch4_particle *p) {
     for (int side = 0; side < 2; side++) {
       const int crossed = side == 0 ? p->y < radius : p->y >= c->SY - radius;
       if (!crossed) continue;
+      crossings |= 1 << side;
       if (!reinj) {
         if (side == 0) {
           p->y = fac1 * (p->y - radius) + radius;
@@ -998,9 +1000,17 @@ static void particle_walls(ch4o_state *s, ch4_particle *p) {
       if (p->vz > 0.0) p->vz *= fac1;
     }
   }
+  return crossings;
 }
 
-static void move_particle(ch4o_state *s, ch4_particle *p, int first, double dtl) {
+/* LAGRANGE_ORIENTATION_BC (src/lagrange.c:3866-3870, 3942-3946): after the orientation
+ * update, a particle that crossed the bottom y wall turns p_y upwards, the top one downwards */
+static void orientation_bc(ch4_particle *p, int crossings) {
+  if ((crossings & 1) && p->py < 0.0) p->py *= -1.0;
+  if ((crossings & 2) && p->py > 0.0) p->py *= -1.0;
+}
+
+static int move_particle(ch4o_state *s, ch4_particle *p, int first, double dtl) {
   if (s->tf) { /* time derivatives of t along the path, src/lagrange.c:2997-3010 */
     if (first) {
       p->t_old = p->t;
@@ -1133,7 +1143,7 @@ static void move_particle(ch4o_state *s, ch4_particle *p, int first, double dtl)
       p->vz += fac1 * (-s->cfg.gravity_z - p->Dt_uz);
     }
   }
-  particle_walls(s, p);
+  const int crossings = particle_walls(s, p);
   if (s->cfg.flags2 & CH4_F2_LAGRANGE_TEMPERATURE) {
     /* particle temperature, src/lagrange.c:4007-4018: 1/tau_heat =
      * 2 kappa / (tau_drag nu cp_p (3 - beta)), T_p <- (T_p + fac1 T) exp(-fac1) */
@@ -1141,6 +1151,7 @@ static void move_particle(ch4o_state *s, ch4_particle *p, int first, double dtl)
     fac1 *= dtl;
     p->t_p = (p->t_p + fac1 * p->t) * exp(-fac1);
   }
+  return crossings;
 }
 
 /* sendrecv_particles on one rank (src/lagrange.c:4028-4221): LAGRANGE_WRAP puts
@@ -1657,9 +1668,10 @@ static void one_step(ch4o_state *s) {
       if (s->tf)
         for (int ip = 0; ip < s->npart; ip++) interp_particle_t(s, s->tf, &s->part[ip]);
       for (int ip = 0; ip < s->npart; ip++) {
-        move_particle(s, &s->part[ip], first, dtl);
+        const int crossings = move_particle(s, &s->part[ip], first, dtl);
         if (s->cfg.flags & CH4_F_LAGRANGE_ORIENTATION)
           orient_particle(s, &s->part[ip], (s->cfg.flags & CH4_F_LAGRANGE_ORIENTATION_JEFFREY) != 0, first, dtl);
+        if (s->cfg.flags2 & CH4_F2_LAGRANGE_ORIENTATION_BC) orientation_bc(&s->part[ip], crossings);
       }
       wrap_particles(s);
     }

@@ -178,6 +178,11 @@ FLAGSETS.update({
                       "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY", "LAGRANGE_TEMPERATURE",
                       "LAGRANGE_BC_INELASTIC", "LAGRANGE_BC_INELASTIC_REINJECT", "LAGRANGE_TWOWAY",
                       "LAGRANGE_TWOWAY_MOMENTUM"],
+    # elongated particles in convection whose orientation is turned back into the cell at the y walls
+    "particles_orbc": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+                       "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
+                       "LAGRANGE_GRAVITY", "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY",
+                       "LAGRANGE_ORIENTATION_BC"],
     # run-and-tumble swimmers: jumps triggered by the shear rate, or (high-pass) by a low temperature
     "particles_jump": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",

@@ -112,6 +112,10 @@ CASES = {
                           params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
                                       gravity_y=1e-3, gravity_x=2e-4, gravity_z=-1e-4, seed=19,
                                       time_dt_lagr_factor=2.0, particle_number=250)),
+    "particles_orbc": dict(flagset="particles_orbc", NX=9, NY=8, NZ=7, npart=250,
+                           params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
+                                       gravity_y=1e-3, gravity_x=2e-4, seed=20, time_dt_lagr_factor=2.0,
+                                       particle_number=250)),
     "particles_bc": dict(flagset="particles_bc", NX=9, NY=8, NZ=7, npart=250,
                          params=dict(tau_u=0.56, tau_t=0.6, Amp_x=2e-3, Amp_y=1.5e-3, Amp_z=1e-3, seed=18,
                                      T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.2, gravity_y=1e-3, gravity_x=3e-4,
