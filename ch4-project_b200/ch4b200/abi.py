@@ -130,6 +130,8 @@ FLAGS2 = {
     "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE": 1 << 41,
     "LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS": 1 << 42,
     "LAGRANGE_ORIENTATION_BC": 1 << 43,
+    "LAGRANGE_GRAVITY_VARIABLE": 1 << 44,
+    "LAGRANGE_BC_INELASTIC_SEDIMENT": 1 << 45,
 }
 
 
@@ -160,6 +162,7 @@ class Config(C.Structure):
         ("particle_types", C.c_int),
         ("nz_global", C.c_int), ("z_offset", C.c_int),
         ("flags2", C.c_uint64),
+        ("time_start", C.c_double),
     ]
 
 
@@ -177,6 +180,7 @@ PARTICLE_FIELDS = [
     "nx", "ny", "nz", "dt_nx", "dt_ny", "dt_nz", "gyrotaxis_velocity", "swim_velocity",
     "rotational_diffusion",
     "shear_rate", "critical_shear_rate", "time_from_jump", "jump_time", "px_jump", "py_jump", "pz_jump",
+    "gravity_coeff", "sediment",
 ]
 
 

@@ -160,7 +160,7 @@ const uint64_t SUPPORTED2 =
     CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM | CH4_F2_FLUID_LES_SISM |
     CH4_F2_FLUID_LES_SISM_KALMAN | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP |
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS |
-    CH4_F2_LAGRANGE_ORIENTATION_BC;
+    CH4_F2_LAGRANGE_ORIENTATION_BC | CH4_F2_LAGRANGE_GRAVITY_VARIABLE | CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -358,6 +358,7 @@ struct ch4_handle {
   double phi[NK][3];
   double hit_fac[NK];
   int itime = 0;
+  double time_now = 0.0;  // the step loop's clock: time_start + time_dt per step, summed (src/main.c:67)
   bool initialized = false;
   Lattice lat;
   // running rulers of ch4_dump_averages (ruler_*_running, src/output.c:765-768)
@@ -851,6 +852,8 @@ struct Engine : EngineBase {
     Q.noise = noise();
     Q.rj_random = rj_random();
     Q.orient_bc = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_BC) != 0;
+    Q.gravity_var = (c.flags2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) != 0;
+    Q.sediment = (c.flags2 & CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT) != 0;
     Q.rj_count = rj_count;
     Q.jump_flags = ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) ? 1 : 0) |
                    ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS) ? 2 : 0);
@@ -1840,6 +1843,7 @@ struct Engine : EngineBase {
         if (fmoments()) fm_i ^= 1;
         cur ^= 1;
         H->itime++;
+        H->time_now += c.time_dt;
         if (lagr()) {
           // u^{n+1} with dt/2 F^n, then the Lagrangian sub-steps (src/main.c:164-185)
           bind_pops(cur);
@@ -1852,6 +1856,7 @@ struct Engine : EngineBase {
             if (noise() && np > 0 && (st = draw_noise())) return st;
             PartParams<A> Q = part_params();
             Q.first = (n_step == 1 && c.resume == 0);
+            Q.time_now = H->time_now;
             if ((st = H->cuda(launch_particle_substep(Q, H->stream), "particle substep"))) return st;
             if (rj_random() && np > 0 && (st = reinject_random())) return st;
             if (pslab() && (st = migrate())) return st;  // move_particles ends with sendrecv_particles
@@ -2026,7 +2031,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   };
   double NX, NY, NZ, particle_number = 0, resume = 0, tau_drag_types = 1, beta_coeff_types = 1, cp_coeff_types = 1;
   double aspect_ratio_types = 1, gyrotaxis_velocity_types = 1, swim_velocity_types = 1, rotational_diffusion_types = 1;
-  double critical_shear_rate_types = 1, jump_time_types = 1;
+  double critical_shear_rate_types = 1, jump_time_types = 1, gravity_coeff_types = 1;
   const uint64_t fl = cfg->flags;
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
@@ -2074,6 +2079,9 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
            (cfg->flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP)},
       {"noise_u", &cfg->noise_u, (fl & CH4_F_FLUID_INITIAL_ADD_NOISE) != 0},  // src/parameters.c:216-220
       {"noise_t", &cfg->noise_t, T && (fl & CH4_F_TEMPERATURE_INITIAL_ADD_NOISE)},  // src/parameters.c:347-351
+      // gravity classes, src/parameters.c:590-602
+      {"gravity_coeff_types", &gravity_coeff_types,
+       (fl & CH4_F_LAGRANGE) && (fl & CH4_F_LAGRANGE_GRAVITY) && (cfg->flags2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE)},
   };
   for (auto& k : keys) {
     if (!k.needed) continue;
@@ -2092,7 +2100,10 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   cfg->resume = (int)resume;
   cfg->particle_types = (int)tau_drag_types * (int)beta_coeff_types * (int)cp_coeff_types * (int)aspect_ratio_types *
                         (int)gyrotaxis_velocity_types * (int)rotational_diffusion_types * (int)swim_velocity_types *
-                        (int)critical_shear_rate_types * (int)jump_time_types;
+                        (int)critical_shear_rate_types * (int)jump_time_types * (int)gravity_coeff_types;
+  // time_start (src/parameters.c:138-140); a file without it starts the clock at 0
+  double t0 = 0.0;
+  if (ch4_read_parameter(path, "time_start", &t0) == CH4_OK) cfg->time_start = t0;
   // derived values, src/parameters.c:156-160,233-240 (METHOD_STREAMING)
   cfg->nu = (cfg->tau_u - 0.5 * cfg->time_dt) / 3.0;
   cfg->kappa = (cfg->tau_t - 0.5 * cfg->time_dt) / 3.0;
@@ -2237,6 +2248,8 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE},
       {"LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS", CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS},
       {"LAGRANGE_ORIENTATION_BC", CH4_F2_LAGRANGE_ORIENTATION_BC},
+      {"LAGRANGE_GRAVITY_VARIABLE", CH4_F2_LAGRANGE_GRAVITY_VARIABLE},
+      {"LAGRANGE_BC_INELASTIC_SEDIMENT", CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation
@@ -2452,6 +2465,11 @@ static ch4_status validate(const ch4_config* c, std::string& why) {
       if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) && !(c->flags & CH4_F_LB_TEMPERATURE))
         return why = "LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE needs LB_TEMPERATURE", CH4_ERR_UNSUPPORTED;
       const uint64_t noise = CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM;
+      // the particle members exist only under their parent flags (src/typedef.h:403-407, 454-458)
+      if ((f2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) && !(c->flags & CH4_F_LAGRANGE_GRAVITY))
+        return why = "LAGRANGE_GRAVITY_VARIABLE needs LAGRANGE_GRAVITY", CH4_ERR_UNSUPPORTED;
+      if ((f2 & CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT) && !(f2 & CH4_F2_LAGRANGE_BC_INELASTIC))
+        return why = "LAGRANGE_BC_INELASTIC_SEDIMENT needs LAGRANGE_BC_INELASTIC", CH4_ERR_UNSUPPORTED;
       if ((f2 & CH4_F2_LAGRANGE_ORIENTATION_BC) && !(c->flags & CH4_F_LAGRANGE_ORIENTATION))
         return why = "LAGRANGE_ORIENTATION_BC needs LAGRANGE_ORIENTATION", CH4_ERR_UNSUPPORTED;
       if ((f2 & noise) && !(c->flags & CH4_F_LAGRANGE_ORIENTATION))
@@ -2492,6 +2510,7 @@ ch4_status ch4_create(const ch4_config* cfg, ch4_handle** out) {
   }
   auto* h = new ch4_handle();
   h->cfg = *cfg;
+  h->time_now = cfg->time_start;
   // srand48(seed) state (src/parallel.c:238-240 with a fixed seed)
   seed48_state(cfg->seed, h->rng);
   std::memset(h->phi, 0, sizeof h->phi);
@@ -3168,6 +3187,7 @@ std::vector<PField> lagrange_fields(uint64_t fl, uint64_t fl2, bool output_fluid
                            {"z", &P::z},       {"vx", &P::vx},             {"vy", &P::vy}, {"vz", &P::vz},
                            {"ax", &P::ax},     {"ay", &P::ay},             {"az", &P::az}};
   const bool grad = fl & CH4_F_LAGRANGE_GRADIENT, am = fl & CH4_F_LAGRANGE_ADDEDMASS;
+  if (fl2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) v.push_back({"gravity_coeff", &P::gravity_coeff});  // src/lagrange.c:1772-1780
   // the fluid-at-particle and orientation datasets sit inside the LAGRANGE_GRADIENT block
   // of output_particles (src/lagrange.c:1783-2014)
   if (grad) {
@@ -3191,6 +3211,7 @@ std::vector<PField> lagrange_fields(uint64_t fl, uint64_t fl2, bool output_fluid
     if (fl2 & CH4_F2_LAGRANGE_TEMPERATURE)  // src/lagrange.c:2090-2103
       v.insert(v.end(), {{"temperature_particle", &P::t_p}, {"cp_particle", &P::cp_p}});
   }
+  if (fl2 & CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT) v.push_back({"sediment", &P::sediment});  // src/lagrange.c:2105-2114
   return v;
 }
 
@@ -3206,6 +3227,7 @@ std::vector<PField> part_members(uint64_t fl, uint64_t fl2) {
   if (fl & CH4_F_LB_FLUID) {
     v.insert(v.end(), {{"ux", &P::ux}, {"uy", &P::uy}, {"uz", &P::uz}, {"ux_old", &P::ux_old},
                        {"uy_old", &P::uy_old}, {"uz_old", &P::uz_old}});
+    if (fl2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) v.push_back({"gravity_coeff", &P::gravity_coeff});  // src/lagrange.c:4336-4341
     if (fl & CH4_F_LAGRANGE_GRADIENT) {
       v.insert(v.end(), {{"dx_ux", &P::dx_ux}, {"dy_ux", &P::dy_ux}, {"dz_ux", &P::dz_ux}, {"dx_uy", &P::dx_uy},
                          {"dy_uy", &P::dy_uy}, {"dz_uy", &P::dz_uy}, {"dx_uz", &P::dx_uz}, {"dy_uz", &P::dy_uz},
@@ -3274,6 +3296,7 @@ bool write_particle_xmf(const std::string& path, const std::string& h5name, int 
   scalar("tau_drag");
   joined("velocity", "Vector", {"vx", "vy", "vz"});
   joined("acceleration", "Vector", {"ax", "ay", "az"});
+  if (fl2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) scalar("gravity_coeff");  // src/lagrange.c:2260-2268
   if (fl & CH4_F_LAGRANGE_GRADIENT) {  // src/lagrange.c:2271-2456
     joined("fluid velocity gradient", "Tensor",
            {"dx_ux", "dy_ux", "dz_ux", "dx_uy", "dy_uy", "dz_uy", "dx_uz", "dy_uz", "dz_uz"});
@@ -3312,6 +3335,7 @@ bool write_particle_xmf(const std::string& path, const std::string& h5name, int 
       scalar("cp_particle");
     }
   }
+  if (fl2 & CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT) scalar("sediment");  // src/lagrange.c:2532-2540
   std::fprintf(f, "<Time Value=\" %e\" />\n</Grid>\n</Domain>\n</Xdmf>\n", time_now);
   return std::fclose(f) == 0;
 }

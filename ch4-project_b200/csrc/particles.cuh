@@ -118,6 +118,9 @@ struct PartParams {
   int rj_random;
   int* rj_count;
   int orient_bc;  // LAGRANGE_ORIENTATION_BC: p_y turned back into the cell at the y walls
+  int gravity_var;  // LAGRANGE_GRAVITY_VARIABLE: gravity times the particle's gravity_coeff
+  int sediment;     // LAGRANGE_BC_INELASTIC_SEDIMENT: wall depositions recorded per particle
+  double time_now;  // the step loop's clock (the top wall's deposition time)
   // orientation noise (bit 0 rotational diffusion, bit 1 a random p every sub-step): per
   // particle index, the three gaussian draws xi and the random unit vector, drawn by the
   // host from the handle's drand48 stream in particle order for this sub-step
@@ -511,7 +514,7 @@ __device__ __forceinline__ void interp_lines(const PartParams<C>& P, const Stenc
 template <typename A>
 __device__ __forceinline__ int particle_walls(const PartParams<A>& P, double tau, double beta, double& x, double& y,
                                               double& z, double& vx, double& vy, double& vz, double& tp,
-                                              int& crossings) {
+                                              int& crossings, double gc, double& sed) {
   const double fac1 = P.inelastic ? 0.0 : -1.0, fac2 = P.inelastic ? 0.0 : 1.0;
   const double radius = 0.0, eps = (double)FLT_EPSILON;
   int random_reentries = 0;
@@ -543,9 +546,10 @@ __device__ __forceinline__ int particle_walls(const PartParams<A>& P, double tau
           vy = 0.0;
           vz = 0.0;
         } else {
-          vx = -P.g[0] * (1.0 - beta) * tau;
-          vy = -P.g[1] * (1.0 - beta) * tau;
-          vz = -P.g[2] * (1.0 - beta) * tau;
+          // gc = gravity_coeff, 1 without LAGRANGE_GRAVITY_VARIABLE (exact), src/lagrange.c:3824-3832
+          vx = -P.g[0] * gc * (1.0 - beta) * tau;
+          vy = -P.g[1] * gc * (1.0 - beta) * tau;
+          vz = -P.g[2] * gc * (1.0 - beta) * tau;
         }
         if (side == 0 && P.rj_half) {
           vx /= 2.0;
@@ -555,6 +559,9 @@ __device__ __forceinline__ int particle_walls(const PartParams<A>& P, double tau
         if (P.lagr_temp) tp = side == 0 ? P.T_top : P.T_bot;
         if (P.rj_random) random_reentries++;
       }
+      // depositions: counted at the bottom wall, the last one's time at the top wall
+      // (src/lagrange.c:3845-3863, 3920-3938)
+      if (P.sediment) sed = side == 0 ? sed + 1.0 : P.time_now;
     }
   }
   // a randomly re-entered particle's x and z are SX u, SZ u with u in [0, 1): inside the
@@ -933,13 +940,16 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
     F(uy_old) = uy;
     F(uz_old) = uz;
   }
+  // gravity_coeff; 1 without LAGRANGE_GRAVITY_VARIABLE, where c g and (-beta) c g equal g and
+  // (-beta) g exactly
+  const double gc = P.gravity_var ? F(gravity_coeff) : 1.0;
   if (tau > 0.0) {  // Stokes drag (+ added mass)
     const double invtau = 1.0 / tau;
     double ax = (ux - vx) * invtau, ay = (uy - vy) * invtau, az = (uz - vz) * invtau;
-    if (P.gravity) {  // -g, src/lagrange.c:3312-3323
-      ax -= P.g[0];
-      ay -= P.g[1];
-      az -= P.g[2];
+    if (P.gravity) {  // -c g, src/lagrange.c:3312-3323
+      ax -= gc * P.g[0];
+      ay -= gc * P.g[1];
+      az -= gc * P.g[2];
     }
     // Du/Dt of the added-mass term (the stored one where the term is off, as the
     // small-tau_drag models read it)
@@ -950,10 +960,10 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
       Dz = F(Dt_uz);
     }
     if (P.addedmass && beta != 0.0) {
-      if (P.gravity) {  // -(-beta) g, src/lagrange.c:3330-3339
-        ax -= (-beta) * P.g[0];
-        ay -= (-beta) * P.g[1];
-        az -= (-beta) * P.g[2];
+      if (P.gravity) {  // -(-beta) c g, src/lagrange.c:3330-3339
+        ax -= (-beta) * gc * P.g[0];
+        ay -= (-beta) * gc * P.g[1];
+        az -= (-beta) * gc * P.g[2];
       }
       double uxo = F(ux_old), uyo = F(uy_old), uzo = F(uz_old);
       if (first) {
@@ -1033,8 +1043,10 @@ __global__ void __launch_bounds__(128, sizeof(A) == 8 ? 2 : 4) particle_substep_
   double tp = P.lagr_temp ? F(t_p) : 0.0;
   if constexpr (HALO) {
     int crossings = 0;
-    const int reentries = particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp, crossings);
+    double sed = P.sediment ? F(sediment) : 0.0;
+    const int reentries = particle_walls(P, tau, beta, xn, yn, zn, vx, vy, vz, tp, crossings, gc, sed);
     if (P.rj_random) P.rj_count[P.pid[ip]] = reentries;
+    if (P.sediment) F(sediment) = sed;
     if constexpr (ORIENT) {
       if (P.orient_bc) {  // after the orientation update, src/lagrange.c:3866-3870, 3942-3946
         if ((crossings & 1) && F(py) < 0.0) F(py) *= -1.0;

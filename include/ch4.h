@@ -199,7 +199,9 @@ enum {
   CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS = 1ull << 42,
   /* orientation at the y walls, src/lagrange.c:3866-3870, 3942-3946: a particle crossing the
    * bottom wall turns p_y upwards, one crossing the top wall downwards */
-  CH4_F2_LAGRANGE_ORIENTATION_BC = 1ull << 43
+  CH4_F2_LAGRANGE_ORIENTATION_BC = 1ull << 43,
+  CH4_F2_LAGRANGE_GRAVITY_VARIABLE = 1ull << 44,
+  CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT = 1ull << 45
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */
@@ -256,6 +258,9 @@ typedef struct {
   int nz_global, z_offset;
   /* CH4_F2_* bits (the second word of define.h flags) */
   uint64_t flags2;
+  /* time_start of param.in (src/parameters.c:138-140): the step loop's clock starts there and
+   * advances by time_dt per step (src/main.c:67) */
+  double time_start;
 } ch4_config;
 
 /* One Lagrangian particle (the fields of point_particle, src/typedef.h:391-481,
@@ -291,6 +296,10 @@ typedef struct {
    * critical one, the time since the last jump, the jump's decay time and its direction */
   double shear_rate, critical_shear_rate, time_from_jump, jump_time;
   double px_jump, py_jump, pz_jump;
+  /* LAGRANGE_GRAVITY_VARIABLE: the factor on gravity of this particle (src/typedef.h:403-407);
+   * LAGRANGE_BC_INELASTIC_SEDIMENT: bottom-wall depositions counted, the time of the last top-wall
+   * one (src/typedef.h:454-458) */
+  double gravity_coeff, sediment;
 } ch4_particle;
 
 /* Global averages of dump_averages (src/output.c:63-~760), FP64 sums over the

@@ -62,6 +62,7 @@ struct ch4o_state {
   double hit_fac[NK];
   unsigned short rng[3];
   int itime, initialized;
+  double time_now; /* the step loop's clock, src/main.c:58,67 */
   /* constant force tables */
   double *kol_x, *kol_y, *kol_z; /* Kolmogorov: F.x(y), F.y(x), F.z(y) */
   double pois[3];
@@ -958,6 +959,10 @@ static int particle_walls(ch4o_state *s, ch4_particle *p) {
           p->vx = 0.0;
           p->vy = 0.0;
           p->vz = 0.0;
+        } else if (f2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) { /* src/lagrange.c:3824-3828 */
+          p->vx = -c->gravity_x * p->gravity_coeff * (1.0 - p->beta_coeff) * p->tau_drag;
+          p->vy = -c->gravity_y * p->gravity_coeff * (1.0 - p->beta_coeff) * p->tau_drag;
+          p->vz = -c->gravity_z * p->gravity_coeff * (1.0 - p->beta_coeff) * p->tau_drag;
         } else {
           p->vx = -c->gravity_x * (1.0 - p->beta_coeff) * p->tau_drag;
           p->vy = -c->gravity_y * (1.0 - p->beta_coeff) * p->tau_drag;
@@ -969,6 +974,14 @@ static int particle_walls(ch4o_state *s, ch4_particle *p) {
           p->vz /= 2.0;
         }
         if (f2 & CH4_F2_LAGRANGE_TEMPERATURE) p->t_p = side == 0 ? c->T_top : c->T_bot;
+      }
+      /* deposition count at the bottom wall, time of the last one at the top wall
+       * (src/lagrange.c:3845-3863, 3920-3938) */
+      if (inel && (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT)) {
+        if (side == 0)
+          p->sediment += 1.0;
+        else
+          p->sediment = s->time_now;
       }
     }
   }
@@ -1060,13 +1073,24 @@ static int move_particle(ch4o_state *s, ch4_particle *p, int first, double dtl) 
     p->ax = (p->ux - p->vx) * invtau;
     p->ay = (p->uy - p->vy) * invtau;
     p->az = (p->uz - p->vz) * invtau;
+    const int gvar = (s->cfg.flags2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) != 0;
     if (s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) { /* -g, src/lagrange.c:3312-3323 */
-      p->ax -= s->cfg.gravity_x;
-      p->ay -= s->cfg.gravity_y;
-      p->az -= s->cfg.gravity_z;
+      if (gvar) {
+        p->ax -= p->gravity_coeff * s->cfg.gravity_x;
+        p->ay -= p->gravity_coeff * s->cfg.gravity_y;
+        p->az -= p->gravity_coeff * s->cfg.gravity_z;
+      } else {
+        p->ax -= s->cfg.gravity_x;
+        p->ay -= s->cfg.gravity_y;
+        p->az -= s->cfg.gravity_z;
+      }
     }
     if ((s->cfg.flags & CH4_F_LAGRANGE_ADDEDMASS) && p->beta_coeff != 0.0) {
-      if (s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) { /* -(-beta) g, src/lagrange.c:3330-3339 */
+      if ((s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) && gvar) { /* -(-beta) c g, src/lagrange.c:3330-3335 */
+        p->ax -= (-(p->beta_coeff)) * p->gravity_coeff * s->cfg.gravity_x;
+        p->ay -= (-(p->beta_coeff)) * p->gravity_coeff * s->cfg.gravity_y;
+        p->az -= (-(p->beta_coeff)) * p->gravity_coeff * s->cfg.gravity_z;
+      } else if (s->cfg.flags & CH4_F_LAGRANGE_GRAVITY) { /* -(-beta) g, src/lagrange.c:3336-3339 */
         p->ax -= (-(p->beta_coeff)) * s->cfg.gravity_x;
         p->ay -= (-(p->beta_coeff)) * s->cfg.gravity_y;
         p->az -= (-(p->beta_coeff)) * s->cfg.gravity_z;
@@ -1415,6 +1439,7 @@ static void one_step(ch4o_state *s) {
   const int forcing = (c->flags & CH4_F_LB_FLUID_FORCING) != 0;
   const double hdt = 0.5 * c->time_dt;
   s->itime++;
+  s->time_now += c->time_dt;
 
   /* build_forcing phase update (src/forcing.c:36-79) */
   if (c->flags & CH4_F_FORCING_HIT) {
@@ -1682,6 +1707,7 @@ int ch4o_create(const ch4_config *cfg, ch4o_state **out) {
   if (!cfg || !out || cfg->NX <= 0 || cfg->NY <= 0 || cfg->NZ <= 0) return CH4_ERR_ARG;
   ch4o_state *s = (ch4o_state *)calloc(1, sizeof(ch4o_state));
   s->cfg = *cfg;
+  s->time_now = cfg->time_start;
   s->fm_cur[3] = s->fm_cur[4] = s->fm_cur[5] = 1.0;
   s->fm_prev[3] = s->fm_prev[4] = s->fm_prev[5] = 1.0;
   s->NX = cfg->NX;

@@ -110,6 +110,12 @@ static void write_part_layout(void) {
 #endif
 #endif
 #endif
+#if defined(LAGRANGE_GRAVITY) && defined(LAGRANGE_GRAVITY_VARIABLE)
+  F(gravity_coeff);
+#endif
+#if defined(LAGRANGE_BC_INELASTIC) && defined(LAGRANGE_BC_INELASTIC_SEDIMENT)
+  F(sediment);
+#endif
 #ifdef LB_TEMPERATURE
   F(t); F(t_old); F(dt_t); F(Dt_t);
 #ifdef LAGRANGE_GRADIENT

@@ -183,6 +183,12 @@ FLAGSETS.update({
                        "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
                        "LAGRANGE_GRAVITY", "LAGRANGE_ORIENTATION", "LAGRANGE_ORIENTATION_JEFFREY",
                        "LAGRANGE_ORIENTATION_BC"],
+    # inelastic y walls that record depositions (count at the bottom, time at the top), gravity
+    # scaled per particle
+    "particles_sed": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+                      "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
+                      "LAGRANGE_GRAVITY", "LAGRANGE_GRAVITY_VARIABLE", "LAGRANGE_BC_INELASTIC",
+                      "LAGRANGE_BC_INELASTIC_SEDIMENT", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
     # run-and-tumble swimmers: jumps triggered by the shear rate, or (high-pass) by a low temperature
     "particles_jump": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
@@ -255,7 +261,7 @@ PARAM_KEYS = ["resume", "resume_u", "resume_t", "resume_s", "NX", "NY", "NZ", "S
 
 def write_param_in(path, cfg, nsteps=1, overrides=None):
     vals = {"resume": int(cfg.resume), "resume_u": 0, "resume_t": 0, "resume_s": 0,
-            "time_start": 0.0, "time_end": float(nsteps), "time_dump_field": 1e12,
+            "time_start": float(cfg.time_start), "time_end": float(cfg.time_start) + float(nsteps), "time_dump_field": 1e12,
             "time_dump_diagn": 1e12, "time_dump_lagr": 1e12,
             "tau_drag_types": max(1, int(cfg.particle_types)), "tau_drag_min": 1.0, "tau_drag_max": 1.0,
             "beta_coeff_types": 1, "beta_coeff_min": 1.0, "beta_coeff_max": 1.0}
@@ -273,6 +279,9 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
         for key in ("critical_shear_rate", "jump_time"):
             keys += [key + "_types", key + "_min", key + "_max"]
             vals.update({key + "_types": 1, key + "_min": 1.0, key + "_max": 1.0})
+    if int(cfg.flags2) & abi.FLAGS2["LAGRANGE_GRAVITY_VARIABLE"]:  # src/parameters.c:590-602
+        keys += ["gravity_coeff_types", "gravity_coeff_min", "gravity_coeff_max"]
+        vals.update({"gravity_coeff_types": 1, "gravity_coeff_min": 1.0, "gravity_coeff_max": 1.0})
     if int(cfg.flags) & abi.FLAGS["LB_TEMPERATURE_FORCING"]:  # src/parameters.c: the source amplitude
         keys += ["Amp_t"]
         vals.update({"Amp_t": 0.0})

@@ -31,6 +31,7 @@ for name in sys.argv[1:] or sorted(CASES):
         if "t_p" in ref["part"]:
             temperature += ("t_p",)
         orientation = tuple(f for f in ("px", "py", "pz", "dt_px", "nx", "ny", "nz", "dt_nx") if f in ref["part"])
+        orientation += tuple(f for f in ("sediment",) if f in ref["part"])
         for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux") + temperature + orientation:
             out["out_part_" + f] = ref["part"][f]
     for k, v in pop_items(state):

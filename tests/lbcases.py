@@ -112,6 +112,10 @@ CASES = {
                           params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
                                       gravity_y=1e-3, gravity_x=2e-4, gravity_z=-1e-4, seed=19,
                                       time_dt_lagr_factor=2.0, particle_number=250)),
+    "particles_sed": dict(flagset="particles_sed", NX=9, NY=8, NZ=7, npart=250,
+                          params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
+                                      gravity_y=1e-3, gravity_x=2e-4, seed=21, time_dt_lagr_factor=2.0,
+                                      particle_number=250, time_start=2.5)),
     "particles_orbc": dict(flagset="particles_orbc", NX=9, NY=8, NZ=7, npart=250,
                            params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
                                        gravity_y=1e-3, gravity_x=2e-4, seed=20, time_dt_lagr_factor=2.0,
@@ -260,6 +264,10 @@ def make_case(name, seed=0, storage=0, dims=None, **over):
         if "LAGRANGE_ORIENTATION_DIFFUSION" in flags:  # 0 for some: their p is still normalised
             for i, p in enumerate(state["part"]):
                 p.rotational_diffusion = [0.0, 0.01, 0.1, 0.002][(i // 2) % 4]
+        if "LAGRANGE_GRAVITY_VARIABLE" in flags:  # gravity off, scaled down and up; earlier depositions
+            for i, p in enumerate(state["part"]):
+                p.gravity_coeff = [1.0, 0.0, 0.3, 2.5][i % 4]
+                p.sediment = [0.0, 0.0, 3.0, 1.25][(i // 4) % 4]
     return c["flagset"], cfg, state
 
 

@@ -35,7 +35,8 @@ def _assert_same(a, b, what):
                                           ("particles_swims", 8), ("particles_swimn", 8), ("particles_rdiff", 8),
                                           ("particles_rand", 8), ("les_sism", 20), ("les_kalman", 20),
                                           ("particles_jump", 8), ("particles_jumpt", 8),
-                                          ("particles_rjr", 8), ("particles_orbc", 8)])
+                                          ("particles_rjr", 8), ("particles_orbc", 8),
+                                          ("particles_sed", 8)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
@@ -89,7 +90,7 @@ def test_restatement_matches_golden_fixture(name):
     for k, _ in pop_items(state):
         _assert_same(mine[k], g["out_" + k], k)
     for f in ("x", "y", "z", "vx", "vy", "vz", "ux", "Dt_ux", "t", "dt_t", "Dt_t", "dx_t", "t_p", "px", "py", "pz",
-              "dt_px", "nx", "ny", "nz", "dt_nx"):
+              "dt_px", "nx", "ny", "nz", "dt_nx", "sediment"):
         if "out_part_" + f in g.files:
             _assert_same(mine["part"][f], g["out_part_" + f], "particle " + f)
     for k in ("u", "t", "s", "phi"):
