@@ -132,6 +132,8 @@ FLAGS2 = {
     "LAGRANGE_ORIENTATION_BC": 1 << 43,
     "LAGRANGE_GRAVITY_VARIABLE": 1 << 44,
     "LAGRANGE_BC_INELASTIC_SEDIMENT": 1 << 45,
+    "LAGRANGE_RADIUSandDENSITY": 1 << 46,
+    "LAGRANGE_BC_RADIUSandDENSITY": 1 << 47,
 }
 
 

@@ -160,7 +160,8 @@ const uint64_t SUPPORTED2 =
     CH4_F2_LAGRANGE_ORIENTATION_DIFFUSION | CH4_F2_LAGRANGE_ORIENTATION_RANDOM | CH4_F2_FLUID_LES_SISM |
     CH4_F2_FLUID_LES_SISM_KALMAN | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP |
     CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE | CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS |
-    CH4_F2_LAGRANGE_ORIENTATION_BC | CH4_F2_LAGRANGE_GRAVITY_VARIABLE | CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT;
+    CH4_F2_LAGRANGE_ORIENTATION_BC | CH4_F2_LAGRANGE_GRAVITY_VARIABLE | CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT |
+    CH4_F2_LAGRANGE_RADIUSandDENSITY | CH4_F2_LAGRANGE_BC_RADIUSandDENSITY;
 
 // drand48 of the reference (SYSTEM_RANDOM48, src/random.c:4-16) on an explicit state
 inline double myrand48(unsigned short st[3]) { return erand48(st); }
@@ -854,6 +855,8 @@ struct Engine : EngineBase {
     Q.orient_bc = (c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_BC) != 0;
     Q.gravity_var = (c.flags2 & CH4_F2_LAGRANGE_GRAVITY_VARIABLE) != 0;
     Q.sediment = (c.flags2 & CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT) != 0;
+    Q.wall_radius = (c.flags2 & CH4_F2_LAGRANGE_BC_RADIUSandDENSITY) && (c.flags2 & CH4_F2_LAGRANGE_RADIUSandDENSITY) &&
+                    (c.flags & CH4_F_LAGRANGE_ADDEDMASS);
     Q.rj_count = rj_count;
     Q.jump_flags = ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_TEMPERATURE) ? 1 : 0) |
                    ((c.flags2 & CH4_F2_LAGRANGE_ORIENTATION_ACTIVE_JUMP_HIGHPASS) ? 2 : 0);
@@ -2036,6 +2039,7 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
   const bool T = fl & CH4_F_LB_TEMPERATURE, S = fl & CH4_F_LB_SCALAR;
   const bool forcing = fl & CH4_F_LB_FLUID_FORCING;
   const bool orient = (fl & CH4_F_LAGRANGE_GRADIENT) && (fl & CH4_F_LAGRANGE_ORIENTATION);
+  const bool rad = (cfg->flags2 & CH4_F2_LAGRANGE_RADIUSandDENSITY) != 0;
   // gravity_x/y/z (src/parameters.c:234-241, with LB_FLUID_FORCING_GRAVITY): read where
   // buoyancy, the particles' gravity, their Stokes re-injection or a small-tau_drag model uses it
   const bool grav = (forcing && (fl & (CH4_F_TEMPERATURE_BUOYANCY | CH4_F_SCALAR_BUOYANCY))) ||
@@ -2056,9 +2060,12 @@ ch4_status ch4_config_read_param(ch4_config* cfg, const char* path, char* bad, s
       {"time_dt_lagr_factor", &cfg->time_dt_lagr_factor, (fl & CH4_F_LAGRANGE) != 0},
       {"particle_number", &particle_number, (fl & CH4_F_LAGRANGE) != 0},
       // particle types of the Lagrangian averages, src/parameters.c:556-586
-      {"tau_drag_types", &tau_drag_types, (fl & CH4_F_LAGRANGE) != 0},
+      // with LAGRANGE_RADIUSandDENSITY the classes are radii and densities instead (src/parameters.c:530-556)
+      {"tau_drag_types", &tau_drag_types, (fl & CH4_F_LAGRANGE) && !rad},
       {"beta_coeff_types", &beta_coeff_types,
-       (fl & CH4_F_LAGRANGE) && (fl & CH4_F_LAGRANGE_GRADIENT) && (fl & CH4_F_LAGRANGE_ADDEDMASS)},
+       (fl & CH4_F_LAGRANGE) && !rad && (fl & CH4_F_LAGRANGE_GRADIENT) && (fl & CH4_F_LAGRANGE_ADDEDMASS)},
+      {"particle_radius_types", &tau_drag_types, (fl & CH4_F_LAGRANGE) && rad},
+      {"particle_density_types", &beta_coeff_types, (fl & CH4_F_LAGRANGE) && rad},
       // LAGRANGE_TEMPERATURE multiplies the types by the specific-heat classes, src/parameters.c:606-618
       {"cp_coeff_types", &cp_coeff_types, (fl & CH4_F_LAGRANGE) && (cfg->flags2 & CH4_F2_LAGRANGE_TEMPERATURE)},
       // ... and the orientation classes, src/parameters.c:620-696 (under LAGRANGE_GRADIENT and
@@ -2250,6 +2257,8 @@ ch4_status ch4_config_read_define(ch4_config* cfg, const char* path, char* bad, 
       {"LAGRANGE_ORIENTATION_BC", CH4_F2_LAGRANGE_ORIENTATION_BC},
       {"LAGRANGE_GRAVITY_VARIABLE", CH4_F2_LAGRANGE_GRAVITY_VARIABLE},
       {"LAGRANGE_BC_INELASTIC_SEDIMENT", CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT},
+      {"LAGRANGE_RADIUSandDENSITY", CH4_F2_LAGRANGE_RADIUSandDENSITY},
+      {"LAGRANGE_BC_RADIUSandDENSITY", CH4_F2_LAGRANGE_BC_RADIUSandDENSITY},
   };
   // flags that select the configuration the hot path already is, or that only
   // concern I/O, timing, debugging or initial-state generation

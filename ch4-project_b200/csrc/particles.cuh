@@ -121,6 +121,7 @@ struct PartParams {
   int gravity_var;  // LAGRANGE_GRAVITY_VARIABLE: gravity times the particle's gravity_coeff
   int sediment;     // LAGRANGE_BC_INELASTIC_SEDIMENT: wall depositions recorded per particle
   double time_now;  // the step loop's clock (the top wall's deposition time)
+  int wall_radius;  // LAGRANGE_BC_RADIUSandDENSITY: walls met at the particle's radius
   // orientation noise (bit 0 rotational diffusion, bit 1 a random p every sub-step): per
   // particle index, the three gaussian draws xi and the random unit vector, drawn by the
   // host from the handle's drand48 stream in particle order for this sub-step
@@ -516,7 +517,8 @@ __device__ __forceinline__ int particle_walls(const PartParams<A>& P, double tau
                                               double& z, double& vx, double& vy, double& vz, double& tp,
                                               int& crossings, double gc, double& sed) {
   const double fac1 = P.inelastic ? 0.0 : -1.0, fac2 = P.inelastic ? 0.0 : 1.0;
-  const double radius = 0.0, eps = (double)FLT_EPSILON;
+  // the radius from tau = r^2 / (3 beta nu), src/lagrange.c:3777-3790; 0 otherwise
+  const double radius = P.wall_radius ? sqrt(tau * P.nu * 3.0 * beta) : 0.0, eps = (double)FLT_EPSILON;
   int random_reentries = 0;
   if (P.fw & 2) {
 #pragma unroll

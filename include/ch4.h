@@ -201,7 +201,12 @@ enum {
    * bottom wall turns p_y upwards, one crossing the top wall downwards */
   CH4_F2_LAGRANGE_ORIENTATION_BC = 1ull << 43,
   CH4_F2_LAGRANGE_GRAVITY_VARIABLE = 1ull << 44,
-  CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT = 1ull << 45
+  CH4_F2_LAGRANGE_BC_INELASTIC_SEDIMENT = 1ull << 45,
+  /* particle types by radius and density (src/parameters.c:530-556; the types are the caller's
+   * particles) and, with LAGRANGE_BC_RADIUSandDENSITY and LAGRANGE_ADDEDMASS, walls that a
+   * particle touches at its radius sqrt(3 nu tau_drag beta) (src/lagrange.c:3777-3790) */
+  CH4_F2_LAGRANGE_RADIUSandDENSITY = 1ull << 46,
+  CH4_F2_LAGRANGE_BC_RADIUSandDENSITY = 1ull << 47
 };
 
 /* Buoyancy reference temperature T0 (src/forcing.c:622-637). */

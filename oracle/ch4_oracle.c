@@ -925,7 +925,11 @@ static int particle_walls(ch4o_state *s, ch4_particle *p) {
   if (!fluid_bc(c)) return 0;
   const int inel = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC) != 0, reinj = (f2 & CH4_F2_LAGRANGE_BC_INELASTIC_REINJECT) != 0;
   const double fac1 = inel ? 0.0 : -1.0, fac2 = inel ? 0.0 : 1.0;
-  const double radius = 0.0;
+  /* the radius from tau = r^2 / (3 beta nu) (src/lagrange.c:3777-3790), else 0 */
+  const double radius = ((f2 & CH4_F2_LAGRANGE_BC_RADIUSandDENSITY) && (f2 & CH4_F2_LAGRANGE_RADIUSandDENSITY) &&
+                         (c->flags & CH4_F_LAGRANGE_ADDEDMASS))
+                            ? sqrt(p->tau_drag * c->nu * 3.0 * p->beta_coeff)
+                            : 0.0;
   const double flt_eps = (double)FLT_EPSILON;
   if (c->flags & CH4_F_FLUID_BC_Y) {
     for (int side = 0; side < 2; side++) {

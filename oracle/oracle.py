@@ -189,6 +189,11 @@ FLAGSETS.update({
                       "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
                       "LAGRANGE_GRAVITY", "LAGRANGE_GRAVITY_VARIABLE", "LAGRANGE_BC_INELASTIC",
                       "LAGRANGE_BC_INELASTIC_SEDIMENT", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
+    # particles that meet the elastic y walls at their radius sqrt(3 nu tau beta)
+    "particles_rad": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_BC_Y", "LB_TEMPERATURE", "LB_TEMPERATURE_BUOYANCY",
+                      "LB_TEMPERATURE_BC_Y", "LAGRANGE", "LAGRANGE_WRAP", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS",
+                      "LAGRANGE_GRAVITY", "LAGRANGE_RADIUSandDENSITY", "LAGRANGE_BC_RADIUSandDENSITY",
+                      "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM"],
     # run-and-tumble swimmers: jumps triggered by the shear rate, or (high-pass) by a low temperature
     "particles_jump": ["LB_FLUID", "LB_FLUID_FORCING", "LB_FLUID_FORCING_HIT", "LAGRANGE", "LAGRANGE_WRAP",
                        "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_TWOWAY", "LAGRANGE_TWOWAY_MOMENTUM",
@@ -279,6 +284,11 @@ def write_param_in(path, cfg, nsteps=1, overrides=None):
         for key in ("critical_shear_rate", "jump_time"):
             keys += [key + "_types", key + "_min", key + "_max"]
             vals.update({key + "_types": 1, key + "_min": 1.0, key + "_max": 1.0})
+    if int(cfg.flags2) & abi.FLAGS2["LAGRANGE_RADIUSandDENSITY"]:  # src/parameters.c:530-553
+        keys += ["particle_radius_types", "particle_radius_min", "particle_radius_max",
+                 "particle_density_types", "particle_density_min", "particle_density_max"]
+        vals.update({"particle_radius_types": 1, "particle_radius_min": 1.0, "particle_radius_max": 1.0,
+                     "particle_density_types": 1, "particle_density_min": 1.0, "particle_density_max": 1.0})
     if int(cfg.flags2) & abi.FLAGS2["LAGRANGE_GRAVITY_VARIABLE"]:  # src/parameters.c:590-602
         keys += ["gravity_coeff_types", "gravity_coeff_min", "gravity_coeff_max"]
         vals.update({"gravity_coeff_types": 1, "gravity_coeff_min": 1.0, "gravity_coeff_max": 1.0})

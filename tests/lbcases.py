@@ -116,6 +116,10 @@ CASES = {
                           params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
                                       gravity_y=1e-3, gravity_x=2e-4, seed=21, time_dt_lagr_factor=2.0,
                                       particle_number=250, time_start=2.5)),
+    "particles_rad": dict(flagset="particles_rad", NX=9, NY=8, NZ=7, npart=250,
+                          params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
+                                      gravity_y=1e-3, gravity_x=2e-4, seed=22, time_dt_lagr_factor=2.0,
+                                      particle_number=250)),
     "particles_orbc": dict(flagset="particles_orbc", NX=9, NY=8, NZ=7, npart=250,
                            params=dict(tau_u=0.56, tau_t=0.6, T_bot=1.0, T_top=0.0, T_ref=0.5, beta_t=0.3,
                                        gravity_y=1e-3, gravity_x=2e-4, seed=20, time_dt_lagr_factor=2.0,

@@ -57,7 +57,7 @@ def rel_l2(a, b):
                                           ("particles_swims", 12), ("particles_swimn", 12), ("particles_rdiff", 12),
                                           ("particles_rand", 12), ("les_sism", 25), ("les_kalman", 25),
                                           ("particles_rjr", 12), ("particles_orbc", 12),
-                                          ("particles_sed", 12)])
+                                          ("particles_sed", 12), ("particles_rad", 12)])
 def test_fp64_bit_identical_to_oracle(name, nsteps):
     _, cfg, state = make_case(name, seed=11)
     ref = run_restatement(cfg, state, nsteps)
@@ -86,7 +86,7 @@ def test_fp64_bit_identical_to_oracle(name, nsteps):
                                   "particles_reinj", "particles_bc", "particles_or2", "particles_swimt",
                                   "particles_swimb", "particles_swims", "particles_swimn", "particles_rdiff",
                                   "particles_rand", "les_sism", "les_kalman", "particles_rjr", "particles_orbc",
-                                  "particles_sed"])
+                                  "particles_sed", "particles_rad"])
 def test_fp64_matches_compiled_reference(name):
     flagset, cfg, state = make_case(name, seed=5)
     if not O.ref_available(flagset):

@@ -36,7 +36,7 @@ def _assert_same(a, b, what):
                                           ("particles_rand", 8), ("les_sism", 20), ("les_kalman", 20),
                                           ("particles_jump", 8), ("particles_jumpt", 8),
                                           ("particles_rjr", 8), ("particles_orbc", 8),
-                                          ("particles_sed", 8)])
+                                          ("particles_sed", 8), ("particles_rad", 8)])
 def test_restatement_matches_compiled_reference(name, nsteps):
     flagset, cfg, state = make_case(name, seed=3)
     if not O.ref_available(flagset):
