@@ -130,7 +130,7 @@ def test_slip_wall_beside_another_wall_is_refused(names):
 
 def test_particle_wall_and_small_tau_flags_are_read_from_define_h(tmp_path):
     """The particles' wall rules and small-tau_drag models are flags of the second word;
-    random re-injection (the reference's drand48 stream) is refused at create."""
+    the beta small-tau_drag model without added mass and gradients is refused at create."""
     import ctypes as C
     d = tmp_path / "define.h"
     d.write_text("#define GRID_POP_D3Q19\n#define METHOD_STREAMING\n#define LB_FLUID\n#define LB_FLUID_BC\n"
@@ -146,3 +146,32 @@ def test_particle_wall_and_small_tau_flags_are_read_from_define_h(tmp_path):
     c.tau_u, c.time_dt, c.time_dt_lagr_factor = 0.6, 1.0, 1.0
     h = C.c_void_p()
     assert ch4b200.lib().ch4_create(C.byref(c), C.byref(h)) == abi.ERR_UNSUPPORTED and not h.value
+
+
+@pytest.mark.parametrize("flagset", ["particles_orbc", "particles_sed", "particles_rad"])
+def test_particle_wall_variants_read_from_the_oracle_define_h(flagset):
+    """The define.h of each particle-wall variant gives the flag words the oracle runs."""
+    import oracle as O
+    c = ch4b200.default_config()
+    ch4b200.read_define(c, os.path.join(REPO, "oracle", "configs", flagset + ".h"))
+    names = O.FLAGSETS[flagset]
+    assert all(abi.has_flag(c, n) for n in names)
+    assert int(c.flags2) & ~sum(abi.FLAGS2[n] for n in names if n in abi.FLAGS2) == 0
+
+
+def test_param_reader_radius_density_types_and_time_start(tmp_path):
+    """LAGRANGE_RADIUSandDENSITY counts the types by radius and density instead of tau_drag and
+    beta (src/parameters.c:530-556); GRAVITY_VARIABLE multiplies them by the gravity classes
+    (src/parameters.c:590-602); time_start starts the step clock (src/parameters.c:138-140)."""
+    p = tmp_path / "param.in"
+    p.write_text("resume 0\nNX 8\nNY 8\nNZ 8\nSX 8\nSY 8\nSZ 8\ntime_dt 1.0\ntime_start 2.5\ntau_u 0.6\n"
+                 "gravity_x 0\ngravity_y 1e-3\ngravity_z 0\ntime_dt_lagr_factor 1\nparticle_number 10\n"
+                 "tau_drag_types 7\nbeta_coeff_types 5\nparticle_radius_types 2\nparticle_density_types 3\n"
+                 "gravity_coeff_types 4\n")
+    c = ch4b200.default_config()
+    c.flags = abi.flags_of(["LB_FLUID", "LAGRANGE", "LAGRANGE_GRADIENT", "LAGRANGE_ADDEDMASS", "LAGRANGE_GRAVITY"])
+    ch4b200.read_param(c, str(p))
+    assert c.particle_types == 7 * 5 and c.time_start == 2.5
+    c.flags2 = abi.FLAGS2["LAGRANGE_RADIUSandDENSITY"] | abi.FLAGS2["LAGRANGE_GRAVITY_VARIABLE"]
+    ch4b200.read_param(c, str(p))
+    assert c.particle_types == 2 * 3 * 4
